@@ -1,0 +1,297 @@
+// C-ABI entry points (include/dsmsgt.h) and the batch driver shared by the
+// SH and PSV engines.
+//
+// One call of dsm_run_freqs replaces, for every requested frequency index,
+// one pass of the reference's omega loop (src/SGTsh/SGTsh-MPI.f90:389-613,
+// src/SGTpsv/SGTpsv-MPI.f90:535-1152) minus the file writes.  Frequencies are
+// processed in batches of F.  For a batch the driver
+//   1. builds the per-omega operator pieces          (mode kernel)
+//   2. solves chunks of Lc angular orders of every frequency of the batch at
+//      once, then runs the reference's cutoff test on the device; chunks
+//      continue until every frequency has met its cutoff (the test is the
+//      reference's, evaluated in the same order, so the number of orders
+//      summed is the reference's llog)
+//   3. contracts the per-order receiver fields with the vector-harmonic
+//      tables over l (one GEMM per frequency and |m|)
+//   4. turns the contractions into TSGT/RSGT/SYNN (mode epilogue kernel)
+//   5. packs complex64 catalogue records when asked.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+#include "engine.cuh"
+
+namespace dsm {
+
+void Engine::init_common(int dev) {
+    DSM_CUDA(cudaSetDevice(dev));
+    DSM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    DSM_CUBLAS(cublasCreate(&cub));
+    DSM_CUBLAS(cublasSetStream(cub, st));
+    for (auto& e : ev) DSM_CUDA(cudaEventCreate(&e));
+}
+
+Engine::~Engine() {
+    if (st) cudaStreamSynchronize(st);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (cub) cublasDestroy(cub);
+    if (st) cudaStreamDestroy(st);
+}
+
+void Engine::build_basis(int lneed) {
+    if (lneed <= lcapB) return;
+    int cap = std::max(lcapB, 1024);
+    while (cap < lneed) cap *= 2;
+    cap = std::min(cap, maxlmax + 1);
+    if (cap < lneed) cap = lneed;
+    launch_basis_tables(*this, cap);
+}
+
+void Engine::build_weights(const double* d_r, const double* d_rrsta) {
+    launch_interp_weights(*this, d_r, d_rrsta);
+}
+
+// C[mi] (rows x 2Th, column-major) = A^T (A stored [row][l], ld Lcap) x
+// B (stored [col][l], ld lcapB), summed over the K orders of frequency w.
+void Engine::gemm_fp64(int w, int mi, int K) {
+    const int M = rows_m[mi], N = 2 * Th;
+    if (M == 0) return;
+    const double one = 1.0, zero = 0.0;
+    const double* A = Afld[mi].p + (size_t)w * M * Lcap;
+    DSM_CUBLAS(cublasDgemm(cub, CUBLAS_OP_T, CUBLAS_OP_N, M, N, K, &one, A, Lcap, basis[mi].p, lcapB,
+                           &zero, Cgemm.p + c_off(mi), M));
+    launches++;
+}
+
+void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const void** dr,
+                 const void** ds, int* llog_out) {
+    if (n <= 0) throw Error(DSM_ERR_INVALID, "empty frequency list");
+    for (int k = 0; k < n; ++k)
+        if (ilist[k] <= 0) throw Error(DSM_ERR_INVALID, "frequency index must be > 0 (i = 0 is never computed)");
+    if (dt && n > F) throw Error(DSM_ERR_INVALID, "device outputs hold at most one batch of frequencies");
+    std::memset(&stats, 0, sizeof(stats));
+    launches = 0;
+    cudaEvent_t e0 = ev[0], e1 = ev[1], es0 = ev[2], es1 = ev[3], eg0 = ev[4], eg1 = ev[5];
+    DSM_CUDA(cudaEventRecord(e0, st));
+    float ms_solve = 0, ms_lsum = 0;
+    size_t pt, pr, ps;
+    out_sizes(&pt, &pr, &ps);
+    for (int b0 = 0; b0 < n; b0 += F) {
+        int nf = std::min(F, n - b0);
+        d_freqs.upload(ilist + b0, nf, st);
+        // --- 1+2: per-omega pieces and chunked solves with the cutoff scan
+        DSM_CUDA(cudaEventRecord(es0, st));
+        omega_pieces(d_freqs.p, nf);
+        {
+            std::vector<CutState> init(nf);
+            for (auto& c : init) { c.ismall = 0; c.done = 0; c.llog = maxlmax; c.norders = 0; c.maxamp = -1.0; }
+            cut.upload(init, st);
+        }
+        std::vector<CutState> hc(nf);
+        int l0 = 0;
+        for (;;) {
+            if (l0 > maxlmax) break;
+            int lc = std::min(Lc, maxlmax + 1 - l0);
+            if (l0 + lc > Lcap) throw Error(DSM_ERR_LMAX, "cutoff beyond the order capacity of the context");
+            solve_chunk(d_freqs.p, nf, l0, lc);
+            scan_chunk(nf, l0, lc);
+            stats.systems += (long long)nf * lc;
+            DSM_CUDA(cudaMemcpyAsync(hc.data(), cut.p, sizeof(CutState) * nf, cudaMemcpyDeviceToHost, st));
+            DSM_CUDA(cudaStreamSynchronize(st));
+            bool all = true;
+            for (auto& c : hc) all = all && c.done;
+            l0 += lc;
+            if (all) break;
+        }
+        for (auto& c : hc) {
+            if (!c.done) { c.norders = maxlmax + 1; c.llog = maxlmax; }
+        }
+        DSM_CUDA(cudaEventRecord(es1, st));
+        // --- 3+4: contraction and epilogue per frequency
+        int lneed = 1;
+        for (auto& c : hc) lneed = std::max(lneed, c.norders);
+        build_basis(lneed);
+        DSM_CUDA(cudaEventRecord(eg0, st));
+        for (int w = 0; w < nf; ++w) {
+            stats.orders_used += hc[w].norders;
+            stats.orders_padded += (long long)l0 - hc[w].norders;
+            for (int mi = m_lo; mi <= 2; ++mi) gemm_fp64(w, mi, hc[w].norders);
+            epilogue(d_freqs.p, w, nf);
+            for (int mi = m_lo; mi <= 2; ++mi)
+                stats.lsum_flops += 2.0 * rows_m[mi] * 2.0 * Th * hc[w].norders;
+        }
+        DSM_CUDA(cudaEventRecord(eg1, st));
+        // --- 5: outputs
+        if (llog_out)
+            for (int w = 0; w < nf; ++w) llog_out[b0 + w] = hc[w].llog;
+        if (ho) {
+            if (ho->llog)
+                for (int w = 0; w < nf; ++w) ho->llog[b0 + w] = hc[w].llog;
+            if (ho->tsgt)
+                DSM_CUDA(cudaMemcpyAsync(ho->tsgt + 2 * pt * b0, out_t.p, 16 * pt * nf, cudaMemcpyDeviceToHost, st));
+            if (ho->rsgt && rsgt_sw)
+                DSM_CUDA(cudaMemcpyAsync(ho->rsgt + 2 * pr * b0, out_r.p, 16 * pr * nf, cudaMemcpyDeviceToHost, st));
+            if (ho->synn && synn_sw)
+                DSM_CUDA(cudaMemcpyAsync(ho->synn + 2 * ps * b0, out_s.p, 16 * ps * nf, cudaMemcpyDeviceToHost, st));
+            if (ho->tsgt32 || ho->rsgt32 || ho->synn32) {
+                launch_pack32(*this, nf, pt, pr, ps);
+                const float* o = out32.p;
+                if (ho->tsgt32)
+                    DSM_CUDA(cudaMemcpyAsync(ho->tsgt32 + 2 * pt * b0, o, 8 * pt * nf, cudaMemcpyDeviceToHost, st));
+                if (ho->rsgt32 && rsgt_sw)
+                    DSM_CUDA(cudaMemcpyAsync(ho->rsgt32 + 2 * pr * b0, o + 2 * pt * nf, 8 * pr * nf,
+                                             cudaMemcpyDeviceToHost, st));
+                if (ho->synn32 && synn_sw)
+                    DSM_CUDA(cudaMemcpyAsync(ho->synn32 + 2 * ps * b0, o + 2 * (pt + pr) * nf, 8 * ps * nf,
+                                             cudaMemcpyDeviceToHost, st));
+            }
+        }
+        DSM_CUDA(cudaStreamSynchronize(st));
+        float a = 0, g = 0;
+        cudaEventElapsedTime(&a, es0, es1);
+        cudaEventElapsedTime(&g, eg0, eg1);
+        ms_solve += a;
+        ms_lsum += g;
+    }
+    if (dt) *dt = out_t.p;
+    if (dr) *dr = out_r.p;
+    if (ds) *ds = out_s.p;
+    DSM_CUDA(cudaEventRecord(e1, st));
+    DSM_CUDA(cudaEventSynchronize(e1));
+    float tot = 0;
+    cudaEventElapsedTime(&tot, e0, e1);
+    stats.ms_total = tot;
+    stats.ms_solve = ms_solve;
+    stats.ms_lsum = ms_lsum;
+    stats.launches = launches;
+}
+
+}  // namespace dsm
+
+// ------------------------------------------------------------------ C-ABI
+using dsm::Error;
+
+namespace {
+thread_local std::string g_create_err;
+
+template <class F>
+int guarded(dsm_ctx_t* ctx, F f) {
+    try {
+        f();
+        return DSM_OK;
+    } catch (const Error& e) {
+        if (ctx) ctx->err = e.what();
+        else g_create_err = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->err = e.what();
+        else g_create_err = e.what();
+        return DSM_ERR_INVALID;
+    }
+}
+}  // namespace
+
+extern "C" int dsm_abi_version(void) { return DSM_ABI_VERSION; }
+
+extern "C" const char* dsm_strerror(int code) {
+    switch (code) {
+        case DSM_OK: return "ok";
+        case DSM_ERR_INVALID: return "invalid argument";
+        case DSM_ERR_CUDA: return "CUDA error";
+        case DSM_ERR_NONFINITE: return "non-finite value";
+        case DSM_ERR_LMAX: return "angular-order cutoff beyond the allowed maximum";
+        case DSM_ERR_TIMEOUT: return "device wait timed out";
+        case DSM_ERR_NOMEM: return "out of memory";
+        case DSM_ERR_NODEVICE: return "no usable CUDA device";
+        default: return "unknown error";
+    }
+}
+
+extern "C" const char* dsm_last_error(const dsm_ctx_t* ctx) {
+    return ctx ? ctx->err.c_str() : g_create_err.c_str();
+}
+
+static int check_device(int dev) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= dev || dev < 0) {
+        g_create_err = "no CUDA device (or the requested ordinal is out of range)";
+        return DSM_ERR_NODEVICE;
+    }
+    cudaDeviceProp p{};
+    cudaGetDeviceProperties(&p, dev);
+    if (p.major < 10) {
+        g_create_err = "the engine is built for sm_100a (B200); device compute capability is too low";
+        return DSM_ERR_NODEVICE;
+    }
+    return DSM_OK;
+}
+
+extern "C" int dsm_sh_create(const dsm_sh_setup_t* s, const dsm_options_t* o, dsm_ctx_t** out) {
+    if (!s || !out) { g_create_err = "null argument"; return DSM_ERR_INVALID; }
+    *out = nullptr;
+    dsm_options_t opt{};
+    if (o) opt = *o;
+    int rc = check_device(opt.device);
+    if (rc) return rc;
+    return guarded(nullptr, [&] {
+        DSM_CUDA(cudaSetDevice(opt.device));
+        auto* c = new dsm_ctx;
+        try {
+            c->eng.reset(dsm::make_sh_engine(s, &opt));
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+extern "C" int dsm_psv_create(const dsm_psv_setup_t* s, const dsm_options_t* o, dsm_ctx_t** out) {
+    if (!s || !out) { g_create_err = "null argument"; return DSM_ERR_INVALID; }
+    *out = nullptr;
+    dsm_options_t opt{};
+    if (o) opt = *o;
+    int rc = check_device(opt.device);
+    if (rc) return rc;
+    return guarded(nullptr, [&] {
+        DSM_CUDA(cudaSetDevice(opt.device));
+        auto* c = new dsm_ctx;
+        try {
+            c->eng.reset(dsm::make_psv_engine(s, &opt));
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+extern "C" int dsm_run_freqs(dsm_ctx_t* ctx, const int* ilist, int n, dsm_out_t* out) {
+    if (!ctx || !ilist || !out) return DSM_ERR_INVALID;
+    return guarded(ctx, [&] {
+        DSM_CUDA(cudaSetDevice(ctx->eng->opt.device));
+        ctx->eng->run(ilist, n, out, nullptr, nullptr, nullptr, nullptr);
+    });
+}
+
+extern "C" int dsm_run_freqs_device(dsm_ctx_t* ctx, const int* ilist, int n, const void** d_tsgt,
+                                    const void** d_rsgt, const void** d_synn, int* llog) {
+    if (!ctx || !ilist) return DSM_ERR_INVALID;
+    return guarded(ctx, [&] {
+        DSM_CUDA(cudaSetDevice(ctx->eng->opt.device));
+        ctx->eng->run(ilist, n, nullptr, d_tsgt, d_rsgt, d_synn, llog);
+    });
+}
+
+extern "C" int dsm_ctx_destroy(dsm_ctx_t* ctx) {
+    if (!ctx) return DSM_OK;
+    delete ctx;
+    return DSM_OK;
+}
+
+extern "C" int dsm_get_stats(const dsm_ctx_t* ctx, dsm_stats_t* s) {
+    if (!ctx || !s) return DSM_ERR_INVALID;
+    *s = ctx->eng->stats;
+    return DSM_OK;
+}

@@ -1,0 +1,111 @@
+// Engine context: device state of one SGT computation (SH or PSV).
+#pragma once
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace dsm {
+
+// Per-frequency cutoff state of the plain DSM l-cutoff (calamp + the
+// ismall > 20 exit, src/SGTpsv/SGTpsv-MPI.f90:606-609, 902-905).
+struct CutState {
+    int ismall;
+    int done;     // 1 once the exit condition fired (or maxlmax reached)
+    int llog;     // the reference's llog
+    int norders;  // orders summed: llog if the exit fired, else maxlmax+1
+    double maxamp;
+};
+
+// angular tables shared by both modes
+struct ThetaTables {
+    int th_n = 0;
+    std::vector<double> h_x, h_s;   // cos, sin of theta (host libm)
+    std::vector<int> h_pole;        // 0, 1 (theta = 0), 2 (theta = pi)
+    DBuf<double> x, s;              // device copies
+    DBuf<int> pole;
+};
+
+class Engine {
+  public:
+    int mode = 0;                    // 0 SH, 1 PSV
+    dsm_options_t opt{};
+    std::string err;
+    cudaStream_t st = nullptr;
+    cublasHandle_t cub = nullptr;
+    cudaEvent_t ev[8] = {};
+    long long launches = 0;
+    dsm_stats_t stats{};
+
+    // common geometry
+    int R = 0, Th = 0;              // receivers, epicentral distances
+    int num_t = 0, num_r = 0, num_s = 0;
+    double tlen = 0, omegai = 0, ratl = 0;
+    int maxlmax = 0, imin = 0, imax = 0;
+    int rsgt_sw = 0, synn_sw = 0;
+    ThetaTables th;
+
+    // vector-harmonic basis tables B[m][col][l], col = basis*Th + itheta,
+    // basis 0 = c_lm P_l^m, 1 = c_lm (m x/sin P_l^m + P_l^{m+1})
+    int lcapB = 0;
+    int m_lo = 0;                    // 0 (PSV) or 1 (SH)
+    DBuf<double> basis[3];
+
+    // receivers: interpolation weights (value, d/dr) from the three nodes
+    DBuf<double> wv, wd;             // [R][3]
+
+    // batch work buffers
+    int F = 0, Lc = 0, Lcap = 0;     // frequencies per batch, l chunk, A capacity
+    DBuf<double> Afld[3];            // field matrices per |m| [F][rows][Lcap]
+    DBuf<double> Cgemm;              // GEMM output of one (omega, |m|)
+    DBuf<CutState> cut;              // [F]
+    DBuf<double> amps;               // [F][Lcap][5]
+    DBuf<double> out_t, out_r, out_s;  // complex128 outputs of a batch
+    DBuf<float> out32;                 // complex64 catalogue packing
+    DBuf<int> d_freqs;
+    std::vector<int> h_norders;
+
+    // rows of the field matrix per |m| (set by the mode)
+    int rows_m[3] = {0, 0, 0};
+    // offset of the |m| block inside Cgemm (one frequency)
+    size_t c_off(int mi) const {
+        size_t off = 0;
+        for (int m = m_lo; m < mi; ++m) off += (size_t)rows_m[m] * 2 * Th;
+        return off;
+    }
+    size_t c_total() const { return c_off(3); }
+    void init_common(int dev);
+    virtual ~Engine();
+
+    void build_basis(int lneed);
+    void build_weights(const double* r, const double* rrsta);
+    void gemm_fp64(int w, int mi, int K);
+
+    // mode hooks
+    virtual void omega_pieces(const int* freqs_dev, int nf) = 0;
+    virtual void solve_chunk(const int* freqs_dev, int nf, int l0, int lc) = 0;
+    virtual void scan_chunk(int nf, int l0, int lc) = 0;
+    virtual void epilogue(const int* freqs_dev, int w, int nf) = 0;
+    virtual size_t out_sizes(size_t* nt, size_t* nr, size_t* ns) const = 0;
+
+    // drivers
+    void run(const int* ilist, int n, dsm_out_t* host_out, const void** dt, const void** dr,
+             const void** ds, int* llog);
+};
+
+Engine* make_sh_engine(const dsm_sh_setup_t* s, const dsm_options_t* o);
+Engine* make_psv_engine(const dsm_psv_setup_t* s, const dsm_options_t* o);
+
+// shared kernels (tables.cu)
+void launch_basis_tables(Engine& e, int lcap);
+void launch_interp_weights(Engine& e, const double* d_r, const double* d_rrsta);
+void launch_pack32(Engine& e, int nf, size_t per_t, size_t per_r, size_t per_s);
+
+}  // namespace dsm
+
+struct dsm_ctx {
+    std::unique_ptr<dsm::Engine> eng;
+    std::string err;
+};

@@ -1,0 +1,267 @@
+"""ctypes harness of the SGT engine (tests and benchmarks only).
+
+The product is the C-ABI library ``lib/libdsmsgt.so`` declared in
+``include/dsmsgt.h`` (engine) and ``include/dsmsgt_host.h`` (driver-side
+set-up helpers).  This module loads it, mirrors the structs, and offers
+numpy-returning wrappers.  It never computes anything itself: when the
+library is missing every call fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import synth  # noqa: F401  (re-export)
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG_DIR)                 # dsm-kernel_b200/
+REPO = os.path.dirname(ROOT)
+LIB_PATH = os.path.join(ROOT, "lib", "libdsmsgt.so")
+
+DSM_PREC_FP64 = 0
+DSM_PREC_MIXED = 1
+
+SH_NUM = (10, 5, 5)
+PSV_NUM = (20, 10, 10)
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_fp = C.POINTER(C.c_float)
+
+
+class ShSetup(C.Structure):
+    _fields_ = [
+        ("nzone", C.c_int), ("vrmin", _dp), ("vrmax", _dp), ("vsv", _dp), ("qmu", _dp),
+        ("nlayer", _ip), ("isp", _ip), ("jsp", _ip), ("nnlayer", C.c_int),
+        ("t", _dp), ("h1", _dp), ("h2", _dp), ("h3", _dp), ("h4", _dp),
+        ("spn", C.c_int), ("spo", C.c_double), ("r0", C.c_double), ("mu0", C.c_double),
+        ("ins", C.c_int), ("gt", _dp), ("gh1", _dp), ("gh2", _dp), ("gh3", _dp), ("gh4", _dp),
+        ("r_n", C.c_int), ("r", _dp), ("rrsta", _dp), ("iista", _ip),
+        ("theta_n", C.c_int), ("theta", _dp),
+        ("tlen", C.c_double), ("omegai", C.c_double), ("ratl", C.c_double),
+        ("maxlmax", C.c_int), ("imin", C.c_int), ("imax", C.c_int),
+        ("rsgt_switch", C.c_int), ("tsgt_switch", C.c_int), ("synn_switch", C.c_int),
+    ]
+
+
+class PsvSetup(C.Structure):
+    _fields_ = [
+        ("nzone", C.c_int), ("iphase", _ip), ("nlayer", _ip), ("isp", _ip), ("kkdr", _ip),
+        ("elem", _ip), ("hmoff", _ip),
+        ("vrmin", _dp), ("vrmax", _dp), ("qmu", _dp), ("qkappa", _dp), ("vsv", _dp),
+        ("nn", C.c_int), ("rmin", C.c_double), ("rmax", C.c_double),
+        ("n_sel", C.c_int), ("n_fel", C.c_int), ("n_hm", C.c_int),
+        ("solid_el", _dp), ("fluid_el", _dp), ("hm_el", _dp),
+        ("spn", C.c_int), ("spo", C.c_double), ("r0", C.c_double),
+        ("ecC0", C.c_double), ("ecF0", C.c_double), ("ecL0", C.c_double),
+        ("ra_src", C.c_double * 2), ("src_poly", C.c_double * 24), ("jsrc", C.c_int),
+        ("r_n", C.c_int), ("r", _dp), ("rrsta", _dp), ("iista", _ip), ("istazone", _ip),
+        ("lambda_", _dp), ("qkp", _dp),
+        ("theta_n", C.c_int), ("theta", _dp),
+        ("tlen", C.c_double), ("omegai", C.c_double), ("ratl", C.c_double),
+        ("maxlmax", C.c_int), ("imin", C.c_int), ("imax", C.c_int),
+        ("rsgt_switch", C.c_int), ("tsgt_switch", C.c_int), ("synn_switch", C.c_int),
+    ]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("dsmconf", C.c_char * 256), ("outdir", C.c_char * 256), ("model", C.c_char * 256),
+        ("modelname", C.c_char * 128),
+        ("tlen", C.c_double), ("rmin_", C.c_double), ("rmax_", C.c_double),
+        ("rdelta_", C.c_double), ("r0min", C.c_double),
+        ("thetamin", C.c_double), ("thetamax", C.c_double), ("thetadelta", C.c_double),
+        ("imin", C.c_int), ("imax", C.c_int),
+        ("rsgt_switch", C.c_int), ("tsgt_switch", C.c_int), ("synn_switch", C.c_int),
+        ("psgt_switch", C.c_int),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [("precision", C.c_int), ("device", C.c_int), ("use_lmax_predictor", C.c_int),
+                ("l_chunk", C.c_int), ("freq_batch", C.c_int)]
+
+
+class Out(C.Structure):
+    _fields_ = [("tsgt", _dp), ("rsgt", _dp), ("synn", _dp),
+                ("tsgt32", _fp), ("rsgt32", _fp), ("synn32", _fp), ("llog", _ip)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("ms_solve", C.c_double), ("ms_lsum", C.c_double),
+                ("ms_pack", C.c_double), ("ms_h2d", C.c_double), ("ms_d2h", C.c_double),
+                ("launches", C.c_longlong), ("systems", C.c_longlong),
+                ("orders_used", C.c_longlong), ("orders_padded", C.c_longlong),
+                ("lsum_flops", C.c_double), ("solve_bytes", C.c_double)]
+
+
+class DsmError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libdsmsgt.so (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise DsmError(f"{LIB_PATH} is missing: run __graft_entry__.build() first")
+        L = C.CDLL(LIB_PATH)
+        L.dsm_parse_params.argtypes = [C.c_char_p, C.POINTER(Params)]
+        L.dsm_sh_setup_build.argtypes = [C.POINTER(Params), C.c_char_p, C.c_char_p,
+                                         C.POINTER(C.c_void_p), C.POINTER(C.POINTER(ShSetup))]
+        L.dsm_psv_setup_build.argtypes = [C.POINTER(Params), C.c_char_p, C.c_char_p,
+                                          C.POINTER(C.c_void_p), C.POINTER(C.POINTER(PsvSetup))]
+        L.dsm_bundle_free.argtypes = [C.c_void_p]
+        L.dsm_bundle_info.argtypes = [C.c_void_p, _ip, _ip]
+        L.dsm_host_last_error.restype = C.c_char_p
+        L.dsm_sh_create.argtypes = [C.POINTER(ShSetup), C.POINTER(Options), C.POINTER(C.c_void_p)]
+        L.dsm_psv_create.argtypes = [C.POINTER(PsvSetup), C.POINTER(Options), C.POINTER(C.c_void_p)]
+        L.dsm_run_freqs.argtypes = [C.c_void_p, _ip, C.c_int, C.POINTER(Out)]
+        L.dsm_run_freqs_device.argtypes = [C.c_void_p, _ip, C.c_int, C.POINTER(C.c_void_p),
+                                           C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), _ip]
+        L.dsm_ctx_destroy.argtypes = [C.c_void_p]
+        L.dsm_last_error.argtypes = [C.c_void_p]
+        L.dsm_last_error.restype = C.c_char_p
+        L.dsm_strerror.restype = C.c_char_p
+        L.dsm_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray, typ):
+    return a.ctypes.data_as(typ)
+
+
+@dataclass
+class Job:
+    """Inputs of one run: parameter file, DSM.config and model contents."""
+    param_text: str
+    conf_text: str
+    model_text: str
+
+
+class Setup:
+    """Driver-side set-up (grid and element integrals) built by the library."""
+
+    def __init__(self, job: Job, mode: str):
+        L = lib()
+        self.mode = mode
+        self.job = job
+        self.params = Params()
+        rc = L.dsm_parse_params(job.param_text.encode(), C.byref(self.params))
+        if rc:
+            raise DsmError(L.dsm_host_last_error().decode())
+        self._bundle = C.c_void_p()
+        if mode == "sh":
+            self.ptr = C.POINTER(ShSetup)()
+            rc = L.dsm_sh_setup_build(C.byref(self.params), job.conf_text.encode(),
+                                      job.model_text.encode(), C.byref(self._bundle),
+                                      C.byref(self.ptr))
+            self.num = SH_NUM
+        elif mode == "psv":
+            self.ptr = C.POINTER(PsvSetup)()
+            rc = L.dsm_psv_setup_build(C.byref(self.params), job.conf_text.encode(),
+                                       job.model_text.encode(), C.byref(self._bundle),
+                                       C.byref(self.ptr))
+            self.num = PSV_NUM
+        else:
+            raise ValueError(mode)
+        if rc:
+            raise DsmError(L.dsm_host_last_error().decode())
+        self.s = self.ptr.contents
+        nodes, unk = C.c_int(), C.c_int()
+        L.dsm_bundle_info(self._bundle, C.byref(nodes), C.byref(unk))
+        self.n_nodes, self.n_unknowns = nodes.value, unk.value
+
+    @property
+    def r_n(self) -> int:
+        return self.s.r_n
+
+    @property
+    def theta_n(self) -> int:
+        return self.s.theta_n
+
+    def out_shapes(self, n: int):
+        nt, nr, ns = self.num
+        return ((n, self.theta_n, self.r_n, nt), (n, self.theta_n, self.r_n, nr),
+                (n, self.theta_n, ns))
+
+    def __del__(self):
+        try:
+            if getattr(self, "_bundle", None) and self._bundle.value:
+                lib().dsm_bundle_free(self._bundle)
+                self._bundle = C.c_void_p()
+        except Exception:
+            pass
+
+
+def alloc_outputs(setup: Setup, n: int):
+    """Complex128 outputs in the reference's column-major order, returned as
+    C-order arrays [k][itheta][ir][comp] (same memory layout)."""
+    st, sr, ss = setup.out_shapes(n)
+    return (np.zeros(st, np.complex128), np.zeros(sr, np.complex128),
+            np.zeros(ss, np.complex128), np.zeros(n, np.int32))
+
+
+class Context:
+    """A device context of the engine (dsm_sh_create / dsm_psv_create)."""
+
+    def __init__(self, setup: Setup, precision: int = DSM_PREC_FP64, device: int = 0,
+                 use_lmax_predictor: int = 0, l_chunk: int = 0, freq_batch: int = 0):
+        L = lib()
+        self.setup = setup
+        self.opt = Options(precision, device, use_lmax_predictor, l_chunk, freq_batch)
+        self.h = C.c_void_p()
+        fn = L.dsm_sh_create if setup.mode == "sh" else L.dsm_psv_create
+        rc = fn(setup.ptr, C.byref(self.opt), C.byref(self.h))
+        if rc:
+            msg = L.dsm_last_error(self.h).decode() if self.h.value else L.dsm_strerror(rc).decode()
+            raise DsmError(f"create failed ({rc}): {msg}")
+
+    def run(self, freqs, want32: bool = False):
+        L = lib()
+        fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+        n = len(fl)
+        t, r, y, llog = alloc_outputs(self.setup, n)
+        out = Out()
+        out.tsgt = t.ctypes.data_as(_dp)
+        out.rsgt = r.ctypes.data_as(_dp)
+        out.synn = y.ctypes.data_as(_dp)
+        out.llog = llog.ctypes.data_as(_ip)
+        t32 = r32 = y32 = None
+        if want32:
+            nt, nr, ns = self.setup.num
+            t32 = np.zeros((n, self.setup.r_n, self.setup.theta_n, nt), np.complex64)
+            r32 = np.zeros((n, self.setup.r_n, self.setup.theta_n, nr), np.complex64)
+            y32 = np.zeros((n, self.setup.theta_n, ns), np.complex64)
+            out.tsgt32 = t32.ctypes.data_as(_fp)
+            out.rsgt32 = r32.ctypes.data_as(_fp)
+            out.synn32 = y32.ctypes.data_as(_fp)
+        rc = L.dsm_run_freqs(self.h, _ptr(fl, _ip), n, C.byref(out))
+        if rc:
+            raise DsmError(f"dsm_run_freqs failed ({rc}): {L.dsm_last_error(self.h).decode()}")
+        if want32:
+            return t, r, y, llog, (t32, r32, y32)
+        return t, r, y, llog
+
+    def stats(self) -> Stats:
+        s = Stats()
+        lib().dsm_get_stats(self.h, C.byref(s))
+        return s
+
+    def close(self):
+        if self.h.value:
+            lib().dsm_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,240 @@
+/*
+ * dsmsgt.h -- C-ABI of the B200 strain Green's tensor (SGT) engine.
+ *
+ * The engine replaces the body of the frequency loop of the DSM Kernel
+ * Suite programs SGTsh and SGTpsv:
+ *   SH : src/SGTsh/SGTsh-MPI.f90:404-555   (per-omega operator, l loop,
+ *        m loop, sources, banded solve, receiver l-sum)
+ *   PSV: src/SGTpsv/SGTpsv-MPI.f90:551-1095
+ * Everything before that loop (parameter parsing, grid, element integrals)
+ * and after it (catalogue files, logs) stays with the caller, which in the
+ * reference is the Fortran driver.  The caller fills one of the setup
+ * structs below with the arrays that driver holds after its set-up phase
+ * (1-based indices are kept exactly as the Fortran computes them), creates
+ * a context, and asks for any list of frequency indices.
+ *
+ * All pointers are plain host pointers; sizes are element counts.  Complex
+ * numbers are interleaved (re, im) pairs of double (complex128) or float
+ * (complex64).  No type in this header depends on CUDA or on PyTorch.
+ *
+ * Error behaviour: every entry point returns DSM_OK (0) or one of the
+ * DSM_ERR_* codes.  The library never prints, stops or pauses (the
+ * reference pauses on bad input, src/SGTpsv/others.f90:536); the text of
+ * the last error of a context is available from dsm_last_error().
+ */
+#ifndef DSMSGT_H
+#define DSMSGT_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSM_ABI_VERSION 1
+
+/* return codes */
+#define DSM_OK               0
+#define DSM_ERR_INVALID      1  /* bad argument or inconsistent set-up        */
+#define DSM_ERR_CUDA         2  /* CUDA runtime / driver / library error      */
+#define DSM_ERR_NONFINITE    3  /* a pivot or output became Inf/NaN           */
+#define DSM_ERR_LMAX         4  /* a cutoff needs more orders than allowed    */
+#define DSM_ERR_TIMEOUT      5  /* a bounded device wait gave up              */
+#define DSM_ERR_NOMEM        6  /* device or host allocation failed           */
+#define DSM_ERR_NODEVICE     7  /* no CUDA device / kernels not loadable      */
+
+/* precision modes of a context */
+#define DSM_PREC_FP64        0  /* plain path: every stage in FP64            */
+#define DSM_PREC_MIXED       1  /* FP32 factors + FP64 refinement; split
+                                   16-bit tensor-core l-sum, FP32 accumulate  */
+
+/* number of output components per point (src/SGTsh/modules.f90:371-373,
+   src/SGTpsv/modules.f90:112-114) */
+#define DSM_SH_NUM_TSGT   10
+#define DSM_SH_NUM_RSGT    5
+#define DSM_SH_NUM_SYNN    5
+#define DSM_PSV_NUM_TSGT  20
+#define DSM_PSV_NUM_RSGT  10
+#define DSM_PSV_NUM_SYNN  10
+
+/* ------------------------------------------------------------------------
+ * SH set-up: the state of SGTsh after src/SGTsh/SGTsh-MPI.f90:33-347.
+ * ---------------------------------------------------------------------- */
+typedef struct dsm_sh_setup {
+    int nzone;                 /* solid zones kept (outer core cut, :96-102)   */
+    const double *vrmin;       /* [nzone] km                                   */
+    const double *vrmax;       /* [nzone] km                                   */
+    const double *vsv;         /* [4*nzone] column-major (4,nzone), for callsuf */
+    const double *qmu;         /* [nzone]                                      */
+    const int    *nlayer;      /* [nzone]                                      */
+    const int    *isp;         /* [nzone] 1-based first node of each zone      */
+    const int    *jsp;         /* [nzone] 1-based first element entry          */
+    int           nnlayer;     /* total layers; the system has nnlayer+1 rows  */
+    const double *t, *h1, *h2, *h3, *h4;   /* [4*nnlayer] element integrals   */
+    /* source (single depth, src/SGTsh/others.f90:37-41) */
+    int           spn;         /* zone of the source                           */
+    double        spo;         /* position inside the zone (calspo)            */
+    double        r0;          /* source radius after calspo adjustment        */
+    double        mu0;         /* rigidity at the source (calgstg)             */
+    int           ins;         /* 1-based element entry of the source layer    */
+    const double *gt, *gh1, *gh2, *gh3, *gh4;  /* [8] split source element     */
+    /* receivers */
+    int           r_n;
+    const double *r;           /* [r_n] km                                     */
+    const double *rrsta;       /* [3*r_n] (3,r_n) interpolation node radii     */
+    const int    *iista;       /* [3*r_n] (3,r_n) 1-based node indices         */
+    int           theta_n;
+    const double *theta;       /* [theta_n] degrees                            */
+    /* DSM parameters */
+    double        tlen;        /* s                                            */
+    double        omegai;      /* imaginary frequency, already -ln(conf)/tlen  */
+    double        ratl;        /* l-cutoff amplitude ratio                     */
+    int           maxlmax;
+    int           imin, imax;  /* frequency range of the run (zig-zag owner)   */
+    int           rsgt_switch, tsgt_switch, synn_switch;
+} dsm_sh_setup_t;
+
+/* ------------------------------------------------------------------------
+ * PSV set-up: the state of SGTpsv after src/SGTpsv/SGTpsv-MPI.f90:39-477.
+ * Element arrays are passed whole, with the Fortran 1-based offsets the
+ * driver uses to address them (itmp = isdr+issp(isl) etc.).
+ * ---------------------------------------------------------------------- */
+typedef struct dsm_psv_setup {
+    int nzone;
+    const int    *iphase;      /* [nzone] 1 solid, 2 fluid (calnl)             */
+    const int    *nlayer;      /* [nzone]                                      */
+    const int    *isp;         /* [nzone] 1-based first node (calsp)           */
+    const int    *kkdr;        /* [nzone] 1-based first unknown (calspdr)      */
+    const int    *elem;        /* [nzone] 1-based element offset: solid
+                                  isdr+issp(isl), fluid ildr+ilsp(ill)         */
+    const int    *hmoff;       /* [nzone] solid: 1-based column jsdr+jssp(isl)
+                                  of the modified-derivative arrays; fluid 0   */
+    const double *vrmin, *vrmax, *qmu, *qkappa;   /* [nzone]                   */
+    const double *vsv;         /* [4*nzone] (4,nzone), for callsuf             */
+    int           nn;          /* unknowns: kkdr(nzone)+2*nlayer(nzone)+1      */
+    double        rmin, rmax;
+    /* solid element arrays, each n_sel entries, order fixed by
+       DSM_PSV_SOLID_* below; fluid arrays p1,p2,p3 each n_fel entries;
+       modified first-derivative operators, each (4, n_hm) column-major with
+       the first index running over the Fortran bounds (-2:1) or (-1:2).    */
+    int           n_sel, n_fel, n_hm;
+    const double *solid_el;    /* [DSM_PSV_NSOLID * n_sel]                     */
+    const double *fluid_el;    /* [3 * n_fel]                                  */
+    const double *hm_el;       /* [DSM_PSV_NHM * 4 * n_hm]                     */
+    /* source */
+    int           spn;
+    double        spo;
+    double        r0;          /* after calspo adjustment                      */
+    double        ecC0, ecF0, ecL0;  /* elastic constants at r0 (calstg)      */
+    double        ra_src[2];   /* ra(mtmp), ra(mtmp+1) around the source       */
+    double        src_poly[24];/* rho,vpv,vph,vsv,vsh,eta (4 each), zone spn  */
+    int           jsrc;        /* 1-based first excitation row (jtmp, :636)    */
+    /* receivers */
+    int           r_n;
+    const double *r;           /* [r_n]                                        */
+    const double *rrsta;       /* [3*r_n]                                      */
+    const int    *iista;       /* [3*r_n] zone-local node indices (calra2_psv) */
+    const int    *istazone;    /* [r_n]                                        */
+    const double *lambda;      /* [r_n] A at the receiver (fluid receivers)    */
+    const double *qkp;         /* [r_n] Qkappa at the receiver                 */
+    int           theta_n;
+    const double *theta;       /* [theta_n] degrees                            */
+    double        tlen, omegai, ratl;
+    int           maxlmax;
+    int           imin, imax;
+    int           rsgt_switch, tsgt_switch, synn_switch;
+} dsm_psv_setup_t;
+
+/* packing order of dsm_psv_setup_t.solid_el */
+enum {
+    DSM_PSV_T = 0, DSM_PSV_H1X, DSM_PSV_H2L, DSM_PSV_H2N, DSM_PSV_H3AY,
+    DSM_PSV_H4AL, DSM_PSV_H4AN, DSM_PSV_H5AY, DSM_PSV_H6AL, DSM_PSV_H6AN,
+    DSM_PSV_H7Y, DSM_PSV_H7Z, DSM_PSV_H8L, DSM_PSV_H8N, DSM_PSV_H3Y,
+    DSM_PSV_H4L, DSM_PSV_H4N, DSM_PSV_H5Y, DSM_PSV_H6L, DSM_PSV_H6N,
+    DSM_PSV_NSOLID
+};
+/* packing order of dsm_psv_setup_t.hm_el */
+enum {
+    DSM_PSV_H3MY = 0,   /* (-2:1) */
+    DSM_PSV_H5MY,       /* (-1:2) */
+    DSM_PSV_H4M1L,      /* (-1:2) */
+    DSM_PSV_H4M2N,      /* (-2:1) */
+    DSM_PSV_H6M1N,      /* (-1:2) */
+    DSM_PSV_H6M2L,      /* (-2:1) */
+    DSM_PSV_NHM
+};
+
+/* ------------------------------------------------------------------------
+ * Context options and outputs
+ * ---------------------------------------------------------------------- */
+typedef struct dsm_options {
+    int precision;        /* DSM_PREC_FP64 or DSM_PREC_MIXED                */
+    int device;           /* CUDA device ordinal                             */
+    int use_lmax_predictor;/* 1: size l batches with the learned cutoff      */
+    int l_chunk;          /* orders solved speculatively per batch (0: auto) */
+    int freq_batch;       /* frequencies processed together (0: auto)        */
+} dsm_options_t;
+
+/* Host output buffers for dsm_run_freqs.  Any pointer may be NULL.  For
+ * frequency k of the request (0 <= k < n):
+ *   tsgt   complex128, column-major (num_tsgt, r_n, theta_n), block k
+ *   rsgt   complex128, column-major (num_rsgt, r_n, theta_n), block k
+ *   synn   complex128, column-major (num_synn, theta_n),      block k
+ *   tsgt32/rsgt32/synn32: complex64 in catalogue record order, i.e. for each
+ *          receiver the (num, theta_n) record the reference writes to one
+ *          file (SGTpsv-MPI.f90:1113-1116): layout [k][ir][itheta][comp]
+ *   llog   the reference's cutoff variable per frequency (the log line
+ *          prints llog-1, SGTpsv-MPI.f90:1098)
+ */
+typedef struct dsm_out {
+    double *tsgt, *rsgt, *synn;
+    float  *tsgt32, *rsgt32, *synn32;
+    int    *llog;
+} dsm_out_t;
+
+typedef struct dsm_ctx dsm_ctx_t;
+
+/* Context creation uploads the set-up to the device, builds the
+ * omega-independent tables (vector-harmonic bases, interpolation weights)
+ * and reserves device memory.  Replaces the reference's per-run state in
+ * src/SGTsh/modules.f90 / src/SGTpsv/modules.f90. */
+int dsm_sh_create(const dsm_sh_setup_t *setup, const dsm_options_t *opt,
+                  dsm_ctx_t **ctx);
+int dsm_psv_create(const dsm_psv_setup_t *setup, const dsm_options_t *opt,
+                   dsm_ctx_t **ctx);
+
+/* Computes the SGTs of n frequency indices (each in [imin, imax], i != 0;
+ * replaces one pass of the omega loop per index, SGTsh-MPI.f90:389-613,
+ * SGTpsv-MPI.f90:535-1152).  Output is copied to the host buffers. */
+int dsm_run_freqs(dsm_ctx_t *ctx, const int *ilist, int n, dsm_out_t *out);
+
+/* Same computation with outputs left on the device: *d_tsgt etc. receive
+ * device pointers owned by the context, valid until the next call.  Used
+ * by callers that consume the SGT on the GPU. */
+int dsm_run_freqs_device(dsm_ctx_t *ctx, const int *ilist, int n,
+                         const void **d_tsgt, const void **d_rsgt,
+                         const void **d_synn, int *llog);
+
+int dsm_ctx_destroy(dsm_ctx_t *ctx);
+const char *dsm_last_error(const dsm_ctx_t *ctx);
+const char *dsm_strerror(int code);
+int dsm_abi_version(void);
+
+/* Stage timing of the last run (device time in ms, CUDA events): the
+ * per-(omega,l) solve, the l-sum contraction, the epilogue/packing, and
+ * the whole call.  Also the number of kernel launches of the call. */
+typedef struct dsm_stats {
+    double ms_total, ms_solve, ms_lsum, ms_pack, ms_h2d, ms_d2h;
+    long long launches;
+    long long systems;      /* (omega,l) systems solved                    */
+    long long orders_used;  /* sum over frequencies of the realised cutoff */
+    long long orders_padded;/* orders solved beyond the cutoff             */
+    double lsum_flops;      /* algorithmic flops of the contraction        */
+    double solve_bytes;     /* algorithmic bytes of the banded solves      */
+} dsm_stats_t;
+int dsm_get_stats(const dsm_ctx_t *ctx, dsm_stats_t *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSMSGT_H */

@@ -1,0 +1,66 @@
+"""Oracle loader -- test infrastructure only.
+
+ctypes wrapper of ``oracle/build/liboracle.so``, the CPU FP64 restatement of
+the SGTsh / SGTpsv frequency loops.  Only tests/, ``__graft_entry__.smoke()``
+and the CPU-baseline leg of ``bench.py`` may import this module; the product
+(``dsm-kernel_b200``) never does.  Parity status: unpinned (the Fortran
+reference cannot be built here and ships no test vectors).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "build", "liboracle.so")
+
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        for name in ("oracle_sh_run", "oracle_psv_run"):
+            getattr(L, name).argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
+        for name in ("oracle_sh_run_parallel", "oracle_psv_run_parallel"):
+            getattr(L, name).argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.c_int]
+        _lib = L
+    return _lib
+
+
+def run(setup, freqs, threads: int = 1):
+    """Runs the oracle on a dsmsgt.Setup; returns (tsgt, rsgt, synn, llog)
+    in the same array layout as dsmsgt.Context.run."""
+    from dsmsgt import alloc_outputs  # the harness package, not the product path
+    fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+    n = len(fl)
+    t, r, y, llog = alloc_outputs(setup, n)
+    L = lib()
+    ip = fl.ctypes.data_as(C.POINTER(C.c_int))
+    lp = llog.ctypes.data_as(C.POINTER(C.c_int))
+    sp = C.cast(setup.ptr, C.c_void_p)
+    args = (sp, ip, n, t.ctypes.data, r.ctypes.data, y.ctypes.data, lp)
+    if setup.mode == "sh":
+        if threads > 1:
+            L.oracle_sh_run_parallel(*args, threads)
+        else:
+            L.oracle_sh_run(*args)
+    else:
+        if threads > 1:
+            L.oracle_psv_run_parallel(*args, threads)
+        else:
+            L.oracle_psv_run(*args)
+    return t, r, y, llog

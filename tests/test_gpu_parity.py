@@ -1,0 +1,41 @@
+"""CUDA engine vs the FP64 oracle (the CPU restatement of the reference).
+
+The plain FP64 path must match the oracle to 1e-10 relative L2 per output
+array, with an identical realised cutoff (llog) per frequency.
+"""
+import numpy as np
+import pytest
+
+import dsmsgt
+from cases import psv_small, sh_small
+from conftest import rel_l2
+
+TOL_FP64 = 1e-10
+
+
+def _compare(setup, freqs, ctx_kwargs=None, tol=TOL_FP64):
+    from oracle import oracle as orc
+    ctx = dsmsgt.Context(setup, **(ctx_kwargs or {}))
+    t, r, y, llog = ctx.run(freqs)
+    ot, orr, oy, ollog = orc.run(setup, freqs, threads=8)
+    assert list(llog) == list(ollog)
+    errs = {"tsgt": rel_l2(t, ot), "rsgt": rel_l2(r, orr), "synn": rel_l2(y, oy)}
+    for k, v in errs.items():
+        assert v <= tol, (k, v, errs)
+    assert np.all(np.isfinite(t))
+    ctx.close()
+    return errs
+
+
+@pytest.mark.gpu
+def test_sh_fp64_matches_oracle(built):
+    s = dsmsgt.Setup(sh_small(), "sh")
+    errs = _compare(s, [1, 7, 16, 31])
+    print(errs)
+
+
+@pytest.mark.gpu
+def test_sh_fp64_small_chunks(built):
+    """Several speculative l chunks per frequency must give the same result."""
+    s = dsmsgt.Setup(sh_small(seed=3), "sh")
+    _compare(s, [5, 20], {"l_chunk": 64, "freq_batch": 2})
