@@ -25,6 +25,11 @@ namespace dsm {
 
 void Engine::init_common(int dev) {
     DSM_CUDA(cudaSetDevice(dev));
+    // the source-term kernels keep the 4x4x10 Runge-Kutta coefficient
+    // tables of calabnum in thread-local memory
+    size_t stack = 0;
+    DSM_CUDA(cudaDeviceGetLimit(&stack, cudaLimitStackSize));
+    if (stack < 16384) DSM_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 16384));
     DSM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     DSM_CUBLAS(cublasCreate(&cub));
     DSM_CUBLAS(cublasSetStream(cub, st));
@@ -64,6 +69,41 @@ void Engine::gemm_fp64(int w, int mi, int K) {
     launches++;
 }
 
+// Grows the order capacity of the field matrices and of the probe table,
+// keeping the columns already written (the cutoff of a frequency is not
+// known before its orders are solved; the reference allows up to maxlmax).
+void Engine::grow_orders(int need) {
+    if (need <= Lcap) return;
+    int cap = Lcap;
+    while (cap < need) cap *= 2;
+    cap = std::min(cap, maxlmax + 1 + Lc);
+    if (cap < need) cap = need;
+    for (int m = m_lo; m <= 2; ++m) {
+        size_t h = (size_t)F * rows_m[m];
+        if (h == 0) continue;
+        double* np_ = nullptr;
+        if (cudaMalloc(&np_, h * cap * sizeof(double)) != cudaSuccess)
+            throw Error(DSM_ERR_NOMEM, "cannot grow the field matrices to " + std::to_string(cap) + " orders");
+        DSM_CUDA(cudaMemcpy2DAsync(np_, (size_t)cap * sizeof(double), Afld[m].p, (size_t)Lcap * sizeof(double),
+                                   (size_t)Lcap * sizeof(double), h, cudaMemcpyDeviceToDevice, st));
+        DSM_CUDA(cudaStreamSynchronize(st));
+        Afld[m].release();
+        Afld[m].p = np_;
+        Afld[m].n = h * cap;
+    }
+    double* na = nullptr;
+    if (cudaMalloc(&na, (size_t)F * cap * amp_k * sizeof(double)) != cudaSuccess)
+        throw Error(DSM_ERR_NOMEM, "cannot grow the probe table");
+    DSM_CUDA(cudaMemcpy2DAsync(na, (size_t)cap * amp_k * sizeof(double), amps.p,
+                               (size_t)Lcap * amp_k * sizeof(double), (size_t)Lcap * amp_k * sizeof(double),
+                               (size_t)F, cudaMemcpyDeviceToDevice, st));
+    DSM_CUDA(cudaStreamSynchronize(st));
+    amps.release();
+    amps.p = na;
+    amps.n = (size_t)F * cap * amp_k;
+    Lcap = cap;
+}
+
 void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const void** dr,
                  const void** ds, int* llog_out) {
     if (n <= 0) throw Error(DSM_ERR_INVALID, "empty frequency list");
@@ -93,7 +133,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
         for (;;) {
             if (l0 > maxlmax) break;
             int lc = std::min(Lc, maxlmax + 1 - l0);
-            if (l0 + lc > Lcap) throw Error(DSM_ERR_LMAX, "cutoff beyond the order capacity of the context");
+            if (l0 + lc > Lcap) grow_orders(l0 + lc);
             solve_chunk(d_freqs.p, nf, l0, lc);
             scan_chunk(nf, l0, lc);
             stats.systems += (long long)nf * lc;
@@ -288,6 +328,30 @@ extern "C" int dsm_ctx_destroy(dsm_ctx_t* ctx) {
     if (!ctx) return DSM_OK;
     delete ctx;
     return DSM_OK;
+}
+
+// Diagnostics: copies an internal device buffer of the last run to host
+// memory ("amps": per-order cutoff probes, [F][Lcap][k]).  Returns the
+// number of bytes copied, or a negative error code.
+extern "C" long long dsm_debug_copy(dsm_ctx_t* ctx, const char* name, void* dst, long long bytes) {
+    if (!ctx || !name || !dst) return -DSM_ERR_INVALID;
+    dsm::Engine& e = *ctx->eng;
+    const void* src = nullptr;
+    size_t have = 0;
+    if (std::strcmp(name, "amps") == 0) { src = e.amps.p; have = e.amps.n * sizeof(double); }
+    for (int m = 0; m < 3; ++m) {
+        char nm[8] = {'a', 'f', 'l', 'd', (char)('0' + m), 0};
+        if (std::strcmp(name, nm) == 0) { src = e.Afld[m].p; have = e.Afld[m].n * sizeof(double); }
+    }
+    if (std::strcmp(name, "lcap") == 0) {
+        long long v = e.Lcap;
+        std::memcpy(dst, &v, sizeof(v));
+        return sizeof(v);
+    }
+    if (!src) return -DSM_ERR_INVALID;
+    size_t nb = std::min((size_t)bytes, have);
+    if (cudaMemcpy(dst, src, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return -DSM_ERR_CUDA;
+    return (long long)nb;
 }
 
 extern "C" int dsm_get_stats(const dsm_ctx_t* ctx, dsm_stats_t* s) {

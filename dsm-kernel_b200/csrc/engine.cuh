@@ -58,6 +58,7 @@ class Engine {
 
     // batch work buffers
     int F = 0, Lc = 0, Lcap = 0;     // frequencies per batch, l chunk, A capacity
+    int amp_k = 1;                   // cutoff probes stored per order
     DBuf<double> Afld[3];            // field matrices per |m| [F][rows][Lcap]
     DBuf<double> Cgemm;              // GEMM output of one (omega, |m|)
     DBuf<CutState> cut;              // [F]
@@ -82,6 +83,7 @@ class Engine {
     void build_basis(int lneed);
     void build_weights(const double* r, const double* rrsta);
     void gemm_fp64(int w, int mi, int K);
+    void grow_orders(int need);
 
     // mode hooks
     virtual void omega_pieces(const int* freqs_dev, int nf) = 0;

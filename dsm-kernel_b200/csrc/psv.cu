@@ -1,7 +1,1359 @@
-// PSV engine (in progress).
+// P-SV engine: replaces src/SGTpsv/SGTpsv-MPI.f90:551-1095.
+//
+// Kernels (plain FP64 path; compiled without fused multiply-add):
+//   k_psv_omega  per-omega, per-zone band blocks A0, A1, A2 (cala0, cala1,
+//                cala2, calhml, overlapa, calb0, calb2, overlapb,
+//                src/SGTpsv/calmat.f90:452-742; calcoef :409-447)
+//   k_psv_solve  one thread per (omega, l >= 1): assembly a = A0 + l(l+1) A2
+//                (rows 2,4) + sqrt(l(l+1)) A1 (rows 1,3), fluid rows 3,4,
+//                fluid-solid boundary rows (cala, calbc, :747-809) streamed
+//                into the unpivoted complex-symmetric band LDL^T of
+//                half-width 3 (dcsymbdl0, src/SGTpsv/dcsymbdl.f90:2-88,
+//                including its different update order in the last two
+//                steps) and the substitutions (dcsbdlv0, :93-166;
+//                mydcsbdlv3 is the same arithmetic) of six basis
+//                right-hand sides: the four source rows jtmp..jtmp+3 and the
+//                surface rows nn-1, nn.  Factors stay in HBM between the
+//                downward and upward sweeps.
+//   k_psv_l0     l = 0: the tridiagonal compaction (rea2 / rea2_back,
+//                calmat.f90:1247-1389) and its solves (dcsymbdl0/dcsbdlv0
+//                with half-width 1), one thread per frequency.
+//   k_psv_fields source terms (calabnum, calya + rk3, calg, glu,
+//                calmat.f90:815-1171), back-propagation sources
+//                (caldveczero, trial.f90:326-364), receiver interpolation
+//                (interpolate, others.f90:1170-1212); writes the per-order
+//                receiver fields of every active slot and the probe of
+//                calamp (imt = 1, m = 0).
+//   k_psv_scan   the cutoff test (calamp, others.f90:1246-1264, the
+//                ismall > 20 exit, SGTpsv-MPI.f90:606-609, 902-905).
+//   k_psv_epi    TSGT / RSGT / SYNN from the l-contractions (calup,
+//                calupfluid, locallyCartesianDerivatives, udertotsgt,
+//                udertorsgt, utosynn, others.f90:161-344, 983-1031).
+#include <algorithm>
+#include <cmath>
+
 #include "engine.cuh"
+
 namespace dsm {
-Engine* make_psv_engine(const dsm_psv_setup_t*, const dsm_options_t*) {
-    throw Error(DSM_ERR_INVALID, "PSV engine not built yet");
+namespace {
+
+constexpr int NS0 = 4, NS1 = 8, NS2 = 6;  // slots per |m|
+constexpr int NFLD = 5;                   // U, U', V/lsq, V'/lsq, l(l+1) V/lsq
+constexpr int NB = 6;                     // basis right-hand sides of a solve
+
+struct PsvDev {
+    int nzone, nn, itmp, R, Th, jsrc, spn;
+    int n_sel, n_fel, n_hm;
+    const int *iphase, *nlayer, *kkdr, *elem, *hmoff;
+    const int* blkoff;      // [nzone] first block column of each zone
+    int ncol_tot;
+    const double *qmu, *qkappa;
+    const double *sel, *fel, *hm;
+    // assembly map per global column (1-based, [nn+1])
+    const int *amz, *amc;   // [nn+1][2] zone (or -1) and zone-local column
+    const int* bcrow;       // 0, 2 or 3
+    const double* bcval;
+    double tlen, omegai, rmax, r0, ecC0, ecF0, ecL0, ra0, ra1;
+    const double* poly;     // [24]
+    // receivers
+    const int* rcap;        // [R][6] capture index of g0(ksta-1 .. ksta+4)
+    int cap_n1, cap_n;      // capture index of rows nn-1, nn
+    int cap_p0, cap_p1;     // capture index of the probe rows ksta(r_n)-1, ksta(r_n)
+    const double *wv, *wd;
+    const int* fluid;       // [R]
+    const double *lam, *qkp, *fr;  // [R]  lambda, Qkappa, float(r)
+    // l = 0 compaction
+    int nn0, itmp0, kc0;    // compact size, first row kept, compact row of jtmp
+    const int* comp_src;    // global row -> compact row (or 0 when dropped), [nn+1]
+    const int* jsta;        // [R]
+};
+
+__device__ __forceinline__ cd coefq(double omega, double q) {
+    if (q <= 0.0) return mk(1.0);
+    double aa = (omega == 0.0) ? 1.0 : 1.0 + log(omega / (2.0 * kPi)) / (kPi * q);
+    double bb = 1.0 / (2.0 * q);
+    return mk(aa, bb) * mk(aa, bb);
 }
+
+// ----------------------------------------------------------- omega pieces
+struct ZoneCtx {
+    const PsvDev* d;
+    int z, off;
+    cd c1, c2, comega2;
+    __device__ double E(int k, int nnn) const {
+        return d->sel[(size_t)k * d->n_sel + (off - 1) + (nnn - 1)];
+    }
+    // cala0 entry n (1-based, cwork)
+    __device__ cd cw0(int n) const {
+        if (n % 4 == 1) {
+            int nnn = (n + 3) / 4;
+            if (nnn % 4 == 3) return mk(0.0);
+            cd hh0 = c2 * mk(4.0 * E(DSM_PSV_H1X, nnn)) + c1 * mk(16.0 / 3.0 * E(DSM_PSV_H2N, nnn)) +
+                     c1 * mk(-4.0 * E(DSM_PSV_H2N, nnn)) +
+                     c2 * mk(2.0 * (E(DSM_PSV_H3AY, nnn) + E(DSM_PSV_H5AY, nnn))) -
+                     c1 * mk(4.0 / 3.0 * (E(DSM_PSV_H4AN, nnn) + E(DSM_PSV_H6AN, nnn))) +
+                     c2 * mk(3.0 * E(DSM_PSV_H7Z, nnn) - 2.0 * E(DSM_PSV_H7Y, nnn)) +
+                     c1 * mk(4.0 / 3.0 * E(DSM_PSV_H8N, nnn));
+            return comega2 * mk(E(DSM_PSV_T, nnn)) - hh0;
+        }
+        if (n % 4 == 0) {
+            int nnn = n / 4;
+            if (nnn % 4 == 3) return mk(0.0);
+            cd hh0 = c1 * mk(E(DSM_PSV_H2L, nnn)) + c1 * mk(-2.0 * E(DSM_PSV_H2N, nnn)) -
+                     c1 * mk(E(DSM_PSV_H4AL, nnn) + E(DSM_PSV_H6AL, nnn)) + c1 * mk(E(DSM_PSV_H8L, nnn));
+            return comega2 * mk(E(DSM_PSV_T, nnn)) - hh0;
+        }
+        return mk(0.0);
+    }
+    // cala1 entry n
+    __device__ cd cw1(int n) const {
+        if (n % 4 == 2) {
+            int nnn = (n + 2) / 4;
+            if (nnn % 4 == 3) return mk(0.0);
+            cd hh1 = -c2 * mk(2.0 * E(DSM_PSV_H1X, nnn)) - c1 * mk(8.0 / 3.0 * E(DSM_PSV_H2N, nnn)) -
+                     c1 * mk(E(DSM_PSV_H2L, nnn)) - c1 * mk(-2.0 * E(DSM_PSV_H2N, nnn)) -
+                     c2 * mk(E(DSM_PSV_H3Y, nnn)) - c1 * mk(-2.0 / 3.0 * E(DSM_PSV_H4N, nnn)) +
+                     c1 * mk(E(DSM_PSV_H6L, nnn));
+            return -hh1;
+        }
+        if (n % 4 == 3) {
+            int nnn = (n + 1) / 4;
+            if (nnn % 4 != 2) return mk(0.0);
+            cd hh1 = -c2 * mk(2.0 * E(DSM_PSV_H1X, nnn)) - c1 * mk(8.0 / 3.0 * E(DSM_PSV_H2N, nnn)) -
+                     c1 * mk(-2.0 * E(DSM_PSV_H2N, nnn)) - c1 * mk(E(DSM_PSV_H2L, nnn)) +
+                     c1 * mk(E(DSM_PSV_H4L, nnn)) - c2 * mk(E(DSM_PSV_H5Y, nnn)) +
+                     c1 * mk(2.0 / 3.0 * E(DSM_PSV_H6N, nnn));
+            return -hh1;
+        }
+        return mk(0.0);
+    }
+    // cala2 entry n
+    __device__ cd cw2(int n) const {
+        if (n % 4 == 1) {
+            int nnn = (n + 3) / 4;
+            if (nnn % 4 == 3) return mk(0.0);
+            return -(c1 * mk(E(DSM_PSV_H2L, nnn)));
+        }
+        if (n % 4 == 0) {
+            int nnn = n / 4;
+            if (nnn % 4 == 3) return mk(0.0);
+            return -(c2 * mk(E(DSM_PSV_H1X, nnn)) + c1 * mk(4.0 / 3.0 * E(DSM_PSV_H2N, nnn)));
+        }
+        return mk(0.0);
+    }
+};
+
+// overlapa (calmat.f90:670-714): band entry (ii, i) of a zone block from the
+// element array entries cw(n)
+template <class F>
+__device__ cd overlapa_entry(int nl, int ii, int i, F cw) {
+    int nsize = 2 * (nl + 1), msize = 16 * nl;
+    if (i == 1) return ii == 4 ? cw(1) : mk(0.0);
+    if (i == 2) return ii == 3 ? cw(2) : (ii == 4 ? cw(4) : mk(0.0));
+    if (i % 2 == 1) {  // 3 .. nsize-1
+        int n1 = 16 * (i - 3) / 2 + 5;
+        if (ii == 2) return cw(n1);
+        if (ii == 3) return cw(n1 + 2);
+        if (ii == 4) return (i != nsize - 1) ? cw(n1 + 8) + cw(n1 + 12) : cw(msize - 3);
+        return mk(0.0);
+    }
+    int n1 = 16 * (i - 4) / 2 + 6;  // even, 4 .. nsize
+    if (ii == 1) return cw(n1);
+    if (ii == 2) return cw(n1 + 2);
+    if (i != nsize) {
+        if (ii == 3) return cw(n1 + 8) + cw(n1 + 12);
+        return cw(n1 + 10) + cw(n1 + 14);
+    }
+    if (ii == 3) return cw(msize - 2);
+    return cw(msize);
+}
+
+__global__ void k_psv_omega(PsvDev d, const int* __restrict__ freqs, cd* __restrict__ B0,
+                            cd* __restrict__ B1, cd* __restrict__ B2) {
+    int w = blockIdx.y;
+    int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= d.ncol_tot) return;
+    int z = 0;
+    while (z + 1 < d.nzone && d.blkoff[z + 1] <= col) ++z;
+    int c = col - d.blkoff[z] + 1;
+    double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
+    cd comega2 = mk(omega, -d.omegai) * mk(omega, -d.omegai);
+    cd c1 = coefq(omega, d.qmu[z]);
+    cd c2 = coefq(omega, d.qkappa[z]);
+    int nl = d.nlayer[z];
+    size_t o = ((size_t)w * d.ncol_tot + col) * 4;
+    if (d.iphase[z] == 1) {
+        ZoneCtx zc{&d, z, d.elem[z], c1, c2, comega2};
+        for (int ii = 1; ii <= 4; ++ii) {
+            B0[o + ii - 1] = overlapa_entry(nl, ii, c, [&](int n) { return zc.cw0(n); });
+            B2[o + ii - 1] = overlapa_entry(nl, ii, c, [&](int n) { return zc.cw2(n); });
+            cd a1 = overlapa_entry(nl, ii, c, [&](int n) { return zc.cw1(n); });
+            // calhml (calmat.f90:629-664)
+            if (ii == 1 || ii == 3) {
+                auto H = [&](int k, int lo, int m, int n) {
+                    return d.hm[(size_t)k * 4 * d.n_hm + 4 * (size_t)(d.hmoff[z] - 1 + n - 1) + (m - lo)];
+                };
+                if (c % 2 == 0 && !(ii == 1 && c == 2)) {
+                    int m = (-ii + 3) / 2, n = (ii + c - 3) / 2;
+                    a1 = a1 - (-(c2 * mk(H(DSM_PSV_H3MY, -2, m, n))) +
+                               c1 * mk(2.0 / 3.0 * H(DSM_PSV_H4M2N, -2, m, n)) +
+                               c1 * mk(H(DSM_PSV_H6M2L, -2, m, n)));
+                } else if (c % 2 == 1 && c >= 3 && c <= 2 * nl + 1 && !(ii == 1 && c == 3)) {
+                    int m = (-ii + 5) / 2, n = (ii + c - 4) / 2;
+                    a1 = a1 - (c1 * mk(H(DSM_PSV_H4M1L, -1, m, n)) -
+                               c2 * mk(H(DSM_PSV_H5MY, -1, m, n)) +
+                               c1 * mk(2.0 / 3.0 * H(DSM_PSV_H6M1N, -1, m, n)));
+                }
+            }
+            B1[o + ii - 1] = a1;
+        }
+    } else {
+        cd coef = mk(1.0) / c2;
+        const double* p1 = d.fel + (d.elem[z] - 1);
+        const double* p2 = d.fel + d.n_fel + (d.elem[z] - 1);
+        const double* p3 = d.fel + 2 * (size_t)d.n_fel + (d.elem[z] - 1);
+        auto b0 = [&](int n) {
+            if (n % 4 == 3) return mk(0.0);
+            return -(mk(p1[n - 1]) / comega2) + coef * mk(p3[n - 1]);
+        };
+        auto b2 = [&](int n) {
+            if (n % 4 == 3) return mk(0.0);
+            return -(mk(p2[n - 1]) / comega2);
+        };
+        // overlapb (calmat.f90:720-742)
+        auto ovb = [&](int ii, auto f) -> cd {
+            if (ii == 4) {
+                if (c == 1) return f(1);
+                if (c == nl + 1) return f(4 * nl);
+                return f(4 * (c - 1)) + f(4 * (c - 1) + 1);
+            }
+            if (ii == 3 && c >= 2) return f(4 * (c - 2) + 2);
+            return mk(0.0);
+        };
+        for (int ii = 1; ii <= 4; ++ii) {
+            B0[o + ii - 1] = ovb(ii, b0);
+            B2[o + ii - 1] = ovb(ii, b2);
+            B1[o + ii - 1] = mk(0.0);
+        }
+    }
+}
+
+// band entries a(1..4, jj) of one global column for order l (cala + calbc)
+__device__ __forceinline__ void assemble(const PsvDev& d, int jj, const cd* __restrict__ B0,
+                                         const cd* __restrict__ B1, const cd* __restrict__ B2,
+                                         double l2, double lsq, cd a[4]) {
+    a[0] = a[1] = a[2] = a[3] = mk(0.0);
+    for (int e = 0; e < 2; ++e) {
+        int z = d.amz[2 * jj + e];
+        if (z < 0) break;
+        size_t o = ((size_t)d.blkoff[z] + d.amc[2 * jj + e] - 1) * 4;
+        if (d.iphase[z] == 1) {
+            for (int ii = 2; ii <= 4; ii += 2) {
+                cd x0 = B0[o + ii - 1], x2 = B2[o + ii - 1];
+                a[ii - 1] = a[ii - 1] + mk(x0.re + l2 * x2.re, x0.im + l2 * x2.im);
+            }
+            for (int ii = 1; ii <= 3; ii += 2) {
+                cd x1 = B1[o + ii - 1];
+                a[ii - 1] = a[ii - 1] + mk(lsq * x1.re, lsq * x1.im);
+            }
+        } else {
+            for (int ii = 3; ii <= 4; ++ii) {
+                cd x0 = B0[o + ii - 1], x2 = B2[o + ii - 1];
+                a[ii - 1] = a[ii - 1] + mk(x0.re + l2 * x2.re, x0.im + l2 * x2.im);
+            }
+        }
+    }
+    int br = d.bcrow[jj];
+    if (br == 2) a[1] = mk(d.bcval[jj]);
+    else if (br == 3) a[2] = -mk(d.bcval[jj]);
+}
+
+// ---------------------------------------------------------------- solve
+// Streaming LDL^T of the band system rows itmp..nn (local rows 1..n).
+// Window W[p][q] holds the current values of A(k+p, k+q), q <= p <= 3.
+__global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restrict__ B0all,
+                                                   const cd* __restrict__ B1all,
+                                                   const cd* __restrict__ B2all, int lc, int l0,
+                                                   int nsys, int jmin_loc, const int* __restrict__ capmap,
+                                                   cd* __restrict__ Lst, cd* __restrict__ Zst,
+                                                   cd* __restrict__ Xcap) {
+    int sys = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sys >= nsys) return;
+    int w = sys / lc, l = l0 + sys % lc;
+    const size_t bo = (size_t)w * d.ncol_tot * 4;
+    const cd *B0 = B0all + bo, *B1 = B1all + bo, *B2 = B2all + bo;
+    const double l2 = (double)l * (double)(l + 1);
+    const double lsq = sqrt(l2);
+    const int it = d.itmp, n = d.nn - it + 1;
+    const int ls = d.jsrc - it + 1;  // local row of the first source row
+    cd W[4][4];
+    for (int p = 0; p < 4; ++p)
+        for (int q = 0; q < 4; ++q) W[p][q] = mk(0.0);
+    cd a[4];
+    for (int p = 0; p < 4 && p < n; ++p) {
+        assemble(d, it + p, B0, B1, B2, l2, lsq, a);
+        for (int q = 0; q <= p; ++q) W[p][q] = a[4 - (p - q) - 1];
+    }
+    // dcsbdlv0 reads a(m-1,2) = a(2,2) of the unfactored band at row 2
+    assemble(d, it + 1, B0, B1, B2, l2, lsq, a);
+    const cd a22raw = a[1];
+    // forward-substitution state of the four source basis vectors
+    cd zs[4][3];  // z(j-3), z(j-2), z(j-1) of each basis (unscaled)
+    for (int b = 0; b < 4; ++b) zs[b][0] = zs[b][1] = zs[b][2] = mk(0.0);
+    cd wp1[3] = {mk(0.0), mk(0.0), mk(0.0)}, wp2[3] = {mk(0.0), mk(0.0), mk(0.0)};  // w of steps k-1, k-2
+    cd zcur[4];
+    for (int b = 0; b < 4; ++b) zcur[b] = mk(ls + b == 1 ? 1.0 : 0.0);  // z(1) = b(1)
+    cd Dm1 = mk(1.0), Lnn1 = mk(0.0);
+    for (int k = 1; k <= n; ++k) {
+        const cd D = W[0][0];
+        // finish z(k): scaled value zh(k) = z(k) / D(k)
+        for (int b = 0; b < 4; ++b) {
+            if (k >= ls) Zst[((size_t)k * 4 + b) * nsys + sys] = zcur[b] / D;
+            zs[b][0] = zs[b][1];
+            zs[b][1] = zs[b][2];
+            zs[b][2] = zcur[b];
+        }
+        if (k == n) break;
+        if (k == n - 1) Dm1 = D;
+        cd piv = mk(1.0) / D;
+        int nw = min(3, n - k);
+        cd wv_[3] = {mk(0.0), mk(0.0), mk(0.0)}, zv[3] = {mk(0.0), mk(0.0), mk(0.0)};
+        for (int p = 1; p <= nw; ++p) {
+            zv[p - 1] = -W[p][0];
+            wv_[p - 1] = W[p][0] * piv;
+        }
+        if (k >= jmin_loc)
+            for (int p = 0; p < 3; ++p) Lst[((size_t)k * 3 + p) * nsys + sys] = wv_[p];
+        if (k == n - 1) Lnn1 = wv_[0];
+        if (k <= n - 3) {  // main loop of dcsymbdl0: A(k+p,k+q) += w_q z_p
+            W[1][1] = W[1][1] + wv_[0] * zv[0];
+            W[2][2] = W[2][2] + wv_[1] * zv[1];
+            W[3][3] = W[3][3] + wv_[2] * zv[2];
+            W[2][1] = W[2][1] + wv_[0] * zv[1];
+            W[3][2] = W[3][2] + wv_[1] * zv[2];
+            W[3][1] = W[3][1] + wv_[0] * zv[2];
+        } else {  // last two steps: A(k+p,k+q) += w_p z_q
+            for (int jj = 2; jj <= nw + 1; ++jj)
+                for (int ii = 2; ii <= jj; ++ii)
+                    W[jj - 1][ii - 1] = W[jj - 1][ii - 1] + wv_[jj - 2] * zv[ii - 2];
+        }
+        // shift the window and bring in row k+4
+        for (int p = 0; p < 3; ++p)
+            for (int q = 0; q <= p; ++q) W[p][q] = W[p + 1][q + 1];
+        for (int q = 0; q < 4; ++q) W[3][q] = mk(0.0);
+        if (k + 4 <= n) {
+            assemble(d, it + k + 3, B0, B1, B2, l2, lsq, a);
+            for (int q = 0; q < 4; ++q) W[3][q] = a[q];
+        }
+        // forward substitution of row j = k+1 (dcsbdlv0, m = 3)
+        int j = k + 1;
+        for (int b = 0; b < 4; ++b) {
+            cd rhs = mk(ls + b == j ? 1.0 : 0.0);
+            if (j == 2) {
+                zcur[b] = rhs - a22raw * zs[b][2];
+            } else if (j == 3) {  // a(2,3) z(1) + a(3,3) z(2)
+                cd sum = mk(0.0) + wp1[1] * zs[b][1] + wv_[0] * zs[b][2];
+                zcur[b] = rhs - sum;
+            } else {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
+                cd sum = mk(0.0) + wp2[2] * zs[b][0] + wp1[1] * zs[b][1] + wv_[0] * zs[b][2];
+                zcur[b] = rhs - sum;
+            }
+        }
+        for (int p = 0; p < 3; ++p) { wp2[p] = wp1[p]; wp1[p] = wv_[p]; }
+    }
+    // upward substitution.  x(n) = zh(n); x(n-1) = zh(n-1) - L(n,n-1) x(n);
+    // x(j) = zh(j) - [L(j+3,j) x(j+3) + L(j+2,j) x(j+2) + L(j+1,j) x(j+1)]
+    const cd Dn = W[0][0];
+    cd x[NB][3];  // x(j+1), x(j+2), x(j+3)
+    cd xn[NB];
+    for (int b = 0; b < 4; ++b) xn[b] = (n >= ls) ? Zst[((size_t)n * 4 + b) * nsys + sys] : mk(0.0);
+    // surface basis: e_{n-1}: z(n-1) = 1, z(n) = -L(n,n-1); e_n: z(n) = 1
+    xn[4] = (mk(0.0) - Lnn1 * mk(1.0)) / Dn;
+    xn[5] = mk(1.0) / Dn;
+    auto capture = [&](int jloc, const cd* v) {
+        int c = capmap[jloc + it - 1];
+        if (c >= 0)
+            for (int b = 0; b < NB; ++b) Xcap[((size_t)c * NB + b) * nsys + sys] = v[b];
+    };
+    capture(n, xn);
+    for (int b = 0; b < NB; ++b) { x[b][0] = xn[b]; x[b][1] = mk(0.0); x[b][2] = mk(0.0); }
+    if (n - 1 >= jmin_loc) {
+        cd v[NB];
+        cd L1 = Lst[((size_t)(n - 1) * 3 + 0) * nsys + sys];
+        for (int b = 0; b < NB; ++b) {
+            cd zh = mk(0.0);
+            if (b < 4 && n - 1 >= ls) zh = Zst[((size_t)(n - 1) * 4 + b) * nsys + sys];
+            if (b == 4) zh = mk(1.0) / Dm1;
+            v[b] = zh - L1 * x[b][0];
+        }
+        capture(n - 1, v);
+        for (int b = 0; b < NB; ++b) { x[b][1] = x[b][0]; x[b][0] = v[b]; }
+    }
+    for (int j1 = n - 2; j1 >= jmin_loc; --j1) {
+        cd L1 = Lst[((size_t)j1 * 3 + 0) * nsys + sys];
+        cd L2 = Lst[((size_t)j1 * 3 + 1) * nsys + sys];
+        cd L3 = Lst[((size_t)j1 * 3 + 2) * nsys + sys];
+        cd v[NB];
+        for (int b = 0; b < NB; ++b) {
+            cd zh = mk(0.0);
+            if (b < 4 && j1 >= ls) zh = Zst[((size_t)j1 * 4 + b) * nsys + sys];
+            cd sum;
+            if (j1 == n - 2) sum = mk(0.0) + L2 * x[b][1] + L1 * x[b][0];
+            else sum = mk(0.0) + L3 * x[b][2] + L2 * x[b][1] + L1 * x[b][0];
+            v[b] = zh - sum;
+        }
+        capture(j1, v);
+        for (int b = 0; b < NB; ++b) { x[b][2] = x[b][1]; x[b][1] = x[b][0]; x[b][0] = v[b]; }
+    }
+}
+
+// ------------------------------------------------------------ l = 0 path
+// One thread per frequency: compacted tridiagonal (rea2), its LDL^T and the
+// solves of the three m = 0 sources (imt 1..3) and the back-propagated
+// vertical force.  Writes the fields of column l = 0.
+__device__ void calabnum_dev(const PsvDev& d, double omega, cd c1, cd c2, cd* anum, cd* bnum);
+__device__ void calya_dev(const cd* anum, const cd* bnum, double l2, double ra0, double ra1, double r0,
+                          cd* ya, cd* yb, cd* yc, cd* yd);
+__device__ void calg_dev(const PsvDev& d, int l, int m, cd c1, cd c2, double lsq, const cd* ya,
+                         const cd* yb, const cd* yc, const cd* yd, int imt, cd* g);
+
+__device__ __forceinline__ void put_field(double* Aw, int Lcap, int R, int q, int r, int f, cd v) {
+    size_t row = ((size_t)(q * (R + 1) + r) * NFLD + f) * 2;
+    Aw[row * Lcap] = v.re;
+    Aw[(row + 1) * Lcap] = v.im;
+}
+
+__global__ void k_psv_l0(PsvDev d, const int* __restrict__ freqs, int nf, const cd* __restrict__ B0all,
+                         const cd* __restrict__ B1all, const cd* __restrict__ B2all,
+                         cd* __restrict__ scratch, double* __restrict__ A0f, double* __restrict__ A1f,
+                         double* __restrict__ A2f, int Lcap, int back) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nf) return;
+    const int nn = d.nn, R = d.R;
+    const size_t bo = (size_t)w * d.ncol_tot * 4;
+    const cd *B0 = B0all + bo, *B1 = B1all + bo, *B2 = B2all + bo;
+    // scratch per frequency: c(2, nn0) and 4 right-hand sides d(nn0)
+    cd* C = scratch + (size_t)w * (d.nn0 + 1) * 6;
+    auto Cc = [&](int i, int j) -> cd& { return C[(size_t)j * 6 + (i - 1)]; };
+    auto Dv = [&](int b, int j) -> cd& { return C[(size_t)j * 6 + 2 + b]; };
+    // rea2: rearranged band of the assembled l = 0 matrix
+    int itmp = 0;
+    cd a[4];
+    for (int iz = 0; iz < d.nzone; ++iz) {
+        int kk = d.kkdr[iz], i1 = itmp + 1, i2;
+        if (d.iphase[iz] == 1) {
+            i2 = (iz != d.nzone - 1) ? i1 + (d.kkdr[iz + 1] - kk) / 2 - 1 : i1 + (nn + 1 - kk) / 2 - 1;
+            assemble(d, kk, B0, B1, B2, 0.0, 0.0, a);
+            if (iz != 0) {
+                cd ap[4];
+                assemble(d, kk, B0, B1, B2, 0.0, 0.0, ap);
+                Cc(1, i1) = (d.iphase[iz - 1] == 2) ? ap[2] : ap[1];
+            }
+            Cc(2, i1) = a[3];
+            for (int i = i1 + 1; i <= i2; ++i) {
+                assemble(d, kk + 2 * (i - i1), B0, B1, B2, 0.0, 0.0, a);
+                Cc(1, i) = a[1];
+                Cc(2, i) = a[3];
+            }
+        } else {
+            i2 = i1 + (d.kkdr[iz + 1] - kk) - 1;
+            assemble(d, kk, B0, B1, B2, 0.0, 0.0, a);
+            if (iz != 0) Cc(1, i1) = (d.iphase[iz - 1] == 1) ? a[1] : a[2];
+            Cc(2, i1) = a[3];
+            for (int i = i1 + 1; i <= i2; ++i) {
+                assemble(d, kk + (i - i1), B0, B1, B2, 0.0, 0.0, a);
+                Cc(1, i) = a[2];
+                Cc(2, i) = a[3];
+            }
+        }
+        itmp = i2;
+    }
+    const int n0 = d.nn0, it0 = d.itmp0, n = n0 - it0 + 1;
+    // right-hand sides: calg at l = 0, m = 0 for imt 1..3; back source
+    const double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
+    cd c1 = coefq(omega, d.qmu[d.spn - 1]), c2 = coefq(omega, d.qkappa[d.spn - 1]);
+    cd anum[160], bnum[160], ya[4], yb[4], yc[4], yd[4];
+    calabnum_dev(d, omega, c1, c2, anum, bnum);
+    calya_dev(anum, bnum, 0.0, d.ra0, d.ra1, d.r0, ya, yb, yc, yd);
+    for (int j = 1; j <= n0; ++j)
+        for (int b = 0; b < 4; ++b) Dv(b, j) = mk(0.0);
+    for (int imt = 1; imt <= 3; ++imt) {
+        cd g[4];
+        calg_dev(d, 0, 0, c1, c2, 0.0, ya, yb, yc, yd, imt, g);
+        // rea2 maps rows jtmp..jtmp+3 of g0; only the U rows survive
+        for (int k = 0; k < 4; ++k) {
+            int cr = d.comp_src[d.jsrc + k];
+            if (cr > 0) Dv(imt - 1, cr) = g[k];
+        }
+    }
+    {
+        // caldveczero m = 0: bvec(1,0) = cmplx(coef), single precision
+        double coef = sqrt((double)1 / (4.0 * kPi) / 1.0);
+        cd rd = mk((double)(float)coef);
+        int cr = d.comp_src[nn - 1];
+        if (cr > 0) Dv(3, cr) = -conj(rd);
+    }
+    // dcsymbdl0 with m = 1 on rows it0..n0 (local 1..n)
+    // local row i -> compact row i + it0 - 1
+    auto CL = [&](int i, int j) -> cd& { return Cc(i, j + it0 - 1); };
+    for (int k = 1; k <= n - 1; ++k) {
+        cd piv = mk(1.0) / CL(2, k);
+        cd z2 = -CL(1, k + 1);
+        cd w2 = CL(1, k + 1) * piv;
+        CL(1, k + 1) = w2;
+        CL(2, k + 1) = CL(2, k + 1) + w2 * z2;
+    }
+    // dcsbdlv0 (m = 1) for the four right-hand sides
+    for (int b = 0; b < 4; ++b) {
+        if (b == 3 && !back) continue;
+        auto DL = [&](int j) -> cd& { return Dv(b, j + it0 - 1); };
+        // z stored in place of d: z(j) = b(j) - a(1,j) z(j-1)
+        cd zprev = DL(1);
+        for (int j = 2; j <= n; ++j) {
+            cd zj = DL(j) - CL(1, j) * zprev;
+            DL(j) = zj;
+            zprev = zj;
+        }
+        for (int j = 1; j <= n; ++j) DL(j) = DL(j) / CL(2, j);
+        for (int j = 1; j <= n - 1; ++j) DL(n - j) = DL(n - j) - CL(1, n - j + 1) * DL(n - j + 1);
+    }
+    // fields of column l = 0: m = 0 slots q = 0..2 (imt 1..3), 3 (back)
+    const int rows0 = NS0 * (R + 1) * NFLD * 2, rows1 = NS1 * (R + 1) * NFLD * 2,
+              rows2 = NS2 * (R + 1) * NFLD * 2;
+    double* A0w = A0f + (size_t)w * rows0 * Lcap;
+    double* A1w = A1f + (size_t)w * rows1 * Lcap;
+    double* A2w = A2f + (size_t)w * rows2 * Lcap;
+    for (int r = 0; r <= R; ++r) {
+        for (int q = 0; q < NS0; ++q) {
+            cd U = mk(0.0), Ud = mk(0.0);
+            if (q < 3 || back) {
+                if (r < R) {
+                    for (int i = 0; i < 3; ++i) {
+                        cd v = Dv(q, d.jsta[r] + i);
+                        U = U + d.wv[3 * r + i] * v;
+                        Ud = Ud + d.wd[3 * r + i] * v;
+                    }
+                } else if (q < 3) {
+                    U = Dv(q, n0);
+                }
+            }
+            put_field(A0w, Lcap, R, q, r, 0, U);
+            put_field(A0w, Lcap, R, q, r, 1, Ud);
+            for (int f = 2; f < NFLD; ++f) put_field(A0w, Lcap, R, q, r, f, mk(0.0));
+        }
+        for (int q = 0; q < NS1; ++q)
+            for (int f = 0; f < NFLD; ++f) put_field(A1w, Lcap, R, q, r, f, mk(0.0));
+        for (int q = 0; q < NS2; ++q)
+            for (int f = 0; f < NFLD; ++f) put_field(A2w, Lcap, R, q, r, f, mk(0.0));
+    }
+}
+
+// ------------------------------------------------------- source terms
+__device__ void calabnum_dev(const PsvDev& d, double omega, cd coef1, cd coef2, cd* anum, cd* bnum) {
+    for (int k = 0; k < 160; ++k) anum[k] = bnum[k] = mk(0.0);
+    auto AN = [&](int i, int j, int k) -> cd& { return anum[(k - 1) * 16 + (j - 1) * 4 + (i - 1)]; };
+    auto BN = [&](int i, int j, int k) -> cd& { return bnum[(k - 1) * 16 + (j - 1) * 4 + (i - 1)]; };
+    const double* P = d.poly;
+    for (int i = 1; i <= 10; ++i) {
+        double r;
+        if (i <= 5) r = d.ra0 + (double)(i - 1) / 4.0 * (d.r0 - d.ra0);
+        else r = d.ra1 - (double)(10 - i) / 4.0 * (d.ra1 - d.r0);
+        double trho = 0, tvpv = 0, tvph = 0, tvsv = 0, tvsh = 0, teta = 0, coef = 1.0;
+        for (int j = 1; j <= 4; ++j) {
+            if (j == 1) coef = 1.0;
+            else coef = coef * (r / d.rmax);
+            trho = trho + P[0 + j - 1] * coef;
+            tvpv = tvpv + P[4 + j - 1] * coef;
+            tvph = tvph + P[8 + j - 1] * coef;
+            tvsv = tvsv + P[12 + j - 1] * coef;
+            tvsh = tvsh + P[16 + j - 1] * coef;
+            teta = teta + P[20 + j - 1] * coef;
+        }
+        double tecA = trho * tvph * tvph, tecC = trho * tvpv * tvpv;
+        double tecL = trho * tvsv * tvsv, tecN = trho * tvsh * tvsh, tmu = trho * tvsv * tvsv;
+        double tAkappa = tecA - tmu * 4.0 / 3.0, tCkappa = tecC - tmu * 4.0 / 3.0;
+        cd xAkappa = mk(tAkappa) * coef2, xCkappa = mk(tCkappa) * coef2;
+        cd xrho = mk(trho), xmu = mk(tmu) * coef1, xecL = mk(tecL) * coef1, xecN = mk(tecN) * coef1;
+        cd xecA = xAkappa + xmu * mk(4.0 / 3.0);
+        cd xecC = xCkappa + xmu * mk(4.0 / 3.0);
+        cd xecF = mk(teta) * (xecA - mk(2.0) * xecL);
+        cd xFdC = xecF / xecC;
+        cd xAmF2dC = xecA - xecF * xFdC;
+        double r2 = r * r;
+        cd comega2 = mk(omega, -d.omegai) * mk(omega, -d.omegai);
+        AN(1, 1, i) = -(mk(2.0 / r) * xFdC);
+        AN(1, 2, i) = mk(1.0) / xecC;
+        AN(2, 1, i) = -(xrho * comega2) + mk(4.0 / r2) * (xAmF2dC - xecN);
+        AN(2, 2, i) = mk(2.0 / r) * (xFdC - mk(1.0));
+        AN(3, 1, i) = -mk(1.0 / r);
+        AN(3, 3, i) = mk(1.0 / r);
+        AN(3, 4, i) = mk(1.0) / xecL;
+        AN(4, 1, i) = -(mk(2.0 / r2) * (xAmF2dC - xecN));
+        AN(4, 2, i) = -(mk(1.0 / r) * xFdC);
+        AN(4, 3, i) = -(xrho * comega2) - mk(2.0 / r2) * xecN;
+        AN(4, 4, i) = -mk(3.0 / r);
+        BN(1, 3, i) = mk(1.0 / r) * xFdC;
+        BN(2, 3, i) = -(mk(2.0 / r2) * (xAmF2dC - xecN));
+        BN(2, 4, i) = mk(1.0 / r);
+        BN(4, 3, i) = xAmF2dC / mk(r2);
+    }
+}
+
+__device__ void eqm(const cd* anum, const cd* bnum, int blk, double l2, const cd* y, cd* f) {
+    int mt = 16 * (blk - 1);
+    for (int i = 0; i < 4; ++i) f[i] = mk(0.0);
+    cd c[4][4];
+    for (int j = 0; j < 4; ++j)
+        for (int i = 0; i < 4; ++i) {
+            cd b = bnum[mt];
+            c[i][j] = anum[mt] + mk(l2 * b.re, l2 * b.im);
+            mt++;
+        }
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) f[i] = f[i] + c[i][j] * y[j];
+}
+
+// rk3 with one rkstep (src/SGTpsv/rk3.f90); x0 becomes xe
+__device__ void rk1(const cd* anum, const cd* bnum, const int* blk, double l2, double& x0, double xe,
+                    cd* y0) {
+    const double c1 = 1.0 / 6.0, c2 = 1.0 / 3.0, c3 = c2, c4 = c1, b2 = 0.5, b3 = b2;
+    double h = (xe - x0) / 1.0;
+    cd ak[4], yn[4], w[4];
+    eqm(anum, bnum, blk[0], l2, y0, ak);
+    for (int i = 0; i < 4; ++i) yn[i] = y0[i] + mk(h * c1) * ak[i];
+    for (int i = 0; i < 4; ++i) w[i] = y0[i] + mk(h * b2) * ak[i];
+    eqm(anum, bnum, blk[1], l2, w, ak);
+    for (int i = 0; i < 4; ++i) yn[i] = yn[i] + mk(h * c2) * ak[i];
+    for (int i = 0; i < 4; ++i) w[i] = y0[i] + mk(h * b3) * ak[i];
+    eqm(anum, bnum, blk[2], l2, w, ak);
+    for (int i = 0; i < 4; ++i) yn[i] = yn[i] + mk(h * c3) * ak[i];
+    for (int i = 0; i < 4; ++i) w[i] = y0[i] + mk(h) * ak[i];
+    eqm(anum, bnum, blk[3], l2, w, ak);
+    for (int i = 0; i < 4; ++i) yn[i] = yn[i] + mk(h * c4) * ak[i];
+    for (int i = 0; i < 4; ++i) y0[i] = yn[i];
+    x0 = xe;
+}
+
+__device__ void calya_dev(const cd* anum, const cd* bnum, double l2, double ra0, double ra1, double r0,
+                          cd* ya, cd* yb, cd* yc, cd* yd) {
+    for (int i = 0; i < 4; ++i) ya[i] = yb[i] = yc[i] = yd[i] = mk(0.0);
+    ya[1] = mk(1.0);
+    yb[3] = mk(1.0);
+    double dr = (r0 - ra0) / 2.0;
+    if (dr > 0.0) {
+        double xs = ra0;
+        const int blk[2][4] = {{1, 2, 2, 3}, {3, 4, 4, 5}};
+        for (int k = 0; k < 2; ++k) {
+            double xe = xs + dr;
+            rk1(anum, bnum, blk[k], l2, xs, xe, ya);
+            xs = xe - dr;
+            rk1(anum, bnum, blk[k], l2, xs, xe, yb);
+        }
+    }
+    yc[1] = mk(1.0);
+    yd[3] = mk(1.0);
+    dr = (ra1 - r0) / 2.0;
+    if (dr > 0.0) {
+        double xs = ra1;
+        const int blk[2][4] = {{10, 9, 9, 8}, {8, 7, 7, 6}};
+        for (int k = 0; k < 2; ++k) {
+            double xe = xs - dr;
+            rk1(anum, bnum, blk[k], l2, xs, xe, yc);
+            xs = xe + dr;
+            rk1(anum, bnum, blk[k], l2, xs, xe, yd);
+        }
+    }
+}
+
+// glu (src/SGTpsv/glu2.f90) on an n x n complex matrix, leading dim 4
+__device__ void glu_dev(cd* a, int n, cd* b) {
+    const double eps = 3.52e-15;
+    auto A = [&](int i, int j) -> cd& { return a[(i - 1) + 4 * (j - 1)]; };
+    int ip[4];
+    cd wk[5];
+    for (int k = 1; k <= n; ++k) {
+        double amax = cabs_(A(k, k));
+        int ipk = k;
+        for (int i = k + 1; i <= n; ++i) {
+            double aik = cabs_(A(i, k));
+            if (aik > amax) { ipk = i; amax = aik; }
+        }
+        ip[k - 1] = ipk;
+        if (!(amax > eps)) return;
+        if (ipk != k) { cd t = A(ipk, k); A(ipk, k) = A(k, k); A(k, k) = t; }
+        for (int i = k + 1; i <= n; ++i) {
+            A(i, k) = -A(i, k) / A(k, k);
+            wk[i] = A(i, k);
+        }
+        for (int j = k + 1; j <= n; ++j) {
+            if (ipk != k) { cd t = A(ipk, j); A(ipk, j) = A(k, j); A(k, j) = t; }
+            cd t = A(k, j);
+            for (int i = k + 1; i <= n; ++i) A(i, j) = A(i, j) + wk[i] * t;
+        }
+    }
+    for (int k = 1; k <= n; ++k) {
+        if (ip[k - 1] != k) { cd t = b[ip[k - 1] - 1]; b[ip[k - 1] - 1] = b[k - 1]; b[k - 1] = t; }
+        cd t = b[k - 1];
+        for (int i = k + 1; i <= n; ++i) b[i - 1] = b[i - 1] + A(i, k) * t;
+    }
+    b[n - 1] = b[n - 1] / A(n, n);
+    for (int k = n - 1; k >= 1; --k) {
+        cd t = b[k];
+        for (int i = 1; i <= k; ++i) b[i - 1] = b[i - 1] - A(i, k + 1) * t;
+        b[k - 1] = b[k - 1] / A(k, k);
+    }
+}
+
+// calg (calmat.f90:1075-1171) for the unit moment tensor imt
+__device__ void calg_dev(const PsvDev& d, int l, int m, cd coef1, cd coef2, double lsq, const cd* ya,
+                         const cd* yb, const cd* yc, const cd* yd, int imt, cd* g) {
+    double mt11 = imt == 1, mt22 = imt == 2, mt33 = imt == 3, mt12 = imt == 4, mt13 = imt == 5,
+           mt23 = imt == 6;
+    double sgn = (m >= 0) ? 1.0 : -1.0;
+    double b1 = sqrt((double)(2 * l + 1) / (16.0 * kPi));
+    double b2 = 0.0;
+    if (l != 0) b2 = sqrt((double)(2 * l + 1) * (double)(l - 1) * (double)(l + 2) / (64.0 * kPi));
+    const double r0 = d.r0, ecC0 = d.ecC0, ecF0 = d.ecF0, ecL0 = d.ecL0;
+    cd dd = mk(0.0), ee = mk(0.0), s1 = mk(0.0), s2 = mk(0.0);
+    int am = abs(m);
+    if (am == 1) ee = mk(-b1 * sgn * mt12, b1 * mt13) / (mk(r0 * r0 * ecL0) * coef1);
+    if (am == 0) {
+        dd = mk(2.0 * b1 * mt11 / (r0 * r0)) /
+             (mk(ecC0 - 4.0 / 3.0 * ecL0) * coef2 + mk(4.0 / 3.0 * ecL0) * coef1);
+        double r03 = r0 * r0 * r0;
+        cd xtmp = ((ecF0 + 2.0 / 3.0 * ecL0) * coef2 - 2.0 / 3.0 * ecL0 * coef1) /
+                  ((ecC0 - 4.0 / 3.0 * ecL0) * coef2 + 4.0 / 3.0 * ecL0 * coef1);
+        s1 = mk(-2.0 * b1 * (mt22 + mt33) / r03) + mk(4.0 * b1 * mt11 / r03) * xtmp;
+        s2 = mk(b1 * lsq * (mt22 + mt33) / r03) - mk(2.0 * b1 * lsq * mt11 / r03) * xtmp;
+    }
+    if (am == 2) {
+        double r03 = r0 * r0 * r0;
+        s2 = mk(-b2 * (mt22 - mt33) / r03, sgn * 2.0 * b2 * mt23 / r03);
+    }
+    cd sv[4];
+    sv[0] = dd;
+    sv[1] = s1;
+    if (l != 0) {
+        sv[2] = mk(ee.re / lsq, ee.im / lsq);
+        sv[3] = mk(s2.re / lsq, s2.im / lsq);
+    } else {
+        sv[2] = sv[3] = mk(0.0);
+    }
+    cd a[16], b[4];
+    if (l != 0) {
+        for (int i = 0; i < 4; ++i) {
+            a[i] = -ya[i]; a[i + 4] = -yb[i]; a[i + 8] = yc[i]; a[i + 12] = yd[i];
+            b[i] = sv[i];
+        }
+        glu_dev(a, 4, b);
+    } else {
+        for (int i = 0; i < 2; ++i) {
+            a[i] = -ya[i]; a[i + 4] = yc[i];
+            b[i] = sv[i];
+        }
+        glu_dev(a, 2, b);
+        b[2] = b[1];
+        b[1] = mk(0.0);
+        b[3] = mk(0.0);
+    }
+    double dt[4];
+    dt[0] = -d.ra0 * d.ra0;
+    dt[1] = dt[0] * lsq;
+    dt[2] = d.ra1 * d.ra1;
+    dt[3] = dt[2] * lsq;
+    for (int i = 0; i < 4; ++i) g[i] = mk(b[i].re * dt[i], b[i].im * dt[i]);
+}
+
+// ----------------------------------------------------------------- fields
+// Flat slot order (18 slots): 0..2 m = 0, imt 1..3; 3 m = 0 back-propagated
+// vertical force; 4..11 |m| = 1: 4 + 4 sg + k (k: imt 4, imt 5, back 2,
+// back 3; sg 0: m = -1, 1: m = +1); 12..17 |m| = 2: 12 + 3 sg + k (imt 2, 3, 6).
+constexpr int NSLOT = 18;
+
+__device__ __forceinline__ int slot_mi(int s) { return s < 4 ? 0 : (s < 12 ? 1 : 2); }
+__device__ __forceinline__ int slot_q(int s) { return s < 4 ? s : (s < 12 ? s - 4 : s - 12); }
+
+// calabnum of every frequency (once per omega)
+__global__ void k_psv_abnum(PsvDev d, const int* __restrict__ freqs, int nf, cd* __restrict__ ab) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nf) return;
+    const double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
+    cd c1 = coefq(omega, d.qmu[d.spn - 1]), c2 = coefq(omega, d.qkappa[d.spn - 1]);
+    calabnum_dev(d, omega, c1, c2, ab + (size_t)w * 320, ab + (size_t)w * 320 + 160);
+}
+
+// Per (omega, l >= 1): weights of the six basis solutions for every slot
+// (calya + calg for the 13 forward sources, caldveczero for the back ones).
+// Layout co[(slot * NB + b) * nsys + sys].
+__global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restrict__ freqs, int lc,
+                                                  int l0, int nsys, const cd* __restrict__ ab,
+                                                  cd* __restrict__ co, int back) {
+    int sys = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sys >= nsys) return;
+    int w = sys / lc, l = l0 + sys % lc;
+    auto put = [&](int slot, const cd* g) {
+        for (int b = 0; b < NB; ++b) co[((size_t)slot * NB + b) * nsys + sys] = g[b];
+    };
+    cd g[NB];
+    for (int b = 0; b < NB; ++b) g[b] = mk(0.0);
+    if (l == 0) {
+        for (int s = 0; s < NSLOT; ++s) put(s, g);
+        return;
+    }
+    const double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
+    const cd c1 = coefq(omega, d.qmu[d.spn - 1]), c2 = coefq(omega, d.qkappa[d.spn - 1]);
+    const double l2 = (double)l * (double)(l + 1), lsq = sqrt(l2);
+    const cd* anum = ab + (size_t)w * 320;
+    const cd* bnum = anum + 160;
+    cd ya[4], yb[4], yc[4], yd[4];
+    calya_dev(anum, bnum, l2, d.ra0, d.ra1, d.r0, ya, yb, yc, yd);
+    for (int s = 0; s < NSLOT; ++s) {
+        for (int b = 0; b < NB; ++b) g[b] = mk(0.0);
+        int mi = slot_mi(s), q = slot_q(s);
+        if (mi == 0) {
+            if (q < 3) {
+                calg_dev(d, l, 0, c1, c2, lsq, ya, yb, yc, yd, q + 1, g);
+            } else if (back) {
+                double coef = sqrt((double)(2 * l + 1) / (4.0 * kPi) / 1.0);
+                g[4] = -conj(mk((double)(float)coef));  // g0(nn-1) = -conjg(rdvec(1,0))
+            }
+        } else if (mi == 1) {
+            int sg = q / 4, k = q % 4, m = sg == 0 ? -1 : 1;
+            if (k < 2) {
+                calg_dev(d, l, m, c1, c2, lsq, ya, yb, yc, yd, 4 + k, g);
+            } else if (back) {
+                // caldveczero, m = 1: bvec(2,1) = -xl2 coef/2, bvec(3,1) = i xl2 coef/2;
+                // m = -1: conjugated and negated (odd m).  g0(nn) = conjg(rdvec)/lsq
+                double fact = (double)l * (double)(l + 1);
+                double coef = sqrt((double)(2 * l + 1) / (4.0 * kPi) / fact);
+                cd v = (k == 2) ? mk(-1.0, 0.0) * l2 * coef / 2.0 : mk(0.0, 1.0) * l2 * coef / 2.0;
+                if (m < 0) v = -conj(v);
+                g[5] = conj(v) / mk(lsq);
+            }
+        } else if (l >= 2) {
+            int sg = q / 3, k = q % 3, m = sg == 0 ? -2 : 2;
+            calg_dev(d, l, m, c1, c2, lsq, ya, yb, yc, yd, k == 0 ? 2 : (k == 1 ? 3 : 6), g);
+        }
+        put(s, g);
+    }
+}
+
+// Per (omega, l >= 1, receiver group): receiver fields of every slot and the
+// cutoff probe (group 0).
+__global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, int lc, int l0, int nsys,
+                                                    const cd* __restrict__ Xcap, const cd* __restrict__ co,
+                                                    double* __restrict__ A0f, double* __restrict__ A1f,
+                                                    double* __restrict__ A2f, int Lcap,
+                                                    double* __restrict__ amps) {
+    int sys = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sys >= nsys) return;
+    int w = sys / lc, l = l0 + sys % lc;
+    if (l == 0) return;  // written by k_psv_l0
+    const int R = d.R;
+    const size_t rows[3] = {(size_t)NS0 * (R + 1) * NFLD * 2, (size_t)NS1 * (R + 1) * NFLD * 2,
+                            (size_t)NS2 * (R + 1) * NFLD * 2};
+    double* Aw[3] = {A0f + (size_t)w * rows[0] * Lcap + l, A1f + (size_t)w * rows[1] * Lcap + l,
+                     A2f + (size_t)w * rows[2] * Lcap + l};
+    const double l2 = (double)l * (double)(l + 1), lsq = sqrt(l2);
+    int rlo = blockIdx.y * 16, rhi = min(rlo + 16, R);
+    bool g0 = blockIdx.y == 0;
+    auto X = [&](int cap, int b) { return Xcap[((size_t)cap * NB + b) * nsys + sys]; };
+    auto C = [&](int s, int b) { return co[((size_t)s * NB + b) * nsys + sys]; };
+    if (g0) {  // probe: calamp on g0(ksta(r_n)-1), g0(ksta(r_n)) of imt = 1, m = 0
+        cd p0 = mk(0.0), p1 = mk(0.0);
+        for (int b = 0; b < 4; ++b) {
+            cd cb = C(0, b);
+            p0 = p0 + cb * X(d.cap_p0, b);
+            p1 = p1 + cb * X(d.cap_p1, b);
+        }
+        double a1 = cabs_(p0), a2 = cabs_(p1);
+        amps[(size_t)w * Lcap + l] = sqrt(a1 * a1 + a2 * a2);
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+        int r_lo = pass == 0 ? rlo : R, r_hi = pass == 0 ? rhi : (g0 ? R + 1 : R);
+        for (int r = r_lo; r < r_hi; ++r) {
+            bool surf = r == R;
+            cd bU[NB], bV[NB], bUd[NB], bVd[NB];
+            for (int b = 0; b < NB; ++b) bU[b] = bV[b] = bUd[b] = bVd[b] = mk(0.0);
+            if (surf) {
+                for (int b = 0; b < NB; ++b) { bU[b] = X(d.cap_n1, b); bV[b] = X(d.cap_n, b); }
+            } else {
+                for (int i = 0; i < 3; ++i) {
+                    double wvi = d.wv[3 * r + i], wdi = d.wd[3 * r + i];
+                    int cu = d.rcap[6 * r + 2 * i], cvv = d.rcap[6 * r + 2 * i + 1];
+                    for (int b = 0; b < NB; ++b) {
+                        cd xu = X(cu, b), xv = X(cvv, b);
+                        bU[b] = bU[b] + wvi * xu;
+                        bV[b] = bV[b] + wvi * xv;
+                        bUd[b] = bUd[b] + wdi * xu;
+                        bVd[b] = bVd[b] + wdi * xv;
+                    }
+                }
+            }
+            for (int s = 0; s < NSLOT; ++s) {
+                int mi = slot_mi(s), q = slot_q(s);
+                bool isback = (s == 3) || (mi == 1 && (q % 4) >= 2);
+                cd U = mk(0.0), V = mk(0.0), Ud = mk(0.0), Vd = mk(0.0);
+                if (!(surf && isback)) {
+                    for (int b = 0; b < NB; ++b) {
+                        cd cb = C(s, b);
+                        U = U + cb * bU[b];
+                        V = V + cb * bV[b];
+                        Ud = Ud + cb * bUd[b];
+                        Vd = Vd + cb * bVd[b];
+                    }
+                }
+                cd Vh = V / lsq, Vdh = Vd / lsq;
+                put_field(Aw[mi], Lcap, R, q, r, 0, U);
+                put_field(Aw[mi], Lcap, R, q, r, 1, Ud);
+                put_field(Aw[mi], Lcap, R, q, r, 2, Vh);
+                put_field(Aw[mi], Lcap, R, q, r, 3, Vdh);
+                put_field(Aw[mi], Lcap, R, q, r, 4, l2 * Vh);
+            }
+        }
+    }
+}
+
+__global__ void k_psv_scan(int nf, int l0, int lc, int Lcap, int maxlmax, double ratl, double tlen,
+                           double vtop, double rtop, const int* __restrict__ freqs,
+                           const double* __restrict__ amps, CutState* __restrict__ cut) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nf) return;
+    CutState c = cut[w];
+    if (c.done) return;
+    double omega = 2.0 * kPi * (double)freqs[w] / tlen;
+    int lsuf = (int)(omega * rtop / vtop - 0.5) + 1;
+    for (int l = l0; l < l0 + lc; ++l) {
+        if (c.ismall > 20) {
+            if (c.llog > l) c.llog = l;
+            c.done = 1;
+            c.norders = l;
+            break;
+        }
+        if (l >= 1) {  // calamp is called for imt = 1 of every m of the l != 0 branch
+            for (int m = -2; m <= 2; ++m) {
+                if (abs(m) > l) continue;
+                double amp = (m == 0) ? amps[(size_t)w * Lcap + l] : 0.0, ampratio = 0.0;
+                if (amp > c.maxamp) c.maxamp = amp;
+                if (amp != 0.0 && c.maxamp != 0.0) ampratio = amp / c.maxamp;
+                if (ampratio < ratl && l >= lsuf) c.ismall++;
+                else c.ismall = 0;
+            }
+        }
+        if (l == maxlmax) { c.done = 1; c.norders = maxlmax + 1; }
+    }
+    cut[w] = c;
+}
+
+// ---------------------------------------------------------------- epilogue
+__global__ void k_psv_epi(PsvDev d, int w, const double* __restrict__ thx, const double* __restrict__ ths,
+                          const int* __restrict__ pole, const int* __restrict__ freqs,
+                          const double* __restrict__ C0, const double* __restrict__ C1,
+                          const double* __restrict__ C2, double* __restrict__ tsgt,
+                          double* __restrict__ rsgt, double* __restrict__ synn, int back) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int R = d.R, Th = d.Th;
+    if (idx >= Th * (R + 1)) return;
+    int it = idx / (R + 1), r = idx % (R + 1);
+    const bool surf = r == R;
+    const bool isp = pole[it] != 0;
+    const int M[3] = {NS0 * (R + 1) * NFLD * 2, NS1 * (R + 1) * NFLD * 2, NS2 * (R + 1) * NFLD * 2};
+    const double* Cm[3] = {C0, C1, C2};
+    const double x = thx[it], s = ths[it];
+    const double fs = (double)(float)s, fc = (double)(float)(x / s);
+    const double fr = surf ? 1.0 : d.fr[r];
+    const bool fluid = !surf && d.fluid[r];
+    const double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
+    const cd comega = mk(omega, -d.omegai);
+    cd T[20], Rg[10], S[10];
+    for (auto& v : T) v = mk(0.0);
+    for (auto& v : Rg) v = mk(0.0);
+    for (auto& v : S) v = mk(0.0);
+    cd efl = mk(0.0);
+    if (fluid) {  // calupfluid factor omega/3/lambda(omega)
+        const double deuxsurpi = 0.63661977236, unsurdeuxpi = 0.15915494309,
+                     unsurtrois = 0.33333333333333333333;
+        double lam = d.lam[r], qk = d.qkp[r];
+        cd fl = mk(lam * 1.0, lam * (1.0 / qk));
+        double fac = 1 + deuxsurpi / qk * log(unsurdeuxpi * comega.re);
+        fl = mk(fl.re * fac, fl.im * fac);
+        efl = comega * unsurtrois / fl;
+    }
+    for (int mi = 0; mi < 3; ++mi) {
+        int nq = mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2);
+        for (int q = 0; q < nq; ++q) {
+            int per = mi == 0 ? 4 : (mi == 1 ? 4 : 3);
+            int sg = q / per, k = q % per;
+            int m = mi == 0 ? 0 : (sg == 0 ? -mi : mi);
+            bool isback = (mi == 0 && k == 3) || (mi == 1 && k >= 2);
+            if (isback && !back) continue;
+            int imt = 0, icomp = 0;
+            if (mi == 0) { if (k < 3) imt = k + 1; else icomp = 1; }
+            else if (mi == 1) { if (k < 2) imt = 4 + k; else icomp = k; }
+            else imt = k == 0 ? 2 : (k == 1 ? 3 : 6);
+            if (surf && isback) continue;
+            if (isp && mi != 0) continue;  // only bvec(1,0) survives at the poles
+            auto G = [&](int f, int b) {
+                size_t row = ((size_t)(q * (R + 1) + r) * NFLD + f) * 2;
+                size_t col = (size_t)b * Th + it;
+                const double* C = Cm[mi];
+                return mk(C[row + (size_t)M[mi] * col], C[row + 1 + (size_t)M[mi] * col]);
+            };
+            double sigma = (m < 0 && (mi & 1)) ? -1.0 : 1.0;
+            double mm = (double)m, m2 = mm * mm;
+            cd d11 = mk(0.0), d12 = mk(0.0), d13 = mk(0.0), d21 = mk(0.0), d22 = mk(0.0),
+               d23 = mk(0.0), d31 = mk(0.0), d32 = mk(0.0), d33 = mk(0.0);
+            cd PU = G(0, 0);
+            if (surf) {
+                cd u1, u2 = mk(0.0), u3 = mk(0.0);
+                if (isp) {
+                    u1 = PU;
+                } else {
+                    u1 = sigma * PU;
+                    u2 = sigma * G(2, 1);
+                    u3 = sigma * cmul_i(mm / s, G(2, 0));
+                }
+                if (imt == 1) { S[0] = S[0] + u1; S[4] = S[4] + u2; }
+                if (imt == 2) {
+                    S[2] = S[2] + 5.e-1 * u1; S[3] = S[3] - 5.e-1 * u1;
+                    S[5] = S[5] - 5.e-1 * u2; S[6] = S[6] - 5.e-1 * u2;
+                }
+                if (imt == 3) {
+                    S[2] = S[2] - 5.e-1 * u1; S[3] = S[3] - 5.e-1 * u1;
+                    S[5] = S[5] - 5.e-1 * u2; S[6] = S[6] + 5.e-1 * u2;
+                }
+                if (imt == 4) { S[1] = S[1] + u1; S[8] = S[8] + u2; }
+                if (imt == 5) { S[9] = S[9] + u3; }
+                if (imt == 6) { S[7] = S[7] - u3; }
+                continue;
+            }
+            if (fluid) {
+                cd e = efl * (isp ? PU : sigma * PU);
+                d11 = e; d22 = e; d33 = e;
+            } else if (isp) {
+                cd u1 = PU, udr1 = G(1, 0);
+                d11 = udr1;
+                d22 = u1 / fr;
+                d33 = u1 / fr;
+            } else {
+                cd PV = G(2, 0), DV = G(2, 1);
+                cd u1 = sigma * PU, u2 = sigma * DV, u3 = sigma * cmul_i(mm / s, PV);
+                cd udr1 = sigma * G(1, 0), udr2 = sigma * G(3, 1), udr3 = sigma * cmul_i(mm / s, G(3, 0));
+                cd udt1 = (m >= 0) ? G(0, 1) : mk(0.0);
+                cd udt2 = sigma * (-(x / s) * DV + (m2 / (1 - x * x)) * PV - G(4, 0));
+                cd udt3 = sigma * cmul_i(mm, -(x / (1 - x * x)) * PV + (1.0 / s) * DV);
+                cd udp1 = sigma * cmul_i(mm, PU), udp2 = sigma * cmul_i(mm, DV);
+                cd udp3 = sigma * ((-m2 / s) * PV);
+                d11 = udr1;
+                d12 = (udt1 - u2) / fr;
+                d13 = (udp1 / fs - u3) / fr;
+                d21 = udr2;
+                d22 = (udt2 + u1) / fr;
+                d23 = (udp2 / fs - u3 * fc) / fr;
+                d31 = udr3;
+                d32 = udt3 / fr;
+                d33 = (udp3 / fs + u1 + u2 * fc) / fr;
+            }
+            if (icomp) {  // udertorsgt
+                if (icomp == 1) {
+                    Rg[0] = Rg[0] + d11;
+                    Rg[1] = Rg[1] - 5.e-1 * d21 - 5.e-1 * d12;
+                    Rg[2] = Rg[2] + 5.e-1 * d22 - 5.e-1 * d33;
+                    Rg[3] = Rg[3] - 5.e-1 * d22 - 5.e-1 * d33;
+                } else if (icomp == 2) {
+                    Rg[4] = Rg[4] + d11;
+                    Rg[5] = Rg[5] - 5.e-1 * d22 - 5.e-1 * d33;
+                    Rg[6] = Rg[6] - 5.e-1 * d22 + 5.e-1 * d33;
+                    Rg[8] = Rg[8] - 5.e-1 * d12 - 5.e-1 * d21;
+                } else {
+                    Rg[7] = Rg[7] - 5.e-1 * d23 - 5.e-1 * d32;
+                    Rg[9] = Rg[9] + 5.e-1 * d13 + 5.e-1 * d31;
+                }
+                continue;
+            }
+            // udertotsgt
+            if (imt == 1) {
+                T[0] = T[0] + d11;
+                T[2] = T[2] - 5.e-1 * d22 - 5.e-1 * d33;
+                T[5] = T[5] - 5.e-1 * d12 - 5.e-1 * d21;
+                T[9] = T[9] + 5.e-1 * d22 - 5.e-1 * d33;
+            } else if (imt == 2 || imt == 3) {
+                double sgn = imt == 2 ? 1.0 : -1.0;
+                T[1] = T[1] - 5.e-1 * d11;
+                T[3] = T[3] + 2.5e-1 * d22 + 2.5e-1 * d33;
+                T[7] = T[7] + (sgn * 2.5e-1) * d12 + (sgn * 2.5e-1) * d21;
+                T[8] = T[8] + (sgn * 5.e-1) * d11;
+                T[10] = T[10] - 2.5e-1 * d22 + 2.5e-1 * d33;
+                T[11] = T[11] - (sgn * 2.5e-1) * d22 - (sgn * 2.5e-1) * d33;
+                T[16] = T[16] - 1.25e-1 * d12 - 1.25e-1 * d21;
+                T[17] = T[17] + 1.25e-1 * d12 + 1.25e-1 * d21;
+                T[18] = T[18] + (sgn * 1.25e-1) * d22 - (sgn * 1.25e-1) * d33;
+                T[19] = T[19] + (sgn * 1.25e-1) * d22 - (sgn * 1.25e-1) * d33;
+            } else if (imt == 4) {
+                T[4] = T[4] + d11;
+                T[6] = T[6] - 5.e-1 * d22 - 5.e-1 * d33;
+                T[12] = T[12] - 2.5e-1 * d12 - 2.5e-1 * d21;
+                T[13] = T[13] + 2.5e-1 * d12 + 2.5e-1 * d21;
+                T[14] = T[14] + 2.5e-1 * d22 - 2.5e-1 * d33;
+                T[15] = T[15] - 2.5e-1 * d22 + 2.5e-1 * d33;
+            } else if (imt == 5) {
+                T[12] = T[12] + 2.5e-1 * d13 + 2.5e-1 * d31;
+                T[13] = T[13] + 2.5e-1 * d13 + 2.5e-1 * d31;
+                T[14] = T[14] - 2.5e-1 * d23 - 2.5e-1 * d32;
+                T[15] = T[15] - 2.5e-1 * d23 - 2.5e-1 * d32;
+            } else if (imt == 6) {
+                T[16] = T[16] + 2.5e-1 * d13 + 2.5e-1 * d31;
+                T[17] = T[17] + 2.5e-1 * d13 + 2.5e-1 * d31;
+                T[18] = T[18] - 2.5e-1 * d23 - 2.5e-1 * d32;
+                T[19] = T[19] + 2.5e-1 * d23 + 2.5e-1 * d32;
+            }
+        }
+    }
+    if (surf) {
+        if (synn)
+            for (int c = 0; c < 10; ++c) {
+                size_t o = ((size_t)w * Th + it) * 10 + c;
+                synn[2 * o] = S[c].re;
+                synn[2 * o + 1] = S[c].im;
+            }
+        return;
+    }
+    size_t pt = ((size_t)w * Th + it) * R + r;
+    for (int c = 0; c < 20; ++c) {
+        tsgt[2 * (pt * 20 + c)] = T[c].re;
+        tsgt[2 * (pt * 20 + c) + 1] = T[c].im;
+    }
+    if (rsgt)
+        for (int c = 0; c < 10; ++c) {
+            rsgt[2 * (pt * 10 + c)] = Rg[c].re;
+            rsgt[2 * (pt * 10 + c) + 1] = Rg[c].im;
+        }
+}
+
+// ---------------------------------------------------------------- engine
+class PsvEngine : public Engine {
+  public:
+    PsvDev d{};
+    DBuf<int> iphase, nlayer, kkdr, elem, hmoff, blkoff, amz, amc, bcrow, rcap, fluid, comp_src, jsta,
+        capmap;
+    DBuf<double> qmu, qkappa, sel, fel, hm, bcval, poly, lam, qkp, fr, r, rrsta;
+    DBuf<cd> B0, B1, B2, Lst, Zst, Xcap, l0scr, ab, co;
+    int jmin_loc = 1, ncap = 0;
+    double vtop = 0, rtop = 0;
+
+    PsvEngine(const dsm_psv_setup_t* s, const dsm_options_t* o) {
+        mode = 1;
+        opt = *o;
+        init_common(opt.device);
+        m_lo = 0;
+        R = s->r_n;
+        Th = s->theta_n;
+        num_t = DSM_PSV_NUM_TSGT; num_r = DSM_PSV_NUM_RSGT; num_s = DSM_PSV_NUM_SYNN;
+        tlen = s->tlen; omegai = s->omegai; ratl = s->ratl; maxlmax = s->maxlmax;
+        imin = s->imin; imax = s->imax;
+        rsgt_sw = s->rsgt_switch == 1;
+        synn_sw = s->synn_switch == 1;
+        const int nz = s->nzone, nn = s->nn;
+        if (R <= 0 || Th <= 0 || nz <= 0 || nn <= 4) throw Error(DSM_ERR_INVALID, "empty PSV set-up");
+        d.nzone = nz; d.nn = nn; d.R = R; d.Th = Th;
+        d.itmp = (s->rmin == 0.0) ? 3 : 1;
+        d.jsrc = s->jsrc; d.spn = s->spn;
+        if (d.jsrc < d.itmp || d.jsrc + 3 > nn) throw Error(DSM_ERR_INVALID, "source rows outside the system");
+        d.n_sel = s->n_sel; d.n_fel = s->n_fel; d.n_hm = s->n_hm;
+        d.tlen = tlen; d.omegai = omegai; d.rmax = s->rmax; d.r0 = s->r0;
+        d.ecC0 = s->ecC0; d.ecF0 = s->ecF0; d.ecL0 = s->ecL0; d.ra0 = s->ra_src[0]; d.ra1 = s->ra_src[1];
+        iphase.upload(s->iphase, nz, st); nlayer.upload(s->nlayer, nz, st); kkdr.upload(s->kkdr, nz, st);
+        elem.upload(s->elem, nz, st); hmoff.upload(s->hmoff, nz, st);
+        qmu.upload(s->qmu, nz, st); qkappa.upload(s->qkappa, nz, st);
+        sel.upload(s->solid_el, (size_t)DSM_PSV_NSOLID * s->n_sel, st);
+        fel.upload(s->fluid_el, (size_t)3 * s->n_fel, st);
+        hm.upload(s->hm_el, (size_t)DSM_PSV_NHM * 4 * s->n_hm, st);
+        poly.upload(s->src_poly, 24, st);
+        // zone blocks and the column assembly map
+        std::vector<int> bo(nz);
+        int tot = 0;
+        for (int z = 0; z < nz; ++z) {
+            bo[z] = tot;
+            tot += (s->iphase[z] == 1) ? 2 * (s->nlayer[z] + 1) : s->nlayer[z] + 1;
+        }
+        d.ncol_tot = tot;
+        blkoff.upload(bo, st);
+        std::vector<int> az(2 * (nn + 1), -1), ac(2 * (nn + 1), 0), br(nn + 1, 0);
+        std::vector<double> bv(nn + 1, 0.0);
+        for (int z = 0; z < nz; ++z) {
+            int kk = s->kkdr[z];
+            int hi = (s->iphase[z] == 1) ? kk + 2 * s->nlayer[z] + 1 : kk + s->nlayer[z];
+            for (int jj = kk; jj <= hi && jj <= nn; ++jj) {
+                int e = (az[2 * jj] < 0) ? 0 : 1;
+                if (e == 1 && az[2 * jj + 1] >= 0) throw Error(DSM_ERR_INVALID, "three zones overlap a column");
+                az[2 * jj + e] = z;
+                ac[2 * jj + e] = jj - kk + 1;
+            }
+        }
+        for (int i = 1; i <= nz - 1; ++i) {
+            double rv = s->vrmax[i - 1] * s->vrmax[i - 1];
+            if (s->iphase[i - 1] == 1 && s->iphase[i] == 2) { br[s->kkdr[i]] = 2; bv[s->kkdr[i]] = rv; }
+            if (s->iphase[i - 1] == 2 && s->iphase[i] == 1) { br[s->kkdr[i]] = 3; bv[s->kkdr[i]] = rv; }
+        }
+        amz.upload(az, st); amc.upload(ac, st); bcrow.upload(br, st); bcval.upload(bv, st);
+        // receivers
+        r.upload(s->r, R, st);
+        rrsta.upload(s->rrsta, 3 * (size_t)R, st);
+        std::vector<int> ks(R), fl(R), cm(nn + 1, -1), rc(6 * (size_t)R);
+        std::vector<double> frv(R);
+        int jmin = nn;
+        auto addcap = [&](int j) {
+            if (j < d.itmp || j > nn) throw Error(DSM_ERR_INVALID, "receiver stencil outside the system");
+            if (cm[j] < 0) cm[j] = ncap++;
+            jmin = std::min(jmin, j);
+            return cm[j];
+        };
+        for (int ir = 0; ir < R; ++ir) {
+            int z = s->istazone[ir] - 1;
+            ks[ir] = s->kkdr[z] + 2 * s->iista[3 * ir] - 1;
+            fl[ir] = s->iphase[z] == 2;
+            frv[ir] = (double)(float)s->r[ir];
+            for (int k = 0; k < 6; ++k) rc[6 * ir + k] = addcap(ks[ir] - 1 + k);
+        }
+        d.cap_n1 = addcap(nn - 1);
+        d.cap_n = addcap(nn);
+        d.cap_p0 = cm[ks[R - 1] - 1];
+        d.cap_p1 = cm[ks[R - 1]];
+
+        jmin_loc = jmin - d.itmp + 1;
+        capmap.upload(cm, st); rcap.upload(rc, st); fluid.upload(fl, st);
+        lam.upload(s->lambda, R, st); qkp.upload(s->qkp, R, st); fr.upload(frv, st);
+        // l = 0 compaction (rea2): jsta, compact row of every kept global row
+        {
+            std::vector<int> js(R, 0), cs(nn + 1, 0);
+            int itmp = 0;
+            for (int iz = 0; iz < nz; ++iz) {
+                for (int ir = 0; ir < R; ++ir)
+                    if (iz + 1 == s->istazone[ir]) js[ir] = itmp + s->iista[3 * ir];
+                int kk = s->kkdr[iz], i1 = itmp + 1, i2;
+                if (s->iphase[iz] == 1) {
+                    i2 = (iz != nz - 1) ? i1 + (s->kkdr[iz + 1] - kk) / 2 - 1 : i1 + (nn + 1 - kk) / 2 - 1;
+                    for (int i = i1; i <= i2; ++i) cs[kk + 2 * (i - i1)] = i;
+                } else {
+                    i2 = i1 + (s->kkdr[iz + 1] - kk) - 1;
+                    for (int i = i1; i <= i2; ++i) cs[kk + (i - i1)] = i;
+                }
+                itmp = i2;
+            }
+            d.nn0 = itmp;
+            d.itmp0 = (s->rmin == 0.0) ? 2 : 1;
+            jsta.upload(js, st);
+            comp_src.upload(cs, st);
+            for (int ir = 0; ir < R; ++ir)
+                if (js[ir] < 1 || js[ir] + 2 > d.nn0) throw Error(DSM_ERR_INVALID, "receiver outside the l=0 system");
+        }
+        vtop = 0.0;
+        for (int i = 0; i < 4; ++i) vtop = vtop + s->vsv[4 * (nz - 1) + i] * 1.0;
+        rtop = s->vrmax[nz - 1];
+        // theta tables
+        th.th_n = Th;
+        th.h_x.resize(Th); th.h_s.resize(Th); th.h_pole.resize(Th);
+        for (int i = 0; i < Th; ++i) {
+            double tr = s->theta[i] / 180.0 * kPi;
+            th.h_x[i] = std::cos(tr);
+            th.h_s[i] = std::sin(tr);
+            th.h_pole[i] = (tr == 0.0) ? 1 : (tr == kPi ? 2 : 0);
+        }
+        th.x.upload(th.h_x, st); th.s.upload(th.h_s, st); th.pole.upload(th.h_pole, st);
+        build_weights(r.p, rrsta.p);
+        d.iphase = iphase.p; d.nlayer = nlayer.p; d.kkdr = kkdr.p; d.elem = elem.p; d.hmoff = hmoff.p;
+        d.blkoff = blkoff.p; d.qmu = qmu.p; d.qkappa = qkappa.p; d.sel = sel.p; d.fel = fel.p; d.hm = hm.p;
+        d.amz = amz.p; d.amc = amc.p; d.bcrow = bcrow.p; d.bcval = bcval.p; d.poly = poly.p;
+        d.rcap = rcap.p; d.wv = wv.p; d.wd = wd.p; d.fluid = fluid.p; d.lam = lam.p; d.qkp = qkp.p;
+        d.fr = fr.p; d.comp_src = comp_src.p; d.jsta = jsta.p;
+        F = opt.freq_batch > 0 ? opt.freq_batch : 8;
+        Lc = opt.l_chunk > 0 ? ((opt.l_chunk + 31) / 32) * 32 : 256;
+        Lcap = std::min(maxlmax + 1 + Lc, 2048);
+        amp_k = 1;
+        rows_m[0] = NS0 * (R + 1) * NFLD * 2;
+        rows_m[1] = NS1 * (R + 1) * NFLD * 2;
+        rows_m[2] = NS2 * (R + 1) * NFLD * 2;
+        alloc_batch();
+        build_basis(std::min(maxlmax + 1, 2048));
+        DSM_CUDA(cudaStreamSynchronize(st));
+    }
+
+    void alloc_batch() {
+        size_t nsys = (size_t)F * Lc, n = (size_t)d.nn - d.itmp + 1;
+        B0.reserve((size_t)F * d.ncol_tot * 4);
+        B1.reserve((size_t)F * d.ncol_tot * 4);
+        B2.reserve((size_t)F * d.ncol_tot * 4);
+        Lst.reserve((n + 1) * 3 * nsys);
+        Zst.reserve((n + 1) * 4 * nsys);
+        Xcap.reserve((size_t)ncap * NB * nsys);
+        l0scr.reserve((size_t)F * (d.nn0 + 1) * 6);
+        ab.reserve((size_t)F * 320);
+        co.reserve((size_t)NSLOT * NB * nsys);
+        for (int m = 0; m < 3; ++m) Afld[m].reserve((size_t)F * rows_m[m] * Lcap);
+        Cgemm.reserve(c_total());
+        cut.reserve(F);
+        amps.reserve((size_t)F * Lcap);
+        size_t pt, pr, ps;
+        out_sizes(&pt, &pr, &ps);
+        out_t.reserve(2 * pt * F);
+        out_r.reserve(2 * pr * F);
+        out_s.reserve(2 * ps * F);
+    }
+
+    size_t out_sizes(size_t* nt, size_t* nr, size_t* ns) const override {
+        *nt = (size_t)num_t * R * Th;
+        *nr = (size_t)num_r * R * Th;
+        *ns = (size_t)num_s * Th;
+        return *nt;
+    }
+
+    void omega_pieces(const int* fr_, int nf) override {
+        dim3 grid((d.ncol_tot + 127) / 128, nf);
+        k_psv_omega<<<grid, 128, 0, st>>>(d, fr_, B0.p, B1.p, B2.p);
+        DSM_LAUNCH(*this);
+        k_psv_abnum<<<(nf + 31) / 32, 32, 0, st>>>(d, fr_, nf, ab.p);
+        DSM_LAUNCH(*this);
+    }
+
+    void solve_chunk(const int* fr_, int nf, int l0, int lc) override {
+        int nsys = nf * lc;
+        if (l0 == 0) {
+            k_psv_l0<<<(nf + 31) / 32, 32, 0, st>>>(d, fr_, nf, B0.p, B1.p, B2.p, l0scr.p, Afld[0].p,
+                                                    Afld[1].p, Afld[2].p, Lcap, rsgt_sw);
+            DSM_LAUNCH(*this);
+        }
+        k_psv_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, B0.p, B1.p, B2.p, lc, l0, nsys, jmin_loc,
+                                                        capmap.p, Lst.p, Zst.p, Xcap.p);
+        DSM_LAUNCH(*this);
+        k_psv_coef<<<(nsys + 127) / 128, 128, 0, st>>>(d, fr_, lc, l0, nsys, ab.p, co.p, rsgt_sw);
+        DSM_LAUNCH(*this);
+        dim3 grid((nsys + 127) / 128, (R + 15) / 16);
+        k_psv_fields<<<grid, 128, 0, st>>>(d, lc, l0, nsys, Xcap.p, co.p, Afld[0].p, Afld[1].p, Afld[2].p,
+                                           Lcap, amps.p);
+        DSM_LAUNCH(*this);
+        stats.solve_bytes += (double)nsys * (d.nn - d.itmp + 1) * 3 * 16.0 * 2;
+    }
+
+    void scan_chunk(int nf, int l0, int lc) override {
+        k_psv_scan<<<(nf + 31) / 32, 32, 0, st>>>(nf, l0, lc, Lcap, maxlmax, ratl, tlen, vtop, rtop,
+                                                  d_freqs.p, amps.p, cut.p);
+        DSM_LAUNCH(*this);
+    }
+
+    void epilogue(const int* fr_, int w, int nf) override {
+        (void)nf;
+        int n = Th * (R + 1);
+        k_psv_epi<<<(n + 127) / 128, 128, 0, st>>>(d, w, th.x.p, th.s.p, th.pole.p, fr_,
+                                                   Cgemm.p + c_off(0), Cgemm.p + c_off(1),
+                                                   Cgemm.p + c_off(2), out_t.p,
+                                                   rsgt_sw ? out_r.p : nullptr,
+                                                   synn_sw ? out_s.p : nullptr, rsgt_sw);
+        DSM_LAUNCH(*this);
+    }
+};
+
+}  // namespace
+
+Engine* make_psv_engine(const dsm_psv_setup_t* s, const dsm_options_t* o) { return new PsvEngine(s, o); }
+
 }  // namespace dsm

@@ -593,7 +593,8 @@ class ShEngine : public Engine {
         // batch geometry
         F = opt.freq_batch > 0 ? opt.freq_batch : 16;
         Lc = opt.l_chunk > 0 ? ((opt.l_chunk + 31) / 32) * 32 : 256;
-        Lcap = std::min(maxlmax + 1 + Lc, 4096);
+        Lcap = std::min(maxlmax + 1 + Lc, 2048);
+        amp_k = 4;
         rows_m[1] = SH_NSLOT1 * (R + 1) * SH_NF * 2;
         rows_m[2] = SH_NSLOT2 * (R + 1) * SH_NF * 2;
         alloc_batch();

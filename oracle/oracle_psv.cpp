@@ -784,7 +784,7 @@ void rea2(const dsm_psv_setup_t& s, int nn, const cplx* a /*1-based packed (4,nn
 
 // One frequency of src/SGTpsv/SGTpsv-MPI.f90:535-1152.
 void psv_one_frequency(const dsm_psv_setup_t& s, int ifreq, cplx* tsgt, cplx* rsgt, cplx* synn,
-                       int* llog_out) {
+                       int* llog_out, double* probe_out = nullptr, int probe_n = 0) {
     const int nzone = s.nzone, nn = s.nn, r_n = s.r_n, th_n = s.theta_n;
     const int NT = DSM_PSV_NUM_TSGT, NR = DSM_PSV_NUM_RSGT, NS = DSM_PSV_NUM_SYNN;
     for (long k = 0; k < (long)NT * r_n * th_n; ++k) tsgt[k] = cplx(0.0);
@@ -1000,7 +1000,13 @@ void psv_one_frequency(const dsm_psv_setup_t& s, int ifreq, cplx* tsgt, cplx* rs
                     bool solve = (am == 0 && imt <= 3) || (am == 1 && (imt == 4 || imt == 5)) ||
                                  (am == 2 && (imt == 2 || imt == 3 || imt == 6));
                     if (solve) dcsbdlv0(a.data() + 4 * (it - 1), g0.data() + (it - 1), 3, n1, z.data());
-                    if (imt == 1) calamp_psv(g0.data() + ksta[r_n - 1] - 1, l, lsuf, maxamp, ismall, s.ratl);
+                    if (imt == 1) {
+                        calamp_psv(g0.data() + ksta[r_n - 1] - 1, l, lsuf, maxamp, ismall, s.ratl);
+                        if (probe_out && m == 0 && l < probe_n) {
+                            double a1 = cabs(g0[ksta[r_n - 1] - 1]), a2 = cabs(g0[ksta[r_n - 1]]);
+                            probe_out[l] = std::sqrt(a1 * a1 + a2 * a2);
+                        }
+                    }
                     if (s.synn_switch == 1) {
                         for (int th = 0; th < th_n; ++th) {
                             cplx u[3] = {};
@@ -1033,6 +1039,17 @@ void psv_one_frequency(const dsm_psv_setup_t& s, int ifreq, cplx* tsgt, cplx* rs
 }
 
 }  // namespace oracle
+
+extern "C" int oracle_psv_probe(const dsm_psv_setup_t* s, int ifreq, double* probe, int n) {
+    using oracle::cplx;
+    long nt = (long)DSM_PSV_NUM_TSGT * s->r_n * s->theta_n;
+    long nr = (long)DSM_PSV_NUM_RSGT * s->r_n * s->theta_n;
+    long ns = (long)DSM_PSV_NUM_SYNN * s->theta_n;
+    std::vector<cplx> t(nt), r(nr), y(ns);
+    int lg = 0;
+    oracle::psv_one_frequency(*s, ifreq, t.data(), r.data(), y.data(), &lg, probe, n);
+    return lg;
+}
 
 extern "C" int oracle_psv_run(const dsm_psv_setup_t* s, const int* ilist, int n, double* tsgt,
                               double* rsgt, double* synn, int* llog) {

@@ -16,7 +16,7 @@ def sh_small(seed=0, imax=32, thdelta=15.0, rdelta=350.0):
         synth.dsm_config(), synth.sh_mantle_model(seed))
 
 
-def psv_small(seed=0, imax=16, thdelta=15.0, rdelta=500.0, r0=6071.0, rmin=1000.0):
+def psv_small(seed=0, imax=64, thdelta=15.0, rdelta=500.0, r0=6071.0, rmin=1000.0):
     """PSV Earth model with inner core, fluid outer core and mantle; receivers
     from the inner core to the surface (fluid receivers included)."""
     return dsmsgt.Job(

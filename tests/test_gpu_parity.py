@@ -39,3 +39,26 @@ def test_sh_fp64_small_chunks(built):
     """Several speculative l chunks per frequency must give the same result."""
     s = dsmsgt.Setup(sh_small(seed=3), "sh")
     _compare(s, [5, 20], {"l_chunk": 64, "freq_batch": 2})
+
+
+@pytest.mark.gpu
+def test_psv_fp64_matches_oracle(built):
+    """Solid inner core, fluid outer core (fluid receivers), mantle; poles included."""
+    s = dsmsgt.Setup(psv_small(), "psv")
+    errs = _compare(s, [1, 17, 50])
+    print(errs)
+
+
+@pytest.mark.gpu
+def test_psv_fp64_deep_source_small_chunks(built):
+    s = dsmsgt.Setup(psv_small(seed=2, r0=5771.0, rdelta=700.0), "psv")
+    _compare(s, [4, 33], {"l_chunk": 64, "freq_batch": 1})
+
+
+@pytest.mark.gpu
+def test_psv_fp64_order_capacity_growth(built):
+    """A coarse grid (imax = 16) with the top receiver 71 km below the source
+    needs ~15 000 orders before the cutoff fires: the engine must grow its
+    order capacity several times and still match the oracle."""
+    s = dsmsgt.Setup(psv_small(imax=16, thdelta=45.0), "psv")
+    _compare(s, [6], {"l_chunk": 1024, "freq_batch": 1})
