@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""Benchmark of the SGT engine: frequency slices per second.
+
+Workload (default): the P-SV engine on a synthetic 1-D Earth (solid inner
+core, fluid outer core, 6 mantle/crust zones; seeded quadratic profiles),
+tlen 3276.8 s, 1024 frequencies (fmax 0.3125 Hz), source 300 km deep,
+201 receiver radii 1000-6350 km, 721 epicentral distances (0.25 deg).
+A step is one batch of frequency slices spread across the band, each fully
+processed (all orders up to the reference's cutoff, all m, all sources,
+TSGT + RSGT + SYNN on the full (r, theta) grid).
+
+  python bench.py [--gpus N --steps K --warmup W] [--precision mixed|fp64]
+  python bench.py --impl reference ...   # CPU restatement of the reference
+
+One JSON line is printed by rank 0.  Under torchrun (N > 1) every rank
+processes its own frequencies (weak scaling, no collective on the data
+path); the time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "dsm-kernel_b200"))
+sys.path.insert(0, REPO)
+
+import numpy as np  # noqa: E402
+
+METRIC = "SGT freq-slices/s (P-SV, all orders to the DSM cutoff)"
+UNIT = "freq-slices/s"
+
+
+def workload(mode: str):
+    import dsmsgt
+    from dsmsgt import synth
+    if mode == "psv":
+        job = dsmsgt.Job(
+            synth.param_file(tlen=3276.8, rmin=1000.0, rmax=6350.0, rdelta=26.75, r0=6071.0,
+                             thmin=0.0, thmax=180.0, thdelta=0.25, imin=0, imax=1024),
+            synth.dsm_config(), synth.psv_earth_model(0))
+        desc = {"workload": "SGTpsv synthetic Earth (IC solid, OC fluid, 6 mantle/crust zones, seed 0)",
+                "tlen_s": 3276.8, "np": 1024, "source_depth_km": 300, "receivers": 201,
+                "thetas": 721}
+    else:
+        job = dsmsgt.Job(
+            synth.param_file(tlen=1638.4, rmin=3500.0, rmax=6321.5, rdelta=28.5, r0=6271.0,
+                             thmin=0.0, thmax=180.0, thdelta=0.5, imin=0, imax=256),
+            synth.dsm_config(), synth.sh_mantle_model(0))
+        desc = {"workload": "SGTsh synthetic mantle (5 solid zones, seed 0)", "tlen_s": 1638.4,
+                "np": 256, "source_depth_km": 100, "receivers": 100, "thetas": 361}
+    return job, desc
+
+
+def step_freqs(step: int, per_step: int, imax: int, rank: int = 0, world: int = 1) -> list[int]:
+    """Frequencies of one step: per_step indices spread evenly over 1..imax,
+    shifted per step and per rank so that steps and ranks differ."""
+    off = (step * 37 + rank * 11) % max(1, imax // per_step)
+    return [1 + (j * imax // per_step + off) % imax for j in range(per_step)]
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True,
+                                         text=True, timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        mhz = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(mhz)) if mhz else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def cpu_baseline(setup_mode: str, freqs: list[int], threads: int, budget_s: float = 25.0):
+    """Times the oracle (the CPU FP64 restatement of the reference's
+    frequency loop, all host threads, parallel over frequencies) on a
+    bounded sample and scales to the full epicentral grid.
+
+    The sample keeps the workload's model, grid, source and all receivers,
+    and uses two reduced epicentral grids (7 and 13 distances); CPU time per
+    slice is linear in the number of distances (the receiver x theta loop)
+    plus an order-solve part that does not depend on it, so the two points
+    give the full-grid time per slice."""
+    from oracle import oracle as orc
+    import dsmsgt
+    job, desc = workload(setup_mode)
+    times = {}
+    for thd, nth in ((30.0, 7), (15.0, 13)):
+        text = job.param_text.replace(" 0.25\n", f" {thd}\n").replace(" 0.5\n", f" {thd}\n")
+        sjob = dsmsgt.Job(text, job.conf_text, job.model_text)
+        s = dsmsgt.Setup(sjob, setup_mode)
+        assert s.theta_n == nth, (s.theta_n, nth)
+        t0 = time.perf_counter()
+        orc.run(s, freqs, threads=threads)
+        times[nth] = time.perf_counter() - t0
+    slope = (times[13] - times[7]) / 6.0
+    t_full = times[7] + slope * (desc["thetas"] - 7)
+    value = len(freqs) / t_full
+    return value, times, desc
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--mode", default="psv", choices=["psv", "sh"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--per-step", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    imax = 1024 if args.mode == "psv" else 256
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        # warm-up: one tiny sample (the page cache and the oracle build)
+        for w in range(args.warmup):
+            cpu_baseline(args.mode, [1 + w], 1)
+        t_tot, n_tot, samples = 0.0, 0, []
+        for k in range(args.steps):
+            fr = step_freqs(k, threads, imax)
+            v, times, desc = cpu_baseline(args.mode, fr, threads)
+            t_tot += len(fr) / v
+            n_tot += len(fr)
+            samples.append(times)
+        value = n_tot / t_tot
+        _, desc = workload(args.mode)
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * t_tot / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": desc,
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                                 "sample": f"{threads} frequencies per step spread over the band, "
+                                           "all receivers, 7 and 13 epicentral distances, scaled "
+                                           "linearly to 721 distances"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import dsmsgt
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = local
+    job, desc = workload(args.mode)
+    setup = dsmsgt.Setup(job, args.mode)
+    prec = dsmsgt.DSM_PREC_MIXED if args.precision == "mixed" else dsmsgt.DSM_PREC_FP64
+    ctx = dsmsgt.Context(setup, precision=prec, device=dev, freq_batch=args.per_step)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            torch.distributed.barrier()
+
+    # warm-up (untimed)
+    for w in range(args.warmup):
+        ctx.run_device(step_freqs(1000 + w, args.per_step, imax, rank, world))
+    # device-resident throughput: inputs (set-up, tables) already on the GPU
+    ctx.set_profiling(True)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    kstats = {}
+    ms_dev = 0.0
+    launches = 0
+    llogs = []
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        llogs.append(ctx.run_device(step_freqs(k, args.per_step, imax, rank, world)).tolist())
+        st = ctx.stats()
+        ms_dev += st.ms_total
+        launches += st.launches - sum(v[1] for k, v in st.kernels().items() if k.startswith("lsum_dgemm"))
+        for name, (ms, n, b, f) in st.kernels().items():
+            a = kstats.setdefault(name, [0.0, 0, 0.0, 0.0])
+            a[0] += ms; a[1] += n; a[2] += b; a[3] += f
+    barrier()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    ctx.set_profiling(False)
+    t_step = ms_dev / 1e3
+    if world > 1:
+        tt = torch.tensor([t_step], device=f"cuda:{dev}", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_step = float(tt.item())
+    slices = args.steps * args.per_step * world
+    value = slices / t_step
+
+    # end to end through the C-ABI: complex64 catalogue records copied to
+    # pinned host memory every step (the frequency list goes host -> device)
+    nt, nr, ns = setup.num
+    per_t = nt * setup.r_n * setup.theta_n
+    per_r = nr * setup.r_n * setup.theta_n
+    per_s = ns * setup.theta_n
+    F = args.per_step
+    ht = torch.empty(2 * per_t * F, dtype=torch.float32, pin_memory=True)
+    hr = torch.empty(2 * per_r * F, dtype=torch.float32, pin_memory=True)
+    hy = torch.empty(2 * per_s * F, dtype=torch.float32, pin_memory=True)
+    ll = np.zeros(F, np.int32)
+    ms_e2e = 0.0
+    barrier()
+    for k in range(args.steps):
+        ctx.run_host32(step_freqs(k, F, imax, rank, world), ht.data_ptr(), hr.data_ptr(),
+                       hy.data_ptr(), ll)
+        ms_e2e += ctx.stats().ms_total
+    barrier()
+    t_e2e = ms_e2e / 1e3
+    if world > 1:
+        tt = torch.tensor([t_e2e], device=f"cuda:{dev}", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = {"value": slices / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * F,
+           "d2h_bytes_per_step": 8 * (per_t + per_r + per_s) * F + 4 * F}
+
+    # roofline of the dominant kernel of this library (CUDA events on the
+    # library's stream over the timed region)
+    peaks = {}
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except Exception:
+        pass
+    own = {k: v for k, v in kstats.items() if not k.startswith("lsum_dgemm")}
+    dom = max(own.items(), key=lambda kv: kv[1][0]) if own else None
+    roof = None
+    if dom:
+        name, (ms, n, b, f) = dom
+        if b > 0:
+            ach = b / (ms / 1e3) / 1e9
+            peak = peaks.get("hbm_gbs", 6650.0)
+            roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": ach / peak, "traffic": None,
+                    "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                    "avg_launch_ms": ms / max(n, 1)}
+        else:
+            ach = f / (ms / 1e3) / 1e12
+            peak = peaks.get("bf16_tflops", 1590.0)
+            roof = {"kernel": name, "bound": "tensor", "achieved": ach, "peak": peak,
+                    "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                    "peak_source": "measured" if "bf16_tflops" in peaks else "fallback",
+                    "avg_launch_ms": ms / max(n, 1)}
+    share = {k: round(v[0] / max(ms_dev, 1e-9), 4) for k, v in kstats.items()}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        fr = step_freqs(0, min(threads, 16), imax)
+        v, times, _ = cpu_baseline(args.mode, fr, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{len(fr)} frequencies spread over the band, all receivers, 7 and 13 "
+                         "epicentral distances (oracle, FP64), scaled linearly to the full "
+                         f"{desc['thetas']} distances; measured s: {json.dumps(times)}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t_step / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "bf16/f32",
+                "data": "synthetic (seeded 1-D polynomial model, reference file formats)",
+                "config": dict(desc, precision=args.precision, slices_per_step=args.per_step,
+                               parallelism=f"dp{world} (frequencies per rank)",
+                               l2="inputs larger than L2 (field matrices of several GB per step)"),
+                "e2e": e2e, "gpu_launches": int(launches),
+                "roofline": roof, "kernel_share": share, "cpu_baseline": cpu,
+                "clocks": clk, "wall_s": wall, "llog_first_step": llogs[0]}
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -17,6 +17,7 @@
 //   5. packs complex64 catalogue records when asked.
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstring>
 
 #include "engine.cuh"
@@ -38,10 +39,60 @@ void Engine::init_common(int dev) {
 
 Engine::~Engine() {
     if (st) cudaStreamSynchronize(st);
+    for (auto& r : recs) { evpool.push_back(r.a); evpool.push_back(r.b); }
+    for (auto e : evpool) cudaEventDestroy(e);
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
     if (cub) cublasDestroy(cub);
     if (st) cudaStreamDestroy(st);
+}
+
+int Engine::kid(const char* name) {
+    for (int i = 0; i < stats.nk; ++i)
+        if (std::strncmp(stats.kern[i].name, name, 31) == 0) return i;
+    if (stats.nk >= DSM_MAX_KSTATS) return -1;
+    int i = stats.nk++;
+    std::snprintf(stats.kern[i].name, sizeof(stats.kern[i].name), "%s", name);
+    return i;
+}
+
+void Engine::kbegin(int id) {
+    if (!prof || id < 0) return;
+    if (evpool.size() < 2) {
+        for (int k = 0; k < 64; ++k) {
+            cudaEvent_t e;
+            DSM_CUDA(cudaEventCreate(&e));
+            evpool.push_back(e);
+        }
+    }
+    cudaEvent_t a = evpool.back();
+    evpool.pop_back();
+    cudaEvent_t b = evpool.back();
+    evpool.pop_back();
+    DSM_CUDA(cudaEventRecord(a, st));
+    recs.push_back({id, a, b});
+}
+
+void Engine::kend(int id, double bytes, double flops) {
+    if (id < 0) return;
+    stats.kern[id].launches++;
+    stats.kern[id].alg_bytes += bytes;
+    stats.kern[id].alg_flops += flops;
+    if (!prof) return;
+    DSM_CUDA(cudaEventRecord(recs.back().b, st));
+}
+
+void Engine::kcollect() {
+    if (recs.empty()) return;
+    DSM_CUDA(cudaStreamSynchronize(st));
+    for (auto& r : recs) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        stats.kern[r.id].ms += ms;
+        evpool.push_back(r.a);
+        evpool.push_back(r.b);
+    }
+    recs.clear();
 }
 
 void Engine::build_basis(int lneed) {
@@ -64,8 +115,11 @@ void Engine::gemm_fp64(int w, int mi, int K) {
     if (M == 0) return;
     const double one = 1.0, zero = 0.0;
     const double* A = Afld[mi].p + (size_t)w * M * Lcap;
+    int id = kid("lsum_dgemm");
+    kbegin(id);
     DSM_CUBLAS(cublasDgemm(cub, CUBLAS_OP_T, CUBLAS_OP_N, M, N, K, &one, A, Lcap, basis[mi].p, lcapB,
                            &zero, Cgemm.p + c_off(mi), M));
+    kend(id, 8.0 * ((double)M * K + (double)K * N + (double)M * N), 2.0 * M * N * (double)K);
     launches++;
 }
 
@@ -112,6 +166,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
     if (dt && n > F) throw Error(DSM_ERR_INVALID, "device outputs hold at most one batch of frequencies");
     std::memset(&stats, 0, sizeof(stats));
     launches = 0;
+    recs.clear();
     cudaEvent_t e0 = ev[0], e1 = ev[1], es0 = ev[2], es1 = ev[3], eg0 = ev[4], eg1 = ev[5];
     DSM_CUDA(cudaEventRecord(e0, st));
     float ms_solve = 0, ms_lsum = 0;
@@ -188,6 +243,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             }
         }
         DSM_CUDA(cudaStreamSynchronize(st));
+        kcollect();
         float a = 0, g = 0;
         cudaEventElapsedTime(&a, es0, es1);
         cudaEventElapsedTime(&g, eg0, eg1);
@@ -352,6 +408,12 @@ extern "C" long long dsm_debug_copy(dsm_ctx_t* ctx, const char* name, void* dst,
     size_t nb = std::min((size_t)bytes, have);
     if (cudaMemcpy(dst, src, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return -DSM_ERR_CUDA;
     return (long long)nb;
+}
+
+extern "C" int dsm_set_profiling(dsm_ctx_t* ctx, int on) {
+    if (!ctx) return DSM_ERR_INVALID;
+    ctx->eng->prof = on != 0;
+    return DSM_OK;
 }
 
 extern "C" int dsm_get_stats(const dsm_ctx_t* ctx, dsm_stats_t* s) {

@@ -83,6 +83,16 @@ class Engine {
     void build_basis(int lneed);
     void build_weights(const double* r, const double* rrsta);
     void gemm_fp64(int w, int mi, int K);
+    // optional per-kernel event timing
+    bool prof = false;
+    std::vector<cudaEvent_t> evpool;
+    struct Rec { int id; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+    int kid(const char* name);
+    void kbegin(int id);
+    void kend(int id, double bytes, double flops);
+    void kcollect();
+    std::vector<int> pend_id;
     void grow_orders(int need);
 
     // mode hooks

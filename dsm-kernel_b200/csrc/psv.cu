@@ -1322,14 +1322,28 @@ class PsvEngine : public Engine {
                                                     Afld[1].p, Afld[2].p, Lcap, rsgt_sw);
             DSM_LAUNCH(*this);
         }
+        // algorithmic bytes of a system: band factor (b+1) N complex written
+        // and read once, plus value and derivative of every solved right-hand
+        // side at the receivers
+        const double nrow = (double)(d.nn - d.itmp + 1);
+        const double alg = 2.0 * 4.0 * nrow * 16.0 + 18.0 * R * 2 * 2 * 16.0;
+        int id = kid("psv_band_solve");
+        kbegin(id);
         k_psv_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, B0.p, B1.p, B2.p, lc, l0, nsys, jmin_loc,
                                                         capmap.p, Lst.p, Zst.p, Xcap.p);
+        kend(id, alg * nsys, 0.0);
         DSM_LAUNCH(*this);
+        id = kid("psv_source_coef");
+        kbegin(id);
         k_psv_coef<<<(nsys + 127) / 128, 128, 0, st>>>(d, fr_, lc, l0, nsys, ab.p, co.p, rsgt_sw);
+        kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
         dim3 grid((nsys + 127) / 128, (R + 15) / 16);
+        id = kid("psv_fields");
+        kbegin(id);
         k_psv_fields<<<grid, 128, 0, st>>>(d, lc, l0, nsys, Xcap.p, co.p, Afld[0].p, Afld[1].p, Afld[2].p,
                                            Lcap, amps.p);
+        kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
         stats.solve_bytes += (double)nsys * (d.nn - d.itmp + 1) * 3 * 16.0 * 2;
     }
@@ -1343,11 +1357,14 @@ class PsvEngine : public Engine {
     void epilogue(const int* fr_, int w, int nf) override {
         (void)nf;
         int n = Th * (R + 1);
+        int id = kid("psv_epilogue");
+        kbegin(id);
         k_psv_epi<<<(n + 127) / 128, 128, 0, st>>>(d, w, th.x.p, th.s.p, th.pole.p, fr_,
                                                    Cgemm.p + c_off(0), Cgemm.p + c_off(1),
                                                    Cgemm.p + c_off(2), out_t.p,
                                                    rsgt_sw ? out_r.p : nullptr,
                                                    synn_sw ? out_s.p : nullptr, rsgt_sw);
+        kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
     }
 };

@@ -636,8 +636,12 @@ class ShEngine : public Engine {
 
     void solve_chunk(const int* fr, int nf, int l0, int lc) override {
         int nsys = nf * lc;
+        const double alg = 2.0 * 2.0 * d.nn * 16.0 + 14.0 * R * 2 * 2 * 16.0;
+        int id = kid("sh_band_solve");
+        kbegin(id);
         k_sh_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, a0.p, a2.p, lc, l0, nsys, jmin, capmap.p,
                                                        Lst.p, Zst.p, Xcap.p);
+        kend(id, alg * nsys, 0.0);
         DSM_LAUNCH(*this);
         dim3 grid((nsys + 127) / 128, (R + 31) / 32);
         k_sh_fields<<<grid, 128, 0, st>>>(d, fr, lc, l0, nsys, Xcap.p, Afld[1].p, Afld[2].p, Lcap,

@@ -90,12 +90,23 @@ class Out(C.Structure):
                 ("tsgt32", _fp), ("rsgt32", _fp), ("synn32", _fp), ("llog", _ip)]
 
 
+class KStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("ms", C.c_double), ("launches", C.c_longlong),
+                ("alg_bytes", C.c_double), ("alg_flops", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_solve", C.c_double), ("ms_lsum", C.c_double),
                 ("ms_pack", C.c_double), ("ms_h2d", C.c_double), ("ms_d2h", C.c_double),
                 ("launches", C.c_longlong), ("systems", C.c_longlong),
                 ("orders_used", C.c_longlong), ("orders_padded", C.c_longlong),
-                ("lsum_flops", C.c_double), ("solve_bytes", C.c_double)]
+                ("lsum_flops", C.c_double), ("solve_bytes", C.c_double),
+                ("nk", C.c_int), ("kern", KStat * 12)]
+
+    def kernels(self):
+        return {self.kern[i].name.decode(): (self.kern[i].ms, self.kern[i].launches,
+                                             self.kern[i].alg_bytes, self.kern[i].alg_flops)
+                for i in range(self.nk)}
 
 
 class DsmError(RuntimeError):
@@ -130,6 +141,7 @@ def lib() -> C.CDLL:
         L.dsm_last_error.restype = C.c_char_p
         L.dsm_strerror.restype = C.c_char_p
         L.dsm_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+        L.dsm_set_profiling.argtypes = [C.c_void_p, C.c_int]
         _lib = L
     return _lib
 
@@ -249,6 +261,35 @@ class Context:
         if want32:
             return t, r, y, llog, (t32, r32, y32)
         return t, r, y, llog
+
+    def set_profiling(self, on: bool):
+        lib().dsm_set_profiling(self.h, 1 if on else 0)
+
+    def run_device(self, freqs):
+        """Runs with outputs left on the device; returns llog."""
+        L = lib()
+        fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+        llog = np.zeros(len(fl), np.int32)
+        dt, dr, ds = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        rc = L.dsm_run_freqs_device(self.h, _ptr(fl, _ip), len(fl), C.byref(dt), C.byref(dr),
+                                    C.byref(ds), _ptr(llog, _ip))
+        if rc:
+            raise DsmError(f"dsm_run_freqs_device failed ({rc}): {L.dsm_last_error(self.h).decode()}")
+        return llog
+
+    def run_host32(self, freqs, t32, r32, y32, llog):
+        """Runs with complex64 catalogue outputs copied into caller buffers
+        (addresses of pinned host memory)."""
+        L = lib()
+        fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+        out = Out()
+        out.tsgt32 = C.cast(C.c_void_p(t32), _fp)
+        out.rsgt32 = C.cast(C.c_void_p(r32), _fp) if r32 else None
+        out.synn32 = C.cast(C.c_void_p(y32), _fp) if y32 else None
+        out.llog = _ptr(llog, _ip)
+        rc = L.dsm_run_freqs(self.h, _ptr(fl, _ip), len(fl), C.byref(out))
+        if rc:
+            raise DsmError(f"dsm_run_freqs failed ({rc}): {L.dsm_last_error(self.h).decode()}")
 
     def stats(self) -> Stats:
         s = Stats()

@@ -220,6 +220,17 @@ const char *dsm_last_error(const dsm_ctx_t *ctx);
 const char *dsm_strerror(int code);
 int dsm_abi_version(void);
 
+/* Per-kernel device time of the last run, recorded with CUDA events on the
+ * context's stream when profiling is on (dsm_set_profiling). */
+#define DSM_MAX_KSTATS 12
+typedef struct dsm_kstat {
+    char      name[32];
+    double    ms;          /* summed device time                          */
+    long long launches;
+    double    alg_bytes;   /* algorithmic bytes moved by these launches   */
+    double    alg_flops;   /* algorithmic flops of these launches         */
+} dsm_kstat_t;
+
 /* Stage timing of the last run (device time in ms, CUDA events): the
  * per-(omega,l) solve, the l-sum contraction, the epilogue/packing, and
  * the whole call.  Also the number of kernel launches of the call. */
@@ -231,8 +242,13 @@ typedef struct dsm_stats {
     long long orders_padded;/* orders solved beyond the cutoff             */
     double lsum_flops;      /* algorithmic flops of the contraction        */
     double solve_bytes;     /* algorithmic bytes of the banded solves      */
+    int nk;                 /* entries of kern[] in use                    */
+    dsm_kstat_t kern[DSM_MAX_KSTATS];
 } dsm_stats_t;
 int dsm_get_stats(const dsm_ctx_t *ctx, dsm_stats_t *stats);
+
+/* Turns per-kernel event timing on (1) or off (0) for later runs. */
+int dsm_set_profiling(dsm_ctx_t *ctx, int on);
 
 #ifdef __cplusplus
 }
