@@ -270,6 +270,14 @@ using dsm::Error;
 
 namespace {
 thread_local std::string g_create_err;
+}  // namespace
+
+namespace dsm {
+// error text of context-free entry points, read back by dsm_last_error(NULL)
+void set_global_error(const std::string& e) { g_create_err = e; }
+}  // namespace dsm
+
+namespace {
 
 template <class F>
 int guarded(dsm_ctx_t* ctx, F f) {

@@ -142,6 +142,7 @@ def lib() -> C.CDLL:
         L.dsm_strerror.restype = C.c_char_p
         L.dsm_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.dsm_set_profiling.argtypes = [C.c_void_p, C.c_int]
+        L.dsm_sh_cutoff_noalloc.argtypes = [C.POINTER(ShSetup), _ip, C.c_int, _ip]
         _lib = L
     return _lib
 

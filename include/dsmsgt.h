@@ -250,6 +250,21 @@ int dsm_get_stats(const dsm_ctx_t *ctx, dsm_stats_t *stats);
 /* Turns per-kernel event timing on (1) or off (0) for later runs. */
 int dsm_set_profiling(dsm_ctx_t *ctx, int on);
 
+/* SH angular-order cutoff without allocating device memory.  No
+ * counterpart in the reference: it returns in llog[k] the cutoff the SH
+ * engine reaches for frequency ilist[k] (the same value dsm_run_freqs
+ * reports), for callers that size their work before the SGT run but cannot
+ * call cudaMalloc -- a process whose GPU memory is already reserved by
+ * another framework's caching allocator, or one that must not cause the
+ * implicit device-wide synchronisation of cudaMalloc/cudaFree while other
+ * streams run.  All device buffers live in one fixed 64 MiB array per GPU,
+ * held until the process exits; set-ups needing more are rejected with
+ * DSM_ERR_INVALID (text in dsm_last_error(NULL)).  Runs on the current
+ * device.  The first call on a device looks up the array's address, so
+ * make it before any stream capture.  Calls that overlap on the GPU share
+ * the array and race. */
+int dsm_sh_cutoff_noalloc(const dsm_sh_setup_t *setup, const int *ilist, int n, int *llog);
+
 #ifdef __cplusplus
 }
 #endif
