@@ -32,6 +32,9 @@ void Engine::init_common(int dev) {
     DSM_CUDA(cudaDeviceGetLimit(&stack, cudaLimitStackSize));
     if (stack < 16384) DSM_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 16384));
     DSM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    DSM_CUDA(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+    DSM_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    DSM_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     DSM_CUBLAS(cublasCreate(&cub));
     DSM_CUBLAS(cublasSetStream(cub, st));
     for (auto& e : ev) DSM_CUDA(cudaEventCreate(&e));
@@ -44,6 +47,9 @@ Engine::~Engine() {
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
     if (cub) cublasDestroy(cub);
+    if (st2) { cudaStreamSynchronize(st2); cudaStreamDestroy(st2); }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -56,7 +62,21 @@ int Engine::kid(const char* name) {
     return i;
 }
 
-void Engine::kbegin(int id) {
+void Engine::fork_side() {
+    DSM_CUDA(cudaEventRecord(ev_fork, st));
+    DSM_CUDA(cudaStreamWaitEvent(st2, ev_fork, 0));
+    side_pending = true;
+}
+
+void Engine::join_side() {
+    if (!side_pending) return;
+    DSM_CUDA(cudaEventRecord(ev_join, st2));
+    DSM_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
+    side_pending = false;
+}
+
+void Engine::kbegin(int id, cudaStream_t s) {
+    if (!s) s = st;
     if (!prof || id < 0) return;
     if (evpool.size() < 2) {
         for (int k = 0; k < 64; ++k) {
@@ -69,22 +89,24 @@ void Engine::kbegin(int id) {
     evpool.pop_back();
     cudaEvent_t b = evpool.back();
     evpool.pop_back();
-    DSM_CUDA(cudaEventRecord(a, st));
+    DSM_CUDA(cudaEventRecord(a, s));
     recs.push_back({id, a, b});
 }
 
-void Engine::kend(int id, double bytes, double flops) {
+void Engine::kend(int id, double bytes, double flops, cudaStream_t s) {
+    if (!s) s = st;
     if (id < 0) return;
     stats.kern[id].launches++;
     stats.kern[id].alg_bytes += bytes;
     stats.kern[id].alg_flops += flops;
     if (!prof) return;
-    DSM_CUDA(cudaEventRecord(recs.back().b, st));
+    DSM_CUDA(cudaEventRecord(recs.back().b, s));
 }
 
 void Engine::kcollect() {
     if (recs.empty()) return;
     DSM_CUDA(cudaStreamSynchronize(st));
+    DSM_CUDA(cudaStreamSynchronize(st2));
     for (auto& r : recs) {
         float ms = 0;
         cudaEventElapsedTime(&ms, r.a, r.b);
@@ -128,6 +150,7 @@ void Engine::gemm_fp64(int w, int mi, int K) {
 // known before its orders are solved; the reference allows up to maxlmax).
 void Engine::grow_orders(int need) {
     if (need <= Lcap) return;
+    join_side();  // side-stream work may still write the old field buffers
     int cap = Lcap;
     while (cap < need) cap *= 2;
     cap = std::min(cap, maxlmax + 1 + Lc);
@@ -158,6 +181,16 @@ void Engine::grow_orders(int need) {
     Lcap = cap;
 }
 
+// First order range of a frequency: past lsuf (callsuf), at least 512
+// (or the fixed chunk the options ask for).
+int Engine::first_span(int ifreq) const {
+    if (opt.l_chunk > 0) return ((opt.l_chunk + 31) / 32) * 32;
+    double omega = 2.0 * kPi * (double)ifreq / tlen;
+    int lsuf = (int)(omega * rtop_ / vtop_ - 0.5) + 1;
+    int s = std::max(512, lsuf + 64);
+    return ((s + 31) / 32) * 32;
+}
+
 void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const void** dr,
                  const void** ds, int* llog_out) {
     if (n <= 0) throw Error(DSM_ERR_INVALID, "empty frequency list");
@@ -184,33 +217,66 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             cut.upload(init, st);
         }
         std::vector<CutState> hc(nf);
-        int l0 = 0;
+        for (auto& c : hc) c.done = 0;
+        // Rounds of ragged order ranges: every unfinished frequency continues
+        // from where it stopped.  The first range of a frequency reaches past
+        // lsuf (the cutoff is never below it); later ranges grow by half.
+        std::vector<int> next(nf, 0), span(nf, 0);
+        std::vector<int> hf(ilist + b0, ilist + b0 + nf);
+        for (int w = 0; w < nf; ++w) span[w] = first_span(hf[w]);
+        int maxend = 0;
         for (;;) {
-            if (l0 > maxlmax) break;
-            int lc = std::min(Lc, maxlmax + 1 - l0);
-            if (l0 + lc > Lcap) grow_orders(l0 + lc);
-            solve_chunk(d_freqs.p, nf, l0, lc);
-            scan_chunk(nf, l0, lc);
-            stats.systems += (long long)nf * lc;
+            std::vector<int> off(nf + 1, 0), lb(nf, 0);
+            int tot = 0;
+            for (int w = 0; w < nf; ++w) {
+                lb[w] = next[w];
+                int cnt = 0;
+                if (!hc[w].done && next[w] <= maxlmax) {
+                    cnt = std::min(span[w], maxlmax + 1 - next[w]);
+                    cnt = std::max(0, std::min(cnt, nsys_max - tot));
+                }
+                off[w] = tot;
+                tot += cnt;
+                next[w] += cnt;
+                maxend = std::max(maxend, next[w]);
+            }
+            off[nf] = tot;
+            if (tot == 0) break;
+            if (maxend > Lcap) grow_orders(maxend);
+            wl_off.upload(off, st);
+            wl_lb.upload(lb, st);
+            WorkList wl{wl_off.p, wl_lb.p, nf};
+            solve_chunk(d_freqs.p, nf, wl, tot);
+            scan_chunk(nf, wl);
+            stats.systems += tot;
             DSM_CUDA(cudaMemcpyAsync(hc.data(), cut.p, sizeof(CutState) * nf, cudaMemcpyDeviceToHost, st));
             DSM_CUDA(cudaStreamSynchronize(st));
             bool all = true;
-            for (auto& c : hc) all = all && c.done;
-            l0 += lc;
+            for (int w = 0; w < nf; ++w) {
+                if (!hc[w].done && next[w] > maxlmax) { hc[w].done = 1; }
+                all = all && hc[w].done;
+                if (!hc[w].done && opt.l_chunk <= 0) span[w] = std::min(4096, span[w] + span[w] / 2);
+            }
             if (all) break;
         }
-        for (auto& c : hc) {
-            if (!c.done) { c.norders = maxlmax + 1; c.llog = maxlmax; }
+        for (int w = 0; w < nf; ++w) {
+            if (hc[w].norders == 0) { hc[w].norders = maxlmax + 1; hc[w].llog = maxlmax; }
+            stats.orders_padded += (long long)next[w] - hc[w].norders;
         }
+        join_side();
         DSM_CUDA(cudaEventRecord(es1, st));
         // --- 3+4: contraction and epilogue per frequency
         int lneed = 1;
         for (auto& c : hc) lneed = std::max(lneed, c.norders);
-        build_basis(lneed);
+        {
+            int id = kid("basis_tables");
+            kbegin(id);
+            build_basis(lneed);
+            kend(id, 0.0, 0.0);
+        }
         DSM_CUDA(cudaEventRecord(eg0, st));
         for (int w = 0; w < nf; ++w) {
             stats.orders_used += hc[w].norders;
-            stats.orders_padded += (long long)l0 - hc[w].norders;
             for (int mi = m_lo; mi <= 2; ++mi) gemm_fp64(w, mi, hc[w].norders);
             epilogue(d_freqs.p, w, nf);
             for (int mi = m_lo; mi <= 2; ++mi)

@@ -19,6 +19,20 @@ struct CutState {
     double maxamp;
 };
 
+// Ragged work list of a solve launch: system sys belongs to batch frequency
+// w with off[w] <= sys < off[w+1] and solves order l = lb[w] + sys - off[w].
+struct WorkList {
+    const int* off;  // [nw + 1]
+    const int* lb;   // [nw]
+    int nw;
+};
+__device__ __forceinline__ void wl_map(const WorkList& wl, int sys, int& w, int& l) {
+    int k = 0;
+    while (k + 1 < wl.nw && wl.off[k + 1] <= sys) ++k;
+    w = k;
+    l = wl.lb[k] + sys - wl.off[k];
+}
+
 // angular tables shared by both modes
 struct ThetaTables {
     int th_n = 0;
@@ -34,6 +48,9 @@ class Engine {
     dsm_options_t opt{};
     std::string err;
     cudaStream_t st = nullptr;
+    cudaStream_t st2 = nullptr;      // side stream (independent per-batch work)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool side_pending = false;
     cublasHandle_t cub = nullptr;
     cudaEvent_t ev[8] = {};
     long long launches = 0;
@@ -89,16 +106,22 @@ class Engine {
     struct Rec { int id; cudaEvent_t a, b; };
     std::vector<Rec> recs;
     int kid(const char* name);
-    void kbegin(int id);
-    void kend(int id, double bytes, double flops);
+    void kbegin(int id, cudaStream_t s = nullptr);
+    void kend(int id, double bytes, double flops, cudaStream_t s = nullptr);
+    void fork_side();   // side stream waits for the main stream
+    void join_side();   // main stream waits for the side stream
     void kcollect();
     std::vector<int> pend_id;
     void grow_orders(int need);
 
     // mode hooks
     virtual void omega_pieces(const int* freqs_dev, int nf) = 0;
-    virtual void solve_chunk(const int* freqs_dev, int nf, int l0, int lc) = 0;
-    virtual void scan_chunk(int nf, int l0, int lc) = 0;
+    virtual void solve_chunk(const int* freqs_dev, int nf, const WorkList& wl, int nsys) = 0;
+    virtual void scan_chunk(int nf, const WorkList& wl) = 0;
+    int nsys_max = 0;                // systems per solve launch (scratch size)
+    double vtop_ = 1.0, rtop_ = 1.0;  // top-zone Vsv sum and radius (callsuf)
+    int first_span(int ifreq) const;
+    DBuf<int> wl_off, wl_lb;
     virtual void epilogue(const int* freqs_dev, int w, int nf) = 0;
     virtual size_t out_sizes(size_t* nt, size_t* nr, size_t* ns) const = 0;
 

@@ -273,13 +273,14 @@ __device__ __forceinline__ void assemble(const PsvDev& d, int jj, const cd* __re
 // Window W[p][q] holds the current values of A(k+p, k+q), q <= p <= 3.
 __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restrict__ B0all,
                                                    const cd* __restrict__ B1all,
-                                                   const cd* __restrict__ B2all, int lc, int l0,
+                                                   const cd* __restrict__ B2all, WorkList wl,
                                                    int nsys, int jmin_loc, const int* __restrict__ capmap,
                                                    cd* __restrict__ Lst, cd* __restrict__ Zst,
                                                    cd* __restrict__ Xcap) {
     int sys = blockIdx.x * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
-    int w = sys / lc, l = l0 + sys % lc;
+    int w, l;
+    wl_map(wl, sys, w, l);
     const size_t bo = (size_t)w * d.ncol_tot * 4;
     const cd *B0 = B0all + bo, *B1 = B1all + bo, *B2 = B2all + bo;
     const double l2 = (double)l * (double)(l + 1);
@@ -308,7 +309,7 @@ __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restric
         const cd D = W[0][0];
         // finish z(k): scaled value zh(k) = z(k) / D(k)
         for (int b = 0; b < 4; ++b) {
-            if (k >= ls) Zst[((size_t)k * 4 + b) * nsys + sys] = zcur[b] / D;
+            if (k >= ls) Zst[((size_t)(k - ls) * 4 + b) * nsys + sys] = zcur[b] / D;
             zs[b][0] = zs[b][1];
             zs[b][1] = zs[b][2];
             zs[b][2] = zcur[b];
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restric
     const cd Dn = W[0][0];
     cd x[NB][3];  // x(j+1), x(j+2), x(j+3)
     cd xn[NB];
-    for (int b = 0; b < 4; ++b) xn[b] = (n >= ls) ? Zst[((size_t)n * 4 + b) * nsys + sys] : mk(0.0);
+    for (int b = 0; b < 4; ++b) xn[b] = (n >= ls) ? Zst[((size_t)(n - ls) * 4 + b) * nsys + sys] : mk(0.0);
     // surface basis: e_{n-1}: z(n-1) = 1, z(n) = -L(n,n-1); e_n: z(n) = 1
     xn[4] = (mk(0.0) - Lnn1 * mk(1.0)) / Dn;
     xn[5] = mk(1.0) / Dn;
@@ -382,7 +383,7 @@ __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restric
         cd L1 = Lst[((size_t)(n - 1) * 3 + 0) * nsys + sys];
         for (int b = 0; b < NB; ++b) {
             cd zh = mk(0.0);
-            if (b < 4 && n - 1 >= ls) zh = Zst[((size_t)(n - 1) * 4 + b) * nsys + sys];
+            if (b < 4 && n - 1 >= ls) zh = Zst[((size_t)(n - 1 - ls) * 4 + b) * nsys + sys];
             if (b == 4) zh = mk(1.0) / Dm1;
             v[b] = zh - L1 * x[b][0];
         }
@@ -396,7 +397,7 @@ __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restric
         cd v[NB];
         for (int b = 0; b < NB; ++b) {
             cd zh = mk(0.0);
-            if (b < 4 && j1 >= ls) zh = Zst[((size_t)j1 * 4 + b) * nsys + sys];
+            if (b < 4 && j1 >= ls) zh = Zst[((size_t)(j1 - ls) * 4 + b) * nsys + sys];
             cd sum;
             if (j1 == n - 2) sum = mk(0.0) + L2 * x[b][1] + L1 * x[b][0];
             else sum = mk(0.0) + L3 * x[b][2] + L2 * x[b][1] + L1 * x[b][0];
@@ -417,135 +418,148 @@ __device__ void calya_dev(const cd* anum, const cd* bnum, double l2, double ra0,
 __device__ void calg_dev(const PsvDev& d, int l, int m, cd c1, cd c2, double lsq, const cd* ya,
                          const cd* yb, const cd* yc, const cd* yd, int imt, cd* g);
 
+// (1) compaction, one thread per compact row: c(1,i), c(2,i) of rea2 from the
+// assembled l = 0 band (l0col: global column, l0e1: band row of c(1,i), 0 for none)
+__global__ void k_psv_l0_build(PsvDev d, const cd* __restrict__ B0all, const cd* __restrict__ B1all,
+                               const cd* __restrict__ B2all, const int* __restrict__ l0col,
+                               const int* __restrict__ l0e1, cd* __restrict__ Cc) {
+    int w = blockIdx.y;
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    if (i > d.nn0) return;
+    const size_t bo = (size_t)w * d.ncol_tot * 4;
+    cd a[4];
+    assemble(d, l0col[i], B0all + bo, B1all + bo, B2all + bo, 0.0, 0.0, a);
+    int e1 = l0e1[i];
+    cd* C = Cc + (size_t)w * (d.nn0 + 1) * 2;
+    C[2 * i] = e1 == 2 ? a[1] : (e1 == 3 ? a[2] : mk(0.0));
+    C[2 * i + 1] = a[3];
+}
+
+// (2) one thread per frequency: right-hand sides (calg at l = 0 for imt 1..3,
+// the back-propagated vertical force), dcsymbdl0 with half-width 1 fused
+// with the forward substitution of dcsbdlv0, then the upward substitution,
+// for the four right-hand sides at once.  Solutions in Dv[w][i][4].
+__global__ void k_psv_l0_solve(PsvDev d, const int* __restrict__ freqs, int nf, const cd* __restrict__ ab,
+                               cd* __restrict__ Cc, cd* __restrict__ Dv, int back) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nf) return;
+    const int n0 = d.nn0, it0 = d.itmp0, n = n0 - it0 + 1;
+    cd* C = Cc + (size_t)w * (n0 + 1) * 2;
+    cd* D = Dv + (size_t)w * (n0 + 1) * 4;
+    const double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
+    const cd c1 = coefq(omega, d.qmu[d.spn - 1]), c2 = coefq(omega, d.qkappa[d.spn - 1]);
+    cd ya[4], yb[4], yc[4], yd[4];
+    calya_dev(ab + (size_t)w * 320, ab + (size_t)w * 320 + 160, 0.0, d.ra0, d.ra1, d.r0, ya, yb, yc, yd);
+    // sparse right-hand sides: rea2 keeps the U rows of g0(jtmp..jtmp+3)
+    int rr[5];
+    cd rv[5][4];
+    int nr = 0;
+    for (int k = 0; k < 4; ++k) {
+        int cr = d.comp_src[d.jsrc + k];
+        if (cr <= 0) continue;
+        rr[nr] = cr;
+        for (int b = 0; b < 4; ++b) rv[nr][b] = mk(0.0);
+        ++nr;
+    }
+    for (int imt = 1; imt <= 3; ++imt) {
+        cd g[4];
+        calg_dev(d, 0, 0, c1, c2, 0.0, ya, yb, yc, yd, imt, g);
+        int q = 0;
+        for (int k = 0; k < 4; ++k)
+            if (d.comp_src[d.jsrc + k] > 0) rv[q++][imt - 1] = g[k];
+    }
+    {
+        // caldveczero at l = 0: bvec(1,0) = cmplx(coef), single precision
+        double coef = sqrt((double)1 / (4.0 * kPi) / 1.0);
+        int cr = d.comp_src[d.nn - 1];
+        rr[nr] = cr > 0 ? cr : -1;
+        for (int b = 0; b < 4; ++b) rv[nr][b] = mk(0.0);
+        if (back) rv[nr][3] = -conj(mk((double)(float)coef));
+        ++nr;
+    }
+    auto rhs = [&](int row, int b) {
+        cd v = mk(0.0);
+        for (int k = 0; k < nr; ++k)
+            if (rr[k] == row) v = rv[k][b];
+        return v;
+    };
+    // local row j <-> compact row j + it0 - 1
+    cd zprev[4];
+    for (int b = 0; b < 4; ++b) zprev[b] = rhs(it0, b);  // z(1) = b(1)
+    cd dprev = C[2 * it0 + 1];
+    for (int j = 2; j <= n; ++j) {
+        const int g = j + it0 - 1;
+        // factor step k = j-1: piv = 1/c(2,k); w2 = c(1,k+1) piv; c(2,k+1) += w2 (-c(1,k+1))
+        cd piv = mk(1.0) / dprev;
+        cd off = C[2 * g];
+        cd z2 = -off;
+        cd w2 = off * piv;
+        cd dg = C[2 * g + 1] + w2 * z2;
+        C[2 * g] = w2;
+        C[2 * g + 1] = dg;
+        // forward substitution: z(k) = z(k)/c(2,k), z(j) = b(j) - c(1,j) z(j-1)
+        for (int b = 0; b < 4; ++b) {
+            D[4 * (g - 1) + b] = zprev[b] / dprev;
+            zprev[b] = rhs(g, b) - w2 * zprev[b];
+        }
+        dprev = dg;
+    }
+    for (int b = 0; b < 4; ++b) D[4 * n0 + b] = zprev[b] / dprev;
+    // upward substitution x(n-j) = z(n-j) - c(1,n-j+1) x(n-j+1)
+    cd x[4];
+    for (int b = 0; b < 4; ++b) x[b] = D[4 * n0 + b];
+    for (int j = n - 1; j >= 1; --j) {
+        const int g = j + it0 - 1;
+        cd L = C[2 * (g + 1)];
+        for (int b = 0; b < 4; ++b) {
+            x[b] = D[4 * g + b] - L * x[b];
+            D[4 * g + b] = x[b];
+        }
+    }
+}
+
+// (3) fields of order 0, one thread per (frequency, receiver): m = 0 slots
+// q = 0..2 (imt 1..3) and 3 (back), U and dU/dr (calup0 uses u(1) only)
 __device__ __forceinline__ void put_field(double* Aw, int Lcap, int R, int q, int r, int f, cd v) {
     size_t row = ((size_t)(q * (R + 1) + r) * NFLD + f) * 2;
     Aw[row * Lcap] = v.re;
     Aw[(row + 1) * Lcap] = v.im;
 }
 
-__global__ void k_psv_l0(PsvDev d, const int* __restrict__ freqs, int nf, const cd* __restrict__ B0all,
-                         const cd* __restrict__ B1all, const cd* __restrict__ B2all,
-                         cd* __restrict__ scratch, double* __restrict__ A0f, double* __restrict__ A1f,
-                         double* __restrict__ A2f, int Lcap, int back) {
-    int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= nf) return;
-    const int nn = d.nn, R = d.R;
-    const size_t bo = (size_t)w * d.ncol_tot * 4;
-    const cd *B0 = B0all + bo, *B1 = B1all + bo, *B2 = B2all + bo;
-    // scratch per frequency: c(2, nn0) and 4 right-hand sides d(nn0)
-    cd* C = scratch + (size_t)w * (d.nn0 + 1) * 6;
-    auto Cc = [&](int i, int j) -> cd& { return C[(size_t)j * 6 + (i - 1)]; };
-    auto Dv = [&](int b, int j) -> cd& { return C[(size_t)j * 6 + 2 + b]; };
-    // rea2: rearranged band of the assembled l = 0 matrix
-    int itmp = 0;
-    cd a[4];
-    for (int iz = 0; iz < d.nzone; ++iz) {
-        int kk = d.kkdr[iz], i1 = itmp + 1, i2;
-        if (d.iphase[iz] == 1) {
-            i2 = (iz != d.nzone - 1) ? i1 + (d.kkdr[iz + 1] - kk) / 2 - 1 : i1 + (nn + 1 - kk) / 2 - 1;
-            assemble(d, kk, B0, B1, B2, 0.0, 0.0, a);
-            if (iz != 0) {
-                cd ap[4];
-                assemble(d, kk, B0, B1, B2, 0.0, 0.0, ap);
-                Cc(1, i1) = (d.iphase[iz - 1] == 2) ? ap[2] : ap[1];
-            }
-            Cc(2, i1) = a[3];
-            for (int i = i1 + 1; i <= i2; ++i) {
-                assemble(d, kk + 2 * (i - i1), B0, B1, B2, 0.0, 0.0, a);
-                Cc(1, i) = a[1];
-                Cc(2, i) = a[3];
-            }
-        } else {
-            i2 = i1 + (d.kkdr[iz + 1] - kk) - 1;
-            assemble(d, kk, B0, B1, B2, 0.0, 0.0, a);
-            if (iz != 0) Cc(1, i1) = (d.iphase[iz - 1] == 1) ? a[1] : a[2];
-            Cc(2, i1) = a[3];
-            for (int i = i1 + 1; i <= i2; ++i) {
-                assemble(d, kk + (i - i1), B0, B1, B2, 0.0, 0.0, a);
-                Cc(1, i) = a[2];
-                Cc(2, i) = a[3];
-            }
-        }
-        itmp = i2;
-    }
-    const int n0 = d.nn0, it0 = d.itmp0, n = n0 - it0 + 1;
-    // right-hand sides: calg at l = 0, m = 0 for imt 1..3; back source
-    const double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
-    cd c1 = coefq(omega, d.qmu[d.spn - 1]), c2 = coefq(omega, d.qkappa[d.spn - 1]);
-    cd anum[160], bnum[160], ya[4], yb[4], yc[4], yd[4];
-    calabnum_dev(d, omega, c1, c2, anum, bnum);
-    calya_dev(anum, bnum, 0.0, d.ra0, d.ra1, d.r0, ya, yb, yc, yd);
-    for (int j = 1; j <= n0; ++j)
-        for (int b = 0; b < 4; ++b) Dv(b, j) = mk(0.0);
-    for (int imt = 1; imt <= 3; ++imt) {
-        cd g[4];
-        calg_dev(d, 0, 0, c1, c2, 0.0, ya, yb, yc, yd, imt, g);
-        // rea2 maps rows jtmp..jtmp+3 of g0; only the U rows survive
-        for (int k = 0; k < 4; ++k) {
-            int cr = d.comp_src[d.jsrc + k];
-            if (cr > 0) Dv(imt - 1, cr) = g[k];
-        }
-    }
-    {
-        // caldveczero m = 0: bvec(1,0) = cmplx(coef), single precision
-        double coef = sqrt((double)1 / (4.0 * kPi) / 1.0);
-        cd rd = mk((double)(float)coef);
-        int cr = d.comp_src[nn - 1];
-        if (cr > 0) Dv(3, cr) = -conj(rd);
-    }
-    // dcsymbdl0 with m = 1 on rows it0..n0 (local 1..n)
-    // local row i -> compact row i + it0 - 1
-    auto CL = [&](int i, int j) -> cd& { return Cc(i, j + it0 - 1); };
-    for (int k = 1; k <= n - 1; ++k) {
-        cd piv = mk(1.0) / CL(2, k);
-        cd z2 = -CL(1, k + 1);
-        cd w2 = CL(1, k + 1) * piv;
-        CL(1, k + 1) = w2;
-        CL(2, k + 1) = CL(2, k + 1) + w2 * z2;
-    }
-    // dcsbdlv0 (m = 1) for the four right-hand sides
-    for (int b = 0; b < 4; ++b) {
-        if (b == 3 && !back) continue;
-        auto DL = [&](int j) -> cd& { return Dv(b, j + it0 - 1); };
-        // z stored in place of d: z(j) = b(j) - a(1,j) z(j-1)
-        cd zprev = DL(1);
-        for (int j = 2; j <= n; ++j) {
-            cd zj = DL(j) - CL(1, j) * zprev;
-            DL(j) = zj;
-            zprev = zj;
-        }
-        for (int j = 1; j <= n; ++j) DL(j) = DL(j) / CL(2, j);
-        for (int j = 1; j <= n - 1; ++j) DL(n - j) = DL(n - j) - CL(1, n - j + 1) * DL(n - j + 1);
-    }
-    // fields of column l = 0: m = 0 slots q = 0..2 (imt 1..3), 3 (back)
+__global__ void k_psv_l0_fields(PsvDev d, const cd* __restrict__ Dv, double* __restrict__ A0f,
+                                double* __restrict__ A1f, double* __restrict__ A2f, int Lcap, int back) {
+    int w = blockIdx.y;
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int R = d.R;
+    if (r > R) return;
+    const int n0 = d.nn0;
+    const cd* D = Dv + (size_t)w * (n0 + 1) * 4;
     const int rows0 = NS0 * (R + 1) * NFLD * 2, rows1 = NS1 * (R + 1) * NFLD * 2,
               rows2 = NS2 * (R + 1) * NFLD * 2;
     double* A0w = A0f + (size_t)w * rows0 * Lcap;
     double* A1w = A1f + (size_t)w * rows1 * Lcap;
     double* A2w = A2f + (size_t)w * rows2 * Lcap;
-    for (int r = 0; r <= R; ++r) {
-        for (int q = 0; q < NS0; ++q) {
-            cd U = mk(0.0), Ud = mk(0.0);
-            if (q < 3 || back) {
-                if (r < R) {
-                    for (int i = 0; i < 3; ++i) {
-                        cd v = Dv(q, d.jsta[r] + i);
-                        U = U + d.wv[3 * r + i] * v;
-                        Ud = Ud + d.wd[3 * r + i] * v;
-                    }
-                } else if (q < 3) {
-                    U = Dv(q, n0);
+    for (int q = 0; q < NS0; ++q) {
+        cd U = mk(0.0), Ud = mk(0.0);
+        if (q < 3 || back) {
+            if (r < R) {
+                for (int i = 0; i < 3; ++i) {
+                    cd v = D[4 * (d.jsta[r] + i) + q];
+                    U = U + d.wv[3 * r + i] * v;
+                    Ud = Ud + d.wd[3 * r + i] * v;
                 }
+            } else if (q < 3) {
+                U = D[4 * n0 + q];
             }
-            put_field(A0w, Lcap, R, q, r, 0, U);
-            put_field(A0w, Lcap, R, q, r, 1, Ud);
-            for (int f = 2; f < NFLD; ++f) put_field(A0w, Lcap, R, q, r, f, mk(0.0));
         }
-        for (int q = 0; q < NS1; ++q)
-            for (int f = 0; f < NFLD; ++f) put_field(A1w, Lcap, R, q, r, f, mk(0.0));
-        for (int q = 0; q < NS2; ++q)
-            for (int f = 0; f < NFLD; ++f) put_field(A2w, Lcap, R, q, r, f, mk(0.0));
+        put_field(A0w, Lcap, R, q, r, 0, U);
+        put_field(A0w, Lcap, R, q, r, 1, Ud);
+        for (int f = 2; f < NFLD; ++f) put_field(A0w, Lcap, R, q, r, f, mk(0.0));
     }
+    for (int q = 0; q < NS1; ++q)
+        for (int f = 0; f < NFLD; ++f) put_field(A1w, Lcap, R, q, r, f, mk(0.0));
+    for (int q = 0; q < NS2; ++q)
+        for (int f = 0; f < NFLD; ++f) put_field(A2w, Lcap, R, q, r, f, mk(0.0));
 }
 
 // ------------------------------------------------------- source terms
@@ -785,12 +799,13 @@ __global__ void k_psv_abnum(PsvDev d, const int* __restrict__ freqs, int nf, cd*
 // Per (omega, l >= 1): weights of the six basis solutions for every slot
 // (calya + calg for the 13 forward sources, caldveczero for the back ones).
 // Layout co[(slot * NB + b) * nsys + sys].
-__global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restrict__ freqs, int lc,
-                                                  int l0, int nsys, const cd* __restrict__ ab,
+__global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restrict__ freqs, WorkList wl,
+                                                  int nsys, const cd* __restrict__ ab,
                                                   cd* __restrict__ co, int back) {
     int sys = blockIdx.x * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
-    int w = sys / lc, l = l0 + sys % lc;
+    int w, l;
+    wl_map(wl, sys, w, l);
     auto put = [&](int slot, const cd* g) {
         for (int b = 0; b < NB; ++b) co[((size_t)slot * NB + b) * nsys + sys] = g[b];
     };
@@ -840,14 +855,15 @@ __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restric
 
 // Per (omega, l >= 1, receiver group): receiver fields of every slot and the
 // cutoff probe (group 0).
-__global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, int lc, int l0, int nsys,
+__global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int nsys,
                                                     const cd* __restrict__ Xcap, const cd* __restrict__ co,
                                                     double* __restrict__ A0f, double* __restrict__ A1f,
                                                     double* __restrict__ A2f, int Lcap,
                                                     double* __restrict__ amps) {
     int sys = blockIdx.x * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
-    int w = sys / lc, l = l0 + sys % lc;
+    int w, l;
+    wl_map(wl, sys, w, l);
     if (l == 0) return;  // written by k_psv_l0
     const int R = d.R;
     const size_t rows[3] = {(size_t)NS0 * (R + 1) * NFLD * 2, (size_t)NS1 * (R + 1) * NFLD * 2,
@@ -914,7 +930,7 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, int lc, int l0, in
     }
 }
 
-__global__ void k_psv_scan(int nf, int l0, int lc, int Lcap, int maxlmax, double ratl, double tlen,
+__global__ void k_psv_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ratl, double tlen,
                            double vtop, double rtop, const int* __restrict__ freqs,
                            const double* __restrict__ amps, CutState* __restrict__ cut) {
     int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -923,7 +939,8 @@ __global__ void k_psv_scan(int nf, int l0, int lc, int Lcap, int maxlmax, double
     if (c.done) return;
     double omega = 2.0 * kPi * (double)freqs[w] / tlen;
     int lsuf = (int)(omega * rtop / vtop - 0.5) + 1;
-    for (int l = l0; l < l0 + lc; ++l) {
+    const int l0 = wl.lb[w], l1 = l0 + wl.off[w + 1] - wl.off[w];
+    for (int l = l0; l < l1; ++l) {
         if (c.ismall > 20) {
             if (c.llog > l) c.llog = l;
             c.done = 1;
@@ -1135,9 +1152,9 @@ class PsvEngine : public Engine {
   public:
     PsvDev d{};
     DBuf<int> iphase, nlayer, kkdr, elem, hmoff, blkoff, amz, amc, bcrow, rcap, fluid, comp_src, jsta,
-        capmap;
+        capmap, l0col, l0e1;
     DBuf<double> qmu, qkappa, sel, fel, hm, bcval, poly, lam, qkp, fr, r, rrsta;
-    DBuf<cd> B0, B1, B2, Lst, Zst, Xcap, l0scr, ab, co;
+    DBuf<cd> B0, B1, B2, Lst, Zst, Xcap, l0scr, l0d, ab, co;
     int jmin_loc = 1, ncap = 0;
     double vtop = 0, rtop = 0;
 
@@ -1225,7 +1242,7 @@ class PsvEngine : public Engine {
         lam.upload(s->lambda, R, st); qkp.upload(s->qkp, R, st); fr.upload(frv, st);
         // l = 0 compaction (rea2): jsta, compact row of every kept global row
         {
-            std::vector<int> js(R, 0), cs(nn + 1, 0);
+            std::vector<int> js(R, 0), cs(nn + 1, 0), lc(nn + 2, 0), le(nn + 2, 0);
             int itmp = 0;
             for (int iz = 0; iz < nz; ++iz) {
                 for (int ir = 0; ir < R; ++ir)
@@ -1233,13 +1250,25 @@ class PsvEngine : public Engine {
                 int kk = s->kkdr[iz], i1 = itmp + 1, i2;
                 if (s->iphase[iz] == 1) {
                     i2 = (iz != nz - 1) ? i1 + (s->kkdr[iz + 1] - kk) / 2 - 1 : i1 + (nn + 1 - kk) / 2 - 1;
-                    for (int i = i1; i <= i2; ++i) cs[kk + 2 * (i - i1)] = i;
+                    for (int i = i1; i <= i2; ++i) {
+                        cs[kk + 2 * (i - i1)] = i;
+                        lc[i] = kk + 2 * (i - i1);
+                        le[i] = (i == i1) ? (iz == 0 ? 0 : (s->iphase[iz - 1] == 2 ? 3 : 2)) : 2;
+                    }
                 } else {
                     i2 = i1 + (s->kkdr[iz + 1] - kk) - 1;
-                    for (int i = i1; i <= i2; ++i) cs[kk + (i - i1)] = i;
+                    for (int i = i1; i <= i2; ++i) {
+                        cs[kk + (i - i1)] = i;
+                        lc[i] = kk + (i - i1);
+                        le[i] = (i == i1) ? (iz == 0 ? 0 : (s->iphase[iz - 1] == 1 ? 2 : 3)) : 3;
+                    }
                 }
                 itmp = i2;
             }
+            lc.resize(itmp + 1);
+            le.resize(itmp + 1);
+            l0col.upload(lc, st);
+            l0e1.upload(le, st);
             d.nn0 = itmp;
             d.itmp0 = (s->rmin == 0.0) ? 2 : 1;
             jsta.upload(js, st);
@@ -1250,6 +1279,8 @@ class PsvEngine : public Engine {
         vtop = 0.0;
         for (int i = 0; i < 4; ++i) vtop = vtop + s->vsv[4 * (nz - 1) + i] * 1.0;
         rtop = s->vrmax[nz - 1];
+        vtop_ = vtop;
+        rtop_ = rtop;
         // theta tables
         th.th_n = Th;
         th.h_x.resize(Th); th.h_s.resize(Th); th.h_pole.resize(Th);
@@ -1279,14 +1310,21 @@ class PsvEngine : public Engine {
     }
 
     void alloc_batch() {
-        size_t nsys = (size_t)F * Lc, n = (size_t)d.nn - d.itmp + 1;
+        size_t n = (size_t)d.nn - d.itmp + 1;
+        const size_t ls = (size_t)(d.jsrc - d.itmp + 1);
+        size_t per = (n + 1) * 3 * 16 + (n - ls + 2) * 4 * 16 + (size_t)ncap * NB * 16 + NSLOT * NB * 16;
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(32768, (fr / 3) / per));
+        size_t nsys = nsys_max;
         B0.reserve((size_t)F * d.ncol_tot * 4);
         B1.reserve((size_t)F * d.ncol_tot * 4);
         B2.reserve((size_t)F * d.ncol_tot * 4);
         Lst.reserve((n + 1) * 3 * nsys);
-        Zst.reserve((n + 1) * 4 * nsys);
+        Zst.reserve((n - ls + 2) * 4 * nsys);
         Xcap.reserve((size_t)ncap * NB * nsys);
-        l0scr.reserve((size_t)F * (d.nn0 + 1) * 6);
+        l0scr.reserve((size_t)F * (d.nn0 + 1) * 2);
+        l0d.reserve((size_t)F * (d.nn0 + 1) * 4);
         ab.reserve((size_t)F * 320);
         co.reserve((size_t)NSLOT * NB * nsys);
         for (int m = 0; m < 3; ++m) Afld[m].reserve((size_t)F * rows_m[m] * Lcap);
@@ -1307,20 +1345,34 @@ class PsvEngine : public Engine {
         return *nt;
     }
 
+    bool l0_done = false;
     void omega_pieces(const int* fr_, int nf) override {
+        l0_done = false;
         dim3 grid((d.ncol_tot + 127) / 128, nf);
+        int id = kid("psv_omega_blocks");
+        kbegin(id);
         k_psv_omega<<<grid, 128, 0, st>>>(d, fr_, B0.p, B1.p, B2.p);
+        kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
         k_psv_abnum<<<(nf + 31) / 32, 32, 0, st>>>(d, fr_, nf, ab.p);
         DSM_LAUNCH(*this);
     }
 
-    void solve_chunk(const int* fr_, int nf, int l0, int lc) override {
-        int nsys = nf * lc;
-        if (l0 == 0) {
-            k_psv_l0<<<(nf + 31) / 32, 32, 0, st>>>(d, fr_, nf, B0.p, B1.p, B2.p, l0scr.p, Afld[0].p,
-                                                    Afld[1].p, Afld[2].p, Lcap, rsgt_sw);
+    void solve_chunk(const int* fr_, int nf, const WorkList& wl, int nsys) override {
+        if (!l0_done) {  // order 0 once per batch (its own tridiagonal system)
+            // order 0 is independent of the other orders: it runs on the side
+            // stream while the band solves run, and joins before the l-sum
+            fork_side();
+            int id0 = kid("psv_order0");
+            kbegin(id0, st2);
+            k_psv_l0_build<<<dim3((d.nn0 + 127) / 128, nf), 128, 0, st2>>>(d, B0.p, B1.p, B2.p, l0col.p,
+                                                                            l0e1.p, l0scr.p);
+            k_psv_l0_solve<<<(nf + 31) / 32, 32, 0, st2>>>(d, fr_, nf, ab.p, l0scr.p, l0d.p, rsgt_sw);
+            k_psv_l0_fields<<<dim3((R + 1 + 127) / 128, nf), 128, 0, st2>>>(d, l0d.p, Afld[0].p, Afld[1].p,
+                                                                             Afld[2].p, Lcap, rsgt_sw);
+            kend(id0, 0.0, 0.0, st2);
             DSM_LAUNCH(*this);
+            l0_done = true;
         }
         // algorithmic bytes of a system: band factor (b+1) N complex written
         // and read once, plus value and derivative of every solved right-hand
@@ -1329,28 +1381,31 @@ class PsvEngine : public Engine {
         const double alg = 2.0 * 4.0 * nrow * 16.0 + 18.0 * R * 2 * 2 * 16.0;
         int id = kid("psv_band_solve");
         kbegin(id);
-        k_psv_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, B0.p, B1.p, B2.p, lc, l0, nsys, jmin_loc,
+        k_psv_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, B0.p, B1.p, B2.p, wl, nsys, jmin_loc,
                                                         capmap.p, Lst.p, Zst.p, Xcap.p);
         kend(id, alg * nsys, 0.0);
         DSM_LAUNCH(*this);
         id = kid("psv_source_coef");
         kbegin(id);
-        k_psv_coef<<<(nsys + 127) / 128, 128, 0, st>>>(d, fr_, lc, l0, nsys, ab.p, co.p, rsgt_sw);
+        k_psv_coef<<<(nsys + 127) / 128, 128, 0, st>>>(d, fr_, wl, nsys, ab.p, co.p, rsgt_sw);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
         dim3 grid((nsys + 127) / 128, (R + 15) / 16);
         id = kid("psv_fields");
         kbegin(id);
-        k_psv_fields<<<grid, 128, 0, st>>>(d, lc, l0, nsys, Xcap.p, co.p, Afld[0].p, Afld[1].p, Afld[2].p,
+        k_psv_fields<<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, Afld[0].p, Afld[1].p, Afld[2].p,
                                            Lcap, amps.p);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
         stats.solve_bytes += (double)nsys * (d.nn - d.itmp + 1) * 3 * 16.0 * 2;
     }
 
-    void scan_chunk(int nf, int l0, int lc) override {
-        k_psv_scan<<<(nf + 31) / 32, 32, 0, st>>>(nf, l0, lc, Lcap, maxlmax, ratl, tlen, vtop, rtop,
+    void scan_chunk(int nf, const WorkList& wl) override {
+        int id = kid("psv_cutoff_scan");
+        kbegin(id);
+        k_psv_scan<<<(nf + 31) / 32, 32, 0, st>>>(nf, wl, Lcap, maxlmax, ratl, tlen, vtop, rtop,
                                                   d_freqs.p, amps.p, cut.p);
+        kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
     }
 

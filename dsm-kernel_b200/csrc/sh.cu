@@ -100,13 +100,14 @@ __global__ void k_sh_omega(ShDev d, const int* __restrict__ freqs, cd* __restric
 // (the two rows the source excitation g2 occupies, calg2) and e_nn (the
 // surface row of the back-propagated source).
 __global__ void __launch_bounds__(128) k_sh_solve(ShDev d, const cd* __restrict__ a0,
-                                                  const cd* __restrict__ a2, int lc, int l0, int nsys,
+                                                  const cd* __restrict__ a2, WorkList wl, int nsys,
                                                   int jmin, const int* __restrict__ capmap,
                                                   cd* __restrict__ Lst, cd* __restrict__ Zst,
                                                   cd* __restrict__ Xcap) {
     int sys = blockIdx.x * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
-    int w = sys / lc, l = l0 + sys % lc;
+    int w, l;
+    wl_map(wl, sys, w, l);
     const int nn = d.nn, s = d.srow;
     const cd* A0 = a0 + (size_t)w * (nn + 1) * 2;
     const cd* A2 = a2 + (size_t)w * (nn + 1) * 2;
@@ -116,8 +117,8 @@ __global__ void __launch_bounds__(128) k_sh_solve(ShDev d, const cd* __restrict_
     cd dr = mk(1.0) / dg;
     cd z0 = mk(s == 1 ? 1.0 : 0.0), z1 = mk(0.0);
     if (s == 1) {
-        Zst[((size_t)1 * 2 + 0) * nsys + sys] = z0 * dr;
-        Zst[((size_t)1 * 2 + 1) * nsys + sys] = z1 * dr;
+        Zst[((size_t)0 * 2 + 0) * nsys + sys] = z0 * dr;
+        Zst[((size_t)0 * 2 + 1) * nsys + sys] = z1 * dr;
     }
     for (int j = 2; j <= nn; ++j) {
         cd off = A0[2 * j] + mk(xl2) * A2[2 * j];
@@ -128,9 +129,9 @@ __global__ void __launch_bounds__(128) k_sh_solve(ShDev d, const cd* __restrict_
         if (j > jmin) Lst[(size_t)j * nsys + sys] = L;
         z0 = mk(j == s ? 1.0 : 0.0) - L * z0;      // z(j) = b(j) - a(1,j) z(j-1)
         z1 = mk(j == s + 1 ? 1.0 : 0.0) - L * z1;
-        if (j >= s) {
-            Zst[((size_t)j * 2 + 0) * nsys + sys] = z0 * dr;
-            Zst[((size_t)j * 2 + 1) * nsys + sys] = z1 * dr;
+        if (j >= s) {  // rows below the source have zero scaled forward vectors
+            Zst[((size_t)(j - s) * 2 + 0) * nsys + sys] = z0 * dr;
+            Zst[((size_t)(j - s) * 2 + 1) * nsys + sys] = z1 * dr;
         }
     }
     // upward substitution b(j) = z(j) - a(1,j+1) b(j+1), from the surface down
@@ -145,8 +146,8 @@ __global__ void __launch_bounds__(128) k_sh_solve(ShDev d, const cd* __restrict_
         cd L = Lst[(size_t)(j + 1) * nsys + sys];
         cd zh0 = mk(0.0), zh1 = mk(0.0);
         if (j >= s) {
-            zh0 = Zst[((size_t)j * 2 + 0) * nsys + sys];
-            zh1 = Zst[((size_t)j * 2 + 1) * nsys + sys];
+            zh0 = Zst[((size_t)(j - s) * 2 + 0) * nsys + sys];
+            zh1 = Zst[((size_t)(j - s) * 2 + 1) * nsys + sys];
         }
         x0 = zh0 - L * x0;
         x1 = zh1 - L * x1;
@@ -184,13 +185,14 @@ __device__ cd sh_rvec(int l, int icomp, int m) {
 // Per (omega, l): source coefficients of every slot, receiver fields and
 // the cutoff probe.  blockIdx.y selects a group of 32 receivers (group 0
 // also writes the surface pseudo-receiver and the probe).
-__global__ void __launch_bounds__(128) k_sh_fields(ShDev d, const int* __restrict__ freqs, int lc,
-                                                   int l0, int nsys, const cd* __restrict__ Xcap,
+__global__ void __launch_bounds__(128) k_sh_fields(ShDev d, const int* __restrict__ freqs, WorkList wl,
+                                                   int nsys, const cd* __restrict__ Xcap,
                                                    double* __restrict__ A1, double* __restrict__ A2f,
                                                    int Lcap, double* __restrict__ amps) {
     int sys = blockIdx.x * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
-    int w = sys / lc, l = l0 + sys % lc;
+    int w, l;
+    wl_map(wl, sys, w, l);
     const int R = d.R;
     const int rows1 = SH_NSLOT1 * (R + 1) * SH_NF * 2, rows2 = SH_NSLOT2 * (R + 1) * SH_NF * 2;
     double* A1w = A1 + (size_t)w * rows1 * Lcap + l;
@@ -350,7 +352,7 @@ __global__ void __launch_bounds__(128) k_sh_fields(ShDev d, const int* __restric
 }
 
 // cutoff scan: one thread per frequency
-__global__ void k_sh_scan(int nf, int l0, int lc, int Lcap, int maxlmax, double ratl, double tlen,
+__global__ void k_sh_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ratl, double tlen,
                           double vtop, double rtop, const int* __restrict__ freqs,
                           const double* __restrict__ amps, CutState* __restrict__ cut) {
     int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -359,7 +361,8 @@ __global__ void k_sh_scan(int nf, int l0, int lc, int Lcap, int maxlmax, double 
     if (c.done) return;
     double omega = 2.0 * kPi * (double)freqs[w] / tlen;
     int lsuf = (int)(omega * rtop / vtop - 0.5) + 1;  // callsuf
-    for (int l = l0; l < l0 + lc; ++l) {
+    const int l0 = wl.lb[w], l1 = l0 + wl.off[w + 1] - wl.off[w];
+    for (int l = l0; l < l1; ++l) {
         if (c.ismall > 20) {
             if (c.llog > l) c.llog = l;
             c.done = 1;
@@ -560,6 +563,8 @@ class ShEngine : public Engine {
         vtop = 0.0;
         for (int i = 0; i < 4; ++i) vtop = vtop + s->vsv[4 * (s->nzone - 1) + i] * 1.0;
         rtop = s->vrmax[s->nzone - 1];
+        vtop_ = vtop;
+        rtop_ = rtop;
         // capture rows: receiver stencils and the surface
         std::vector<int> cm(nn + 1, -1), rc(3 * (size_t)R);
         jmin = nn;
@@ -603,11 +608,16 @@ class ShEngine : public Engine {
     }
 
     void alloc_batch() {
-        size_t nsys = (size_t)F * Lc, nn = d.nn;
+        size_t nn = d.nn;
+        size_t per = (nn + 1) * 16 + (nn - d.srow + 2) * 2 * 16 + (size_t)ncap * 3 * 16;
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(32768, (fr / 3) / per));
+        size_t nsys = nsys_max;
         a0.reserve((size_t)F * (nn + 1) * 2);
         a2.reserve((size_t)F * (nn + 1) * 2);
         Lst.reserve((nn + 1) * nsys);
-        Zst.reserve((nn + 1) * 2 * nsys);
+        Zst.reserve((nn - d.srow + 2) * 2 * nsys);
         Xcap.reserve((size_t)ncap * 3 * nsys);
         Afld[1].reserve((size_t)F * rows_m[1] * Lcap);
         Afld[2].reserve((size_t)F * rows_m[2] * Lcap);
@@ -634,24 +644,24 @@ class ShEngine : public Engine {
         DSM_LAUNCH(*this);
     }
 
-    void solve_chunk(const int* fr, int nf, int l0, int lc) override {
-        int nsys = nf * lc;
+    void solve_chunk(const int* fr, int nf, const WorkList& wl, int nsys) override {
+        (void)nf;
         const double alg = 2.0 * 2.0 * d.nn * 16.0 + 14.0 * R * 2 * 2 * 16.0;
         int id = kid("sh_band_solve");
         kbegin(id);
-        k_sh_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, a0.p, a2.p, lc, l0, nsys, jmin, capmap.p,
+        k_sh_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, a0.p, a2.p, wl, nsys, jmin, capmap.p,
                                                        Lst.p, Zst.p, Xcap.p);
         kend(id, alg * nsys, 0.0);
         DSM_LAUNCH(*this);
         dim3 grid((nsys + 127) / 128, (R + 31) / 32);
-        k_sh_fields<<<grid, 128, 0, st>>>(d, fr, lc, l0, nsys, Xcap.p, Afld[1].p, Afld[2].p, Lcap,
+        k_sh_fields<<<grid, 128, 0, st>>>(d, fr, wl, nsys, Xcap.p, Afld[1].p, Afld[2].p, Lcap,
                                           amps.p);
         DSM_LAUNCH(*this);
         stats.solve_bytes += (double)nsys * d.nn * 2 * 16.0 * 2;
     }
 
-    void scan_chunk(int nf, int l0, int lc) override {
-        k_sh_scan<<<(nf + 31) / 32, 32, 0, st>>>(nf, l0, lc, Lcap, maxlmax, ratl, tlen, vtop, rtop,
+    void scan_chunk(int nf, const WorkList& wl) override {
+        k_sh_scan<<<(nf + 31) / 32, 32, 0, st>>>(nf, wl, Lcap, maxlmax, ratl, tlen, vtop, rtop,
                                                  d_freqs.p, amps.p, cut.p);
         DSM_LAUNCH(*this);
     }
