@@ -38,6 +38,14 @@ void Engine::init_common(int dev) {
     DSM_CUBLAS(cublasCreate(&cub));
     DSM_CUBLAS(cublasSetStream(cub, st));
     for (auto& e : ev) DSM_CUDA(cudaEventCreate(&e));
+    DSM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (opt.precision != DSM_PREC_FP64 && !mixed())
+        throw Error(DSM_ERR_INVALID, "unknown precision mode " + std::to_string(opt.precision));
+    tc_fmt = opt.precision == DSM_PREC_MIXED_BF16 ? tc::PIECE_BF16 : tc::PIECE_F16;
+    if (mixed()) {
+        tc_err.reserve(1);
+        DSM_CUDA(cudaMemset(tc_err.p, 0, sizeof(int)));
+    }
 }
 
 Engine::~Engine() {
@@ -124,6 +132,100 @@ void Engine::build_basis(int lneed) {
     cap = std::min(cap, maxlmax + 1);
     if (cap < lneed) cap = lneed;
     launch_basis_tables(*this, cap);
+    if (mixed()) {  // split the new tables once; every batch reuses them
+        kcB = (lcapB + 63) / 64 * 64;
+        for (int m = m_lo; m <= 2; ++m) {
+            Bpc[m].reserve((size_t)2 * 2 * Th * kcB);
+            sB[m].reserve((size_t)2 * Th);
+            tc::split_bases(basis[m].p, 2 * Th, lcapB, Bpc[m].p, sB[m].p, kcB, tc_fmt, st);
+            launches++;
+        }
+    }
+}
+
+// Mixed l-sum of a batch: split the field matrices, then one persistent
+// tensor-core launch over every (frequency, |m|) contraction (in groups of
+// at most tc::MAXP).  Outputs go to Cmix, one block per frequency.
+void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
+    kcA = (Lcap + 63) / 64 * 64;
+    for (int m = m_lo; m <= 2; ++m) {
+        if (!rows_m[m]) continue;
+        Apc[m].reserve((size_t)2 * F * rows_m[m] * kcA);
+        sA[m].reserve((size_t)F * rows_m[m]);
+    }
+    Cmix.reserve((size_t)F * c_total());
+    d_nord.upload(nord, st);
+    double split_bytes = 0.0, tflops = 0.0, tc_bytes = 0.0;
+    for (int m = m_lo; m <= 2; ++m)
+        for (int w = 0; w < nf; ++w) {
+            const double kp = (double)((nord[w] + tc_bk - 1) / tc_bk * tc_bk);
+            split_bytes += (double)rows_m[m] * (8.0 * nord[w] + 4.0 * kp);
+        }
+    int id = kid("lsum_split");
+    kbegin(id);
+    for (int m = m_lo; m <= 2; ++m) {
+        if (!rows_m[m]) continue;
+        tc::split_fields(Afld[m].p, nf, rows_m[m], Lcap, d_nord.p, Apc[m].p, sA[m].p, kcA, F, tc_fmt, tc_bk, st);
+        launches++;
+    }
+    kend(id, split_bytes, 0.0);
+
+    tc::Maps maps;
+    std::memset(&maps, 0, sizeof(maps));
+    for (int m = m_lo; m <= 2; ++m) {
+        if (!rows_m[m]) continue;
+        tc::encode_a(&maps.a[m], Apc[m].p, tc_fmt, kcA, rows_m[m], F, tc_bk);
+        tc::encode_b(&maps.b[m], Bpc[m].p, tc_fmt, kcB, 2 * Th, tc_bk);
+    }
+    std::vector<tc::Problem> hp;
+    const int N = 2 * Th, tn = (N + tc::BN - 1) / tc::BN;
+    for (int w = 0; w < nf; ++w)
+        for (int m = m_lo; m <= 2; ++m) {
+            if (!rows_m[m]) continue;
+            tc::Problem P{};
+            P.amap = m;
+            P.z = w;
+            P.bmap = m;
+            P.kblocks = (nord[w] + tc_bk - 1) / tc_bk;
+            P.M = rows_m[m];
+            P.N = N;
+            P.tiles_n = tn;
+            P.C = Cmix.p + (size_t)w * c_total() + c_off(m);
+            P.sa = sA[m].p + (size_t)w * rows_m[m];
+            P.sb = sB[m].p;
+            P.ldc = P.M;
+            hp.push_back(P);
+            const double kp = (double)P.kblocks * tc_bk;
+            tflops += 3.0 * 2.0 * P.M * (double)N * kp;
+            tc_bytes += 4.0 * ((double)P.M + N) * kp + 4.0 * (double)P.M * N;
+        }
+    tcp.reserve(hp.size());
+    id = kid("lsum_tc");
+    kbegin(id);
+    for (size_t g = 0; g < hp.size(); g += tc::MAXP) {
+        const int np = (int)std::min<size_t>(tc::MAXP, hp.size() - g);
+        int tiles = 0;
+        for (int i = 0; i < np; ++i) {
+            hp[g + i].tile0 = tiles;
+            tiles += ((hp[g + i].M + tc::BM - 1) / tc::BM) * tn;
+        }
+        DSM_CUDA(cudaMemcpyAsync(tcp.p + g, hp.data() + g, sizeof(tc::Problem) * np, cudaMemcpyHostToDevice, st));
+        tc::launch(maps, tcp.p + g, np, tiles, tc_fmt, tc_bk, tc_err.p, nsm, st);
+        launches++;
+    }
+    kend(id, tc_bytes, tflops);
+    // cudaMemcpyAsync from pageable memory has consumed hp when it returns
+}
+
+void Engine::check_tc_error() {
+    if (!mixed()) return;
+    int h = 0;
+    DSM_CUDA(cudaMemcpyAsync(&h, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DSM_CUDA(cudaStreamSynchronize(st));
+    if (h) {
+        DSM_CUDA(cudaMemsetAsync(tc_err.p, 0, sizeof(int), st));
+        throw Error(DSM_ERR_TIMEOUT, "a bounded wait in the tensor-core l-sum gave up");
+    }
 }
 
 void Engine::build_weights(const double* d_r, const double* d_rrsta) {
@@ -275,9 +377,15 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             kend(id, 0.0, 0.0);
         }
         DSM_CUDA(cudaEventRecord(eg0, st));
+        if (mixed()) {
+            std::vector<int> nord(nf);
+            for (int w = 0; w < nf; ++w) nord[w] = hc[w].norders;
+            lsum_mixed(nf, nord);
+        }
         for (int w = 0; w < nf; ++w) {
             stats.orders_used += hc[w].norders;
-            for (int mi = m_lo; mi <= 2; ++mi) gemm_fp64(w, mi, hc[w].norders);
+            if (!mixed())
+                for (int mi = m_lo; mi <= 2; ++mi) gemm_fp64(w, mi, hc[w].norders);
             epilogue(d_freqs.p, w, nf);
             for (int mi = m_lo; mi <= 2; ++mi)
                 stats.lsum_flops += 2.0 * rows_m[mi] * 2.0 * Th * hc[w].norders;
@@ -309,6 +417,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             }
         }
         DSM_CUDA(cudaStreamSynchronize(st));
+        check_tc_error();
         kcollect();
         float a = 0, g = 0;
         cudaEventElapsedTime(&a, es0, es1);

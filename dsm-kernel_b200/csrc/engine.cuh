@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "lsum_tc.cuh"
 
 namespace dsm {
 
@@ -100,6 +101,24 @@ class Engine {
     void build_basis(int lneed);
     void build_weights(const double* r, const double* rrsta);
     void gemm_fp64(int w, int mi, int K);
+
+    // mixed precision: the l-sum as split 16-bit products on the tensor
+    // cores (fields and bases split once per batch / per table build)
+    bool mixed() const { return opt.precision == DSM_PREC_MIXED || opt.precision == DSM_PREC_MIXED_BF16; }
+    int tc_fmt = tc::PIECE_F16, tc_bk = 32, nsm = 148;
+    int kcA = 0, kcB = 0;            // order capacities of the pieces (x64)
+    DBuf<uint16_t> Apc[3];           // [2][F][rows][kcA]
+    DBuf<float> sA[3];               // [F][rows]
+    DBuf<uint16_t> Bpc[3];           // [2][2Th][kcB]
+    DBuf<float> sB[3];               // [2Th]
+    DBuf<float> Cmix;                // [F][c_total] column-major blocks
+    DBuf<tc::Problem> tcp;
+    DBuf<int> tc_err, d_nord;
+    void lsum_mixed(int nf, const std::vector<int>& norders);
+    void check_tc_error();
+    // contraction output of (frequency w, |m|) for the epilogue
+    const double* c64(int mi) const { return Cgemm.p + c_off(mi); }
+    const float* c32(int w, int mi) const { return Cmix.p + (size_t)w * c_total() + c_off(mi); }
     // optional per-kernel event timing
     bool prof = false;
     std::vector<cudaEvent_t> evpool;

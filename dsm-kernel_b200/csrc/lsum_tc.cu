@@ -1,0 +1,451 @@
+// Split-precision l-sum contraction on the sm_100a tensor cores.
+//
+// Persistent, warp-specialised kernel, one CTA per SM:
+//   warp 0      TMA producer: per stage, the hi and lo pieces of a 128 x BK
+//               A tile and of a 256 x BK B tile (four bulk tensor loads,
+//               one mbarrier with the byte count)
+//   warp 1      MMA issuer: per stage and 16-order step, three
+//               tcgen05.mma (hi*hi, hi*lo, lo*hi) into a 128 x 256 FP32
+//               accumulator in tensor memory; tcgen05.commit frees the stage
+//   warps 2..5  epilogue: tcgen05.ld of the accumulator (each warp its
+//               32-lane quarter), row x column scaling, coalesced stores of
+//               the column-major output (consecutive lanes = consecutive rows)
+// Two accumulators (2 x 256 columns, all of tensor memory) let the epilogue
+// of one tile overlap the MMAs of the next.  Every wait is bounded: after
+// about a second a role raises the CTA's abort flag, all roles leave their
+// loops, the issued copies and MMAs are waited for (again bounded), the
+// tensor memory is freed and the error word is set for the host.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <mutex>
+
+#include "lsum_tc.cuh"
+
+namespace dsm {
+namespace tc {
+
+namespace {
+
+constexpr int NTHREADS = 192;
+constexpr uint32_t TMEM_COLS = 512;
+constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait.  Gives up when another role has aborted or after the limit
+// (then it aborts the CTA itself).
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+    const unsigned long long t0 = gtimer();
+    for (uint32_t n = 0;; ++n) {
+        if (mbar_try(b, parity)) return true;
+        if ((n & 63) == 63) {
+            if (*abort_flag) return false;
+            if (gtimer() - t0 > WAIT_LIMIT_NS) {
+                *abort_flag = 1;
+                return false;
+            }
+        }
+    }
+}
+// Bounded wait used while draining after an abort (ignores the flag).
+__device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity) {
+    const unsigned long long t0 = gtimer();
+    while (!mbar_try(b, parity))
+        if (gtimer() - t0 > WAIT_LIMIT_NS) return;
+}
+
+__device__ __forceinline__ void tma_a(const CUtensorMap* m, void* dst, uint64_t* bar, int x, int y, int z, int w) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+        "[%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(m)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z), "r"(w)
+        : "memory");
+}
+__device__ __forceinline__ void tma_b(const CUtensorMap* m, void* dst, uint64_t* bar, int x, int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+        "[%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(m)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor of an order-major tile whose rows are
+// BK*2 bytes, swizzled as the TMA wrote them (64B or 128B pattern), 8-row
+// groups at 8*BK*2 bytes.
+template <int BK>
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
+    constexpr uint64_t layout = BK == 32 ? 4 : 2;   // SWIZZLE_64B : SWIZZLE_128B
+    constexpr uint64_t sbo = (8 * BK * 2) >> 4;
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | (1ull << 16) | (sbo << 32) | (1ull << 46) | (layout << 61);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void decode(const Problem* ps, int np, int t, int& p, int& mt, int& nt) {
+    p = 0;
+    while (p + 1 < np && ps[p + 1].tile0 <= t) ++p;
+    const int loc = t - ps[p].tile0;
+    mt = loc / ps[p].tiles_n;
+    nt = loc - mt * ps[p].tiles_n;
+}
+
+template <int BK>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    k_lsum_tc(const __grid_constant__ Maps maps, const Problem* __restrict__ probs, int np, int ntiles,
+              uint32_t idesc, int* __restrict__ err) {
+    constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
+    constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
+    constexpr int STAGES = (4 * 48 * 1024) / STAGE;
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], tfull[2], tempty[2], fin;
+    __shared__ uint32_t tmem_sh;
+    __shared__ int abort_sh;
+    __shared__ Problem ps[MAXP];
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    volatile int* abort_flag = &abort_sh;
+
+    for (int i = threadIdx.x; i < np; i += NTHREADS) ps[i] = probs[i];
+    if (threadIdx.x == 0) {
+        abort_sh = 0;
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 128);
+        }
+        mbar_init(&fin, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.a[0])) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.b[0])) : "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_sh;
+
+    if (warp == 0) {
+        if (lane == 0) {  // ---------------------------------------- producer
+            int it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                int p, mt, nt;
+                decode(ps, np, t, p, mt, nt);
+                const Problem& P = ps[p];
+                for (int kb = 0; kb < P.kblocks; ++kb, ++it) {
+                    const int s = it % STAGES;
+                    const uint32_t ph = (it / STAGES) & 1;
+                    if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    unsigned char* sp = base + s * STAGE;
+                    mbar_expect_tx(&full[s], STAGE);
+                    tma_a(&maps.a[P.amap], sp, &full[s], kb * BK, mt * BM, P.z, 0);
+                    tma_a(&maps.a[P.amap], sp + A_BYTES, &full[s], kb * BK, mt * BM, P.z, 1);
+                    tma_b(&maps.b[P.bmap], sp + 2 * A_BYTES, &full[s], kb * BK, nt * BN, 0);
+                    tma_b(&maps.b[P.bmap], sp + 2 * A_BYTES + B_BYTES, &full[s], kb * BK, nt * BN, 1);
+                }
+            }
+            // every issued copy has landed before the CTA may exit
+            for (int s = 0; s < STAGES && s < it; ++s) {
+                const int last = s + ((it - 1 - s) / STAGES) * STAGES;
+                mbar_drain(&full[s], (last / STAGES) & 1);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {  // ---------------------------------------- MMA issuer
+            int it = 0, tcnt = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tcnt) {
+                int p, mt, nt;
+                decode(ps, np, t, p, mt, nt);
+                const int b = tcnt & 1;
+                if (!mbar_wait(&tempty[b], ((tcnt >> 1) & 1) ^ 1, abort_flag)) break;
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(b * BN);
+                const int kbn = ps[p].kblocks;
+                for (int kb = 0; kb < kbn; ++kb, ++it) {
+                    const int s = it % STAGES;
+                    if (!mbar_wait(&full[s], (it / STAGES) & 1, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t ah = smem_u32(base + s * STAGE), al = ah + A_BYTES;
+                    const uint32_t bh = ah + 2 * A_BYTES, bl = bh + B_BYTES;
+#pragma unroll
+                    for (int j = 0; j < BK / 16; ++j) {
+                        const uint32_t o = 32u * j;
+                        mma_f16(d, sdesc<BK>(ah + o), sdesc<BK>(bh + o), idesc, (kb | j) != 0);
+                        mma_f16(d, sdesc<BK>(ah + o), sdesc<BK>(bl + o), idesc, 1);
+                        mma_f16(d, sdesc<BK>(al + o), sdesc<BK>(bh + o), idesc, 1);
+                    }
+                    mma_commit(&empty[s]);
+                }
+                if (ok) mma_commit(&tfull[b]);
+            }
+            // all issued MMAs complete before tensor memory is released
+            mma_commit(&fin);
+            mbar_drain(&fin, 0);
+        }
+    } else {  // ------------------------------------------------------ epilogue
+        const int q = warp & 3;  // tensor-memory lane quarter of this warp
+        int tcnt = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcnt) {
+            int p, mt, nt;
+            decode(ps, np, t, p, mt, nt);
+            const int b = tcnt & 1;
+            const bool got = mbar_wait(&tfull[b], (tcnt >> 1) & 1, abort_flag);
+            if (!__all_sync(0xffffffffu, got)) break;
+            tc_fence_after();
+            const Problem& P = ps[p];
+            const int m = mt * BM + q * 32 + lane;
+            const bool mv = m < P.M;
+            const float rs = mv ? P.sa[m] : 0.0f;
+            float* Cm = P.C + m;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                uint32_t r[32];
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + c0), r);
+                const int n0 = nt * BN + c0;
+                if (mv) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int n = n0 + j;
+                        if (n < P.N) Cm[(long long)n * P.ldc] = __uint_as_float(r[j]) * rs * P.sb[n];
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&tempty[b]);
+        }
+    }
+
+    __syncthreads();
+    if (warp == 0) {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
+                     : "memory");
+    }
+    if (threadIdx.x == 0 && abort_sh) atomicExch(err, 1);
+}
+
+// ------------------------------------------------------------ piece split
+// x = s (hi + lo): s = 2^e with the row (column) maximum scaled into
+// [2^14, 2^15), below the fp16 limit with a factor-two margin.  The scale is
+// exact, so hi + lo carries ~22 (fp16) or ~16 (bf16) significant bits.
+__device__ __forceinline__ int piece_exp(double mx) {
+    if (!(mx > 0.0)) return 0;
+    int e = ilogb(mx) - 14;
+    return max(-126, min(127, e));
+}
+__device__ __forceinline__ void split2(double x, int fmt, uint16_t& hi, uint16_t& lo) {
+    if (fmt == PIECE_BF16) {
+        __nv_bfloat16 h = __double2bfloat16(x);
+        __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
+        hi = __bfloat16_as_ushort(h);
+        lo = __bfloat16_as_ushort(l);
+    } else {
+        __half h = __double2half(x);
+        __half l = __double2half(x - (double)__half2float(h));
+        hi = __half_as_ushort(h);
+        lo = __half_as_ushort(l);
+    }
+}
+
+// one warp per row: row maximum over the counted orders, then the pieces
+__global__ void k_split_rows(const double* __restrict__ A, int nrows, int per_w, int lcap,
+                             const int* __restrict__ nord, int kcap, int bk, uint16_t* __restrict__ P,
+                             size_t piece_stride, float* __restrict__ sa, int fmt) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= nrows) return;
+    const int K = nord ? min(nord[row / per_w], lcap) : lcap;
+    const int Kp = min(kcap, (K + bk - 1) / bk * bk);
+    const double* a = A + (size_t)row * lcap;
+    double mx = 0.0;
+    for (int l = lane; l < K; l += 32) mx = fmax(mx, fabs(a[l]));
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const int e = piece_exp(mx);
+    if (lane == 0) sa[row] = __int_as_float((127 + e) << 23);
+    uint16_t* ph = P + (size_t)row * kcap;
+    uint16_t* pl = ph + piece_stride;
+    for (int l = lane; l < Kp; l += 32) {
+        uint16_t h = 0, lo = 0;
+        if (l < K) split2(scalbn(a[l], -e), fmt, h, lo);
+        ph[l] = h;
+        pl[l] = lo;
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    if (!fn) throw Error(DSM_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    return fn;
+}
+
+CUtensorMapDataType dtype(int piece_fmt) {
+    return piece_fmt == PIECE_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+}
+
+void check(CUresult r, const char* what) {
+    if (r != CUDA_SUCCESS) throw Error(DSM_ERR_CUDA, std::string("tensor map for ") + what + " rejected (" +
+                                                         std::to_string((int)r) + ")");
+}
+
+}  // namespace
+
+void encode_a(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int rows, int nfreq, int bk) {
+    if (kcap % bk) throw Error(DSM_ERR_INVALID, "order capacity of the split fields is not a multiple of BK");
+    cuuint64_t dims[4] = {(cuuint64_t)kcap, (cuuint64_t)rows, (cuuint64_t)nfreq, 2};
+    cuuint64_t strides[3] = {(cuuint64_t)kcap * 2, (cuuint64_t)kcap * 2 * rows, (cuuint64_t)kcap * 2 * rows * nfreq};
+    cuuint32_t box[4] = {(cuuint32_t)bk, BM, 1, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    check(encoder()(m, dtype(piece_fmt), 4, const_cast<void*>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    bk == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE),
+          "the split fields");
+}
+
+void encode_b(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int cols, int bk) {
+    if (kcap % bk) throw Error(DSM_ERR_INVALID, "order capacity of the split bases is not a multiple of BK");
+    cuuint64_t dims[3] = {(cuuint64_t)kcap, (cuuint64_t)cols, 2};
+    cuuint64_t strides[2] = {(cuuint64_t)kcap * 2, (cuuint64_t)kcap * 2 * cols};
+    cuuint32_t box[3] = {(cuuint32_t)bk, BN, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    check(encoder()(m, dtype(piece_fmt), 3, const_cast<void*>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    bk == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE),
+          "the split bases");
+}
+
+void split_fields(const double* A, int nf, int rows, int lcap, const int* d_nord, uint16_t* P, float* sa,
+                  int kcap, int F, int piece_fmt, int bk, cudaStream_t st) {
+    const int n = nf * rows;
+    if (n <= 0) return;
+    if (kcap % bk) throw Error(DSM_ERR_INVALID, "order capacity of the split fields is not a multiple of BK");
+    k_split_rows<<<(n + 7) / 8, 256, 0, st>>>(A, n, rows, lcap, d_nord, kcap, bk, P, (size_t)F * rows * kcap, sa,
+                                              piece_fmt);
+    DSM_CUDA(cudaGetLastError());
+}
+
+void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, int kcap, int piece_fmt,
+                 cudaStream_t st) {
+    if (cols <= 0) return;
+    k_split_rows<<<(cols + 7) / 8, 256, 0, st>>>(B, cols, cols, lcap, nullptr, kcap, kcap, P,
+                                                 (size_t)cols * kcap, sb, piece_fmt);
+    DSM_CUDA(cudaGetLastError());
+}
+
+void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int piece_fmt, int bk, int* d_err,
+            int nsm, cudaStream_t st) {
+    if (np <= 0 || ntiles <= 0) return;
+    if (np > MAXP) throw Error(DSM_ERR_INVALID, "too many contractions in one launch");
+    // kind::f16 instruction descriptor: FP32 accumulator, both operands of
+    // the piece type and order-major, N = 256, M = 128
+    const uint32_t fmt = piece_fmt == PIECE_BF16 ? 1u : 0u;
+    const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+    const int grid = std::min(ntiles, nsm);
+    const size_t smem = 4 * 48 * 1024 + 1024;
+    if (bk == 32) {
+        static bool attr32 = false;
+        if (!attr32) {
+            DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr32 = true;
+        }
+        k_lsum_tc<32><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, d_err);
+    } else if (bk == 64) {
+        static bool attr64 = false;
+        if (!attr64) {
+            DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr64 = true;
+        }
+        k_lsum_tc<64><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, d_err);
+    } else {
+        throw Error(DSM_ERR_INVALID, "BK must be 32 or 64");
+    }
+    DSM_CUDA(cudaGetLastError());
+}
+
+}  // namespace tc
+}  // namespace dsm

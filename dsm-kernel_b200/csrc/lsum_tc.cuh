@@ -1,0 +1,65 @@
+// Split-precision l-sum contraction on the sm_100a tensor cores (tcgen05).
+//
+// One launch contracts every (frequency, |m|) problem of a batch:
+//     C[M x N] = sum_l A[M x l] * B[N x l]^T ,   both operands order-major,
+// with A (the receiver fields) and B (the Legendre bases) each stored as two
+// 16-bit pieces, x = s * (x_hi + x_lo) with a power-of-two scale s per row of
+// A and per column of B.  The product runs as x_hi*y_hi + x_hi*y_lo +
+// x_lo*y_hi on the tensor cores with FP32 accumulation in tensor memory;
+// the epilogue applies s_row * s_col and writes C column-major (ld = M),
+// the layout the FP64 contraction writes.
+#pragma once
+
+#include <cuda.h>
+
+#include "common.cuh"
+
+namespace dsm {
+namespace tc {
+
+constexpr int BM = 128;          // rows of a tile (tensor-memory lanes)
+constexpr int BN = 256;          // columns of a tile (tensor-memory columns)
+constexpr int MAXP = 96;         // problems per launch
+constexpr int PIECE_F16 = 0;     // fp16 pieces (11-bit significand each)
+constexpr int PIECE_BF16 = 1;    // bf16 pieces (8-bit significand each)
+
+// One contraction of a launch.  Rows of A beyond M and columns beyond N are
+// read as zeros by the tensor-map bounds and never stored.
+struct Problem {
+    int amap, z, bmap, kblocks;  // A map (|m|), frequency slot, B map, orders / BK
+    int M, N, tiles_n, tile0;    // shape, column tiles, index of the first tile
+    float* C;                    // column-major M x N
+    const float* sa;             // M row scales
+    const float* sb;             // N column scales
+    long long ldc;
+};
+
+struct Maps {
+    CUtensorMap a[3];  // [piece][frequency][row][order] fp16/bf16
+    CUtensorMap b[3];  // [piece][column][order]
+};
+
+// Encodes the tensor maps of a launch.  BK selects the stage depth: 32
+// orders (64-byte rows, 64B swizzle) or 64 orders (128B swizzle).
+void encode_a(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int rows, int nfreq, int bk);
+void encode_b(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int cols, int bk);
+
+// Splits the FP64 field matrices of a batch, A[F][rows][lcap] (orders
+// contiguous), into pieces P[2][F][rows][kcap] with one power-of-two scale
+// per row (sa[F][rows]); orders at or beyond the frequency's count
+// nord[w] become zeros up to the next multiple of bk (the contraction reads
+// whole BK blocks).
+void split_fields(const double* A, int nf, int rows, int lcap, const int* d_nord, uint16_t* P, float* sa,
+                  int kcap, int F, int piece_fmt, int bk, cudaStream_t st);
+// Splits the basis table B[cols][lcap] into P[2][cols][kcap] with one scale
+// per column (sb[cols]); orders >= lcap become zeros.
+void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, int kcap, int piece_fmt,
+                 cudaStream_t st);
+
+// Launches the persistent contraction over all tiles of probs[0..np).
+// err (device int) is set nonzero if a bounded wait inside gave up.
+void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int piece_fmt, int bk,
+            int* d_err, int nsm, cudaStream_t st);
+
+}  // namespace tc
+}  // namespace dsm

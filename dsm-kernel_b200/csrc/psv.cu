@@ -435,86 +435,119 @@ __global__ void k_psv_l0_build(PsvDev d, const cd* __restrict__ B0all, const cd*
     C[2 * i + 1] = a[3];
 }
 
-// (2) one thread per frequency: right-hand sides (calg at l = 0 for imt 1..3,
+// (2) one CTA per frequency: right-hand sides (calg at l = 0 for imt 1..3,
 // the back-propagated vertical force), dcsymbdl0 with half-width 1 fused
 // with the forward substitution of dcsbdlv0, then the upward substitution,
-// for the four right-hand sides at once.  Solutions in Dv[w][i][4].
-__global__ void k_psv_l0_solve(PsvDev d, const int* __restrict__ freqs, int nf, const cd* __restrict__ ab,
-                               cd* __restrict__ Cc, cd* __restrict__ Dv, int back) {
-    int w = blockIdx.x * blockDim.x + threadIdx.x;
+// for the four right-hand sides.  Solutions in Dv[w][i][4].
+// The recurrences are sequential in the row; the CTA streams the compact
+// tridiagonal through shared memory in chunks (coalesced loads and stores
+// by all threads) so that the chains run on shared-memory latency: thread 0
+// factors a chunk, threads 0..3 then carry one right-hand side each.
+constexpr int L0_CH = 384;  // rows per chunk (12 KB factor + 24 KB solution)
+
+__global__ void __launch_bounds__(128) k_psv_l0_solve(PsvDev d, const int* __restrict__ freqs, int nf,
+                                                      const cd* __restrict__ ab, cd* __restrict__ Cc,
+                                                      cd* __restrict__ Dv, int back) {
+    const int w = blockIdx.x;
     if (w >= nf) return;
-    const int n0 = d.nn0, it0 = d.itmp0, n = n0 - it0 + 1;
+    const int n0 = d.nn0, it0 = d.itmp0, tid = threadIdx.x;
     cd* C = Cc + (size_t)w * (n0 + 1) * 2;
     cd* D = Dv + (size_t)w * (n0 + 1) * 4;
-    const double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
-    const cd c1 = coefq(omega, d.qmu[d.spn - 1]), c2 = coefq(omega, d.qkappa[d.spn - 1]);
-    cd ya[4], yb[4], yc[4], yd[4];
-    calya_dev(ab + (size_t)w * 320, ab + (size_t)w * 320 + 160, 0.0, d.ra0, d.ra1, d.r0, ya, yb, yc, yd);
-    // sparse right-hand sides: rea2 keeps the U rows of g0(jtmp..jtmp+3)
-    int rr[5];
-    cd rv[5][4];
-    int nr = 0;
-    for (int k = 0; k < 4; ++k) {
-        int cr = d.comp_src[d.jsrc + k];
-        if (cr <= 0) continue;
-        rr[nr] = cr;
-        for (int b = 0; b < 4; ++b) rv[nr][b] = mk(0.0);
-        ++nr;
-    }
-    for (int imt = 1; imt <= 3; ++imt) {
-        cd g[4];
-        calg_dev(d, 0, 0, c1, c2, 0.0, ya, yb, yc, yd, imt, g);
-        int q = 0;
-        for (int k = 0; k < 4; ++k)
-            if (d.comp_src[d.jsrc + k] > 0) rv[q++][imt - 1] = g[k];
-    }
-    {
+    __shared__ cd sC[L0_CH][2];
+    __shared__ cd sD[L0_CH][4];
+    __shared__ int srr[5];
+    __shared__ cd srv[5][4];
+    __shared__ int snr;
+    if (tid == 0) {
+        const double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
+        const cd c1 = coefq(omega, d.qmu[d.spn - 1]), c2 = coefq(omega, d.qkappa[d.spn - 1]);
+        cd ya[4], yb[4], yc[4], yd[4];
+        calya_dev(ab + (size_t)w * 320, ab + (size_t)w * 320 + 160, 0.0, d.ra0, d.ra1, d.r0, ya, yb, yc, yd);
+        // sparse right-hand sides: rea2 keeps the U rows of g0(jtmp..jtmp+3)
+        int nr = 0;
+        for (int k = 0; k < 4; ++k) {
+            int cr = d.comp_src[d.jsrc + k];
+            if (cr <= 0) continue;
+            srr[nr] = cr;
+            for (int b = 0; b < 4; ++b) srv[nr][b] = mk(0.0);
+            ++nr;
+        }
+        for (int imt = 1; imt <= 3; ++imt) {
+            cd g[4];
+            calg_dev(d, 0, 0, c1, c2, 0.0, ya, yb, yc, yd, imt, g);
+            int q = 0;
+            for (int k = 0; k < 4; ++k)
+                if (d.comp_src[d.jsrc + k] > 0) srv[q++][imt - 1] = g[k];
+        }
         // caldveczero at l = 0: bvec(1,0) = cmplx(coef), single precision
         double coef = sqrt((double)1 / (4.0 * kPi) / 1.0);
         int cr = d.comp_src[d.nn - 1];
-        rr[nr] = cr > 0 ? cr : -1;
-        for (int b = 0; b < 4; ++b) rv[nr][b] = mk(0.0);
-        if (back) rv[nr][3] = -conj(mk((double)(float)coef));
-        ++nr;
+        srr[nr] = cr > 0 ? cr : -1;
+        for (int b = 0; b < 4; ++b) srv[nr][b] = mk(0.0);
+        if (back) srv[nr][3] = -conj(mk((double)(float)coef));
+        snr = nr + 1;
     }
+    __syncthreads();
+    const int nr = snr;
     auto rhs = [&](int row, int b) {
         cd v = mk(0.0);
         for (int k = 0; k < nr; ++k)
-            if (rr[k] == row) v = rv[k][b];
+            if (srr[k] == row) v = srv[k][b];
         return v;
     };
-    // local row j <-> compact row j + it0 - 1
-    cd zprev[4];
-    for (int b = 0; b < 4; ++b) zprev[b] = rhs(it0, b);  // z(1) = b(1)
-    cd dprev = C[2 * it0 + 1];
-    for (int j = 2; j <= n; ++j) {
-        const int g = j + it0 - 1;
-        // factor step k = j-1: piv = 1/c(2,k); w2 = c(1,k+1) piv; c(2,k+1) += w2 (-c(1,k+1))
-        cd piv = mk(1.0) / dprev;
-        cd off = C[2 * g];
-        cd z2 = -off;
-        cd w2 = off * piv;
-        cd dg = C[2 * g + 1] + w2 * z2;
-        C[2 * g] = w2;
-        C[2 * g + 1] = dg;
-        // forward substitution: z(k) = z(k)/c(2,k), z(j) = b(j) - c(1,j) z(j-1)
-        for (int b = 0; b < 4; ++b) {
-            D[4 * (g - 1) + b] = zprev[b] / dprev;
-            zprev[b] = rhs(g, b) - w2 * zprev[b];
+    // forward: factor step k = g-1 (piv = 1/c(2,k); w2 = c(1,k+1) piv;
+    // c(2,k+1) += w2 (-c(1,k+1))), then z(k) = z(k)/c(2,k) and
+    // z(g) = b(g) - c(1,g) z(g-1) for each right-hand side
+    cd dfac = C[2 * it0 + 1];      // thread 0: running pivot
+    cd zb = mk(0.0), db = dfac;    // threads 0..3: z and pivot of the previous row
+    if (tid < 4) zb = rhs(it0, tid);
+    for (int g0 = it0 + 1; g0 <= n0; g0 += L0_CH) {
+        const int cnt = min(L0_CH, n0 + 1 - g0);
+        for (int i = tid; i < 2 * cnt; i += blockDim.x) sC[i >> 1][i & 1] = C[2 * g0 + i];
+        __syncthreads();
+        if (tid == 0) {
+            for (int i = 0; i < cnt; ++i) {
+                cd piv = mk(1.0) / dfac;
+                cd off = sC[i][0];
+                cd z2 = -off;
+                cd w2 = off * piv;
+                cd dg = sC[i][1] + w2 * z2;
+                sC[i][0] = w2;
+                sC[i][1] = dg;
+                dfac = dg;
+            }
         }
-        dprev = dg;
+        __syncthreads();
+        if (tid < 4) {
+            for (int i = 0; i < cnt; ++i) {
+                const int g = g0 + i;
+                D[4 * (g - 1) + tid] = zb / db;
+                zb = rhs(g, tid) - sC[i][0] * zb;
+                db = sC[i][1];
+            }
+        }
+        for (int i = tid; i < 2 * cnt; i += blockDim.x) C[2 * g0 + i] = sC[i >> 1][i & 1];
+        __syncthreads();
     }
-    for (int b = 0; b < 4; ++b) D[4 * n0 + b] = zprev[b] / dprev;
-    // upward substitution x(n-j) = z(n-j) - c(1,n-j+1) x(n-j+1)
-    cd x[4];
-    for (int b = 0; b < 4; ++b) x[b] = D[4 * n0 + b];
-    for (int j = n - 1; j >= 1; --j) {
-        const int g = j + it0 - 1;
-        cd L = C[2 * (g + 1)];
-        for (int b = 0; b < 4; ++b) {
-            x[b] = D[4 * g + b] - L * x[b];
-            D[4 * g + b] = x[b];
+    if (tid < 4) D[4 * n0 + tid] = zb / db;
+    __syncthreads();
+    // upward substitution x(g) = z(g) - c(1,g+1) x(g+1), g = n0-1 .. it0
+    cd x = mk(0.0);
+    if (tid < 4) x = D[4 * n0 + tid];
+    for (int ghi = n0 - 1; ghi >= it0; ghi -= L0_CH) {
+        const int glo = max(it0, ghi - L0_CH + 1), cnt = ghi - glo + 1;
+        for (int i = tid; i < cnt; i += blockDim.x) sC[i][0] = C[2 * (glo + i + 1)];
+        for (int i = tid; i < 4 * cnt; i += blockDim.x) sD[i >> 2][i & 3] = D[4 * glo + i];
+        __syncthreads();
+        if (tid < 4) {
+            for (int i = cnt - 1; i >= 0; --i) {
+                x = sD[i][tid] - sC[i][0] * x;
+                sD[i][tid] = x;
+            }
         }
+        __syncthreads();
+        for (int i = tid; i < 4 * cnt; i += blockDim.x) D[4 * glo + i] = sD[i >> 2][i & 3];
+        __syncthreads();
     }
 }
 
@@ -963,10 +996,12 @@ __global__ void k_psv_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ra
 }
 
 // ---------------------------------------------------------------- epilogue
+// TC: double (FP64 contraction) or float (tensor-core contraction)
+template <class TC>
 __global__ void k_psv_epi(PsvDev d, int w, const double* __restrict__ thx, const double* __restrict__ ths,
                           const int* __restrict__ pole, const int* __restrict__ freqs,
-                          const double* __restrict__ C0, const double* __restrict__ C1,
-                          const double* __restrict__ C2, double* __restrict__ tsgt,
+                          const TC* __restrict__ C0, const TC* __restrict__ C1,
+                          const TC* __restrict__ C2, double* __restrict__ tsgt,
                           double* __restrict__ rsgt, double* __restrict__ synn, int back) {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     const int R = d.R, Th = d.Th;
@@ -975,7 +1010,7 @@ __global__ void k_psv_epi(PsvDev d, int w, const double* __restrict__ thx, const
     const bool surf = r == R;
     const bool isp = pole[it] != 0;
     const int M[3] = {NS0 * (R + 1) * NFLD * 2, NS1 * (R + 1) * NFLD * 2, NS2 * (R + 1) * NFLD * 2};
-    const double* Cm[3] = {C0, C1, C2};
+    const TC* Cm[3] = {C0, C1, C2};
     const double x = thx[it], s = ths[it];
     const double fs = (double)(float)s, fc = (double)(float)(x / s);
     const double fr = surf ? 1.0 : d.fr[r];
@@ -1013,8 +1048,8 @@ __global__ void k_psv_epi(PsvDev d, int w, const double* __restrict__ thx, const
             auto G = [&](int f, int b) {
                 size_t row = ((size_t)(q * (R + 1) + r) * NFLD + f) * 2;
                 size_t col = (size_t)b * Th + it;
-                const double* C = Cm[mi];
-                return mk(C[row + (size_t)M[mi] * col], C[row + 1 + (size_t)M[mi] * col]);
+                const TC* C = Cm[mi];
+                return mk((double)C[row + (size_t)M[mi] * col], (double)C[row + 1 + (size_t)M[mi] * col]);
             };
             double sigma = (m < 0 && (mi & 1)) ? -1.0 : 1.0;
             double mm = (double)m, m2 = mm * mm;
@@ -1367,7 +1402,7 @@ class PsvEngine : public Engine {
             kbegin(id0, st2);
             k_psv_l0_build<<<dim3((d.nn0 + 127) / 128, nf), 128, 0, st2>>>(d, B0.p, B1.p, B2.p, l0col.p,
                                                                             l0e1.p, l0scr.p);
-            k_psv_l0_solve<<<(nf + 31) / 32, 32, 0, st2>>>(d, fr_, nf, ab.p, l0scr.p, l0d.p, rsgt_sw);
+            k_psv_l0_solve<<<nf, 128, 0, st2>>>(d, fr_, nf, ab.p, l0scr.p, l0d.p, rsgt_sw);
             k_psv_l0_fields<<<dim3((R + 1 + 127) / 128, nf), 128, 0, st2>>>(d, l0d.p, Afld[0].p, Afld[1].p,
                                                                              Afld[2].p, Lcap, rsgt_sw);
             kend(id0, 0.0, 0.0, st2);
@@ -1414,11 +1449,16 @@ class PsvEngine : public Engine {
         int n = Th * (R + 1);
         int id = kid("psv_epilogue");
         kbegin(id);
-        k_psv_epi<<<(n + 127) / 128, 128, 0, st>>>(d, w, th.x.p, th.s.p, th.pole.p, fr_,
-                                                   Cgemm.p + c_off(0), Cgemm.p + c_off(1),
-                                                   Cgemm.p + c_off(2), out_t.p,
-                                                   rsgt_sw ? out_r.p : nullptr,
-                                                   synn_sw ? out_s.p : nullptr, rsgt_sw);
+        if (mixed())
+            k_psv_epi<float><<<(n + 127) / 128, 128, 0, st>>>(d, w, th.x.p, th.s.p, th.pole.p, fr_, c32(w, 0),
+                                                              c32(w, 1), c32(w, 2), out_t.p,
+                                                              rsgt_sw ? out_r.p : nullptr,
+                                                              synn_sw ? out_s.p : nullptr, rsgt_sw);
+        else
+            k_psv_epi<double><<<(n + 127) / 128, 128, 0, st>>>(d, w, th.x.p, th.s.p, th.pole.p, fr_, c64(0),
+                                                               c64(1), c64(2), out_t.p,
+                                                               rsgt_sw ? out_r.p : nullptr,
+                                                               synn_sw ? out_s.p : nullptr, rsgt_sw);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
     }

@@ -387,10 +387,12 @@ __global__ void k_sh_scan(int nf, WorkList wl, int Lcap, int maxlmax, double rat
 
 // Epilogue of one frequency: thread per (itheta, receiver); receiver R is
 // the surface (SYNN).
+// TC: double (FP64 contraction) or float (tensor-core contraction)
+template <class TC>
 __global__ void k_sh_epi(ShDev d, int w, int Th, const double* __restrict__ thx,
                          const double* __restrict__ ths, const int* __restrict__ pole,
-                         const double* __restrict__ rr, const double* __restrict__ C1,
-                         const double* __restrict__ C2, double* __restrict__ tsgt,
+                         const double* __restrict__ rr, const TC* __restrict__ C1,
+                         const TC* __restrict__ C2, double* __restrict__ tsgt,
                          double* __restrict__ rsgt, double* __restrict__ synn) {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     const int R = d.R;
@@ -407,7 +409,7 @@ __global__ void k_sh_epi(ShDev d, int w, int Th, const double* __restrict__ thx,
         const double tc = x / s;  // thetacot = cos/sin
         const double ri = surf ? 1.0 : rr[r];
         for (int ma = 1; ma <= 2; ++ma) {
-            const double* C = ma == 1 ? C1 : C2;
+            const TC* C = ma == 1 ? C1 : C2;
             const int M = ma == 1 ? M1 : M2;
             const int nslot = ma == 1 ? SH_NSLOT1 : SH_NSLOT2;
             for (int q = 0; q < nslot; ++q) {
@@ -418,7 +420,7 @@ __global__ void k_sh_epi(ShDev d, int w, int Th, const double* __restrict__ thx,
                 auto G = [&](int f, int b) {
                     size_t row = ((size_t)(q * (R + 1) + r) * SH_NF + f) * 2;
                     size_t col = (size_t)b * Th + it;
-                    return mk(C[row + (size_t)M * col], C[row + 1 + (size_t)M * col]);
+                    return mk((double)C[row + (size_t)M * col], (double)C[row + 1 + (size_t)M * col]);
                 };
                 cd P = G(0, 0), D = G(0, 1);
                 double mm = (double)m, m2 = mm * mm;
@@ -669,9 +671,17 @@ class ShEngine : public Engine {
     void epilogue(const int* fr, int w, int nf) override {
         (void)fr; (void)nf;
         int n = Th * (R + 1);
-        k_sh_epi<<<(n + 127) / 128, 128, 0, st>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p,
-                                                  Cgemm.p + c_off(1), Cgemm.p + c_off(2), out_t.p,
-                                                  out_r.p, synn_sw ? out_s.p : nullptr);
+        int id = kid("sh_epilogue");
+        kbegin(id);
+        if (mixed())
+            k_sh_epi<float><<<(n + 127) / 128, 128, 0, st>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p, c32(w, 1),
+                                                             c32(w, 2), out_t.p, out_r.p,
+                                                             synn_sw ? out_s.p : nullptr);
+        else
+            k_sh_epi<double><<<(n + 127) / 128, 128, 0, st>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p, c64(1),
+                                                              c64(2), out_t.p, out_r.p,
+                                                              synn_sw ? out_s.p : nullptr);
+        kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
     }
 };

@@ -45,8 +45,10 @@ extern "C" {
 
 /* precision modes of a context */
 #define DSM_PREC_FP64        0  /* plain path: every stage in FP64            */
-#define DSM_PREC_MIXED       1  /* FP32 factors + FP64 refinement; split
-                                   16-bit tensor-core l-sum, FP32 accumulate  */
+#define DSM_PREC_MIXED       1  /* l-sum as split fp16 products (hi/lo of
+                                   both operands, three products) on the
+                                   tensor cores with FP32 accumulation      */
+#define DSM_PREC_MIXED_BF16  2  /* same with bf16 pieces                   */
 
 /* number of output components per point (src/SGTsh/modules.f90:371-373,
    src/SGTpsv/modules.f90:112-114) */
@@ -168,7 +170,7 @@ enum {
  * Context options and outputs
  * ---------------------------------------------------------------------- */
 typedef struct dsm_options {
-    int precision;        /* DSM_PREC_FP64 or DSM_PREC_MIXED                */
+    int precision;        /* DSM_PREC_FP64, DSM_PREC_MIXED(_BF16)           */
     int device;           /* CUDA device ordinal                             */
     int use_lmax_predictor;/* 1: size l batches with the learned cutoff      */
     int l_chunk;          /* orders solved speculatively per batch (0: auto) */

@@ -1,0 +1,53 @@
+"""Mixed-precision path (split 16-bit tensor-core l-sum with FP32
+accumulation) against the plain FP64 GPU path on the same inputs.
+
+Target: relative L2 <= 1e-6 per output component with fp16 pieces; the
+realised cutoff is the plain method's (the solves are unchanged).  bf16
+pieces carry ~16 significant bits and are held to a looser bound."""
+import numpy as np
+import pytest
+
+import dsmsgt
+from cases import psv_small, sh_small
+from conftest import rel_l2
+
+TOL_F16 = 1e-6
+TOL_BF16 = 1e-4
+
+
+def per_component(a, b):
+    """rel-L2 of each output component over frequencies, radii, distances."""
+    return [rel_l2(a[..., c], b[..., c]) for c in range(a.shape[-1])]
+
+
+def _mixed_vs_fp64(setup, freqs, prec):
+    c64 = dsmsgt.Context(setup, precision=dsmsgt.DSM_PREC_FP64)
+    t, r, y, llog = c64.run(freqs)
+    c64.close()
+    cm = dsmsgt.Context(setup, precision=prec)
+    tm, rm, ym, llogm = cm.run(freqs)
+    cm.close()
+    assert list(llog) == list(llogm)
+    assert np.all(np.isfinite(tm)) and np.all(np.isfinite(rm))
+    errs = {"tsgt": per_component(tm, t), "rsgt": per_component(rm, r), "synn": per_component(ym, y)}
+    return errs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [(dsmsgt.DSM_PREC_MIXED, TOL_F16), (dsmsgt.DSM_PREC_MIXED_BF16, TOL_BF16)])
+def test_sh_mixed_close_to_fp64(built, prec, tol):
+    s = dsmsgt.Setup(sh_small(), "sh")
+    errs = _mixed_vs_fp64(s, [1, 7, 16, 31], prec)
+    print(prec, {k: max(v) for k, v in errs.items()})
+    for k, v in errs.items():
+        assert max(v) <= tol, (k, v)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [(dsmsgt.DSM_PREC_MIXED, TOL_F16), (dsmsgt.DSM_PREC_MIXED_BF16, TOL_BF16)])
+def test_psv_mixed_close_to_fp64(built, prec, tol):
+    s = dsmsgt.Setup(psv_small(), "psv")
+    errs = _mixed_vs_fp64(s, [1, 17, 50], prec)
+    print(prec, {k: max(v) for k, v in errs.items()})
+    for k, v in errs.items():
+        assert max(v) <= tol, (k, v)

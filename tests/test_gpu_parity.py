@@ -28,6 +28,27 @@ def _compare(setup, freqs, ctx_kwargs=None, tol=TOL_FP64):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["sh_small_seed0", "psv_small_seed0", "psv_deep_seed1"])
+def test_fp64_matches_golden(built, name):
+    """The FP64 engine against the committed oracle fixtures."""
+    import os
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    import make_golden
+    import cases
+    mode, fn, kw, freqs = make_golden.CASES[name]
+    g = np.load(os.path.join(here, "golden", name + ".npz"))
+    s = dsmsgt.Setup(getattr(cases, fn)(**kw), mode)
+    ctx = dsmsgt.Context(s)
+    t, r, y, llog = ctx.run(freqs)
+    ctx.close()
+    assert list(llog) == list(g["llog"])
+    for k, v in (("tsgt", t), ("rsgt", r), ("synn", y)):
+        assert rel_l2(v, g[k]) <= TOL_FP64, k
+
+
+@pytest.mark.gpu
 def test_sh_fp64_matches_oracle(built):
     s = dsmsgt.Setup(sh_small(), "sh")
     errs = _compare(s, [1, 7, 16, 31])
