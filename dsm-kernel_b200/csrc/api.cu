@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "engine.cuh"
@@ -42,6 +43,10 @@ void Engine::init_common(int dev) {
     if (opt.precision != DSM_PREC_FP64 && !mixed())
         throw Error(DSM_ERR_INVALID, "unknown precision mode " + std::to_string(opt.precision));
     tc_fmt = opt.precision == DSM_PREC_MIXED_BF16 ? tc::PIECE_BF16 : tc::PIECE_F16;
+    // tuning knobs of the tensor-core contraction (stage depth, accumulation
+    // order and split), overridable for measurements
+    if (const char* e = std::getenv("DSM_TC_FLAGS")) tc_flags = (uint32_t)std::atoi(e);
+    if (const char* e = std::getenv("DSM_TC_BK")) tc_bk = std::atoi(e) == 64 ? 64 : 32;
     if (mixed()) {
         tc_err.reserve(1);
         DSM_CUDA(cudaMemset(tc_err.p, 0, sizeof(int)));
@@ -210,7 +215,7 @@ void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
             tiles += ((hp[g + i].M + tc::BM - 1) / tc::BM) * tn;
         }
         DSM_CUDA(cudaMemcpyAsync(tcp.p + g, hp.data() + g, sizeof(tc::Problem) * np, cudaMemcpyHostToDevice, st));
-        tc::launch(maps, tcp.p + g, np, tiles, tc_fmt, tc_bk, tc_err.p, nsm, st);
+        tc::launch(maps, tcp.p + g, np, tiles, tc_fmt, tc_bk, tc_flags, tc_err.p, nsm, st);
         launches++;
     }
     kend(id, tc_bytes, tflops);

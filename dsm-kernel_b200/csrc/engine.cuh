@@ -106,6 +106,7 @@ class Engine {
     // cores (fields and bases split once per batch / per table build)
     bool mixed() const { return opt.precision == DSM_PREC_MIXED || opt.precision == DSM_PREC_MIXED_BF16; }
     int tc_fmt = tc::PIECE_F16, tc_bk = 32, nsm = 148;
+    uint32_t tc_flags = tc::TC_REVERSE | tc::TC_SPLIT_ACC;
     int kcA = 0, kcB = 0;            // order capacities of the pieces (x64)
     DBuf<uint16_t> Apc[3];           // [2][F][rows][kcA]
     DBuf<float> sA[3];               // [F][rows]

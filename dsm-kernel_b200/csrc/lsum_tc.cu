@@ -10,8 +10,14 @@
 //   warps 2..5  epilogue: tcgen05.ld of the accumulator (each warp its
 //               32-lane quarter), row x column scaling, coalesced stores of
 //               the column-major output (consecutive lanes = consecutive rows)
-// Two accumulators (2 x 256 columns, all of tensor memory) let the epilogue
-// of one tile overlap the MMAs of the next.  Every wait is bounded: after
+// Tensor memory (512 columns) holds either two tiles' accumulators, so that
+// the epilogue of one tile overlaps the MMAs of the next, or (TC_SPLIT_ACC)
+// one tile with the hi*hi products and the two cross products in separate
+// accumulators: the tensor-core FP32 accumulation rounds each step relative
+// to the accumulator's magnitude, so keeping the cross terms (2^-11 smaller)
+// out of the hi*hi accumulator cuts the steps that accumulator takes by
+// three.  TC_REVERSE runs the orders from high to low, so that the small
+// high-order terms are added while the accumulator is still small.  Every wait is bounded: after
 // about a second a role raises the CTA's abort flag, all roles leave their
 // loops, the issued copies and MMAs are waited for (again bounded), the
 // tensor memory is freed and the error word is set for the host.
@@ -149,7 +155,7 @@ __device__ __forceinline__ void decode(const Problem* ps, int np, int t, int& p,
 template <int BK>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_lsum_tc(const __grid_constant__ Maps maps, const Problem* __restrict__ probs, int np, int ntiles,
-              uint32_t idesc, int* __restrict__ err) {
+              uint32_t idesc, uint32_t flags, int* __restrict__ err) {
     constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
     constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
     constexpr int STAGES = (4 * 48 * 1024) / STAGE;
@@ -160,6 +166,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     __shared__ Problem ps[MAXP];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool reverse = (flags & TC_REVERSE) != 0, split = (flags & TC_SPLIT_ACC) != 0;
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
     volatile int* abort_flag = &abort_sh;
@@ -207,11 +214,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         break;
                     }
                     unsigned char* sp = base + s * STAGE;
+                    const int x = (reverse ? P.kblocks - 1 - kb : kb) * BK;
                     mbar_expect_tx(&full[s], STAGE);
-                    tma_a(&maps.a[P.amap], sp, &full[s], kb * BK, mt * BM, P.z, 0);
-                    tma_a(&maps.a[P.amap], sp + A_BYTES, &full[s], kb * BK, mt * BM, P.z, 1);
-                    tma_b(&maps.b[P.bmap], sp + 2 * A_BYTES, &full[s], kb * BK, nt * BN, 0);
-                    tma_b(&maps.b[P.bmap], sp + 2 * A_BYTES + B_BYTES, &full[s], kb * BK, nt * BN, 1);
+                    tma_a(&maps.a[P.amap], sp, &full[s], x, mt * BM, P.z, 0);
+                    tma_a(&maps.a[P.amap], sp + A_BYTES, &full[s], x, mt * BM, P.z, 1);
+                    tma_b(&maps.b[P.bmap], sp + 2 * A_BYTES, &full[s], x, nt * BN, 0);
+                    tma_b(&maps.b[P.bmap], sp + 2 * A_BYTES + B_BYTES, &full[s], x, nt * BN, 1);
                 }
             }
             // every issued copy has landed before the CTA may exit
@@ -227,10 +235,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tcnt) {
                 int p, mt, nt;
                 decode(ps, np, t, p, mt, nt);
-                const int b = tcnt & 1;
-                if (!mbar_wait(&tempty[b], ((tcnt >> 1) & 1) ^ 1, abort_flag)) break;
+                // split: hi*hi in columns [0, BN), the cross terms in [BN, 2BN),
+                // one tile in flight; otherwise two tiles double-buffered
+                const int b = split ? 0 : (tcnt & 1);
+                const uint32_t par = split ? (tcnt & 1) : ((tcnt >> 1) & 1);
+                if (!mbar_wait(&tempty[b], par ^ 1, abort_flag)) break;
                 tc_fence_after();
                 const uint32_t d = tmem + (uint32_t)(b * BN);
+                const uint32_t dx = split ? tmem + (uint32_t)BN : d;
                 const int kbn = ps[p].kblocks;
                 for (int kb = 0; kb < kbn; ++kb, ++it) {
                     const int s = it % STAGES;
@@ -244,9 +256,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
                     for (int j = 0; j < BK / 16; ++j) {
                         const uint32_t o = 32u * j;
-                        mma_f16(d, sdesc<BK>(ah + o), sdesc<BK>(bh + o), idesc, (kb | j) != 0);
-                        mma_f16(d, sdesc<BK>(ah + o), sdesc<BK>(bl + o), idesc, 1);
-                        mma_f16(d, sdesc<BK>(al + o), sdesc<BK>(bh + o), idesc, 1);
+                        const uint32_t first = (kb | j) == 0 ? 0u : 1u;
+                        mma_f16(d, sdesc<BK>(ah + o), sdesc<BK>(bh + o), idesc, first);
+                        mma_f16(dx, sdesc<BK>(ah + o), sdesc<BK>(bl + o), idesc, split ? first : 1u);
+                        mma_f16(dx, sdesc<BK>(al + o), sdesc<BK>(bh + o), idesc, 1);
                     }
                     mma_commit(&empty[s]);
                 }
@@ -262,8 +275,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcnt) {
             int p, mt, nt;
             decode(ps, np, t, p, mt, nt);
-            const int b = tcnt & 1;
-            const bool got = mbar_wait(&tfull[b], (tcnt >> 1) & 1, abort_flag);
+            const int b = split ? 0 : (tcnt & 1);
+            const uint32_t par = split ? (tcnt & 1) : ((tcnt >> 1) & 1);
+            const bool got = mbar_wait(&tfull[b], par, abort_flag);
             if (!__all_sync(0xffffffffu, got)) break;
             tc_fence_after();
             const Problem& P = ps[p];
@@ -274,13 +288,22 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll 1
             for (int c0 = 0; c0 < BN; c0 += 32) {
                 uint32_t r[32];
-                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + c0), r);
+                float v[32];
+                const uint32_t lanes = (uint32_t)(q * 32) << 16;
+                tmem_ld32(tmem + lanes + (uint32_t)(b * BN + c0), r);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+                if (split) {
+                    tmem_ld32(tmem + lanes + (uint32_t)(BN + c0), r);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] += __uint_as_float(r[j]);
+                }
                 const int n0 = nt * BN + c0;
                 if (mv) {
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
                         const int n = n0 + j;
-                        if (n < P.N) Cm[(long long)n * P.ldc] = __uint_as_float(r[j]) * rs * P.sb[n];
+                        if (n < P.N) Cm[(long long)n * P.ldc] = v[j] * rs * P.sb[n];
                     }
                 }
             }
@@ -416,8 +439,8 @@ void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, in
     DSM_CUDA(cudaGetLastError());
 }
 
-void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int piece_fmt, int bk, int* d_err,
-            int nsm, cudaStream_t st) {
+void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int piece_fmt, int bk, uint32_t flags,
+            int* d_err, int nsm, cudaStream_t st) {
     if (np <= 0 || ntiles <= 0) return;
     if (np > MAXP) throw Error(DSM_ERR_INVALID, "too many contractions in one launch");
     // kind::f16 instruction descriptor: FP32 accumulator, both operands of
@@ -433,14 +456,14 @@ void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int pi
             DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr32 = true;
         }
-        k_lsum_tc<32><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, d_err);
+        k_lsum_tc<32><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, d_err);
     } else if (bk == 64) {
         static bool attr64 = false;
         if (!attr64) {
             DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr64 = true;
         }
-        k_lsum_tc<64><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, d_err);
+        k_lsum_tc<64><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, d_err);
     } else {
         throw Error(DSM_ERR_INVALID, "BK must be 32 or 64");
     }

@@ -22,6 +22,8 @@ constexpr int BN = 256;          // columns of a tile (tensor-memory columns)
 constexpr int MAXP = 96;         // problems per launch
 constexpr int PIECE_F16 = 0;     // fp16 pieces (11-bit significand each)
 constexpr int PIECE_BF16 = 1;    // bf16 pieces (8-bit significand each)
+constexpr uint32_t TC_REVERSE = 1;    // orders summed from high to low
+constexpr uint32_t TC_SPLIT_ACC = 2;  // hi*hi and cross products in separate accumulators
 
 // One contraction of a launch.  Rows of A beyond M and columns beyond N are
 // read as zeros by the tensor-map bounds and never stored.
@@ -58,7 +60,7 @@ void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, in
 
 // Launches the persistent contraction over all tiles of probs[0..np).
 // err (device int) is set nonzero if a bounded wait inside gave up.
-void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int piece_fmt, int bk,
+void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int piece_fmt, int bk, uint32_t flags,
             int* d_err, int nsm, cudaStream_t st);
 
 }  // namespace tc

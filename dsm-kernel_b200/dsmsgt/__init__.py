@@ -144,20 +144,21 @@ def lib() -> C.CDLL:
         L.dsm_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.dsm_set_profiling.argtypes = [C.c_void_p, C.c_int]
         L.dsm_sh_cutoff_noalloc.argtypes = [C.POINTER(ShSetup), _ip, C.c_int, _ip]
-        L.dsm_tc_selftest.argtypes = [C.c_int] * 8 + [C.POINTER(C.c_double)]
+        L.dsm_tc_selftest.argtypes = [C.c_int] * 9 + [C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
 
 def tc_selftest(M: int, N: int, K: int, nfreq: int = 1, fmt: int = 0, bk: int = 32, reps: int = 0,
-                check: bool = True) -> dict:
+                check: bool = True, flags: int = 3) -> dict:
     """Runs the tensor-core split contraction on seeded pieces (fmt 0 fp16,
     1 bf16) and, with check, compares it with an FP64 sum of the same piece
-    products.  Returns max |error|, max |reference|, ms per launch and the
-    tensor flops of one launch."""
+    products.  flags: 1 high-to-low order, 2 separate hi*hi accumulator.
+    Returns max |error|, max |reference|, ms per launch and the tensor
+    flops of one launch."""
     L = lib()
     res = (C.c_double * 4)()
-    rc = L.dsm_tc_selftest(M, N, K, nfreq, fmt, bk, reps, int(check), res)
+    rc = L.dsm_tc_selftest(M, N, K, nfreq, fmt, bk, flags, reps, int(check), res)
     if rc:
         raise DsmError(f"dsm_tc_selftest failed ({rc}): {L.dsm_last_error(None).decode()}")
     return {"max_err": res[0], "ref_max": res[1], "ms": res[2], "flops": res[3]}
