@@ -47,6 +47,7 @@ void Engine::init_common(int dev) {
     // order and split), overridable for measurements
     if (const char* e = std::getenv("DSM_TC_FLAGS")) tc_flags = (uint32_t)std::atoi(e);
     if (const char* e = std::getenv("DSM_TC_BK")) tc_bk = std::atoi(e) == 64 ? 64 : 32;
+    if (const char* e = std::getenv("DSM_TC_CHUNK")) tc_chunk = std::max(0, std::atoi(e));
     if (mixed()) {
         tc_err.reserve(1);
         DSM_CUDA(cudaMemset(tc_err.p, 0, sizeof(int)));
@@ -215,7 +216,7 @@ void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
             tiles += ((hp[g + i].M + tc::BM - 1) / tc::BM) * tn;
         }
         DSM_CUDA(cudaMemcpyAsync(tcp.p + g, hp.data() + g, sizeof(tc::Problem) * np, cudaMemcpyHostToDevice, st));
-        tc::launch(maps, tcp.p + g, np, tiles, tc_fmt, tc_bk, tc_flags, tc_err.p, nsm, st);
+        tc::launch(maps, tcp.p + g, np, tiles, tc_fmt, tc_bk, tc_flags, tc_chunk, tc_err.p, nsm, st);
         launches++;
     }
     kend(id, tc_bytes, tflops);
@@ -290,6 +291,45 @@ void Engine::grow_orders(int need) {
 
 // First order range of a frequency: past lsuf (callsuf), at least 512
 // (or the fixed chunk the options ask for).
+void Engine::set_summaries(int is_psv, int nzone, const double* vrmin, const double* vrmax, const double* vsv,
+                           const double* qmu, double r0, double rrcv) {
+    const double rmax = vrmax[nzone - 1];
+    auto vs_at = [&](int z, double r) {
+        const double x = r / rmax;
+        return vsv[4 * z] + vsv[4 * z + 1] * x + vsv[4 * z + 2] * x * x + vsv[4 * z + 3] * x * x * x;
+    };
+    int zs = nzone - 1;
+    for (int z = 0; z < nzone; ++z)
+        if (r0 >= vrmin[z] && r0 <= vrmax[z]) { zs = z; break; }
+    double vmin = 1e30, vmax = 0.0;
+    for (int z = 0; z < nzone; ++z) {
+        const double v = vs_at(z, 0.5 * (vrmin[z] + vrmax[z]));
+        if (v <= 0.0) continue;  // fluid zone
+        vmin = std::min(vmin, v);
+        vmax = std::max(vmax, v);
+    }
+    if (vmax == 0.0) vmin = 0.0;
+    summ[0] = (float)(r0 / rmax);
+    summ[1] = (float)(rrcv / rmax);
+    summ[2] = (float)(vtop_ / 10.0);
+    summ[3] = (float)(vs_at(zs, r0) / 10.0);
+    summ[4] = (float)(vmin / 10.0);
+    summ[5] = (float)(vmax / 10.0);
+    summ[6] = (float)((rmax - r0) / 1000.0);
+    summ[7] = (float)((vrmax[nzone - 1] - vrmin[nzone - 1]) / 100.0);
+    summ[8] = (float)is_psv;
+    summ[9] = (float)(std::log10(std::max(1.0, std::fabs(qmu[zs]))) / 3.0);
+}
+
+void Engine::lmax_features(const int* ilist, int n, float* out) const {
+    for (int k = 0; k < n; ++k) {
+        const double omega = 2.0 * kPi * (double)ilist[k] / tlen;
+        float* f = out + (size_t)k * DSM_LMAX_NFEAT;
+        f[0] = (float)std::log1p(omega * rtop_ / vtop_);
+        for (int i = 0; i < 10; ++i) f[1 + i] = summ[i];
+    }
+}
+
 int Engine::first_span(int ifreq) const {
     if (opt.l_chunk > 0) return ((opt.l_chunk + 31) / 32) * 32;
     double omega = 2.0 * kPi * (double)ifreq / tlen;
@@ -306,6 +346,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
     if (dt && n > F) throw Error(DSM_ERR_INVALID, "device outputs hold at most one batch of frequencies");
     std::memset(&stats, 0, sizeof(stats));
     launches = 0;
+    rounds = 0;
     recs.clear();
     cudaEvent_t e0 = ev[0], e1 = ev[1], es0 = ev[2], es1 = ev[3], eg0 = ev[4], eg1 = ev[5];
     DSM_CUDA(cudaEventRecord(e0, st));
@@ -331,6 +372,21 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
         std::vector<int> next(nf, 0), span(nf, 0);
         std::vector<int> hf(ilist + b0, ilist + b0 + nf);
         for (int w = 0; w < nf; ++w) span[w] = first_span(hf[w]);
+        if (opt.use_lmax_predictor && pred.ready && opt.l_chunk <= 0) {
+            // the learned cutoff with a 5% margin; never below lsuf, where
+            // the amplitude test cannot yet stop
+            std::vector<float> f((size_t)nf * DSM_LMAX_NFEAT), lp(nf);
+            lmax_features(hf.data(), nf, f.data());
+            pred.predict(f.data(), nf, lp.data(), st);
+            for (int w = 0; w < nf; ++w) {
+                const double omega = 2.0 * kPi * (double)hf[w] / tlen;
+                const int lsuf = (int)(omega * rtop_ / vtop_ - 0.5) + 1;
+                const double pl = std::exp((double)lp[w]);
+                int sp = (int)std::ceil(std::min(pl * 1.05 + 16.0, (double)maxlmax + 1.0));
+                sp = std::max(sp, lsuf + 32);
+                span[w] = (sp + 31) / 32 * 32;
+            }
+        }
         int maxend = 0;
         for (;;) {
             std::vector<int> off(nf + 1, 0), lb(nf, 0);
@@ -356,6 +412,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             solve_chunk(d_freqs.p, nf, wl, tot);
             scan_chunk(nf, wl);
             stats.systems += tot;
+            rounds++;
             DSM_CUDA(cudaMemcpyAsync(hc.data(), cut.p, sizeof(CutState) * nf, cudaMemcpyDeviceToHost, st));
             DSM_CUDA(cudaStreamSynchronize(st));
             bool all = true;
@@ -372,6 +429,18 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
         }
         join_side();
         DSM_CUDA(cudaEventRecord(es1, st));
+        if (cutoffs_only) {  // the realised cutoffs are all that was asked for
+            for (int w = 0; w < nf; ++w) {
+                if (llog_out) llog_out[b0 + w] = hc[w].llog;
+                stats.orders_used += hc[w].norders;
+            }
+            DSM_CUDA(cudaStreamSynchronize(st));
+            kcollect();
+            float a = 0;
+            cudaEventElapsedTime(&a, es0, es1);
+            ms_solve += a;
+            continue;
+        }
         // --- 3+4: contraction and epilogue per frequency
         int lneed = 1;
         for (auto& c : hc) lneed = std::max(lneed, c.norders);
@@ -565,6 +634,68 @@ extern "C" int dsm_run_freqs_device(dsm_ctx_t* ctx, const int* ilist, int n, con
     return guarded(ctx, [&] {
         DSM_CUDA(cudaSetDevice(ctx->eng->opt.device));
         ctx->eng->run(ilist, n, nullptr, d_tsgt, d_rsgt, d_synn, llog);
+    });
+}
+
+extern "C" int dsm_lmax_features(const dsm_ctx_t* ctx, const int* ilist, int n, float* feats) {
+    if (!ctx || !ilist || !feats || n <= 0) return DSM_ERR_INVALID;
+    ctx->eng->lmax_features(ilist, n, feats);
+    return DSM_OK;
+}
+
+extern "C" int dsm_cutoffs(dsm_ctx_t* ctx, const int* ilist, int n, int* llog) {
+    if (!ctx || !ilist || !llog) return DSM_ERR_INVALID;
+    return guarded(ctx, [&] {
+        DSM_CUDA(cudaSetDevice(ctx->eng->opt.device));
+        ctx->eng->cutoffs_only = true;
+        try {
+            ctx->eng->run(ilist, n, nullptr, nullptr, nullptr, nullptr, llog);
+        } catch (...) {
+            ctx->eng->cutoffs_only = false;
+            throw;
+        }
+        ctx->eng->cutoffs_only = false;
+    });
+}
+
+extern "C" int dsm_lmax_init(const float* feats, const float* target, int n, unsigned seed, float* params) {
+    if (!feats || !target || !params || n <= 0) return DSM_ERR_INVALID;
+    return guarded(nullptr, [&] { dsm::lmax::init_params(feats, target, n, seed, params); });
+}
+
+extern "C" int dsm_lmax_train(const float* feats, const float* target, int n, int epochs, int batch, float lr,
+                              unsigned seed, float* params, float* losses, int device) {
+    if (!feats || !target || !params || n <= 0) return DSM_ERR_INVALID;
+    int rc = check_device(device);
+    if (rc) return rc;
+    return guarded(nullptr, [&] {
+        dsm::lmax::train(feats, target, n, epochs, batch, lr, seed, params, losses, device);
+    });
+}
+
+extern "C" int dsm_lmax_grad(const float* params, const float* feats, const float* target, int n, float* grad,
+                             float* loss, int device) {
+    if (!feats || !target || !params || !grad || !loss || n <= 0) return DSM_ERR_INVALID;
+    int rc = check_device(device);
+    if (rc) return rc;
+    return guarded(nullptr, [&] { dsm::lmax::grad(params, feats, target, n, grad, loss, device); });
+}
+
+extern "C" int dsm_set_lmax_model(dsm_ctx_t* ctx, const float* params) {
+    if (!ctx || !params) return DSM_ERR_INVALID;
+    return guarded(ctx, [&] {
+        DSM_CUDA(cudaSetDevice(ctx->eng->opt.device));
+        ctx->eng->pred.load(params, ctx->eng->st);
+    });
+}
+
+extern "C" int dsm_lmax_predict(dsm_ctx_t* ctx, const int* ilist, int n, float* out) {
+    if (!ctx || !ilist || !out || n <= 0) return DSM_ERR_INVALID;
+    return guarded(ctx, [&] {
+        DSM_CUDA(cudaSetDevice(ctx->eng->opt.device));
+        std::vector<float> f((size_t)n * DSM_LMAX_NFEAT);
+        ctx->eng->lmax_features(ilist, n, f.data());
+        ctx->eng->pred.predict(f.data(), n, out, ctx->eng->st);
     });
 }
 

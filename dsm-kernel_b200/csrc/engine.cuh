@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "lmax.cuh"
 #include "lsum_tc.cuh"
 
 namespace dsm {
@@ -106,7 +107,8 @@ class Engine {
     // cores (fields and bases split once per batch / per table build)
     bool mixed() const { return opt.precision == DSM_PREC_MIXED || opt.precision == DSM_PREC_MIXED_BF16; }
     int tc_fmt = tc::PIECE_F16, tc_bk = 32, nsm = 148;
-    uint32_t tc_flags = tc::TC_REVERSE | tc::TC_SPLIT_ACC;
+    uint32_t tc_flags = tc::TC_REVERSE;
+    int tc_chunk = tc::TC_CHUNK;
     int kcA = 0, kcB = 0;            // order capacities of the pieces (x64)
     DBuf<uint16_t> Apc[3];           // [2][F][rows][kcA]
     DBuf<float> sA[3];               // [F][rows]
@@ -144,6 +146,16 @@ class Engine {
     DBuf<int> wl_off, wl_lb;
     virtual void epilogue(const int* freqs_dev, int w, int nf) = 0;
     virtual size_t out_sizes(size_t* nt, size_t* nr, size_t* ns) const = 0;
+
+    // learned cutoff: per-context model summaries, the device network, and
+    // the cutoff-only mode used to harvest training data
+    float summ[10] = {};             // r_src/rmax, r_rcv/rmax, 8 model summaries
+    lmax::Predictor pred;
+    bool cutoffs_only = false;
+    void set_summaries(int is_psv, int nzone, const double* vrmin, const double* vrmax, const double* vsv,
+                       const double* qmu, double r0, double rrcv);
+    void lmax_features(const int* ilist, int n, float* out) const;
+    long long rounds = 0;            // solve rounds of the last run
 
     // drivers
     void run(const int* ilist, int n, dsm_out_t* host_out, const void** dt, const void** dr,

@@ -2,25 +2,26 @@
 //
 // Persistent, warp-specialised kernel, one CTA per SM:
 //   warp 0      TMA producer: per stage, the hi and lo pieces of a 128 x BK
-//               A tile and of a 256 x BK B tile (four bulk tensor loads,
+//               A tile and of a 128 x BK B tile (four bulk tensor loads,
 //               one mbarrier with the byte count)
 //   warp 1      MMA issuer: per stage and 16-order step, three
-//               tcgen05.mma (hi*hi, hi*lo, lo*hi) into a 128 x 256 FP32
-//               accumulator in tensor memory; tcgen05.commit frees the stage
-//   warps 2..5  epilogue: tcgen05.ld of the accumulator (each warp its
-//               32-lane quarter), row x column scaling, coalesced stores of
-//               the column-major output (consecutive lanes = consecutive rows)
-// Tensor memory (512 columns) holds either two tiles' accumulators, so that
-// the epilogue of one tile overlaps the MMAs of the next, or (TC_SPLIT_ACC)
-// one tile with the hi*hi products and the two cross products in separate
-// accumulators: the tensor-core FP32 accumulation rounds each step relative
-// to the accumulator's magnitude, so keeping the cross terms (2^-11 smaller)
-// out of the hi*hi accumulator cuts the steps that accumulator takes by
-// three.  TC_REVERSE runs the orders from high to low, so that the small
-// high-order terms are added while the accumulator is still small.  Every wait is bounded: after
-// about a second a role raises the CTA's abort flag, all roles leave their
-// loops, the issued copies and MMAs are waited for (again bounded), the
-// tensor memory is freed and the error word is set for the host.
+//               tcgen05.mma: hi*hi into a chunk accumulator, hi*lo and
+//               lo*hi into the tile's cross-term accumulator; tcgen05.commit
+//               frees the stage and hands finished accumulators over
+//   warps 2..9  epilogue: tcgen05.ld of the accumulators (two warps per
+//               32-lane quarter, 64 columns each), FP64 sum of the hi*hi
+//               chunks, row x column scaling, coalesced column-major stores
+// Accuracy: the tensor cores add each step into the FP32 accumulator with a
+// rounding relative to the accumulator's magnitude, so a long order sum
+// loses bits in proportion to its length.  The hi*hi products therefore go
+// into short chunks (chunk stages of BK orders) whose partial sums the
+// epilogue adds in FP64, and the cross terms (2^-11 smaller) get their own
+// accumulator.  Tensor memory (512 columns): three hi*hi chunk buffers of
+// 128 columns, so the epilogue drains one while the MMAs fill the next, and
+// the tile's cross-term accumulator (freed as soon as it is read).  TC_REVERSE runs the orders from high to low.
+// Every wait is bounded: after about a second a role raises the CTA's abort
+// flag, all roles leave their loops, the issued copies and MMAs are waited
+// for (again bounded), the tensor memory is freed and the error word is set.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -36,8 +37,11 @@ namespace tc {
 
 namespace {
 
-constexpr int NTHREADS = 192;
+constexpr int EPI_THREADS = 256;                 // warps 2..9
+constexpr int NTHREADS = 64 + EPI_THREADS;
 constexpr uint32_t TMEM_COLS = 512;
+constexpr int SMEM_STAGES = 192 * 1024;         // operand stages
+constexpr int NHB = 3;                          // hi*hi chunk buffers in tensor memory
 constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;  // 1 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -155,18 +159,18 @@ __device__ __forceinline__ void decode(const Problem* ps, int np, int t, int& p,
 template <int BK>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_lsum_tc(const __grid_constant__ Maps maps, const Problem* __restrict__ probs, int np, int ntiles,
-              uint32_t idesc, uint32_t flags, int* __restrict__ err) {
+              uint32_t idesc, uint32_t flags, int chunk, int* __restrict__ err) {
     constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
     constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
-    constexpr int STAGES = (4 * 48 * 1024) / STAGE;
+    constexpr int STAGES = SMEM_STAGES / STAGE;
     extern __shared__ unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], tfull[2], tempty[2], fin;
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], hfull[NHB], hempty[NHB], xfull, xempty, fin;
     __shared__ uint32_t tmem_sh;
     __shared__ int abort_sh;
     __shared__ Problem ps[MAXP];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool reverse = (flags & TC_REVERSE) != 0, split = (flags & TC_SPLIT_ACC) != 0;
+    const bool reverse = (flags & TC_REVERSE) != 0;
     unsigned char* base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
     volatile int* abort_flag = &abort_sh;
@@ -178,10 +182,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 128);
+        for (int b = 0; b < NHB; ++b) {
+            mbar_init(&hfull[b], 1);
+            mbar_init(&hempty[b], EPI_THREADS);
         }
+        mbar_init(&xfull, 1);
+        mbar_init(&xempty, EPI_THREADS);
         mbar_init(&fin, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.a[0])) : "memory");
@@ -197,6 +203,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_sh;
+    // tensor memory: hi*hi chunk accumulators hh[0..NHB) at columns
+    // [0, NHB BN), the tile's cross-term accumulator x at [NHB BN, 4 BN)
 
     if (warp == 0) {
         if (lane == 0) {  // ---------------------------------------- producer
@@ -230,21 +238,28 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {  // ---------------------------------------- MMA issuer
-            int it = 0, tcnt = 0;
+            int it = 0, tcnt = 0, cc = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tcnt) {
                 int p, mt, nt;
                 decode(ps, np, t, p, mt, nt);
-                // split: hi*hi in columns [0, BN), the cross terms in [BN, 2BN),
-                // one tile in flight; otherwise two tiles double-buffered
-                const int b = split ? 0 : (tcnt & 1);
-                const uint32_t par = split ? (tcnt & 1) : ((tcnt >> 1) & 1);
-                if (!mbar_wait(&tempty[b], par ^ 1, abort_flag)) break;
+                const int kbn = ps[p].kblocks, ch = chunk > 0 ? chunk : kbn;
+                if (!mbar_wait(&xempty, (tcnt & 1) ^ 1, abort_flag)) break;
                 tc_fence_after();
-                const uint32_t d = tmem + (uint32_t)(b * BN);
-                const uint32_t dx = split ? tmem + (uint32_t)BN : d;
-                const int kbn = ps[p].kblocks;
+                const uint32_t dx = tmem + (uint32_t)(NHB * BN);
+                uint32_t dh = tmem;
+                int hb = 0;
                 for (int kb = 0; kb < kbn; ++kb, ++it) {
+                    const bool cfirst = kb % ch == 0;
+                    if (cfirst) {
+                        hb = cc % NHB;
+                        if (!mbar_wait(&hempty[hb], ((cc / NHB) & 1) ^ 1, abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        dh = tmem + (uint32_t)(hb * BN);
+                    }
                     const int s = it % STAGES;
                     if (!mbar_wait(&full[s], (it / STAGES) & 1, abort_flag)) {
                         ok = false;
@@ -256,59 +271,87 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
                     for (int j = 0; j < BK / 16; ++j) {
                         const uint32_t o = 32u * j;
-                        const uint32_t first = (kb | j) == 0 ? 0u : 1u;
-                        mma_f16(d, sdesc<BK>(ah + o), sdesc<BK>(bh + o), idesc, first);
-                        mma_f16(dx, sdesc<BK>(ah + o), sdesc<BK>(bl + o), idesc, split ? first : 1u);
-                        mma_f16(dx, sdesc<BK>(al + o), sdesc<BK>(bh + o), idesc, 1);
+                        mma_f16(dh, sdesc<BK>(ah + o), sdesc<BK>(bh + o), idesc, (cfirst && j == 0) ? 0u : 1u);
+                        mma_f16(dx, sdesc<BK>(ah + o), sdesc<BK>(bl + o), idesc, (kb == 0 && j == 0) ? 0u : 1u);
+                        mma_f16(dx, sdesc<BK>(al + o), sdesc<BK>(bh + o), idesc, 1u);
                     }
                     mma_commit(&empty[s]);
+                    if (kb % ch == ch - 1 || kb == kbn - 1) {
+                        mma_commit(&hfull[hb]);
+                        ++cc;
+                    }
                 }
-                if (ok) mma_commit(&tfull[b]);
+                if (ok) mma_commit(&xfull);
             }
             // all issued MMAs complete before tensor memory is released
             mma_commit(&fin);
             mbar_drain(&fin, 0);
         }
     } else {  // ------------------------------------------------------ epilogue
-        const int q = warp & 3;  // tensor-memory lane quarter of this warp
-        int tcnt = 0;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcnt) {
+        // two warps per tensor-memory lane quarter, each owning 64 columns;
+        // the hi*hi chunks are summed in FP64 registers
+        const int q = warp & 3, half = (warp - 2) >> 2;
+        const uint32_t lanes = (uint32_t)(q * 32) << 16;
+        int tcnt = 0, cc = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tcnt) {
             int p, mt, nt;
             decode(ps, np, t, p, mt, nt);
-            const int b = split ? 0 : (tcnt & 1);
-            const uint32_t par = split ? (tcnt & 1) : ((tcnt >> 1) & 1);
-            const bool got = mbar_wait(&tfull[b], par, abort_flag);
+            const Problem& P = ps[p];
+            const int kbn = P.kblocks, ch = chunk > 0 ? chunk : kbn, nch = (kbn + ch - 1) / ch;
+            double acc[64];
+#pragma unroll
+            for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+            for (int c = 0; c < nch; ++c, ++cc) {
+                const int hb = cc % NHB;
+                const bool got = mbar_wait(&hfull[hb], (cc / NHB) & 1, abort_flag);
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t ta = tmem + lanes + (uint32_t)(hb * BN + half * 64);
+#pragma unroll
+                for (int g = 0; g < 2; ++g) {
+                    uint32_t r[32];
+                    tmem_ld32(ta + 32 * g, r);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) acc[g * 32 + j] += (double)__uint_as_float(r[j]);
+                }
+                tc_fence_before();
+                mbar_arrive(&hempty[hb]);
+            }
+            if (!ok) break;
+            const bool got = mbar_wait(&xfull, tcnt & 1, abort_flag);
             if (!__all_sync(0xffffffffu, got)) break;
             tc_fence_after();
-            const Problem& P = ps[p];
             const int m = mt * BM + q * 32 + lane;
             const bool mv = m < P.M;
-            const float rs = mv ? P.sa[m] : 0.0f;
+            const double rs = mv ? (double)P.sa[m] : 0.0;
             float* Cm = P.C + m;
-#pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 32) {
+            // the cross terms join the FP64 sums; then the accumulator is free
+#pragma unroll
+            for (int g = 0; g < 2; ++g) {
                 uint32_t r[32];
-                float v[32];
-                const uint32_t lanes = (uint32_t)(q * 32) << 16;
-                tmem_ld32(tmem + lanes + (uint32_t)(b * BN + c0), r);
+                tmem_ld32(tmem + lanes + (uint32_t)(NHB * BN + half * 64 + g * 32), r);
 #pragma unroll
-                for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
-                if (split) {
-                    tmem_ld32(tmem + lanes + (uint32_t)(BN + c0), r);
+                for (int j = 0; j < 32; ++j) acc[g * 32 + j] += (double)__uint_as_float(r[j]);
+            }
+            tc_fence_before();
+            mbar_arrive(&xempty);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) v[j] += __uint_as_float(r[j]);
-                }
-                const int n0 = nt * BN + c0;
+            for (int g = 0; g < 2; ++g) {
+                const int n0 = nt * BN + half * 64 + g * 32;
                 if (mv) {
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
                         const int n = n0 + j;
-                        if (n < P.N) Cm[(long long)n * P.ldc] = v[j] * rs * P.sb[n];
+                        if (n < P.N)
+                            Cm[(long long)n * P.ldc] =
+                                (float)(acc[g * 32 + j] * rs * (double)P.sb[n]);
                     }
                 }
             }
-            tc_fence_before();
-            mbar_arrive(&tempty[b]);
         }
     }
 
@@ -440,30 +483,30 @@ void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, in
 }
 
 void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int piece_fmt, int bk, uint32_t flags,
-            int* d_err, int nsm, cudaStream_t st) {
+            int chunk, int* d_err, int nsm, cudaStream_t st) {
     if (np <= 0 || ntiles <= 0) return;
     if (np > MAXP) throw Error(DSM_ERR_INVALID, "too many contractions in one launch");
     // kind::f16 instruction descriptor: FP32 accumulator, both operands of
-    // the piece type and order-major, N = 256, M = 128
+    // the piece type and order-major, N = BN, M = BM
     const uint32_t fmt = piece_fmt == PIECE_BF16 ? 1u : 0u;
     const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(BN >> 3) << 17) |
                            ((uint32_t)(BM >> 4) << 24);
     const int grid = std::min(ntiles, nsm);
-    const size_t smem = 4 * 48 * 1024 + 1024;
+    const size_t smem = SMEM_STAGES + 1024;
     if (bk == 32) {
         static bool attr32 = false;
         if (!attr32) {
             DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr32 = true;
         }
-        k_lsum_tc<32><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, d_err);
+        k_lsum_tc<32><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, chunk, d_err);
     } else if (bk == 64) {
         static bool attr64 = false;
         if (!attr64) {
             DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr64 = true;
         }
-        k_lsum_tc<64><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, d_err);
+        k_lsum_tc<64><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, chunk, d_err);
     } else {
         throw Error(DSM_ERR_INVALID, "BK must be 32 or 64");
     }

@@ -7,7 +7,8 @@
 // A and per column of B.  The product runs as x_hi*y_hi + x_hi*y_lo +
 // x_lo*y_hi on the tensor cores with FP32 accumulation in tensor memory;
 // the epilogue applies s_row * s_col and writes C column-major (ld = M),
-// the layout the FP64 contraction writes.
+// the layout the FP64 contraction writes.  The hi*hi products are summed in
+// chunks of `chunk` stages whose partial sums are added in FP64.
 #pragma once
 
 #include <cuda.h>
@@ -18,12 +19,12 @@ namespace dsm {
 namespace tc {
 
 constexpr int BM = 128;          // rows of a tile (tensor-memory lanes)
-constexpr int BN = 256;          // columns of a tile (tensor-memory columns)
+constexpr int BN = 128;          // columns of a tile (tensor-memory columns)
 constexpr int MAXP = 96;         // problems per launch
 constexpr int PIECE_F16 = 0;     // fp16 pieces (11-bit significand each)
 constexpr int PIECE_BF16 = 1;    // bf16 pieces (8-bit significand each)
 constexpr uint32_t TC_REVERSE = 1;    // orders summed from high to low
-constexpr uint32_t TC_SPLIT_ACC = 2;  // hi*hi and cross products in separate accumulators
+constexpr int TC_CHUNK = 2;           // stages of BK orders per hi*hi chunk
 
 // One contraction of a launch.  Rows of A beyond M and columns beyond N are
 // read as zeros by the tensor-map bounds and never stored.
@@ -61,7 +62,7 @@ void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, in
 // Launches the persistent contraction over all tiles of probs[0..np).
 // err (device int) is set nonzero if a bounded wait inside gave up.
 void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int piece_fmt, int bk, uint32_t flags,
-            int* d_err, int nsm, cudaStream_t st);
+            int chunk, int* d_err, int nsm, cudaStream_t st);
 
 }  // namespace tc
 }  // namespace dsm

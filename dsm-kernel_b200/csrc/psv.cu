@@ -53,6 +53,9 @@ struct PsvDev {
     const int *amz, *amc;   // [nn+1][2] zone (or -1) and zone-local column
     const int* bcrow;       // 0, 2 or 3
     const double* bcval;
+    const int4* rowasm;     // [nn+1] per row: element offsets of the two zones
+                            // (x4, -1 none), phase bits (1: zone 0 solid,
+                            // 2: zone 1 solid), bcrow
     double tlen, omegai, rmax, r0, ecC0, ecF0, ecL0, ra0, ra1;
     const double* poly;     // [24]
     // receivers
@@ -243,11 +246,13 @@ __device__ __forceinline__ void assemble(const PsvDev& d, int jj, const cd* __re
                                          const cd* __restrict__ B1, const cd* __restrict__ B2,
                                          double l2, double lsq, cd a[4]) {
     a[0] = a[1] = a[2] = a[3] = mk(0.0);
+    const int4 ra = d.rowasm[jj];
+#pragma unroll
     for (int e = 0; e < 2; ++e) {
-        int z = d.amz[2 * jj + e];
-        if (z < 0) break;
-        size_t o = ((size_t)d.blkoff[z] + d.amc[2 * jj + e] - 1) * 4;
-        if (d.iphase[z] == 1) {
+        const int off = e == 0 ? ra.x : ra.y;
+        if (off < 0) break;
+        const size_t o = (size_t)off;
+        if (ra.z & (1 << e)) {
             for (int ii = 2; ii <= 4; ii += 2) {
                 cd x0 = B0[o + ii - 1], x2 = B2[o + ii - 1];
                 a[ii - 1] = a[ii - 1] + mk(x0.re + l2 * x2.re, x0.im + l2 * x2.im);
@@ -263,20 +268,24 @@ __device__ __forceinline__ void assemble(const PsvDev& d, int jj, const cd* __re
             }
         }
     }
-    int br = d.bcrow[jj];
-    if (br == 2) a[1] = mk(d.bcval[jj]);
-    else if (br == 3) a[2] = -mk(d.bcval[jj]);
+    if (ra.w == 2) a[1] = mk(d.bcval[jj]);
+    else if (ra.w == 3) a[2] = -mk(d.bcval[jj]);
 }
 
 // ---------------------------------------------------------------- solve
 // Streaming LDL^T of the band system rows itmp..nn (local rows 1..n).
 // Window W[p][q] holds the current values of A(k+p, k+q), q <= p <= 3.
+// last pivots and multiplier of a factorisation, for the upward pass
+struct SysTail {
+    cd Dn, Dm1, Lnn1;
+};
+
 __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restrict__ B0all,
                                                    const cd* __restrict__ B1all,
                                                    const cd* __restrict__ B2all, WorkList wl,
                                                    int nsys, int jmin_loc, const int* __restrict__ capmap,
                                                    cd* __restrict__ Lst, cd* __restrict__ Zst,
-                                                   cd* __restrict__ Xcap) {
+                                                   SysTail* __restrict__ tail) {
     int sys = blockIdx.x * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
     int w, l;
@@ -349,6 +358,10 @@ __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restric
         // forward substitution of row j = k+1 (dcsbdlv0, m = 3)
         int j = k + 1;
         for (int b = 0; b < 4; ++b) {
+            if (j < ls) {  // below the source rows every z is exactly zero
+                zcur[b] = mk(0.0);
+                continue;
+            }
             cd rhs = mk(ls + b == j ? 1.0 : 0.0);
             if (j == 2) {
                 zcur[b] = rhs - a22raw * zs[b][2];
@@ -362,49 +375,69 @@ __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restric
         }
         for (int p = 0; p < 3; ++p) { wp2[p] = wp1[p]; wp1[p] = wv_[p]; }
     }
-    // upward substitution.  x(n) = zh(n); x(n-1) = zh(n-1) - L(n,n-1) x(n);
-    // x(j) = zh(j) - [L(j+3,j) x(j+3) + L(j+2,j) x(j+2) + L(j+1,j) x(j+1)]
-    const cd Dn = W[0][0];
-    cd x[NB][3];  // x(j+1), x(j+2), x(j+3)
-    cd xn[NB];
-    for (int b = 0; b < 4; ++b) xn[b] = (n >= ls) ? Zst[((size_t)(n - ls) * 4 + b) * nsys + sys] : mk(0.0);
-    // surface basis: e_{n-1}: z(n-1) = 1, z(n) = -L(n,n-1); e_n: z(n) = 1
-    xn[4] = (mk(0.0) - Lnn1 * mk(1.0)) / Dn;
-    xn[5] = mk(1.0) / Dn;
+    tail[sys] = SysTail{W[0][0], Dm1, Lnn1};
+}
+
+// Upward substitution of the six basis right-hand sides, two threads per
+// system (three right-hand sides each; the pair reads the same factor
+// entries in the same instruction).  x(n) = zh(n); x(n-1) = zh(n-1) -
+// L(n,n-1) x(n); x(j) = zh(j) - [L(j+3,j) x(j+3) + L(j+2,j) x(j+2) +
+// L(j+1,j) x(j+1)] (dcsbdlv0's backward loop), down to the deepest
+// captured row.  Values at receiver stencil rows go to Xcap.
+__global__ void __launch_bounds__(128) k_psv_back(PsvDev d, int nsys, int jmin_loc, const int* __restrict__ capmap,
+                                                  const cd* __restrict__ Lst, const cd* __restrict__ Zst,
+                                                  const SysTail* __restrict__ tail, cd* __restrict__ Xcap) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int sys = t >> 1, b0 = (t & 1) * 3;
+    if (sys >= nsys) return;
+    const int it = d.itmp, n = d.nn - it + 1;
+    const int ls = d.jsrc - it + 1;
+    const SysTail tl = tail[sys];
+    cd x[3][3];  // x(j+1), x(j+2), x(j+3) of this thread's three bases
+    cd xn[3];
+    for (int k = 0; k < 3; ++k) {
+        const int b = b0 + k;
+        if (b < 4) xn[k] = (n >= ls) ? Zst[((size_t)(n - ls) * 4 + b) * nsys + sys] : mk(0.0);
+        // surface basis: e_{n-1}: z(n-1) = 1, z(n) = -L(n,n-1); e_n: z(n) = 1
+        else if (b == 4) xn[k] = (mk(0.0) - tl.Lnn1 * mk(1.0)) / tl.Dn;
+        else xn[k] = mk(1.0) / tl.Dn;
+    }
     auto capture = [&](int jloc, const cd* v) {
         int c = capmap[jloc + it - 1];
         if (c >= 0)
-            for (int b = 0; b < NB; ++b) Xcap[((size_t)c * NB + b) * nsys + sys] = v[b];
+            for (int k = 0; k < 3; ++k) Xcap[((size_t)c * NB + b0 + k) * nsys + sys] = v[k];
     };
     capture(n, xn);
-    for (int b = 0; b < NB; ++b) { x[b][0] = xn[b]; x[b][1] = mk(0.0); x[b][2] = mk(0.0); }
+    for (int k = 0; k < 3; ++k) { x[k][0] = xn[k]; x[k][1] = mk(0.0); x[k][2] = mk(0.0); }
     if (n - 1 >= jmin_loc) {
-        cd v[NB];
+        cd v[3];
         cd L1 = Lst[((size_t)(n - 1) * 3 + 0) * nsys + sys];
-        for (int b = 0; b < NB; ++b) {
+        for (int k = 0; k < 3; ++k) {
+            const int b = b0 + k;
             cd zh = mk(0.0);
             if (b < 4 && n - 1 >= ls) zh = Zst[((size_t)(n - 1 - ls) * 4 + b) * nsys + sys];
-            if (b == 4) zh = mk(1.0) / Dm1;
-            v[b] = zh - L1 * x[b][0];
+            if (b == 4) zh = mk(1.0) / tl.Dm1;
+            v[k] = zh - L1 * x[k][0];
         }
         capture(n - 1, v);
-        for (int b = 0; b < NB; ++b) { x[b][1] = x[b][0]; x[b][0] = v[b]; }
+        for (int k = 0; k < 3; ++k) { x[k][1] = x[k][0]; x[k][0] = v[k]; }
     }
     for (int j1 = n - 2; j1 >= jmin_loc; --j1) {
         cd L1 = Lst[((size_t)j1 * 3 + 0) * nsys + sys];
         cd L2 = Lst[((size_t)j1 * 3 + 1) * nsys + sys];
         cd L3 = Lst[((size_t)j1 * 3 + 2) * nsys + sys];
-        cd v[NB];
-        for (int b = 0; b < NB; ++b) {
+        cd v[3];
+        for (int k = 0; k < 3; ++k) {
+            const int b = b0 + k;
             cd zh = mk(0.0);
             if (b < 4 && j1 >= ls) zh = Zst[((size_t)(j1 - ls) * 4 + b) * nsys + sys];
             cd sum;
-            if (j1 == n - 2) sum = mk(0.0) + L2 * x[b][1] + L1 * x[b][0];
-            else sum = mk(0.0) + L3 * x[b][2] + L2 * x[b][1] + L1 * x[b][0];
-            v[b] = zh - sum;
+            if (j1 == n - 2) sum = mk(0.0) + L2 * x[k][1] + L1 * x[k][0];
+            else sum = mk(0.0) + L3 * x[k][2] + L2 * x[k][1] + L1 * x[k][0];
+            v[k] = zh - sum;
         }
         capture(j1, v);
-        for (int b = 0; b < NB; ++b) { x[b][2] = x[b][1]; x[b][1] = x[b][0]; x[b][0] = v[b]; }
+        for (int k = 0; k < 3; ++k) { x[k][2] = x[k][1]; x[k][1] = x[k][0]; x[k][0] = v[k]; }
     }
 }
 
@@ -1190,6 +1223,8 @@ class PsvEngine : public Engine {
         capmap, l0col, l0e1;
     DBuf<double> qmu, qkappa, sel, fel, hm, bcval, poly, lam, qkp, fr, r, rrsta;
     DBuf<cd> B0, B1, B2, Lst, Zst, Xcap, l0scr, l0d, ab, co;
+    DBuf<int4> rowasm;
+    DBuf<SysTail> tails;
     int jmin_loc = 1, ncap = 0;
     double vtop = 0, rtop = 0;
 
@@ -1248,6 +1283,21 @@ class PsvEngine : public Engine {
             if (s->iphase[i - 1] == 2 && s->iphase[i] == 1) { br[s->kkdr[i]] = 3; bv[s->kkdr[i]] = rv; }
         }
         amz.upload(az, st); amc.upload(ac, st); bcrow.upload(br, st); bcval.upload(bv, st);
+        {
+            std::vector<int4> ra(nn + 1);
+            for (int jj = 0; jj <= nn; ++jj) {
+                int4 v = make_int4(-1, -1, 0, br[jj]);
+                for (int e = 0; e < 2; ++e) {
+                    const int z = az[2 * jj + e];
+                    if (z < 0) break;
+                    const int o = (bo[z] + ac[2 * jj + e] - 1) * 4;
+                    if (e == 0) v.x = o; else v.y = o;
+                    if (s->iphase[z] == 1) v.z |= 1 << e;
+                }
+                ra[jj] = v;
+            }
+            rowasm.upload(ra, st);
+        }
         // receivers
         r.upload(s->r, R, st);
         rrsta.upload(s->rrsta, 3 * (size_t)R, st);
@@ -1316,6 +1366,7 @@ class PsvEngine : public Engine {
         rtop = s->vrmax[nz - 1];
         vtop_ = vtop;
         rtop_ = rtop;
+        set_summaries(1, nz, s->vrmin, s->vrmax, s->vsv, s->qmu, s->r0, s->r[R - 1]);
         // theta tables
         th.th_n = Th;
         th.h_x.resize(Th); th.h_s.resize(Th); th.h_pole.resize(Th);
@@ -1330,6 +1381,7 @@ class PsvEngine : public Engine {
         d.iphase = iphase.p; d.nlayer = nlayer.p; d.kkdr = kkdr.p; d.elem = elem.p; d.hmoff = hmoff.p;
         d.blkoff = blkoff.p; d.qmu = qmu.p; d.qkappa = qkappa.p; d.sel = sel.p; d.fel = fel.p; d.hm = hm.p;
         d.amz = amz.p; d.amc = amc.p; d.bcrow = bcrow.p; d.bcval = bcval.p; d.poly = poly.p;
+        d.rowasm = rowasm.p;
         d.rcap = rcap.p; d.wv = wv.p; d.wd = wd.p; d.fluid = fluid.p; d.lam = lam.p; d.qkp = qkp.p;
         d.fr = fr.p; d.comp_src = comp_src.p; d.jsta = jsta.p;
         F = opt.freq_batch > 0 ? opt.freq_batch : 8;
@@ -1358,6 +1410,7 @@ class PsvEngine : public Engine {
         Lst.reserve((n + 1) * 3 * nsys);
         Zst.reserve((n - ls + 2) * 4 * nsys);
         Xcap.reserve((size_t)ncap * NB * nsys);
+        tails.reserve(nsys);
         l0scr.reserve((size_t)F * (d.nn0 + 1) * 2);
         l0d.reserve((size_t)F * (d.nn0 + 1) * 4);
         ab.reserve((size_t)F * 320);
@@ -1417,7 +1470,10 @@ class PsvEngine : public Engine {
         int id = kid("psv_band_solve");
         kbegin(id);
         k_psv_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, B0.p, B1.p, B2.p, wl, nsys, jmin_loc,
-                                                        capmap.p, Lst.p, Zst.p, Xcap.p);
+                                                        capmap.p, Lst.p, Zst.p, tails.p);
+        DSM_LAUNCH(*this);
+        k_psv_back<<<(2 * nsys + 127) / 128, 128, 0, st>>>(d, nsys, jmin_loc, capmap.p, Lst.p, Zst.p, tails.p,
+                                                           Xcap.p);
         kend(id, alg * nsys, 0.0);
         DSM_LAUNCH(*this);
         id = kid("psv_source_coef");

@@ -567,6 +567,7 @@ class ShEngine : public Engine {
         rtop = s->vrmax[s->nzone - 1];
         vtop_ = vtop;
         rtop_ = rtop;
+        set_summaries(0, s->nzone, s->vrmin, s->vrmax, s->vsv, s->qmu, s->r0, s->vrmax[s->nzone - 1]);
         // capture rows: receiver stencils and the surface
         std::vector<int> cm(nn + 1, -1), rc(3 * (size_t)R);
         jmin = nn;

@@ -88,7 +88,7 @@ __global__ void k_scales(float* sa, int M, float* sb, int N) {
 }
 
 template <class T>
-int run(int M, int N, int K, int nf, int fmt, int bk, uint32_t flags, int reps, int check, double* res) {
+int run(int M, int N, int K, int nf, int fmt, int bk, uint32_t flags, int chunk, int reps, int check, double* res) {
     const int kcap = K + bk;  // capacity beyond K holds nonzero values the kernel must not read
     const size_t An = (size_t)nf * M * kcap, Bn = (size_t)N * kcap;
     DBuf<T> A, B;
@@ -141,13 +141,13 @@ int run(int M, int N, int K, int nf, int fmt, int bk, uint32_t flags, int reps, 
     DSM_CUDA(cudaGetDevice(&dev));
     DSM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
 
-    tc::launch(maps, dp.p, nf, tiles, fmt, bk, flags, err.p, nsm, 0);
+    tc::launch(maps, dp.p, nf, tiles, fmt, bk, flags, chunk, err.p, nsm, 0);
     DSM_CUDA(cudaDeviceSynchronize());
     cudaEvent_t e0, e1;
     DSM_CUDA(cudaEventCreate(&e0));
     DSM_CUDA(cudaEventCreate(&e1));
     DSM_CUDA(cudaEventRecord(e0, 0));
-    for (int r = 0; r < reps; ++r) tc::launch(maps, dp.p, nf, tiles, fmt, bk, flags, err.p, nsm, 0);
+    for (int r = 0; r < reps; ++r) tc::launch(maps, dp.p, nf, tiles, fmt, bk, flags, chunk, err.p, nsm, 0);
     DSM_CUDA(cudaEventRecord(e1, 0));
     DSM_CUDA(cudaEventSynchronize(e1));
     float ms = 0.0f;
@@ -176,14 +176,14 @@ int run(int M, int N, int K, int nf, int fmt, int bk, uint32_t flags, int reps, 
 
 // res[0] max |C - ref|, res[1] max |ref| (both 0 unless check), res[2] ms per
 // launch over reps timed launches, res[3] tensor flops per launch
-extern "C" int dsm_tc_selftest(int M, int N, int K, int nfreq, int piece_fmt, int bk, int flags, int reps,
-                               int check, double* res) {
+extern "C" int dsm_tc_selftest(int M, int N, int K, int nfreq, int piece_fmt, int bk, int flags, int chunk,
+                               int reps, int check, double* res) {
     try {
         if (M <= 0 || N <= 0 || K <= 0 || nfreq <= 0 || nfreq > dsm::tc::MAXP || (K % bk) != 0 || !res)
             return DSM_ERR_INVALID;
         if (piece_fmt == dsm::tc::PIECE_BF16)
-            return dsm::run<__nv_bfloat16>(M, N, K, nfreq, piece_fmt, bk, (uint32_t)flags, reps, check, res);
-        return dsm::run<__half>(M, N, K, nfreq, piece_fmt, bk, (uint32_t)flags, reps, check, res);
+            return dsm::run<__nv_bfloat16>(M, N, K, nfreq, piece_fmt, bk, (uint32_t)flags, chunk, reps, check, res);
+        return dsm::run<__half>(M, N, K, nfreq, piece_fmt, bk, (uint32_t)flags, chunk, reps, check, res);
     } catch (const dsm::Error& e) {
         dsm::set_global_error(std::string("dsm_tc_selftest: ") + e.what());
         return e.code;

@@ -144,24 +144,83 @@ def lib() -> C.CDLL:
         L.dsm_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.dsm_set_profiling.argtypes = [C.c_void_p, C.c_int]
         L.dsm_sh_cutoff_noalloc.argtypes = [C.POINTER(ShSetup), _ip, C.c_int, _ip]
-        L.dsm_tc_selftest.argtypes = [C.c_int] * 9 + [C.POINTER(C.c_double)]
+        L.dsm_tc_selftest.argtypes = [C.c_int] * 10 + [C.POINTER(C.c_double)]
+        _f = C.POINTER(C.c_float)
+        L.dsm_lmax_features.argtypes = [C.c_void_p, _ip, C.c_int, _f]
+        L.dsm_cutoffs.argtypes = [C.c_void_p, _ip, C.c_int, _ip]
+        L.dsm_lmax_init.argtypes = [_f, _f, C.c_int, C.c_uint, _f]
+        L.dsm_lmax_train.argtypes = [_f, _f, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint, _f, _f,
+                                     C.c_int]
+        L.dsm_lmax_grad.argtypes = [_f, _f, _f, C.c_int, _f, _f, C.c_int]
+        L.dsm_set_lmax_model.argtypes = [C.c_void_p, _f]
+        L.dsm_lmax_predict.argtypes = [C.c_void_p, _ip, C.c_int, _f]
         _lib = L
     return _lib
 
 
 def tc_selftest(M: int, N: int, K: int, nfreq: int = 1, fmt: int = 0, bk: int = 32, reps: int = 0,
-                check: bool = True, flags: int = 3) -> dict:
+                check: bool = True, flags: int = 1, chunk: int = 2) -> dict:
     """Runs the tensor-core split contraction on seeded pieces (fmt 0 fp16,
     1 bf16) and, with check, compares it with an FP64 sum of the same piece
-    products.  flags: 1 high-to-low order, 2 separate hi*hi accumulator.
+    products.  flags: 1 high-to-low order; chunk: stages per hi*hi chunk
+    summed in FP64 (0: one chunk per tile).
     Returns max |error|, max |reference|, ms per launch and the tensor
     flops of one launch."""
     L = lib()
     res = (C.c_double * 4)()
-    rc = L.dsm_tc_selftest(M, N, K, nfreq, fmt, bk, flags, reps, int(check), res)
+    rc = L.dsm_tc_selftest(M, N, K, nfreq, fmt, bk, flags, chunk, reps, int(check), res)
     if rc:
         raise DsmError(f"dsm_tc_selftest failed ({rc}): {L.dsm_last_error(None).decode()}")
     return {"max_err": res[0], "ref_max": res[1], "ms": res[2], "flops": res[3]}
+
+
+LMAX_NFEAT = 11
+LMAX_WIDTH = 128
+LMAX_NPARAM = 34713
+
+
+def _fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def lmax_init(X, T, seed: int = 0) -> np.ndarray:
+    """Parameter block: standardisation from (X, T) and He-initialised weights."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    P = np.zeros(LMAX_NPARAM, np.float32)
+    rc = lib().dsm_lmax_init(_fptr(X), _fptr(T), len(T), seed, _fptr(P))
+    if rc:
+        raise DsmError("dsm_lmax_init failed")
+    return P
+
+
+def lmax_train(X, T, params, epochs: int = 200, batch: int = 256, lr: float = 1e-3, seed: int = 0,
+               device: int = 0):
+    """Adam on the GPU with the project's forward/backward kernels; returns
+    (trained parameters, per-epoch loss)."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    P = np.ascontiguousarray(params, dtype=np.float32).copy()
+    losses = np.zeros(epochs, np.float32)
+    rc = lib().dsm_lmax_train(_fptr(X), _fptr(T), len(T), epochs, batch, lr, seed, _fptr(P), _fptr(losses),
+                              device)
+    if rc:
+        raise DsmError(f"dsm_lmax_train failed ({rc}): {lib().dsm_last_error(None).decode()}")
+    return P, losses
+
+
+def lmax_grad(params, X, T, device: int = 0):
+    """Loss and gradient of the network on (X, T) from the GPU kernels."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    P = np.ascontiguousarray(params, dtype=np.float32)
+    G = np.zeros(LMAX_NPARAM, np.float32)
+    loss = np.zeros(1, np.float32)
+    rc = lib().dsm_lmax_grad(_fptr(P), _fptr(X), _fptr(T), len(T), _fptr(G), _fptr(loss), device)
+    if rc:
+        raise DsmError(f"dsm_lmax_grad failed ({rc}): {lib().dsm_last_error(None).decode()}")
+    return G, float(loss[0])
 
 
 def _ptr(a: np.ndarray, typ):
@@ -308,6 +367,41 @@ class Context:
         rc = L.dsm_run_freqs(self.h, _ptr(fl, _ip), len(fl), C.byref(out))
         if rc:
             raise DsmError(f"dsm_run_freqs failed ({rc}): {L.dsm_last_error(self.h).decode()}")
+
+    def cutoffs(self, freqs):
+        """Realised cutoffs (llog) only: banded solves and the amplitude
+        test, no l-sum (dsm_cutoffs)."""
+        L = lib()
+        fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+        llog = np.zeros(len(fl), np.int32)
+        rc = L.dsm_cutoffs(self.h, _ptr(fl, _ip), len(fl), _ptr(llog, _ip))
+        if rc:
+            raise DsmError(f"dsm_cutoffs failed ({rc}): {L.dsm_last_error(self.h).decode()}")
+        return llog
+
+    def lmax_features(self, freqs):
+        fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+        f = np.zeros((len(fl), LMAX_NFEAT), np.float32)
+        rc = lib().dsm_lmax_features(self.h, _ptr(fl, _ip), len(fl), _fptr(f))
+        if rc:
+            raise DsmError("dsm_lmax_features failed")
+        return f
+
+    def set_lmax_model(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == LMAX_NPARAM
+        rc = lib().dsm_set_lmax_model(self.h, _fptr(p))
+        if rc:
+            raise DsmError(f"dsm_set_lmax_model failed ({rc}): {lib().dsm_last_error(self.h).decode()}")
+
+    def lmax_predict(self, freqs):
+        """log(lmax) predicted by the attached network."""
+        fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+        out = np.zeros(len(fl), np.float32)
+        rc = lib().dsm_lmax_predict(self.h, _ptr(fl, _ip), len(fl), _fptr(out))
+        if rc:
+            raise DsmError(f"dsm_lmax_predict failed ({rc}): {lib().dsm_last_error(self.h).decode()}")
+        return out
 
     def stats(self) -> Stats:
         s = Stats()

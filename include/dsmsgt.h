@@ -267,6 +267,46 @@ int dsm_set_profiling(dsm_ctx_t *ctx, int on);
  * the array and race. */
 int dsm_sh_cutoff_noalloc(const dsm_sh_setup_t *setup, const int *ilist, int n, int *llog);
 
+/* ------------------------------------------------------------------------
+ * Learned angular-order cutoff.  No counterpart in the reference.  A
+ * 4-layer MLP (width 128, GELU, bf16 weights, FP32 accumulation) maps
+ * DSM_LMAX_NFEAT features of a frequency to log(lmax); a context with
+ * opt.use_lmax_predictor = 1 and a loaded parameter block sizes the first
+ * order range of each frequency with it.  The plain amplitude test still
+ * runs on the device and extends any short range, so the cutoff (llog) and
+ * the outputs are those of the plain method; only padded work changes.
+ * ---------------------------------------------------------------------- */
+#define DSM_LMAX_NFEAT   11
+#define DSM_LMAX_WIDTH   128
+#define DSM_LMAX_NPARAM  34713   /* floats in a parameter block          */
+
+/* Features of frequencies ilist[0..n) for the context's set-up, n x NFEAT:
+ * log(1 + omega rtop / vtop) (the reference's lsuf scale, callsuf),
+ * source radius / rmax, probe receiver radius / rmax, and 8 model
+ * summaries: surface Vs, Vs at the source, min and max zone Vs (/10),
+ * source depth (/1000 km), top-zone thickness (/100 km), mode (0 SH,
+ * 1 P-SV), log10(Qmu at the source) / 3. */
+int dsm_lmax_features(const dsm_ctx_t *ctx, const int *ilist, int n, float *feats);
+
+/* Realised cutoffs only (banded solves and the amplitude test, no l-sum):
+ * llog[k] as dsm_run_freqs reports it.  Used to harvest training data. */
+int dsm_cutoffs(dsm_ctx_t *ctx, const int *ilist, int n, int *llog);
+
+/* Parameter block: standardisation from (feats, target), He-initialised
+ * weights from seed. target = log(llog) per row. */
+int dsm_lmax_init(const float *feats, const float *target, int n, unsigned seed, float *params);
+/* Adam on the GPU (device ordinal): params in/out, losses[epochs] out. */
+int dsm_lmax_train(const float *feats, const float *target, int n, int epochs, int batch,
+                   float lr, unsigned seed, float *params, float *losses, int device);
+/* Loss (mean squared error of the standardised output) and its gradient
+ * with respect to every parameter, on the n rows given. */
+int dsm_lmax_grad(const float *params, const float *feats, const float *target, int n,
+                  float *grad, float *loss, int device);
+/* Attaches a parameter block to a context; log(lmax) predictions of
+ * frequencies ilist[0..n) go to out (may be NULL). */
+int dsm_set_lmax_model(dsm_ctx_t *ctx, const float *params);
+int dsm_lmax_predict(dsm_ctx_t *ctx, const int *ilist, int n, float *out);
+
 #ifdef __cplusplus
 }
 #endif
