@@ -9,8 +9,14 @@ A step is one batch of frequency slices spread across the band, each fully
 processed (all orders up to the reference's cutoff, all m, all sources,
 TSGT + RSGT + SYNN on the full (r, theta) grid).
 
-  python bench.py [--gpus N --steps K --warmup W] [--precision mixed|fp64]
+  python bench.py [--gpus N --steps K --warmup W] [--precision mixed|mixed_bf16|fp64]
   python bench.py --impl reference ...   # CPU restatement of the reference
+
+The headline path is the mixed-precision one (split fp16 l-sum on the
+tensor cores, learned first order ranges when a trained parameter block is
+present); the plain FP64 GPU path runs the same steps for the speedup, and
+both paths' outputs on a sample of the first step give the per-component
+relative L2.
 
 One JSON line is printed by rank 0.  Under torchrun (N > 1) every rank
 processes its own frequencies (weak scaling, no collective on the data
@@ -32,7 +38,7 @@ sys.path.insert(0, REPO)
 
 import numpy as np  # noqa: E402
 
-METRIC = "SGT freq-slices/s (P-SV, all orders to the DSM cutoff)"
+METRIC = "SGT freq-slices/s at rel-L2<=1e-6 vs FP64; speedup over plain FP64 GPU path"
 UNIT = "freq-slices/s"
 
 
@@ -55,6 +61,29 @@ def workload(mode: str):
         desc = {"workload": "SGTsh synthetic mantle (5 solid zones, seed 0)", "tlen_s": 1638.4,
                 "np": 256, "source_depth_km": 100, "receivers": 100, "thetas": 361}
     return job, desc
+
+
+def per_component_rel_l2(a, b):
+    """Relative L2 of each output component (last axis) over frequencies,
+    radii and distances; components that vanish identically for the path
+    (round-off only) are measured against the whole array's norm."""
+    tot = np.sqrt(np.sum(np.abs(b) ** 2))
+    out = []
+    for c in range(a.shape[-1]):
+        nb = np.sqrt(np.sum(np.abs(b[..., c]) ** 2))
+        d = np.sqrt(np.sum(np.abs(a[..., c] - b[..., c]) ** 2))
+        out.append(float(d / (nb if nb >= 1e-10 * tot else tot)) if tot > 0 else float(d))
+    return out
+
+
+def load_lmax_params(mode: str):
+    """Trained parameter block of the learned cutoff (written by
+    dsmsgt.lmax_data), or None."""
+    path = os.path.join(REPO, "dsm-kernel_b200", "dsmsgt", f"lmax_{mode}.f32")
+    if not os.path.exists(path):
+        return None
+    p = np.fromfile(path, dtype=np.float32)
+    return p if p.size == 34713 else None
 
 
 def step_freqs(step: int, per_step: int, imax: int, rank: int = 0, world: int = 1) -> list[int]:
@@ -149,7 +178,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--mode", default="psv", choices=["psv", "sh"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_bf16"])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-lmax", dest="lmax", action="store_false", help="plain first order ranges")
     ap.add_argument("--per-step", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -201,72 +232,96 @@ def main():
     dev = local
     job, desc = workload(args.mode)
     setup = dsmsgt.Setup(job, args.mode)
-    prec = dsmsgt.DSM_PREC_MIXED if args.precision == "mixed" else dsmsgt.DSM_PREC_FP64
-    ctx = dsmsgt.Context(setup, precision=prec, device=dev, freq_batch=args.per_step)
+    lmax_params = load_lmax_params(args.mode) if args.lmax else None
 
     def barrier():
         torch.cuda.synchronize(dev)
         if world > 1:
             torch.distributed.barrier()
 
-    # warm-up (untimed)
-    for w in range(args.warmup):
-        ctx.run_device(step_freqs(1000 + w, args.per_step, imax, rank, world))
-    # device-resident throughput: inputs (set-up, tables) already on the GPU
-    ctx.set_profiling(True)
-    clocks = ClockSampler(dev)
-    clocks.start()
-    kstats = {}
-    ms_dev = 0.0
-    launches = 0
-    llogs = []
-    barrier()
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        llogs.append(ctx.run_device(step_freqs(k, args.per_step, imax, rank, world)).tolist())
-        st = ctx.stats()
-        ms_dev += st.ms_total
-        launches += st.launches - sum(v[1] for k, v in st.kernels().items() if k.startswith("lsum_dgemm"))
-        for name, (ms, n, b, f) in st.kernels().items():
-            a = kstats.setdefault(name, [0.0, 0, 0.0, 0.0])
-            a[0] += ms; a[1] += n; a[2] += b; a[3] += f
-    barrier()
-    wall = time.perf_counter() - t0
-    clk = clocks.stop()
-    ctx.set_profiling(False)
-    t_step = ms_dev / 1e3
-    if world > 1:
-        tt = torch.tensor([t_step], device=f"cuda:{dev}", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_step = float(tt.item())
-    slices = args.steps * args.per_step * world
-    value = slices / t_step
+    def max_over_ranks(t):
+        if world > 1:
+            tt = torch.tensor([t], device=f"cuda:{dev}", dtype=torch.float64)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
 
-    # end to end through the C-ABI: complex64 catalogue records copied to
-    # pinned host memory every step (the frequency list goes host -> device)
-    nt, nr, ns = setup.num
-    per_t = nt * setup.r_n * setup.theta_n
-    per_r = nr * setup.r_n * setup.theta_n
-    per_s = ns * setup.theta_n
-    F = args.per_step
-    ht = torch.empty(2 * per_t * F, dtype=torch.float32, pin_memory=True)
-    hr = torch.empty(2 * per_r * F, dtype=torch.float32, pin_memory=True)
-    hy = torch.empty(2 * per_s * F, dtype=torch.float32, pin_memory=True)
-    ll = np.zeros(F, np.int32)
-    ms_e2e = 0.0
-    barrier()
-    for k in range(args.steps):
-        ctx.run_host32(step_freqs(k, F, imax, rank, world), ht.data_ptr(), hr.data_ptr(),
-                       hy.data_ptr(), ll)
-        ms_e2e += ctx.stats().ms_total
-    barrier()
-    t_e2e = ms_e2e / 1e3
-    if world > 1:
-        tt = torch.tensor([t_e2e], device=f"cuda:{dev}", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_e2e = float(tt.item())
-    e2e = {"value": slices / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * F,
-           "d2h_bytes_per_step": 8 * (per_t + per_r + per_s) * F + 4 * F}
+    def measure(prec, use_lmax):
+        """Device and end-to-end throughput of one precision mode over the
+        same steps; per-kernel CUDA-event times; solve statistics."""
+        ctx = dsmsgt.Context(setup, precision=prec, device=dev, freq_batch=args.per_step,
+                             use_lmax_predictor=1 if use_lmax else 0)
+        if use_lmax:
+            ctx.set_lmax_model(lmax_params)
+        for w in range(args.warmup):  # untimed
+            ctx.run_device(step_freqs(1000 + w, args.per_step, imax, rank, world))
+        ctx.set_profiling(True)
+        clocks = ClockSampler(dev)
+        clocks.start()
+        kstats, ms_dev, launches, llogs, systems, padded, used = {}, 0.0, 0, [], 0, 0, 0
+        barrier()
+        for k in range(args.steps):
+            llogs.append(ctx.run_device(step_freqs(k, args.per_step, imax, rank, world)).tolist())
+            st = ctx.stats()
+            ms_dev += st.ms_total
+            systems += st.systems
+            padded += st.orders_padded
+            used += st.orders_used
+            launches += st.launches - sum(v[1] for n_, v in st.kernels().items() if n_.startswith("lsum_dgemm"))
+            for name, (ms, n, b, f) in st.kernels().items():
+                acc = kstats.setdefault(name, [0.0, 0, 0.0, 0.0])
+                acc[0] += ms; acc[1] += n; acc[2] += b; acc[3] += f
+        barrier()
+        clk = clocks.stop()
+        ctx.set_profiling(False)
+        t_dev = max_over_ranks(ms_dev / 1e3)
+        # end to end through the C-ABI: complex64 catalogue records copied to
+        # pinned host memory every step (the frequency list goes host -> device)
+        nt, nr, ns = setup.num
+        per_t = nt * setup.r_n * setup.theta_n
+        per_r = nr * setup.r_n * setup.theta_n
+        per_s = ns * setup.theta_n
+        F = args.per_step
+        ht = torch.empty(2 * per_t * F, dtype=torch.float32, pin_memory=True)
+        hr = torch.empty(2 * per_r * F, dtype=torch.float32, pin_memory=True)
+        hy = torch.empty(2 * per_s * F, dtype=torch.float32, pin_memory=True)
+        ll = np.zeros(F, np.int32)
+        ms_e2e = 0.0
+        barrier()
+        for k in range(args.steps):
+            ctx.run_host32(step_freqs(k, F, imax, rank, world), ht.data_ptr(), hr.data_ptr(),
+                           hy.data_ptr(), ll)
+            ms_e2e += ctx.stats().ms_total
+        barrier()
+        t_e2e = max_over_ranks(ms_e2e / 1e3)
+        ctx.close()
+        slices = args.steps * args.per_step * world
+        return {"value": slices / t_dev, "t": t_dev, "kstats": kstats, "launches": launches,
+                "llogs": llogs, "clocks": clk, "systems": systems, "padded": padded, "used": used,
+                "e2e": {"value": slices / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * F,
+                        "d2h_bytes_per_step": 8 * (per_t + per_r + per_s) * F + 4 * F}}
+
+    headline_prec = {"fp64": dsmsgt.DSM_PREC_FP64, "mixed": dsmsgt.DSM_PREC_MIXED,
+                     "mixed_bf16": dsmsgt.DSM_PREC_MIXED_BF16}[args.precision]
+    mixed = headline_prec != dsmsgt.DSM_PREC_FP64
+    use_lmax = mixed and lmax_params is not None
+    run = measure(headline_prec, use_lmax)
+    plain = measure(dsmsgt.DSM_PREC_FP64, False) if mixed and not args.no_fp64 else None
+
+    # accuracy of the headline path against the FP64 GPU path: per output
+    # component relative L2 on a sample of the first step's frequencies
+    rel = None
+    if mixed and rank == 0:
+        fr = step_freqs(0, args.per_step, imax)[:: max(1, args.per_step // 4)]
+        c64 = dsmsgt.Context(setup, precision=dsmsgt.DSM_PREC_FP64, device=dev, freq_batch=len(fr))
+        ref = c64.run(fr)
+        c64.close()
+        cm = dsmsgt.Context(setup, precision=headline_prec, device=dev, freq_batch=len(fr))
+        got = cm.run(fr)
+        cm.close()
+        rel = {"frequencies": fr, "llog_equal": list(ref[3]) == list(got[3])}
+        for name, a, b_ in (("tsgt", got[0], ref[0]), ("rsgt", got[1], ref[1]), ("synn", got[2], ref[2])):
+            rel[name] = max(per_component_rel_l2(a, b_))
 
     # roofline of the dominant kernel of this library (CUDA events on the
     # library's stream over the timed region)
@@ -276,26 +331,34 @@ def main():
             peaks = json.load(fh)
     except Exception:
         pass
+    kstats = run["kstats"]
     own = {k: v for k, v in kstats.items() if not k.startswith("lsum_dgemm")}
     dom = max(own.items(), key=lambda kv: kv[1][0]) if own else None
     roof = None
     if dom:
         name, (ms, n, b, f) = dom
-        if b > 0:
-            ach = b / (ms / 1e3) / 1e9
-            peak = peaks.get("hbm_gbs", 6650.0)
-            roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                    "frac": ach / peak, "traffic": None,
-                    "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                    "avg_launch_ms": ms / max(n, 1)}
-        else:
+        if f > 0:
             ach = f / (ms / 1e3) / 1e12
             peak = peaks.get("bf16_tflops", 1590.0)
             roof = {"kernel": name, "bound": "tensor", "achieved": ach, "peak": peak,
                     "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
                     "peak_source": "measured" if "bf16_tflops" in peaks else "fallback",
                     "avg_launch_ms": ms / max(n, 1)}
-    share = {k: round(v[0] / max(ms_dev, 1e-9), 4) for k, v in kstats.items()}
+        else:
+            ach = b / (ms / 1e3) / 1e9
+            peak = peaks.get("hbm_gbs", 6650.0)
+            roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": ach / peak, "traffic": None,
+                    "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                    "avg_launch_ms": ms / max(n, 1)}
+    share = {k: round(v[0] / max(run["t"] * 1e3, 1e-9), 4) for k, v in kstats.items()}
+    tc = kstats.get("lsum_tc")
+    tensor = None
+    if tc and tc[0] > 0:
+        ach = tc[3] / (tc[0] / 1e3) / 1e12
+        peak = peaks.get("bf16_tflops", 1590.0)
+        tensor = {"kernel": "lsum_tc", "achieved": ach, "peak": peak, "unit": "TFLOP/s (tensor)",
+                  "frac": ach / peak, "avg_launch_ms": tc[0] / max(tc[1], 1)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -308,19 +371,33 @@ def main():
                          f"{desc['thetas']} distances; measured s: {json.dumps(times)}"}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": 1e3 * t_step / args.steps,
+        line = {"metric": METRIC, "value": run["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * run["t"] / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if args.precision == "fp64" else "bf16/f32",
+                "dtype": "f64" if not mixed else ("fp16x2 pieces, f32 accumulate (l-sum); f64 solves"
+                                                 if args.precision == "mixed" else
+                                                 "bf16x3 pieces, f32 accumulate (l-sum); f64 solves"),
                 "data": "synthetic (seeded 1-D polynomial model, reference file formats)",
                 "config": dict(desc, precision=args.precision, slices_per_step=args.per_step,
+                               learned_lmax=bool(use_lmax),
                                parallelism=f"dp{world} (frequencies per rank)",
                                l2="inputs larger than L2 (field matrices of several GB per step)"),
-                "e2e": e2e, "gpu_launches": int(launches),
-                "roofline": roof, "kernel_share": share, "cpu_baseline": cpu,
-                "clocks": clk, "wall_s": wall, "llog_first_step": llogs[0]}
+                "e2e": run["e2e"], "gpu_launches": int(run["launches"]),
+                "roofline": roof, "tensor_roofline": tensor, "kernel_share": share,
+                "cpu_baseline": cpu, "clocks": run["clocks"],
+                "solve": {"systems": run["systems"], "orders_used": run["used"],
+                          "orders_padded": run["padded"]},
+                "llog_first_step": run["llogs"][0]}
+        if plain:
+            line["fp64"] = {"value": plain["value"], "ms_per_step": 1e3 * plain["t"] / args.steps,
+                            "e2e": plain["e2e"]["value"], "systems": plain["systems"],
+                            "orders_padded": plain["padded"], "clocks": plain["clocks"]}
+            line["speedup_vs_fp64"] = run["value"] / plain["value"]
+            line["speedup_vs_fp64_e2e"] = run["e2e"]["value"] / plain["e2e"]["value"]
+        if rel:
+            line["rel_l2_vs_fp64"] = rel
         print(json.dumps(line))
-    ctx.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

@@ -275,124 +275,255 @@ __device__ __forceinline__ void assemble(const PsvDev& d, int jj, const cd* __re
 // ---------------------------------------------------------------- solve
 // Streaming LDL^T of the band system rows itmp..nn (local rows 1..n).
 // Window W[p][q] holds the current values of A(k+p, k+q), q <= p <= 3.
-// last pivots and multiplier of a factorisation, for the upward pass
+// Per-omega band pieces by row: for row jj and band entry q, the l-free
+// parts of a(q) = A[q] + l(l+1) B[q] + sqrt(l(l+1)) C[q] (cala), summed over
+// the zones that share the row, with the calbc boundary value in A.  Rows
+// of a single zone assemble to exactly what assemble() gives; rows where two
+// zones meet add the two zones' sums before the l terms (a rounding-level
+// difference).  Layout [omega][row][A0..3, B0..3, C0..3].
+__global__ void k_psv_rows(PsvDev d, const cd* __restrict__ B0all, const cd* __restrict__ B1all,
+                           const cd* __restrict__ B2all, cd* __restrict__ Prow) {
+    const int w = blockIdx.y;
+    const int jj = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jj > d.nn) return;
+    const size_t bo = (size_t)w * d.ncol_tot * 4;
+    const cd *B0 = B0all + bo, *B1 = B1all + bo, *B2 = B2all + bo;
+    cd A[4], B[4], C[4];
+    for (int q = 0; q < 4; ++q) A[q] = B[q] = C[q] = mk(0.0);
+    if (jj >= 1) {
+        const int4 ra = d.rowasm[jj];
+        for (int e = 0; e < 2; ++e) {
+            const int off = e == 0 ? ra.x : ra.y;
+            if (off < 0) break;
+            const size_t o = (size_t)off;
+            if (ra.z & (1 << e)) {
+                for (int ii = 2; ii <= 4; ii += 2) {
+                    A[ii - 1] = A[ii - 1] + B0[o + ii - 1];
+                    B[ii - 1] = B[ii - 1] + B2[o + ii - 1];
+                }
+                for (int ii = 1; ii <= 3; ii += 2) C[ii - 1] = C[ii - 1] + B1[o + ii - 1];
+            } else {
+                for (int ii = 3; ii <= 4; ++ii) {
+                    A[ii - 1] = A[ii - 1] + B0[o + ii - 1];
+                    B[ii - 1] = B[ii - 1] + B2[o + ii - 1];
+                }
+            }
+        }
+        if (ra.w == 2) { A[1] = mk(d.bcval[jj]); B[1] = C[1] = mk(0.0); }
+        else if (ra.w == 3) { A[2] = -mk(d.bcval[jj]); B[2] = C[2] = mk(0.0); }
+    }
+    cd* out = Prow + ((size_t)w * (d.nn + 1) + jj) * 12;
+    for (int q = 0; q < 4; ++q) {
+        out[q] = A[q];
+        out[4 + q] = B[q];
+        out[8 + q] = C[q];
+    }
+}
+
+// raw pieces of one row (loaded ahead of use) and their assembly at order l
+struct RowPieces {
+    cd v[12];
+};
+__device__ __forceinline__ void load_row(const cd* __restrict__ P, RowPieces& r) {
+#pragma unroll
+    for (int i = 0; i < 12; ++i) r.v[i] = P[i];
+}
+__device__ __forceinline__ void assemble_row(const RowPieces& r, double l2, double lsq, cd a[4]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const cd A = r.v[q], B = r.v[4 + q], C = r.v[8 + q];
+        a[q] = mk(A.re + l2 * B.re, A.im + l2 * B.im);
+        a[q] = mk(a[q].re + lsq * C.re, a[q].im + lsq * C.im);
+    }
+}
+
+// last pivots and multiplier of a factorisation, for the substitution pass
 struct SysTail {
-    cd Dn, Dm1, Lnn1;
+    cd Dn, Dm1, Lnn1, a22raw;
 };
 
-__global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restrict__ B0all,
-                                                   const cd* __restrict__ B1all,
-                                                   const cd* __restrict__ B2all, WorkList wl,
-                                                   int nsys, int jmin_loc, const int* __restrict__ capmap,
-                                                   cd* __restrict__ Lst, cd* __restrict__ Zst,
-                                                   SysTail* __restrict__ tail) {
+struct FactorCtx {
+    const PsvDev* d;
+    const cd* P;  // this frequency's row pieces, [row][12]
+    double l2, lsq;
+    int it, n, ls, lmin, nsys, sys;
+    cd *Lst, *Dst;
+};
+
+// Step k of dcsymbdl0 (half-width 3), P = k % 4.  The 4x4 window of the
+// band is a ring: entry (r, c) of local rows r-3 <= c <= r lives in
+// M[r % 4][c % 4], so a step writes the entering row into the slot of the
+// row it eliminated and moves nothing.  Same operations, in the same order,
+// as the reference's band loop (main update for k <= n-3, the last two
+// steps' order otherwise).
+template <int P>
+__device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], RowPieces& nxt, SysTail& T,
+                                            const FactorCtx& c) {
+    constexpr int S0 = P, S1 = (P + 1) & 3, S2 = (P + 2) & 3, S3 = (P + 3) & 3;
+    const cd D = M[S0][S0];
+    if (k >= c.ls) c.Dst[(size_t)(k - c.ls) * c.nsys + c.sys] = D;
+    if (k == c.n) return true;
+    if (k == c.n - 1) T.Dm1 = D;
+    const cd piv = mk(1.0) / D;
+    const int nw = min(3, c.n - k);
+    cd wv0, wv1 = mk(0.0), wv2 = mk(0.0), zv0, zv1 = mk(0.0), zv2 = mk(0.0);
+    zv0 = -M[S1][S0];
+    wv0 = M[S1][S0] * piv;
+    if (nw >= 2) {
+        zv1 = -M[S2][S0];
+        wv1 = M[S2][S0] * piv;
+    }
+    if (nw >= 3) {
+        zv2 = -M[S3][S0];
+        wv2 = M[S3][S0] * piv;
+    }
+    if (k >= c.lmin) {
+        cd* L = c.Lst + (size_t)k * 3 * c.nsys + c.sys;
+        L[0] = wv0;
+        L[c.nsys] = wv1;
+        L[2 * (size_t)c.nsys] = wv2;
+    }
+    if (k == c.n - 1) T.Lnn1 = wv0;
+    if (k <= c.n - 3) {  // main loop of dcsymbdl0: A(k+p,k+q) += w_q z_p
+        M[S1][S1] = M[S1][S1] + wv0 * zv0;
+        M[S2][S2] = M[S2][S2] + wv1 * zv1;
+        M[S3][S3] = M[S3][S3] + wv2 * zv2;
+        M[S2][S1] = M[S2][S1] + wv0 * zv1;
+        M[S3][S2] = M[S3][S2] + wv1 * zv2;
+        M[S3][S1] = M[S3][S1] + wv0 * zv2;
+    } else {  // last two steps: A(k+p,k+q) += w_p z_q
+        M[S1][S1] = M[S1][S1] + wv0 * zv0;
+        if (nw >= 2) {
+            M[S2][S1] = M[S2][S1] + wv1 * zv0;
+            M[S2][S2] = M[S2][S2] + wv1 * zv1;
+        }
+    }
+    // row k+4 enters the slot of row k (columns k+1 .. k+4); its pieces were
+    // loaded one step ago, and row k+5's loads go out now
+    if (k + 4 <= c.n) {
+        cd a[4];
+        assemble_row(nxt, c.l2, c.lsq, a);
+        M[S0][S1] = a[0];
+        M[S0][S2] = a[1];
+        M[S0][S3] = a[2];
+        M[S0][S0] = a[3];
+        if (k + 5 <= c.n) load_row(c.P + (size_t)(c.it + k + 4) * 12, nxt);
+    } else {
+        M[S0][S1] = M[S0][S2] = M[S0][S3] = M[S0][S0] = mk(0.0);
+    }
+    return false;
+}
+
+// One thread per (omega, l) system: band assembly row by row and the
+// unpivoted complex-symmetric LDL^T (dcsymbdl0) streamed through the ring
+// window.  Multipliers of the rows the substitutions need go to Lst, pivots
+// of the rows at and above the source to Dst, the last ones to tail.
+__global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
+                                                   int nsys, int lmin, cd* __restrict__ Lst,
+                                                   cd* __restrict__ Dst, SysTail* __restrict__ tail) {
     int sys = blockIdx.x * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
     int w, l;
     wl_map(wl, sys, w, l);
-    const size_t bo = (size_t)w * d.ncol_tot * 4;
-    const cd *B0 = B0all + bo, *B1 = B1all + bo, *B2 = B2all + bo;
-    const double l2 = (double)l * (double)(l + 1);
-    const double lsq = sqrt(l2);
-    const int it = d.itmp, n = d.nn - it + 1;
-    const int ls = d.jsrc - it + 1;  // local row of the first source row
-    cd W[4][4];
+    FactorCtx c;
+    c.d = &d;
+    c.P = Prow + (size_t)w * (d.nn + 1) * 12;
+    c.l2 = (double)l * (double)(l + 1);
+    c.lsq = sqrt(c.l2);
+    c.it = d.itmp;
+    c.n = d.nn - c.it + 1;
+    c.ls = d.jsrc - c.it + 1;  // local row of the first source row
+    c.lmin = lmin;
+    c.nsys = nsys;
+    c.sys = sys;
+    c.Lst = Lst;
+    c.Dst = Dst;
+    cd M[4][4];
+#pragma unroll
     for (int p = 0; p < 4; ++p)
-        for (int q = 0; q < 4; ++q) W[p][q] = mk(0.0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) M[p][q] = mk(0.0);
     cd a[4];
-    for (int p = 0; p < 4 && p < n; ++p) {
-        assemble(d, it + p, B0, B1, B2, l2, lsq, a);
-        for (int q = 0; q <= p; ++q) W[p][q] = a[4 - (p - q) - 1];
+    RowPieces nxt;
+    // local rows 1..4 go to slots 1, 2, 3, 0
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        if (p >= c.n) break;
+        load_row(c.P + (size_t)(c.it + p) * 12, nxt);
+        assemble_row(nxt, c.l2, c.lsq, a);
+#pragma unroll
+        for (int q = 0; q <= p; ++q) M[(1 + p) & 3][(1 + q) & 3] = a[4 - (p - q) - 1];
     }
+    SysTail T;
     // dcsbdlv0 reads a(m-1,2) = a(2,2) of the unfactored band at row 2
-    assemble(d, it + 1, B0, B1, B2, l2, lsq, a);
-    const cd a22raw = a[1];
-    // forward-substitution state of the four source basis vectors
-    cd zs[4][3];  // z(j-3), z(j-2), z(j-1) of each basis (unscaled)
-    for (int b = 0; b < 4; ++b) zs[b][0] = zs[b][1] = zs[b][2] = mk(0.0);
-    cd wp1[3] = {mk(0.0), mk(0.0), mk(0.0)}, wp2[3] = {mk(0.0), mk(0.0), mk(0.0)};  // w of steps k-1, k-2
-    cd zcur[4];
-    for (int b = 0; b < 4; ++b) zcur[b] = mk(ls + b == 1 ? 1.0 : 0.0);  // z(1) = b(1)
-    cd Dm1 = mk(1.0), Lnn1 = mk(0.0);
-    for (int k = 1; k <= n; ++k) {
-        const cd D = W[0][0];
-        // finish z(k): scaled value zh(k) = z(k) / D(k)
-        for (int b = 0; b < 4; ++b) {
-            if (k >= ls) Zst[((size_t)(k - ls) * 4 + b) * nsys + sys] = zcur[b] / D;
-            zs[b][0] = zs[b][1];
-            zs[b][1] = zs[b][2];
-            zs[b][2] = zcur[b];
-        }
-        if (k == n) break;
-        if (k == n - 1) Dm1 = D;
-        cd piv = mk(1.0) / D;
-        int nw = min(3, n - k);
-        cd wv_[3] = {mk(0.0), mk(0.0), mk(0.0)}, zv[3] = {mk(0.0), mk(0.0), mk(0.0)};
-        for (int p = 1; p <= nw; ++p) {
-            zv[p - 1] = -W[p][0];
-            wv_[p - 1] = W[p][0] * piv;
-        }
-        if (k >= jmin_loc)
-            for (int p = 0; p < 3; ++p) Lst[((size_t)k * 3 + p) * nsys + sys] = wv_[p];
-        if (k == n - 1) Lnn1 = wv_[0];
-        if (k <= n - 3) {  // main loop of dcsymbdl0: A(k+p,k+q) += w_q z_p
-            W[1][1] = W[1][1] + wv_[0] * zv[0];
-            W[2][2] = W[2][2] + wv_[1] * zv[1];
-            W[3][3] = W[3][3] + wv_[2] * zv[2];
-            W[2][1] = W[2][1] + wv_[0] * zv[1];
-            W[3][2] = W[3][2] + wv_[1] * zv[2];
-            W[3][1] = W[3][1] + wv_[0] * zv[2];
-        } else {  // last two steps: A(k+p,k+q) += w_p z_q
-            for (int jj = 2; jj <= nw + 1; ++jj)
-                for (int ii = 2; ii <= jj; ++ii)
-                    W[jj - 1][ii - 1] = W[jj - 1][ii - 1] + wv_[jj - 2] * zv[ii - 2];
-        }
-        // shift the window and bring in row k+4
-        for (int p = 0; p < 3; ++p)
-            for (int q = 0; q <= p; ++q) W[p][q] = W[p + 1][q + 1];
-        for (int q = 0; q < 4; ++q) W[3][q] = mk(0.0);
-        if (k + 4 <= n) {
-            assemble(d, it + k + 3, B0, B1, B2, l2, lsq, a);
-            for (int q = 0; q < 4; ++q) W[3][q] = a[q];
-        }
-        // forward substitution of row j = k+1 (dcsbdlv0, m = 3)
-        int j = k + 1;
-        for (int b = 0; b < 4; ++b) {
-            if (j < ls) {  // below the source rows every z is exactly zero
-                zcur[b] = mk(0.0);
-                continue;
-            }
-            cd rhs = mk(ls + b == j ? 1.0 : 0.0);
-            if (j == 2) {
-                zcur[b] = rhs - a22raw * zs[b][2];
-            } else if (j == 3) {  // a(2,3) z(1) + a(3,3) z(2)
-                cd sum = mk(0.0) + wp1[1] * zs[b][1] + wv_[0] * zs[b][2];
-                zcur[b] = rhs - sum;
-            } else {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
-                cd sum = mk(0.0) + wp2[2] * zs[b][0] + wp1[1] * zs[b][1] + wv_[0] * zs[b][2];
-                zcur[b] = rhs - sum;
-            }
-        }
-        for (int p = 0; p < 3; ++p) { wp2[p] = wp1[p]; wp1[p] = wv_[p]; }
+    load_row(c.P + (size_t)(c.it + 1) * 12, nxt);
+    assemble_row(nxt, c.l2, c.lsq, a);
+    T.a22raw = a[1];
+    T.Dm1 = mk(1.0);
+    T.Lnn1 = mk(0.0);
+    if (5 <= c.n) load_row(c.P + (size_t)(c.it + 4) * 12, nxt);  // local row 5
+    for (int k = 1;; k += 4) {
+        if (factor_step<1>(k, M, nxt, T, c)) { T.Dn = M[1][1]; break; }
+        if (factor_step<2>(k + 1, M, nxt, T, c)) { T.Dn = M[2][2]; break; }
+        if (factor_step<3>(k + 2, M, nxt, T, c)) { T.Dn = M[3][3]; break; }
+        if (factor_step<0>(k + 3, M, nxt, T, c)) { T.Dn = M[0][0]; break; }
     }
-    tail[sys] = SysTail{W[0][0], Dm1, Lnn1};
+    tail[sys] = T;
 }
 
-// Upward substitution of the six basis right-hand sides, two threads per
-// system (three right-hand sides each; the pair reads the same factor
-// entries in the same instruction).  x(n) = zh(n); x(n-1) = zh(n-1) -
-// L(n,n-1) x(n); x(j) = zh(j) - [L(j+3,j) x(j+3) + L(j+2,j) x(j+2) +
-// L(j+1,j) x(j+1)] (dcsbdlv0's backward loop), down to the deepest
-// captured row.  Values at receiver stencil rows go to Xcap.
+// Substitutions of the six basis right-hand sides, two threads per system
+// (three bases each; the pair reads the same factor entries in the same
+// instruction).  Forward (dcsbdlv0, m = 3) from the first source row, where
+// the source bases' z start (everything below is zero), to the top, keeping
+// zh = z / D in Zst; then upward: x(n) = zh(n); x(n-1) = zh(n-1) - L(n,n-1)
+// x(n); x(j) = zh(j) - [L(j+3,j) x(j+3) + L(j+2,j) x(j+2) + L(j+1,j) x(j+1)],
+// down to the deepest captured row.  Values at receiver stencil rows go to
+// Xcap.  Bases 4 and 5 are the surface unit vectors e_{n-1}, e_n.
 __global__ void __launch_bounds__(128) k_psv_back(PsvDev d, int nsys, int jmin_loc, const int* __restrict__ capmap,
-                                                  const cd* __restrict__ Lst, const cd* __restrict__ Zst,
-                                                  const SysTail* __restrict__ tail, cd* __restrict__ Xcap) {
+                                                  const cd* __restrict__ Lst, const cd* __restrict__ Dst,
+                                                  cd* __restrict__ Zst, const SysTail* __restrict__ tail,
+                                                  cd* __restrict__ Xcap) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int sys = t >> 1, b0 = (t & 1) * 3;
     if (sys >= nsys) return;
     const int it = d.itmp, n = d.nn - it + 1;
     const int ls = d.jsrc - it + 1;
     const SysTail tl = tail[sys];
+    auto L = [&](int row, int p) { return Lst[((size_t)row * 3 + p) * nsys + sys]; };
+    // forward substitution of this thread's source bases (b < 4)
+    {
+        cd z[3][3];  // z(j-3), z(j-2), z(j-1) per basis
+        for (int k = 0; k < 3; ++k) z[k][0] = z[k][1] = z[k][2] = mk(0.0);
+        for (int j = max(ls, 1); j <= n; ++j) {
+            const cd D = Dst[(size_t)(j - ls) * nsys + sys];
+            cd l1 = mk(0.0), l2 = mk(0.0), l3 = mk(0.0);
+            if (j >= 4) { l3 = L(j - 3, 2); l2 = L(j - 2, 1); l1 = L(j - 1, 0); }
+            else if (j == 3) { l2 = L(1, 1); l1 = L(2, 0); }
+            for (int k = 0; k < 3; ++k) {
+                const int b = b0 + k;
+                if (b >= 4) break;
+                cd zc;
+                if (j == 1) {
+                    zc = mk(ls + b == 1 ? 1.0 : 0.0);
+                } else {
+                    const cd rhs = mk(ls + b == j ? 1.0 : 0.0);
+                    if (j == 2) {
+                        zc = rhs - tl.a22raw * z[k][2];
+                    } else if (j == 3) {  // a(2,3) z(1) + a(3,3) z(2)
+                        cd sum = mk(0.0) + l2 * z[k][1] + l1 * z[k][2];
+                        zc = rhs - sum;
+                    } else {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
+                        cd sum = mk(0.0) + l3 * z[k][0] + l2 * z[k][1] + l1 * z[k][2];
+                        zc = rhs - sum;
+                    }
+                }
+                Zst[((size_t)(j - ls) * 4 + b) * nsys + sys] = zc / D;
+                z[k][0] = z[k][1];
+                z[k][1] = z[k][2];
+                z[k][2] = zc;
+            }
+        }
+    }
     cd x[3][3];  // x(j+1), x(j+2), x(j+3) of this thread's three bases
     cd xn[3];
     for (int k = 0; k < 3; ++k) {
@@ -411,7 +542,7 @@ __global__ void __launch_bounds__(128) k_psv_back(PsvDev d, int nsys, int jmin_l
     for (int k = 0; k < 3; ++k) { x[k][0] = xn[k]; x[k][1] = mk(0.0); x[k][2] = mk(0.0); }
     if (n - 1 >= jmin_loc) {
         cd v[3];
-        cd L1 = Lst[((size_t)(n - 1) * 3 + 0) * nsys + sys];
+        cd L1 = L(n - 1, 0);
         for (int k = 0; k < 3; ++k) {
             const int b = b0 + k;
             cd zh = mk(0.0);
@@ -422,10 +553,20 @@ __global__ void __launch_bounds__(128) k_psv_back(PsvDev d, int nsys, int jmin_l
         capture(n - 1, v);
         for (int k = 0; k < 3; ++k) { x[k][1] = x[k][0]; x[k][0] = v[k]; }
     }
-    for (int j1 = n - 2; j1 >= jmin_loc; --j1) {
-        cd L1 = Lst[((size_t)j1 * 3 + 0) * nsys + sys];
-        cd L2 = Lst[((size_t)j1 * 3 + 1) * nsys + sys];
-        cd L3 = Lst[((size_t)j1 * 3 + 2) * nsys + sys];
+    // multipliers of row j in Lr[j & 3], loaded four rows ahead
+    cd Lr[4][3];
+    auto fetch = [&](int j, cd* dst) {
+        dst[0] = L(j, 0);
+        dst[1] = L(j, 1);
+        dst[2] = L(j, 2);
+    };
+#pragma unroll
+    for (int P = 0; P < 4; ++P) {  // slot P: the highest row <= n-2 congruent to P
+        const int j = (n - 2) - (((n - 2) - P) & 3);
+        if (j >= jmin_loc) fetch(j, Lr[P]);
+    }
+    auto row = [&](int j1, const cd* Lj) {
+        const cd L1 = Lj[0], L2 = Lj[1], L3 = Lj[2];
         cd v[3];
         for (int k = 0; k < 3; ++k) {
             const int b = b0 + k;
@@ -438,7 +579,23 @@ __global__ void __launch_bounds__(128) k_psv_back(PsvDev d, int nsys, int jmin_l
         }
         capture(j1, v);
         for (int k = 0; k < 3; ++k) { x[k][2] = x[k][1]; x[k][1] = x[k][0]; x[k][0] = v[k]; }
+    };
+    // rows in descending order; the slot a row frees takes the row four below
+#define DSM_BACK_ROW(P)                                                \
+    if ((j1 & 3) == P) {                                               \
+        if (j1 < jmin_loc) break;                                      \
+        cd Lj[3] = {Lr[P][0], Lr[P][1], Lr[P][2]};                     \
+        if (j1 - 4 >= jmin_loc) fetch(j1 - 4, Lr[P]);                  \
+        row(j1, Lj);                                                   \
+        --j1;                                                          \
     }
+    for (int j1 = n - 2;;) {
+        DSM_BACK_ROW(3)
+        DSM_BACK_ROW(2)
+        DSM_BACK_ROW(1)
+        DSM_BACK_ROW(0)
+    }
+#undef DSM_BACK_ROW
 }
 
 // ------------------------------------------------------------ l = 0 path
@@ -1222,7 +1379,7 @@ class PsvEngine : public Engine {
     DBuf<int> iphase, nlayer, kkdr, elem, hmoff, blkoff, amz, amc, bcrow, rcap, fluid, comp_src, jsta,
         capmap, l0col, l0e1;
     DBuf<double> qmu, qkappa, sel, fel, hm, bcval, poly, lam, qkp, fr, r, rrsta;
-    DBuf<cd> B0, B1, B2, Lst, Zst, Xcap, l0scr, l0d, ab, co;
+    DBuf<cd> B0, B1, B2, Prow, Lst, Zst, Dst, Xcap, l0scr, l0d, ab, co;
     DBuf<int4> rowasm;
     DBuf<SysTail> tails;
     int jmin_loc = 1, ncap = 0;
@@ -1407,8 +1564,10 @@ class PsvEngine : public Engine {
         B0.reserve((size_t)F * d.ncol_tot * 4);
         B1.reserve((size_t)F * d.ncol_tot * 4);
         B2.reserve((size_t)F * d.ncol_tot * 4);
+        Prow.reserve((size_t)F * (d.nn + 1) * 12);
         Lst.reserve((n + 1) * 3 * nsys);
         Zst.reserve((n - ls + 2) * 4 * nsys);
+        Dst.reserve((n - ls + 2) * nsys);
         Xcap.reserve((size_t)ncap * NB * nsys);
         tails.reserve(nsys);
         l0scr.reserve((size_t)F * (d.nn0 + 1) * 2);
@@ -1440,6 +1599,8 @@ class PsvEngine : public Engine {
         int id = kid("psv_omega_blocks");
         kbegin(id);
         k_psv_omega<<<grid, 128, 0, st>>>(d, fr_, B0.p, B1.p, B2.p);
+        DSM_LAUNCH(*this);
+        k_psv_rows<<<dim3((d.nn + 1 + 127) / 128, nf), 128, 0, st>>>(d, B0.p, B1.p, B2.p, Prow.p);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
         k_psv_abnum<<<(nf + 31) / 32, 32, 0, st>>>(d, fr_, nf, ab.p);
@@ -1469,11 +1630,11 @@ class PsvEngine : public Engine {
         const double alg = 2.0 * 4.0 * nrow * 16.0 + 18.0 * R * 2 * 2 * 16.0;
         int id = kid("psv_band_solve");
         kbegin(id);
-        k_psv_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, B0.p, B1.p, B2.p, wl, nsys, jmin_loc,
-                                                        capmap.p, Lst.p, Zst.p, tails.p);
+        const int lmin = std::max(1, std::min(jmin_loc, d.jsrc - d.itmp + 1 - 3));
+        k_psv_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Dst.p, tails.p);
         DSM_LAUNCH(*this);
-        k_psv_back<<<(2 * nsys + 127) / 128, 128, 0, st>>>(d, nsys, jmin_loc, capmap.p, Lst.p, Zst.p, tails.p,
-                                                           Xcap.p);
+        k_psv_back<<<(2 * nsys + 127) / 128, 128, 0, st>>>(d, nsys, jmin_loc, capmap.p, Lst.p, Dst.p, Zst.p,
+                                                           tails.p, Xcap.p);
         kend(id, alg * nsys, 0.0);
         DSM_LAUNCH(*this);
         id = kid("psv_source_coef");

@@ -40,15 +40,14 @@ def test_training_fits_a_smooth_cutoff_law(built):
     assert np.median(np.abs(pred - T[:256])) < 0.05
 
 
-def harvest_small(seeds, r0s=(6071.0, 5771.0)):
+def harvest_small(seeds, imax, freqs, r0s=(6071.0, 5771.0)):
     X, T = [], []
     for sd in seeds:
         for r0 in r0s:
-            s = dsmsgt.Setup(psv_small(seed=sd, r0=r0), "psv")
+            s = dsmsgt.Setup(psv_small(seed=sd, imax=imax, r0=r0), "psv")
             ctx = dsmsgt.Context(s)
-            fr = list(range(1, 65))
-            ll = ctx.cutoffs(fr)
-            X.append(ctx.lmax_features(fr))
+            ll = ctx.cutoffs(freqs)
+            X.append(ctx.lmax_features(freqs))
             T.append(np.log(ll).astype(np.float32))
             ctx.close()
     return np.concatenate(X), np.concatenate(T)
@@ -67,11 +66,18 @@ def test_cutoffs_only_equal_full_run(built):
 
 @pytest.mark.gpu
 def test_learned_ranges_gain_without_changing_results(built):
-    X, T = harvest_small([1, 2, 3, 4])
+    """Trained on six seeded models, evaluated on a seventh: the learned first
+    ranges solve fewer systems, and the cutoffs and every output equal the
+    plain method's.  At low frequencies the amplitude test stops far above
+    lsuf, where the plain first range (max(512, lsuf + 64)) needs extra
+    rounds; the network predicts those cutoffs."""
+    imax = 256
+    train_freqs = list(range(1, imax + 1, 8))
+    X, T = harvest_small([1, 2, 3, 4, 5, 6], imax, train_freqs)
     P = dsmsgt.lmax_init(X, T, seed=0)
-    P, losses = dsmsgt.lmax_train(X, T, P, epochs=400, batch=64, lr=2e-3)
-    s = dsmsgt.Setup(psv_small(seed=0), "psv")
-    fr = list(range(1, 65, 3))
+    P, losses = dsmsgt.lmax_train(X, T, P, epochs=300, batch=64, lr=2e-3)
+    s = dsmsgt.Setup(psv_small(seed=0, imax=imax), "psv")
+    fr = list(range(3, imax + 1, 16))
     plain = dsmsgt.Context(s, freq_batch=8)
     t0, r0, y0, l0 = plain.run(fr)
     st0 = plain.stats()
@@ -88,5 +94,5 @@ def test_learned_ranges_gain_without_changing_results(built):
     miss = float(np.mean(np.exp(pl) * lmax_data.MARGIN + lmax_data.PAD < l0))
     print(f"systems plain {st0.systems} learned {st1.systems}; padded orders {st0.orders_padded} -> "
           f"{st1.orders_padded}; miss rate {miss:.3f}; final loss {losses[-1]:.4f}")
-    assert st1.systems < st0.systems
+    assert st1.systems < 0.9 * st0.systems
     assert st1.orders_padded < st0.orders_padded
