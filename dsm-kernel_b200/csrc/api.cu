@@ -33,7 +33,11 @@ void Engine::init_common(int dev) {
     DSM_CUDA(cudaDeviceGetLimit(&stack, cudaLimitStackSize));
     if (stack < 16384) DSM_CUDA(cudaDeviceSetLimit(cudaLimitStackSize, 16384));
     DSM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    DSM_CUDA(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+    {  // the side stream carries latency-bound chains: give its blocks priority
+        int lo = 0, hi = 0;
+        DSM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        DSM_CUDA(cudaStreamCreateWithPriority(&st2, cudaStreamNonBlocking, hi));
+    }
     DSM_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     DSM_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     DSM_CUBLAS(cublasCreate(&cub));

@@ -328,13 +328,40 @@ __device__ __forceinline__ void load_row(const cd* __restrict__ P, RowPieces& r)
 #pragma unroll
     for (int i = 0; i < 12; ++i) r.v[i] = P[i];
 }
+// FAST = false: the plain path's arithmetic (separate multiply and add,
+// Smith's complex reciprocal), the reference's rounding.  FAST = true (mixed
+// precision): fused multiply-adds and a one-division reciprocal
+// conj(D) / |D|^2, still in FP64.
+template <bool FAST>
 __device__ __forceinline__ void assemble_row(const RowPieces& r, double l2, double lsq, cd a[4]) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const cd A = r.v[q], B = r.v[4 + q], C = r.v[8 + q];
-        a[q] = mk(A.re + l2 * B.re, A.im + l2 * B.im);
-        a[q] = mk(a[q].re + lsq * C.re, a[q].im + lsq * C.im);
+        if (FAST) {
+            a[q] = mk(fma(lsq, C.re, fma(l2, B.re, A.re)), fma(lsq, C.im, fma(l2, B.im, A.im)));
+        } else {
+            a[q] = mk(A.re + l2 * B.re, A.im + l2 * B.im);
+            a[q] = mk(a[q].re + lsq * C.re, a[q].im + lsq * C.im);
+        }
     }
+}
+template <bool FAST>
+__device__ __forceinline__ cd cmulT(cd a, cd b) {
+    if (FAST) return mk(fma(a.re, b.re, -a.im * b.im), fma(a.re, b.im, a.im * b.re));
+    return a * b;
+}
+template <bool FAST>
+__device__ __forceinline__ cd caddmulT(cd c, cd a, cd b) {  // c + a b
+    if (FAST) return mk(fma(a.re, b.re, fma(-a.im, b.im, c.re)), fma(a.re, b.im, fma(a.im, b.re, c.im)));
+    return c + a * b;
+}
+template <bool FAST>
+__device__ __forceinline__ cd crecipT(cd D) {
+    if (FAST) {
+        const double r = 1.0 / fma(D.re, D.re, D.im * D.im);
+        return mk(D.re * r, -D.im * r);
+    }
+    return mk(1.0) / D;
 }
 
 // last pivots and multiplier of a factorisation, for the substitution pass
@@ -356,7 +383,7 @@ struct FactorCtx {
 // row it eliminated and moves nothing.  Same operations, in the same order,
 // as the reference's band loop (main update for k <= n-3, the last two
 // steps' order otherwise).
-template <int P>
+template <int P, bool FAST>
 __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], RowPieces& nxt, SysTail& T,
                                             const FactorCtx& c) {
     constexpr int S0 = P, S1 = (P + 1) & 3, S2 = (P + 2) & 3, S3 = (P + 3) & 3;
@@ -364,18 +391,18 @@ __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], RowPieces& nxt
     if (k >= c.ls) c.Dst[(size_t)(k - c.ls) * c.nsys + c.sys] = D;
     if (k == c.n) return true;
     if (k == c.n - 1) T.Dm1 = D;
-    const cd piv = mk(1.0) / D;
+    const cd piv = crecipT<FAST>(D);
     const int nw = min(3, c.n - k);
     cd wv0, wv1 = mk(0.0), wv2 = mk(0.0), zv0, zv1 = mk(0.0), zv2 = mk(0.0);
     zv0 = -M[S1][S0];
-    wv0 = M[S1][S0] * piv;
+    wv0 = cmulT<FAST>(M[S1][S0], piv);
     if (nw >= 2) {
         zv1 = -M[S2][S0];
-        wv1 = M[S2][S0] * piv;
+        wv1 = cmulT<FAST>(M[S2][S0], piv);
     }
     if (nw >= 3) {
         zv2 = -M[S3][S0];
-        wv2 = M[S3][S0] * piv;
+        wv2 = cmulT<FAST>(M[S3][S0], piv);
     }
     if (k >= c.lmin) {
         cd* L = c.Lst + (size_t)k * 3 * c.nsys + c.sys;
@@ -385,24 +412,24 @@ __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], RowPieces& nxt
     }
     if (k == c.n - 1) T.Lnn1 = wv0;
     if (k <= c.n - 3) {  // main loop of dcsymbdl0: A(k+p,k+q) += w_q z_p
-        M[S1][S1] = M[S1][S1] + wv0 * zv0;
-        M[S2][S2] = M[S2][S2] + wv1 * zv1;
-        M[S3][S3] = M[S3][S3] + wv2 * zv2;
-        M[S2][S1] = M[S2][S1] + wv0 * zv1;
-        M[S3][S2] = M[S3][S2] + wv1 * zv2;
-        M[S3][S1] = M[S3][S1] + wv0 * zv2;
+        M[S1][S1] = caddmulT<FAST>(M[S1][S1], wv0, zv0);
+        M[S2][S2] = caddmulT<FAST>(M[S2][S2], wv1, zv1);
+        M[S3][S3] = caddmulT<FAST>(M[S3][S3], wv2, zv2);
+        M[S2][S1] = caddmulT<FAST>(M[S2][S1], wv0, zv1);
+        M[S3][S2] = caddmulT<FAST>(M[S3][S2], wv1, zv2);
+        M[S3][S1] = caddmulT<FAST>(M[S3][S1], wv0, zv2);
     } else {  // last two steps: A(k+p,k+q) += w_p z_q
-        M[S1][S1] = M[S1][S1] + wv0 * zv0;
+        M[S1][S1] = caddmulT<FAST>(M[S1][S1], wv0, zv0);
         if (nw >= 2) {
-            M[S2][S1] = M[S2][S1] + wv1 * zv0;
-            M[S2][S2] = M[S2][S2] + wv1 * zv1;
+            M[S2][S1] = caddmulT<FAST>(M[S2][S1], wv1, zv0);
+            M[S2][S2] = caddmulT<FAST>(M[S2][S2], wv1, zv1);
         }
     }
     // row k+4 enters the slot of row k (columns k+1 .. k+4); its pieces were
     // loaded one step ago, and row k+5's loads go out now
     if (k + 4 <= c.n) {
         cd a[4];
-        assemble_row(nxt, c.l2, c.lsq, a);
+        assemble_row<FAST>(nxt, c.l2, c.lsq, a);
         M[S0][S1] = a[0];
         M[S0][S2] = a[1];
         M[S0][S3] = a[2];
@@ -418,6 +445,7 @@ __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], RowPieces& nxt
 // unpivoted complex-symmetric LDL^T (dcsymbdl0) streamed through the ring
 // window.  Multipliers of the rows the substitutions need go to Lst, pivots
 // of the rows at and above the source to Dst, the last ones to tail.
+template <bool FAST>
 __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
                                                    int nsys, int lmin, cd* __restrict__ Lst,
                                                    cd* __restrict__ Dst, SysTail* __restrict__ tail) {
@@ -450,144 +478,125 @@ __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restric
     for (int p = 0; p < 4; ++p) {
         if (p >= c.n) break;
         load_row(c.P + (size_t)(c.it + p) * 12, nxt);
-        assemble_row(nxt, c.l2, c.lsq, a);
+        assemble_row<FAST>(nxt, c.l2, c.lsq, a);
 #pragma unroll
         for (int q = 0; q <= p; ++q) M[(1 + p) & 3][(1 + q) & 3] = a[4 - (p - q) - 1];
     }
     SysTail T;
     // dcsbdlv0 reads a(m-1,2) = a(2,2) of the unfactored band at row 2
     load_row(c.P + (size_t)(c.it + 1) * 12, nxt);
-    assemble_row(nxt, c.l2, c.lsq, a);
+    assemble_row<FAST>(nxt, c.l2, c.lsq, a);
     T.a22raw = a[1];
     T.Dm1 = mk(1.0);
     T.Lnn1 = mk(0.0);
     if (5 <= c.n) load_row(c.P + (size_t)(c.it + 4) * 12, nxt);  // local row 5
     for (int k = 1;; k += 4) {
-        if (factor_step<1>(k, M, nxt, T, c)) { T.Dn = M[1][1]; break; }
-        if (factor_step<2>(k + 1, M, nxt, T, c)) { T.Dn = M[2][2]; break; }
-        if (factor_step<3>(k + 2, M, nxt, T, c)) { T.Dn = M[3][3]; break; }
-        if (factor_step<0>(k + 3, M, nxt, T, c)) { T.Dn = M[0][0]; break; }
+        if (factor_step<1, FAST>(k, M, nxt, T, c)) { T.Dn = M[1][1]; break; }
+        if (factor_step<2, FAST>(k + 1, M, nxt, T, c)) { T.Dn = M[2][2]; break; }
+        if (factor_step<3, FAST>(k + 2, M, nxt, T, c)) { T.Dn = M[3][3]; break; }
+        if (factor_step<0, FAST>(k + 3, M, nxt, T, c)) { T.Dn = M[0][0]; break; }
     }
     tail[sys] = T;
 }
 
-// Substitutions of the six basis right-hand sides, two threads per system
-// (three bases each; the pair reads the same factor entries in the same
-// instruction).  Forward (dcsbdlv0, m = 3) from the first source row, where
-// the source bases' z start (everything below is zero), to the top, keeping
-// zh = z / D in Zst; then upward: x(n) = zh(n); x(n-1) = zh(n-1) - L(n,n-1)
-// x(n); x(j) = zh(j) - [L(j+3,j) x(j+3) + L(j+2,j) x(j+2) + L(j+1,j) x(j+1)],
-// down to the deepest captured row.  Values at receiver stencil rows go to
-// Xcap.  Bases 4 and 5 are the surface unit vectors e_{n-1}, e_n.
+// Substitutions of the six basis right-hand sides, one thread per (system,
+// basis); the six threads of a system read the same factor entries in the
+// same instruction.  Forward (dcsbdlv0, m = 3) from the first source row,
+// where the source bases' z start (everything below is zero), to the top,
+// keeping zh = z / D in Zst; then upward: x(n) = zh(n); x(n-1) = zh(n-1) -
+// L(n,n-1) x(n); x(j) = zh(j) - [L(j+3,j) x(j+3) + L(j+2,j) x(j+2) +
+// L(j+1,j) x(j+1)], down to the deepest captured row, with the multipliers
+// loaded four rows ahead.  Values at receiver stencil rows go to Xcap.
+// Bases 4 and 5 are the surface unit vectors e_{n-1}, e_n.
 __global__ void __launch_bounds__(128) k_psv_back(PsvDev d, int nsys, int jmin_loc, const int* __restrict__ capmap,
                                                   const cd* __restrict__ Lst, const cd* __restrict__ Dst,
                                                   cd* __restrict__ Zst, const SysTail* __restrict__ tail,
                                                   cd* __restrict__ Xcap) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int sys = t >> 1, b0 = (t & 1) * 3;
+    const int sys = t / NB, b = t - sys * NB;
     if (sys >= nsys) return;
     const int it = d.itmp, n = d.nn - it + 1;
     const int ls = d.jsrc - it + 1;
-    const SysTail tl = tail[sys];
     auto L = [&](int row, int p) { return Lst[((size_t)row * 3 + p) * nsys + sys]; };
-    // forward substitution of this thread's source bases (b < 4)
-    {
-        cd z[3][3];  // z(j-3), z(j-2), z(j-1) per basis
-        for (int k = 0; k < 3; ++k) z[k][0] = z[k][1] = z[k][2] = mk(0.0);
+    auto ZH = [&](int row) { return Zst[((size_t)(row - ls) * 4 + b) * nsys + sys]; };
+    if (b < 4) {  // forward substitution of a source basis
+        const cd a22raw = tail[sys].a22raw;
+        cd z0 = mk(0.0), z1 = mk(0.0), z2 = mk(0.0);  // z(j-3), z(j-2), z(j-1)
         for (int j = max(ls, 1); j <= n; ++j) {
             const cd D = Dst[(size_t)(j - ls) * nsys + sys];
-            cd l1 = mk(0.0), l2 = mk(0.0), l3 = mk(0.0);
-            if (j >= 4) { l3 = L(j - 3, 2); l2 = L(j - 2, 1); l1 = L(j - 1, 0); }
-            else if (j == 3) { l2 = L(1, 1); l1 = L(2, 0); }
-            for (int k = 0; k < 3; ++k) {
-                const int b = b0 + k;
-                if (b >= 4) break;
-                cd zc;
-                if (j == 1) {
-                    zc = mk(ls + b == 1 ? 1.0 : 0.0);
-                } else {
-                    const cd rhs = mk(ls + b == j ? 1.0 : 0.0);
-                    if (j == 2) {
-                        zc = rhs - tl.a22raw * z[k][2];
-                    } else if (j == 3) {  // a(2,3) z(1) + a(3,3) z(2)
-                        cd sum = mk(0.0) + l2 * z[k][1] + l1 * z[k][2];
-                        zc = rhs - sum;
-                    } else {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
-                        cd sum = mk(0.0) + l3 * z[k][0] + l2 * z[k][1] + l1 * z[k][2];
-                        zc = rhs - sum;
-                    }
+            cd zc;
+            if (j == 1) {
+                zc = mk(ls + b == 1 ? 1.0 : 0.0);
+            } else {
+                const cd rhs = mk(ls + b == j ? 1.0 : 0.0);
+                if (j == 2) {
+                    zc = rhs - a22raw * z2;
+                } else if (j == 3) {  // a(2,3) z(1) + a(3,3) z(2)
+                    cd sum = mk(0.0) + L(1, 1) * z1 + L(2, 0) * z2;
+                    zc = rhs - sum;
+                } else {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
+                    cd sum = mk(0.0) + L(j - 3, 2) * z0 + L(j - 2, 1) * z1 + L(j - 1, 0) * z2;
+                    zc = rhs - sum;
                 }
-                Zst[((size_t)(j - ls) * 4 + b) * nsys + sys] = zc / D;
-                z[k][0] = z[k][1];
-                z[k][1] = z[k][2];
-                z[k][2] = zc;
             }
+            Zst[((size_t)(j - ls) * 4 + b) * nsys + sys] = zc / D;
+            z0 = z1;
+            z1 = z2;
+            z2 = zc;
         }
     }
-    cd x[3][3];  // x(j+1), x(j+2), x(j+3) of this thread's three bases
-    cd xn[3];
-    for (int k = 0; k < 3; ++k) {
-        const int b = b0 + k;
-        if (b < 4) xn[k] = (n >= ls) ? Zst[((size_t)(n - ls) * 4 + b) * nsys + sys] : mk(0.0);
-        // surface basis: e_{n-1}: z(n-1) = 1, z(n) = -L(n,n-1); e_n: z(n) = 1
-        else if (b == 4) xn[k] = (mk(0.0) - tl.Lnn1 * mk(1.0)) / tl.Dn;
-        else xn[k] = mk(1.0) / tl.Dn;
-    }
-    auto capture = [&](int jloc, const cd* v) {
-        int c = capmap[jloc + it - 1];
-        if (c >= 0)
-            for (int k = 0; k < 3; ++k) Xcap[((size_t)c * NB + b0 + k) * nsys + sys] = v[k];
+    const SysTail tl = tail[sys];
+    cd xn;
+    if (b < 4) xn = (n >= ls) ? ZH(n) : mk(0.0);
+    // surface basis: e_{n-1}: z(n-1) = 1, z(n) = -L(n,n-1); e_n: z(n) = 1
+    else if (b == 4) xn = (mk(0.0) - tl.Lnn1 * mk(1.0)) / tl.Dn;
+    else xn = mk(1.0) / tl.Dn;
+    auto capture = [&](int jloc, cd v) {
+        const int c = capmap[jloc + it - 1];
+        if (c >= 0) Xcap[((size_t)c * NB + b) * nsys + sys] = v;
     };
     capture(n, xn);
-    for (int k = 0; k < 3; ++k) { x[k][0] = xn[k]; x[k][1] = mk(0.0); x[k][2] = mk(0.0); }
+    cd x0 = xn, x1 = mk(0.0), x2 = mk(0.0);  // x(j+1), x(j+2), x(j+3)
     if (n - 1 >= jmin_loc) {
-        cd v[3];
-        cd L1 = L(n - 1, 0);
-        for (int k = 0; k < 3; ++k) {
-            const int b = b0 + k;
-            cd zh = mk(0.0);
-            if (b < 4 && n - 1 >= ls) zh = Zst[((size_t)(n - 1 - ls) * 4 + b) * nsys + sys];
-            if (b == 4) zh = mk(1.0) / tl.Dm1;
-            v[k] = zh - L1 * x[k][0];
-        }
+        cd zh = mk(0.0);
+        if (b < 4 && n - 1 >= ls) zh = ZH(n - 1);
+        if (b == 4) zh = mk(1.0) / tl.Dm1;
+        const cd v = zh - L(n - 1, 0) * x0;
         capture(n - 1, v);
-        for (int k = 0; k < 3; ++k) { x[k][1] = x[k][0]; x[k][0] = v[k]; }
+        x1 = x0;
+        x0 = v;
     }
     // multipliers of row j in Lr[j & 3], loaded four rows ahead
     cd Lr[4][3];
-    auto fetch = [&](int j, cd* dst) {
-        dst[0] = L(j, 0);
-        dst[1] = L(j, 1);
-        dst[2] = L(j, 2);
-    };
 #pragma unroll
     for (int P = 0; P < 4; ++P) {  // slot P: the highest row <= n-2 congruent to P
         const int j = (n - 2) - (((n - 2) - P) & 3);
-        if (j >= jmin_loc) fetch(j, Lr[P]);
+        if (j >= jmin_loc) { Lr[P][0] = L(j, 0); Lr[P][1] = L(j, 1); Lr[P][2] = L(j, 2); }
     }
-    auto row = [&](int j1, const cd* Lj) {
-        const cd L1 = Lj[0], L2 = Lj[1], L3 = Lj[2];
-        cd v[3];
-        for (int k = 0; k < 3; ++k) {
-            const int b = b0 + k;
-            cd zh = mk(0.0);
-            if (b < 4 && j1 >= ls) zh = Zst[((size_t)(j1 - ls) * 4 + b) * nsys + sys];
-            cd sum;
-            if (j1 == n - 2) sum = mk(0.0) + L2 * x[k][1] + L1 * x[k][0];
-            else sum = mk(0.0) + L3 * x[k][2] + L2 * x[k][1] + L1 * x[k][0];
-            v[k] = zh - sum;
-        }
+    auto row = [&](int j1, cd L1, cd L2, cd L3) {
+        cd zh = mk(0.0);
+        if (b < 4 && j1 >= ls) zh = ZH(j1);
+        cd sum;
+        if (j1 == n - 2) sum = mk(0.0) + L2 * x1 + L1 * x0;
+        else sum = mk(0.0) + L3 * x2 + L2 * x1 + L1 * x0;
+        const cd v = zh - sum;
         capture(j1, v);
-        for (int k = 0; k < 3; ++k) { x[k][2] = x[k][1]; x[k][1] = x[k][0]; x[k][0] = v[k]; }
+        x2 = x1;
+        x1 = x0;
+        x0 = v;
     };
     // rows in descending order; the slot a row frees takes the row four below
-#define DSM_BACK_ROW(P)                                                \
-    if ((j1 & 3) == P) {                                               \
-        if (j1 < jmin_loc) break;                                      \
-        cd Lj[3] = {Lr[P][0], Lr[P][1], Lr[P][2]};                     \
-        if (j1 - 4 >= jmin_loc) fetch(j1 - 4, Lr[P]);                  \
-        row(j1, Lj);                                                   \
-        --j1;                                                          \
+#define DSM_BACK_ROW(P)                                                           \
+    if ((j1 & 3) == P) {                                                          \
+        if (j1 < jmin_loc) break;                                                 \
+        const cd L1 = Lr[P][0], L2 = Lr[P][1], L3 = Lr[P][2];                     \
+        if (j1 - 4 >= jmin_loc) {                                                 \
+            Lr[P][0] = L(j1 - 4, 0);                                              \
+            Lr[P][1] = L(j1 - 4, 1);                                              \
+            Lr[P][2] = L(j1 - 4, 2);                                              \
+        }                                                                         \
+        row(j1, L1, L2, L3);                                                      \
+        --j1;                                                                     \
     }
     for (int j1 = n - 2;;) {
         DSM_BACK_ROW(3)
@@ -633,8 +642,9 @@ __global__ void k_psv_l0_build(PsvDev d, const cd* __restrict__ B0all, const cd*
 // tridiagonal through shared memory in chunks (coalesced loads and stores
 // by all threads) so that the chains run on shared-memory latency: thread 0
 // factors a chunk, threads 0..3 then carry one right-hand side each.
-constexpr int L0_CH = 384;  // rows per chunk (12 KB factor + 24 KB solution)
+constexpr int L0_CH = 256;  // rows per chunk (3 x 8 KB factor stages + 16 KB solution)
 
+template <bool FAST>
 __global__ void __launch_bounds__(128) k_psv_l0_solve(PsvDev d, const int* __restrict__ freqs, int nf,
                                                       const cd* __restrict__ ab, cd* __restrict__ Cc,
                                                       cd* __restrict__ Dv, int back) {
@@ -643,7 +653,7 @@ __global__ void __launch_bounds__(128) k_psv_l0_solve(PsvDev d, const int* __res
     const int n0 = d.nn0, it0 = d.itmp0, tid = threadIdx.x;
     cd* C = Cc + (size_t)w * (n0 + 1) * 2;
     cd* D = Dv + (size_t)w * (n0 + 1) * 4;
-    __shared__ cd sC[L0_CH][2];
+    __shared__ cd sC[3][L0_CH][2];
     __shared__ cd sD[L0_CH][4];
     __shared__ int srr[5];
     __shared__ cd srv[5][4];
@@ -687,51 +697,70 @@ __global__ void __launch_bounds__(128) k_psv_l0_solve(PsvDev d, const int* __res
     };
     // forward: factor step k = g-1 (piv = 1/c(2,k); w2 = c(1,k+1) piv;
     // c(2,k+1) += w2 (-c(1,k+1))), then z(k) = z(k)/c(2,k) and
-    // z(g) = b(g) - c(1,g) z(g-1) for each right-hand side
+    // z(g) = b(g) - c(1,g) z(g-1) for each right-hand side.  Three-stage
+    // pipeline over chunks: in phase p warps 2-3 store chunk p-3 and load
+    // chunk p, thread 0 (warp 0) factors chunk p-1 and threads 32..35
+    // (warp 1) carry the right-hand sides through chunk p-2.
     cd dfac = C[2 * it0 + 1];      // thread 0: running pivot
-    cd zb = mk(0.0), db = dfac;    // threads 0..3: z and pivot of the previous row
-    if (tid < 4) zb = rhs(it0, tid);
-    for (int g0 = it0 + 1; g0 <= n0; g0 += L0_CH) {
-        const int cnt = min(L0_CH, n0 + 1 - g0);
-        for (int i = tid; i < 2 * cnt; i += blockDim.x) sC[i >> 1][i & 1] = C[2 * g0 + i];
-        __syncthreads();
-        if (tid == 0) {
-            for (int i = 0; i < cnt; ++i) {
-                cd piv = mk(1.0) / dfac;
-                cd off = sC[i][0];
-                cd z2 = -off;
-                cd w2 = off * piv;
-                cd dg = sC[i][1] + w2 * z2;
-                sC[i][0] = w2;
-                sC[i][1] = dg;
-                dfac = dg;
+    cd zb = mk(0.0), db = dfac;    // threads 32..35: z and pivot of the previous row
+    const int rt = tid - 32;       // right-hand side of threads 32..35
+    if (rt >= 0 && rt < 4) zb = rhs(it0, rt);
+    const int nch = (n0 - it0 + L0_CH - 1) / L0_CH;  // chunks of rows it0+1 .. n0
+    auto chunk_g0 = [&](int c) { return it0 + 1 + c * L0_CH; };
+    auto chunk_cnt = [&](int c) { return min(L0_CH, n0 + 1 - chunk_g0(c)); };
+    for (int p = 0; p < nch + 3; ++p) {
+        if (tid >= 64) {
+            const int lt = tid - 64, nl = blockDim.x - 64;
+            if (p - 3 >= 0 && p - 3 < nch) {  // chunk p-3 is final: back to global
+                const int c = p - 3, g0 = chunk_g0(c), cnt = chunk_cnt(c);
+                for (int i = lt; i < 2 * cnt; i += nl) C[2 * g0 + i] = sC[c % 3][i >> 1][i & 1];
+            }
+            if (p < nch) {
+                const int g0 = chunk_g0(p), cnt = chunk_cnt(p);
+                for (int i = lt; i < 2 * cnt; i += nl) sC[p % 3][i >> 1][i & 1] = C[2 * g0 + i];
+            }
+        } else if (tid == 0) {
+            if (p - 1 >= 0 && p - 1 < nch) {
+                const int c = p - 1, cnt = chunk_cnt(c);
+                cd(*sc)[2] = sC[c % 3];
+                for (int i = 0; i < cnt; ++i) {
+                    cd piv = crecipT<FAST>(dfac);
+                    cd off = sc[i][0];
+                    cd z2 = -off;
+                    cd w2 = cmulT<FAST>(off, piv);
+                    cd dg = caddmulT<FAST>(sc[i][1], w2, z2);
+                    sc[i][0] = w2;
+                    sc[i][1] = dg;
+                    dfac = dg;
+                }
+            }
+        } else if (rt >= 0 && rt < 4) {
+            if (p - 2 >= 0 && p - 2 < nch) {
+                const int c = p - 2, g0 = chunk_g0(c), cnt = chunk_cnt(c);
+                cd(*sc)[2] = sC[c % 3];
+                for (int i = 0; i < cnt; ++i) {
+                    const int g = g0 + i;
+                    D[4 * (g - 1) + rt] = FAST ? cmulT<true>(zb, crecipT<true>(db)) : zb / db;
+                    zb = FAST ? caddmulT<true>(rhs(g, rt), -sc[i][0], zb) : rhs(g, rt) - sc[i][0] * zb;
+                    db = sc[i][1];
+                }
             }
         }
-        __syncthreads();
-        if (tid < 4) {
-            for (int i = 0; i < cnt; ++i) {
-                const int g = g0 + i;
-                D[4 * (g - 1) + tid] = zb / db;
-                zb = rhs(g, tid) - sC[i][0] * zb;
-                db = sC[i][1];
-            }
-        }
-        for (int i = tid; i < 2 * cnt; i += blockDim.x) C[2 * g0 + i] = sC[i >> 1][i & 1];
         __syncthreads();
     }
-    if (tid < 4) D[4 * n0 + tid] = zb / db;
+    if (rt >= 0 && rt < 4) D[4 * n0 + rt] = zb / db;
     __syncthreads();
     // upward substitution x(g) = z(g) - c(1,g+1) x(g+1), g = n0-1 .. it0
     cd x = mk(0.0);
     if (tid < 4) x = D[4 * n0 + tid];
     for (int ghi = n0 - 1; ghi >= it0; ghi -= L0_CH) {
         const int glo = max(it0, ghi - L0_CH + 1), cnt = ghi - glo + 1;
-        for (int i = tid; i < cnt; i += blockDim.x) sC[i][0] = C[2 * (glo + i + 1)];
+        for (int i = tid; i < cnt; i += blockDim.x) sC[0][i][0] = C[2 * (glo + i + 1)];
         for (int i = tid; i < 4 * cnt; i += blockDim.x) sD[i >> 2][i & 3] = D[4 * glo + i];
         __syncthreads();
         if (tid < 4) {
             for (int i = cnt - 1; i >= 0; --i) {
-                x = sD[i][tid] - sC[i][0] * x;
+                x = sD[i][tid] - sC[0][i][0] * x;
                 sD[i][tid] = x;
             }
         }
@@ -1616,7 +1645,8 @@ class PsvEngine : public Engine {
             kbegin(id0, st2);
             k_psv_l0_build<<<dim3((d.nn0 + 127) / 128, nf), 128, 0, st2>>>(d, B0.p, B1.p, B2.p, l0col.p,
                                                                             l0e1.p, l0scr.p);
-            k_psv_l0_solve<<<nf, 128, 0, st2>>>(d, fr_, nf, ab.p, l0scr.p, l0d.p, rsgt_sw);
+            if (mixed()) k_psv_l0_solve<true><<<nf, 128, 0, st2>>>(d, fr_, nf, ab.p, l0scr.p, l0d.p, rsgt_sw);
+            else k_psv_l0_solve<false><<<nf, 128, 0, st2>>>(d, fr_, nf, ab.p, l0scr.p, l0d.p, rsgt_sw);
             k_psv_l0_fields<<<dim3((R + 1 + 127) / 128, nf), 128, 0, st2>>>(d, l0d.p, Afld[0].p, Afld[1].p,
                                                                              Afld[2].p, Lcap, rsgt_sw);
             kend(id0, 0.0, 0.0, st2);
@@ -1631,10 +1661,15 @@ class PsvEngine : public Engine {
         int id = kid("psv_band_solve");
         kbegin(id);
         const int lmin = std::max(1, std::min(jmin_loc, d.jsrc - d.itmp + 1 - 3));
-        k_psv_solve<<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Dst.p, tails.p);
+        if (mixed())
+            k_psv_solve<true><<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Dst.p,
+                                                                  tails.p);
+        else
+            k_psv_solve<false><<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Dst.p,
+                                                                   tails.p);
         DSM_LAUNCH(*this);
-        k_psv_back<<<(2 * nsys + 127) / 128, 128, 0, st>>>(d, nsys, jmin_loc, capmap.p, Lst.p, Dst.p, Zst.p,
-                                                           tails.p, Xcap.p);
+        k_psv_back<<<(NB * nsys + 127) / 128, 128, 0, st>>>(d, nsys, jmin_loc, capmap.p, Lst.p, Dst.p, Zst.p,
+                                                            tails.p, Xcap.p);
         kend(id, alg * nsys, 0.0);
         DSM_LAUNCH(*this);
         id = kid("psv_source_coef");
