@@ -42,25 +42,46 @@ METRIC = "SGT freq-slices/s at rel-L2<=1e-6 vs FP64; speedup over plain FP64 GPU
 UNIT = "freq-slices/s"
 
 
-def workload(mode: str):
+WORKLOADS = {
+    # P-SV on the GPU (the FP64 configuration; default)
+    "psv1024": dict(mode="psv", tlen=3276.8, imax=1024, thdelta=0.25, rdelta=26.75, rmin=1000.0,
+                    rmax=6350.0, r0=6071.0, thetas=721),
+    # its mixed-precision form at twice the band (lmax ~5000-7000, 1441 distances)
+    "psv2048": dict(mode="psv", tlen=3276.8, imax=2048, thdelta=0.125, rdelta=26.75, rmin=1000.0,
+                    rmax=6350.0, r0=6071.0, thetas=1441),
+    # SH (the reference's CPU configuration)
+    "sh256": dict(mode="sh", tlen=1638.4, imax=256, thdelta=0.5, rdelta=28.5, rmin=3500.0,
+                  rmax=6321.5, r0=6271.0, thetas=361),
+}
+
+
+def workload(name: str):
+    """Job (parameter file, DSM.config, model) and description of a workload."""
     import dsmsgt
     from dsmsgt import synth
-    if mode == "psv":
-        job = dsmsgt.Job(
-            synth.param_file(tlen=3276.8, rmin=1000.0, rmax=6350.0, rdelta=26.75, r0=6071.0,
-                             thmin=0.0, thmax=180.0, thdelta=0.25, imin=0, imax=1024),
-            synth.dsm_config(), synth.psv_earth_model(0))
-        desc = {"workload": "SGTpsv synthetic Earth (IC solid, OC fluid, 6 mantle/crust zones, seed 0)",
-                "tlen_s": 3276.8, "np": 1024, "source_depth_km": 300, "receivers": 201,
-                "thetas": 721}
+    name = {"psv": "psv1024", "sh": "sh256"}.get(name, name)
+    w = WORKLOADS[name]
+    model = synth.psv_earth_model(0) if w["mode"] == "psv" else synth.sh_mantle_model(0)
+    job = dsmsgt.Job(
+        synth.param_file(tlen=w["tlen"], rmin=w["rmin"], rmax=w["rmax"], rdelta=w["rdelta"], r0=w["r0"],
+                         thmin=0.0, thmax=180.0, thdelta=w["thdelta"], imin=0, imax=w["imax"]),
+        synth.dsm_config(), model)
+    nrec = int(round((w["rmax"] - w["rmin"]) / w["rdelta"])) + 1
+    if w["mode"] == "psv":
+        what = "SGTpsv synthetic Earth (IC solid, OC fluid, 6 mantle/crust zones, seed 0)"
     else:
-        job = dsmsgt.Job(
-            synth.param_file(tlen=1638.4, rmin=3500.0, rmax=6321.5, rdelta=28.5, r0=6271.0,
-                             thmin=0.0, thmax=180.0, thdelta=0.5, imin=0, imax=256),
-            synth.dsm_config(), synth.sh_mantle_model(0))
-        desc = {"workload": "SGTsh synthetic mantle (5 solid zones, seed 0)", "tlen_s": 1638.4,
-                "np": 256, "source_depth_km": 100, "receivers": 100, "thetas": 361}
+        what = "SGTsh synthetic mantle (5 solid zones, seed 0)"
+    desc = {"workload": what, "name": name, "tlen_s": w["tlen"], "np": w["imax"],
+            "source_depth_km": round(6371.0 - w["r0"]), "receivers": nrec, "thetas": w["thetas"]}
     return job, desc
+
+
+def workload_mode(name: str) -> str:
+    return WORKLOADS[{"psv": "psv1024", "sh": "sh256"}.get(name, name)]["mode"]
+
+
+def workload_imax(name: str) -> int:
+    return WORKLOADS[{"psv": "psv1024", "sh": "sh256"}.get(name, name)]["imax"]
 
 
 def per_component_rel_l2(a, b):
@@ -76,10 +97,11 @@ def per_component_rel_l2(a, b):
     return out
 
 
-def load_lmax_params(mode: str):
-    """Trained parameter block of the learned cutoff (written by
-    dsmsgt.lmax_data), or None."""
-    path = os.path.join(REPO, "dsm-kernel_b200", "dsmsgt", f"lmax_{mode}.f32")
+def load_lmax_params(name: str):
+    """Trained parameter block of the learned cutoff for a workload (written
+    by dsmsgt.lmax_data for that workload's band and grid), or None."""
+    name = {"psv": "psv1024", "sh": "sh256"}.get(name, name)
+    path = os.path.join(REPO, "dsm-kernel_b200", "dsmsgt", f"lmax_{name}.f32")
     if not os.path.exists(path):
         return None
     p = np.fromfile(path, dtype=np.float32)
@@ -156,10 +178,11 @@ def cpu_baseline(setup_mode: str, freqs: list[int], threads: int, slope: float |
     job, desc = workload(setup_mode)
     times = {}
     grids = ((30.0, 7),) if slope is not None else ((30.0, 7), (15.0, 13))
+    w = WORKLOADS[desc["name"]]
     for thd, nth in grids:
-        text = job.param_text.replace(" 0.25\n", f" {thd}\n").replace(" 0.5\n", f" {thd}\n")
+        text = job.param_text.replace(f" {w['thdelta']!r}\n", f" {thd}\n")
         sjob = dsmsgt.Job(text, job.conf_text, job.model_text)
-        s = dsmsgt.Setup(sjob, setup_mode)
+        s = dsmsgt.Setup(sjob, w["mode"])
         assert s.theta_n == nth, (s.theta_n, nth)
         t0 = time.perf_counter()
         orc.run(s, freqs, threads=threads)
@@ -177,7 +200,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--mode", default="psv", choices=["psv", "sh"])
+    ap.add_argument("--workload", "--mode", dest="mode", default="psv1024",
+                    choices=["psv1024", "psv2048", "sh256", "psv", "sh"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_bf16"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-lmax", dest="lmax", action="store_false", help="plain first order ranges")
@@ -188,7 +212,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    imax = 1024 if args.mode == "psv" else 256
+    imax = workload_imax(args.mode)
+    mode = workload_mode(args.mode)
 
     if args.impl == "reference":
         if rank != 0:
@@ -231,7 +256,7 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     dev = local
     job, desc = workload(args.mode)
-    setup = dsmsgt.Setup(job, args.mode)
+    setup = dsmsgt.Setup(job, mode)
     lmax_params = load_lmax_params(args.mode) if args.lmax else None
 
     def barrier():

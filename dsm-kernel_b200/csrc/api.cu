@@ -377,17 +377,18 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
         std::vector<int> hf(ilist + b0, ilist + b0 + nf);
         for (int w = 0; w < nf; ++w) span[w] = first_span(hf[w]);
         if (opt.use_lmax_predictor && pred.ready && opt.l_chunk <= 0) {
-            // the learned cutoff with a 5% margin; never below lsuf, where
-            // the amplitude test cannot yet stop
+            // the network predicts log(lmax) - f0, f0 = log(1 + omega rtop /
+            // vtop) (the lsuf scale); first range = lmax * 1.02 + 24, never
+            // below lsuf + 8 (the amplitude test cannot stop before lsuf)
             std::vector<float> f((size_t)nf * DSM_LMAX_NFEAT), lp(nf);
             lmax_features(hf.data(), nf, f.data());
             pred.predict(f.data(), nf, lp.data(), st);
             for (int w = 0; w < nf; ++w) {
                 const double omega = 2.0 * kPi * (double)hf[w] / tlen;
                 const int lsuf = (int)(omega * rtop_ / vtop_ - 0.5) + 1;
-                const double pl = std::exp((double)lp[w]);
-                int sp = (int)std::ceil(std::min(pl * 1.05 + 16.0, (double)maxlmax + 1.0));
-                sp = std::max(sp, lsuf + 32);
+                const double pl = std::exp((double)lp[w] + (double)f[(size_t)w * DSM_LMAX_NFEAT]);
+                int sp = (int)std::ceil(std::min(pl * 1.02 + 24.0, (double)maxlmax + 1.0));
+                sp = std::max(sp, lsuf + 8);
                 span[w] = (sp + 31) / 32 * 32;
             }
         }
@@ -668,12 +669,12 @@ extern "C" int dsm_lmax_init(const float* feats, const float* target, int n, uns
 }
 
 extern "C" int dsm_lmax_train(const float* feats, const float* target, int n, int epochs, int batch, float lr,
-                              unsigned seed, float* params, float* losses, int device) {
+                              float weight_decay, unsigned seed, float* params, float* losses, int device) {
     if (!feats || !target || !params || n <= 0) return DSM_ERR_INVALID;
     int rc = check_device(device);
     if (rc) return rc;
     return guarded(nullptr, [&] {
-        dsm::lmax::train(feats, target, n, epochs, batch, lr, seed, params, losses, device);
+        dsm::lmax::train(feats, target, n, epochs, batch, lr, weight_decay, seed, params, losses, device);
     });
 }
 
@@ -700,6 +701,7 @@ extern "C" int dsm_lmax_predict(dsm_ctx_t* ctx, const int* ilist, int n, float* 
         std::vector<float> f((size_t)n * DSM_LMAX_NFEAT);
         ctx->eng->lmax_features(ilist, n, f.data());
         ctx->eng->pred.predict(f.data(), n, out, ctx->eng->st);
+        for (int k = 0; k < n; ++k) out[k] += f[(size_t)k * DSM_LMAX_NFEAT];  // log(lmax)
     });
 }
 

@@ -106,9 +106,9 @@ class Engine {
     // mixed precision: the l-sum as split 16-bit products on the tensor
     // cores (fields and bases split once per batch / per table build)
     bool mixed() const { return opt.precision == DSM_PREC_MIXED || opt.precision == DSM_PREC_MIXED_BF16; }
-    int tc_fmt = tc::PIECE_F16, tc_bk = 32, nsm = 148;
+    int tc_fmt = tc::PIECE_F16, tc_bk = 64, nsm = 148;
     uint32_t tc_flags = tc::TC_REVERSE;
-    int tc_chunk = tc::TC_CHUNK;
+    int tc_chunk = 1;                // stages (of tc_bk orders) per hi*hi chunk: 64 orders
     int kcA = 0, kcB = 0;            // order capacities of the pieces (x64)
     DBuf<uint16_t> Apc[3];           // [2][F][rows][kcA]
     DBuf<float> sA[3];               // [F][rows]

@@ -189,7 +189,8 @@ __global__ void k_wgrad(int layer, const float* __restrict__ Xn, const float* __
 
 // Adam on the weights and biases (the normalisation block is not trained)
 __global__ void k_adam(float* __restrict__ P, const float* __restrict__ G, float* __restrict__ m1,
-                       float* __restrict__ m2, int* __restrict__ step, float lr, __nv_bfloat16* __restrict__ Pb) {
+                       float* __restrict__ m2, int* __restrict__ step, float lr, float wd,
+                       __nv_bfloat16* __restrict__ Pb) {
     const int i = OFF_W1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int t = *step + 1;
     if (i < DSM_LMAX_NPARAM) {
@@ -199,7 +200,9 @@ __global__ void k_adam(float* __restrict__ P, const float* __restrict__ G, float
         m1[i] = a;
         m2[i] = b;
         const float ah = a / (1.0f - powf(b1, (float)t)), bh = b / (1.0f - powf(b2, (float)t));
-        P[i] -= lr * ah / (sqrtf(bh) + 1e-8f);
+        // decoupled weight decay (AdamW) keeps the network from leaning on
+        // inputs that hardly vary between the training models
+        P[i] -= lr * (ah / (sqrtf(bh) + 1e-8f) + wd * P[i]);
         Pb[i] = __float2bfloat16_rn(P[i]);
     }
 }
@@ -266,8 +269,8 @@ void init_params(const float* X, const float* T, int n, unsigned seed, float* P)
     fill(OFF_W4, 1, H);
 }
 
-void train(const float* X, const float* T, int n, int epochs, int batch, float lr, unsigned seed, float* P,
-           float* losses, int device) {
+void train(const float* X, const float* T, int n, int epochs, int batch, float lr, float wd, unsigned seed,
+           float* P, float* losses, int device) {
     if (n <= 0 || batch <= 0 || epochs <= 0) throw Error(DSM_ERR_INVALID, "empty training set");
     DSM_CUDA(cudaSetDevice(device));
     cudaStream_t st;
@@ -307,7 +310,7 @@ void train(const float* X, const float* T, int n, int epochs, int batch, float l
     DSM_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     {
         grad_step(net, cur.p, batch, lossacc.p, st);
-        k_adam<<<nadam, 256, 0, st>>>(net.P.p, net.G.p, net.m1.p, net.m2.p, net.step.p, lr, net.Pb.p);
+        k_adam<<<nadam, 256, 0, st>>>(net.P.p, net.G.p, net.m1.p, net.m2.p, net.step.p, lr, wd, net.Pb.p);
         k_step<<<1, 1, 0, st>>>(net.step.p);
     }
     DSM_CUDA(cudaStreamEndCapture(st, &graph));

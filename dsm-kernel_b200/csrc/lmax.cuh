@@ -20,10 +20,10 @@ static_assert(OFF_B4 + 1 == DSM_LMAX_NPARAM, "parameter block layout");
 
 // standardisation from the data, He-initialised weights
 void init_params(const float* X, const float* T, int n, unsigned seed, float* P);
-// Adam on the GPU; P in/out; losses[epochs] (mean squared error of the
-// standardised log lmax per epoch)
-void train(const float* X, const float* T, int n, int epochs, int batch, float lr, unsigned seed, float* P,
-           float* losses, int device);
+// AdamW on the GPU (weight decay wd); P in/out; losses[epochs] (mean
+// squared error of the standardised target per epoch)
+void train(const float* X, const float* T, int n, int epochs, int batch, float lr, float wd, unsigned seed,
+           float* P, float* losses, int device);
 // loss and gradient of one batch (the first n rows), for checks
 void grad(const float* P, const float* X, const float* T, int n, float* G, float* loss, int device);
 

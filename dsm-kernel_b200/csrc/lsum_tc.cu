@@ -136,6 +136,15 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
+__device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -302,24 +311,51 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             double acc[64];
 #pragma unroll
             for (int j = 0; j < 64; ++j) acc[j] = 0.0;
-            for (int c = 0; c < nch; ++c, ++cc) {
-                const int hb = cc % NHB;
-                const bool got = mbar_wait(&hfull[hb], (cc / NHB) & 1, abort_flag);
+            // chunks in pairs: the two FP32 chunk sums are added in FP32
+            // (one rounding, unbiased) before the FP64 accumulation, which
+            // halves the conversions and FP64 additions
+            for (int c = 0; c + 1 < nch; c += 2, cc += 2) {
+                const int hb0 = cc % NHB, hb1 = (cc + 1) % NHB;
+                bool got = mbar_wait(&hfull[hb0], (cc / NHB) & 1, abort_flag);
+                got = got && mbar_wait(&hfull[hb1], ((cc + 1) / NHB) & 1, abort_flag);
                 if (!__all_sync(0xffffffffu, got)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
+                const uint32_t ta0 = tmem + lanes + (uint32_t)(hb0 * BN + half * 64);
+                const uint32_t ta1 = tmem + lanes + (uint32_t)(hb1 * BN + half * 64);
+#pragma unroll
+                for (int g = 0; g < 4; ++g) {
+                    uint32_t r0[16], r1[16];
+                    tmem_ld16(ta0 + 16 * g, r0);
+                    tmem_ld16(ta1 + 16 * g, r1);
+                    tmem_wait();
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        acc[g * 16 + j] += (double)(__uint_as_float(r0[j]) + __uint_as_float(r1[j]));
+                }
+                tc_fence_before();
+                mbar_arrive(&hempty[hb0]);
+                mbar_arrive(&hempty[hb1]);
+            }
+            if (ok && (nch & 1)) {  // the odd last chunk
+                const int hb = cc % NHB;
+                const bool got = mbar_wait(&hfull[hb], (cc / NHB) & 1, abort_flag);
+                if (!__all_sync(0xffffffffu, got)) break;
+                tc_fence_after();
                 const uint32_t ta = tmem + lanes + (uint32_t)(hb * BN + half * 64);
 #pragma unroll
-                for (int g = 0; g < 2; ++g) {
-                    uint32_t r[32];
-                    tmem_ld32(ta + 32 * g, r);
+                for (int g = 0; g < 4; ++g) {
+                    uint32_t r0[16];
+                    tmem_ld16(ta + 16 * g, r0);
+                    tmem_wait();
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) acc[g * 32 + j] += (double)__uint_as_float(r[j]);
+                    for (int j = 0; j < 16; ++j) acc[g * 16 + j] += (double)__uint_as_float(r0[j]);
                 }
                 tc_fence_before();
                 mbar_arrive(&hempty[hb]);
+                ++cc;
             }
             if (!ok) break;
             const bool got = mbar_wait(&xfull, tcnt & 1, abort_flag);

@@ -24,7 +24,6 @@ constexpr int MAXP = 96;         // problems per launch
 constexpr int PIECE_F16 = 0;     // fp16 pieces (11-bit significand each)
 constexpr int PIECE_BF16 = 1;    // bf16 pieces (8-bit significand each)
 constexpr uint32_t TC_REVERSE = 1;    // orders summed from high to low
-constexpr int TC_CHUNK = 2;           // stages of BK orders per hi*hi chunk
 
 // One contraction of a launch.  Rows of A beyond M and columns beyond N are
 // read as zeros by the tensor-map bounds and never stored.

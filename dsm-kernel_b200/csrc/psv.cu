@@ -355,14 +355,34 @@ __device__ __forceinline__ cd caddmulT(cd c, cd a, cd b) {  // c + a b
     if (FAST) return mk(fma(a.re, b.re, fma(-a.im, b.im, c.re)), fma(a.re, b.im, fma(a.im, b.re, c.im)));
     return c + a * b;
 }
+// 1/x for the fast path: the hardware's approximate reciprocal refined by
+// two Newton-Raphson steps y <- y + y (1 - x y) (each roughly doubles the
+// correct bits), a few ulp from the correctly rounded quotient.
+__device__ __forceinline__ double rcp_newton(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    y = fma(y, fma(-x, y, 1.0), y);
+    y = fma(y, fma(-x, y, 1.0), y);
+    return y;
+}
 template <bool FAST>
 __device__ __forceinline__ cd crecipT(cd D) {
     if (FAST) {
-        const double r = 1.0 / fma(D.re, D.re, D.im * D.im);
+        const double r = rcp_newton(fma(D.re, D.re, D.im * D.im));
         return mk(D.re * r, -D.im * r);
     }
     return mk(1.0) / D;
 }
+
+// asynchronous global -> shared copies (16 B) and their groups
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // last pivots and multiplier of a factorisation, for the substitution pass
 struct SysTail {
@@ -374,6 +394,7 @@ struct FactorCtx {
     const cd* P;  // this frequency's row pieces, [row][12]
     double l2, lsq;
     int it, n, ls, lmin, nsys, sys;
+    bool store;  // false for threads that only repeat another system
     cd *Lst, *Dst;
 };
 
@@ -384,11 +405,11 @@ struct FactorCtx {
 // as the reference's band loop (main update for k <= n-3, the last two
 // steps' order otherwise).
 template <int P, bool FAST>
-__device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], RowPieces& nxt, SysTail& T,
+__device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], const cd (&anew)[4], SysTail& T,
                                             const FactorCtx& c) {
     constexpr int S0 = P, S1 = (P + 1) & 3, S2 = (P + 2) & 3, S3 = (P + 3) & 3;
     const cd D = M[S0][S0];
-    if (k >= c.ls) c.Dst[(size_t)(k - c.ls) * c.nsys + c.sys] = D;
+    if (c.store && k >= c.ls) c.Dst[(size_t)(k - c.ls) * c.nsys + c.sys] = D;
     if (k == c.n) return true;
     if (k == c.n - 1) T.Dm1 = D;
     const cd piv = crecipT<FAST>(D);
@@ -404,7 +425,7 @@ __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], RowPieces& nxt
         zv2 = -M[S3][S0];
         wv2 = cmulT<FAST>(M[S3][S0], piv);
     }
-    if (k >= c.lmin) {
+    if (c.store && k >= c.lmin) {
         cd* L = c.Lst + (size_t)k * 3 * c.nsys + c.sys;
         L[0] = wv0;
         L[c.nsys] = wv1;
@@ -425,16 +446,12 @@ __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], RowPieces& nxt
             M[S2][S2] = caddmulT<FAST>(M[S2][S2], wv1, zv1);
         }
     }
-    // row k+4 enters the slot of row k (columns k+1 .. k+4); its pieces were
-    // loaded one step ago, and row k+5's loads go out now
+    // row k+4 enters the slot of row k (columns k+1 .. k+4)
     if (k + 4 <= c.n) {
-        cd a[4];
-        assemble_row<FAST>(nxt, c.l2, c.lsq, a);
-        M[S0][S1] = a[0];
-        M[S0][S2] = a[1];
-        M[S0][S3] = a[2];
-        M[S0][S0] = a[3];
-        if (k + 5 <= c.n) load_row(c.P + (size_t)(c.it + k + 4) * 12, nxt);
+        M[S0][S1] = anew[0];
+        M[S0][S2] = anew[1];
+        M[S0][S3] = anew[2];
+        M[S0][S0] = anew[3];
     } else {
         M[S0][S1] = M[S0][S2] = M[S0][S3] = M[S0][S0] = mk(0.0);
     }
@@ -445,14 +462,34 @@ __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], RowPieces& nxt
 // unpivoted complex-symmetric LDL^T (dcsymbdl0) streamed through the ring
 // window.  Multipliers of the rows the substitutions need go to Lst, pivots
 // of the rows at and above the source to Dst, the last ones to tail.
+// The row pieces stream through shared memory: a block (128 consecutive
+// systems: consecutive orders of at most a few frequencies) copies FAC_CH
+// rows of each of its frequencies with cp.async one chunk ahead, so the
+// factor recurrence waits on shared-memory latency only.  Systems of
+// frequencies beyond the first FAC_NW of a block read their rows from global
+// memory.  All threads of a block take the same steps (the same n), so the
+// block-wide barriers at chunk boundaries are uniform; threads past nsys
+// repeat the last system's work without storing it.
+constexpr int FAC_THREADS = 128;
+constexpr int FAC_CH = 16;  // rows per chunk (multiple of 4)
+constexpr int FAC_NW = 4;   // frequencies staged per block
+
 template <bool FAST>
-__global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
-                                                   int nsys, int lmin, cd* __restrict__ Lst,
-                                                   cd* __restrict__ Dst, SysTail* __restrict__ tail) {
-    int sys = blockIdx.x * blockDim.x + threadIdx.x;
-    if (sys >= nsys) return;
-    int w, l;
+__global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
+                                                           int nsys, int lmin, cd* __restrict__ Lst,
+                                                           cd* __restrict__ Dst, SysTail* __restrict__ tail) {
+    __shared__ __align__(16) cd sP[2][FAC_NW][FAC_CH][12];
+    const int sys0 = blockIdx.x * FAC_THREADS;
+    const int sysv = sys0 + threadIdx.x;
+    const bool valid = sysv < nsys;
+    const int sys = valid ? sysv : nsys - 1;
+    int w, l, w0, w1, ltmp;
     wl_map(wl, sys, w, l);
+    wl_map(wl, sys0, w0, ltmp);
+    wl_map(wl, min(sys0 + FAC_THREADS, nsys) - 1, w1, ltmp);
+    const int nws = min(FAC_NW, w1 - w0 + 1);
+    const int ws = w - w0;
+    const bool staged = ws < nws;
     FactorCtx c;
     c.d = &d;
     c.P = Prow + (size_t)w * (d.nn + 1) * 12;
@@ -464,62 +501,112 @@ __global__ void __launch_bounds__(128) k_psv_solve(PsvDev d, const cd* __restric
     c.lmin = lmin;
     c.nsys = nsys;
     c.sys = sys;
+    c.store = valid;
     c.Lst = Lst;
     c.Dst = Dst;
+    const int n = c.n;
+    // local rows 5 .. n in chunks: chunk q = rows 5 + q CH .. (global it + r - 1)
+    auto stage = [&](int q, int buf) {
+        const int r0 = 5 + q * FAC_CH;
+        const int cnt = min(FAC_CH, n - r0 + 1);
+        if (cnt <= 0) return;
+        const int per = cnt * 12;
+        for (int e = threadIdx.x; e < nws * per; e += FAC_THREADS) {
+            const int wi = e / per, rem = e - wi * per, i = rem / 12, v = rem - i * 12;
+            cp_async16(&sP[buf][wi][i][v], Prow + ((size_t)(w0 + wi) * (d.nn + 1) + c.it + r0 + i - 1) * 12 + v);
+        }
+    };
+    stage(0, 0);
+    cp_async_commit();
     cd M[4][4];
 #pragma unroll
     for (int p = 0; p < 4; ++p)
 #pragma unroll
         for (int q = 0; q < 4; ++q) M[p][q] = mk(0.0);
     cd a[4];
-    RowPieces nxt;
+    RowPieces rp;
     // local rows 1..4 go to slots 1, 2, 3, 0
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
-        if (p >= c.n) break;
-        load_row(c.P + (size_t)(c.it + p) * 12, nxt);
-        assemble_row<FAST>(nxt, c.l2, c.lsq, a);
+        if (p >= n) break;
+        load_row(c.P + (size_t)(c.it + p) * 12, rp);
+        assemble_row<FAST>(rp, c.l2, c.lsq, a);
 #pragma unroll
         for (int q = 0; q <= p; ++q) M[(1 + p) & 3][(1 + q) & 3] = a[4 - (p - q) - 1];
     }
     SysTail T;
     // dcsbdlv0 reads a(m-1,2) = a(2,2) of the unfactored band at row 2
-    load_row(c.P + (size_t)(c.it + 1) * 12, nxt);
-    assemble_row<FAST>(nxt, c.l2, c.lsq, a);
+    load_row(c.P + (size_t)(c.it + 1) * 12, rp);
+    assemble_row<FAST>(rp, c.l2, c.lsq, a);
     T.a22raw = a[1];
     T.Dm1 = mk(1.0);
     T.Lnn1 = mk(0.0);
-    if (5 <= c.n) load_row(c.P + (size_t)(c.it + 4) * 12, nxt);  // local row 5
+    // row entering at step k: local row k+4, chunk (k-1)/CH, index (k-1)%CH
+    auto entering = [&](int k, cd (&an)[4]) {
+        if (k + 4 > n) return;
+        const int i = (k - 1) % FAC_CH, buf = ((k - 1) / FAC_CH) & 1;
+        if (staged) {
+#pragma unroll
+            for (int v = 0; v < 12; ++v) rp.v[v] = sP[buf][ws][i][v];
+        } else {
+            load_row(c.P + (size_t)(c.it + k + 3) * 12, rp);
+        }
+        assemble_row<FAST>(rp, c.l2, c.lsq, an);
+    };
+    cd an[4];
     for (int k = 1;; k += 4) {
-        if (factor_step<1, FAST>(k, M, nxt, T, c)) { T.Dn = M[1][1]; break; }
-        if (factor_step<2, FAST>(k + 1, M, nxt, T, c)) { T.Dn = M[2][2]; break; }
-        if (factor_step<3, FAST>(k + 2, M, nxt, T, c)) { T.Dn = M[3][3]; break; }
-        if (factor_step<0, FAST>(k + 3, M, nxt, T, c)) { T.Dn = M[0][0]; break; }
+        if ((k - 1) % FAC_CH == 0) {  // chunk boundary: next chunk's copies go out
+            const int q = (k - 1) / FAC_CH;
+            stage(q + 1, (q + 1) & 1);
+            cp_async_commit();
+            cp_async_wait<1>();
+            __syncthreads();
+        }
+        entering(k, an);
+        if (factor_step<1, FAST>(k, M, an, T, c)) { T.Dn = M[1][1]; break; }
+        entering(k + 1, an);
+        if (factor_step<2, FAST>(k + 1, M, an, T, c)) { T.Dn = M[2][2]; break; }
+        entering(k + 2, an);
+        if (factor_step<3, FAST>(k + 2, M, an, T, c)) { T.Dn = M[3][3]; break; }
+        entering(k + 3, an);
+        if (factor_step<0, FAST>(k + 3, M, an, T, c)) { T.Dn = M[0][0]; break; }
+        if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
     }
-    tail[sys] = T;
+    cp_async_wait<0>();  // no copy outlives the block
+    if (valid) tail[sys] = T;
 }
 
 // Substitutions of the six basis right-hand sides, one thread per (system,
-// basis); the six threads of a system read the same factor entries in the
-// same instruction.  Forward (dcsbdlv0, m = 3) from the first source row,
-// where the source bases' z start (everything below is zero), to the top,
-// keeping zh = z / D in Zst; then upward: x(n) = zh(n); x(n-1) = zh(n-1) -
-// L(n,n-1) x(n); x(j) = zh(j) - [L(j+3,j) x(j+3) + L(j+2,j) x(j+2) +
-// L(j+1,j) x(j+1)], down to the deepest captured row, with the multipliers
-// loaded four rows ahead.  Values at receiver stencil rows go to Xcap.
-// Bases 4 and 5 are the surface unit vectors e_{n-1}, e_n.
-__global__ void __launch_bounds__(128) k_psv_back(PsvDev d, int nsys, int jmin_loc, const int* __restrict__ capmap,
-                                                  const cd* __restrict__ Lst, const cd* __restrict__ Dst,
-                                                  cd* __restrict__ Zst, const SysTail* __restrict__ tail,
-                                                  cd* __restrict__ Xcap) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int sys = t / NB, b = t - sys * NB;
-    if (sys >= nsys) return;
+// basis), BACK_SYS systems per block.  Forward (dcsbdlv0, m = 3) from the
+// first source row, where the source bases' z start (everything below is
+// zero), to the top, keeping zh = z / D in Zst; then upward: x(n) = zh(n);
+// x(n-1) = zh(n-1) - L(n,n-1) x(n); x(j) = zh(j) - [L(j+3,j) x(j+3) +
+// L(j+2,j) x(j+2) + L(j+1,j) x(j+1)], down to the deepest captured row.  The
+// multipliers stream through shared memory: the block copies BACK_CH rows of
+// its systems' factors with cp.async one chunk ahead of use (coalesced 512 B
+// rows), so the recurrence runs on shared-memory latency.  Values at
+// receiver stencil rows go to Xcap.  Bases 4 and 5 are the surface unit
+// vectors e_{n-1}, e_n.
+constexpr int BACK_SYS = 32;
+constexpr int BACK_THREADS = BACK_SYS * NB;  // 192
+constexpr int BACK_CH = 12;                  // rows per staged chunk (2 x 18 KB)
+
+__global__ void __launch_bounds__(BACK_THREADS) k_psv_back(PsvDev d, int nsys, int jmin_loc,
+                                                           const int* __restrict__ capmap,
+                                                           const cd* __restrict__ Lst, const cd* __restrict__ Dst,
+                                                           cd* __restrict__ Zst, const SysTail* __restrict__ tail,
+                                                           cd* __restrict__ Xcap) {
+    __shared__ __align__(16) cd sL[2][BACK_CH][3][BACK_SYS];
+    const int sys0 = blockIdx.x * BACK_SYS;
+    const int sl = threadIdx.x / NB, b = threadIdx.x - sl * NB;
+    const int sys = sys0 + sl;
+    const bool valid = sys < nsys;
+    const int nsb = min(BACK_SYS, nsys - sys0);  // systems of this block
     const int it = d.itmp, n = d.nn - it + 1;
     const int ls = d.jsrc - it + 1;
     auto L = [&](int row, int p) { return Lst[((size_t)row * 3 + p) * nsys + sys]; };
     auto ZH = [&](int row) { return Zst[((size_t)(row - ls) * 4 + b) * nsys + sys]; };
-    if (b < 4) {  // forward substitution of a source basis
+    if (valid && b < 4) {  // forward substitution of a source basis
         const cd a22raw = tail[sys].a22raw;
         cd z0 = mk(0.0), z1 = mk(0.0), z2 = mk(0.0);  // z(j-3), z(j-2), z(j-1)
         for (int j = max(ls, 1); j <= n; ++j) {
@@ -545,66 +632,70 @@ __global__ void __launch_bounds__(128) k_psv_back(PsvDev d, int nsys, int jmin_l
             z2 = zc;
         }
     }
-    const SysTail tl = tail[sys];
-    cd xn;
-    if (b < 4) xn = (n >= ls) ? ZH(n) : mk(0.0);
-    // surface basis: e_{n-1}: z(n-1) = 1, z(n) = -L(n,n-1); e_n: z(n) = 1
-    else if (b == 4) xn = (mk(0.0) - tl.Lnn1 * mk(1.0)) / tl.Dn;
-    else xn = mk(1.0) / tl.Dn;
+    cd x0 = mk(0.0), x1 = mk(0.0), x2 = mk(0.0);  // x(j+1), x(j+2), x(j+3)
     auto capture = [&](int jloc, cd v) {
         const int c = capmap[jloc + it - 1];
         if (c >= 0) Xcap[((size_t)c * NB + b) * nsys + sys] = v;
     };
-    capture(n, xn);
-    cd x0 = xn, x1 = mk(0.0), x2 = mk(0.0);  // x(j+1), x(j+2), x(j+3)
-    if (n - 1 >= jmin_loc) {
-        cd zh = mk(0.0);
-        if (b < 4 && n - 1 >= ls) zh = ZH(n - 1);
-        if (b == 4) zh = mk(1.0) / tl.Dm1;
-        const cd v = zh - L(n - 1, 0) * x0;
-        capture(n - 1, v);
-        x1 = x0;
-        x0 = v;
+    if (valid) {
+        const SysTail tl = tail[sys];
+        cd xn;
+        if (b < 4) xn = (n >= ls) ? ZH(n) : mk(0.0);
+        // surface basis: e_{n-1}: z(n-1) = 1, z(n) = -L(n,n-1); e_n: z(n) = 1
+        else if (b == 4) xn = (mk(0.0) - tl.Lnn1 * mk(1.0)) / tl.Dn;
+        else xn = mk(1.0) / tl.Dn;
+        capture(n, xn);
+        x0 = xn;
+        if (n - 1 >= jmin_loc) {
+            cd zh = mk(0.0);
+            if (b < 4 && n - 1 >= ls) zh = ZH(n - 1);
+            if (b == 4) zh = mk(1.0) / tl.Dm1;
+            const cd v = zh - L(n - 1, 0) * x0;
+            capture(n - 1, v);
+            x1 = x0;
+            x0 = v;
+        }
     }
-    // multipliers of row j in Lr[j & 3], loaded four rows ahead
-    cd Lr[4][3];
-#pragma unroll
-    for (int P = 0; P < 4; ++P) {  // slot P: the highest row <= n-2 congruent to P
-        const int j = (n - 2) - (((n - 2) - P) & 3);
-        if (j >= jmin_loc) { Lr[P][0] = L(j, 0); Lr[P][1] = L(j, 1); Lr[P][2] = L(j, 2); }
-    }
-    auto row = [&](int j1, cd L1, cd L2, cd L3) {
-        cd zh = mk(0.0);
-        if (b < 4 && j1 >= ls) zh = ZH(j1);
-        cd sum;
-        if (j1 == n - 2) sum = mk(0.0) + L2 * x1 + L1 * x0;
-        else sum = mk(0.0) + L3 * x2 + L2 * x1 + L1 * x0;
-        const cd v = zh - sum;
-        capture(j1, v);
-        x2 = x1;
-        x1 = x0;
-        x0 = v;
+    // rows n-2 .. jmin_loc in chunks of BACK_CH, staged one chunk ahead
+    const int top = n - 2;
+    const int nrows = top - jmin_loc + 1;
+    if (nrows <= 0) return;
+    const int nch = (nrows + BACK_CH - 1) / BACK_CH;
+    auto stage = [&](int c, int buf) {
+        const int hi = top - c * BACK_CH, cnt = min(BACK_CH, hi - jmin_loc + 1);
+        // cnt rows x 3 multipliers x nsb systems, 16 B each
+        for (int e = threadIdx.x; e < cnt * 3 * nsb; e += BACK_THREADS) {
+            const int sidx = e % nsb, rp = e / nsb, i = rp / 3, p = rp - 3 * i;
+            cp_async16(&sL[buf][i][p][sidx], &Lst[((size_t)(hi - i) * 3 + p) * nsys + sys0 + sidx]);
+        }
     };
-    // rows in descending order; the slot a row frees takes the row four below
-#define DSM_BACK_ROW(P)                                                           \
-    if ((j1 & 3) == P) {                                                          \
-        if (j1 < jmin_loc) break;                                                 \
-        const cd L1 = Lr[P][0], L2 = Lr[P][1], L3 = Lr[P][2];                     \
-        if (j1 - 4 >= jmin_loc) {                                                 \
-            Lr[P][0] = L(j1 - 4, 0);                                              \
-            Lr[P][1] = L(j1 - 4, 1);                                              \
-            Lr[P][2] = L(j1 - 4, 2);                                              \
-        }                                                                         \
-        row(j1, L1, L2, L3);                                                      \
-        --j1;                                                                     \
+    stage(0, 0);
+    cp_async_commit();
+    for (int c = 0; c < nch; ++c) {
+        if (c + 1 < nch) stage(c + 1, (c + 1) & 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        if (valid) {
+            const int hi = top - c * BACK_CH, cnt = min(BACK_CH, hi - jmin_loc + 1);
+            const int buf = c & 1;
+            for (int i = 0; i < cnt; ++i) {
+                const int j1 = hi - i;
+                const cd L1 = sL[buf][i][0][sl], L2 = sL[buf][i][1][sl], L3 = sL[buf][i][2][sl];
+                cd zh = mk(0.0);
+                if (b < 4 && j1 >= ls) zh = ZH(j1);
+                cd sum;
+                if (j1 == n - 2) sum = mk(0.0) + L2 * x1 + L1 * x0;
+                else sum = mk(0.0) + L3 * x2 + L2 * x1 + L1 * x0;
+                const cd v = zh - sum;
+                capture(j1, v);
+                x2 = x1;
+                x1 = x0;
+                x0 = v;
+            }
+        }
+        __syncthreads();  // the buffer is refilled two chunks later
     }
-    for (int j1 = n - 2;;) {
-        DSM_BACK_ROW(3)
-        DSM_BACK_ROW(2)
-        DSM_BACK_ROW(1)
-        DSM_BACK_ROW(0)
-    }
-#undef DSM_BACK_ROW
 }
 
 // ------------------------------------------------------------ l = 0 path
@@ -773,9 +864,11 @@ __global__ void __launch_bounds__(128) k_psv_l0_solve(PsvDev d, const int* __res
 // (3) fields of order 0, one thread per (frequency, receiver): m = 0 slots
 // q = 0..2 (imt 1..3) and 3 (back), U and dU/dr (calup0 uses u(1) only)
 __device__ __forceinline__ void put_field(double* Aw, int Lcap, int R, int q, int r, int f, cd v) {
-    size_t row = ((size_t)(q * (R + 1) + r) * NFLD + f) * 2;
+    // rows ordered (slot, field, re/im, receiver): receivers contiguous, so
+    // the epilogue's threads (consecutive receivers) read consecutive rows
+    const size_t row = ((size_t)(q * NFLD + f) * 2) * (R + 1) + r;
     Aw[row * Lcap] = v.re;
-    Aw[(row + 1) * Lcap] = v.im;
+    Aw[(row + (R + 1)) * Lcap] = v.im;
 }
 
 __global__ void k_psv_l0_fields(PsvDev d, const cd* __restrict__ Dv, double* __restrict__ A0f,
@@ -1107,27 +1200,38 @@ __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restric
 
 // Per (omega, l >= 1, receiver group): receiver fields of every slot and the
 // cutoff probe (group 0).
+// Fields of every slot at the receivers, one thread per (system, receiver):
+// a warp holds 8 consecutive systems (orders) x 4 receivers, so each
+// coefficient load serves four receivers and each field store writes 8
+// consecutive orders of one row.  Values and radial derivatives of the six
+// basis solutions come from the three-node weights (interpolate, calup),
+// then U, V and derivatives of each slot are their combinations with the
+// source coefficients.  Block row 0 also writes the cutoff probe (calamp of
+// imt = 1, m = 0 at the top receiver's stencil); the last block row holds
+// the surface (rows n-1, n).
+constexpr int FLD_SYS = 8, FLD_REC = 4;
+
 __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int nsys,
                                                     const cd* __restrict__ Xcap, const cd* __restrict__ co,
                                                     double* __restrict__ A0f, double* __restrict__ A1f,
                                                     double* __restrict__ A2f, int Lcap,
                                                     double* __restrict__ amps) {
-    int sys = blockIdx.x * blockDim.x + threadIdx.x;
-    if (sys >= nsys) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sys = (blockIdx.x * 4 + warp) * FLD_SYS + (lane & (FLD_SYS - 1));
+    const int r = blockIdx.y * FLD_REC + (lane >> 3);
+    const int R = d.R;
+    if (sys >= nsys || r > R) return;
     int w, l;
     wl_map(wl, sys, w, l);
-    if (l == 0) return;  // written by k_psv_l0
-    const int R = d.R;
+    if (l == 0) return;  // written by the order-0 kernels
     const size_t rows[3] = {(size_t)NS0 * (R + 1) * NFLD * 2, (size_t)NS1 * (R + 1) * NFLD * 2,
                             (size_t)NS2 * (R + 1) * NFLD * 2};
     double* Aw[3] = {A0f + (size_t)w * rows[0] * Lcap + l, A1f + (size_t)w * rows[1] * Lcap + l,
                      A2f + (size_t)w * rows[2] * Lcap + l};
     const double l2 = (double)l * (double)(l + 1), lsq = sqrt(l2);
-    int rlo = blockIdx.y * 16, rhi = min(rlo + 16, R);
-    bool g0 = blockIdx.y == 0;
     auto X = [&](int cap, int b) { return Xcap[((size_t)cap * NB + b) * nsys + sys]; };
     auto C = [&](int s, int b) { return co[((size_t)s * NB + b) * nsys + sys]; };
-    if (g0) {  // probe: calamp on g0(ksta(r_n)-1), g0(ksta(r_n)) of imt = 1, m = 0
+    if (r == 0) {  // probe: calamp on g0(ksta(r_n)-1), g0(ksta(r_n)) of imt = 1, m = 0
         cd p0 = mk(0.0), p1 = mk(0.0);
         for (int b = 0; b < 4; ++b) {
             cd cb = C(0, b);
@@ -1137,48 +1241,43 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
         double a1 = cabs_(p0), a2 = cabs_(p1);
         amps[(size_t)w * Lcap + l] = sqrt(a1 * a1 + a2 * a2);
     }
-    for (int pass = 0; pass < 2; ++pass) {
-        int r_lo = pass == 0 ? rlo : R, r_hi = pass == 0 ? rhi : (g0 ? R + 1 : R);
-        for (int r = r_lo; r < r_hi; ++r) {
-            bool surf = r == R;
-            cd bU[NB], bV[NB], bUd[NB], bVd[NB];
-            for (int b = 0; b < NB; ++b) bU[b] = bV[b] = bUd[b] = bVd[b] = mk(0.0);
-            if (surf) {
-                for (int b = 0; b < NB; ++b) { bU[b] = X(d.cap_n1, b); bV[b] = X(d.cap_n, b); }
-            } else {
-                for (int i = 0; i < 3; ++i) {
-                    double wvi = d.wv[3 * r + i], wdi = d.wd[3 * r + i];
-                    int cu = d.rcap[6 * r + 2 * i], cvv = d.rcap[6 * r + 2 * i + 1];
-                    for (int b = 0; b < NB; ++b) {
-                        cd xu = X(cu, b), xv = X(cvv, b);
-                        bU[b] = bU[b] + wvi * xu;
-                        bV[b] = bV[b] + wvi * xv;
-                        bUd[b] = bUd[b] + wdi * xu;
-                        bVd[b] = bVd[b] + wdi * xv;
-                    }
-                }
-            }
-            for (int s = 0; s < NSLOT; ++s) {
-                int mi = slot_mi(s), q = slot_q(s);
-                bool isback = (s == 3) || (mi == 1 && (q % 4) >= 2);
-                cd U = mk(0.0), V = mk(0.0), Ud = mk(0.0), Vd = mk(0.0);
-                if (!(surf && isback)) {
-                    for (int b = 0; b < NB; ++b) {
-                        cd cb = C(s, b);
-                        U = U + cb * bU[b];
-                        V = V + cb * bV[b];
-                        Ud = Ud + cb * bUd[b];
-                        Vd = Vd + cb * bVd[b];
-                    }
-                }
-                cd Vh = V / lsq, Vdh = Vd / lsq;
-                put_field(Aw[mi], Lcap, R, q, r, 0, U);
-                put_field(Aw[mi], Lcap, R, q, r, 1, Ud);
-                put_field(Aw[mi], Lcap, R, q, r, 2, Vh);
-                put_field(Aw[mi], Lcap, R, q, r, 3, Vdh);
-                put_field(Aw[mi], Lcap, R, q, r, 4, l2 * Vh);
+    const bool surf = r == R;
+    cd bU[NB], bV[NB], bUd[NB], bVd[NB];
+    for (int b = 0; b < NB; ++b) bU[b] = bV[b] = bUd[b] = bVd[b] = mk(0.0);
+    if (surf) {
+        for (int b = 0; b < NB; ++b) { bU[b] = X(d.cap_n1, b); bV[b] = X(d.cap_n, b); }
+    } else {
+        for (int i = 0; i < 3; ++i) {
+            double wvi = d.wv[3 * r + i], wdi = d.wd[3 * r + i];
+            int cu = d.rcap[6 * r + 2 * i], cvv = d.rcap[6 * r + 2 * i + 1];
+            for (int b = 0; b < NB; ++b) {
+                cd xu = X(cu, b), xv = X(cvv, b);
+                bU[b] = bU[b] + wvi * xu;
+                bV[b] = bV[b] + wvi * xv;
+                bUd[b] = bUd[b] + wdi * xu;
+                bVd[b] = bVd[b] + wdi * xv;
             }
         }
+    }
+    for (int s = 0; s < NSLOT; ++s) {
+        int mi = slot_mi(s), q = slot_q(s);
+        bool isback = (s == 3) || (mi == 1 && (q % 4) >= 2);
+        cd U = mk(0.0), V = mk(0.0), Ud = mk(0.0), Vd = mk(0.0);
+        if (!(surf && isback)) {
+            for (int b = 0; b < NB; ++b) {
+                cd cb = C(s, b);
+                U = U + cb * bU[b];
+                V = V + cb * bV[b];
+                Ud = Ud + cb * bUd[b];
+                Vd = Vd + cb * bVd[b];
+            }
+        }
+        cd Vh = V / lsq, Vdh = Vd / lsq;
+        put_field(Aw[mi], Lcap, R, q, r, 0, U);
+        put_field(Aw[mi], Lcap, R, q, r, 1, Ud);
+        put_field(Aw[mi], Lcap, R, q, r, 2, Vh);
+        put_field(Aw[mi], Lcap, R, q, r, 3, Vdh);
+        put_field(Aw[mi], Lcap, R, q, r, 4, l2 * Vh);
     }
 }
 
@@ -1265,10 +1364,10 @@ __global__ void k_psv_epi(PsvDev d, int w, const double* __restrict__ thx, const
             if (surf && isback) continue;
             if (isp && mi != 0) continue;  // only bvec(1,0) survives at the poles
             auto G = [&](int f, int b) {
-                size_t row = ((size_t)(q * (R + 1) + r) * NFLD + f) * 2;
+                size_t row = ((size_t)(q * NFLD + f) * 2) * (R + 1) + r;
                 size_t col = (size_t)b * Th + it;
                 const TC* C = Cm[mi];
-                return mk((double)C[row + (size_t)M[mi] * col], (double)C[row + 1 + (size_t)M[mi] * col]);
+                return mk((double)C[row + (size_t)M[mi] * col], (double)C[row + (R + 1) + (size_t)M[mi] * col]);
             };
             double sigma = (m < 0 && (mi & 1)) ? -1.0 : 1.0;
             double mm = (double)m, m2 = mm * mm;
@@ -1668,8 +1767,8 @@ class PsvEngine : public Engine {
             k_psv_solve<false><<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Dst.p,
                                                                    tails.p);
         DSM_LAUNCH(*this);
-        k_psv_back<<<(NB * nsys + 127) / 128, 128, 0, st>>>(d, nsys, jmin_loc, capmap.p, Lst.p, Dst.p, Zst.p,
-                                                            tails.p, Xcap.p);
+        k_psv_back<<<(nsys + BACK_SYS - 1) / BACK_SYS, BACK_THREADS, 0, st>>>(d, nsys, jmin_loc, capmap.p, Lst.p,
+                                                                              Dst.p, Zst.p, tails.p, Xcap.p);
         kend(id, alg * nsys, 0.0);
         DSM_LAUNCH(*this);
         id = kid("psv_source_coef");
@@ -1677,7 +1776,7 @@ class PsvEngine : public Engine {
         k_psv_coef<<<(nsys + 127) / 128, 128, 0, st>>>(d, fr_, wl, nsys, ab.p, co.p, rsgt_sw);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
-        dim3 grid((nsys + 127) / 128, (R + 15) / 16);
+        dim3 grid((nsys + 4 * FLD_SYS - 1) / (4 * FLD_SYS), (R + 1 + FLD_REC - 1) / FLD_REC);
         id = kid("psv_fields");
         kbegin(id);
         k_psv_fields<<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, Afld[0].p, Afld[1].p, Afld[2].p,

@@ -201,9 +201,10 @@ __global__ void __launch_bounds__(128) k_sh_fields(ShDev d, const int* __restric
     bool g0 = blockIdx.y == 0;
     auto X = [&](int cap, int k) { return Xcap[((size_t)cap * 3 + k) * nsys + sys]; };
     auto put = [&](double* Aw, int q, int r, int f, cd v) {
-        size_t row = ((size_t)(q * (R + 1) + r) * SH_NF + f) * 2;
+        // rows ordered (slot, field, re/im, receiver): receivers contiguous
+        const size_t row = ((size_t)(q * SH_NF + f) * 2) * (R + 1) + r;
         Aw[row * Lcap] = v.re;
-        Aw[(row + 1) * Lcap] = v.im;
+        Aw[(row + (R + 1)) * Lcap] = v.im;
     };
     if (l == 0) {  // the SH m loop is empty at l = 0
         for (int r = rlo; r < rhi; ++r)
@@ -418,9 +419,9 @@ __global__ void k_sh_epi(ShDev d, int w, int Th, const double* __restrict__ thx,
                 int m = sg == 0 ? -ma : ma;
                 double sigma = (m < 0 && (ma & 1)) ? -1.0 : 1.0;
                 auto G = [&](int f, int b) {
-                    size_t row = ((size_t)(q * (R + 1) + r) * SH_NF + f) * 2;
+                    size_t row = ((size_t)(q * SH_NF + f) * 2) * (R + 1) + r;
                     size_t col = (size_t)b * Th + it;
-                    return mk((double)C[row + (size_t)M * col], (double)C[row + 1 + (size_t)M * col]);
+                    return mk((double)C[row + (size_t)M * col], (double)C[row + (R + 1) + (size_t)M * col]);
                 };
                 cd P = G(0, 0), D = G(0, 1);
                 double mm = (double)m, m2 = mm * mm;

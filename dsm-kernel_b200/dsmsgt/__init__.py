@@ -149,8 +149,8 @@ def lib() -> C.CDLL:
         L.dsm_lmax_features.argtypes = [C.c_void_p, _ip, C.c_int, _f]
         L.dsm_cutoffs.argtypes = [C.c_void_p, _ip, C.c_int, _ip]
         L.dsm_lmax_init.argtypes = [_f, _f, C.c_int, C.c_uint, _f]
-        L.dsm_lmax_train.argtypes = [_f, _f, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint, _f, _f,
-                                     C.c_int]
+        L.dsm_lmax_train.argtypes = [_f, _f, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint, _f,
+                                     _f, C.c_int]
         L.dsm_lmax_grad.argtypes = [_f, _f, _f, C.c_int, _f, _f, C.c_int]
         L.dsm_set_lmax_model.argtypes = [C.c_void_p, _f]
         L.dsm_lmax_predict.argtypes = [C.c_void_p, _ip, C.c_int, _f]
@@ -196,15 +196,15 @@ def lmax_init(X, T, seed: int = 0) -> np.ndarray:
 
 
 def lmax_train(X, T, params, epochs: int = 200, batch: int = 256, lr: float = 1e-3, seed: int = 0,
-               device: int = 0):
+               device: int = 0, weight_decay: float = 0.0):
     """Adam on the GPU with the project's forward/backward kernels; returns
     (trained parameters, per-epoch loss)."""
     X = np.ascontiguousarray(X, dtype=np.float32)
     T = np.ascontiguousarray(T, dtype=np.float32)
     P = np.ascontiguousarray(params, dtype=np.float32).copy()
     losses = np.zeros(epochs, np.float32)
-    rc = lib().dsm_lmax_train(_fptr(X), _fptr(T), len(T), epochs, batch, lr, seed, _fptr(P), _fptr(losses),
-                              device)
+    rc = lib().dsm_lmax_train(_fptr(X), _fptr(T), len(T), epochs, batch, lr, weight_decay, seed, _fptr(P),
+                              _fptr(losses), device)
     if rc:
         raise DsmError(f"dsm_lmax_train failed ({rc}): {lib().dsm_last_error(None).decode()}")
     return P, losses

@@ -6,7 +6,7 @@ seed-randomised 1-D models, and the network is trained on the GPU by the
 library's forward/backward/Adam kernels (dsm_lmax_train).
 
     python -m dsmsgt.lmax_data --out lmax_params.f32 \\
-        --train-seeds 1000:1016 --eval-seeds 2000:2004 --imax 2048
+        --train-seeds 1000:1064 --eval-seeds 2000:2016 --imax 1024
 
 writes the parameter block (DSM_LMAX_NPARAM float32, raw) and prints the
 held-out miss rate and padded-work fraction."""
@@ -20,8 +20,8 @@ import numpy as np
 import dsmsgt
 from dsmsgt import synth
 
-MARGIN = 1.05   # the engine's span = predicted cutoff * MARGIN + 16
-PAD = 16.0
+MARGIN = 1.02   # the engine's span = predicted cutoff * MARGIN + PAD
+PAD = 24.0
 
 
 def psv_job(seed: int, imax: int, r0: float, tlen: float = 3276.8, rrec: float = 6350.0):
@@ -44,8 +44,10 @@ def harvest(seeds, imax: int, depths_km=(10.0, 300.0, 600.0), nfreq: int = 64, t
             s = dsmsgt.Setup(psv_job(sd, imax, 6371.0 - dep, tlen), "psv")
             ctx = dsmsgt.Context(s, device=device, freq_batch=16)
             ll = ctx.cutoffs(freqs)
-            X.append(ctx.lmax_features(freqs))
-            T.append(np.log(np.maximum(ll, 1)).astype(np.float32))
+            f = ctx.lmax_features(freqs)
+            X.append(f)
+            # target: the cutoff relative to the lsuf scale exp(f0)
+            T.append((np.log(np.maximum(ll, 1)) - f[:, 0]).astype(np.float32))
             G.append(np.full(len(freqs), sd))
             ctx.close()
             log(f"seed {sd} depth {dep} km: cutoffs {ll.min()}..{ll.max()} ({time.perf_counter() - t0:.1f} s)")
@@ -82,7 +84,7 @@ def evaluate(params, seeds, imax: int, depths_km=(10.0, 300.0, 600.0), nfreq: in
             ctx.close()
             lsuf = (np.expm1(f[:, 0].astype(np.float64)) - 0.5).astype(np.int64) + 1
             for k, i in enumerate(freqs):
-                learned = int(np.ceil(max(np.exp(pl[k]) * MARGIN + PAD, lsuf[k] + 32) / 32) * 32)
+                learned = int(np.ceil(max(np.exp(pl[k]) * MARGIN + PAD, lsuf[k] + 8) / 32) * 32)
                 plain = int(np.ceil(max(512, lsuf[k] + 64) / 32) * 32)
                 ls, lr = plain_ranges(learned, int(ll[k]))
                 ps, pr = plain_ranges(plain, int(ll[k]))
@@ -99,22 +101,24 @@ def evaluate(params, seeds, imax: int, depths_km=(10.0, 300.0, 600.0), nfreq: in
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
-    ap.add_argument("--train-seeds", default="1000:1016")
-    ap.add_argument("--eval-seeds", default="2000:2004")
+    ap.add_argument("--train-seeds", default="1000:1064")
+    ap.add_argument("--eval-seeds", default="2000:2016")
+    ap.add_argument("--weight-decay", type=float, default=1e-3)
     ap.add_argument("--imax", type=int, default=2048)
     ap.add_argument("--nfreq", type=int, default=64)
-    ap.add_argument("--epochs", type=int, default=400)
+    ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--lr", type=float, default=1e-3)
     a = ap.parse_args()
     lo, hi = (int(v) for v in a.train_seeds.split(":"))
     X, T, _ = harvest(range(lo, hi), a.imax, nfreq=a.nfreq)
     P = dsmsgt.lmax_init(X, T, seed=0)
-    P, losses = dsmsgt.lmax_train(X, T, P, epochs=a.epochs, batch=a.batch, lr=a.lr)
+    P, losses = dsmsgt.lmax_train(X, T, P, epochs=a.epochs, batch=a.batch, lr=a.lr, weight_decay=a.weight_decay)
     print(f"loss {losses[0]:.4f} -> {losses[-1]:.5f} on {len(T)} cutoffs")
     P.astype(np.float32).tofile(a.out)
     lo, hi = (int(v) for v in a.eval_seeds.split(":"))
     print("held-out", evaluate(P, range(lo, hi), a.imax, nfreq=a.nfreq))
+    print("benchmark model (seed 0)", evaluate(P, [0], a.imax, depths_km=(300.0,), nfreq=a.nfreq))
 
 
 if __name__ == "__main__":

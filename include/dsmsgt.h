@@ -270,7 +270,9 @@ int dsm_sh_cutoff_noalloc(const dsm_sh_setup_t *setup, const int *ilist, int n, 
 /* ------------------------------------------------------------------------
  * Learned angular-order cutoff.  No counterpart in the reference.  A
  * 4-layer MLP (width 128, GELU, bf16 weights, FP32 accumulation) maps
- * DSM_LMAX_NFEAT features of a frequency to log(lmax); a context with
+ * DSM_LMAX_NFEAT features of a frequency to log(lmax) - log(1 + omega
+ * r_top / v_top) (the cutoff relative to the reference's lsuf scale); a
+ * context with
  * opt.use_lmax_predictor = 1 and a loaded parameter block sizes the first
  * order range of each frequency with it.  The plain amplitude test still
  * runs on the device and extends any short range, so the cutoff (llog) and
@@ -293,17 +295,21 @@ int dsm_lmax_features(const dsm_ctx_t *ctx, const int *ilist, int n, float *feat
 int dsm_cutoffs(dsm_ctx_t *ctx, const int *ilist, int n, int *llog);
 
 /* Parameter block: standardisation from (feats, target), He-initialised
- * weights from seed. target = log(llog) per row. */
+ * weights from seed.  The network's target is the cutoff relative to the
+ * lsuf scale: target = log(llog) - feats[0] per row. */
 int dsm_lmax_init(const float *feats, const float *target, int n, unsigned seed, float *params);
-/* Adam on the GPU (device ordinal): params in/out, losses[epochs] out. */
+/* AdamW on the GPU (device ordinal, decoupled weight decay):
+ * params in/out, losses[epochs] out. */
 int dsm_lmax_train(const float *feats, const float *target, int n, int epochs, int batch,
-                   float lr, unsigned seed, float *params, float *losses, int device);
+                   float lr, float weight_decay, unsigned seed, float *params,
+                   float *losses, int device);
 /* Loss (mean squared error of the standardised output) and its gradient
  * with respect to every parameter, on the n rows given. */
 int dsm_lmax_grad(const float *params, const float *feats, const float *target, int n,
                   float *grad, float *loss, int device);
-/* Attaches a parameter block to a context; log(lmax) predictions of
- * frequencies ilist[0..n) go to out (may be NULL). */
+/* Attaches a parameter block to a context.  dsm_lmax_predict writes the
+ * predicted log(lmax) (network output + feats[0]) of frequencies
+ * ilist[0..n) to out. */
 int dsm_set_lmax_model(dsm_ctx_t *ctx, const float *params);
 int dsm_lmax_predict(dsm_ctx_t *ctx, const int *ilist, int n, float *out);
 
