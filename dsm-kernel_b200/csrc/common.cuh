@@ -43,10 +43,22 @@ __host__ __device__ __forceinline__ cd conj(cd a) { return {a.re, -a.im}; }
 __host__ __device__ __forceinline__ cd cmul_i(double m, cd a) { return {-m * a.im, m * a.re}; }  // (i m) a
 __device__ __forceinline__ double cabs_(cd a) { return hypot(a.re, a.im); }
 
-// FP32 complex for the mixed path
-struct cf {
-    float re, im;
+// complex of a chosen real type (float on the mixed path, double on the
+// plain one); division by a real multiplies by its reciprocal
+template <class RL>
+struct cx {
+    RL re, im;
+    __host__ __device__ __forceinline__ friend cx operator+(cx a, cx b) { return {a.re + b.re, a.im + b.im}; }
+    __host__ __device__ __forceinline__ friend cx operator-(cx a, cx b) { return {a.re - b.re, a.im - b.im}; }
+    __host__ __device__ __forceinline__ friend cx operator-(cx a) { return {-a.re, -a.im}; }
+    __host__ __device__ __forceinline__ friend cx operator*(cx a, cx b) {
+        return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+    }
+    __host__ __device__ __forceinline__ friend cx operator*(RL a, cx b) { return {a * b.re, a * b.im}; }
+    __host__ __device__ __forceinline__ friend cx operator*(cx a, RL b) { return {a.re * b, a.im * b}; }
 };
+template <class RL>
+__host__ __device__ __forceinline__ cx<RL> cmul_i(RL m, cx<RL> a) { return {-m * a.im, m * a.re}; }  // (i m) a
 
 // ------------------------------------------------------------ errors
 struct Error : std::runtime_error {

@@ -26,19 +26,20 @@
 //                calamp (imt = 1, m = 0).
 //   k_psv_scan   the cutoff test (calamp, others.f90:1246-1264, the
 //                ismall > 20 exit, SGTpsv-MPI.f90:606-609, 902-905).
-//   k_psv_epi    TSGT / RSGT / SYNN from the l-contractions (calup,
-//                calupfluid, locallyCartesianDerivatives, udertotsgt,
-//                udertorsgt, utosynn, others.f90:161-344, 983-1031).
+// The epilogue (TSGT / RSGT / SYNN from the l-contractions) is psv_epi.cu.
 #include <algorithm>
 #include <cmath>
 
 #include "engine.cuh"
+#include "psv_epi.cuh"
 
 namespace dsm {
 namespace {
 
-constexpr int NS0 = 4, NS1 = 8, NS2 = 6;  // slots per |m|
-constexpr int NFLD = 5;                   // U, U', V/lsq, V'/lsq, l(l+1) V/lsq
+using psvk::NS0;
+using psvk::NS1;
+using psvk::NS2;
+using psvk::NFLD;  // U, U', V/lsq, V'/lsq, l(l+1) V/lsq
 constexpr int NB = 6;                     // basis right-hand sides of a solve
 
 struct PsvDev {
@@ -458,6 +459,37 @@ __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], const cd (&ane
     return false;
 }
 
+// Step k of the band loop away from its end (k <= n - 4: three
+// multipliers, the main update, a row entering): factor_step without the
+// end-of-band cases.
+template <int P, bool FAST>
+__device__ __forceinline__ void factor_step_main(int k, cd (&M)[4][4], const cd (&anew)[4], const FactorCtx& c) {
+    constexpr int S0 = P, S1 = (P + 1) & 3, S2 = (P + 2) & 3, S3 = (P + 3) & 3;
+    const cd D = M[S0][S0];
+    if (c.store && k >= c.ls) c.Dst[(size_t)(k - c.ls) * c.nsys + c.sys] = D;
+    const cd piv = crecipT<FAST>(D);
+    const cd zv0 = -M[S1][S0], zv1 = -M[S2][S0], zv2 = -M[S3][S0];
+    const cd wv0 = cmulT<FAST>(M[S1][S0], piv);
+    const cd wv1 = cmulT<FAST>(M[S2][S0], piv);
+    const cd wv2 = cmulT<FAST>(M[S3][S0], piv);
+    if (c.store && k >= c.lmin) {
+        cd* L = c.Lst + (size_t)k * 3 * c.nsys + c.sys;
+        L[0] = wv0;
+        L[c.nsys] = wv1;
+        L[2 * (size_t)c.nsys] = wv2;
+    }
+    M[S1][S1] = caddmulT<FAST>(M[S1][S1], wv0, zv0);
+    M[S2][S2] = caddmulT<FAST>(M[S2][S2], wv1, zv1);
+    M[S3][S3] = caddmulT<FAST>(M[S3][S3], wv2, zv2);
+    M[S2][S1] = caddmulT<FAST>(M[S2][S1], wv0, zv1);
+    M[S3][S2] = caddmulT<FAST>(M[S3][S2], wv1, zv2);
+    M[S3][S1] = caddmulT<FAST>(M[S3][S1], wv0, zv2);
+    M[S0][S1] = anew[0];
+    M[S0][S2] = anew[1];
+    M[S0][S3] = anew[2];
+    M[S0][S0] = anew[3];
+}
+
 // One thread per (omega, l) system: band assembly row by row and the
 // unpivoted complex-symmetric LDL^T (dcsymbdl0) streamed through the ring
 // window.  Multipliers of the rows the substitutions need go to Lst, pivots
@@ -562,6 +594,18 @@ __global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* _
             cp_async_wait<1>();
             __syncthreads();
         }
+        if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
+            entering(k, an);
+            factor_step_main<1, FAST>(k, M, an, c);
+            entering(k + 1, an);
+            factor_step_main<2, FAST>(k + 1, M, an, c);
+            entering(k + 2, an);
+            factor_step_main<3, FAST>(k + 2, M, an, c);
+            entering(k + 3, an);
+            factor_step_main<0, FAST>(k + 3, M, an, c);
+            if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+            continue;
+        }
         entering(k, an);
         if (factor_step<1, FAST>(k, M, an, T, c)) { T.Dn = M[1][1]; break; }
         entering(k + 1, an);
@@ -584,19 +628,24 @@ __global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* _
 // L(j+2,j) x(j+2) + L(j+1,j) x(j+1)], down to the deepest captured row.  The
 // multipliers stream through shared memory: the block copies BACK_CH rows of
 // its systems' factors with cp.async one chunk ahead of use (coalesced 512 B
-// rows), so the recurrence runs on shared-memory latency.  Values at
-// receiver stencil rows go to Xcap.  Bases 4 and 5 are the surface unit
-// vectors e_{n-1}, e_n.
+// rows), together with the rows' capture slots, so the recurrence runs on
+// shared-memory latency; zh is loaded one row ahead.  Values at receiver
+// stencil rows go to Xcap.  Bases 4 and 5 are the surface unit vectors
+// e_{n-1}, e_n.  FAST (mixed precision) uses fused multiply-adds and one
+// reciprocal per pivot; otherwise the reference's operation order.
 constexpr int BACK_SYS = 32;
 constexpr int BACK_THREADS = BACK_SYS * NB;  // 192
 constexpr int BACK_CH = 12;                  // rows per staged chunk (2 x 18 KB)
+static_assert(BACK_CH % 3 == 0, "the upward pass rotates three values per three rows");
 
-__global__ void __launch_bounds__(BACK_THREADS) k_psv_back(PsvDev d, int nsys, int jmin_loc,
+template <bool FAST>
+__global__ void __launch_bounds__(BACK_THREADS, 5) k_psv_back(PsvDev d, int nsys, int jmin_loc,
                                                            const int* __restrict__ capmap,
                                                            const cd* __restrict__ Lst, const cd* __restrict__ Dst,
                                                            cd* __restrict__ Zst, const SysTail* __restrict__ tail,
                                                            cd* __restrict__ Xcap) {
     __shared__ __align__(16) cd sL[2][BACK_CH][3][BACK_SYS];
+    __shared__ int sC[2][BACK_CH];
     const int sys0 = blockIdx.x * BACK_SYS;
     const int sl = threadIdx.x / NB, b = threadIdx.x - sl * NB;
     const int sys = sys0 + sl;
@@ -609,35 +658,49 @@ __global__ void __launch_bounds__(BACK_THREADS) k_psv_back(PsvDev d, int nsys, i
     if (valid && b < 4) {  // forward substitution of a source basis
         const cd a22raw = tail[sys].a22raw;
         cd z0 = mk(0.0), z1 = mk(0.0), z2 = mk(0.0);  // z(j-3), z(j-2), z(j-1)
-        for (int j = max(ls, 1); j <= n; ++j) {
-            const cd D = Dst[(size_t)(j - ls) * nsys + sys];
+        const int j0 = max(ls, 1);
+        // operands of row j, loaded one row ahead: D(j), L(j-3,2), L(j-2,1), L(j-1,0)
+        auto fetch = [&](int j, cd& D, cd& l3, cd& l2, cd& l1) {
+            D = Dst[(size_t)(j - ls) * nsys + sys];
+            l3 = j >= 4 ? L(j - 3, 2) : mk(0.0);
+            l2 = j >= 3 ? L(j - 2, 1) : mk(0.0);
+            l1 = j >= 3 ? L(j - 1, 0) : mk(0.0);
+        };
+        cd Dn, l3n, l2n, l1n;
+        if (j0 <= n) fetch(j0, Dn, l3n, l2n, l1n);
+        for (int j = j0; j <= n; ++j) {
+            const cd D = Dn, l3 = l3n, l2 = l2n, l1 = l1n;
+            if (j < n) fetch(j + 1, Dn, l3n, l2n, l1n);
             cd zc;
+            const cd rhs = mk(ls + b == j ? 1.0 : 0.0);
             if (j == 1) {
-                zc = mk(ls + b == 1 ? 1.0 : 0.0);
+                zc = rhs;
+            } else if (j == 2) {
+                zc = rhs - a22raw * z2;
+            } else if (FAST) {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
+                cd sum = cmulT<true>(l3, z0);
+                sum = caddmulT<true>(sum, l2, z1);
+                sum = caddmulT<true>(sum, l1, z2);
+                zc = rhs - sum;
+            } else if (j == 3) {  // a(2,3) z(1) + a(3,3) z(2)
+                cd sum = mk(0.0) + l2 * z1 + l1 * z2;
+                zc = rhs - sum;
             } else {
-                const cd rhs = mk(ls + b == j ? 1.0 : 0.0);
-                if (j == 2) {
-                    zc = rhs - a22raw * z2;
-                } else if (j == 3) {  // a(2,3) z(1) + a(3,3) z(2)
-                    cd sum = mk(0.0) + L(1, 1) * z1 + L(2, 0) * z2;
-                    zc = rhs - sum;
-                } else {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
-                    cd sum = mk(0.0) + L(j - 3, 2) * z0 + L(j - 2, 1) * z1 + L(j - 1, 0) * z2;
-                    zc = rhs - sum;
-                }
+                cd sum = mk(0.0) + l3 * z0 + l2 * z1 + l1 * z2;
+                zc = rhs - sum;
             }
-            Zst[((size_t)(j - ls) * 4 + b) * nsys + sys] = zc / D;
+            Zst[((size_t)(j - ls) * 4 + b) * nsys + sys] = FAST ? cmulT<true>(zc, crecipT<true>(D)) : zc / D;
             z0 = z1;
             z1 = z2;
             z2 = zc;
         }
     }
     cd x0 = mk(0.0), x1 = mk(0.0), x2 = mk(0.0);  // x(j+1), x(j+2), x(j+3)
-    auto capture = [&](int jloc, cd v) {
-        const int c = capmap[jloc + it - 1];
-        if (c >= 0) Xcap[((size_t)c * NB + b) * nsys + sys] = v;
-    };
     if (valid) {
+        auto capture = [&](int jloc, cd v) {
+            const int c = capmap[jloc + it - 1];
+            if (c >= 0) Xcap[((size_t)c * NB + b) * nsys + sys] = v;
+        };
         const SysTail tl = tail[sys];
         cd xn;
         if (b < 4) xn = (n >= ls) ? ZH(n) : mk(0.0);
@@ -668,6 +731,34 @@ __global__ void __launch_bounds__(BACK_THREADS) k_psv_back(PsvDev d, int nsys, i
             const int sidx = e % nsb, rp = e / nsb, i = rp / 3, p = rp - 3 * i;
             cp_async16(&sL[buf][i][p][sidx], &Lst[((size_t)(hi - i) * 3 + p) * nsys + sys0 + sidx]);
         }
+        if (threadIdx.x < cnt) sC[buf][threadIdx.x] = capmap[hi - threadIdx.x + it - 1];
+    };
+    // zh of a source basis at local row j (zero below the source rows)
+    const bool src = valid && b < 4;
+    auto zh_at = [&](int j) { return (src && j >= ls && j >= jmin_loc) ? ZH(j) : mk(0.0); };
+    cd zhn = zh_at(top);
+    // one upward row: x(j) from x(j+1) = xa, x(j+2) = xb, x(j+3) = xc; the
+    // result replaces xc (the oldest).  x(n+1) = 0 makes row n-2 the general form.
+    auto row = [&](int buf, int i, int j1, const cd& xa, const cd& xb, cd& xc) {
+        const cd L1 = sL[buf][i][0][sl], L2 = sL[buf][i][1][sl], L3 = sL[buf][i][2][sl];
+        const cd zh = zhn;
+        zhn = zh_at(j1 - 1);
+        cd v;
+        if (FAST) {
+            cd sum = cmulT<true>(L3, xc);
+            sum = caddmulT<true>(sum, L2, xb);
+            sum = caddmulT<true>(sum, L1, xa);
+            v = zh - sum;
+        } else if (j1 == n - 2) {
+            cd sum = mk(0.0) + L2 * xb + L1 * xa;
+            v = zh - sum;
+        } else {
+            cd sum = mk(0.0) + L3 * xc + L2 * xb + L1 * xa;
+            v = zh - sum;
+        }
+        const int c = sC[buf][i];
+        if (c >= 0) Xcap[((size_t)c * NB + b) * nsys + sys] = v;
+        xc = v;
     };
     stage(0, 0);
     cp_async_commit();
@@ -679,20 +770,17 @@ __global__ void __launch_bounds__(BACK_THREADS) k_psv_back(PsvDev d, int nsys, i
         if (valid) {
             const int hi = top - c * BACK_CH, cnt = min(BACK_CH, hi - jmin_loc + 1);
             const int buf = c & 1;
-            for (int i = 0; i < cnt; ++i) {
-                const int j1 = hi - i;
-                const cd L1 = sL[buf][i][0][sl], L2 = sL[buf][i][1][sl], L3 = sL[buf][i][2][sl];
-                cd zh = mk(0.0);
-                if (b < 4 && j1 >= ls) zh = ZH(j1);
-                cd sum;
-                if (j1 == n - 2) sum = mk(0.0) + L2 * x1 + L1 * x0;
-                else sum = mk(0.0) + L3 * x2 + L2 * x1 + L1 * x0;
-                const cd v = zh - sum;
-                capture(j1, v);
-                x2 = x1;
-                x1 = x0;
-                x0 = v;
+            // rotating roles: (x0, x1, x2) = (x(j+1), x(j+2), x(j+3)) at i % 3 == 0
+            int i = 0;
+            for (; i + 3 <= cnt; i += 3) {
+                row(buf, i, hi - i, x0, x1, x2);          // x2 <- x(j)
+                row(buf, i + 1, hi - i - 1, x2, x0, x1);  // x1 <- x(j-1)
+                row(buf, i + 2, hi - i - 2, x1, x2, x0);  // x0 <- x(j-2)
             }
+            // only the last chunk can end with one or two rows (BACK_CH % 3 == 0),
+            // so the roles need not be restored after them
+            if (i < cnt) row(buf, i, hi - i, x0, x1, x2);
+            if (i + 1 < cnt) row(buf, i + 1, hi - i - 1, x2, x0, x1);
         }
         __syncthreads();  // the buffer is refilled two chunks later
     }
@@ -1313,193 +1401,6 @@ __global__ void k_psv_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ra
     cut[w] = c;
 }
 
-// ---------------------------------------------------------------- epilogue
-// TC: double (FP64 contraction) or float (tensor-core contraction)
-template <class TC>
-__global__ void k_psv_epi(PsvDev d, int w, const double* __restrict__ thx, const double* __restrict__ ths,
-                          const int* __restrict__ pole, const int* __restrict__ freqs,
-                          const TC* __restrict__ C0, const TC* __restrict__ C1,
-                          const TC* __restrict__ C2, double* __restrict__ tsgt,
-                          double* __restrict__ rsgt, double* __restrict__ synn, int back) {
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    const int R = d.R, Th = d.Th;
-    if (idx >= Th * (R + 1)) return;
-    int it = idx / (R + 1), r = idx % (R + 1);
-    const bool surf = r == R;
-    const bool isp = pole[it] != 0;
-    const int M[3] = {NS0 * (R + 1) * NFLD * 2, NS1 * (R + 1) * NFLD * 2, NS2 * (R + 1) * NFLD * 2};
-    const TC* Cm[3] = {C0, C1, C2};
-    const double x = thx[it], s = ths[it];
-    const double fs = (double)(float)s, fc = (double)(float)(x / s);
-    const double fr = surf ? 1.0 : d.fr[r];
-    const bool fluid = !surf && d.fluid[r];
-    const double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
-    const cd comega = mk(omega, -d.omegai);
-    cd T[20], Rg[10], S[10];
-    for (auto& v : T) v = mk(0.0);
-    for (auto& v : Rg) v = mk(0.0);
-    for (auto& v : S) v = mk(0.0);
-    cd efl = mk(0.0);
-    if (fluid) {  // calupfluid factor omega/3/lambda(omega)
-        const double deuxsurpi = 0.63661977236, unsurdeuxpi = 0.15915494309,
-                     unsurtrois = 0.33333333333333333333;
-        double lam = d.lam[r], qk = d.qkp[r];
-        cd fl = mk(lam * 1.0, lam * (1.0 / qk));
-        double fac = 1 + deuxsurpi / qk * log(unsurdeuxpi * comega.re);
-        fl = mk(fl.re * fac, fl.im * fac);
-        efl = comega * unsurtrois / fl;
-    }
-    for (int mi = 0; mi < 3; ++mi) {
-        int nq = mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2);
-        for (int q = 0; q < nq; ++q) {
-            int per = mi == 0 ? 4 : (mi == 1 ? 4 : 3);
-            int sg = q / per, k = q % per;
-            int m = mi == 0 ? 0 : (sg == 0 ? -mi : mi);
-            bool isback = (mi == 0 && k == 3) || (mi == 1 && k >= 2);
-            if (isback && !back) continue;
-            int imt = 0, icomp = 0;
-            if (mi == 0) { if (k < 3) imt = k + 1; else icomp = 1; }
-            else if (mi == 1) { if (k < 2) imt = 4 + k; else icomp = k; }
-            else imt = k == 0 ? 2 : (k == 1 ? 3 : 6);
-            if (surf && isback) continue;
-            if (isp && mi != 0) continue;  // only bvec(1,0) survives at the poles
-            auto G = [&](int f, int b) {
-                size_t row = ((size_t)(q * NFLD + f) * 2) * (R + 1) + r;
-                size_t col = (size_t)b * Th + it;
-                const TC* C = Cm[mi];
-                return mk((double)C[row + (size_t)M[mi] * col], (double)C[row + (R + 1) + (size_t)M[mi] * col]);
-            };
-            double sigma = (m < 0 && (mi & 1)) ? -1.0 : 1.0;
-            double mm = (double)m, m2 = mm * mm;
-            cd d11 = mk(0.0), d12 = mk(0.0), d13 = mk(0.0), d21 = mk(0.0), d22 = mk(0.0),
-               d23 = mk(0.0), d31 = mk(0.0), d32 = mk(0.0), d33 = mk(0.0);
-            cd PU = G(0, 0);
-            if (surf) {
-                cd u1, u2 = mk(0.0), u3 = mk(0.0);
-                if (isp) {
-                    u1 = PU;
-                } else {
-                    u1 = sigma * PU;
-                    u2 = sigma * G(2, 1);
-                    u3 = sigma * cmul_i(mm / s, G(2, 0));
-                }
-                if (imt == 1) { S[0] = S[0] + u1; S[4] = S[4] + u2; }
-                if (imt == 2) {
-                    S[2] = S[2] + 5.e-1 * u1; S[3] = S[3] - 5.e-1 * u1;
-                    S[5] = S[5] - 5.e-1 * u2; S[6] = S[6] - 5.e-1 * u2;
-                }
-                if (imt == 3) {
-                    S[2] = S[2] - 5.e-1 * u1; S[3] = S[3] - 5.e-1 * u1;
-                    S[5] = S[5] - 5.e-1 * u2; S[6] = S[6] + 5.e-1 * u2;
-                }
-                if (imt == 4) { S[1] = S[1] + u1; S[8] = S[8] + u2; }
-                if (imt == 5) { S[9] = S[9] + u3; }
-                if (imt == 6) { S[7] = S[7] - u3; }
-                continue;
-            }
-            if (fluid) {
-                cd e = efl * (isp ? PU : sigma * PU);
-                d11 = e; d22 = e; d33 = e;
-            } else if (isp) {
-                cd u1 = PU, udr1 = G(1, 0);
-                d11 = udr1;
-                d22 = u1 / fr;
-                d33 = u1 / fr;
-            } else {
-                cd PV = G(2, 0), DV = G(2, 1);
-                cd u1 = sigma * PU, u2 = sigma * DV, u3 = sigma * cmul_i(mm / s, PV);
-                cd udr1 = sigma * G(1, 0), udr2 = sigma * G(3, 1), udr3 = sigma * cmul_i(mm / s, G(3, 0));
-                cd udt1 = (m >= 0) ? G(0, 1) : mk(0.0);
-                cd udt2 = sigma * (-(x / s) * DV + (m2 / (1 - x * x)) * PV - G(4, 0));
-                cd udt3 = sigma * cmul_i(mm, -(x / (1 - x * x)) * PV + (1.0 / s) * DV);
-                cd udp1 = sigma * cmul_i(mm, PU), udp2 = sigma * cmul_i(mm, DV);
-                cd udp3 = sigma * ((-m2 / s) * PV);
-                d11 = udr1;
-                d12 = (udt1 - u2) / fr;
-                d13 = (udp1 / fs - u3) / fr;
-                d21 = udr2;
-                d22 = (udt2 + u1) / fr;
-                d23 = (udp2 / fs - u3 * fc) / fr;
-                d31 = udr3;
-                d32 = udt3 / fr;
-                d33 = (udp3 / fs + u1 + u2 * fc) / fr;
-            }
-            if (icomp) {  // udertorsgt
-                if (icomp == 1) {
-                    Rg[0] = Rg[0] + d11;
-                    Rg[1] = Rg[1] - 5.e-1 * d21 - 5.e-1 * d12;
-                    Rg[2] = Rg[2] + 5.e-1 * d22 - 5.e-1 * d33;
-                    Rg[3] = Rg[3] - 5.e-1 * d22 - 5.e-1 * d33;
-                } else if (icomp == 2) {
-                    Rg[4] = Rg[4] + d11;
-                    Rg[5] = Rg[5] - 5.e-1 * d22 - 5.e-1 * d33;
-                    Rg[6] = Rg[6] - 5.e-1 * d22 + 5.e-1 * d33;
-                    Rg[8] = Rg[8] - 5.e-1 * d12 - 5.e-1 * d21;
-                } else {
-                    Rg[7] = Rg[7] - 5.e-1 * d23 - 5.e-1 * d32;
-                    Rg[9] = Rg[9] + 5.e-1 * d13 + 5.e-1 * d31;
-                }
-                continue;
-            }
-            // udertotsgt
-            if (imt == 1) {
-                T[0] = T[0] + d11;
-                T[2] = T[2] - 5.e-1 * d22 - 5.e-1 * d33;
-                T[5] = T[5] - 5.e-1 * d12 - 5.e-1 * d21;
-                T[9] = T[9] + 5.e-1 * d22 - 5.e-1 * d33;
-            } else if (imt == 2 || imt == 3) {
-                double sgn = imt == 2 ? 1.0 : -1.0;
-                T[1] = T[1] - 5.e-1 * d11;
-                T[3] = T[3] + 2.5e-1 * d22 + 2.5e-1 * d33;
-                T[7] = T[7] + (sgn * 2.5e-1) * d12 + (sgn * 2.5e-1) * d21;
-                T[8] = T[8] + (sgn * 5.e-1) * d11;
-                T[10] = T[10] - 2.5e-1 * d22 + 2.5e-1 * d33;
-                T[11] = T[11] - (sgn * 2.5e-1) * d22 - (sgn * 2.5e-1) * d33;
-                T[16] = T[16] - 1.25e-1 * d12 - 1.25e-1 * d21;
-                T[17] = T[17] + 1.25e-1 * d12 + 1.25e-1 * d21;
-                T[18] = T[18] + (sgn * 1.25e-1) * d22 - (sgn * 1.25e-1) * d33;
-                T[19] = T[19] + (sgn * 1.25e-1) * d22 - (sgn * 1.25e-1) * d33;
-            } else if (imt == 4) {
-                T[4] = T[4] + d11;
-                T[6] = T[6] - 5.e-1 * d22 - 5.e-1 * d33;
-                T[12] = T[12] - 2.5e-1 * d12 - 2.5e-1 * d21;
-                T[13] = T[13] + 2.5e-1 * d12 + 2.5e-1 * d21;
-                T[14] = T[14] + 2.5e-1 * d22 - 2.5e-1 * d33;
-                T[15] = T[15] - 2.5e-1 * d22 + 2.5e-1 * d33;
-            } else if (imt == 5) {
-                T[12] = T[12] + 2.5e-1 * d13 + 2.5e-1 * d31;
-                T[13] = T[13] + 2.5e-1 * d13 + 2.5e-1 * d31;
-                T[14] = T[14] - 2.5e-1 * d23 - 2.5e-1 * d32;
-                T[15] = T[15] - 2.5e-1 * d23 - 2.5e-1 * d32;
-            } else if (imt == 6) {
-                T[16] = T[16] + 2.5e-1 * d13 + 2.5e-1 * d31;
-                T[17] = T[17] + 2.5e-1 * d13 + 2.5e-1 * d31;
-                T[18] = T[18] - 2.5e-1 * d23 - 2.5e-1 * d32;
-                T[19] = T[19] + 2.5e-1 * d23 + 2.5e-1 * d32;
-            }
-        }
-    }
-    if (surf) {
-        if (synn)
-            for (int c = 0; c < 10; ++c) {
-                size_t o = ((size_t)w * Th + it) * 10 + c;
-                synn[2 * o] = S[c].re;
-                synn[2 * o + 1] = S[c].im;
-            }
-        return;
-    }
-    size_t pt = ((size_t)w * Th + it) * R + r;
-    for (int c = 0; c < 20; ++c) {
-        tsgt[2 * (pt * 20 + c)] = T[c].re;
-        tsgt[2 * (pt * 20 + c) + 1] = T[c].im;
-    }
-    if (rsgt)
-        for (int c = 0; c < 10; ++c) {
-            rsgt[2 * (pt * 10 + c)] = Rg[c].re;
-            rsgt[2 * (pt * 10 + c) + 1] = Rg[c].im;
-        }
-}
-
 // ---------------------------------------------------------------- engine
 class PsvEngine : public Engine {
   public:
@@ -1687,7 +1588,7 @@ class PsvEngine : public Engine {
         size_t per = (n + 1) * 3 * 16 + (n - ls + 2) * 4 * 16 + (size_t)ncap * NB * 16 + NSLOT * NB * 16;
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
-        nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(32768, (fr / 3) / per));
+        nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(65536, (fr / 3) / per));
         size_t nsys = nsys_max;
         B0.reserve((size_t)F * d.ncol_tot * 4);
         B1.reserve((size_t)F * d.ncol_tot * 4);
@@ -1767,8 +1668,12 @@ class PsvEngine : public Engine {
             k_psv_solve<false><<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Dst.p,
                                                                    tails.p);
         DSM_LAUNCH(*this);
-        k_psv_back<<<(nsys + BACK_SYS - 1) / BACK_SYS, BACK_THREADS, 0, st>>>(d, nsys, jmin_loc, capmap.p, Lst.p,
-                                                                              Dst.p, Zst.p, tails.p, Xcap.p);
+        if (mixed())
+            k_psv_back<true><<<(nsys + BACK_SYS - 1) / BACK_SYS, BACK_THREADS, 0, st>>>(
+                d, nsys, jmin_loc, capmap.p, Lst.p, Dst.p, Zst.p, tails.p, Xcap.p);
+        else
+            k_psv_back<false><<<(nsys + BACK_SYS - 1) / BACK_SYS, BACK_THREADS, 0, st>>>(
+                d, nsys, jmin_loc, capmap.p, Lst.p, Dst.p, Zst.p, tails.p, Xcap.p);
         kend(id, alg * nsys, 0.0);
         DSM_LAUNCH(*this);
         id = kid("psv_source_coef");
@@ -1797,19 +1702,23 @@ class PsvEngine : public Engine {
 
     void epilogue(const int* fr_, int w, int nf) override {
         (void)nf;
-        int n = Th * (R + 1);
+        psvk::EpiDev e{};
+        e.R = R;
+        e.Th = Th;
+        e.tlen = d.tlen;
+        e.omegai = d.omegai;
+        e.fluid = d.fluid;
+        e.lam = d.lam;
+        e.qkp = d.qkp;
+        e.fr = d.fr;
         int id = kid("psv_epilogue");
         kbegin(id);
-        if (mixed())
-            k_psv_epi<float><<<(n + 127) / 128, 128, 0, st>>>(d, w, th.x.p, th.s.p, th.pole.p, fr_, c32(w, 0),
-                                                              c32(w, 1), c32(w, 2), out_t.p,
-                                                              rsgt_sw ? out_r.p : nullptr,
-                                                              synn_sw ? out_s.p : nullptr, rsgt_sw);
-        else
-            k_psv_epi<double><<<(n + 127) / 128, 128, 0, st>>>(d, w, th.x.p, th.s.p, th.pole.p, fr_, c64(0),
-                                                               c64(1), c64(2), out_t.p,
-                                                               rsgt_sw ? out_r.p : nullptr,
-                                                               synn_sw ? out_s.p : nullptr, rsgt_sw);
+        const bool tc = mixed();
+        const void* c0 = tc ? (const void*)c32(w, 0) : (const void*)c64(0);
+        const void* c1 = tc ? (const void*)c32(w, 1) : (const void*)c64(1);
+        const void* c2 = tc ? (const void*)c32(w, 2) : (const void*)c64(2);
+        psvk::launch_epilogue(e, w, th.x.p, th.s.p, th.pole.p, fr_, c0, c1, c2, tc, out_t.p,
+                              rsgt_sw ? out_r.p : nullptr, synn_sw ? out_s.p : nullptr, st);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
     }

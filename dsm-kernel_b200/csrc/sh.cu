@@ -616,7 +616,7 @@ class ShEngine : public Engine {
         size_t per = (nn + 1) * 16 + (nn - d.srow + 2) * 2 * 16 + (size_t)ncap * 3 * 16;
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
-        nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(32768, (fr / 3) / per));
+        nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(65536, (fr / 3) / per));
         size_t nsys = nsys_max;
         a0.reserve((size_t)F * (nn + 1) * 2);
         a2.reserve((size_t)F * (nn + 1) * 2);
