@@ -187,27 +187,34 @@ void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
         tc::encode_a(&maps.a[m], Apc[m].p, tc_fmt, kcA, rows_m[m], F, tc_bk);
         tc::encode_b(&maps.b[m], Bpc[m].p, tc_fmt, kcB, 2 * Th, tc_bk);
     }
+    // per (frequency, |m|): the leading rows against all 2 Th basis
+    // columns, the remaining rows against the first Th
     std::vector<tc::Problem> hp;
-    const int N = 2 * Th, tn = (N + tc::BN - 1) / tc::BN;
     for (int w = 0; w < nf; ++w)
         for (int m = m_lo; m <= 2; ++m) {
             if (!rows_m[m]) continue;
-            tc::Problem P{};
-            P.amap = m;
-            P.z = w;
-            P.bmap = m;
-            P.kblocks = (nord[w] + tc_bk - 1) / tc_bk;
-            P.M = rows_m[m];
-            P.N = N;
-            P.tiles_n = tn;
-            P.C = Cmix.p + (size_t)w * c_total() + c_off(m);
-            P.sa = sA[m].p + (size_t)w * rows_m[m];
-            P.sb = sB[m].p;
-            P.ldc = P.M;
-            hp.push_back(P);
-            const double kp = (double)P.kblocks * tc_bk;
-            tflops += 3.0 * 2.0 * P.M * (double)N * kp;
-            tc_bytes += 4.0 * ((double)P.M + N) * kp + 4.0 * (double)P.M * N;
+            const int rf = full_rows(m);
+            for (int g = 0; g < 2; ++g) {
+                const int row0 = g == 0 ? 0 : rf, M = g == 0 ? rf : rows_m[m] - rf, N = g == 0 ? 2 * Th : Th;
+                if (M <= 0) continue;
+                tc::Problem P{};
+                P.amap = m;
+                P.z = w;
+                P.bmap = m;
+                P.row0 = row0;
+                P.kblocks = (nord[w] + tc_bk - 1) / tc_bk;
+                P.M = M;
+                P.N = N;
+                P.tiles_n = (N + tc::BN - 1) / tc::BN;
+                P.C = Cmix.p + (size_t)w * c_total() + c_off(m) + row0;
+                P.sa = sA[m].p + (size_t)w * rows_m[m] + row0;
+                P.sb = sB[m].p;
+                P.ldc = rows_m[m];
+                hp.push_back(P);
+                const double kp = (double)P.kblocks * tc_bk;
+                tflops += 3.0 * 2.0 * P.M * (double)N * kp;
+                tc_bytes += 4.0 * ((double)P.M + N) * kp + 4.0 * (double)P.M * N;
+            }
         }
     tcp.reserve(hp.size());
     id = kid("lsum_tc");
@@ -217,7 +224,7 @@ void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
         int tiles = 0;
         for (int i = 0; i < np; ++i) {
             hp[g + i].tile0 = tiles;
-            tiles += ((hp[g + i].M + tc::BM - 1) / tc::BM) * tn;
+            tiles += ((hp[g + i].M + tc::BM - 1) / tc::BM) * hp[g + i].tiles_n;
         }
         DSM_CUDA(cudaMemcpyAsync(tcp.p + g, hp.data() + g, sizeof(tc::Problem) * np, cudaMemcpyHostToDevice, st));
         tc::launch(maps, tcp.p + g, np, tiles, tc_fmt, tc_bk, tc_flags, tc_chunk, tc_err.p, nsm, st);
@@ -244,17 +251,25 @@ void Engine::build_weights(const double* d_r, const double* d_rrsta) {
 
 // C[mi] (rows x 2Th, column-major) = A^T (A stored [row][l], ld Lcap) x
 // B (stored [col][l], ld lcapB), summed over the K orders of frequency w.
+// The leading full_rows(mi) rows take all 2 Th columns, the rest the first Th.
 void Engine::gemm_fp64(int w, int mi, int K) {
-    const int M = rows_m[mi], N = 2 * Th;
+    const int M = rows_m[mi], rf = full_rows(mi);
     if (M == 0) return;
     const double one = 1.0, zero = 0.0;
     const double* A = Afld[mi].p + (size_t)w * M * Lcap;
     int id = kid("lsum_dgemm");
     kbegin(id);
-    DSM_CUBLAS(cublasDgemm(cub, CUBLAS_OP_T, CUBLAS_OP_N, M, N, K, &one, A, Lcap, basis[mi].p, lcapB,
-                           &zero, Cgemm.p + c_off(mi), M));
-    kend(id, 8.0 * ((double)M * K + (double)K * N + (double)M * N), 2.0 * M * N * (double)K);
-    launches++;
+    double bytes = 0.0, flops = 0.0;
+    for (int g = 0; g < 2; ++g) {
+        const int row0 = g == 0 ? 0 : rf, Mg = g == 0 ? rf : M - rf, N = g == 0 ? 2 * Th : Th;
+        if (Mg <= 0) continue;
+        DSM_CUBLAS(cublasDgemm(cub, CUBLAS_OP_T, CUBLAS_OP_N, Mg, N, K, &one, A + (size_t)row0 * Lcap, Lcap,
+                               basis[mi].p, lcapB, &zero, Cgemm.p + c_off(mi) + row0, M));
+        bytes += 8.0 * ((double)Mg * K + (double)K * N + (double)Mg * N);
+        flops += 2.0 * Mg * N * (double)K;
+        launches++;
+    }
+    kend(id, bytes, flops);
 }
 
 // Grows the order capacity of the field matrices and of the probe table,
@@ -467,7 +482,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
                 for (int mi = m_lo; mi <= 2; ++mi) gemm_fp64(w, mi, hc[w].norders);
             epilogue(d_freqs.p, w, nf);
             for (int mi = m_lo; mi <= 2; ++mi)
-                stats.lsum_flops += 2.0 * rows_m[mi] * 2.0 * Th * hc[w].norders;
+                stats.lsum_flops += 2.0 * (2.0 * full_rows(mi) + (rows_m[mi] - full_rows(mi))) * Th * hc[w].norders;
         }
         DSM_CUDA(cudaEventRecord(eg1, st));
         // --- 5: outputs

@@ -89,6 +89,11 @@ class Engine {
 
     // rows of the field matrix per |m| (set by the mode)
     int rows_m[3] = {0, 0, 0};
+    // leading rows of each field matrix contracted with all 2 Th basis
+    // columns; the remaining rows need only the first Th (set by the mode,
+    // all rows unless it groups its fields)
+    int rows_full[3] = {-1, -1, -1};
+    int full_rows(int m) const { return rows_full[m] < 0 ? rows_m[m] : rows_full[m]; }
     // offset of the |m| block inside Cgemm (one frequency)
     size_t c_off(int mi) const {
         size_t off = 0;

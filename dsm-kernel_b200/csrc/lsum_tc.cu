@@ -5,20 +5,22 @@
 //               A tile and of a 128 x BK B tile (four bulk tensor loads,
 //               one mbarrier with the byte count)
 //   warp 1      MMA issuer: per stage and 16-order step, three
-//               tcgen05.mma: hi*hi into a chunk accumulator, hi*lo and
-//               lo*hi into the tile's cross-term accumulator; tcgen05.commit
-//               frees the stage and hands finished accumulators over
-//   warps 2..9  epilogue: tcgen05.ld of the accumulators (two warps per
-//               32-lane quarter, 64 columns each), FP64 sum of the hi*hi
+//               tcgen05.mma (hi*hi, hi*lo, lo*hi) into the current chunk
+//               accumulator; tcgen05.commit frees the stage and hands
+//               finished chunk accumulators over
+//   warps 2..9  epilogue: tcgen05.ld of the chunk accumulators (two warps
+//               per 32-lane quarter, 64 columns each), FP64 sum of the
 //               chunks, row x column scaling, coalesced column-major stores
 // Accuracy: the tensor cores add each step into the FP32 accumulator with a
 // rounding relative to the accumulator's magnitude, so a long order sum
-// loses bits in proportion to its length.  The hi*hi products therefore go
-// into short chunks (chunk stages of BK orders) whose partial sums the
-// epilogue adds in FP64, and the cross terms (2^-11 smaller) get their own
-// accumulator.  Tensor memory (512 columns): three hi*hi chunk buffers of
-// 128 columns, so the epilogue drains one while the MMAs fill the next, and
-// the tile's cross-term accumulator (freed as soon as it is read).  TC_REVERSE runs the orders from high to low.
+// loses bits in proportion to its length.  The products therefore go into
+// short chunks (chunk stages of BK orders) whose partial sums the epilogue
+// adds in FP64.  The cross terms (2^-11 smaller than hi*hi) share the chunk
+// accumulator: each stage issues them before its hi*hi products, so in a
+// one-stage chunk they are summed while the accumulator is still small.  Tensor
+// memory (512 columns): four chunk buffers of 128 columns, so the epilogue
+// drains a pair while the MMAs fill the other pair, across tile boundaries
+// too.  TC_REVERSE runs the orders from high to low.
 // Every wait is bounded: after about a second a role raises the CTA's abort
 // flag, all roles leave their loops, the issued copies and MMAs are waited
 // for (again bounded), the tensor memory is freed and the error word is set.
@@ -41,7 +43,7 @@ constexpr int EPI_THREADS = 256;                 // warps 2..9
 constexpr int NTHREADS = 64 + EPI_THREADS;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int SMEM_STAGES = 192 * 1024;         // operand stages
-constexpr int NHB = 3;                          // hi*hi chunk buffers in tensor memory
+constexpr int NHB = 4;                          // chunk buffers in tensor memory
 constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;  // 1 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -145,18 +147,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
 }
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
 __device__ __forceinline__ void decode(const Problem* ps, int np, int t, int& p, int& mt, int& nt) {
     p = 0;
     while (p + 1 < np && ps[p + 1].tile0 <= t) ++p;
@@ -173,7 +163,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
     constexpr int STAGES = SMEM_STAGES / STAGE;
     extern __shared__ unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], hfull[NHB], hempty[NHB], xfull, xempty, fin;
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], hfull[NHB], hempty[NHB], fin;
     __shared__ uint32_t tmem_sh;
     __shared__ int abort_sh;
     __shared__ Problem ps[MAXP];
@@ -195,8 +185,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             mbar_init(&hfull[b], 1);
             mbar_init(&hempty[b], EPI_THREADS);
         }
-        mbar_init(&xfull, 1);
-        mbar_init(&xempty, EPI_THREADS);
         mbar_init(&fin, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.a[0])) : "memory");
@@ -212,8 +200,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_sh;
-    // tensor memory: hi*hi chunk accumulators hh[0..NHB) at columns
-    // [0, NHB BN), the tile's cross-term accumulator x at [NHB BN, 4 BN)
+    // tensor memory: chunk accumulators [0..NHB) at columns [0, NHB BN)
 
     if (warp == 0) {
         if (lane == 0) {  // ---------------------------------------- producer
@@ -233,8 +220,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     unsigned char* sp = base + s * STAGE;
                     const int x = (reverse ? P.kblocks - 1 - kb : kb) * BK;
                     mbar_expect_tx(&full[s], STAGE);
-                    tma_a(&maps.a[P.amap], sp, &full[s], x, mt * BM, P.z, 0);
-                    tma_a(&maps.a[P.amap], sp + A_BYTES, &full[s], x, mt * BM, P.z, 1);
+                    tma_a(&maps.a[P.amap], sp, &full[s], x, P.row0 + mt * BM, P.z, 0);
+                    tma_a(&maps.a[P.amap], sp + A_BYTES, &full[s], x, P.row0 + mt * BM, P.z, 1);
                     tma_b(&maps.b[P.bmap], sp + 2 * A_BYTES, &full[s], x, nt * BN, 0);
                     tma_b(&maps.b[P.bmap], sp + 2 * A_BYTES + B_BYTES, &full[s], x, nt * BN, 1);
                 }
@@ -247,15 +234,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {  // ---------------------------------------- MMA issuer
-            int it = 0, tcnt = 0, cc = 0;
+            int it = 0, cc = 0;
             bool ok = true;
-            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tcnt) {
+            for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 int p, mt, nt;
                 decode(ps, np, t, p, mt, nt);
                 const int kbn = ps[p].kblocks, ch = chunk > 0 ? chunk : kbn;
-                if (!mbar_wait(&xempty, (tcnt & 1) ^ 1, abort_flag)) break;
-                tc_fence_after();
-                const uint32_t dx = tmem + (uint32_t)(NHB * BN);
                 uint32_t dh = tmem;
                 int hb = 0;
                 for (int kb = 0; kb < kbn; ++kb, ++it) {
@@ -277,12 +261,18 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     tc_fence_after();
                     const uint32_t ah = smem_u32(base + s * STAGE), al = ah + A_BYTES;
                     const uint32_t bh = ah + 2 * A_BYTES, bl = bh + B_BYTES;
+                    // the cross terms first: while the accumulator holds only
+                    // them (2^-11 of hi*hi), their roundings are that much smaller
 #pragma unroll
                     for (int j = 0; j < BK / 16; ++j) {
                         const uint32_t o = 32u * j;
-                        mma_f16(dh, sdesc<BK>(ah + o), sdesc<BK>(bh + o), idesc, (cfirst && j == 0) ? 0u : 1u);
-                        mma_f16(dx, sdesc<BK>(ah + o), sdesc<BK>(bl + o), idesc, (kb == 0 && j == 0) ? 0u : 1u);
-                        mma_f16(dx, sdesc<BK>(al + o), sdesc<BK>(bh + o), idesc, 1u);
+                        mma_f16(dh, sdesc<BK>(ah + o), sdesc<BK>(bl + o), idesc, (cfirst && j == 0) ? 0u : 1u);
+                        mma_f16(dh, sdesc<BK>(al + o), sdesc<BK>(bh + o), idesc, 1u);
+                    }
+#pragma unroll
+                    for (int j = 0; j < BK / 16; ++j) {
+                        const uint32_t o = 32u * j;
+                        mma_f16(dh, sdesc<BK>(ah + o), sdesc<BK>(bh + o), idesc, 1u);
                     }
                     mma_commit(&empty[s]);
                     if (kb % ch == ch - 1 || kb == kbn - 1) {
@@ -290,7 +280,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         ++cc;
                     }
                 }
-                if (ok) mma_commit(&xfull);
             }
             // all issued MMAs complete before tensor memory is released
             mma_commit(&fin);
@@ -298,12 +287,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
     } else {  // ------------------------------------------------------ epilogue
         // two warps per tensor-memory lane quarter, each owning 64 columns;
-        // the hi*hi chunks are summed in FP64 registers
+        // the chunks are summed in FP64 registers
         const int q = warp & 3, half = (warp - 2) >> 2;
         const uint32_t lanes = (uint32_t)(q * 32) << 16;
-        int tcnt = 0, cc = 0;
+        int cc = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tcnt) {
+        for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
             int p, mt, nt;
             decode(ps, np, t, p, mt, nt);
             const Problem& P = ps[p];
@@ -342,7 +331,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             if (ok && (nch & 1)) {  // the odd last chunk
                 const int hb = cc % NHB;
                 const bool got = mbar_wait(&hfull[hb], (cc / NHB) & 1, abort_flag);
-                if (!__all_sync(0xffffffffu, got)) break;
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    break;
+                }
                 tc_fence_after();
                 const uint32_t ta = tmem + lanes + (uint32_t)(hb * BN + half * 64);
 #pragma unroll
@@ -358,23 +350,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 ++cc;
             }
             if (!ok) break;
-            const bool got = mbar_wait(&xfull, tcnt & 1, abort_flag);
-            if (!__all_sync(0xffffffffu, got)) break;
-            tc_fence_after();
             const int m = mt * BM + q * 32 + lane;
             const bool mv = m < P.M;
             const double rs = mv ? (double)P.sa[m] : 0.0;
             float* Cm = P.C + m;
-            // the cross terms join the FP64 sums; then the accumulator is free
-#pragma unroll
-            for (int g = 0; g < 2; ++g) {
-                uint32_t r[32];
-                tmem_ld32(tmem + lanes + (uint32_t)(NHB * BN + half * 64 + g * 32), r);
-#pragma unroll
-                for (int j = 0; j < 32; ++j) acc[g * 32 + j] += (double)__uint_as_float(r[j]);
-            }
-            tc_fence_before();
-            mbar_arrive(&xempty);
 #pragma unroll
             for (int g = 0; g < 2; ++g) {
                 const int n0 = nt * BN + half * 64 + g * 32;

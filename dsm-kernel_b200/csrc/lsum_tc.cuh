@@ -25,10 +25,12 @@ constexpr int PIECE_F16 = 0;     // fp16 pieces (11-bit significand each)
 constexpr int PIECE_BF16 = 1;    // bf16 pieces (8-bit significand each)
 constexpr uint32_t TC_REVERSE = 1;    // orders summed from high to low
 
-// One contraction of a launch.  Rows of A beyond M and columns beyond N are
-// read as zeros by the tensor-map bounds and never stored.
+// One contraction of a launch: rows row0 .. row0 + M of the A map against
+// the first N columns of the B map.  Rows beyond the map and columns beyond
+// N are read as zeros (or are other rows' data) and never stored.
 struct Problem {
     int amap, z, bmap, kblocks;  // A map (|m|), frequency slot, B map, orders / BK
+    int row0;                    // first row of A (in the map) and of C
     int M, N, tiles_n, tile0;    // shape, column tiles, index of the first tile
     float* C;                    // column-major M x N
     const float* sa;             // M row scales

@@ -951,10 +951,11 @@ __global__ void __launch_bounds__(128) k_psv_l0_solve(PsvDev d, const int* __res
 
 // (3) fields of order 0, one thread per (frequency, receiver): m = 0 slots
 // q = 0..2 (imt 1..3) and 3 (back), U and dU/dr (calup0 uses u(1) only)
-__device__ __forceinline__ void put_field(double* Aw, int Lcap, int R, int q, int r, int f, cd v) {
-    // rows ordered (slot, field, re/im, receiver): receivers contiguous, so
-    // the epilogue's threads (consecutive receivers) read consecutive rows
-    const size_t row = ((size_t)(q * NFLD + f) * 2) * (R + 1) + r;
+__device__ __forceinline__ void put_field(double* Aw, int Lcap, int nq, int R, int q, int r, int f, cd v) {
+    // rows ordered (field group, slot, field, re/im, receiver): receivers
+    // contiguous, so the epilogue's threads (consecutive receivers) read
+    // consecutive rows
+    const size_t row = psvk::fld_row(nq, R, q, f) + r;
     Aw[row * Lcap] = v.re;
     Aw[(row + (R + 1)) * Lcap] = v.im;
 }
@@ -985,14 +986,14 @@ __global__ void k_psv_l0_fields(PsvDev d, const cd* __restrict__ Dv, double* __r
                 U = D[4 * n0 + q];
             }
         }
-        put_field(A0w, Lcap, R, q, r, 0, U);
-        put_field(A0w, Lcap, R, q, r, 1, Ud);
-        for (int f = 2; f < NFLD; ++f) put_field(A0w, Lcap, R, q, r, f, mk(0.0));
+        put_field(A0w, Lcap, NS0, R, q, r, 0, U);
+        put_field(A0w, Lcap, NS0, R, q, r, 1, Ud);
+        for (int f = 2; f < NFLD; ++f) put_field(A0w, Lcap, NS0, R, q, r, f, mk(0.0));
     }
     for (int q = 0; q < NS1; ++q)
-        for (int f = 0; f < NFLD; ++f) put_field(A1w, Lcap, R, q, r, f, mk(0.0));
+        for (int f = 0; f < NFLD; ++f) put_field(A1w, Lcap, NS1, R, q, r, f, mk(0.0));
     for (int q = 0; q < NS2; ++q)
-        for (int f = 0; f < NFLD; ++f) put_field(A2w, Lcap, R, q, r, f, mk(0.0));
+        for (int f = 0; f < NFLD; ++f) put_field(A2w, Lcap, NS2, R, q, r, f, mk(0.0));
 }
 
 // ------------------------------------------------------- source terms
@@ -1361,11 +1362,12 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
             }
         }
         cd Vh = V / lsq, Vdh = Vd / lsq;
-        put_field(Aw[mi], Lcap, R, q, r, 0, U);
-        put_field(Aw[mi], Lcap, R, q, r, 1, Ud);
-        put_field(Aw[mi], Lcap, R, q, r, 2, Vh);
-        put_field(Aw[mi], Lcap, R, q, r, 3, Vdh);
-        put_field(Aw[mi], Lcap, R, q, r, 4, l2 * Vh);
+        const int nqm = mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2);
+        put_field(Aw[mi], Lcap, nqm, R, q, r, 0, U);
+        put_field(Aw[mi], Lcap, nqm, R, q, r, 1, Ud);
+        put_field(Aw[mi], Lcap, nqm, R, q, r, 2, Vh);
+        put_field(Aw[mi], Lcap, nqm, R, q, r, 3, Vdh);
+        put_field(Aw[mi], Lcap, nqm, R, q, r, 4, l2 * Vh);
     }
 }
 
@@ -1577,6 +1579,9 @@ class PsvEngine : public Engine {
         rows_m[0] = NS0 * (R + 1) * NFLD * 2;
         rows_m[1] = NS1 * (R + 1) * NFLD * 2;
         rows_m[2] = NS2 * (R + 1) * NFLD * 2;
+        rows_full[0] = (int)psvk::fld_rows_full(NS0, R);
+        rows_full[1] = (int)psvk::fld_rows_full(NS1, R);
+        rows_full[2] = (int)psvk::fld_rows_full(NS2, R);
         alloc_batch();
         build_basis(std::min(maxlmax + 1, 2048));
         DSM_CUDA(cudaStreamSynchronize(st));

@@ -67,10 +67,11 @@ template <class TC, class RL>
 struct Fields {
     const TC* C;
     size_t M;
-    int R, Th, it, r, q;
-    // complex entry of field f against basis column b
+    int nq, R, Th, it, r, q;
+    // complex entry of field f against basis column b (b = 1 only for the
+    // fields 0, 2, 3)
     __device__ __forceinline__ cx<RL> operator()(int f, int b) const {
-        const size_t row = ((size_t)(q * NFLD + f) * 2) * (R + 1) + r;
+        const size_t row = fld_row(nq, R, q, f) + r;
         const size_t col = (size_t)b * Th + it;
         return {(RL)C[row + M * col], (RL)C[row + (R + 1) + M * col]};
     }
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(EPI_THREADS) k_psv_epi(EpiDev d, int w, const 
         for (int q = 0; q < nq; ++q) {
             const Slot sl = slot_of(mi, q);
             if (sl.isback && !BACK) continue;
-            const Fields<TC, RL> G{Cm[mi], Mm[mi], R, Th, it, r, q};
+            const Fields<TC, RL> G{Cm[mi], Mm[mi], nq, R, Th, it, r, q};
             const RL sigma = (sl.m < 0 && (mi & 1)) ? RL(-1) : RL(1);
             const RL mm = (RL)sl.m, m2 = mm * mm;
             C d11 = {RL(0), RL(0)}, d12 = d11, d13 = d11, d21 = d11, d22 = d11, d23 = d11, d31 = d11,
@@ -253,7 +254,7 @@ __global__ void __launch_bounds__(EPI_THREADS) k_psv_epi_surf(EpiDev d, int w, c
         for (int q = 0; q < nq; ++q) {
             const Slot sl = slot_of(mi, q);
             if (sl.isback) continue;  // back slots have no surface term
-            const Fields<TC, RL> G{Cm[mi], Mm[mi], R, Th, it, R, q};
+            const Fields<TC, RL> G{Cm[mi], Mm[mi], nq, R, Th, it, R, q};
             const RL sigma = (sl.m < 0 && (mi & 1)) ? RL(-1) : RL(1);
             const C PU = G(0, 0);
             C u1, u2 = {RL(0), RL(0)}, u3 = {RL(0), RL(0)};

@@ -123,6 +123,7 @@ int run(int M, int N, int K, int nf, int fmt, int bk, uint32_t flags, int chunk,
         P.amap = 0;
         P.z = z;
         P.bmap = 0;
+        P.row0 = 0;
         P.kblocks = K / bk;
         P.M = M;
         P.N = N;
