@@ -16,7 +16,8 @@ namespace dsm {
 constexpr double kPi = 3.1415926535897932;
 
 // ------------------------------------------------------------ complex
-struct cd {
+// 16-byte aligned, so a complex moves with one 128-bit load or store
+struct __align__(16) cd {
     double re, im;
 };
 __host__ __device__ __forceinline__ cd mk(double r, double i = 0.0) { return cd{r, i}; }
@@ -46,7 +47,7 @@ __device__ __forceinline__ double cabs_(cd a) { return hypot(a.re, a.im); }
 // complex of a chosen real type (float on the mixed path, double on the
 // plain one); division by a real multiplies by its reciprocal
 template <class RL>
-struct cx {
+struct alignas(2 * sizeof(RL)) cx {
     RL re, im;
     __host__ __device__ __forceinline__ friend cx operator+(cx a, cx b) { return {a.re + b.re, a.im + b.im}; }
     __host__ __device__ __forceinline__ friend cx operator-(cx a, cx b) { return {a.re - b.re, a.im - b.im}; }

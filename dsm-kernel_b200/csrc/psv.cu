@@ -28,6 +28,7 @@
 //                ismall > 20 exit, SGTpsv-MPI.f90:606-609, 902-905).
 // The epilogue (TSGT / RSGT / SYNN from the l-contractions) is psv_epi.cu.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 
 #include "engine.cuh"
@@ -396,7 +397,14 @@ struct FactorCtx {
     double l2, lsq;
     int it, n, ls, lmin, nsys, sys;
     bool store;  // false for threads that only repeat another system
-    cd *Lst, *Dst;
+    cd* Lst;
+    cd* Zst;
+};
+
+// what a step hands to the forward substitution: the pivot D(k) and the
+// multipliers L(k+1,k), L(k+2,k), L(k+3,k)
+struct StepOut {
+    cd D, w0, w1, w2;
 };
 
 // Step k of dcsymbdl0 (half-width 3), P = k % 4.  The 4x4 window of the
@@ -407,10 +415,10 @@ struct FactorCtx {
 // steps' order otherwise).
 template <int P, bool FAST>
 __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], const cd (&anew)[4], SysTail& T,
-                                            const FactorCtx& c) {
+                                            const FactorCtx& c, StepOut& so) {
     constexpr int S0 = P, S1 = (P + 1) & 3, S2 = (P + 2) & 3, S3 = (P + 3) & 3;
     const cd D = M[S0][S0];
-    if (c.store && k >= c.ls) c.Dst[(size_t)(k - c.ls) * c.nsys + c.sys] = D;
+    so.D = D;
     if (k == c.n) return true;
     if (k == c.n - 1) T.Dm1 = D;
     const cd piv = crecipT<FAST>(D);
@@ -426,6 +434,9 @@ __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], const cd (&ane
         zv2 = -M[S3][S0];
         wv2 = cmulT<FAST>(M[S3][S0], piv);
     }
+    so.w0 = wv0;
+    so.w1 = wv1;
+    so.w2 = wv2;
     if (c.store && k >= c.lmin) {
         cd* L = c.Lst + (size_t)k * 3 * c.nsys + c.sys;
         L[0] = wv0;
@@ -463,15 +474,19 @@ __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], const cd (&ane
 // multipliers, the main update, a row entering): factor_step without the
 // end-of-band cases.
 template <int P, bool FAST>
-__device__ __forceinline__ void factor_step_main(int k, cd (&M)[4][4], const cd (&anew)[4], const FactorCtx& c) {
+__device__ __forceinline__ void factor_step_main(int k, cd (&M)[4][4], const cd (&anew)[4], const FactorCtx& c,
+                                                 StepOut& so) {
     constexpr int S0 = P, S1 = (P + 1) & 3, S2 = (P + 2) & 3, S3 = (P + 3) & 3;
     const cd D = M[S0][S0];
-    if (c.store && k >= c.ls) c.Dst[(size_t)(k - c.ls) * c.nsys + c.sys] = D;
     const cd piv = crecipT<FAST>(D);
     const cd zv0 = -M[S1][S0], zv1 = -M[S2][S0], zv2 = -M[S3][S0];
     const cd wv0 = cmulT<FAST>(M[S1][S0], piv);
     const cd wv1 = cmulT<FAST>(M[S2][S0], piv);
     const cd wv2 = cmulT<FAST>(M[S3][S0], piv);
+    so.D = D;
+    so.w0 = wv0;
+    so.w1 = wv1;
+    so.w2 = wv2;
     if (c.store && k >= c.lmin) {
         cd* L = c.Lst + (size_t)k * 3 * c.nsys + c.sys;
         L[0] = wv0;
@@ -490,18 +505,71 @@ __device__ __forceinline__ void factor_step_main(int k, cd (&M)[4][4], const cd 
     M[S0][S0] = anew[3];
 }
 
-// One thread per (omega, l) system: band assembly row by row and the
-// unpivoted complex-symmetric LDL^T (dcsymbdl0) streamed through the ring
-// window.  Multipliers of the rows the substitutions need go to Lst, pivots
-// of the rows at and above the source to Dst, the last ones to tail.
-// The row pieces stream through shared memory: a block (128 consecutive
-// systems: consecutive orders of at most a few frequencies) copies FAC_CH
-// rows of each of its frequencies with cp.async one chunk ahead, so the
-// factor recurrence waits on shared-memory latency only.  Systems of
-// frequencies beyond the first FAC_NW of a block read their rows from global
-// memory.  All threads of a block take the same steps (the same n), so the
-// block-wide barriers at chunk boundaries are uniform; threads past nsys
-// repeat the last system's work without storing it.
+// Forward substitution of the four source bases (dcsbdlv0, m = 3), run by
+// the factorisation itself: at step k it has D(k) and, from the three steps
+// before, L(k,k-3), L(k,k-2), L(k,k-1).  Below the first source row every
+// z is zero, so the rows start there.  zh = z / D goes to Zst.
+struct FwdState {
+    cd z[4][3];                          // z(k-3), z(k-2), z(k-1) per basis
+    cd w0_1, w1_1, w1_2, w2_1, w2_2, w2_3;  // w<p>_<d>: multiplier p of step k-d
+};
+template <bool FAST>
+__device__ __forceinline__ void fwd_row(int k, const StepOut& so, FwdState& F, const SysTail& T,
+                                        const FactorCtx& c) {
+    if (k >= c.ls) {
+        const cd l3 = F.w2_3, l2 = F.w1_2, l1 = F.w0_1;  // L(k,k-3), L(k,k-2), L(k,k-1)
+        cd rcp = mk(0.0);
+        if (FAST) rcp = crecipT<true>(so.D);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const cd rhs = mk(c.ls + b == k ? 1.0 : 0.0);
+            const cd z0 = F.z[b][0], z1 = F.z[b][1], z2 = F.z[b][2];
+            cd zc;
+            if (k == 1) {
+                zc = rhs;
+            } else if (k == 2) {
+                zc = rhs - T.a22raw * z2;
+            } else if (FAST) {
+                cd sum = cmulT<true>(l3, z0);
+                sum = caddmulT<true>(sum, l2, z1);
+                sum = caddmulT<true>(sum, l1, z2);
+                zc = rhs - sum;
+            } else if (k == 3) {  // a(2,3) z(1) + a(3,3) z(2)
+                cd sum = mk(0.0) + l2 * z1 + l1 * z2;
+                zc = rhs - sum;
+            } else {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
+                cd sum = mk(0.0) + l3 * z0 + l2 * z1 + l1 * z2;
+                zc = rhs - sum;
+            }
+            if (c.store) c.Zst[((size_t)(k - c.ls) * 4 + b) * c.nsys + c.sys] = FAST ? cmulT<true>(zc, rcp) : zc / so.D;
+            F.z[b][0] = z1;
+            F.z[b][1] = z2;
+            F.z[b][2] = zc;
+        }
+    }
+    F.w2_3 = F.w2_2;
+    F.w2_2 = F.w2_1;
+    F.w2_1 = so.w2;
+    F.w1_2 = F.w1_1;
+    F.w1_1 = so.w1;
+    F.w0_1 = so.w0;
+}
+
+// One thread per (omega, l) system: band assembly row by row, the unpivoted
+// complex-symmetric LDL^T (dcsymbdl0) streamed through the ring window and,
+// from the first source row up, the forward substitution of the source
+// bases.  Multipliers of the rows the upward substitution needs go to Lst,
+// zh of the source bases to Zst, the last pivots to tail.  The row pieces
+// stream through shared memory: a block (128 consecutive systems:
+// consecutive orders of at most a few frequencies) copies FAC_CH rows of
+// each of its frequencies with cp.async one chunk ahead, so the recurrence
+// waits on shared-memory latency only.  Systems of frequencies beyond the
+// first FAC_NW of a block read their rows from global memory.  All threads
+// of a block take the same steps (the same n), so the block-wide barriers at
+// chunk boundaries are uniform; threads past nsys repeat the last system's
+// work without storing it.  The steps below the source rows run without the
+// forward-substitution state, which keeps the registers of that (long) part
+// down.
 constexpr int FAC_THREADS = 128;
 constexpr int FAC_CH = 16;  // rows per chunk (multiple of 4)
 constexpr int FAC_NW = 4;   // frequencies staged per block
@@ -509,7 +577,7 @@ constexpr int FAC_NW = 4;   // frequencies staged per block
 template <bool FAST>
 __global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
                                                            int nsys, int lmin, cd* __restrict__ Lst,
-                                                           cd* __restrict__ Dst, SysTail* __restrict__ tail) {
+                                                           cd* __restrict__ Zst, SysTail* __restrict__ tail) {
     __shared__ __align__(16) cd sP[2][FAC_NW][FAC_CH][12];
     const int sys0 = blockIdx.x * FAC_THREADS;
     const int sysv = sys0 + threadIdx.x;
@@ -535,7 +603,7 @@ __global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* _
     c.sys = sys;
     c.store = valid;
     c.Lst = Lst;
-    c.Dst = Dst;
+    c.Zst = Zst;
     const int n = c.n;
     // local rows 5 .. n in chunks: chunk q = rows 5 + q CH .. (global it + r - 1)
     auto stage = [&](int q, int buf) {
@@ -585,67 +653,108 @@ __global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* _
         }
         assemble_row<FAST>(rp, c.l2, c.lsq, an);
     };
-    cd an[4];
-    for (int k = 1;; k += 4) {
-        if ((k - 1) % FAC_CH == 0) {  // chunk boundary: next chunk's copies go out
+    // chunk boundary at k (k - 1 a multiple of FAC_CH): the next chunk's copies go out
+    auto boundary = [&](int k) {
+        if ((k - 1) % FAC_CH == 0) {
             const int q = (k - 1) / FAC_CH;
             stage(q + 1, (q + 1) & 1);
             cp_async_commit();
             cp_async_wait<1>();
             __syncthreads();
         }
+    };
+    cd an[4];
+    StepOut so;
+    int k = 1;
+    // steps whose multipliers the forward substitution never reads: four
+    // main steps at a time, up to the group that reaches row ls - 4
+    const int kf = c.ls - 3;
+    for (; k + 3 < kf && k + 3 <= n - 4; k += 4) {
+        boundary(k);
+        entering(k, an);
+        factor_step_main<1, FAST>(k, M, an, c, so);
+        entering(k + 1, an);
+        factor_step_main<2, FAST>(k + 1, M, an, c, so);
+        entering(k + 2, an);
+        factor_step_main<3, FAST>(k + 2, M, an, c, so);
+        entering(k + 3, an);
+        factor_step_main<0, FAST>(k + 3, M, an, c, so);
+        if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+    }
+    // the rest, with the forward substitution
+    FwdState F;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) F.z[b][0] = F.z[b][1] = F.z[b][2] = mk(0.0);
+    F.w0_1 = F.w1_1 = F.w1_2 = F.w2_1 = F.w2_2 = F.w2_3 = mk(0.0);
+    for (;; k += 4) {
+        boundary(k);
         if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
             entering(k, an);
-            factor_step_main<1, FAST>(k, M, an, c);
+            factor_step_main<1, FAST>(k, M, an, c, so);
+            fwd_row<FAST>(k, so, F, T, c);
             entering(k + 1, an);
-            factor_step_main<2, FAST>(k + 1, M, an, c);
+            factor_step_main<2, FAST>(k + 1, M, an, c, so);
+            fwd_row<FAST>(k + 1, so, F, T, c);
             entering(k + 2, an);
-            factor_step_main<3, FAST>(k + 2, M, an, c);
+            factor_step_main<3, FAST>(k + 2, M, an, c, so);
+            fwd_row<FAST>(k + 2, so, F, T, c);
             entering(k + 3, an);
-            factor_step_main<0, FAST>(k + 3, M, an, c);
-            if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+            factor_step_main<0, FAST>(k + 3, M, an, c, so);
+            fwd_row<FAST>(k + 3, so, F, T, c);
+            if ((k + 3) % FAC_CH == 0) __syncthreads();
             continue;
         }
+        bool last;
         entering(k, an);
-        if (factor_step<1, FAST>(k, M, an, T, c)) { T.Dn = M[1][1]; break; }
+        last = factor_step<1, FAST>(k, M, an, T, c, so);
+        fwd_row<FAST>(k, so, F, T, c);
+        if (last) { T.Dn = M[1][1]; break; }
         entering(k + 1, an);
-        if (factor_step<2, FAST>(k + 1, M, an, T, c)) { T.Dn = M[2][2]; break; }
+        last = factor_step<2, FAST>(k + 1, M, an, T, c, so);
+        fwd_row<FAST>(k + 1, so, F, T, c);
+        if (last) { T.Dn = M[2][2]; break; }
         entering(k + 2, an);
-        if (factor_step<3, FAST>(k + 2, M, an, T, c)) { T.Dn = M[3][3]; break; }
+        last = factor_step<3, FAST>(k + 2, M, an, T, c, so);
+        fwd_row<FAST>(k + 2, so, F, T, c);
+        if (last) { T.Dn = M[3][3]; break; }
         entering(k + 3, an);
-        if (factor_step<0, FAST>(k + 3, M, an, T, c)) { T.Dn = M[0][0]; break; }
+        last = factor_step<0, FAST>(k + 3, M, an, T, c, so);
+        fwd_row<FAST>(k + 3, so, F, T, c);
+        if (last) { T.Dn = M[0][0]; break; }
         if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
     }
     cp_async_wait<0>();  // no copy outlives the block
     if (valid) tail[sys] = T;
 }
 
-// Substitutions of the six basis right-hand sides, one thread per (system,
-// basis), BACK_SYS systems per block.  Forward (dcsbdlv0, m = 3) from the
-// first source row, where the source bases' z start (everything below is
-// zero), to the top, keeping zh = z / D in Zst; then upward: x(n) = zh(n);
-// x(n-1) = zh(n-1) - L(n,n-1) x(n); x(j) = zh(j) - [L(j+3,j) x(j+3) +
-// L(j+2,j) x(j+2) + L(j+1,j) x(j+1)], down to the deepest captured row.  The
-// multipliers stream through shared memory: the block copies BACK_CH rows of
-// its systems' factors with cp.async one chunk ahead of use (coalesced 512 B
-// rows), together with the rows' capture slots, so the recurrence runs on
-// shared-memory latency; zh is loaded one row ahead.  Values at receiver
-// stencil rows go to Xcap.  Bases 4 and 5 are the surface unit vectors
-// e_{n-1}, e_n.  FAST (mixed precision) uses fused multiply-adds and one
-// reciprocal per pivot; otherwise the reference's operation order.
+// Upward substitution of the six basis right-hand sides, one thread per
+// (system, basis), BACK_SYS systems per block: x(n) = zh(n); x(n-1) =
+// zh(n-1) - L(n,n-1) x(n); x(j) = zh(j) - [L(j+3,j) x(j+3) + L(j+2,j)
+// x(j+2) + L(j+1,j) x(j+1)], down to the deepest captured row (dcsbdlv0,
+// m = 3; zh of the source bases comes from the factorisation's forward
+// pass, zero below the source).  The multipliers stream through shared
+// memory: the block copies BACK_CH rows of its systems' factors (coalesced
+// 512 B rows) with cp.async BACK_NBUF - 1 chunks ahead of use, together with
+// the rows' capture slots, so the recurrence runs on shared-memory latency;
+// zh is loaded one row ahead.  Values at receiver stencil rows go to Xcap.
+// Bases 4 and 5 are the surface unit vectors e_{n-1}, e_n.  FAST (mixed
+// precision) uses fused multiply-adds; otherwise the reference's operation
+// order.
 constexpr int BACK_SYS = 32;
 constexpr int BACK_THREADS = BACK_SYS * NB;  // 192
-constexpr int BACK_CH = 12;                  // rows per staged chunk (2 x 18 KB)
+constexpr int BACK_CH = 9;                   // rows per staged chunk (13.5 KB)
+constexpr int BACK_NBUF = 4;                 // staged chunks: three in flight ahead of use
+constexpr size_t BACK_SMEM = sizeof(cd) * BACK_NBUF * BACK_CH * 3 * BACK_SYS;  // dynamic
 static_assert(BACK_CH % 3 == 0, "the upward pass rotates three values per three rows");
 
 template <bool FAST>
-__global__ void __launch_bounds__(BACK_THREADS, 5) k_psv_back(PsvDev d, int nsys, int jmin_loc,
+__global__ void __launch_bounds__(BACK_THREADS, 4) k_psv_back(PsvDev d, int nsys, int jmin_loc,
                                                            const int* __restrict__ capmap,
-                                                           const cd* __restrict__ Lst, const cd* __restrict__ Dst,
-                                                           cd* __restrict__ Zst, const SysTail* __restrict__ tail,
-                                                           cd* __restrict__ Xcap) {
-    __shared__ __align__(16) cd sL[2][BACK_CH][3][BACK_SYS];
-    __shared__ int sC[2][BACK_CH];
+                                                           const cd* __restrict__ Lst, const cd* __restrict__ Zst,
+                                                           const SysTail* __restrict__ tail, cd* __restrict__ Xcap) {
+    extern __shared__ __align__(16) unsigned char back_smem[];
+    auto sL = reinterpret_cast<cd(*)[BACK_CH][3][BACK_SYS]>(back_smem);
+    __shared__ int sC[BACK_NBUF][BACK_CH];
     const int sys0 = blockIdx.x * BACK_SYS;
     const int sl = threadIdx.x / NB, b = threadIdx.x - sl * NB;
     const int sys = sys0 + sl;
@@ -655,46 +764,6 @@ __global__ void __launch_bounds__(BACK_THREADS, 5) k_psv_back(PsvDev d, int nsys
     const int ls = d.jsrc - it + 1;
     auto L = [&](int row, int p) { return Lst[((size_t)row * 3 + p) * nsys + sys]; };
     auto ZH = [&](int row) { return Zst[((size_t)(row - ls) * 4 + b) * nsys + sys]; };
-    if (valid && b < 4) {  // forward substitution of a source basis
-        const cd a22raw = tail[sys].a22raw;
-        cd z0 = mk(0.0), z1 = mk(0.0), z2 = mk(0.0);  // z(j-3), z(j-2), z(j-1)
-        const int j0 = max(ls, 1);
-        // operands of row j, loaded one row ahead: D(j), L(j-3,2), L(j-2,1), L(j-1,0)
-        auto fetch = [&](int j, cd& D, cd& l3, cd& l2, cd& l1) {
-            D = Dst[(size_t)(j - ls) * nsys + sys];
-            l3 = j >= 4 ? L(j - 3, 2) : mk(0.0);
-            l2 = j >= 3 ? L(j - 2, 1) : mk(0.0);
-            l1 = j >= 3 ? L(j - 1, 0) : mk(0.0);
-        };
-        cd Dn, l3n, l2n, l1n;
-        if (j0 <= n) fetch(j0, Dn, l3n, l2n, l1n);
-        for (int j = j0; j <= n; ++j) {
-            const cd D = Dn, l3 = l3n, l2 = l2n, l1 = l1n;
-            if (j < n) fetch(j + 1, Dn, l3n, l2n, l1n);
-            cd zc;
-            const cd rhs = mk(ls + b == j ? 1.0 : 0.0);
-            if (j == 1) {
-                zc = rhs;
-            } else if (j == 2) {
-                zc = rhs - a22raw * z2;
-            } else if (FAST) {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
-                cd sum = cmulT<true>(l3, z0);
-                sum = caddmulT<true>(sum, l2, z1);
-                sum = caddmulT<true>(sum, l1, z2);
-                zc = rhs - sum;
-            } else if (j == 3) {  // a(2,3) z(1) + a(3,3) z(2)
-                cd sum = mk(0.0) + l2 * z1 + l1 * z2;
-                zc = rhs - sum;
-            } else {
-                cd sum = mk(0.0) + l3 * z0 + l2 * z1 + l1 * z2;
-                zc = rhs - sum;
-            }
-            Zst[((size_t)(j - ls) * 4 + b) * nsys + sys] = FAST ? cmulT<true>(zc, crecipT<true>(D)) : zc / D;
-            z0 = z1;
-            z1 = z2;
-            z2 = zc;
-        }
-    }
     cd x0 = mk(0.0), x1 = mk(0.0), x2 = mk(0.0);  // x(j+1), x(j+2), x(j+3)
     if (valid) {
         auto capture = [&](int jloc, cd v) {
@@ -719,7 +788,7 @@ __global__ void __launch_bounds__(BACK_THREADS, 5) k_psv_back(PsvDev d, int nsys
             x0 = v;
         }
     }
-    // rows n-2 .. jmin_loc in chunks of BACK_CH, staged one chunk ahead
+    // rows n-2 .. jmin_loc in chunks of BACK_CH
     const int top = n - 2;
     const int nrows = top - jmin_loc + 1;
     if (nrows <= 0) return;
@@ -760,16 +829,20 @@ __global__ void __launch_bounds__(BACK_THREADS, 5) k_psv_back(PsvDev d, int nsys
         if (c >= 0) Xcap[((size_t)c * NB + b) * nsys + sys] = v;
         xc = v;
     };
-    stage(0, 0);
-    cp_async_commit();
-    for (int c = 0; c < nch; ++c) {
-        if (c + 1 < nch) stage(c + 1, (c + 1) & 1);
+#pragma unroll
+    for (int c = 0; c < BACK_NBUF - 1; ++c) {
+        if (c < nch) stage(c, c);
         cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
+    }
+    for (int c = 0; c < nch; ++c) {
+        cp_async_wait<BACK_NBUF - 2>();  // chunk c has landed (for this thread's copies)
+        __syncthreads();                 // ... for every thread, and chunk c - 1's buffer is free
+        const int cn = c + BACK_NBUF - 1;
+        if (cn < nch) stage(cn, cn % BACK_NBUF);
+        cp_async_commit();
         if (valid) {
             const int hi = top - c * BACK_CH, cnt = min(BACK_CH, hi - jmin_loc + 1);
-            const int buf = c & 1;
+            const int buf = c % BACK_NBUF;
             // rotating roles: (x0, x1, x2) = (x(j+1), x(j+2), x(j+3)) at i % 3 == 0
             int i = 0;
             for (; i + 3 <= cnt; i += 3) {
@@ -782,8 +855,8 @@ __global__ void __launch_bounds__(BACK_THREADS, 5) k_psv_back(PsvDev d, int nsys
             if (i < cnt) row(buf, i, hi - i, x0, x1, x2);
             if (i + 1 < cnt) row(buf, i + 1, hi - i - 1, x2, x0, x1);
         }
-        __syncthreads();  // the buffer is refilled two chunks later
     }
+    cp_async_wait<0>();  // no copy outlives the block
 }
 
 // ------------------------------------------------------------ l = 0 path
@@ -1410,7 +1483,7 @@ class PsvEngine : public Engine {
     DBuf<int> iphase, nlayer, kkdr, elem, hmoff, blkoff, amz, amc, bcrow, rcap, fluid, comp_src, jsta,
         capmap, l0col, l0e1;
     DBuf<double> qmu, qkappa, sel, fel, hm, bcval, poly, lam, qkp, fr, r, rrsta;
-    DBuf<cd> B0, B1, B2, Prow, Lst, Zst, Dst, Xcap, l0scr, l0d, ab, co;
+    DBuf<cd> B0, B1, B2, Prow, Lst, Zst, Xcap, l0scr, l0d, ab, co;
     DBuf<int4> rowasm;
     DBuf<SysTail> tails;
     int jmin_loc = 1, ncap = 0;
@@ -1420,6 +1493,9 @@ class PsvEngine : public Engine {
         mode = 1;
         opt = *o;
         init_common(opt.device);
+        // the substitution's staged multipliers exceed the default 48 KB
+        DSM_CUDA(cudaFuncSetAttribute(k_psv_back<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BACK_SMEM));
+        DSM_CUDA(cudaFuncSetAttribute(k_psv_back<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BACK_SMEM));
         m_lo = 0;
         R = s->r_n;
         Th = s->theta_n;
@@ -1601,7 +1677,6 @@ class PsvEngine : public Engine {
         Prow.reserve((size_t)F * (d.nn + 1) * 12);
         Lst.reserve((n + 1) * 3 * nsys);
         Zst.reserve((n - ls + 2) * 4 * nsys);
-        Dst.reserve((n - ls + 2) * nsys);
         Xcap.reserve((size_t)ncap * NB * nsys);
         tails.reserve(nsys);
         l0scr.reserve((size_t)F * (d.nn0 + 1) * 2);
@@ -1658,28 +1733,35 @@ class PsvEngine : public Engine {
             DSM_LAUNCH(*this);
             l0_done = true;
         }
-        // algorithmic bytes of a system: band factor (b+1) N complex written
-        // and read once, plus value and derivative of every solved right-hand
-        // side at the receivers
-        const double nrow = (double)(d.nn - d.itmp + 1);
-        const double alg = 2.0 * 4.0 * nrow * 16.0 + 18.0 * R * 2 * 2 * 16.0;
-        int id = kid("psv_band_solve");
+        // algorithmic bytes per system: the factorisation writes the three
+        // multipliers of every row the upward substitution reads (rows lmin
+        // .. n) and zh of the four source bases above the source; the
+        // substitution reads both back and stores six solutions at the
+        // captured rows
+        const int n = d.nn - d.itmp + 1, ls = d.jsrc - d.itmp + 1;
+        const int lmin = std::max(1, std::min(jmin_loc, ls - 3));
+        const double fac_bytes = (double)(n - lmin + 1) * 3 * 16.0 + (double)(n - ls + 1) * 4 * 16.0;
+        const double sub_bytes = (double)(n - jmin_loc + 1) * 3 * 16.0 + (double)(n - ls + 1) * 4 * 16.0 +
+                                 (double)ncap * NB * 16.0;
+        int id = kid("psv_factor");
         kbegin(id);
-        const int lmin = std::max(1, std::min(jmin_loc, d.jsrc - d.itmp + 1 - 3));
         if (mixed())
-            k_psv_solve<true><<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Dst.p,
+            k_psv_solve<true><<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
                                                                   tails.p);
         else
-            k_psv_solve<false><<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Dst.p,
+            k_psv_solve<false><<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
                                                                    tails.p);
+        kend(id, fac_bytes * nsys, 0.0);
         DSM_LAUNCH(*this);
+        id = kid("psv_substitution");
+        kbegin(id);
         if (mixed())
-            k_psv_back<true><<<(nsys + BACK_SYS - 1) / BACK_SYS, BACK_THREADS, 0, st>>>(
-                d, nsys, jmin_loc, capmap.p, Lst.p, Dst.p, Zst.p, tails.p, Xcap.p);
+            k_psv_back<true><<<(nsys + BACK_SYS - 1) / BACK_SYS, BACK_THREADS, BACK_SMEM, st>>>(
+                d, nsys, jmin_loc, capmap.p, Lst.p, Zst.p, tails.p, Xcap.p);
         else
-            k_psv_back<false><<<(nsys + BACK_SYS - 1) / BACK_SYS, BACK_THREADS, 0, st>>>(
-                d, nsys, jmin_loc, capmap.p, Lst.p, Dst.p, Zst.p, tails.p, Xcap.p);
-        kend(id, alg * nsys, 0.0);
+            k_psv_back<false><<<(nsys + BACK_SYS - 1) / BACK_SYS, BACK_THREADS, BACK_SMEM, st>>>(
+                d, nsys, jmin_loc, capmap.p, Lst.p, Zst.p, tails.p, Xcap.p);
+        kend(id, sub_bytes * nsys, 0.0);
         DSM_LAUNCH(*this);
         id = kid("psv_source_coef");
         kbegin(id);
@@ -1693,7 +1775,7 @@ class PsvEngine : public Engine {
                                            Lcap, amps.p);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
-        stats.solve_bytes += (double)nsys * (d.nn - d.itmp + 1) * 3 * 16.0 * 2;
+        stats.solve_bytes += (fac_bytes + sub_bytes) * nsys;
     }
 
     void scan_chunk(int nf, const WorkList& wl) override {
