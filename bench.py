@@ -417,7 +417,9 @@ def main():
         if plain:
             line["fp64"] = {"value": plain["value"], "ms_per_step": 1e3 * plain["t"] / args.steps,
                             "e2e": plain["e2e"]["value"], "systems": plain["systems"],
-                            "orders_padded": plain["padded"], "clocks": plain["clocks"]}
+                            "orders_padded": plain["padded"], "clocks": plain["clocks"],
+                            "kernel_share": {k: round(v[0] / max(plain["t"] * 1e3, 1e-9), 4)
+                                             for k, v in plain["kstats"].items()}}
             line["speedup_vs_fp64"] = run["value"] / plain["value"]
             line["speedup_vs_fp64_e2e"] = run["e2e"]["value"] / plain["e2e"]["value"]
         if rel:

@@ -169,13 +169,14 @@ void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
     for (int m = m_lo; m <= 2; ++m)
         for (int w = 0; w < nf; ++w) {
             const double kp = (double)((nord[w] + tc_bk - 1) / tc_bk * tc_bk);
-            split_bytes += (double)rows_m[m] * (8.0 * nord[w] + 4.0 * kp);
+            split_bytes += (double)rows_m[m] * ((double)afld_bytes * nord[w] + 4.0 * kp);
         }
     int id = kid("lsum_split");
     kbegin(id);
     for (int m = m_lo; m <= 2; ++m) {
         if (!rows_m[m]) continue;
-        tc::split_fields(Afld[m].p, nf, rows_m[m], Lcap, d_nord.p, Apc[m].p, sA[m].p, kcA, F, tc_fmt, tc_bk, st);
+        tc::split_fields(Afld[m].p, afld_bytes, nf, rows_m[m], Lcap, d_nord.p, Apc[m].p, sA[m].p, kcA, F, tc_fmt,
+                         tc_bk, st);
         launches++;
     }
     kend(id, split_bytes, 0.0);
@@ -255,6 +256,7 @@ void Engine::build_weights(const double* d_r, const double* d_rrsta) {
 void Engine::gemm_fp64(int w, int mi, int K) {
     const int M = rows_m[mi], rf = full_rows(mi);
     if (M == 0) return;
+    if (afld_bytes != 8) throw Error(DSM_ERR_INVALID, "FP64 l-sum of FP32 field matrices");
     const double one = 1.0, zero = 0.0;
     const double* A = Afld[mi].p + (size_t)w * M * Lcap;
     int id = kid("lsum_dgemm");
@@ -285,15 +287,16 @@ void Engine::grow_orders(int need) {
     for (int m = m_lo; m <= 2; ++m) {
         size_t h = (size_t)F * rows_m[m];
         if (h == 0) continue;
+        const size_t eb = (size_t)afld_bytes, bytes = (h * cap * eb + 7) / 8 * 8;
         double* np_ = nullptr;
-        if (cudaMalloc(&np_, h * cap * sizeof(double)) != cudaSuccess)
+        if (cudaMalloc(&np_, bytes) != cudaSuccess)
             throw Error(DSM_ERR_NOMEM, "cannot grow the field matrices to " + std::to_string(cap) + " orders");
-        DSM_CUDA(cudaMemcpy2DAsync(np_, (size_t)cap * sizeof(double), Afld[m].p, (size_t)Lcap * sizeof(double),
-                                   (size_t)Lcap * sizeof(double), h, cudaMemcpyDeviceToDevice, st));
+        DSM_CUDA(cudaMemcpy2DAsync(np_, (size_t)cap * eb, Afld[m].p, (size_t)Lcap * eb, (size_t)Lcap * eb, h,
+                                   cudaMemcpyDeviceToDevice, st));
         DSM_CUDA(cudaStreamSynchronize(st));
         Afld[m].release();
         Afld[m].p = np_;
-        Afld[m].n = h * cap;
+        Afld[m].n = bytes / 8;
     }
     double* na = nullptr;
     if (cudaMalloc(&na, (size_t)F * cap * amp_k * sizeof(double)) != cudaSuccess)

@@ -79,6 +79,7 @@ class Engine {
     int F = 0, Lc = 0, Lcap = 0;     // frequencies per batch, l chunk, A capacity
     int amp_k = 1;                   // cutoff probes stored per order
     DBuf<double> Afld[3];            // field matrices per |m| [F][rows][Lcap]
+    int afld_bytes = 8;              // their element: FP64, or FP32 where the mode's mixed path stores them so
     DBuf<double> Cgemm;              // GEMM output of one (omega, |m|)
     DBuf<CutState> cut;              // [F]
     DBuf<double> amps;               // [F][Lcap][5]

@@ -404,7 +404,8 @@ __device__ __forceinline__ void split2(double x, int fmt, uint16_t& hi, uint16_t
 }
 
 // one warp per row: row maximum over the counted orders, then the pieces
-__global__ void k_split_rows(const double* __restrict__ A, int nrows, int per_w, int lcap,
+template <class TIN>
+__global__ void k_split_rows(const TIN* __restrict__ A, int nrows, int per_w, int lcap,
                              const int* __restrict__ nord, int kcap, int bk, uint16_t* __restrict__ P,
                              size_t piece_stride, float* __restrict__ sa, int fmt) {
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -412,9 +413,9 @@ __global__ void k_split_rows(const double* __restrict__ A, int nrows, int per_w,
     if (row >= nrows) return;
     const int K = nord ? min(nord[row / per_w], lcap) : lcap;
     const int Kp = min(kcap, (K + bk - 1) / bk * bk);
-    const double* a = A + (size_t)row * lcap;
+    const TIN* a = A + (size_t)row * lcap;
     double mx = 0.0;
-    for (int l = lane; l < K; l += 32) mx = fmax(mx, fabs(a[l]));
+    for (int l = lane; l < K; l += 32) mx = fmax(mx, fabs((double)a[l]));
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     const int e = piece_exp(mx);
     if (lane == 0) sa[row] = __int_as_float((127 + e) << 23);
@@ -422,7 +423,7 @@ __global__ void k_split_rows(const double* __restrict__ A, int nrows, int per_w,
     uint16_t* pl = ph + piece_stride;
     for (int l = lane; l < Kp; l += 32) {
         uint16_t h = 0, lo = 0;
-        if (l < K) split2(scalbn(a[l], -e), fmt, h, lo);
+        if (l < K) split2(scalbn((double)a[l], -e), fmt, h, lo);
         ph[l] = h;
         pl[l] = lo;
     }
@@ -479,20 +480,24 @@ void encode_b(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int col
           "the split bases");
 }
 
-void split_fields(const double* A, int nf, int rows, int lcap, const int* d_nord, uint16_t* P, float* sa,
-                  int kcap, int F, int piece_fmt, int bk, cudaStream_t st) {
+void split_fields(const void* A, int in_bytes, int nf, int rows, int lcap, const int* d_nord, uint16_t* P,
+                  float* sa, int kcap, int F, int piece_fmt, int bk, cudaStream_t st) {
     const int n = nf * rows;
     if (n <= 0) return;
     if (kcap % bk) throw Error(DSM_ERR_INVALID, "order capacity of the split fields is not a multiple of BK");
-    k_split_rows<<<(n + 7) / 8, 256, 0, st>>>(A, n, rows, lcap, d_nord, kcap, bk, P, (size_t)F * rows * kcap, sa,
-                                              piece_fmt);
+    if (in_bytes == 4)
+        k_split_rows<float><<<(n + 7) / 8, 256, 0, st>>>(static_cast<const float*>(A), n, rows, lcap, d_nord, kcap,
+                                                         bk, P, (size_t)F * rows * kcap, sa, piece_fmt);
+    else
+        k_split_rows<double><<<(n + 7) / 8, 256, 0, st>>>(static_cast<const double*>(A), n, rows, lcap, d_nord,
+                                                          kcap, bk, P, (size_t)F * rows * kcap, sa, piece_fmt);
     DSM_CUDA(cudaGetLastError());
 }
 
 void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, int kcap, int piece_fmt,
                  cudaStream_t st) {
     if (cols <= 0) return;
-    k_split_rows<<<(cols + 7) / 8, 256, 0, st>>>(B, cols, cols, lcap, nullptr, kcap, kcap, P,
+    k_split_rows<double><<<(cols + 7) / 8, 256, 0, st>>>(B, cols, cols, lcap, nullptr, kcap, kcap, P,
                                                  (size_t)cols * kcap, sb, piece_fmt);
     DSM_CUDA(cudaGetLastError());
 }

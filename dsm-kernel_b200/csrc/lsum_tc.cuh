@@ -48,13 +48,13 @@ struct Maps {
 void encode_a(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int rows, int nfreq, int bk);
 void encode_b(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int cols, int bk);
 
-// Splits the FP64 field matrices of a batch, A[F][rows][lcap] (orders
-// contiguous), into pieces P[2][F][rows][kcap] with one power-of-two scale
-// per row (sa[F][rows]); orders at or beyond the frequency's count
-// nord[w] become zeros up to the next multiple of bk (the contraction reads
-// whole BK blocks).
-void split_fields(const double* A, int nf, int rows, int lcap, const int* d_nord, uint16_t* P, float* sa,
-                  int kcap, int F, int piece_fmt, int bk, cudaStream_t st);
+// Splits the field matrices of a batch, A[F][rows][lcap] (orders
+// contiguous; FP64 or FP32 elements, in_bytes 8 or 4), into pieces
+// P[2][F][rows][kcap] with one power-of-two scale per row (sa[F][rows]);
+// orders at or beyond the frequency's count nord[w] become zeros up to the
+// next multiple of bk (the contraction reads whole BK blocks).
+void split_fields(const void* A, int in_bytes, int nf, int rows, int lcap, const int* d_nord, uint16_t* P,
+                  float* sa, int kcap, int F, int piece_fmt, int bk, cudaStream_t st);
 // Splits the basis table B[cols][lcap] into P[2][cols][kcap] with one scale
 // per column (sb[cols]); orders >= lcap become zeros.
 void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, int kcap, int piece_fmt,

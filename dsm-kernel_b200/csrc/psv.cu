@@ -13,8 +13,10 @@
 //                steps) and the substitutions (dcsbdlv0, :93-166;
 //                mydcsbdlv3 is the same arithmetic) of six basis
 //                right-hand sides: the four source rows jtmp..jtmp+3 and the
-//                surface rows nn-1, nn.  Factors stay in HBM between the
-//                downward and upward sweeps.
+//                surface rows nn-1, nn.  The forward substitution of the
+//                source bases runs inside the factorisation; the multipliers
+//                stay in HBM for the upward sweep (k_psv_up, one lane per
+//                system and six bases).
 //   k_psv_l0     l = 0: the tridiagonal compaction (rea2 / rea2_back,
 //                calmat.f90:1247-1389) and its solves (dcsymbdl0/dcsbdlv0
 //                with half-width 1), one thread per frequency.
@@ -30,6 +32,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cmath>
+#include <type_traits>
 
 #include "engine.cuh"
 #include "psv_epi.cuh"
@@ -367,6 +370,22 @@ __device__ __forceinline__ double rcp_newton(double x) {
     y = fma(y, fma(-x, y, 1.0), y);
     return y;
 }
+// 1/x with one Newton-Raphson step (about 2^-40 relative): enough for the
+// mixed path, whose tolerance is far above it
+__device__ __forceinline__ double rcp_newton1(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    return fma(y, fma(-x, y, 1.0), y);
+}
+// the band multipliers w = m / D of a step.  FAST: w = (m conj(D)) / |D|^2,
+// whose products with conj(D) run beside the reciprocal, so only one
+// multiply follows it on the pivot chain; otherwise 1/D (Smith) times m, the
+// reference's operations.
+template <bool FAST>
+__device__ __forceinline__ cd mult_of(cd m, cd D, double r, cd piv) {
+    if (FAST) return mk(fma(m.re, D.re, m.im * D.im) * r, fma(m.im, D.re, -(m.re * D.im)) * r);
+    return m * piv;
+}
 template <bool FAST>
 __device__ __forceinline__ cd crecipT(cd D) {
     if (FAST) {
@@ -421,18 +440,19 @@ __device__ __forceinline__ bool factor_step(int k, cd (&M)[4][4], const cd (&ane
     so.D = D;
     if (k == c.n) return true;
     if (k == c.n - 1) T.Dm1 = D;
-    const cd piv = crecipT<FAST>(D);
+    const double r = FAST ? rcp_newton1(fma(D.re, D.re, D.im * D.im)) : 0.0;
+    const cd piv = FAST ? mk(0.0) : crecipT<false>(D);
     const int nw = min(3, c.n - k);
     cd wv0, wv1 = mk(0.0), wv2 = mk(0.0), zv0, zv1 = mk(0.0), zv2 = mk(0.0);
     zv0 = -M[S1][S0];
-    wv0 = cmulT<FAST>(M[S1][S0], piv);
+    wv0 = mult_of<FAST>(M[S1][S0], D, r, piv);
     if (nw >= 2) {
         zv1 = -M[S2][S0];
-        wv1 = cmulT<FAST>(M[S2][S0], piv);
+        wv1 = mult_of<FAST>(M[S2][S0], D, r, piv);
     }
     if (nw >= 3) {
         zv2 = -M[S3][S0];
-        wv2 = cmulT<FAST>(M[S3][S0], piv);
+        wv2 = mult_of<FAST>(M[S3][S0], D, r, piv);
     }
     so.w0 = wv0;
     so.w1 = wv1;
@@ -478,11 +498,12 @@ __device__ __forceinline__ void factor_step_main(int k, cd (&M)[4][4], const cd 
                                                  StepOut& so) {
     constexpr int S0 = P, S1 = (P + 1) & 3, S2 = (P + 2) & 3, S3 = (P + 3) & 3;
     const cd D = M[S0][S0];
-    const cd piv = crecipT<FAST>(D);
+    const double r = FAST ? rcp_newton1(fma(D.re, D.re, D.im * D.im)) : 0.0;
+    const cd piv = FAST ? mk(0.0) : crecipT<false>(D);
     const cd zv0 = -M[S1][S0], zv1 = -M[S2][S0], zv2 = -M[S3][S0];
-    const cd wv0 = cmulT<FAST>(M[S1][S0], piv);
-    const cd wv1 = cmulT<FAST>(M[S2][S0], piv);
-    const cd wv2 = cmulT<FAST>(M[S3][S0], piv);
+    const cd wv0 = mult_of<FAST>(M[S1][S0], D, r, piv);
+    const cd wv1 = mult_of<FAST>(M[S2][S0], D, r, piv);
+    const cd wv2 = mult_of<FAST>(M[S3][S0], D, r, piv);
     so.D = D;
     so.w0 = wv0;
     so.w1 = wv1;
@@ -727,136 +748,171 @@ __global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* _
     if (valid) tail[sys] = T;
 }
 
-// Upward substitution of the six basis right-hand sides, one thread per
-// (system, basis), BACK_SYS systems per block: x(n) = zh(n); x(n-1) =
-// zh(n-1) - L(n,n-1) x(n); x(j) = zh(j) - [L(j+3,j) x(j+3) + L(j+2,j)
-// x(j+2) + L(j+1,j) x(j+1)], down to the deepest captured row (dcsbdlv0,
-// m = 3; zh of the source bases comes from the factorisation's forward
-// pass, zero below the source).  The multipliers stream through shared
-// memory: the block copies BACK_CH rows of its systems' factors (coalesced
-// 512 B rows) with cp.async BACK_NBUF - 1 chunks ahead of use, together with
-// the rows' capture slots, so the recurrence runs on shared-memory latency;
-// zh is loaded one row ahead.  Values at receiver stencil rows go to Xcap.
-// Bases 4 and 5 are the surface unit vectors e_{n-1}, e_n.  FAST (mixed
-// precision) uses fused multiply-adds; otherwise the reference's operation
-// order.
-constexpr int BACK_SYS = 32;
-constexpr int BACK_THREADS = BACK_SYS * NB;  // 192
-constexpr int BACK_CH = 9;                   // rows per staged chunk (13.5 KB)
-constexpr int BACK_NBUF = 4;                 // staged chunks: three in flight ahead of use
-constexpr size_t BACK_SMEM = sizeof(cd) * BACK_NBUF * BACK_CH * 3 * BACK_SYS;  // dynamic
-static_assert(BACK_CH % 3 == 0, "the upward pass rotates three values per three rows");
+// Upward substitution of the six basis right-hand sides (dcsbdlv0, m = 3):
+// x(n) = zh(n); x(n-1) = zh(n-1) - L(n,n-1) x(n); x(j) = zh(j) - [L(j+3,j)
+// x(j+3) + L(j+2,j) x(j+2) + L(j+1,j) x(j+1)], down to the deepest captured
+// row; zh of the source bases comes from the factorisation's forward pass
+// (zero below the source), bases 4 and 5 are the surface unit vectors
+// e_{n-1}, e_n, and the values at receiver stencil rows go to Xcap.  One
+// lane per system with all six bases in the lane: six independent
+// recurrences, each multiplier read once.  FAST (mixed precision) uses fused
+// multiply-adds; otherwise the reference's operation order.  Each lane stages its own
+// multipliers (and, above the source, its zh) with cp.async into a private
+// ring of UP_NBUF chunks in shared memory, UP_NBUF - 1 chunks ahead of use,
+// and waits only for its own copies, so no barrier couples the lanes.  The
+// captured rows come from a list in descending row order ({row, slot},
+// ended by row -1).
+constexpr int UP_WARPS = 4;
+constexpr int UP_THREADS = 32 * UP_WARPS;
+constexpr int UP_NBUF = 4;
+constexpr int UP_CH1 = 2, UP_E1 = 7;  // at and above the source: rows per chunk, entries (3 L + 4 zh)
+constexpr int UP_CH2 = 4, UP_E2 = 3;  // below it: rows per chunk, entries (3 L)
+constexpr int UP_ROW_CD = 14;         // complex per lane and chunk, the larger of CH1 E1 and CH2 E2
+constexpr int UP_WARP_CD = UP_NBUF * UP_ROW_CD * 32;
+constexpr size_t UP_SMEM = sizeof(cd) * UP_WARP_CD * UP_WARPS;
+static_assert(UP_CH1 * UP_E1 <= UP_ROW_CD && UP_CH2 * UP_E2 <= UP_ROW_CD, "ring too small");
 
 template <bool FAST>
-__global__ void __launch_bounds__(BACK_THREADS, 4) k_psv_back(PsvDev d, int nsys, int jmin_loc,
-                                                           const int* __restrict__ capmap,
-                                                           const cd* __restrict__ Lst, const cd* __restrict__ Zst,
-                                                           const SysTail* __restrict__ tail, cd* __restrict__ Xcap) {
-    extern __shared__ __align__(16) unsigned char back_smem[];
-    auto sL = reinterpret_cast<cd(*)[BACK_CH][3][BACK_SYS]>(back_smem);
-    __shared__ int sC[BACK_NBUF][BACK_CH];
-    const int sys0 = blockIdx.x * BACK_SYS;
-    const int sl = threadIdx.x / NB, b = threadIdx.x - sl * NB;
-    const int sys = sys0 + sl;
-    const bool valid = sys < nsys;
-    const int nsb = min(BACK_SYS, nsys - sys0);  // systems of this block
-    const int it = d.itmp, n = d.nn - it + 1;
-    const int ls = d.jsrc - it + 1;
-    auto L = [&](int row, int p) { return Lst[((size_t)row * 3 + p) * nsys + sys]; };
-    auto ZH = [&](int row) { return Zst[((size_t)(row - ls) * 4 + b) * nsys + sys]; };
-    cd x0 = mk(0.0), x1 = mk(0.0), x2 = mk(0.0);  // x(j+1), x(j+2), x(j+3)
-    if (valid) {
-        auto capture = [&](int jloc, cd v) {
-            const int c = capmap[jloc + it - 1];
-            if (c >= 0) Xcap[((size_t)c * NB + b) * nsys + sys] = v;
-        };
+__global__ void __launch_bounds__(UP_THREADS, 2) k_psv_up(PsvDev d, int nsys, int jmin_loc,
+                                                          const int* __restrict__ capmap,
+                                                          const int2* __restrict__ caplist,
+                                                          const cd* __restrict__ Lst, const cd* __restrict__ Zst,
+                                                          const SysTail* __restrict__ tail, cd* __restrict__ Xcap) {
+    extern __shared__ __align__(16) unsigned char up_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sys = (blockIdx.x * UP_WARPS + warp) * 32 + lane;
+    if (sys >= nsys) return;  // nothing below synchronises across lanes
+    cd* ring = reinterpret_cast<cd*>(up_smem) + (size_t)warp * UP_WARP_CD + lane;
+    const int it = d.itmp, n = d.nn - it + 1, ls = d.jsrc - it + 1;
+    auto store = [&](int c, int b, cd v) { Xcap[((size_t)c * NB + b) * nsys + sys] = v; };
+    cd x[NB][3];  // x(j+1), x(j+2), x(j+3) of each basis
+    {
         const SysTail tl = tail[sys];
-        cd xn;
-        if (b < 4) xn = (n >= ls) ? ZH(n) : mk(0.0);
-        // surface basis: e_{n-1}: z(n-1) = 1, z(n) = -L(n,n-1); e_n: z(n) = 1
-        else if (b == 4) xn = (mk(0.0) - tl.Lnn1 * mk(1.0)) / tl.Dn;
-        else xn = mk(1.0) / tl.Dn;
-        capture(n, xn);
-        x0 = xn;
-        if (n - 1 >= jmin_loc) {
-            cd zh = mk(0.0);
-            if (b < 4 && n - 1 >= ls) zh = ZH(n - 1);
-            if (b == 4) zh = mk(1.0) / tl.Dm1;
-            const cd v = zh - L(n - 1, 0) * x0;
-            capture(n - 1, v);
-            x1 = x0;
-            x0 = v;
-        }
-    }
-    // rows n-2 .. jmin_loc in chunks of BACK_CH
-    const int top = n - 2;
-    const int nrows = top - jmin_loc + 1;
-    if (nrows <= 0) return;
-    const int nch = (nrows + BACK_CH - 1) / BACK_CH;
-    auto stage = [&](int c, int buf) {
-        const int hi = top - c * BACK_CH, cnt = min(BACK_CH, hi - jmin_loc + 1);
-        // cnt rows x 3 multipliers x nsb systems, 16 B each
-        for (int e = threadIdx.x; e < cnt * 3 * nsb; e += BACK_THREADS) {
-            const int sidx = e % nsb, rp = e / nsb, i = rp / 3, p = rp - 3 * i;
-            cp_async16(&sL[buf][i][p][sidx], &Lst[((size_t)(hi - i) * 3 + p) * nsys + sys0 + sidx]);
-        }
-        if (threadIdx.x < cnt) sC[buf][threadIdx.x] = capmap[hi - threadIdx.x + it - 1];
-    };
-    // zh of a source basis at local row j (zero below the source rows)
-    const bool src = valid && b < 4;
-    auto zh_at = [&](int j) { return (src && j >= ls && j >= jmin_loc) ? ZH(j) : mk(0.0); };
-    cd zhn = zh_at(top);
-    // one upward row: x(j) from x(j+1) = xa, x(j+2) = xb, x(j+3) = xc; the
-    // result replaces xc (the oldest).  x(n+1) = 0 makes row n-2 the general form.
-    auto row = [&](int buf, int i, int j1, const cd& xa, const cd& xb, cd& xc) {
-        const cd L1 = sL[buf][i][0][sl], L2 = sL[buf][i][1][sl], L3 = sL[buf][i][2][sl];
-        const cd zh = zhn;
-        zhn = zh_at(j1 - 1);
-        cd v;
-        if (FAST) {
-            cd sum = cmulT<true>(L3, xc);
-            sum = caddmulT<true>(sum, L2, xb);
-            sum = caddmulT<true>(sum, L1, xa);
-            v = zh - sum;
-        } else if (j1 == n - 2) {
-            cd sum = mk(0.0) + L2 * xb + L1 * xa;
-            v = zh - sum;
-        } else {
-            cd sum = mk(0.0) + L3 * xc + L2 * xb + L1 * xa;
-            v = zh - sum;
-        }
-        const int c = sC[buf][i];
-        if (c >= 0) Xcap[((size_t)c * NB + b) * nsys + sys] = v;
-        xc = v;
-    };
+        const int cn = capmap[n + it - 1], cn1 = n - 1 >= jmin_loc ? capmap[n - 1 + it - 1] : -1;
+        const cd Ln = n - 1 >= jmin_loc ? Lst[((size_t)(n - 1) * 3) * nsys + sys] : mk(0.0);
 #pragma unroll
-    for (int c = 0; c < BACK_NBUF - 1; ++c) {
-        if (c < nch) stage(c, c);
-        cp_async_commit();
-    }
-    for (int c = 0; c < nch; ++c) {
-        cp_async_wait<BACK_NBUF - 2>();  // chunk c has landed (for this thread's copies)
-        __syncthreads();                 // ... for every thread, and chunk c - 1's buffer is free
-        const int cn = c + BACK_NBUF - 1;
-        if (cn < nch) stage(cn, cn % BACK_NBUF);
-        cp_async_commit();
-        if (valid) {
-            const int hi = top - c * BACK_CH, cnt = min(BACK_CH, hi - jmin_loc + 1);
-            const int buf = c % BACK_NBUF;
-            // rotating roles: (x0, x1, x2) = (x(j+1), x(j+2), x(j+3)) at i % 3 == 0
-            int i = 0;
-            for (; i + 3 <= cnt; i += 3) {
-                row(buf, i, hi - i, x0, x1, x2);          // x2 <- x(j)
-                row(buf, i + 1, hi - i - 1, x2, x0, x1);  // x1 <- x(j-1)
-                row(buf, i + 2, hi - i - 2, x1, x2, x0);  // x0 <- x(j-2)
+        for (int b = 0; b < NB; ++b) {
+            cd xn;
+            if (b < 4) xn = (n >= ls) ? Zst[((size_t)(n - ls) * 4 + b) * nsys + sys] : mk(0.0);
+            // surface basis: e_{n-1}: z(n-1) = 1, z(n) = -L(n,n-1); e_n: z(n) = 1
+            else if (b == 4) xn = (mk(0.0) - tl.Lnn1 * mk(1.0)) / tl.Dn;
+            else xn = mk(1.0) / tl.Dn;
+            if (cn >= 0) store(cn, b, xn);
+            x[b][0] = xn;
+            x[b][1] = mk(0.0);
+            x[b][2] = mk(0.0);
+            if (n - 1 >= jmin_loc) {
+                cd zh = mk(0.0);
+                if (b < 4 && n - 1 >= ls) zh = Zst[((size_t)(n - 1 - ls) * 4 + b) * nsys + sys];
+                if (b == 4) zh = mk(1.0) / tl.Dm1;
+                const cd v = zh - Ln * x[b][0];
+                if (cn1 >= 0) store(cn1, b, v);
+                x[b][1] = x[b][0];
+                x[b][0] = v;
             }
-            // only the last chunk can end with one or two rows (BACK_CH % 3 == 0),
-            // so the roles need not be restored after them
-            if (i < cnt) row(buf, i, hi - i, x0, x1, x2);
-            if (i + 1 < cnt) row(buf, i + 1, hi - i - 1, x2, x0, x1);
         }
     }
-    cp_async_wait<0>();  // no copy outlives the block
+    const int top = n - 2;
+    if (top < jmin_loc) return;
+    int2 cap = caplist[0];
+    int ci = 0;
+    // rows j0, j0 - 1, .. (cnt of them) with E staged entries per row, CH rows per chunk
+    auto phase = [&](auto Etag, auto CHtag, int j0, int cnt) {
+        constexpr int E = decltype(Etag)::value, CH = decltype(CHtag)::value, RING = UP_NBUF * CH;
+        if (cnt <= 0) return;
+        const int nq = (cnt + CH - 1) / CH;
+        auto stage = [&](int q) {
+            if (q >= nq) return;
+            for (int i = 0; i < CH; ++i) {
+                const int t = q * CH + i;
+                if (t >= cnt) break;
+                const int j = j0 - t;
+                cd* dst = ring + (size_t)((t % RING) * E) * 32;
+#pragma unroll
+                for (int p = 0; p < 3; ++p) cp_async16(dst + p * 32, &Lst[((size_t)j * 3 + p) * nsys + sys]);
+                if (E == 7) {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        cp_async16(dst + (3 + b) * 32, &Zst[((size_t)(j - ls) * 4 + b) * nsys + sys]);
+                }
+            }
+        };
+#pragma unroll
+        for (int q = 0; q < UP_NBUF - 1; ++q) {
+            stage(q);
+            cp_async_commit();
+        }
+        // row t (j = j0 - t) with roles (xa, xb, xc) = x[b][A], x[b][B], x[b][C]; x(j) replaces xc
+        auto one = [&](int t, auto Atag, auto Btag, auto Ctag) {
+            constexpr int A = decltype(Atag)::value, B = decltype(Btag)::value, C = decltype(Ctag)::value;
+            if (t % CH == 0) {  // a chunk starts: the one UP_NBUF - 1 ahead goes out, this one is waited for
+                stage(t / CH + UP_NBUF - 1);
+                cp_async_commit();
+                cp_async_wait<UP_NBUF - 1>();
+            }
+            const int j = j0 - t;
+            const cd* src = ring + (size_t)((t % RING) * E) * 32;
+            const cd L1 = src[0], L2 = src[32], L3 = src[64];
+            const bool cap_here = j == cap.x;
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const cd zh = (E == 7 && b < 4) ? src[(3 + b) * 32] : mk(0.0);
+                const cd xa = x[b][A], xb = x[b][B], xc = x[b][C];
+                cd v;
+                if (FAST) {
+                    cd sum = cmulT<true>(L3, xc);
+                    sum = caddmulT<true>(sum, L2, xb);
+                    sum = caddmulT<true>(sum, L1, xa);
+                    v = zh - sum;
+                } else if (j == n - 2) {
+                    cd sum = mk(0.0) + L2 * xb + L1 * xa;
+                    v = zh - sum;
+                } else {
+                    cd sum = mk(0.0) + L3 * xc + L2 * xb + L1 * xa;
+                    v = zh - sum;
+                }
+                if (cap_here) store(cap.y, b, v);
+                x[b][C] = v;
+            }
+            if (cap_here) cap = caplist[++ci];
+        };
+        using I0 = std::integral_constant<int, 0>;
+        using I1 = std::integral_constant<int, 1>;
+        using I2 = std::integral_constant<int, 2>;
+        int t = 0;
+        for (; t + 3 <= cnt; t += 3) {
+            one(t, I0{}, I1{}, I2{});      // x[.][2] <- x(j)
+            one(t + 1, I2{}, I0{}, I1{});  // x[.][1] <- x(j-1)
+            one(t + 2, I1{}, I2{}, I0{});  // x[.][0] <- x(j-2)
+        }
+        if (t < cnt) {  // one or two rows left: run them, then restore the roles
+            one(t, I0{}, I1{}, I2{});
+            if (t + 1 < cnt) {
+                one(t + 1, I2{}, I0{}, I1{});
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {  // (x0, x1, x2) = (x(j+1), x(j+2), x(j+3)) again
+                    const cd a0 = x[b][0];
+                    x[b][0] = x[b][1];
+                    x[b][1] = x[b][2];
+                    x[b][2] = a0;
+                }
+            } else {
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    const cd a2 = x[b][2];
+                    x[b][2] = x[b][1];
+                    x[b][1] = x[b][0];
+                    x[b][0] = a2;
+                }
+            }
+        }
+        cp_async_wait<0>();  // the ring is reused by the next phase
+    };
+    const int lo1 = max(ls, jmin_loc);
+    const int n1 = top >= lo1 ? top - lo1 + 1 : 0;  // rows at and above the source
+    phase(std::integral_constant<int, UP_E1>{}, std::integral_constant<int, UP_CH1>{}, top, n1);
+    phase(std::integral_constant<int, UP_E2>{}, std::integral_constant<int, UP_CH2>{}, top - n1,
+          top - n1 - jmin_loc + 1);
 }
 
 // ------------------------------------------------------------ l = 0 path
@@ -1024,17 +1080,19 @@ __global__ void __launch_bounds__(128) k_psv_l0_solve(PsvDev d, const int* __res
 
 // (3) fields of order 0, one thread per (frequency, receiver): m = 0 slots
 // q = 0..2 (imt 1..3) and 3 (back), U and dU/dr (calup0 uses u(1) only)
-__device__ __forceinline__ void put_field(double* Aw, int Lcap, int nq, int R, int q, int r, int f, cd v) {
+template <class T>
+__device__ __forceinline__ void put_field(T* Aw, int Lcap, int nq, int R, int q, int r, int f, cd v) {
     // rows ordered (field group, slot, field, re/im, receiver): receivers
     // contiguous, so the epilogue's threads (consecutive receivers) read
     // consecutive rows
     const size_t row = psvk::fld_row(nq, R, q, f) + r;
-    Aw[row * Lcap] = v.re;
-    Aw[(row + (R + 1)) * Lcap] = v.im;
+    Aw[row * Lcap] = (T)v.re;
+    Aw[(row + (R + 1)) * Lcap] = (T)v.im;
 }
 
-__global__ void k_psv_l0_fields(PsvDev d, const cd* __restrict__ Dv, double* __restrict__ A0f,
-                                double* __restrict__ A1f, double* __restrict__ A2f, int Lcap, int back) {
+template <class T>
+__global__ void k_psv_l0_fields(PsvDev d, const cd* __restrict__ Dv, T* __restrict__ A0f, T* __restrict__ A1f,
+                                T* __restrict__ A2f, int Lcap, int back) {
     int w = blockIdx.y;
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int R = d.R;
@@ -1043,9 +1101,9 @@ __global__ void k_psv_l0_fields(PsvDev d, const cd* __restrict__ Dv, double* __r
     const cd* D = Dv + (size_t)w * (n0 + 1) * 4;
     const int rows0 = NS0 * (R + 1) * NFLD * 2, rows1 = NS1 * (R + 1) * NFLD * 2,
               rows2 = NS2 * (R + 1) * NFLD * 2;
-    double* A0w = A0f + (size_t)w * rows0 * Lcap;
-    double* A1w = A1f + (size_t)w * rows1 * Lcap;
-    double* A2w = A2f + (size_t)w * rows2 * Lcap;
+    T* A0w = A0f + (size_t)w * rows0 * Lcap;
+    T* A1w = A1f + (size_t)w * rows1 * Lcap;
+    T* A2w = A2f + (size_t)w * rows2 * Lcap;
     for (int q = 0; q < NS0; ++q) {
         cd U = mk(0.0), Ud = mk(0.0);
         if (q < 3 || back) {
@@ -1373,11 +1431,11 @@ __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restric
 // the surface (rows n-1, n).
 constexpr int FLD_SYS = 8, FLD_REC = 4;
 
+template <class T>
 __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int nsys,
                                                     const cd* __restrict__ Xcap, const cd* __restrict__ co,
-                                                    double* __restrict__ A0f, double* __restrict__ A1f,
-                                                    double* __restrict__ A2f, int Lcap,
-                                                    double* __restrict__ amps) {
+                                                    T* __restrict__ A0f, T* __restrict__ A1f, T* __restrict__ A2f,
+                                                    int Lcap, double* __restrict__ amps) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int sys = (blockIdx.x * 4 + warp) * FLD_SYS + (lane & (FLD_SYS - 1));
     const int r = blockIdx.y * FLD_REC + (lane >> 3);
@@ -1388,7 +1446,7 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
     if (l == 0) return;  // written by the order-0 kernels
     const size_t rows[3] = {(size_t)NS0 * (R + 1) * NFLD * 2, (size_t)NS1 * (R + 1) * NFLD * 2,
                             (size_t)NS2 * (R + 1) * NFLD * 2};
-    double* Aw[3] = {A0f + (size_t)w * rows[0] * Lcap + l, A1f + (size_t)w * rows[1] * Lcap + l,
+    T* Aw[3] = {A0f + (size_t)w * rows[0] * Lcap + l, A1f + (size_t)w * rows[1] * Lcap + l,
                      A2f + (size_t)w * rows[2] * Lcap + l};
     const double l2 = (double)l * (double)(l + 1), lsq = sqrt(l2);
     auto X = [&](int cap, int b) { return Xcap[((size_t)cap * NB + b) * nsys + sys]; };
@@ -1482,20 +1540,25 @@ class PsvEngine : public Engine {
     PsvDev d{};
     DBuf<int> iphase, nlayer, kkdr, elem, hmoff, blkoff, amz, amc, bcrow, rcap, fluid, comp_src, jsta,
         capmap, l0col, l0e1;
+    DBuf<int2> caplist;
     DBuf<double> qmu, qkappa, sel, fel, hm, bcval, poly, lam, qkp, fr, r, rrsta;
     DBuf<cd> B0, B1, B2, Prow, Lst, Zst, Xcap, l0scr, l0d, ab, co;
     DBuf<int4> rowasm;
     DBuf<SysTail> tails;
     int jmin_loc = 1, ncap = 0;
+    float* afld32(int m) { return reinterpret_cast<float*>(Afld[m].p); }
     double vtop = 0, rtop = 0;
 
     PsvEngine(const dsm_psv_setup_t* s, const dsm_options_t* o) {
         mode = 1;
         opt = *o;
         init_common(opt.device);
-        // the substitution's staged multipliers exceed the default 48 KB
-        DSM_CUDA(cudaFuncSetAttribute(k_psv_back<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BACK_SMEM));
-        DSM_CUDA(cudaFuncSetAttribute(k_psv_back<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BACK_SMEM));
+        // the mixed path splits the fields into 11-bit pieces: FP32 storage
+        // (24 bits) loses nothing it keeps and halves their traffic
+        afld_bytes = mixed() ? 4 : 8;
+        // the substitution's staging rings exceed the default 48 KB
+        DSM_CUDA(cudaFuncSetAttribute(k_psv_up<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UP_SMEM));
+        DSM_CUDA(cudaFuncSetAttribute(k_psv_up<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UP_SMEM));
         m_lo = 0;
         R = s->r_n;
         Th = s->theta_n;
@@ -1588,6 +1651,14 @@ class PsvEngine : public Engine {
 
         jmin_loc = jmin - d.itmp + 1;
         capmap.upload(cm, st); rcap.upload(rc, st); fluid.upload(fl, st);
+        {  // captured rows below n - 1 in descending order, for the upward substitution
+            std::vector<int2> cl;
+            const int nloc = nn - d.itmp + 1;
+            for (int j = nloc - 2; j >= jmin_loc; --j)
+                if (cm[j + d.itmp - 1] >= 0) cl.push_back(make_int2(j, cm[j + d.itmp - 1]));
+            cl.push_back(make_int2(-1, -1));
+            caplist.upload(cl, st);
+        }
         lam.upload(s->lambda, R, st); qkp.upload(s->qkp, R, st); fr.upload(frv, st);
         // l = 0 compaction (rea2): jsta, compact row of every kept global row
         {
@@ -1683,7 +1754,7 @@ class PsvEngine : public Engine {
         l0d.reserve((size_t)F * (d.nn0 + 1) * 4);
         ab.reserve((size_t)F * 320);
         co.reserve((size_t)NSLOT * NB * nsys);
-        for (int m = 0; m < 3; ++m) Afld[m].reserve((size_t)F * rows_m[m] * Lcap);
+        for (int m = 0; m < 3; ++m) Afld[m].reserve(((size_t)F * rows_m[m] * Lcap * afld_bytes + 7) / 8);
         Cgemm.reserve(c_total());
         cut.reserve(F);
         amps.reserve((size_t)F * Lcap);
@@ -1727,8 +1798,12 @@ class PsvEngine : public Engine {
                                                                             l0e1.p, l0scr.p);
             if (mixed()) k_psv_l0_solve<true><<<nf, 128, 0, st2>>>(d, fr_, nf, ab.p, l0scr.p, l0d.p, rsgt_sw);
             else k_psv_l0_solve<false><<<nf, 128, 0, st2>>>(d, fr_, nf, ab.p, l0scr.p, l0d.p, rsgt_sw);
-            k_psv_l0_fields<<<dim3((R + 1 + 127) / 128, nf), 128, 0, st2>>>(d, l0d.p, Afld[0].p, Afld[1].p,
-                                                                             Afld[2].p, Lcap, rsgt_sw);
+            if (afld_bytes == 4)
+                k_psv_l0_fields<float><<<dim3((R + 1 + 127) / 128, nf), 128, 0, st2>>>(
+                    d, l0d.p, afld32(0), afld32(1), afld32(2), Lcap, rsgt_sw);
+            else
+                k_psv_l0_fields<double><<<dim3((R + 1 + 127) / 128, nf), 128, 0, st2>>>(
+                    d, l0d.p, Afld[0].p, Afld[1].p, Afld[2].p, Lcap, rsgt_sw);
             kend(id0, 0.0, 0.0, st2);
             DSM_LAUNCH(*this);
             l0_done = true;
@@ -1756,11 +1831,11 @@ class PsvEngine : public Engine {
         id = kid("psv_substitution");
         kbegin(id);
         if (mixed())
-            k_psv_back<true><<<(nsys + BACK_SYS - 1) / BACK_SYS, BACK_THREADS, BACK_SMEM, st>>>(
-                d, nsys, jmin_loc, capmap.p, Lst.p, Zst.p, tails.p, Xcap.p);
+            k_psv_up<true><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
+                d, nsys, jmin_loc, capmap.p, caplist.p, Lst.p, Zst.p, tails.p, Xcap.p);
         else
-            k_psv_back<false><<<(nsys + BACK_SYS - 1) / BACK_SYS, BACK_THREADS, BACK_SMEM, st>>>(
-                d, nsys, jmin_loc, capmap.p, Lst.p, Zst.p, tails.p, Xcap.p);
+            k_psv_up<false><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
+                d, nsys, jmin_loc, capmap.p, caplist.p, Lst.p, Zst.p, tails.p, Xcap.p);
         kend(id, sub_bytes * nsys, 0.0);
         DSM_LAUNCH(*this);
         id = kid("psv_source_coef");
@@ -1771,8 +1846,12 @@ class PsvEngine : public Engine {
         dim3 grid((nsys + 4 * FLD_SYS - 1) / (4 * FLD_SYS), (R + 1 + FLD_REC - 1) / FLD_REC);
         id = kid("psv_fields");
         kbegin(id);
-        k_psv_fields<<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, Afld[0].p, Afld[1].p, Afld[2].p,
-                                           Lcap, amps.p);
+        if (afld_bytes == 4)
+            k_psv_fields<float><<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, afld32(0), afld32(1), afld32(2),
+                                                      Lcap, amps.p);
+        else
+            k_psv_fields<double><<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, Afld[0].p, Afld[1].p, Afld[2].p,
+                                                       Lcap, amps.p);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
         stats.solve_bytes += (fac_bytes + sub_bytes) * nsys;
