@@ -1431,7 +1431,16 @@ __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restric
 // the surface (rows n-1, n).
 constexpr int FLD_SYS = 8, FLD_REC = 4;
 
-template <class T>
+// acc + r x for a real r: FAST with fused multiply-adds
+template <bool FAST>
+__device__ __forceinline__ cd caddmulR(cd acc, double r, cd x) {
+    if (FAST) return mk(fma(r, x.re, acc.re), fma(r, x.im, acc.im));
+    return acc + r * x;
+}
+
+// FAST (mixed path, FP32 field storage): fused multiply-adds and one
+// reciprocal of sqrt(l(l+1)); otherwise the reference's operations.
+template <class T, bool FAST>
 __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int nsys,
                                                     const cd* __restrict__ Xcap, const cd* __restrict__ co,
                                                     T* __restrict__ A0f, T* __restrict__ A1f, T* __restrict__ A2f,
@@ -1448,7 +1457,7 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
                             (size_t)NS2 * (R + 1) * NFLD * 2};
     T* Aw[3] = {A0f + (size_t)w * rows[0] * Lcap + l, A1f + (size_t)w * rows[1] * Lcap + l,
                      A2f + (size_t)w * rows[2] * Lcap + l};
-    const double l2 = (double)l * (double)(l + 1), lsq = sqrt(l2);
+    const double l2 = (double)l * (double)(l + 1), lsq = sqrt(l2), ilsq = FAST ? 1.0 / lsq : 0.0;
     auto X = [&](int cap, int b) { return Xcap[((size_t)cap * NB + b) * nsys + sys]; };
     auto C = [&](int s, int b) { return co[((size_t)s * NB + b) * nsys + sys]; };
     if (r == 0) {  // probe: calamp on g0(ksta(r_n)-1), g0(ksta(r_n)) of imt = 1, m = 0
@@ -1472,10 +1481,10 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
             int cu = d.rcap[6 * r + 2 * i], cvv = d.rcap[6 * r + 2 * i + 1];
             for (int b = 0; b < NB; ++b) {
                 cd xu = X(cu, b), xv = X(cvv, b);
-                bU[b] = bU[b] + wvi * xu;
-                bV[b] = bV[b] + wvi * xv;
-                bUd[b] = bUd[b] + wdi * xu;
-                bVd[b] = bVd[b] + wdi * xv;
+                bU[b] = caddmulR<FAST>(bU[b], wvi, xu);
+                bV[b] = caddmulR<FAST>(bV[b], wvi, xv);
+                bUd[b] = caddmulR<FAST>(bUd[b], wdi, xu);
+                bVd[b] = caddmulR<FAST>(bVd[b], wdi, xv);
             }
         }
     }
@@ -1486,13 +1495,27 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
         if (!(surf && isback)) {
             for (int b = 0; b < NB; ++b) {
                 cd cb = C(s, b);
-                U = U + cb * bU[b];
-                V = V + cb * bV[b];
-                Ud = Ud + cb * bUd[b];
-                Vd = Vd + cb * bVd[b];
+                if (FAST) {
+                    U = caddmulT<true>(U, cb, bU[b]);
+                    V = caddmulT<true>(V, cb, bV[b]);
+                    Ud = caddmulT<true>(Ud, cb, bUd[b]);
+                    Vd = caddmulT<true>(Vd, cb, bVd[b]);
+                } else {
+                    U = U + cb * bU[b];
+                    V = V + cb * bV[b];
+                    Ud = Ud + cb * bUd[b];
+                    Vd = Vd + cb * bVd[b];
+                }
             }
         }
-        cd Vh = V / lsq, Vdh = Vd / lsq;
+        cd Vh, Vdh;
+        if (FAST) {
+            Vh = V * ilsq;
+            Vdh = Vd * ilsq;
+        } else {
+            Vh = V / lsq;
+            Vdh = Vd / lsq;
+        }
         const int nqm = mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2);
         put_field(Aw[mi], Lcap, nqm, R, q, r, 0, U);
         put_field(Aw[mi], Lcap, nqm, R, q, r, 1, Ud);
@@ -1502,36 +1525,95 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
     }
 }
 
+// The cutoff test of one frequency is a sequential state machine over
+// (l, m); here one warp runs it 32 orders at a time with the same results.
+// Per order l >= 1 the updates are m = -2 (l >= 2), -1, 0, 1, 2 (l >= 2);
+// only m = 0 has a nonzero amplitude, so
+//   maxamp at the m = 0 update = max(carry, 0, amplitudes of orders <= l),
+//   ismall after l = 0 when l < lsuf, else ismall + nm (m = 0 small) or the
+//   count of updates after m = 0 (not small),
+// a prefix maximum and a prefix composition of v -> a v + b (a in {0, 1}),
+// both exact.  The exit fires at the first order whose incoming ismall
+// exceeds 20.
+__device__ __forceinline__ double warp_prefix_max(double x, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x = fmax(x, y);
+    }
+    return x;
+}
 __global__ void k_psv_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ratl, double tlen,
                            double vtop, double rtop, const int* __restrict__ freqs,
                            const double* __restrict__ amps, CutState* __restrict__ cut) {
-    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
     if (w >= nf) return;
     CutState c = cut[w];
     if (c.done) return;
-    double omega = 2.0 * kPi * (double)freqs[w] / tlen;
-    int lsuf = (int)(omega * rtop / vtop - 0.5) + 1;
+    const double omega = 2.0 * kPi * (double)freqs[w] / tlen;
+    const int lsuf = (int)(omega * rtop / vtop - 0.5) + 1;
     const int l0 = wl.lb[w], l1 = l0 + wl.off[w + 1] - wl.off[w];
-    for (int l = l0; l < l1; ++l) {
-        if (c.ismall > 20) {
-            if (c.llog > l) c.llog = l;
+    double mx = c.maxamp;
+    int v = c.ismall;
+    for (int base = l0; base < l1; base += 32) {
+        const int l = base + lane;
+        const bool in = l < l1, act = in && l >= 1;
+        const double amp = act ? amps[(size_t)w * Lcap + l] : 0.0;
+        // maxamp at this order's m = 0 update (the m = -1 update contributes 0)
+        const double pm = warp_prefix_max(act ? amp : -1.0, lane);
+        const double mxl = fmax(fmax(mx, pm), 0.0);
+        double ratio = 0.0;
+        if (amp != 0.0 && mxl != 0.0) ratio = amp / mxl;
+        const bool small0 = ratio < ratl && l >= lsuf;
+        int ra = 1, rb = 0;  // this order's map v -> ra v + rb
+        if (act) {
+            const int nm = l >= 2 ? 5 : 3, after = l >= 2 ? 2 : 1;
+            if (l < lsuf) { ra = 0; rb = 0; }
+            else if (small0) { ra = 1; rb = nm; }
+            else { ra = 0; rb = after; }
+        }
+        // inclusive composition over lanes <= this one
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int pa = __shfl_up_sync(0xffffffffu, ra, o), pb = __shfl_up_sync(0xffffffffu, rb, o);
+            if (lane >= o) { rb = ra * pb + rb; ra = ra * pa; }
+        }
+        const int vafter = ra * v + rb;
+        int vbefore = __shfl_up_sync(0xffffffffu, vafter, 1);
+        if (lane == 0) vbefore = v;
+        const unsigned ex = __ballot_sync(0xffffffffu, in && vbefore > 20);
+        if (ex) {
+            const int e = __ffs(ex) - 1, le = base + e;
+            const int ve = __shfl_sync(0xffffffffu, vbefore, e);
+            // maxamp after the orders before le (those of this chunk are all active
+            // unless one is order 0)
+            const double pe = __shfl_sync(0xffffffffu, pm, e > 0 ? e - 1 : 0);
+            double me = e > 0 ? fmax(mx, pe) : mx;
+            if (e > 0 && base + e - 1 >= 1) me = fmax(me, 0.0);
+            if (c.llog > le) c.llog = le;
             c.done = 1;
-            c.norders = l;
-            break;
+            c.norders = le;
+            c.ismall = ve;
+            c.maxamp = me;
+            if (lane == 0) cut[w] = c;
+            return;
         }
-        if (l >= 1) {  // calamp is called for imt = 1 of every m of the l != 0 branch
-            for (int m = -2; m <= 2; ++m) {
-                if (abs(m) > l) continue;
-                double amp = (m == 0) ? amps[(size_t)w * Lcap + l] : 0.0, ampratio = 0.0;
-                if (amp > c.maxamp) c.maxamp = amp;
-                if (amp != 0.0 && c.maxamp != 0.0) ampratio = amp / c.maxamp;
-                if (ampratio < ratl && l >= lsuf) c.ismall++;
-                else c.ismall = 0;
-            }
+        // carry past the chunk
+        const int last = min(31, l1 - 1 - base);
+        const double plast = __shfl_sync(0xffffffffu, pm, last);
+        const bool any_act = __ballot_sync(0xffffffffu, act) != 0;
+        mx = fmax(mx, plast);
+        if (any_act) mx = fmax(mx, 0.0);
+        v = __shfl_sync(0xffffffffu, vafter, last);
+        if (base <= maxlmax && maxlmax < base + 32 && maxlmax < l1) {
+            c.done = 1;
+            c.norders = maxlmax + 1;
         }
-        if (l == maxlmax) { c.done = 1; c.norders = maxlmax + 1; }
     }
-    cut[w] = c;
+    c.maxamp = mx;
+    c.ismall = v;
+    if (lane == 0) cut[w] = c;
 }
 
 // ---------------------------------------------------------------- engine
@@ -1847,11 +1929,11 @@ class PsvEngine : public Engine {
         id = kid("psv_fields");
         kbegin(id);
         if (afld_bytes == 4)
-            k_psv_fields<float><<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, afld32(0), afld32(1), afld32(2),
-                                                      Lcap, amps.p);
+            k_psv_fields<float, true><<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, afld32(0), afld32(1),
+                                                            afld32(2), Lcap, amps.p);
         else
-            k_psv_fields<double><<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, Afld[0].p, Afld[1].p, Afld[2].p,
-                                                       Lcap, amps.p);
+            k_psv_fields<double, false><<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, Afld[0].p, Afld[1].p,
+                                                              Afld[2].p, Lcap, amps.p);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
         stats.solve_bytes += (fac_bytes + sub_bytes) * nsys;
@@ -1860,7 +1942,7 @@ class PsvEngine : public Engine {
     void scan_chunk(int nf, const WorkList& wl) override {
         int id = kid("psv_cutoff_scan");
         kbegin(id);
-        k_psv_scan<<<(nf + 31) / 32, 32, 0, st>>>(nf, wl, Lcap, maxlmax, ratl, tlen, vtop, rtop,
+        k_psv_scan<<<(nf + 3) / 4, 128, 0, st>>>(nf, wl, Lcap, maxlmax, ratl, tlen, vtop, rtop,
                                                   d_freqs.p, amps.p, cut.p);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
