@@ -147,8 +147,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
 }
+// Tile t of a launch: its problem p, row tile mt and column tile nt.  A CTA
+// visits its tiles in increasing order, so p only moves forward from the
+// previous tile's problem (the caller keeps it, starting at 0).
 __device__ __forceinline__ void decode(const Problem* ps, int np, int t, int& p, int& mt, int& nt) {
-    p = 0;
     while (p + 1 < np && ps[p + 1].tile0 <= t) ++p;
     const int loc = t - ps[p].tile0;
     mt = loc / ps[p].tiles_n;
@@ -204,10 +206,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 
     if (warp == 0) {
         if (lane == 0) {  // ---------------------------------------- producer
-            int it = 0;
+            int it = 0, p = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                int p, mt, nt;
+                int mt, nt;
                 decode(ps, np, t, p, mt, nt);
                 const Problem& P = ps[p];
                 for (int kb = 0; kb < P.kblocks; ++kb, ++it) {
@@ -234,10 +236,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {  // ---------------------------------------- MMA issuer
-            int it = 0, cc = 0;
+            int it = 0, cc = 0, p = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-                int p, mt, nt;
+                int mt, nt;
                 decode(ps, np, t, p, mt, nt);
                 const int kbn = ps[p].kblocks, ch = chunk > 0 ? chunk : kbn;
                 uint32_t dh = tmem;
@@ -290,10 +292,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         // the chunks are summed in FP64 registers
         const int q = warp & 3, half = (warp - 2) >> 2;
         const uint32_t lanes = (uint32_t)(q * 32) << 16;
-        int cc = 0;
+        int cc = 0, p = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-            int p, mt, nt;
+            int mt, nt;
             decode(ps, np, t, p, mt, nt);
             const Problem& P = ps[p];
             const int kbn = P.kblocks, ch = chunk > 0 ? chunk : kbn, nch = (kbn + ch - 1) / ch;
