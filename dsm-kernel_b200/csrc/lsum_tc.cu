@@ -405,6 +405,60 @@ __device__ __forceinline__ void split2(double x, int fmt, uint16_t& hi, uint16_t
     }
 }
 
+// the same split for an FP32 value already scaled by 2^-e: the residual
+// x - hi has at most 13 (fp16) or 16 (bf16) significant bits, so it is exact
+// in FP32 and each piece is one rounding of an exact value, as in split2
+__device__ __forceinline__ void split2f(float x, int fmt, uint16_t& hi, uint16_t& lo) {
+    if (fmt == PIECE_BF16) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        hi = __bfloat16_as_ushort(h);
+        lo = __bfloat16_as_ushort(__float2bfloat16_rn(x - __bfloat162float(h)));
+    } else {
+        const __half h = __float2half_rn(x);
+        hi = __half_as_ushort(h);
+        lo = __half_as_ushort(__float2half_rn(x - __half2float(h)));
+    }
+}
+
+// FP32 rows whose length is a multiple of four: one warp per row, four
+// orders per lane and step (16-byte loads, 8-byte piece stores)
+__global__ void k_split_rows_f4(const float* __restrict__ A, int nrows, int per_w, int lcap,
+                                const int* __restrict__ nord, int kcap, int bk, uint16_t* __restrict__ P,
+                                size_t piece_stride, float* __restrict__ sa, int fmt) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= nrows) return;
+    const int K = nord ? min(nord[row / per_w], lcap) : lcap;
+    const int Kp = min(kcap, (K + bk - 1) / bk * bk);
+    const float4* a4 = reinterpret_cast<const float4*>(A + (size_t)row * lcap);
+    float mx = 0.0f;
+    for (int i = lane; 4 * i < K; i += 32) {
+        const float4 v = a4[i];
+        mx = fmaxf(mx, fabsf(v.x));
+        if (4 * i + 1 < K) mx = fmaxf(mx, fabsf(v.y));
+        if (4 * i + 2 < K) mx = fmaxf(mx, fabsf(v.z));
+        if (4 * i + 3 < K) mx = fmaxf(mx, fabsf(v.w));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const int e = piece_exp((double)mx);
+    if (lane == 0) sa[row] = __int_as_float((127 + e) << 23);
+    uint2* ph = reinterpret_cast<uint2*>(P + (size_t)row * kcap);
+    uint2* pl = reinterpret_cast<uint2*>(P + piece_stride + (size_t)row * kcap);
+    for (int i = lane; 4 * i < Kp; i += 32) {
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (4 * i < K) v = a4[i];
+        const float x[4] = {v.x, v.y, v.z, v.w};
+        uint16_t h[4], lo[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            h[c] = lo[c] = 0;
+            if (4 * i + c < K) split2f(ldexpf(x[c], -e), fmt, h[c], lo[c]);
+        }
+        ph[i] = make_uint2((uint32_t)h[0] | ((uint32_t)h[1] << 16), (uint32_t)h[2] | ((uint32_t)h[3] << 16));
+        pl[i] = make_uint2((uint32_t)lo[0] | ((uint32_t)lo[1] << 16), (uint32_t)lo[2] | ((uint32_t)lo[3] << 16));
+    }
+}
+
 // one warp per row: row maximum over the counted orders, then the pieces
 template <class TIN>
 __global__ void k_split_rows(const TIN* __restrict__ A, int nrows, int per_w, int lcap,
@@ -487,7 +541,10 @@ void split_fields(const void* A, int in_bytes, int nf, int rows, int lcap, const
     const int n = nf * rows;
     if (n <= 0) return;
     if (kcap % bk) throw Error(DSM_ERR_INVALID, "order capacity of the split fields is not a multiple of BK");
-    if (in_bytes == 4)
+    if (in_bytes == 4 && lcap % 4 == 0 && kcap % 4 == 0)
+        k_split_rows_f4<<<(n + 7) / 8, 256, 0, st>>>(static_cast<const float*>(A), n, rows, lcap, d_nord, kcap, bk,
+                                                     P, (size_t)F * rows * kcap, sa, piece_fmt);
+    else if (in_bytes == 4)
         k_split_rows<float><<<(n + 7) / 8, 256, 0, st>>>(static_cast<const float*>(A), n, rows, lcap, d_nord, kcap,
                                                          bk, P, (size_t)F * rows * kcap, sa, piece_fmt);
     else
