@@ -1823,6 +1823,9 @@ class PsvEngine : public Engine {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
         nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(65536, (fr / 3) / per));
+        // DSM_MAX_SYSTEMS caps the systems per solve launch (and so the
+        // factor scratch) below that, e.g. for small profiling captures
+        if (const char* e = std::getenv("DSM_MAX_SYSTEMS")) nsys_max = std::max(1024, std::min(nsys_max, std::atoi(e)));
         size_t nsys = nsys_max;
         B0.reserve((size_t)F * d.ncol_tot * 4);
         B1.reserve((size_t)F * d.ncol_tot * 4);

@@ -24,6 +24,7 @@
 //                (calu, locallyCartesianDerivatives, udertotsgtSH,
 //                udertorsgtSH, utosynnSH, others.f90:132-367, 829-838).
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 
 #include "engine.cuh"
@@ -617,6 +618,9 @@ class ShEngine : public Engine {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
         nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(65536, (fr / 3) / per));
+        // DSM_MAX_SYSTEMS caps the systems per solve launch (and so the
+        // factor scratch) below that, e.g. for small profiling captures
+        if (const char* e = std::getenv("DSM_MAX_SYSTEMS")) nsys_max = std::max(1024, std::min(nsys_max, std::atoi(e)));
         size_t nsys = nsys_max;
         a0.reserve((size_t)F * (nn + 1) * 2);
         a2.reserve((size_t)F * (nn + 1) * 2);
