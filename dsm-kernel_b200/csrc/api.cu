@@ -40,6 +40,8 @@ void Engine::init_common(int dev) {
     }
     DSM_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     DSM_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    DSM_CUDA(cudaStreamCreateWithFlags(&stc, cudaStreamNonBlocking));
+    for (auto& e : ev_grp) DSM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     DSM_CUBLAS(cublasCreate(&cub));
     DSM_CUBLAS(cublasSetStream(cub, st));
     for (auto& e : ev) DSM_CUDA(cudaEventCreate(&e));
@@ -68,6 +70,9 @@ Engine::~Engine() {
     if (st2) { cudaStreamSynchronize(st2); cudaStreamDestroy(st2); }
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (stc) { cudaStreamSynchronize(stc); cudaStreamDestroy(stc); }
+    for (auto& e : ev_grp)
+        if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -153,10 +158,11 @@ void Engine::build_basis(int lneed) {
     }
 }
 
-// Mixed l-sum of a batch: split the field matrices, then one persistent
-// tensor-core launch over every (frequency, |m|) contraction (in groups of
-// at most tc::MAXP).  Outputs go to Cmix, one block per frequency.
-void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
+// Mixed l-sum of a batch: split the field matrices, then persistent
+// tensor-core launches over the (frequency, |m|) contractions (at most
+// tc::MAXP per launch).  Outputs go to Cmix, one block per frequency.
+void Engine::lsum_prepare(int nf, const std::vector<int>& nord) {
+    (void)nf;
     kcA = (Lcap + 63) / 64 * 64;
     for (int m = m_lo; m <= 2; ++m) {
         if (!rows_m[m]) continue;
@@ -165,9 +171,22 @@ void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
     }
     Cmix.reserve((size_t)F * c_total());
     d_nord.upload(nord, st);
+    std::memset(&tcmaps, 0, sizeof(tcmaps));
+    for (int m = m_lo; m <= 2; ++m) {
+        if (!rows_m[m]) continue;
+        tc::encode_a(&tcmaps.a[m], Apc[m].p, tc_fmt, kcA, rows_m[m], F, tc_bk);
+        tc::encode_b(&tcmaps.b[m], Bpc[m].p, tc_fmt, kcB, 2 * Th, tc_bk);
+    }
+    tcp.reserve((size_t)F * 6);  // at most two row groups per |m| and frequency
+    tcp_next = 0;
+}
+
+void Engine::lsum_group(int w0, int w1, const std::vector<int>& nord) {
+    const int n = w1 - w0;
+    if (n <= 0) return;
     double split_bytes = 0.0, tflops = 0.0, tc_bytes = 0.0;
     for (int m = m_lo; m <= 2; ++m)
-        for (int w = 0; w < nf; ++w) {
+        for (int w = w0; w < w1; ++w) {
             const double kp = (double)((nord[w] + tc_bk - 1) / tc_bk * tc_bk);
             split_bytes += (double)rows_m[m] * ((double)afld_bytes * nord[w] + 4.0 * kp);
         }
@@ -175,23 +194,18 @@ void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
     kbegin(id);
     for (int m = m_lo; m <= 2; ++m) {
         if (!rows_m[m]) continue;
-        tc::split_fields(Afld[m].p, afld_bytes, nf, rows_m[m], Lcap, d_nord.p, Apc[m].p, sA[m].p, kcA, F, tc_fmt,
-                         tc_bk, st);
+        const size_t rw = (size_t)rows_m[m];
+        const char* A = reinterpret_cast<const char*>(Afld[m].p) + (size_t)w0 * rw * Lcap * afld_bytes;
+        tc::split_fields(A, afld_bytes, n, rows_m[m], Lcap, d_nord.p + w0, Apc[m].p + (size_t)w0 * rw * kcA,
+                         sA[m].p + (size_t)w0 * rw, kcA, F, tc_fmt, tc_bk, st);
         launches++;
     }
     kend(id, split_bytes, 0.0);
 
-    tc::Maps maps;
-    std::memset(&maps, 0, sizeof(maps));
-    for (int m = m_lo; m <= 2; ++m) {
-        if (!rows_m[m]) continue;
-        tc::encode_a(&maps.a[m], Apc[m].p, tc_fmt, kcA, rows_m[m], F, tc_bk);
-        tc::encode_b(&maps.b[m], Bpc[m].p, tc_fmt, kcB, 2 * Th, tc_bk);
-    }
     // per (frequency, |m|): the leading rows against all 2 Th basis
     // columns, the remaining rows against the first Th
     std::vector<tc::Problem> hp;
-    for (int w = 0; w < nf; ++w)
+    for (int w = w0; w < w1; ++w)
         for (int m = m_lo; m <= 2; ++m) {
             if (!rows_m[m]) continue;
             const int rf = full_rows(m);
@@ -217,7 +231,7 @@ void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
                 tc_bytes += 4.0 * ((double)P.M + N) * kp + 4.0 * (double)P.M * N;
             }
         }
-    tcp.reserve(hp.size());
+    if (tcp_next + hp.size() > tcp.n) throw Error(DSM_ERR_INVALID, "contraction list exceeds its buffer");
     id = kid("lsum_tc");
     kbegin(id);
     for (size_t g = 0; g < hp.size(); g += tc::MAXP) {
@@ -227,8 +241,12 @@ void Engine::lsum_mixed(int nf, const std::vector<int>& nord) {
             hp[g + i].tile0 = tiles;
             tiles += ((hp[g + i].M + tc::BM - 1) / tc::BM) * hp[g + i].tiles_n;
         }
-        DSM_CUDA(cudaMemcpyAsync(tcp.p + g, hp.data() + g, sizeof(tc::Problem) * np, cudaMemcpyHostToDevice, st));
-        tc::launch(maps, tcp.p + g, np, tiles, tc_fmt, tc_bk, tc_flags, tc_chunk, tc_err.p, nsm, st);
+        // each launch reads its own slots of tcp, so no copy overwrites a
+        // list an earlier launch may still read
+        tc::Problem* dp = tcp.p + tcp_next;
+        DSM_CUDA(cudaMemcpyAsync(dp, hp.data() + g, sizeof(tc::Problem) * np, cudaMemcpyHostToDevice, st));
+        tcp_next += np;
+        tc::launch(tcmaps, dp, np, tiles, tc_fmt, tc_bk, tc_flags, tc_chunk, tc_err.p, nsm, st);
         launches++;
     }
     kend(id, tc_bytes, tflops);
@@ -474,18 +492,42 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             kend(id, 0.0, 0.0);
         }
         DSM_CUDA(cudaEventRecord(eg0, st));
-        if (mixed()) {
-            std::vector<int> nord(nf);
-            for (int w = 0; w < nf; ++w) nord[w] = hc[w].norders;
-            lsum_mixed(nf, nord);
-        }
-        for (int w = 0; w < nf; ++w) {
-            stats.orders_used += hc[w].norders;
-            if (!mixed())
-                for (int mi = m_lo; mi <= 2; ++mi) gemm_fp64(w, mi, hc[w].norders);
-            epilogue(d_freqs.p, w, nf);
-            for (int mi = m_lo; mi <= 2; ++mi)
-                stats.lsum_flops += 2.0 * (2.0 * full_rows(mi) + (rows_m[mi] - full_rows(mi))) * Th * hc[w].norders;
+        std::vector<int> nord(nf);
+        for (int w = 0; w < nf; ++w) nord[w] = hc[w].norders;
+        if (mixed()) lsum_prepare(nf, nord);
+        // complex64 records for the host leave per group of frequencies on
+        // the copy stream while the next group's l-sum runs
+        const bool rec32 = ho && (ho->tsgt32 || ho->rsgt32 || ho->synn32);
+        const int ngrp = rec32 && nf >= 8 ? MAX_OUT_GROUPS : 1;
+        if (rec32) out32.reserve(2 * (pt + pr + ps) * (size_t)nf);
+        for (int g = 0; g < ngrp; ++g) {
+            const int w0 = g * nf / ngrp, w1 = (g + 1) * nf / ngrp;
+            if (mixed()) lsum_group(w0, w1, nord);
+            for (int w = w0; w < w1; ++w) {
+                stats.orders_used += hc[w].norders;
+                if (!mixed())
+                    for (int mi = m_lo; mi <= 2; ++mi) gemm_fp64(w, mi, hc[w].norders);
+                epilogue(d_freqs.p, w, nf);
+                for (int mi = m_lo; mi <= 2; ++mi)
+                    stats.lsum_flops +=
+                        2.0 * (2.0 * full_rows(mi) + (rows_m[mi] - full_rows(mi))) * Th * hc[w].norders;
+            }
+            if (rec32) {
+                launch_pack32(*this, nf, w0, w1, pt, pr, ps);
+                DSM_CUDA(cudaEventRecord(ev_grp[g], st));
+                DSM_CUDA(cudaStreamWaitEvent(stc, ev_grp[g], 0));
+                const float* o = out32.p;
+                const size_t n = (size_t)(w1 - w0);
+                if (ho->tsgt32)
+                    DSM_CUDA(cudaMemcpyAsync(ho->tsgt32 + 2 * pt * (b0 + w0), o + 2 * pt * w0, 8 * pt * n,
+                                             cudaMemcpyDeviceToHost, stc));
+                if (ho->rsgt32 && rsgt_sw)
+                    DSM_CUDA(cudaMemcpyAsync(ho->rsgt32 + 2 * pr * (b0 + w0), o + 2 * pt * nf + 2 * pr * w0,
+                                             8 * pr * n, cudaMemcpyDeviceToHost, stc));
+                if (ho->synn32 && synn_sw)
+                    DSM_CUDA(cudaMemcpyAsync(ho->synn32 + 2 * ps * (b0 + w0), o + 2 * (pt + pr) * nf + 2 * ps * w0,
+                                             8 * ps * n, cudaMemcpyDeviceToHost, stc));
+            }
         }
         DSM_CUDA(cudaEventRecord(eg1, st));
         // --- 5: outputs
@@ -500,18 +542,12 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
                 DSM_CUDA(cudaMemcpyAsync(ho->rsgt + 2 * pr * b0, out_r.p, 16 * pr * nf, cudaMemcpyDeviceToHost, st));
             if (ho->synn && synn_sw)
                 DSM_CUDA(cudaMemcpyAsync(ho->synn + 2 * ps * b0, out_s.p, 16 * ps * nf, cudaMemcpyDeviceToHost, st));
-            if (ho->tsgt32 || ho->rsgt32 || ho->synn32) {
-                launch_pack32(*this, nf, pt, pr, ps);
-                const float* o = out32.p;
-                if (ho->tsgt32)
-                    DSM_CUDA(cudaMemcpyAsync(ho->tsgt32 + 2 * pt * b0, o, 8 * pt * nf, cudaMemcpyDeviceToHost, st));
-                if (ho->rsgt32 && rsgt_sw)
-                    DSM_CUDA(cudaMemcpyAsync(ho->rsgt32 + 2 * pr * b0, o + 2 * pt * nf, 8 * pr * nf,
-                                             cudaMemcpyDeviceToHost, st));
-                if (ho->synn32 && synn_sw)
-                    DSM_CUDA(cudaMemcpyAsync(ho->synn32 + 2 * ps * b0, o + 2 * (pt + pr) * nf, 8 * ps * nf,
-                                             cudaMemcpyDeviceToHost, st));
-            }
+        }
+        // the next batch overwrites out32 and the outputs: its records wait
+        // for this batch's copies
+        if (rec32) {
+            DSM_CUDA(cudaEventRecord(ev_grp[0], stc));
+            DSM_CUDA(cudaStreamWaitEvent(st, ev_grp[0], 0));
         }
         DSM_CUDA(cudaStreamSynchronize(st));
         check_tc_error();

@@ -52,6 +52,11 @@ class Engine {
     cudaStream_t st = nullptr;
     cudaStream_t st2 = nullptr;      // side stream (independent per-batch work)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // copy stream for host records: a group's records go out while the
+    // next group's l-sum runs
+    cudaStream_t stc = nullptr;
+    static constexpr int MAX_OUT_GROUPS = 4;
+    cudaEvent_t ev_grp[MAX_OUT_GROUPS] = {};
     bool side_pending = false;
     cublasHandle_t cub = nullptr;
     cudaEvent_t ev[8] = {};
@@ -123,7 +128,12 @@ class Engine {
     DBuf<float> Cmix;                // [F][c_total] column-major blocks
     DBuf<tc::Problem> tcp;
     DBuf<int> tc_err, d_nord;
-    void lsum_mixed(int nf, const std::vector<int>& norders);
+    // mixed l-sum of a batch: buffers, tensor maps and order counts once,
+    // then the split and the tensor-core launches of frequencies [w0, w1)
+    void lsum_prepare(int nf, const std::vector<int>& norders);
+    void lsum_group(int w0, int w1, const std::vector<int>& norders);
+    tc::Maps tcmaps;
+    size_t tcp_next = 0;  // next free slot of tcp in this batch
     void check_tc_error();
     // contraction output of (frequency w, |m|) for the epilogue
     const double* c64(int mi) const { return Cgemm.p + c_off(mi); }
@@ -174,7 +184,8 @@ Engine* make_psv_engine(const dsm_psv_setup_t* s, const dsm_options_t* o);
 // shared kernels (tables.cu)
 void launch_basis_tables(Engine& e, int lcap);
 void launch_interp_weights(Engine& e, const double* d_r, const double* d_rrsta);
-void launch_pack32(Engine& e, int nf, size_t per_t, size_t per_r, size_t per_s);
+// complex64 records of frequencies [w0, w1) of a batch of nf into out32
+void launch_pack32(Engine& e, int nf, int w0, int w1, size_t per_t, size_t per_r, size_t per_s);
 
 }  // namespace dsm
 

@@ -242,6 +242,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 int mt, nt;
                 decode(ps, np, t, p, mt, nt);
                 const int kbn = ps[p].kblocks, ch = chunk > 0 ? chunk : kbn;
+                // the last column tile of a contraction runs with N cut to
+                // its columns (a multiple of 16): no MMA time on padding
+                const int nrem = ps[p].N - nt * BN;
+                const uint32_t ncols = (uint32_t)min(BN, (nrem + 15) & ~15);
+                const uint32_t idt = (idesc & ~(0x3Fu << 17)) | ((ncols >> 3) << 17);
                 uint32_t dh = tmem;
                 int hb = 0;
                 for (int kb = 0; kb < kbn; ++kb, ++it) {
@@ -268,13 +273,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
                     for (int j = 0; j < BK / 16; ++j) {
                         const uint32_t o = 32u * j;
-                        mma_f16(dh, sdesc<BK>(ah + o), sdesc<BK>(bl + o), idesc, (cfirst && j == 0) ? 0u : 1u);
-                        mma_f16(dh, sdesc<BK>(al + o), sdesc<BK>(bh + o), idesc, 1u);
+                        mma_f16(dh, sdesc<BK>(ah + o), sdesc<BK>(bl + o), idt, (cfirst && j == 0) ? 0u : 1u);
+                        mma_f16(dh, sdesc<BK>(al + o), sdesc<BK>(bh + o), idt, 1u);
                     }
 #pragma unroll
                     for (int j = 0; j < BK / 16; ++j) {
                         const uint32_t o = 32u * j;
-                        mma_f16(dh, sdesc<BK>(ah + o), sdesc<BK>(bh + o), idesc, 1u);
+                        mma_f16(dh, sdesc<BK>(ah + o), sdesc<BK>(bh + o), idt, 1u);
                     }
                     mma_commit(&empty[s]);
                     if (kb % ch == ch - 1 || kb == kbn - 1) {

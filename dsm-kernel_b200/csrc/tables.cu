@@ -204,18 +204,21 @@ void launch_interp_weights(Engine& e, const double* d_r, const double* d_rrsta) 
     DSM_LAUNCH(e);
 }
 
-void launch_pack32(Engine& e, int nf, size_t per_t, size_t per_r, size_t per_s) {
-    e.out32.reserve(2 * (per_t + per_r + per_s) * nf);
+void launch_pack32(Engine& e, int nf, int w0, int w1, size_t per_t, size_t per_r, size_t per_s) {
     float* o = e.out32.p;
-    int grid = 148 * 8;
-    k_pack<<<grid, 256, 0, e.st>>>(nf, e.num_t, e.R, e.Th, e.out_t.p, o);
+    const int n = w1 - w0;
+    if (n <= 0) return;
+    int grid = e.nsm * 8;
+    k_pack<<<grid, 256, 0, e.st>>>(n, e.num_t, e.R, e.Th, e.out_t.p + 2 * per_t * w0, o + 2 * per_t * w0);
     DSM_LAUNCH(e);
     if (e.rsgt_sw) {
-        k_pack<<<grid, 256, 0, e.st>>>(nf, e.num_r, e.R, e.Th, e.out_r.p, o + 2 * per_t * nf);
+        k_pack<<<grid, 256, 0, e.st>>>(n, e.num_r, e.R, e.Th, e.out_r.p + 2 * per_r * w0,
+                                       o + 2 * per_t * nf + 2 * per_r * w0);
         DSM_LAUNCH(e);
     }
     if (e.synn_sw) {
-        k_pack<<<grid, 256, 0, e.st>>>(nf, e.num_s, 1, e.Th, e.out_s.p, o + 2 * (per_t + per_r) * nf);
+        k_pack<<<grid, 256, 0, e.st>>>(n, e.num_s, 1, e.Th, e.out_s.p + 2 * per_s * w0,
+                                       o + 2 * (per_t + per_r) * nf + 2 * per_s * w0);
         DSM_LAUNCH(e);
     }
 }

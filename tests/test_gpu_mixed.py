@@ -63,3 +63,19 @@ def test_psv_mixed_close_to_fp64(built, prec, tol):
     print(prec, {k: max(v) for k, v in errs.items()})
     for k, v in errs.items():
         assert max(v) <= tol, (k, v)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [dsmsgt.DSM_PREC_FP64, dsmsgt.DSM_PREC_MIXED])
+def test_records_match_outputs_when_copied_in_groups(prec):
+    # ten frequencies in one batch: the complex64 records leave in groups on
+    # the copy stream while later groups run; each must be the complex64 cast
+    # of the same run's complex128 output, in record order [r][theta][comp]
+    s = dsmsgt.Setup(psv_small(), "psv")
+    freqs = [3, 5, 8, 11, 14, 17, 20, 23, 26, 29]
+    ctx = dsmsgt.Context(s, precision=prec, freq_batch=len(freqs))
+    t, r, y, llog, (t32, r32, y32) = ctx.run(freqs, want32=True)
+    ctx.close()
+    assert np.array_equal(t32, np.transpose(t, (0, 2, 1, 3)).astype(np.complex64))
+    assert np.array_equal(r32, np.transpose(r, (0, 2, 1, 3)).astype(np.complex64))
+    assert np.array_equal(y32, y.astype(np.complex64))
