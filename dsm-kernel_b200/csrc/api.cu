@@ -498,7 +498,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
         // complex64 records for the host leave per group of frequencies on
         // the copy stream while the next group's l-sum runs
         const bool rec32 = ho && (ho->tsgt32 || ho->rsgt32 || ho->synn32);
-        const int ngrp = rec32 && nf >= 8 ? MAX_OUT_GROUPS : 1;
+        const int ngrp = !rec32 ? 1 : (nf >= 2 * MAX_OUT_GROUPS ? MAX_OUT_GROUPS : std::max(1, nf / 2));
         if (rec32) out32.reserve(2 * (pt + pr + ps) * (size_t)nf);
         for (int g = 0; g < ngrp; ++g) {
             const int w0 = g * nf / ngrp, w1 = (g + 1) * nf / ngrp;

@@ -55,7 +55,7 @@ class Engine {
     // copy stream for host records: a group's records go out while the
     // next group's l-sum runs
     cudaStream_t stc = nullptr;
-    static constexpr int MAX_OUT_GROUPS = 4;
+    static constexpr int MAX_OUT_GROUPS = 8;
     cudaEvent_t ev_grp[MAX_OUT_GROUPS] = {};
     bool side_pending = false;
     cublasHandle_t cub = nullptr;
