@@ -226,8 +226,11 @@ void Engine::lsum_group(int w0, int w1, const std::vector<int>& nord) {
                 P.sb = sB[m].p;
                 P.ldc = rows_m[m];
                 hp.push_back(P);
+                // algorithmic: one real product per (row, column, order) up to
+                // the cutoff (the tensor cores run three piece products on
+                // orders padded to BK)
                 const double kp = (double)P.kblocks * tc_bk;
-                tflops += 3.0 * 2.0 * P.M * (double)N * kp;
+                tflops += 2.0 * P.M * (double)N * (double)nord[w];
                 tc_bytes += 4.0 * ((double)P.M + N) * kp + 4.0 * (double)P.M * N;
             }
         }
