@@ -69,6 +69,8 @@ struct PsvDev {
     int cap_p0, cap_p1;     // capture index of the probe rows ksta(r_n)-1, ksta(r_n)
     const double *wv, *wd;
     const int* fluid;       // [R]
+    int Rs1, Rf;            // receiver rows of the solid class (incl. the surface), fluid receivers
+    const int* rrow;        // [R+1] class index of each receiver row (psvk::fld_row)
     const double *lam, *qkp, *fr;  // [R]  lambda, Qkappa, float(r)
     // l = 0 compaction
     int nn0, itmp0, kc0;    // compact size, first row kept, compact row of jtmp
@@ -1080,14 +1082,16 @@ __global__ void __launch_bounds__(128) k_psv_l0_solve(PsvDev d, const int* __res
 
 // (3) fields of order 0, one thread per (frequency, receiver): m = 0 slots
 // q = 0..2 (imt 1..3) and 3 (back), U and dU/dr (calup0 uses u(1) only)
+// rows ordered (field group, slot, field, re/im, receiver): receivers
+// contiguous, so the epilogue's threads (consecutive receivers) read
+// consecutive rows; fields a fluid receiver does not need have no row
 template <class T>
-__device__ __forceinline__ void put_field(T* Aw, int Lcap, int nq, int R, int q, int r, int f, cd v) {
-    // rows ordered (field group, slot, field, re/im, receiver): receivers
-    // contiguous, so the epilogue's threads (consecutive receivers) read
-    // consecutive rows
-    const size_t row = psvk::fld_row(nq, R, q, f) + r;
-    Aw[row * Lcap] = (T)v.re;
-    Aw[(row + (R + 1)) * Lcap] = (T)v.im;
+__device__ __forceinline__ void put_field(T* Aw, int Lcap, int nq, const PsvDev& d, int rr, int q, int f, cd v) {
+    int im;
+    const long long row = psvk::fld_row(nq, d.Rs1, d.Rf, q, f, rr, &im);
+    if (row < 0) return;
+    Aw[(size_t)row * Lcap] = (T)v.re;
+    Aw[((size_t)row + im) * Lcap] = (T)v.im;
 }
 
 template <class T>
@@ -1099,11 +1103,12 @@ __global__ void k_psv_l0_fields(PsvDev d, const cd* __restrict__ Dv, T* __restri
     if (r > R) return;
     const int n0 = d.nn0;
     const cd* D = Dv + (size_t)w * (n0 + 1) * 4;
-    const int rows0 = NS0 * (R + 1) * NFLD * 2, rows1 = NS1 * (R + 1) * NFLD * 2,
-              rows2 = NS2 * (R + 1) * NFLD * 2;
+    const size_t rows0 = psvk::fld_rows(NS0, d.Rs1, d.Rf), rows1 = psvk::fld_rows(NS1, d.Rs1, d.Rf),
+                 rows2 = psvk::fld_rows(NS2, d.Rs1, d.Rf);
     T* A0w = A0f + (size_t)w * rows0 * Lcap;
     T* A1w = A1f + (size_t)w * rows1 * Lcap;
     T* A2w = A2f + (size_t)w * rows2 * Lcap;
+    const int rr = d.rrow[r];
     for (int q = 0; q < NS0; ++q) {
         cd U = mk(0.0), Ud = mk(0.0);
         if (q < 3 || back) {
@@ -1117,14 +1122,14 @@ __global__ void k_psv_l0_fields(PsvDev d, const cd* __restrict__ Dv, T* __restri
                 U = D[4 * n0 + q];
             }
         }
-        put_field(A0w, Lcap, NS0, R, q, r, 0, U);
-        put_field(A0w, Lcap, NS0, R, q, r, 1, Ud);
-        for (int f = 2; f < NFLD; ++f) put_field(A0w, Lcap, NS0, R, q, r, f, mk(0.0));
+        put_field(A0w, Lcap, NS0, d, rr, q, 0, U);
+        put_field(A0w, Lcap, NS0, d, rr, q, 1, Ud);
+        for (int f = 2; f < NFLD; ++f) put_field(A0w, Lcap, NS0, d, rr, q, f, mk(0.0));
     }
     for (int q = 0; q < NS1; ++q)
-        for (int f = 0; f < NFLD; ++f) put_field(A1w, Lcap, NS1, R, q, r, f, mk(0.0));
+        for (int f = 0; f < NFLD; ++f) put_field(A1w, Lcap, NS1, d, rr, q, f, mk(0.0));
     for (int q = 0; q < NS2; ++q)
-        for (int f = 0; f < NFLD; ++f) put_field(A2w, Lcap, NS2, R, q, r, f, mk(0.0));
+        for (int f = 0; f < NFLD; ++f) put_field(A2w, Lcap, NS2, d, rr, q, f, mk(0.0));
 }
 
 // ------------------------------------------------------- source terms
@@ -1453,8 +1458,9 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
     int w, l;
     wl_map(wl, sys, w, l);
     if (l == 0) return;  // written by the order-0 kernels
-    const size_t rows[3] = {(size_t)NS0 * (R + 1) * NFLD * 2, (size_t)NS1 * (R + 1) * NFLD * 2,
-                            (size_t)NS2 * (R + 1) * NFLD * 2};
+    const size_t rows[3] = {psvk::fld_rows(NS0, d.Rs1, d.Rf), psvk::fld_rows(NS1, d.Rs1, d.Rf),
+                            psvk::fld_rows(NS2, d.Rs1, d.Rf)};
+    const int rr = d.rrow[r];
     T* Aw[3] = {A0f + (size_t)w * rows[0] * Lcap + l, A1f + (size_t)w * rows[1] * Lcap + l,
                      A2f + (size_t)w * rows[2] * Lcap + l};
     const double l2 = (double)l * (double)(l + 1), lsq = sqrt(l2), ilsq = FAST ? 1.0 / lsq : 0.0;
@@ -1517,11 +1523,11 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
             Vdh = Vd / lsq;
         }
         const int nqm = mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2);
-        put_field(Aw[mi], Lcap, nqm, R, q, r, 0, U);
-        put_field(Aw[mi], Lcap, nqm, R, q, r, 1, Ud);
-        put_field(Aw[mi], Lcap, nqm, R, q, r, 2, Vh);
-        put_field(Aw[mi], Lcap, nqm, R, q, r, 3, Vdh);
-        put_field(Aw[mi], Lcap, nqm, R, q, r, 4, l2 * Vh);
+        put_field(Aw[mi], Lcap, nqm, d, rr, q, 0, U);
+        put_field(Aw[mi], Lcap, nqm, d, rr, q, 1, Ud);
+        put_field(Aw[mi], Lcap, nqm, d, rr, q, 2, Vh);
+        put_field(Aw[mi], Lcap, nqm, d, rr, q, 3, Vdh);
+        put_field(Aw[mi], Lcap, nqm, d, rr, q, 4, l2 * Vh);
     }
 }
 
@@ -1620,7 +1626,7 @@ __global__ void k_psv_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ra
 class PsvEngine : public Engine {
   public:
     PsvDev d{};
-    DBuf<int> iphase, nlayer, kkdr, elem, hmoff, blkoff, amz, amc, bcrow, rcap, fluid, comp_src, jsta,
+    DBuf<int> iphase, nlayer, kkdr, elem, hmoff, blkoff, amz, amc, bcrow, rcap, fluid, rrow, comp_src, jsta,
         capmap, l0col, l0e1;
     DBuf<int2> caplist;
     DBuf<double> qmu, qkappa, sel, fel, hm, bcval, poly, lam, qkp, fr, r, rrsta;
@@ -1733,6 +1739,16 @@ class PsvEngine : public Engine {
 
         jmin_loc = jmin - d.itmp + 1;
         capmap.upload(cm, st); rcap.upload(rc, st); fluid.upload(fl, st);
+        {  // receiver rows of the field matrices: solid class (with the surface) and fluid
+            std::vector<int> rw(R + 1);
+            int ns = 0, nf = 0;
+            for (int ir = 0; ir < R; ++ir) rw[ir] = fl[ir] ? -(++nf) : ns++;
+            rw[R] = ns++;
+            d.Rs1 = ns;
+            d.Rf = nf;
+            rrow.upload(rw, st);
+            d.rrow = rrow.p;
+        }
         {  // captured rows below n - 1 in descending order, for the upward substitution
             std::vector<int2> cl;
             const int nloc = nn - d.itmp + 1;
@@ -1805,12 +1821,12 @@ class PsvEngine : public Engine {
         Lc = opt.l_chunk > 0 ? ((opt.l_chunk + 31) / 32) * 32 : 256;
         Lcap = std::min(maxlmax + 1 + Lc, 2048);
         amp_k = 1;
-        rows_m[0] = NS0 * (R + 1) * NFLD * 2;
-        rows_m[1] = NS1 * (R + 1) * NFLD * 2;
-        rows_m[2] = NS2 * (R + 1) * NFLD * 2;
-        rows_full[0] = (int)psvk::fld_rows_full(NS0, R);
-        rows_full[1] = (int)psvk::fld_rows_full(NS1, R);
-        rows_full[2] = (int)psvk::fld_rows_full(NS2, R);
+        rows_m[0] = (int)psvk::fld_rows(NS0, d.Rs1, d.Rf);
+        rows_m[1] = (int)psvk::fld_rows(NS1, d.Rs1, d.Rf);
+        rows_m[2] = (int)psvk::fld_rows(NS2, d.Rs1, d.Rf);
+        rows_full[0] = (int)psvk::fld_rows_full(NS0, d.Rs1);
+        rows_full[1] = (int)psvk::fld_rows_full(NS1, d.Rs1);
+        rows_full[2] = (int)psvk::fld_rows_full(NS2, d.Rs1);
         alloc_batch();
         build_basis(std::min(maxlmax + 1, 2048));
         DSM_CUDA(cudaStreamSynchronize(st));
@@ -1959,6 +1975,9 @@ class PsvEngine : public Engine {
         e.tlen = d.tlen;
         e.omegai = d.omegai;
         e.fluid = d.fluid;
+        e.Rs1 = d.Rs1;
+        e.Rf = d.Rf;
+        e.rrow = d.rrow;
         e.lam = d.lam;
         e.qkp = d.qkp;
         e.fr = d.fr;

@@ -67,13 +67,14 @@ template <class TC, class RL>
 struct Fields {
     const TC* C;
     size_t M;
-    int nq, R, Th, it, r, q;
+    int nq, Rs1, Rf, Th, it, rr, q;
     // complex entry of field f against basis column b (b = 1 only for the
-    // fields 0, 2, 3)
+    // fields 0, 2, 3; fluid receivers have field 0 against P only)
     __device__ __forceinline__ cx<RL> operator()(int f, int b) const {
-        const size_t row = fld_row(nq, R, q, f) + r;
+        int im;
+        const size_t row = (size_t)fld_row(nq, Rs1, Rf, q, f, rr, &im);
         const size_t col = (size_t)b * Th + it;
-        return {(RL)C[row + M * col], (RL)C[row + (R + 1) + M * col]};
+        return {(RL)C[row + M * col], (RL)C[row + im + M * col]};
     }
 };
 
@@ -93,8 +94,8 @@ __global__ void __launch_bounds__(EPI_THREADS) k_psv_epi(EpiDev d, int w, const 
     const int it = idx / R, r = idx % R;
     const bool isp = pole[it] != 0;
     const TC* Cm[3] = {C0, C1, C2};
-    const size_t Mm[3] = {(size_t)NS0 * (R + 1) * NFLD * 2, (size_t)NS1 * (R + 1) * NFLD * 2,
-                          (size_t)NS2 * (R + 1) * NFLD * 2};
+    const size_t Mm[3] = {fld_rows(NS0, d.Rs1, d.Rf), fld_rows(NS1, d.Rs1, d.Rf), fld_rows(NS2, d.Rs1, d.Rf)};
+    const int rr = d.rrow[r];
     const double x = thx[it], s = ths[it];
     const PointConst<RL> pc = point_const<RL>(x, s, d.fr[r]);
     const bool fluid = d.fluid[r] != 0;
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(EPI_THREADS) k_psv_epi(EpiDev d, int w, const 
         for (int q = 0; q < nq; ++q) {
             const Slot sl = slot_of(mi, q);
             if (sl.isback && !BACK) continue;
-            const Fields<TC, RL> G{Cm[mi], Mm[mi], nq, R, Th, it, r, q};
+            const Fields<TC, RL> G{Cm[mi], Mm[mi], nq, d.Rs1, d.Rf, Th, it, rr, q};
             const RL sigma = (sl.m < 0 && (mi & 1)) ? RL(-1) : RL(1);
             const RL mm = (RL)sl.m, m2 = mm * mm;
             C d11 = {RL(0), RL(0)}, d12 = d11, d13 = d11, d21 = d11, d22 = d11, d23 = d11, d31 = d11,
@@ -240,8 +241,8 @@ __global__ void __launch_bounds__(EPI_THREADS) k_psv_epi_surf(EpiDev d, int w, c
     if (it >= Th) return;
     const bool isp = pole[it] != 0;
     const TC* Cm[3] = {C0, C1, C2};
-    const size_t Mm[3] = {(size_t)NS0 * (R + 1) * NFLD * 2, (size_t)NS1 * (R + 1) * NFLD * 2,
-                          (size_t)NS2 * (R + 1) * NFLD * 2};
+    const size_t Mm[3] = {fld_rows(NS0, d.Rs1, d.Rf), fld_rows(NS1, d.Rs1, d.Rf), fld_rows(NS2, d.Rs1, d.Rf)};
+    const int rr = d.rrow[R];
     const RL s_inv = (RL)(1.0 / ths[it]);
     (void)thx;
     C S[10];
@@ -254,7 +255,7 @@ __global__ void __launch_bounds__(EPI_THREADS) k_psv_epi_surf(EpiDev d, int w, c
         for (int q = 0; q < nq; ++q) {
             const Slot sl = slot_of(mi, q);
             if (sl.isback) continue;  // back slots have no surface term
-            const Fields<TC, RL> G{Cm[mi], Mm[mi], nq, R, Th, it, R, q};
+            const Fields<TC, RL> G{Cm[mi], Mm[mi], nq, d.Rs1, d.Rf, Th, it, rr, q};
             const RL sigma = (sl.m < 0 && (mi & 1)) ? RL(-1) : RL(1);
             const C PU = G(0, 0);
             C u1, u2 = {RL(0), RL(0)}, u3 = {RL(0), RL(0)};

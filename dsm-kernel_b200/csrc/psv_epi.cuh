@@ -9,28 +9,44 @@ namespace psvk {
 constexpr int NS0 = 4, NS1 = 8, NS2 = 6;  // slots per |m|
 constexpr int NFLD = 5;                   // U, U', V/lsq, V'/lsq, l(l+1) V/lsq
 
-// Row layout of the per-order field matrix of one |m| (nq slots, R + 1
-// receiver rows r): fields 0, 2, 3 (U, V/lsq, V'/lsq), which the epilogue
-// contracts with both basis columns (P and dP/dtheta), come first; fields 1
-// and 4 (U', l(l+1) V/lsq), needed against P only, follow, so the l-sum of
-// the second group runs over half the columns.  Row of the real part of
-// (q, f) at r = 0; the imaginary part is R + 1 rows further.
-__host__ __device__ __forceinline__ size_t fld_rows_full(int nq, int R) { return (size_t)nq * 3 * 2 * (R + 1); }
-__host__ __device__ __forceinline__ size_t fld_row(int nq, int R, int q, int f) {
-    if (f == 1 || f == 4) return fld_rows_full(nq, R) + ((size_t)(q * 2 + (f == 4)) * 2) * (R + 1);
-    return ((size_t)(q * 3 + (f == 0 ? 0 : f - 1)) * 2) * (R + 1);
+// Row layout of the per-order field matrix of one |m| (nq slots).  The
+// receiver rows are split into the solid class (solid receivers and the
+// surface row, Rs1 of them, index rr >= 0) and fluid receivers (Rf, index
+// -rr - 1): a fluid receiver's strain needs only U against P.
+//   group A (contracted with both basis columns P and dP/dtheta): fields
+//     U, V/lsq, V'/lsq of the solid class, rows ((q*3 + fa)*2 + re/im)*Rs1 + rr;
+//   group B (against P only): fields U', l(l+1)V/lsq of the solid class,
+//     then U of the fluid receivers, rows (q*2 + re/im)*Rf + fluid index.
+// Row of the real part of (q, f) for receiver class index rr, or -1 when the
+// receiver has no row for f; *im is the offset of the imaginary part.
+__host__ __device__ __forceinline__ size_t fld_rows_full(int nq, int Rs1) { return (size_t)nq * 6 * Rs1; }
+__host__ __device__ __forceinline__ size_t fld_rows(int nq, int Rs1, int Rf) {
+    return (size_t)nq * (10 * (size_t)Rs1 + 2 * (size_t)Rf);
+}
+__host__ __device__ __forceinline__ long long fld_row(int nq, int Rs1, int Rf, int q, int f, int rr, int* im) {
+    if (rr >= 0) {
+        *im = Rs1;
+        if (f == 1 || f == 4)
+            return (long long)fld_rows_full(nq, Rs1) + ((long long)(q * 2 + (f == 4)) * 2) * Rs1 + rr;
+        return ((long long)(q * 3 + (f == 0 ? 0 : f - 1)) * 2) * Rs1 + rr;
+    }
+    *im = Rf;
+    if (f != 0) return -1;
+    return (long long)nq * 10 * Rs1 + (long long)(q * 2) * Rf + (-rr - 1);
 }
 
 // receiver data the epilogue reads
 struct EpiDev {
     int R, Th;
+    int Rs1, Rf;                   // receiver rows of the solid class and fluid receivers
     double tlen, omegai;
     const int* fluid;              // [R]
+    const int* rrow;               // [R+1] class index of each receiver row (fld_row)
     const double *lam, *qkp, *fr;  // [R]  lambda, Qkappa, float(r)
 };
 
-// Contraction outputs C0..C2 (one per |m|, column-major, rows
-// ((q*NFLD+f)*2+{re,im})*(R+1)+r, columns b*Th+it) are FP64 when tc is
+// Contraction outputs C0..C2 (one per |m|, column-major, rows as fld_row,
+// columns b*Th+it) are FP64 when tc is
 // false and FP32 (tensor-core path, FP32 arithmetic) when it is true.
 // Writes tsgt[w][Th][R][20], rsgt[w][Th][R][10] (when rsgt) and
 // synn[w][Th][10] (when synn) as complex128.
