@@ -1476,6 +1476,25 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
         double a1 = cabs_(p0), a2 = cabs_(p1);
         amps[(size_t)w * Lcap + l] = sqrt(a1 * a1 + a2 * a2);
     }
+    if (rr < 0) {  // fluid receiver: only U is stored
+        cd bU[NB];
+        for (int b = 0; b < NB; ++b) bU[b] = mk(0.0);
+        for (int i = 0; i < 3; ++i) {
+            const double wvi = d.wv[3 * r + i];
+            const int cu = d.rcap[6 * r + 2 * i];
+            for (int b = 0; b < NB; ++b) bU[b] = caddmulR<FAST>(bU[b], wvi, X(cu, b));
+        }
+        for (int s = 0; s < NSLOT; ++s) {
+            const int mi = slot_mi(s), q = slot_q(s);
+            cd U = mk(0.0);
+            for (int b = 0; b < NB; ++b) {
+                if (FAST) U = caddmulT<true>(U, C(s, b), bU[b]);
+                else U = U + C(s, b) * bU[b];
+            }
+            put_field(Aw[mi], Lcap, mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2), d, rr, q, 0, U);
+        }
+        return;
+    }
     const bool surf = r == R;
     cd bU[NB], bV[NB], bUd[NB], bVd[NB];
     for (int b = 0; b < NB; ++b) bU[b] = bV[b] = bUd[b] = bVd[b] = mk(0.0);
