@@ -79,3 +79,12 @@ def test_records_match_outputs_when_copied_in_groups(prec):
     assert np.array_equal(t32, np.transpose(t, (0, 2, 1, 3)).astype(np.complex64))
     assert np.array_equal(r32, np.transpose(r, (0, 2, 1, 3)).astype(np.complex64))
     assert np.array_equal(y32, y.astype(np.complex64))
+
+
+@pytest.mark.gpu
+def test_psv_mixed_receivers_all_solid():
+    # no fluid receiver rows: the second row group holds only U' and l(l+1)V/lsq
+    s = dsmsgt.Setup(psv_small(seed=1, rmin=3800.0, rdelta=400.0), "psv")
+    errs = _mixed_vs_fp64(s, [3, 17, 29], dsmsgt.DSM_PREC_MIXED)
+    for k, v in errs.items():
+        assert max(v) <= TOL_F16, (k, v)

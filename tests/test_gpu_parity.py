@@ -83,3 +83,11 @@ def test_psv_fp64_order_capacity_growth(built):
     order capacity several times and still match the oracle."""
     s = dsmsgt.Setup(psv_small(imax=16, thdelta=45.0), "psv")
     _compare(s, [6], {"l_chunk": 1024, "freq_batch": 1})
+
+
+@pytest.mark.gpu
+def test_psv_fp64_receivers_all_solid(built):
+    """Receivers in the mantle only (no fluid receiver rows in the field
+    matrices) must match the oracle as well."""
+    s = dsmsgt.Setup(psv_small(seed=1, rmin=3800.0, rdelta=400.0), "psv")
+    _compare(s, [3, 29])
