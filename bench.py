@@ -206,6 +206,197 @@ def cpu_baseline(setup_mode: str, freqs: list[int], threads: int, slope: float |
     return value, times, slope
 
 
+CAT_METRIC = "catalogue points/s (6 windowed time series per point from 30 SGT components)"
+CAT_UNIT = "points/s"
+# one receiver radius of the mixed-precision catalogue (imax 2048, 1441
+# distances at 0.125 deg) read the way KernelMaker reads it for a kernel grid
+CAT_WORKLOAD = dict(name="catalogue", tlen=3276.8, fmin=0, fmax=2048, theta_n=1441, theta_delta=0.125,
+                    sampling_hz=2.0, window_s=[400.0, 1000.0], ipdistance=10.0, c_red_reci=0.0,
+                    points=1681, distances_deg=[30.0, 90.0], outputs=6,
+                    record_sets="P-SV TSGT (20 components) + SH TSGT (10, into 7 and 12-20), complex64")
+
+
+def catalogue_params():
+    import dsmsgt
+    w = CAT_WORKLOAD
+    np1, shz, s0, s1 = dsmsgt.cat_np1(w["tlen"], w["fmax"], w["sampling_hz"], *w["window_s"])
+    return dict(num=20, theta_n=w["theta_n"], theta_min=0.0, theta_delta=w["theta_delta"], fmin=w["fmin"],
+                fmax=w["fmax"], np1=np1, tlen=w["tlen"], omegai=float(np.log(100.0) / w["tlen"]),
+                ipdistance=w["ipdistance"], c_red_reci=w["c_red_reci"], iwin_start=s0, iwin_end=s1)
+
+
+def catalogue_inputs(seed: int):
+    """Seeded points (sorted distances) and per-point combination matrices."""
+    rng = np.random.default_rng(seed)
+    w = CAT_WORKLOAD
+    dist = np.sort(rng.uniform(*w["distances_deg"], w["points"]))
+    coef = rng.standard_normal((w["points"], w["outputs"], 20))
+    return dist, coef
+
+
+def catalogue_cpu(p, recs_host, dist, coef, npts: int):
+    """The oracle (numpy FP64, one thread) on one radius: rdsgtomega over the
+    full records once, then clsgt + combination + transform per point on a
+    sample of points; scaled to the workload's points."""
+    from oracle import catalogue as cat
+    t0 = time.perf_counter()
+    theta = p["theta_min"] + np.arange(p["theta_n"]) * p["theta_delta"]
+    sets = [(recs_host[0], np.arange(20), np.ones(20)),
+            (recs_host[1], cat.kind_dst(cat.TSGT_SH, 10), np.ones(10))]
+    om = cat.omega_sgt(sets, 20, p["fmin"], p["fmax"], theta, p["tlen"], p["c_red_reci"])
+    t_omega = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for k in range(npts):
+        f = cat.clsgt(float(dist[k]), om, p["fmin"], p["theta_min"], p["theta_delta"], p["ipdistance"],
+                      p["tlen"], p["c_red_reci"])
+        cat.vector_fft_double(coef[k] @ f.T, p["fmin"], p["fmax"], p["np1"], p["omegai"], p["tlen"],
+                              p["iwin_start"], p["iwin_end"])
+    t_pt = (time.perf_counter() - t0) / npts
+    t_step = t_omega + t_pt * len(dist)
+    return len(dist) / t_step, {"rdsgtomega_s": t_omega, "per_point_s": t_pt}
+
+
+def catalogue_bench(args):
+    """Catalogue consumer: one step = one receiver radius (two record sets
+    registered, series at every point)."""
+    w = CAT_WORKLOAD
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    nf, nt = w["fmax"] - w["fmin"] + 1, w["theta_n"]
+
+    def host_records(seed):
+        rng = np.random.default_rng(seed)
+        out = []
+        for nc in (20, 10):
+            a = np.empty((nf, nt, nc), np.complex64)
+            a.real = rng.standard_normal((nf, nt, nc), dtype=np.float32)
+            a.imag = rng.standard_normal((nf, nt, nc), dtype=np.float32)
+            out.append(a)
+        return out
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        p = catalogue_params()
+        dist, coef = catalogue_inputs(0)
+        recs = host_records(1)
+        for _ in range(args.warmup):
+            catalogue_cpu(p, recs, dist, coef, 1)
+        tot, samples = 0.0, []
+        for _ in range(args.steps):
+            v, t = catalogue_cpu(p, recs, dist, coef, 8)
+            tot += len(dist) / v
+            samples.append(t)
+        value = args.steps * len(dist) / tot
+        cpu = {"value": value, "unit": CAT_UNIT, "cores": 1, "kind": "port",
+               "sample": "rdsgtomega over the full records once per step, clsgt + combination + "
+                         "transform on 8 points per step scaled to 1681 points"}
+        print(json.dumps({"impl": "reference", "metric": CAT_METRIC, "value": value, "unit": CAT_UNIT,
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": {"workload": "catalogue", **w}, "cpu_baseline": cpu,
+                          "e2e": {"value": value, "unit": CAT_UNIT, "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    import dsmsgt
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    p = catalogue_params()
+    dist, coef = catalogue_inputs(rank)
+    # two radii, alternating; host copies in pinned memory (the e2e leg copies them in every step)
+    pinned = [[torch.from_numpy(a).pin_memory() for a in host_records(10 * rank + k)] for k in range(2)]
+    hrec = [[t_.numpy() for t_ in r] for r in pinned]
+    drec = [[t_.to(f"cuda:{dev}") for t_ in r] for r in pinned]
+    dst_sh = np.array([6] + list(range(11, 20)), np.int32)
+    c = dsmsgt.Catalogue(p, device=dev)
+    nwin = p["iwin_end"] - p["iwin_start"] + 1
+    out = torch.empty((len(dist), w["outputs"], nwin), dtype=torch.float64, device=f"cuda:{dev}")
+
+    def step(k, host):
+        c.clear()
+        r = hrec[k % 2] if host else drec[k % 2]
+        c.add(r[0])
+        c.add(r[1], dst_sh)
+        return c.series(dist, coef) if host else c.series(dist, coef, out=out)
+
+    for k in range(args.warmup):
+        step(k, False)
+    c.set_profiling(True)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    torch.cuda.synchronize()
+    ms, launches, kst = 0.0, 0, {}
+    for k in range(args.steps):
+        step(k, False)
+        st = c.stats()
+        ms += st.ms_total
+        launches += st.launches
+        for name, (t, n, b, f) in st.kernels().items():
+            a = kst.setdefault(name, [0.0, 0, 0.0, 0.0])
+            a[0] += t; a[1] += n; a[2] += b; a[3] += f
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    # end to end: host records (pageable numpy) copied in, series copied out
+    for k in range(2):
+        step(k, True)
+    t_e2e = 0.0
+    for k in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step(k, True)
+        t_e2e += time.perf_counter() - t0
+    c.close()
+    t = ms / 1e3
+    peaks = {}
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except Exception:
+        pass
+    fp64 = max(dsmsgt.fp64_peak(dev), dsmsgt.fp64_peak(dev, mma=True))
+    rooflines = {}
+    for name, (tk, nk, bk, fk) in kst.items():
+        if fk > 0:
+            ach = fk / (tk / 1e3) / 1e12
+            rooflines[name] = {"kernel": name, "bound": "fp64", "achieved": ach, "peak": fp64,
+                               "unit": "TFLOP/s (algorithmic)", "frac": ach / fp64, "traffic": None,
+                               "peak_source": "measured (FP64 FMA and tensor-core probes, this run; the larger)",
+                               "avg_launch_ms": tk / max(nk, 1)}
+        else:
+            ach = bk / (tk / 1e3) / 1e9
+            peak = peaks.get("hbm_gbs", 6650.0)
+            rooflines[name] = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                               "frac": ach / peak, "traffic": None,
+                               "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                               "avg_launch_ms": tk / max(nk, 1)}
+    roof = rooflines[max(kst.items(), key=lambda kv: kv[1][0])[0]]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, tt = catalogue_cpu(p, hrec[0], dist, coef, 8)
+        cpu = {"value": v, "unit": CAT_UNIT, "cores": 1, "kind": "port",
+               "sample": "oracle: rdsgtomega over the full records once, clsgt + combination + transform "
+                         f"on 8 points scaled to {len(dist)} points; measured: {json.dumps(tt)}"}
+    if rank == 0:
+        rec_bytes = sum(a.nbytes for a in hrec[0])
+        print(json.dumps({
+            "metric": CAT_METRIC, "value": args.steps * len(dist) * world / t, "unit": CAT_UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded complex64 records, seeded distances and combination matrices)",
+            "config": {"workload": "catalogue", **w, "np1": p["np1"], "window_samples": nwin,
+                       "l2": "inputs larger than L2 (708 MB of records per step, two radii alternating)"},
+            "e2e": {"value": args.steps * len(dist) / t_e2e, "unit": CAT_UNIT,
+                    "h2d_bytes_per_step": int(rec_bytes + dist.nbytes + coef.nbytes),
+                    "d2h_bytes_per_step": int(len(dist) * w["outputs"] * nwin * 8)},
+            "gpu_launches": int(launches), "roofline": roof, "stage_rooflines": rooflines,
+            "kernel_share": {k: round(v[0] / max(ms, 1e-9), 4) for k, v in kst.items()},
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kst.items()},
+            "cpu_baseline": cpu, "clocks": clk}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -213,13 +404,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", "--mode", dest="mode", default="psv1024",
-                    choices=["psv1024", "psv2048", "sh256", "psv", "sh"])
+                    choices=["psv1024", "psv2048", "sh256", "psv", "sh", "catalogue"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_bf16"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-lmax", dest="lmax", action="store_false", help="plain first order ranges")
     ap.add_argument("--per-step", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.mode == "catalogue":
+        catalogue_bench(args)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -1,0 +1,920 @@
+// Catalogue consumer: SGT records of one receiver radius (frequency indices
+// fmin..fmax, all catalogue distances) -> windowed time series at arbitrary
+// epicentral distances, on the device.
+//
+// Restates KernelMaker's
+//   rdsgtomega        src/KernelMaker/fourier.f90:1-123   (scale, 1e-21, reduction phase)
+//   clsgt             src/KernelMaker/fourier.f90:128-162 (normalised sinc in distance)
+//   findIdeltaRegion  src/KernelMaker/fourier.f90:165-190
+//   vectorFFT_double  src/KernelMaker/fourier.f90:418-450 (Hermitian extension,
+//                     length-2 np1 inverse transform, exp(omegai t) / tlen * 1e3)
+//
+// The sinc interpolation is a banded product: for every frequency n,
+// sgtF[p][d] = sum_kk W[p][kk] omega[n][kk][d] with W nonzero on a window of
+// 2 nhregion + 1 catalogue distances around each point.  Points are sorted by
+// distance and grouped in tiles of up to 32 whose windows overlap; a tile's
+// union of windows is its band of catalogue distances.
+//
+// Device plan, per call:
+//   k_cat_omega   rdsgtomega over the catalogue distances some window covers:
+//                 records (complex64/128) widened, times scale, reduction
+//                 phase and 1e-21, record sets summed, as the reference's
+//                 frequency-domain SGT [n][distance][component] in FP64.
+// and per batch of sorted points:
+//   k_cat_interp  one 4-warp CTA per (point tile, 4 frequencies), one warp per
+//                 frequency, four CTAs per SM.  The band is walked in chunks
+//                 of 16 distances, double-buffered in shared memory by
+//                 cp.async (the chunk's SGT rows of the 4 frequencies and the
+//                 tile's dense weights, zero outside each point's window),
+//                 and multiplied on the FP64 tensor cores (mma.m16n8k4.f64:
+//                 32 points x all components per warp, accumulated in
+//                 registers).  Epilogue: divide by the weight sum, clsgt
+//                 phase, the per-point component combination, and the
+//                 Hermitian projection H_n = (x_n + conj(x_{N-n})) / 2
+//                 (n = 0..np1) of the reference's extended vector x:
+//                 Re(IDFT(x)) = IDFT(H), so a real-output transform gives the
+//                 reference's Re(cvec).
+//   cuFFT Z2D     in place, length N = 2 np1, batch = points x outputs.
+//   k_cat_window  samples iwin_start..iwin_end, times exp(omegai t / sHz) /
+//                 tlen * 1e3, written in the caller's point order.
+//
+// Compiled without fused multiply-add so the rdsgtomega and normalisation
+// arithmetic rounds like the Fortran; the weighted sums (tensor-core
+// products) and the component combination round once per term.
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <numeric>
+
+#include "common.cuh"
+
+namespace dsm {
+namespace cat {
+
+constexpr int PT = 32;          // points per tile: 8 lane groups x 4 points
+constexpr int KC = 16;          // catalogue distances per staged chunk (a multiple of 4)
+constexpr int CAT_WARPS = 4;
+constexpr int CAT_THREADS = 32 * CAT_WARPS;
+constexpr int MAX_SETS = 4;
+constexpr int MAX_NUM = 32;     // components of the frequency-domain SGT
+constexpr int MAX_OUT = 64;     // outputs per point
+constexpr int MAX_NW = 256;     // catalogue distances in one sinc window
+
+struct SetDev {
+    const void* rec;   // [nf][theta_n][ncomp]
+    int cplx64;        // 1: complex64 records, 0: complex128
+    int ncomp;
+    int src[MAX_NUM];  // record component feeding destination d, or -1
+    double scale[MAX_NUM];  // factor of that record component
+};
+
+struct Tile {
+    int p0, np;        // sorted positions [p0, p0 + np) of the batch
+    int u0, U;         // band: rows [u0, u0 + U) of the frequency-domain SGT
+    long long woff;    // offset of the tile's dense weights [U][WS] in wt
+};
+
+struct InterpArgs {
+    int num, nout, identity;
+    int fmin, fmax, np1, ucov;   // ucov: rows of om per frequency
+    double tlen, c_red_reci;
+    const Tile* tiles;
+    const cd* om;          // [nf][ucov][nump] frequency-domain SGT (k_cat_omega)
+    const double* wt;      // dense tile weights (zero outside each point's window)
+    // per sorted position of the batch
+    const double* norm;    // sum of the weights
+    const double* dist;    // distance (deg)
+    const int* orig;       // the caller's index of the point
+    const double* coef;    // [caller point][nout][num] or null (identity)
+    cd* h;                 // [sorted position][nout][np1+1]
+};
+
+__device__ __forceinline__ cd load_rec(const SetDev& s, size_t idx) {
+    if (s.cplx64) {
+        float2 v = __ldg(reinterpret_cast<const float2*>(s.rec) + idx);
+        return cd{(double)v.x, (double)v.y};
+    }
+    const double2 v = __ldg(reinterpret_cast<const double2*>(s.rec) + idx);
+    return cd{v.x, v.y};
+}
+
+// exp(i arg) as Fortran's exp(cmplx(0, arg))
+__device__ __forceinline__ cd expi(double arg) {
+    double sn, cs;
+    sincos(arg, &sn, &cs);
+    return cd{cs, sn};
+}
+
+// rdsgtomega (fourier.f90:87-116) on catalogue distances [u0, u0 + Ucov):
+// om[n - fmin][u - u0][d] = sum over record sets of ((rec * scale) * phase) * 1e-21,
+// components padded to nump with zeros; index 0 is never read (zero)
+struct OmegaArgs {
+    SetDev set[MAX_SETS];
+    int nset, num, nump, theta_n, fmin, nf, u0, ucov, urows;   // rows >= ucov are zero
+    double theta_min, theta_delta, tlen, c_red_reci;
+    cd* om;   // [nf][urows][nump]
+};
+
+// grid (ceil(urows * nump / 256), nf): one thread per (distance, component).
+// The per-component set tables are copied to shared memory first: threads of
+// a warp index them by different components, which kernel-parameter memory
+// would serve one address at a time.
+__global__ void __launch_bounds__(256) k_cat_omega(const OmegaArgs a) {
+    __shared__ int src_s[MAX_SETS][MAX_NUM];
+    __shared__ double scale_s[MAX_SETS][MAX_NUM];
+    for (int i = threadIdx.x; i < MAX_SETS * MAX_NUM; i += blockDim.x) {
+        const int s = i / MAX_NUM, d = i % MAX_NUM;
+        src_s[s][d] = s < a.nset ? a.set[s].src[d] : -1;
+        scale_s[s][d] = s < a.nset ? a.set[s].scale[d] : 0.0;
+    }
+    __syncthreads();
+    const int k = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= a.urows * a.nump) return;
+    const int d = j % a.nump, u = j / a.nump;
+    const int n = a.fmin + k;
+    cd om = mk(0.0);
+    if (d < a.num && n != 0 && u < a.ucov) {
+        const size_t base = (size_t)k * a.theta_n + (a.u0 + u);
+        cd ph = mk(1.0);
+        const bool reduce = a.c_red_reci != 0.0;
+        if (reduce) {
+            const double th = a.theta_min + (double)(a.u0 + u) * a.theta_delta;
+            const double redtime = -th * a.c_red_reci;
+            ph = expi(-(2.0 * kPi * (double)n / a.tlen * redtime));
+        }
+        for (int s = 0; s < a.nset; ++s) {
+            const SetDev& S = a.set[s];
+            const int c = src_s[s][d];
+            if (c < 0) continue;
+            cd t = load_rec(S, base * S.ncomp + c) * scale_s[s][c];
+            if (reduce) t = t * ph;
+            t = t * 1.0e-21;
+            om = om + t;   // the first set adds to an exact zero
+        }
+    }
+    a.om[((size_t)k * a.urows + u) * a.nump + d] = om;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// k_cat_interp<C>: the band product on the FP64 tensor cores.  Per
+// frequency it is D[point][column] += W[point][distance] * B[distance][column]
+// with the real columns (re, im of each of 4C components); one
+// mma.m16n8k4.f64 takes 16 points x 4 distances of W and 4 distances x 8
+// columns of B.  A warp owns one frequency of the CTA: all PT = 32 points
+// (two m16 tiles) x 8C real columns (C n8 tiles), 2C accumulator tiles.
+//
+// Fragments of mma.m16n8k4 .f64 (g = lane / 4, t = lane % 4):
+//   A 16x4: a0 = A[g][t], a1 = A[g + 8][t];   B 4x8: b0 = B[t][g];
+//   C 16x8: c0, c1 = C[g][2t], C[g][2t + 1];  c2, c3 = same in row g + 8.
+// Shared-memory rows are padded so the 16 lanes of a half-warp hit distinct
+// banks: weights [KC][WS] with WS = 36, SGT rows of SS = 8C + 4 doubles
+// (2 SS mod 32 is 8 or 24, and 2 WS mod 32 is 8).
+constexpr int WS = 36;
+__host__ __device__ constexpr int sgt_stride(int C) { return 8 * C + 4; }
+
+// shared memory of k_cat_interp (bytes): two staged chunks [CAT_WARPS][KC][SS]
+// doubles, reused by the epilogue as [CAT_WARPS][PT * 4C + 1] cd, and two
+// weight chunks [KC][WS] doubles
+__host__ __device__ inline size_t interp_smem_bytes(int C) {
+    const size_t om = (size_t)2 * CAT_WARPS * KC * sgt_stride(C) * sizeof(double);
+    const size_t ep = (size_t)CAT_WARPS * (PT * 4 * C + 1) * sizeof(cd);
+    return (om > ep ? om : ep) + (size_t)2 * KC * WS * sizeof(double);
+}
+
+__device__ __forceinline__ void mma_f64_16x8x4(double (&d)[4], double a0, double a1, double b0) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, "
+        "{%0, %1, %2, %3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
+
+template <int C>
+__global__ void __launch_bounds__(CAT_THREADS, C <= 5 ? 4 : 2) k_cat_interp(const InterpArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int NUMP = 4 * C, SS = sgt_stride(C);
+    constexpr size_t OM_D = (size_t)2 * CAT_WARPS * KC * SS, EP_D = (size_t)CAT_WARPS * (PT * NUMP + 1) * 2;
+    double* Om = reinterpret_cast<double*>(smem);                            // [2][CAT_WARPS][KC][SS]
+    double* Wc = Om + (OM_D > EP_D ? OM_D : EP_D);                            // [2][KC][WS]
+    const Tile tl = a.tiles[blockIdx.x];
+    const int n0 = blockIdx.y * CAT_WARPS;
+    const int nh = a.np1 + 1;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const bool reduce = a.c_red_reci != 0.0;
+    const int nlo = max(n0, max(a.fmin, 1)), nhi = min(n0 + CAT_WARPS - 1, a.fmax);
+    const bool any = nlo <= nhi;
+    const int n = n0 + warp;
+    const bool mine = n >= nlo && n <= nhi;
+    const int nchunk = (tl.U + KC - 1) / KC;   // U is a multiple of 4
+
+    // chunk k: the SGT rows of distances u0 + k KC .. of the CTA's
+    // frequencies and the tile's weights of those distances
+    auto issue = [&](int k) {
+        const int buf = k & 1, k0 = k * KC, kc = min(KC, tl.U - k0);
+        double* ob = Om + (size_t)buf * CAT_WARPS * KC * SS;
+        for (int i = tid; i < CAT_WARPS * KC * NUMP; i += CAT_THREADS) {
+            const int nl = i / (KC * NUMP), e = i % (KC * NUMP);
+            const int kk = e / NUMP, d = e % NUMP;
+            const int nn = n0 + nl;
+            if (kk >= kc || nn < nlo || nn > nhi) continue;
+            cp_async16(ob + ((size_t)nl * KC + kk) * SS + 2 * d,
+                       a.om + ((size_t)(nn - a.fmin) * a.ucov + tl.u0 + k0 + kk) * NUMP + d);
+        }
+        double* wb = Wc + buf * KC * WS;
+        const double* wsrc = a.wt + (size_t)tl.woff + (size_t)k0 * WS;
+        for (int i = tid; i < kc * WS / 2; i += CAT_THREADS) cp_async16(wb + 2 * i, wsrc + 2 * i);
+        cp_async_commit();
+    };
+
+    double acc[2][C][4];
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+        for (int q = 0; q < C; ++q)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[m][q][e] = 0.0;
+
+    if (any) {
+        issue(0);
+        for (int k = 0; k < nchunk; ++k) {
+            if (k + 1 < nchunk) {
+                issue(k + 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            if (mine) {
+                const int kc = min(KC, tl.U - k * KC);
+                const double* orow = Om + ((size_t)(k & 1) * CAT_WARPS + warp) * KC * SS + t * SS + g;
+                const double* wrow = Wc + (k & 1) * KC * WS + t * WS + g;
+                for (int k4 = 0; k4 < kc; k4 += 4) {
+                    const double a00 = wrow[k4 * WS], a01 = wrow[k4 * WS + 8];
+                    const double a10 = wrow[k4 * WS + 16], a11 = wrow[k4 * WS + 24];
+#pragma unroll
+                    for (int q = 0; q < C; ++q) {
+                        const double b = orow[k4 * SS + 8 * q];
+                        mma_f64_16x8x4(acc[0][q], a00, a01, b);
+                        mma_f64_16x8x4(acc[1][q], a10, a11, b);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // epilogue 1: normalise, clsgt phase; stage [CAT_WARPS][PT * NUMP + 1] cd
+        cd* E = reinterpret_cast<cd*>(smem);
+        const int es = PT * NUMP + 1;
+        if (mine) {
+#pragma unroll
+            for (int m = 0; m < 2; ++m)
+#pragma unroll
+                for (int hr = 0; hr < 2; ++hr) {
+                    const int pl = m * 16 + g + 8 * hr;
+                    if (pl >= tl.np) continue;
+                    const int ps = tl.p0 + pl;
+                    const double nrm = a.norm[ps];
+                    cd phs = mk(1.0);
+                    if (reduce) phs = expi(-(2.0 * kPi) * (double)n / a.tlen * a.dist[ps] * a.c_red_reci);
+#pragma unroll
+                    for (int q = 0; q < C; ++q) {
+                        cd v = cd{acc[m][q][2 * hr], acc[m][q][2 * hr + 1]} / nrm;
+                        if (reduce) v = v * phs;
+                        E[(size_t)warp * es + pl * NUMP + 4 * q + t] = v;
+                    }
+                }
+        }
+        __syncthreads();
+    }
+    // epilogue 2: combine, Hermitian projection, store CAT_WARPS consecutive n per row
+    const cd* E = reinterpret_cast<const cd*>(smem);
+    const int es = PT * NUMP + 1;
+    for (int i = tid; i < tl.np * a.nout * CAT_WARPS; i += CAT_THREADS) {
+        const int nl = i % CAT_WARPS, rest = i / CAT_WARPS;
+        const int j = rest % a.nout, pl = rest / a.nout;
+        const int nn = n0 + nl;
+        if (nn >= nh) continue;
+        cd v = mk(0.0);
+        if (any && nn >= nlo && nn <= nhi) {
+            const cd* e = E + (size_t)nl * es + pl * NUMP;
+            if (a.identity) {
+                v = e[j];
+            } else {
+                const double* m = a.coef + ((size_t)a.orig[tl.p0 + pl] * a.nout + j) * a.num;
+                for (int d = 0; d < a.num; ++d) {
+                    v.re = fma(m[d], e[d].re, v.re);
+                    v.im = fma(m[d], e[d].im, v.im);
+                }
+            }
+        }
+        cd hv;
+        if (nn == 0 || nn == a.np1) hv = cd{v.re, 0.0};
+        else if (nn <= a.np1 - a.fmin) hv = v;
+        else hv = v * 0.5;
+        a.h[((size_t)(tl.p0 + pl) * a.nout + j) * nh + nn] = hv;
+    }
+}
+
+// out[orig point][j][t] = y[row][iws + t] * e[t] / tlen * 1e3; rows of y (sorted
+// position x nout + j) are 2 (np1+1) reals apart
+__global__ void k_cat_window(const double* __restrict__ y, int row, int iws, int nwin, int nb, int nout,
+                             const int* __restrict__ orig, const double* __restrict__ e, double tlen,
+                             double* __restrict__ out) {
+    const size_t total = (size_t)nb * nwin;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t b = i / nwin;
+        const int t = (int)(i - b * nwin);
+        const int ps = (int)(b / nout), j = (int)(b - (size_t)ps * nout);
+        out[((size_t)orig[ps] * nout + j) * nwin + t] = y[b * row + iws + t] * e[t] / tlen * 1.0e3;
+    }
+}
+
+}  // namespace cat
+
+#define DSM_CUFFT(x)                                                                        \
+    do {                                                                                    \
+        cufftResult r_ = (x);                                                               \
+        if (r_ != CUFFT_SUCCESS)                                                            \
+            throw ::dsm::Error(DSM_ERR_CUDA, std::string(#x ": cufft status ") + std::to_string((int)r_)); \
+    } while (0)
+
+}  // namespace dsm
+
+using namespace dsm;
+using namespace dsm::cat;
+
+struct dsm_cat {
+    dsm_cat_params_t p{};
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    std::string err;
+    std::vector<SetDev> sets;
+    DBuf<unsigned char> own[MAX_SETS];   // device copies of host record sets, kept across clears
+    DBuf<int> orig;
+    DBuf<Tile> tiles;
+    DBuf<double> wt, norm, dist, coef, e, out;
+    DBuf<cd> om;     // frequency-domain SGT of the covered catalogue distances
+    DBuf<cd> h;
+    std::vector<double> he;
+    std::map<int, cufftHandle> plans;   // batch -> plan
+    size_t max_batch_bytes = (size_t)2 << 30;
+    bool profiling = false;
+    dsm_stats_t stats{};
+    cudaEvent_t ev[8]{};
+
+    ~dsm_cat() {
+        if (dev >= 0) cudaSetDevice(dev);
+        for (auto& kv : plans) cufftDestroy(kv.second);
+        for (auto& x : ev)
+            if (x) cudaEventDestroy(x);
+        if (st) cudaStreamDestroy(st);
+    }
+    int nwin() const { return p.iwin_end - p.iwin_start + 1; }
+    cufftHandle plan(int batch) {
+        auto it = plans.find(batch);
+        if (it != plans.end()) return it->second;
+        if (plans.size() >= 8) {
+            DSM_CUDA(cudaStreamSynchronize(st));
+            for (auto& kv : plans) cufftDestroy(kv.second);
+            plans.clear();
+        }
+        cufftHandle h0;
+        int N = 2 * p.np1, inembed = p.np1 + 1, onembed = 2 * (p.np1 + 1);
+        DSM_CUFFT(cufftPlanMany(&h0, 1, &N, &inembed, 1, p.np1 + 1, &onembed, 1, 2 * (p.np1 + 1), CUFFT_Z2D, batch));
+        DSM_CUFFT(cufftSetStream(h0, st));
+        plans[batch] = h0;
+        return h0;
+    }
+};
+
+namespace {
+thread_local std::string g_cat_err;
+
+template <class F>
+int cat_guard(dsm_cat_t* c, F f) {
+    try {
+        f();
+        return DSM_OK;
+    } catch (const Error& e) {
+        (c ? c->err : g_cat_err) = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        (c ? c->err : g_cat_err) = e.what();
+        return DSM_ERR_INVALID;
+    }
+}
+
+void need(bool ok, const std::string& m) {
+    if (!ok) throw Error(DSM_ERR_INVALID, m);
+}
+
+// findIdeltaRegion (fourier.f90:165-190), 1-based
+void idelta_region(int ix, int nhalf, int nmax, int& is, int& ie) {
+    is = ix - nhalf;
+    ie = ix + nhalf;
+    if (is < 1) {
+        ie += 1 - is;
+        is = 1;
+    }
+    if (ie > nmax) {
+        is -= ie - nmax;
+        ie = nmax;
+    }
+    if (is < 1) is = 1;
+    if (ie > nmax) ie = nmax;
+}
+}  // namespace
+
+extern "C" int dsm_cat_np1(double tlen, int fmax, double sampling_hz, double start, double end, int* np1,
+                           double* sampling_hz_out, int* iwin_start, int* iwin_end) {
+    return cat_guard(nullptr, [&] {
+        need(tlen > 0 && fmax >= 0 && sampling_hz > 0 && np1, "dsm_cat_np1: bad argument");
+        // lsmoothfinder (others.f90:288-308) and KernelMaker-1.0.0.f90:311-330
+        long long np_ = 1;
+        while (np_ < fmax) np_ *= 2;
+        int lsmooth = (int)(0.5 * tlen * sampling_hz / (double)np_);
+        int i = 1;
+        while (i < lsmooth) i *= 2;
+        lsmooth = i;
+        long long n1 = 1;
+        while (n1 < fmax) n1 *= 2;
+        n1 *= lsmooth;
+        need(n1 <= (1 << 26), "dsm_cat_np1: transform length too large");
+        *np1 = (int)n1;
+        const double shz = (double)(2 * n1) / tlen;
+        if (sampling_hz_out) *sampling_hz_out = shz;
+        if (iwin_start) *iwin_start = (int)(start * shz);
+        if (iwin_end) *iwin_end = (int)(end * shz);
+    });
+}
+
+extern "C" int dsm_cat_create(const dsm_cat_params_t* p, dsm_cat_t** out) {
+    if (!out) return DSM_ERR_INVALID;
+    *out = nullptr;
+    auto c = std::make_unique<dsm_cat_t>();
+    const int rc = cat_guard(nullptr, [&] {
+        need(p != nullptr, "dsm_cat_create: null parameters");
+        need(p->num >= 1 && p->num <= MAX_NUM, "dsm_cat_create: num must be in [1, 32]");
+        need(p->theta_n >= 1 && p->theta_delta > 0, "dsm_cat_create: bad catalogue distance grid");
+        need(p->fmin >= 0 && p->fmax >= p->fmin, "dsm_cat_create: bad frequency range");
+        need(p->np1 >= 1 && (p->np1 & (p->np1 - 1)) == 0 && p->np1 >= p->fmax,
+             "dsm_cat_create: np1 must be a power of two >= fmax");
+        need(p->np1 <= (1 << 26), "dsm_cat_create: np1 too large");
+        need(p->tlen > 0, "dsm_cat_create: tlen must be positive");
+        need(p->iwin_start >= 0 && p->iwin_end >= p->iwin_start && p->iwin_end < 2 * p->np1,
+             "dsm_cat_create: window must lie in [0, 2 np1)");
+        need(p->ipdistance >= 0, "dsm_cat_create: negative ipdistance");
+        need((int)(p->ipdistance / p->theta_delta / 2.0) <= (MAX_NW - 1) / 2,
+             "dsm_cat_create: sinc window wider than 255 catalogue distances");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || p->device < 0 || p->device >= n)
+            throw Error(DSM_ERR_NODEVICE, "dsm_cat_create: no CUDA device (or the ordinal is out of range)");
+        c->p = *p;
+        c->dev = p->device;
+        DSM_CUDA(cudaSetDevice(c->dev));
+        DSM_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+        for (auto& x : c->ev) DSM_CUDA(cudaEventCreate(&x));
+        // window factors exp(omegai i / samplingHz), samplingHz = 2 np1 / tlen
+        const double shz = (double)(2 * p->np1) / p->tlen;
+        c->he.resize(c->nwin());
+        for (int t = 0; t < c->nwin(); ++t) c->he[t] = std::exp(p->omegai * (double)(p->iwin_start + t) / shz);
+        c->e.upload(c->he, c->st);
+        DSM_CUDA(cudaStreamSynchronize(c->st));
+    });
+    if (rc != DSM_OK) return rc;
+    *out = c.release();
+    return DSM_OK;
+}
+
+extern "C" int dsm_cat_clear(dsm_cat_t* c) {
+    if (!c) return DSM_ERR_INVALID;
+    return cat_guard(c, [&] { c->sets.clear(); });
+}
+
+extern "C" int dsm_cat_add(dsm_cat_t* c, const void* rec, int elem_bytes, int ncomp, const int* dst,
+                           const double* scale, int on_device) {
+    if (!c) return DSM_ERR_INVALID;
+    return cat_guard(c, [&] {
+        need(rec != nullptr, "dsm_cat_add: null records");
+        need(elem_bytes == 8 || elem_bytes == 16, "dsm_cat_add: elem_bytes must be 8 (complex64) or 16 (complex128)");
+        need(ncomp >= 1 && ncomp <= MAX_NUM, "dsm_cat_add: ncomp must be in [1, 32]");
+        need((int)c->sets.size() < MAX_SETS, "dsm_cat_add: at most 4 record sets");
+        SetDev s{};
+        for (int d = 0; d < MAX_NUM; ++d) s.src[d] = -1;
+        for (int k = 0; k < ncomp; ++k) {
+            const int d = dst ? dst[k] : k;
+            need(d >= 0 && d < c->p.num, "dsm_cat_add: destination component out of range");
+            need(s.src[d] < 0, "dsm_cat_add: two record components map to one destination");
+            s.src[d] = k;
+            s.scale[k] = scale ? scale[k] : 1.0;
+            need(std::isfinite(s.scale[k]), "dsm_cat_add: non-finite scale");
+        }
+        s.cplx64 = elem_bytes == 8;
+        s.ncomp = ncomp;
+        const size_t bytes = (size_t)(c->p.fmax - c->p.fmin + 1) * c->p.theta_n * ncomp * elem_bytes;
+        DSM_CUDA(cudaSetDevice(c->dev));
+        if (on_device) {
+            need(((uintptr_t)rec % elem_bytes) == 0, "dsm_cat_add: misaligned device records");
+            s.rec = rec;
+        } else {
+            auto& buf = c->own[c->sets.size()];
+            buf.reserve(bytes);
+            DSM_CUDA(cudaMemcpyAsync(buf.p, rec, bytes, cudaMemcpyHostToDevice, c->st));
+            s.rec = buf.p;
+        }
+        c->sets.push_back(s);
+    });
+}
+
+namespace {
+template <int C>
+void launch_interp(const InterpArgs& a, dim3 grid, size_t smem, cudaStream_t st) {
+    DSM_CUDA(cudaFuncSetAttribute(k_cat_interp<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_cat_interp<C><<<grid, CAT_THREADS, smem, st>>>(a);
+}
+void launch_interp_c(int C, const InterpArgs& a, dim3 grid, size_t smem, cudaStream_t st) {
+    switch (C) {
+        case 1: launch_interp<1>(a, grid, smem, st); break;
+        case 2: launch_interp<2>(a, grid, smem, st); break;
+        case 3: launch_interp<3>(a, grid, smem, st); break;
+        case 4: launch_interp<4>(a, grid, smem, st); break;
+        case 5: launch_interp<5>(a, grid, smem, st); break;
+        case 6: launch_interp<6>(a, grid, smem, st); break;
+        case 7: launch_interp<7>(a, grid, smem, st); break;
+        default: launch_interp<8>(a, grid, smem, st); break;
+    }
+    DSM_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, int nout, const double* coef,
+                              double* out, int out_on_device) {
+    if (!c) return DSM_ERR_INVALID;
+    return cat_guard(c, [&] {
+        const dsm_cat_params_t& p = c->p;
+        need(npoint >= 0 && (npoint == 0 || (distance && out)), "dsm_cat_series: null argument");
+        need(!c->sets.empty(), "dsm_cat_series: no record set added");
+        const bool identity = coef == nullptr;
+        if (identity) nout = p.num;
+        need(nout >= 1 && nout <= MAX_OUT, "dsm_cat_series: nout must be in [1, 64]");
+        if (npoint == 0) return;
+        DSM_CUDA(cudaSetDevice(c->dev));
+        const int nh = p.np1 + 1, nwin = c->nwin();
+        // sinc windows and weights (clsgt, fourier.f90:136-155), on the host
+        const int nhregion = (int)(p.ipdistance / p.theta_delta / 2.0);
+        const int nwmax = std::min(2 * nhregion + 1, p.theta_n);
+        std::vector<int> wid(npoint), wn(npoint);
+        std::vector<double> ww((size_t)npoint * nwmax, 0.0), wnorm(npoint);
+        for (int k = 0; k < npoint; ++k) {
+            const double dk = distance[k];
+            need(std::isfinite(dk), "dsm_cat_series: non-finite distance");
+            const double q = (dk - p.theta_min) / p.theta_delta;
+            need(std::fabs(q) < 1e9, "dsm_cat_series: distance far outside the catalogue");
+            const int idelta = 1 + (int)q;   // Fortran int(): truncation toward zero
+            int is, ie;
+            idelta_region(idelta, nhregion, p.theta_n, is, ie);
+            wid[k] = is - 1;
+            wn[k] = ie - is + 1;
+            const double th_s = p.theta_min + (double)(is - 1) * p.theta_delta;
+            double nrm = 0.0;
+            for (int kk = is; kk <= ie; ++kk) {
+                const double t = kPi * ((dk - th_s) / p.theta_delta - (double)(kk - is));
+                const double wv = t == 0.0 ? 1.0 : std::sin(t) / t;
+                ww[(size_t)k * nwmax + (kk - is)] = wv;
+                nrm = nrm + wv;
+            }
+            need(nrm != 0.0 && std::isfinite(nrm), "dsm_cat_series: sinc weights sum to zero");
+            wnorm[k] = nrm;
+        }
+        if (!identity)
+            for (size_t i = 0; i < (size_t)npoint * nout * p.num; ++i)
+                need(std::isfinite(coef[i]), "dsm_cat_series: non-finite coefficient");
+        // points sorted by window start (then distance); per-point arrays in that order
+        std::vector<int> ord(npoint);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
+            return wid[x] != wid[y] ? wid[x] < wid[y] : distance[x] < distance[y];
+        });
+        std::vector<int> hids(npoint), hnw(npoint);
+        std::vector<double> hw((size_t)npoint * nwmax), hnorm(npoint), hdist(npoint);
+        for (int s = 0; s < npoint; ++s) {
+            const int k = ord[s];
+            hids[s] = wid[k];
+            hnw[s] = wn[k];
+            hnorm[s] = wnorm[k];
+            hdist[s] = distance[k];
+            std::copy(ww.begin() + (size_t)k * nwmax, ww.begin() + (size_t)(k + 1) * nwmax, hw.begin() + (size_t)s * nwmax);
+        }
+
+        // points per batch: the in-place transform buffer stays under max_batch_bytes
+        const size_t per_point = (size_t)nout * nh * sizeof(cd);
+        int pc = (int)std::max<size_t>(1, c->max_batch_bytes / per_point);
+        pc = std::min(pc, npoint);
+        const int nump = (p.num + 3) / 4 * 4;
+        // rows of the frequency-domain SGT: the catalogue distances some window covers
+        int ubase = p.theta_n, uend = 0;
+        for (int k = 0; k < npoint; ++k) {
+            ubase = std::min(ubase, hids[k]);
+            uend = std::max(uend, hids[k] + hnw[k]);
+        }
+        const int ucov = uend - ubase;
+        // tiles: consecutive sorted points of one batch, at most PT, band at
+        // most nwmax + 64 catalogue distances wide and rounded up to a
+        // multiple of 4 (the product's k step); dense weights [U][WS], zero
+        // outside each point's window.  The frequency-domain SGT has 4 zero
+        // rows after the covered distances for the rounding.
+        std::vector<Tile> tiles;
+        std::vector<int> tile_begin;   // first tile of each batch
+        std::vector<double> hwt;
+        for (int b0 = 0; b0 < npoint; b0 += pc) {
+            const int b1 = std::min(npoint, b0 + pc);
+            tile_begin.push_back((int)tiles.size());
+            int s = b0;
+            while (s < b1) {
+                int lo = hids[s], hi = hids[s] + hnw[s];
+                int e = s + 1;
+                while (e < b1 && e - s < PT) {
+                    const int lo2 = std::min(lo, hids[e]), hi2 = std::max(hi, hids[e] + hnw[e]);
+                    if (hi2 - lo2 > nwmax + 64) break;
+                    lo = lo2;
+                    hi = hi2;
+                    ++e;
+                }
+                const int U = (hi - lo + 3) / 4 * 4;
+                const long long woff = (long long)hwt.size();
+                hwt.resize(hwt.size() + (size_t)U * WS, 0.0);
+                for (int t = s; t < e; ++t)
+                    for (int q = 0; q < hnw[t]; ++q)
+                        hwt[woff + (size_t)(hids[t] + q - lo) * WS + (t - s)] = hw[(size_t)t * nwmax + q];
+                tiles.push_back(Tile{s - b0, e - s, lo - ubase, U, woff});
+                s = e;
+            }
+        }
+        tile_begin.push_back((int)tiles.size());
+
+        auto& S = c->stats;
+        S = dsm_stats_t{};
+        const bool prof = c->profiling;
+        if (prof) DSM_CUDA(cudaEventRecord(c->ev[0], c->st));
+        c->wt.upload(hwt.data(), hwt.size(), c->st);
+        c->norm.upload(hnorm.data(), npoint, c->st);
+        c->dist.upload(hdist.data(), npoint, c->st);
+        c->orig.upload(ord.data(), npoint, c->st);
+        c->tiles.upload(tiles.data(), tiles.size(), c->st);
+        if (!identity) c->coef.upload(coef, (size_t)npoint * nout * p.num, c->st);
+        double* dout = out;
+        if (!out_on_device) {
+            c->out.reserve((size_t)npoint * nout * nwin);
+            dout = c->out.p;
+        }
+        c->h.reserve((size_t)pc * nout * nh);
+
+        const int nf = p.fmax - p.fmin + 1;
+        const int urows = ucov + 4;
+        c->om.reserve((size_t)nf * urows * nump);
+        OmegaArgs oa{};
+        oa.nset = (int)c->sets.size();
+        for (int s = 0; s < oa.nset; ++s) oa.set[s] = c->sets[s];
+        oa.num = p.num;
+        oa.nump = nump;
+        oa.theta_n = p.theta_n;
+        oa.fmin = p.fmin;
+        oa.nf = nf;
+        oa.u0 = ubase;
+        oa.ucov = ucov;
+        oa.urows = urows;
+        oa.theta_min = p.theta_min;
+        oa.theta_delta = p.theta_delta;
+        oa.tlen = p.tlen;
+        oa.c_red_reci = p.c_red_reci;
+        oa.om = c->om.p;
+        if (prof) DSM_CUDA(cudaEventRecord(c->ev[6], c->st));
+        need((size_t)urows * nump < (1u << 30), "dsm_cat_series: catalogue rows too large");
+        k_cat_omega<<<dim3((urows * nump + 255) / 256, nf), 256, 0, c->st>>>(oa);
+        DSM_CUDA(cudaGetLastError());
+        if (prof) DSM_CUDA(cudaEventRecord(c->ev[7], c->st));
+        S.launches += 1;
+
+        InterpArgs a{};
+        a.num = p.num;
+        a.nout = nout;
+        a.identity = identity;
+        a.fmin = p.fmin;
+        a.fmax = p.fmax;
+        a.np1 = p.np1;
+        a.ucov = urows;
+        a.tlen = p.tlen;
+        a.c_red_reci = p.c_red_reci;
+        a.om = c->om.p;
+        a.wt = c->wt.p;
+        a.coef = identity ? nullptr : c->coef.p;
+        a.h = c->h.p;
+        const size_t smem = interp_smem_bytes(nump / 4);
+        double ms_i = 0, ms_f = 0, ms_w = 0;
+        int nbatch = 0;
+        for (int b0 = 0, bi = 0; b0 < npoint; b0 += pc, ++bi) {
+            const int np_ = std::min(pc, npoint - b0);
+            a.tiles = c->tiles.p + tile_begin[bi];
+            a.norm = c->norm.p + b0;
+            a.dist = c->dist.p + b0;
+            a.orig = c->orig.p + b0;
+            if (prof) DSM_CUDA(cudaEventRecord(c->ev[1], c->st));
+            dim3 grid(tile_begin[bi + 1] - tile_begin[bi], (nh + CAT_WARPS - 1) / CAT_WARPS);
+            launch_interp_c(nump / 4, a, grid, smem, c->st);
+            if (prof) DSM_CUDA(cudaEventRecord(c->ev[2], c->st));
+            const int nb = np_ * nout;
+            DSM_CUFFT(cufftExecZ2D(c->plan(nb), reinterpret_cast<cufftDoubleComplex*>(c->h.p),
+                                   reinterpret_cast<cufftDoubleReal*>(c->h.p)));
+            if (prof) DSM_CUDA(cudaEventRecord(c->ev[3], c->st));
+            const size_t total = (size_t)nb * nwin;
+            const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)148 * 16);
+            k_cat_window<<<blocks, 256, 0, c->st>>>(reinterpret_cast<const double*>(c->h.p), 2 * nh, p.iwin_start,
+                                                    nwin, nb, nout, c->orig.p + b0, c->e.p, p.tlen, dout);
+            DSM_CUDA(cudaGetLastError());
+            S.launches += 2;   // interp + window (the transform is cuFFT's)
+            ++nbatch;
+            if (prof) {
+                DSM_CUDA(cudaEventRecord(c->ev[4], c->st));
+                DSM_CUDA(cudaEventSynchronize(c->ev[4]));
+                float t1, t2, t3;
+                cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]);
+                cudaEventElapsedTime(&t2, c->ev[2], c->ev[3]);
+                cudaEventElapsedTime(&t3, c->ev[3], c->ev[4]);
+                ms_i += t1;
+                ms_f += t2;
+                ms_w += t3;
+            }
+        }
+        if (!out_on_device)
+            DSM_CUDA(cudaMemcpyAsync(out, dout, (size_t)npoint * nout * nwin * sizeof(double), cudaMemcpyDeviceToHost,
+                                     c->st));
+        if (prof) DSM_CUDA(cudaEventRecord(c->ev[5], c->st));
+        DSM_CUDA(cudaStreamSynchronize(c->st));
+        if (prof) {
+            float tt;
+            cudaEventElapsedTime(&tt, c->ev[0], c->ev[5]);
+            S.ms_total = tt;
+            // algorithmic bytes: the records of the covered catalogue
+            // distances read once and the frequency-domain SGT written
+            // (omega); that SGT read once and H written (interp); H read and
+            // written (transform); window samples read and written.  Flops of
+            // the interpolation: 4 per weight, frequency and component.
+            float to;
+            cudaEventElapsedTime(&to, c->ev[6], c->ev[7]);
+            std::vector<char> cover(p.theta_n, 0);
+            double wterms = 0;
+            for (int k = 0; k < npoint; ++k) {
+                for (int q = 0; q < hnw[k]; ++q) cover[hids[k] + q] = 1;
+                wterms += hnw[k];
+            }
+            double ncov = 0;
+            for (char x : cover) ncov += x;
+            double rec_bytes = 0;
+            for (auto& s : c->sets) rec_bytes += (double)nf * ncov * s.ncomp * (s.cplx64 ? 8.0 : 16.0);
+            const double ob = (double)nf * ncov * p.num * sizeof(cd);
+            const double hb = (double)npoint * nout * nh * sizeof(cd);
+            const double wb = 2.0 * npoint * nout * nwin * sizeof(double);
+            const char* nm[4] = {"cat_omega", "cat_interp", "cat_fft", "cat_window"};
+            const double ms[4] = {to, ms_i, ms_f, ms_w};
+            const double by[4] = {rec_bytes + ob, ob + hb, 2.0 * hb, wb};
+            const double fl[4] = {0.0, 4.0 * wterms * nf * p.num, 0.0, 0.0};
+            for (int k = 0; k < 4; ++k) {
+                snprintf(S.kern[k].name, sizeof(S.kern[k].name), "%s", nm[k]);
+                S.kern[k].ms = ms[k];
+                S.kern[k].launches = k == 0 ? 1 : nbatch;
+                S.kern[k].alg_bytes = by[k];
+                S.kern[k].alg_flops = fl[k];
+            }
+            S.nk = 4;
+        }
+    });
+}
+
+extern "C" int dsm_cat_set_profiling(dsm_cat_t* c, int on) {
+    if (!c) return DSM_ERR_INVALID;
+    c->profiling = on != 0;
+    return DSM_OK;
+}
+
+extern "C" int dsm_cat_get_stats(const dsm_cat_t* c, dsm_stats_t* s) {
+    if (!c || !s) return DSM_ERR_INVALID;
+    *s = c->stats;
+    return DSM_OK;
+}
+
+extern "C" int dsm_cat_set_batch_bytes(dsm_cat_t* c, size_t bytes) {
+    if (!c || bytes < ((size_t)1 << 20)) return DSM_ERR_INVALID;
+    c->max_batch_bytes = bytes;
+    return DSM_OK;
+}
+
+namespace {
+// independent FP64 fused multiply-add chains, 8 per thread
+__global__ void k_fp64_probe(double* out, int iters, double a, double b) {
+    double x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3 + k;
+    for (int i = 0; i < iters; ++i)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += x[k];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+}  // namespace
+
+namespace {
+// independent FP64 tensor-core products, 8 accumulator tiles per warp
+__global__ void k_fp64_mma_probe(double* out, int iters, double a) {
+    double acc[8][4];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[k][e] = 0.0;
+    const double a0 = a * threadIdx.x, a1 = a0 + 1.0, b = 1e-3 * (threadIdx.x & 7);
+    for (int i = 0; i < iters; ++i)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) cat::mma_f64_16x8x4(acc[k], a0, a1, b);
+    double s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += acc[k][0] + acc[k][1] + acc[k][2] + acc[k][3];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+}  // namespace
+
+extern "C" int dsm_fp64_peak(int device, double* tflops) {
+    return cat_guard(nullptr, [&] {
+        need(tflops != nullptr, "dsm_fp64_peak: null output");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n)
+            throw Error(DSM_ERR_NODEVICE, "dsm_fp64_peak: no CUDA device");
+        DSM_CUDA(cudaSetDevice(device));
+        int sms = 0;
+        DSM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+        DBuf<double> out;
+        out.reserve((size_t)blocks * threads);
+        cudaEvent_t e0, e1;
+        DSM_CUDA(cudaEventCreate(&e0));
+        DSM_CUDA(cudaEventCreate(&e1));
+        k_fp64_probe<<<blocks, threads>>>(out.p, iters / 16, 0.999999, 1e-7);   // warm-up
+        DSM_CUDA(cudaEventRecord(e0));
+        k_fp64_probe<<<blocks, threads>>>(out.p, iters, 0.999999, 1e-7);
+        DSM_CUDA(cudaEventRecord(e1));
+        DSM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *tflops = 2.0 * 8.0 * iters * (double)blocks * threads / (ms * 1e-3) / 1e12;
+    });
+}
+
+extern "C" int dsm_fp64_mma_peak(int device, double* tflops) {
+    return cat_guard(nullptr, [&] {
+        need(tflops != nullptr, "dsm_fp64_mma_peak: null output");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n)
+            throw Error(DSM_ERR_NODEVICE, "dsm_fp64_mma_peak: no CUDA device");
+        DSM_CUDA(cudaSetDevice(device));
+        int sms = 0;
+        DSM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        const int blocks = sms * 4, threads = 256, iters = 1 << 12;
+        DBuf<double> out;
+        out.reserve((size_t)blocks * threads);
+        cudaEvent_t e0, e1;
+        DSM_CUDA(cudaEventCreate(&e0));
+        DSM_CUDA(cudaEventCreate(&e1));
+        k_fp64_mma_probe<<<blocks, threads>>>(out.p, iters / 16, 1e-6);   // warm-up
+        DSM_CUDA(cudaEventRecord(e0));
+        k_fp64_mma_probe<<<blocks, threads>>>(out.p, iters, 1e-6);
+        DSM_CUDA(cudaEventRecord(e1));
+        DSM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        const double warps = (double)blocks * threads / 32;
+        *tflops = 2.0 * 16 * 8 * 4 * 8.0 * iters * warps / (ms * 1e-3) / 1e12;
+    });
+}
+
+extern "C" int dsm_cat_destroy(dsm_cat_t* c) {
+    delete c;
+    return DSM_OK;
+}
+
+extern "C" const char* dsm_cat_last_error(const dsm_cat_t* c) { return c ? c->err.c_str() : g_cat_err.c_str(); }

@@ -114,6 +114,14 @@ class DsmError(RuntimeError):
     pass
 
 
+class CatParams(C.Structure):
+    _fields_ = [("num", C.c_int), ("theta_n", C.c_int), ("theta_min", C.c_double),
+                ("theta_delta", C.c_double), ("fmin", C.c_int), ("fmax", C.c_int), ("np1", C.c_int),
+                ("tlen", C.c_double), ("omegai", C.c_double), ("ipdistance", C.c_double),
+                ("c_red_reci", C.c_double), ("iwin_start", C.c_int), ("iwin_end", C.c_int),
+                ("device", C.c_int)]
+
+
 _lib = None
 
 
@@ -154,6 +162,20 @@ def lib() -> C.CDLL:
         L.dsm_lmax_grad.argtypes = [_f, _f, _f, C.c_int, _f, _f, C.c_int]
         L.dsm_set_lmax_model.argtypes = [C.c_void_p, _f]
         L.dsm_lmax_predict.argtypes = [C.c_void_p, _ip, C.c_int, _f]
+        L.dsm_cat_np1.argtypes = [C.c_double, C.c_int, C.c_double, C.c_double, C.c_double, _ip, _dp,
+                                  _ip, _ip]
+        L.dsm_cat_create.argtypes = [C.POINTER(CatParams), C.POINTER(C.c_void_p)]
+        L.dsm_cat_add.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, _ip, _dp, C.c_int]
+        L.dsm_cat_clear.argtypes = [C.c_void_p]
+        L.dsm_cat_series.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_void_p, C.c_int]
+        L.dsm_cat_set_profiling.argtypes = [C.c_void_p, C.c_int]
+        L.dsm_cat_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+        L.dsm_cat_set_batch_bytes.argtypes = [C.c_void_p, C.c_size_t]
+        L.dsm_cat_destroy.argtypes = [C.c_void_p]
+        L.dsm_cat_last_error.argtypes = [C.c_void_p]
+        L.dsm_cat_last_error.restype = C.c_char_p
+        L.dsm_fp64_peak.argtypes = [C.c_int, _dp]
+        L.dsm_fp64_mma_peak.argtypes = [C.c_int, _dp]
         _lib = L
     return _lib
 
@@ -412,6 +434,112 @@ class Context:
         if self.h.value:
             lib().dsm_ctx_destroy(self.h)
             self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cat_np1(tlen: float, fmax: int, sampling_hz: float, start: float, end: float):
+    """(np1, samplingHz, iwin_start, iwin_end) of a time window (dsm_cat_np1)."""
+    n1, s0, s1 = C.c_int(), C.c_int(), C.c_int()
+    shz = C.c_double()
+    rc = lib().dsm_cat_np1(tlen, fmax, sampling_hz, start, end, C.byref(n1), C.byref(shz), C.byref(s0),
+                           C.byref(s1))
+    if rc:
+        raise DsmError(f"dsm_cat_np1 failed ({rc}): {lib().dsm_cat_last_error(None).decode()}")
+    return n1.value, shz.value, s0.value, s1.value
+
+
+def fp64_peak(device: int = 0, mma: bool = False) -> float:
+    """Measured FP64 throughput of the device (TFLOP/s): fused multiply-adds,
+    or tensor-core products with mma=True."""
+    v = C.c_double()
+    rc = (lib().dsm_fp64_mma_peak if mma else lib().dsm_fp64_peak)(device, C.byref(v))
+    if rc:
+        raise DsmError(f"dsm_fp64_peak failed ({rc}): {lib().dsm_cat_last_error(None).decode()}")
+    return v.value
+
+
+class Catalogue:
+    """Catalogue consumer (dsm_cat_*): record sets of one receiver radius in,
+    windowed time series at arbitrary distances out."""
+
+    FIELDS = ("num", "theta_n", "theta_min", "theta_delta", "fmin", "fmax", "np1", "tlen", "omegai",
+              "ipdistance", "c_red_reci", "iwin_start", "iwin_end")
+
+    def __init__(self, params: dict, device: int = 0):
+        self.p = dict(params)
+        cp = CatParams(**{k: self.p[k] for k in self.FIELDS}, device=device)
+        h = C.c_void_p()
+        rc = lib().dsm_cat_create(C.byref(cp), C.byref(h))
+        if rc:
+            raise DsmError(f"dsm_cat_create failed ({rc}): {lib().dsm_cat_last_error(None).decode()}")
+        self.h = h
+        self._keep = []
+        self.nwin = self.p["iwin_end"] - self.p["iwin_start"] + 1
+
+    def _check(self, rc, what):
+        if rc:
+            raise DsmError(f"{what} failed ({rc}): {lib().dsm_cat_last_error(self.h).decode()}")
+
+    def add(self, rec, dst=None, scale=None):
+        """rec: numpy [nf][theta_n][ncomp] complex64/complex128 (host), or a
+        torch CUDA tensor of that shape (kept alive until clear())."""
+        dp = None if dst is None else np.ascontiguousarray(dst, np.int32)
+        sp = None if scale is None else np.ascontiguousarray(scale, np.float64)
+        on_dev = 0
+        if hasattr(rec, "data_ptr"):
+            assert rec.is_cuda and rec.is_contiguous()
+            ptr, eb, nc, on_dev = rec.data_ptr(), rec.element_size(), rec.shape[-1], 1
+        else:
+            rec = np.ascontiguousarray(rec)
+            assert rec.dtype in (np.complex64, np.complex128)
+            ptr, eb, nc = rec.ctypes.data, rec.itemsize, rec.shape[-1]
+        self._keep.append(rec)
+        rc = lib().dsm_cat_add(self.h, C.c_void_p(ptr), eb, nc,
+                               None if dp is None else _ptr(dp, _ip),
+                               None if sp is None else _ptr(sp, _dp), on_dev)
+        self._check(rc, "dsm_cat_add")
+
+    def clear(self):
+        self._check(lib().dsm_cat_clear(self.h), "dsm_cat_clear")
+        self._keep = []
+
+    def series(self, distances, coef=None, out=None):
+        """Time series [npoint][nout][nwin] (numpy, or written into the torch
+        CUDA tensor ``out``)."""
+        d = np.ascontiguousarray(distances, np.float64)
+        cf = None if coef is None else np.ascontiguousarray(coef, np.float64)
+        nout = self.p["num"] if cf is None else cf.shape[1]
+        if out is None:
+            res = np.zeros((d.size, nout, self.nwin), np.float64)
+            optr, on_dev = res.ctypes.data, 0
+        else:
+            assert out.is_cuda and out.is_contiguous() and out.numel() == d.size * nout * self.nwin
+            res, optr, on_dev = out, out.data_ptr(), 1
+        rc = lib().dsm_cat_series(self.h, d.size, _ptr(d, _dp), nout,
+                                  None if cf is None else _ptr(cf, _dp), C.c_void_p(optr), on_dev)
+        self._check(rc, "dsm_cat_series")
+        return res
+
+    def set_profiling(self, on: bool):
+        self._check(lib().dsm_cat_set_profiling(self.h, int(on)), "dsm_cat_set_profiling")
+
+    def set_batch_bytes(self, nbytes: int):
+        self._check(lib().dsm_cat_set_batch_bytes(self.h, nbytes), "dsm_cat_set_batch_bytes")
+
+    def stats(self) -> Stats:
+        st = Stats()
+        self._check(lib().dsm_cat_get_stats(self.h, C.byref(st)), "dsm_cat_get_stats")
+        return st
+
+    def close(self):
+        if self.h:
+            lib().dsm_cat_destroy(self.h)
+            self.h = None
 
     def __del__(self):
         try:

@@ -313,6 +313,91 @@ int dsm_lmax_grad(const float *params, const float *feats, const float *target, 
 int dsm_set_lmax_model(dsm_ctx_t *ctx, const float *params);
 int dsm_lmax_predict(dsm_ctx_t *ctx, const int *ilist, int n, float *out);
 
+/* ------------------------------------------------------------------------
+ * Catalogue consumer: the SGT records of one receiver radius (frequency
+ * indices fmin..fmax at every catalogue distance, as SGTpsv / SGTsh write
+ * them) turned into windowed time series at arbitrary epicentral distances
+ * on the device.  Replaces KernelMaker's
+ *   rdsgtomega        src/KernelMaker/fourier.f90:1-123
+ *   clsgt             src/KernelMaker/fourier.f90:128-162
+ *   findIdeltaRegion  src/KernelMaker/fourier.f90:165-190
+ *   vectorFFT_double  src/KernelMaker/fourier.f90:418-450 (with cdft/bitrv2)
+ * and the transform set-up of src/KernelMaker/KernelMaker-1.0.0.f90:311-330.
+ * The per-point real combination of components that KernelMaker applies
+ * before its transform (synn2h3freq, rsgt2h3freq, tsgt2h4freq and the
+ * moment-tensor sums) can be passed as a matrix per point.
+ * ---------------------------------------------------------------------- */
+typedef struct dsm_cat_params {
+    int    num;            /* components of the frequency-domain SGT (<= 32) */
+    int    theta_n;        /* catalogue distances theta_min + k theta_delta  */
+    double theta_min, theta_delta;      /* degrees                           */
+    int    fmin, fmax;     /* frequency indices of the records               */
+    int    np1;            /* half transform length: power of two >= fmax    */
+    double tlen;           /* time length (s)                                */
+    double omegai;         /* imaginary frequency (1/s), -ln(x)/tlen as
+                              KernelMaker-1.0.0.f90:86 computes it           */
+    double ipdistance;     /* sinc interpolation window (deg)                */
+    double c_red_reci;     /* reducing slowness (s/deg), 0: none             */
+    int    iwin_start, iwin_end;        /* output samples, 0 <= s <= e < 2 np1 */
+    int    device;         /* CUDA device ordinal                            */
+} dsm_cat_params_t;
+
+typedef struct dsm_cat dsm_cat_t;
+
+/* np1, the redefined sampling rate and the window samples of a time window
+ * [start, end] (s), from lsmoothfinder (src/KernelMaker/others.f90:288-308)
+ * and KernelMaker-1.0.0.f90:311-330.  Any output pointer but np1 may be
+ * NULL. */
+int dsm_cat_np1(double tlen, int fmax, double sampling_hz, double start, double end,
+                int *np1, double *sampling_hz_out, int *iwin_start, int *iwin_end);
+
+int dsm_cat_create(const dsm_cat_params_t *p, dsm_cat_t **cat);
+
+/* Adds one record set to the frequency-domain SGT (rdsgtomega, one call per
+ * catalogue kind).  rec holds [fmax-fmin+1][theta_n][ncomp] complex numbers
+ * (elem_bytes 8: complex64 as in the catalogue files; 16: complex128), record
+ * k being frequency index fmin + k; the record of index 0 is never read.
+ * Component k is multiplied by scale[k] (NULL: 1; the reference halves
+ * SYNN_PSV components 2, 8-10 and SYNN_SH 3-5, fourier.f90:78-85), by 1e-21
+ * and by the reduction phase, and added to component dst[k] (NULL: k; the
+ * reference puts SH sets into P-SV slots, fourier.f90:103-116).  With
+ * on_device = 1, rec is a device pointer that must stay valid until
+ * dsm_cat_clear or dsm_cat_destroy; otherwise it is copied to the device.
+ * At most 4 sets. */
+int dsm_cat_add(dsm_cat_t *cat, const void *rec, int elem_bytes, int ncomp,
+                const int *dst, const double *scale, int on_device);
+
+/* Forgets every record set (tsgtomega = 0). */
+int dsm_cat_clear(dsm_cat_t *cat);
+
+/* Time series at npoint distances (deg): out[p][j][t], t over the window,
+ * j < nout, from the component combination coef[p][j][c] (c < num; NULL:
+ * the num components themselves, nout ignored).  With out_on_device = 1,
+ * out is a device pointer. */
+int dsm_cat_series(dsm_cat_t *cat, int npoint, const double *distance, int nout,
+                   const double *coef, double *out, int out_on_device);
+
+/* Per-stage device time of the last dsm_cat_series when profiling is on:
+ * kern[] holds cat_interp, cat_fft, cat_window (ms, launches, algorithmic
+ * bytes); ms_total covers the whole call. */
+int dsm_cat_set_profiling(dsm_cat_t *cat, int on);
+int dsm_cat_get_stats(const dsm_cat_t *cat, dsm_stats_t *stats);
+
+/* Upper bound of the transform buffer (bytes, >= 1 MiB; default 2 GiB):
+ * points are processed in batches that fit it. */
+int dsm_cat_set_batch_bytes(dsm_cat_t *cat, size_t bytes);
+
+int dsm_cat_destroy(dsm_cat_t *cat);
+const char *dsm_cat_last_error(const dsm_cat_t *cat);
+
+/* FP64 fused multiply-add throughput of a device (TFLOP/s, independent
+ * chains, all SMs).  No counterpart in the reference; measurement support
+ * for the interpolation's roofline. */
+int dsm_fp64_peak(int device, double *tflops);
+/* The same for FP64 tensor-core products (mma.m16n8k4.f64, independent
+ * accumulators, all SMs). */
+int dsm_fp64_mma_peak(int device, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,272 @@
+"""Oracle (test infrastructure only): FP64 numpy restatement of KernelMaker's
+catalogue consumer, for checking the device catalogue kernels.  Only tests,
+``__graft_entry__.smoke()`` and the CPU leg of ``bench.py`` may import it.
+
+Steps restated (paths inside the DSM Kernel Suite):
+  * transform length: ``lsmoothfinder`` (src/KernelMaker/others.f90:288-308)
+    and the np1 / samplingHz / window set-up of
+    src/KernelMaker/KernelMaker-1.0.0.f90:311-330;
+  * ``rdsgtomega`` (src/KernelMaker/fourier.f90:1-123): complex64 records
+    widened to complex128, the per-kind halvings (:78-85), times
+    exp(-2 pi i f/tlen * (-thetaD c_red_reci)) * 1e-21 (:91-101), summed into
+    the frequency-domain SGT with the SH -> P-SV component map (:103-116);
+  * ``clsgt`` (fourier.f90:128-162) with ``findIdeltaRegion`` (:165-190):
+    normalised sinc interpolation in distance and the slowness-reduction
+    phase;
+  * ``vectorFFT_double`` (fourier.f90:418-450): Hermitian extension, the
+    length-2 np1 transform of ``cdft`` / ``bitrv2`` (:492-600) and the
+    exp(omegai t) / tlen * 1e3 window.
+
+The transform is restated step for step (radix-2 decimation in frequency
+with the reference's twiddle recurrence, then the bit-reversal
+permutation), vectorised over series; ``test_cpu_catalogue_oracle`` pins it
+against the DFT definition X_k = sum_n x_n exp(+2 pi i n k / N).
+
+Parity status: the restatement is pinned by the DFT identity and by
+hand-derivable cases (a single frequency line, a point on a catalogue
+node); the reference itself (Fortran) cannot be built here.
+"""
+from __future__ import annotations
+
+import math
+from functools import lru_cache
+
+import numpy as np
+
+PI = 3.1415926535897932          # src/KernelMaker/module.f90:54
+PI_FFT = 3.141592653589793       # the local constant of vectorFFT_double (fourier.f90:425)
+
+# reference kind codes of rdsgtomega (fourier.f90:13-16)
+SYNN_SH, SYNN_PSV, RSGT_SH, RSGT_PSV, TSGT_SH, TSGT_PSV = 1, 2, 10, 20, 100, 200
+
+
+def lsmoothfinder(tlen: float, np0: int, freq: float) -> int:
+    """src/KernelMaker/others.f90:288-308."""
+    np_ = 1
+    while np_ < np0:
+        np_ *= 2
+    lsmooth = int(0.5 * tlen * freq / float(np_))
+    i = 1
+    while i < lsmooth:
+        i *= 2
+    return i
+
+
+def transform_length(tlen: float, fmax: int, sampling_hz: float, start: float, end: float):
+    """np1, the redefined samplingHz and the window sample range
+    (KernelMaker-1.0.0.f90:311-330)."""
+    lsmooth = lsmoothfinder(tlen, fmax, sampling_hz)
+    i = 1
+    while i < lsmooth:
+        i *= 2
+    lsmooth = i
+    np1 = 1
+    while np1 < fmax:
+        np1 *= 2
+    np1 *= lsmooth
+    shz = float(2 * np1) / tlen
+    return np1, shz, int(start * shz), int(end * shz)
+
+
+def kind_scale(kind: int, num: int) -> np.ndarray:
+    """Per-component factor rdsgtomega applies to one record set
+    (fourier.f90:78-85): SYNN_SH halves components 3..5, SYNN_PSV halves 2
+    and 8..10 (1-based)."""
+    s = np.ones(num)
+    if kind == SYNN_SH:
+        s[2:5] = 0.5
+    elif kind == SYNN_PSV:
+        s[1] = 0.5
+        s[7:10] = 0.5
+    return s
+
+
+def kind_dst(kind: int, num: int) -> np.ndarray:
+    """0-based destination component of each record component in the P-SV
+    sized frequency-domain arrays (fourier.f90:103-116)."""
+    if kind in (SYNN_SH, RSGT_SH):
+        return np.arange(5, 5 + num)
+    if kind == TSGT_SH:
+        return np.array([6] + list(range(11, 11 + num - 1)))
+    return np.arange(num)
+
+
+def omega_sgt(sets, num: int, fmin: int, fmax: int, theta, tlen: float, c_red_reci: float):
+    """rdsgtomega for a list of record sets; each set is (records, dst, scale)
+    with records [fmax-fmin+1][theta_n][ncomp] complex64 or complex128.
+    Returns the frequency-domain SGT [nf][theta_n][num] complex128.  The
+    record of frequency index 0 is never read (fourier.f90:28)."""
+    theta = np.asarray(theta, np.float64)
+    nf = fmax - fmin + 1
+    out = np.zeros((nf, theta.size, num), np.complex128)
+    for rec, dst, scale in sets:
+        rec = np.asarray(rec)
+        assert rec.shape[:2] == (nf, theta.size)
+        for k in range(nf):
+            i = fmin + k
+            if i == 0:
+                continue
+            sd = rec[k].astype(np.complex128) * np.asarray(scale)[None, :]
+            redtime = -theta * c_red_reci
+            arg = -2.0 * PI * float(i) / tlen * redtime
+            ph = np.cos(arg) + 1j * np.sin(arg)
+            sd = sd * ph[:, None] * 1e-21
+            out[k][:, np.asarray(dst)] += sd
+    return out
+
+
+def find_idelta_region(ix: int, nhalf: int, nmax: int):
+    """fourier.f90:165-190 (1-based indices)."""
+    istart, iend = ix - nhalf, ix + nhalf
+    if istart < 1:
+        iend += 1 - istart
+        istart = 1
+    if iend > nmax:
+        istart -= iend - nmax
+        iend = nmax
+    istart = max(istart, 1)
+    iend = min(iend, nmax)
+    return istart, iend
+
+
+def sinc_weights(distance: float, theta_min: float, theta_delta: float, theta_n: int,
+                 ipdistance: float):
+    """Window [idstart, idend] (0-based, inclusive), its weights and their
+    sum, in the operation order of clsgt (fourier.f90:136-155)."""
+    thetaD = lambda i: theta_min + float(i - 1) * theta_delta  # noqa: E731 (KernelMaker-1.0.0.f90:247)
+    idelta = 1 + int((distance - thetaD(1)) / theta_delta)
+    nhregion = int(ipdistance / theta_delta / 2.0)
+    ids, ide = find_idelta_region(idelta, nhregion, theta_n)
+    w = []
+    norm = 0.0
+    for kk in range(ids, ide + 1):
+        t = PI * ((distance - thetaD(ids)) / theta_delta - float(kk - ids))
+        if t == 0.0:
+            w.append(1.0)
+            norm = norm + 1.0
+        else:
+            w.append(math.sin(t) / t)
+            norm = norm + math.sin(t) / t
+    return ids - 1, ide - 1, np.array(w), norm
+
+
+def clsgt(distance: float, omega, fmin: int, theta_min: float, theta_delta: float,
+          ipdistance: float, tlen: float, c_red_reci: float):
+    """Interpolated SGT at one distance: [nf][num] complex128."""
+    omega = np.asarray(omega)
+    ids, ide, w, norm = sinc_weights(distance, theta_min, theta_delta, omega.shape[1], ipdistance)
+    acc = np.zeros((omega.shape[0], omega.shape[2]), np.complex128)
+    for q, kk in enumerate(range(ids, ide + 1)):
+        acc = acc + w[q] * omega[:, kk, :]   # a weight of exactly 1 adds the term unscaled
+    j = np.arange(fmin, fmin + omega.shape[0], dtype=np.float64)
+    arg = -2.0 * PI * j / tlen * distance * c_red_reci
+    ph = np.cos(arg) + 1j * np.sin(arg)
+    return acc / norm * ph[:, None]
+
+
+@lru_cache(maxsize=16)
+def _cdft_twiddles(N: int):
+    """Twiddles of each stage of cdft (fourier.f90:492-560) for N complex
+    points: a list of (half, w[half]) with w[q] the factor of the q-th
+    difference in a block, produced by the reference's recurrence."""
+    wmr, wmi = math.cos(PI_FFT / N), math.sin(PI_FFT / N)
+    stages = []
+    M = N
+    while M > 2:
+        half = M // 2
+        w = np.empty(half, np.complex128)
+        wkr, wki = 1.0, 0.0
+        wdr = 1 - 2 * wmi * wmi
+        wdi = 2 * wmi * wmr
+        ss = 2 * wdi
+        wmr, wmi = wdr, wdi
+        w[0] = 1.0
+        if half > 1:
+            w[1] = complex(wdr, wdi)
+        for q in range(2, half, 2):
+            wkr = wkr - ss * wdi
+            wki = wki + ss * wdr
+            wdr = wdr - ss * wki
+            wdi = wdi + ss * wkr
+            w[q] = complex(wkr, wki)
+            w[q + 1] = complex(wdr, wdi)
+        stages.append((half, w))
+        M = half
+    return stages
+
+
+@lru_cache(maxsize=16)
+def _bit_reverse(N: int) -> np.ndarray:
+    bits = N.bit_length() - 1
+    idx = np.arange(N)
+    rev = np.zeros(N, np.int64)
+    for b in range(bits):
+        rev |= ((idx >> b) & 1) << (bits - 1 - b)
+    return rev
+
+
+def cdft(c: np.ndarray) -> np.ndarray:
+    """The complex transform of cdft(2 N, cos(pi/N), sin(pi/N), c) applied to
+    the last axis of c (N complex points, a power of two >= 2): radix-2
+    decimation in frequency with twiddles from the reference recurrence
+    (complex butterflies written with the reference's real operations),
+    a last twiddle-free radix-2 stage, then the bit-reversal permutation."""
+    a = np.array(c, np.complex128, copy=True)
+    N = a.shape[-1]
+    lead = a.shape[:-1]
+    for half, w in _cdft_twiddles(N):
+        blk = a.reshape(lead + (N // (2 * half), 2, half))
+        lo, hi = blk[..., 0, :].copy(), blk[..., 1, :].copy()
+        xr, xi = lo.real - hi.real, lo.imag - hi.imag
+        blk[..., 0, :] = (lo.real + hi.real) + 1j * (lo.imag + hi.imag)
+        blk[..., 1, :] = (w.real * xr - w.imag * xi) + 1j * (w.real * xi + w.imag * xr)
+        a = blk.reshape(lead + (N,))
+    blk = a.reshape(lead + (N // 2, 2))
+    lo, hi = blk[..., 0].copy(), blk[..., 1].copy()
+    blk[..., 0] = (lo.real + hi.real) + 1j * (lo.imag + hi.imag)
+    blk[..., 1] = (lo.real - hi.real) + 1j * (lo.imag - hi.imag)
+    a = blk.reshape(lead + (N,))
+    if N > 2:
+        a = a[..., _bit_reverse(N)]
+    return a
+
+
+def hermitian_extend(ccvec: np.ndarray, fmin: int, fmax: int, np1: int) -> np.ndarray:
+    """cvec of vectorFFT_double (fourier.f90:430-439) for series on the last
+    axis of ccvec ([..., fmax-fmin+1])."""
+    lead = ccvec.shape[:-1]
+    cvec = np.zeros(lead + (2 * np1,), np.complex128)
+    cvec[..., fmin:fmax + 1] = ccvec
+    for i in range(fmin, np1):
+        cvec[..., np1 + i] = np.conj(cvec[..., np1 - i])
+    return cvec
+
+
+def vector_fft_double(ccvec, fmin: int, fmax: int, np1: int, omegai: float, tlen: float,
+                      iws: int, iwe: int) -> np.ndarray:
+    """Windowed real time series of each series on the last axis."""
+    cvec = cdft(hermitian_extend(np.asarray(ccvec, np.complex128), fmin, fmax, np1))
+    shz = float(2 * np1) / tlen
+    i = np.arange(iws, iwe + 1, dtype=np.float64)
+    return cvec[..., iws:iwe + 1].real * np.exp(omegai * i / shz) / tlen * 1.0e3
+
+
+def series(p: dict, sets, distances, coef=None) -> np.ndarray:
+    """Time series [npoint][nout][nwin] of the catalogue consumer.
+
+    p: num, theta_n, theta_min, theta_delta, fmin, fmax, np1, tlen, omegai,
+       ipdistance, c_red_reci, iwin_start, iwin_end.
+    sets: list of (records, dst, scale) as in omega_sgt.
+    coef: [npoint][nout][num] real combination applied after clsgt (as
+       rsgt2h3freq / tsgt2h4freq / synn2h3freq do), or None for the
+       components themselves."""
+    theta = p["theta_min"] + np.arange(p["theta_n"], dtype=np.float64) * p["theta_delta"]
+    om = omega_sgt(sets, p["num"], p["fmin"], p["fmax"], theta, p["tlen"], p["c_red_reci"])
+    outs = []
+    for k, d in enumerate(distances):
+        f = clsgt(float(d), om, p["fmin"], p["theta_min"], p["theta_delta"], p["ipdistance"],
+                  p["tlen"], p["c_red_reci"])                       # [nf][num]
+        h = f.T if coef is None else np.asarray(coef[k]) @ f.T    # [nout][nf]
+        outs.append(vector_fft_double(h, p["fmin"], p["fmax"], p["np1"], p["omegai"], p["tlen"],
+                                      p["iwin_start"], p["iwin_end"]))
+    return np.stack(outs)

@@ -1,0 +1,159 @@
+"""Device catalogue consumer (dsm_cat_*) against the oracle restatement of
+KernelMaker's rdsgtomega / clsgt / vectorFFT_double.
+
+Every case must match the oracle to 1e-10 relative L2 (FP64 throughout; the
+differences are the transform's and sin/cos rounding).  Cases cover: points
+on catalogue nodes, between nodes, at and beyond both ends of the distance
+grid (window clipping); fmin > 0 (partial Hermitian extension) and
+fmax = np1 (the self-conjugated middle sample); complex64 and complex128
+records; two record sets with the SH -> P-SV component map and halvings; a
+reducing slowness; a per-point combination matrix; batches split by the
+buffer limit; device pointers; and the full-size workload (1441 distances,
+2049 frequencies) on sampled points plus linearity."""
+import numpy as np
+import pytest
+
+import dsmsgt
+from conftest import rel_l2
+
+TOL = 1e-10
+
+
+def _records(p, ncomp, seed, dtype=np.complex64):
+    rng = np.random.default_rng(seed)
+    nf = p["fmax"] - p["fmin"] + 1
+    shp = (nf, p["theta_n"], ncomp)
+    return (rng.standard_normal(shp) + 1j * rng.standard_normal(shp)).astype(dtype)
+
+
+def _params(**kw):
+    p = dict(num=20, theta_n=61, theta_min=0.0, theta_delta=0.5, fmin=0, fmax=48, np1=64, tlen=819.2,
+             omegai=np.log(100.0) / 819.2, ipdistance=5.0, c_red_reci=0.0, iwin_start=3, iwin_end=120)
+    p.update(kw)
+    return p
+
+
+DIST = [0.0, 0.26, 2.0, 7.5, 15.13, 29.9, 30.0, 31.2]
+
+
+def _oracle(p, sets, dist, coef=None):
+    from oracle import catalogue as cat
+    return cat.series(p, sets, dist, coef)
+
+
+def _run(p, sets, dist, coef=None, batch_bytes=None):
+    c = dsmsgt.Catalogue(p)
+    if batch_bytes:
+        c.set_batch_bytes(batch_bytes)
+    for rec, dst, scale in sets:
+        c.add(rec, dst, scale)
+    out = c.series(dist, coef)
+    c.close()
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("c_red", [0.0, 12.5])
+def test_catalogue_components_match_oracle(built, c_red):
+    p = _params(c_red_reci=c_red)
+    sets = [(_records(p, 20, 1), None, None)]
+    got = _run(p, sets, DIST)
+    want = _oracle(p, [(sets[0][0], np.arange(20), np.ones(20))], DIST)
+    assert got.shape == (len(DIST), 20, 118)
+    assert rel_l2(got, want) <= TOL
+    for k in range(len(DIST)):                       # every point, not only the sum
+        assert rel_l2(got[k], want[k]) <= TOL, k
+
+
+@pytest.mark.gpu
+def test_catalogue_combination_matrix_matches_oracle(built):
+    p = _params(c_red_reci=7.0)
+    rng = np.random.default_rng(5)
+    coef = rng.standard_normal((len(DIST), 6, 20))
+    rec = _records(p, 20, 2)
+    got = _run(p, [(rec, None, None)], DIST, coef)
+    want = _oracle(p, [(rec, np.arange(20), np.ones(20))], DIST, coef)
+    assert got.shape == (len(DIST), 6, 118)
+    assert rel_l2(got, want) <= TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fmin,fmax,win", [(5, 64, (0, 127)), (0, 64, (60, 70)), (33, 40, (0, 0))])
+def test_catalogue_two_sets_partial_spectrum(built, fmin, fmax, win):
+    """P-SV TSGT (complex64) plus SH TSGT (complex128, halved, mapped into
+    components 7 and 12-20 as rdsgtomega does)."""
+    from oracle import catalogue as cat
+    p = _params(fmin=fmin, fmax=fmax, iwin_start=win[0], iwin_end=win[1])
+    psv = _records(p, 20, 3)
+    sh = _records(p, 10, 4, np.complex128)
+    dst = cat.kind_dst(cat.TSGT_SH, 10)
+    scale = np.linspace(0.5, 1.5, 10)
+    got = _run(p, [(psv, None, None), (sh, dst, scale)], DIST)
+    want = _oracle(p, [(psv, np.arange(20), np.ones(20)), (sh, dst, scale)], DIST)
+    assert rel_l2(got, want) <= TOL
+
+
+@pytest.mark.gpu
+def test_catalogue_batches_and_device_pointers(built):
+    import torch
+    p = _params(np1=8192, iwin_end=300)
+    rng = np.random.default_rng(9)
+    dist = rng.uniform(-1.0, 31.0, 40)
+    coef = rng.standard_normal((40, 5, 20))
+    rec = _records(p, 20, 6)
+    one = _run(p, [(rec, None, None)], dist, coef)
+    split = _run(p, [(rec, None, None)], dist, coef, batch_bytes=1 << 20)   # one point per batch
+    assert rel_l2(split, one) <= 1e-13
+    c = dsmsgt.Catalogue(p)
+    drec = torch.from_numpy(rec).cuda()
+    c.add(drec)
+    dout = torch.empty((40, 5, p["iwin_end"] - p["iwin_start"] + 1), dtype=torch.float64, device="cuda")
+    c.series(dist, coef, out=dout)
+    torch.cuda.synchronize()
+    assert np.array_equal(dout.cpu().numpy(), one)
+    c.clear()
+    with pytest.raises(dsmsgt.DsmError, match="no record set"):
+        c.series(dist, coef)
+    c.close()
+    want = _oracle(p, [(rec, np.arange(20), np.ones(20))], dist[:6], coef[:6])
+    assert rel_l2(one[:6], want) <= TOL
+
+
+def _full_params():
+    np1, shz, s0, s1 = dsmsgt.cat_np1(3276.8, 2048, 2.0, 400.0, 1000.0)
+    return dict(num=20, theta_n=1441, theta_min=0.0, theta_delta=0.125, fmin=0, fmax=2048, np1=np1,
+                tlen=3276.8, omegai=np.log(100.0) / 3276.8, ipdistance=10.0, c_red_reci=0.0,
+                iwin_start=s0, iwin_end=s1)
+
+
+@pytest.mark.gpu
+def test_catalogue_full_size_sampled_points_and_linearity(built):
+    """1441 distances x 2049 frequencies x 20 components, 1681 points, 6
+    outputs each: three interior points against the oracle (run on the 81
+    catalogue distances around each), and linearity in the records."""
+    import torch
+    p = _full_params()
+    rng = np.random.default_rng(11)
+    P = 1681
+    dist = np.sort(rng.uniform(30.0, 90.0, P))
+    coef = rng.standard_normal((P, 6, 20))
+    g = torch.Generator(device="cuda").manual_seed(0)
+    shp = (p["fmax"] + 1, p["theta_n"], 20)
+    r1 = torch.randn(shp, dtype=torch.complex128, device="cuda", generator=g)
+    r2 = torch.randn(shp, dtype=torch.complex128, device="cuda", generator=g)
+    out = {}
+    for name, recs in (("a", [r1]), ("b", [r2]), ("ab", [r1 + 2.0 * r2])):
+        c = dsmsgt.Catalogue(p)
+        for r in recs:
+            c.add(r)
+        out[name] = c.series(dist, coef)
+        c.close()
+    assert np.all(np.isfinite(out["ab"]))
+    assert rel_l2(out["ab"], out["a"] + 2.0 * out["b"]) <= 1e-12
+    r1h = r1.cpu().numpy()
+    for k in (0, P // 2, P - 1):
+        ids = int(dist[k] / p["theta_delta"]) - 40         # window of +-40 catalogue distances (0-based)
+        q = dict(p, theta_n=81, theta_min=ids * p["theta_delta"])
+        sub = r1h[:, ids:ids + 81, :]
+        want = _oracle(q, [(sub, np.arange(20), np.ones(20))], [dist[k]], coef[k:k + 1])
+        assert rel_l2(out["a"][k:k + 1], want) <= TOL, k
