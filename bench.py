@@ -55,15 +55,19 @@ WORKLOADS = {
 }
 
 
-# DRAM bytes per launch of a kernel on a workload's step (mean of the two
-# warm-up steps), from an ncu capture of the bench's own launches of
-# dram__bytes_read.sum + dram__bytes_write.sum (profiles/dram_traffic_psv1024.md).
+# DRAM bytes per launch of a kernel on a workload's step, from an ncu
+# capture of the bench's own launches of dram__bytes_read.sum +
+# dram__bytes_write.sum (psv1024: mean of the two warm-up steps,
+# profiles/dram_traffic_psv1024.md).
 TRAFFIC = {
     ("psv1024", "lsum_tc"): 14.07e9,
     ("psv1024", "psv_factor"): 21.44e9,
     ("psv1024", "psv_substitution"): 25.09e9,
     ("psv1024", "psv_fields"): 11.49e9,
     ("psv1024", "lsum_split"): 12.45e9,
+    # catalogue workload, one launch each (profiles/k_cat_interp_catalogue1681.md)
+    ("catalogue", "cat_interp"): 0.672e9,
+    ("catalogue", "cat_omega"): 0.598e9,
 }
 
 
@@ -362,14 +366,15 @@ def catalogue_bench(args):
         if fk > 0:
             ach = fk / (tk / 1e3) / 1e12
             rooflines[name] = {"kernel": name, "bound": "fp64", "achieved": ach, "peak": fp64,
-                               "unit": "TFLOP/s (algorithmic)", "frac": ach / fp64, "traffic": None,
+                               "unit": "TFLOP/s (algorithmic)", "frac": ach / fp64,
+                               "traffic": TRAFFIC.get(("catalogue", name)),
                                "peak_source": "measured (FP64 FMA and tensor-core probes, this run; the larger)",
                                "avg_launch_ms": tk / max(nk, 1)}
         else:
             ach = bk / (tk / 1e3) / 1e9
             peak = peaks.get("hbm_gbs", 6650.0)
             rooflines[name] = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                               "frac": ach / peak, "traffic": None,
+                               "frac": ach / peak, "traffic": TRAFFIC.get(("catalogue", name)),
                                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                                "avg_launch_ms": tk / max(nk, 1)}
     roof = rooflines[max(kst.items(), key=lambda kv: kv[1][0])[0]]

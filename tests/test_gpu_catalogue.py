@@ -157,3 +157,36 @@ def test_catalogue_full_size_sampled_points_and_linearity(built):
         sub = r1h[:, ids:ids + 81, :]
         want = _oracle(q, [(sub, np.arange(20), np.ones(20))], [dist[k]], coef[k:k + 1])
         assert rel_l2(out["a"][k:k + 1], want) <= TOL, k
+
+
+@pytest.mark.gpu
+def test_catalogue_rejects_bad_calls_and_stays_usable(built):
+    """Errors come back as codes with a message, and the handle still works
+    afterwards: a fifth record set, a destination outside the components,
+    two record components on one destination, non-finite distances and
+    coefficients, more than 64 outputs."""
+    p = _params()
+    rec = _records(p, 20, 7)
+    c = dsmsgt.Catalogue(p)
+    for _ in range(4):
+        c.add(rec)
+    with pytest.raises(dsmsgt.DsmError, match="at most 4"):
+        c.add(rec)
+    c.clear()
+    with pytest.raises(dsmsgt.DsmError, match="out of range"):
+        c.add(rec[:, :, :2], dst=[0, 20])
+    with pytest.raises(dsmsgt.DsmError, match="one destination"):
+        c.add(rec[:, :, :2], dst=[3, 3])
+    c.add(rec)
+    with pytest.raises(dsmsgt.DsmError, match="non-finite distance"):
+        c.series([1.0, float("nan")])
+    coef = np.ones((2, 3, 20))
+    coef[1, 2, 5] = np.inf
+    with pytest.raises(dsmsgt.DsmError, match="non-finite coefficient"):
+        c.series([1.0, 2.0], coef)
+    with pytest.raises(dsmsgt.DsmError, match="nout"):
+        c.series([1.0], np.ones((1, 65, 20)))
+    got = c.series(DIST)
+    c.close()
+    want = _oracle(p, [(rec, np.arange(20), np.ones(20))], DIST)
+    assert rel_l2(got, want) <= TOL
