@@ -79,7 +79,7 @@ struct Tile {
 };
 
 struct InterpArgs {
-    int num, nout, identity;
+    int num, nout, identity, ntile;
     int fmin, fmax, np1, ucov;   // ucov: rows of om per frequency
     double tlen, c_red_reci;
     const Tile* tiles;
@@ -119,7 +119,8 @@ struct OmegaArgs {
     cd* om;   // [nf][urows][nump]
 };
 
-// grid (ceil(urows * nump / 256), nf): one thread per (distance, component).
+// grid (ceil(urows * nump / 256), min(nf, 65535)): one thread per (distance,
+// component), frequencies strided by the grid height.
 // The per-component set tables are copied to shared memory first: threads of
 // a warp index them by different components, which kernel-parameter memory
 // would serve one address at a time.
@@ -132,32 +133,33 @@ __global__ void __launch_bounds__(256) k_cat_omega(const OmegaArgs a) {
         scale_s[s][d] = s < a.nset ? a.set[s].scale[d] : 0.0;
     }
     __syncthreads();
-    const int k = blockIdx.y;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= a.urows * a.nump) return;
     const int d = j % a.nump, u = j / a.nump;
-    const int n = a.fmin + k;
-    cd om = mk(0.0);
-    if (d < a.num && n != 0 && u < a.ucov) {
-        const size_t base = (size_t)k * a.theta_n + (a.u0 + u);
-        cd ph = mk(1.0);
-        const bool reduce = a.c_red_reci != 0.0;
-        if (reduce) {
-            const double th = a.theta_min + (double)(a.u0 + u) * a.theta_delta;
-            const double redtime = -th * a.c_red_reci;
-            ph = expi(-(2.0 * kPi * (double)n / a.tlen * redtime));
+    for (int k = blockIdx.y; k < a.nf; k += gridDim.y) {   // frequencies, strided by the grid height
+        const int n = a.fmin + k;
+        cd om = mk(0.0);
+        if (d < a.num && n != 0 && u < a.ucov) {
+            const size_t base = (size_t)k * a.theta_n + (a.u0 + u);
+            cd ph = mk(1.0);
+            const bool reduce = a.c_red_reci != 0.0;
+            if (reduce) {
+                const double th = a.theta_min + (double)(a.u0 + u) * a.theta_delta;
+                const double redtime = -th * a.c_red_reci;
+                ph = expi(-(2.0 * kPi * (double)n / a.tlen * redtime));
+            }
+            for (int s = 0; s < a.nset; ++s) {
+                const SetDev& S = a.set[s];
+                const int c = src_s[s][d];
+                if (c < 0) continue;
+                cd t = load_rec(S, base * S.ncomp + c) * scale_s[s][c];
+                if (reduce) t = t * ph;
+                t = t * 1.0e-21;
+                om = om + t;   // the first set adds to an exact zero
+            }
         }
-        for (int s = 0; s < a.nset; ++s) {
-            const SetDev& S = a.set[s];
-            const int c = src_s[s][d];
-            if (c < 0) continue;
-            cd t = load_rec(S, base * S.ncomp + c) * scale_s[s][c];
-            if (reduce) t = t * ph;
-            t = t * 1.0e-21;
-            om = om + t;   // the first set adds to an exact zero
-        }
+        a.om[((size_t)k * a.urows + u) * a.nump + d] = om;
     }
-    a.om[((size_t)k * a.urows + u) * a.nump + d] = om;
 }
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
@@ -208,8 +210,9 @@ __global__ void __launch_bounds__(CAT_THREADS, C <= 5 ? 4 : 2) k_cat_interp(cons
     constexpr size_t OM_D = (size_t)2 * CAT_WARPS * KC * SS, EP_D = (size_t)CAT_WARPS * (PT * NUMP + 1) * 2;
     double* Om = reinterpret_cast<double*>(smem);                            // [2][CAT_WARPS][KC][SS]
     double* Wc = Om + (OM_D > EP_D ? OM_D : EP_D);                            // [2][KC][WS]
-    const Tile tl = a.tiles[blockIdx.x];
-    const int n0 = blockIdx.y * CAT_WARPS;
+    // one-dimensional grid, tiles fastest: block b = frequency block * ntile + tile
+    const Tile tl = a.tiles[blockIdx.x % a.ntile];
+    const int n0 = (int)(blockIdx.x / a.ntile) * CAT_WARPS;
     const int nh = a.np1 + 1;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = lane >> 2, t = lane & 3;
@@ -702,7 +705,7 @@ extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, 
         oa.om = c->om.p;
         if (prof) DSM_CUDA(cudaEventRecord(c->ev[6], c->st));
         need((size_t)urows * nump < (1u << 30), "dsm_cat_series: catalogue rows too large");
-        k_cat_omega<<<dim3((urows * nump + 255) / 256, nf), 256, 0, c->st>>>(oa);
+        k_cat_omega<<<dim3((urows * nump + 255) / 256, std::min(nf, 65535)), 256, 0, c->st>>>(oa);
         DSM_CUDA(cudaGetLastError());
         if (prof) DSM_CUDA(cudaEventRecord(c->ev[7], c->st));
         S.launches += 1;
@@ -731,8 +734,10 @@ extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, 
             a.dist = c->dist.p + b0;
             a.orig = c->orig.p + b0;
             if (prof) DSM_CUDA(cudaEventRecord(c->ev[1], c->st));
-            dim3 grid(tile_begin[bi + 1] - tile_begin[bi], (nh + CAT_WARPS - 1) / CAT_WARPS);
-            launch_interp_c(nump / 4, a, grid, smem, c->st);
+            a.ntile = tile_begin[bi + 1] - tile_begin[bi];
+            const long long nblk = (long long)a.ntile * ((nh + CAT_WARPS - 1) / CAT_WARPS);
+            need(nblk < (1LL << 31), "dsm_cat_series: too many point tiles x frequency blocks in one batch");
+            launch_interp_c(nump / 4, a, dim3((unsigned)nblk), smem, c->st);
             if (prof) DSM_CUDA(cudaEventRecord(c->ev[2], c->st));
             const int nb = np_ * nout;
             DSM_CUFFT(cufftExecZ2D(c->plan(nb), reinterpret_cast<cufftDoubleComplex*>(c->h.p),

@@ -190,3 +190,18 @@ def test_catalogue_rejects_bad_calls_and_stays_usable(built):
     c.close()
     want = _oracle(p, [(rec, np.arange(20), np.ones(20))], DIST)
     assert rel_l2(got, want) <= TOL
+
+
+@pytest.mark.gpu
+def test_catalogue_long_transform_and_many_frequencies(built):
+    """A transform of 2^19 samples (np1 = 2^18) over 70 001 frequencies: more
+    frequency blocks and more frequencies than one grid dimension of 65 535
+    holds, on a small catalogue (9 distances, 4 components, 2 points)."""
+    p = _params(num=4, theta_n=9, theta_min=10.0, fmin=0, fmax=70000, np1=1 << 18, tlen=1000.0,
+                omegai=np.log(100.0) / 1000.0, ipdistance=2.0, iwin_start=100, iwin_end=160)
+    rec = _records(p, 4, 8)
+    dist = [11.3, 12.75]
+    got = _run(p, [(rec, None, None)], dist)
+    want = _oracle(p, [(rec, np.arange(4), np.ones(4))], dist)
+    assert got.shape == (2, 4, 61)
+    assert rel_l2(got, want) <= TOL
