@@ -594,7 +594,11 @@ __device__ __forceinline__ void fwd_row(int k, const StepOut& so, FwdState& F, c
 // forward-substitution state, which keeps the registers of that (long) part
 // down.
 constexpr int FAC_THREADS = 128;
-constexpr int FAC_CH = 16;  // rows per chunk (multiple of 4)
+#ifndef DSM_FAC_CH
+#define DSM_FAC_CH 16
+#endif
+constexpr int FAC_CH = DSM_FAC_CH;  // rows per chunk (multiple of 4)
+static_assert(FAC_CH % 4 == 0, "chunks hold whole groups of four steps");
 constexpr int FAC_NW = 4;   // frequencies staged per block
 
 template <bool FAST>
@@ -1426,15 +1430,20 @@ __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restric
 // Per (omega, l >= 1, receiver group): receiver fields of every slot and the
 // cutoff probe (group 0).
 // Fields of every slot at the receivers, one thread per (system, receiver):
-// a warp holds 8 consecutive systems (orders) x 4 receivers, so each
-// coefficient load serves four receivers and each field store writes 8
-// consecutive orders of one row.  Values and radial derivatives of the six
+// a warp holds FLD_SYS consecutive systems (orders) x FLD_REC receivers, so
+// each coefficient load serves FLD_REC receivers and each field store writes
+// FLD_SYS consecutive orders of one row (16 x 2 measured fastest of 4 x 8,
+// 8 x 4 and 16 x 2 on the benchmark; the results do not depend on it).  Values and radial derivatives of the six
 // basis solutions come from the three-node weights (interpolate, calup),
 // then U, V and derivatives of each slot are their combinations with the
 // source coefficients.  Block row 0 also writes the cutoff probe (calamp of
 // imt = 1, m = 0 at the top receiver's stencil); the last block row holds
 // the surface (rows n-1, n).
-constexpr int FLD_SYS = 8, FLD_REC = 4;
+#ifndef DSM_FLD_SYS
+#define DSM_FLD_SYS 16
+#endif
+constexpr int FLD_SYS = DSM_FLD_SYS, FLD_REC = 32 / FLD_SYS;
+static_assert(FLD_SYS * FLD_REC == 32, "a warp is FLD_SYS systems x FLD_REC receivers");
 
 // acc + r x for a real r: FAST with fused multiply-adds
 template <bool FAST>
@@ -1451,8 +1460,8 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
                                                     T* __restrict__ A0f, T* __restrict__ A1f, T* __restrict__ A2f,
                                                     int Lcap, double* __restrict__ amps) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int sys = (blockIdx.x * 4 + warp) * FLD_SYS + (lane & (FLD_SYS - 1));
-    const int r = blockIdx.y * FLD_REC + (lane >> 3);
+    const int sys = (blockIdx.x * 4 + warp) * FLD_SYS + lane % FLD_SYS;
+    const int r = blockIdx.y * FLD_REC + lane / FLD_SYS;
     const int R = d.R;
     if (sys >= nsys || r > R) return;
     int w, l;
