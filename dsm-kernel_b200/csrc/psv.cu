@@ -1432,15 +1432,16 @@ __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restric
 // Fields of every slot at the receivers, one thread per (system, receiver):
 // a warp holds FLD_SYS consecutive systems (orders) x FLD_REC receivers, so
 // each coefficient load serves FLD_REC receivers and each field store writes
-// FLD_SYS consecutive orders of one row (16 x 2 measured fastest of 4 x 8,
-// 8 x 4 and 16 x 2 on the benchmark; the results do not depend on it).  Values and radial derivatives of the six
+// FLD_SYS consecutive orders of one row (32 x 1 measured fastest of 4 x 8,
+// 8 x 4, 16 x 2 and 32 x 1 on the benchmark; the results do not depend on
+// it).  Values and radial derivatives of the six
 // basis solutions come from the three-node weights (interpolate, calup),
 // then U, V and derivatives of each slot are their combinations with the
 // source coefficients.  Block row 0 also writes the cutoff probe (calamp of
 // imt = 1, m = 0 at the top receiver's stencil); the last block row holds
 // the surface (rows n-1, n).
 #ifndef DSM_FLD_SYS
-#define DSM_FLD_SYS 16
+#define DSM_FLD_SYS 32
 #endif
 constexpr int FLD_SYS = DSM_FLD_SYS, FLD_REC = 32 / FLD_SYS;
 static_assert(FLD_SYS * FLD_REC == 32, "a warp is FLD_SYS systems x FLD_REC receivers");
