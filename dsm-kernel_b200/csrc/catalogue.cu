@@ -91,6 +91,7 @@ struct InterpArgs {
     const int* orig;       // the caller's index of the point
     const double* coef;    // [caller point][nout][num] or null (identity)
     cd* h;                 // [sorted position][nout][np1+1]
+    cd* spec;              // spectra mode: [caller point][nout][fmax-fmin+1], else null
 };
 
 __device__ __forceinline__ cd load_rec(const SetDev& s, size_t idx) {
@@ -107,6 +108,16 @@ __device__ __forceinline__ cd expi(double arg) {
     double sn, cs;
     sincos(arg, &sn, &cs);
     return cd{cs, sn};
+}
+
+// H_n of the reference's extended vector x (vectorFFT_double, fourier.f90:430-439)
+// from the spectrum value v at index n (zero outside fmin..fmax):
+// x_n + conj(x_{N-n}) = 2 v where the extension mirrors n, v where it leaves
+// zeros (n > np1 - fmin), and the real part at n = 0 and n = np1
+__device__ __forceinline__ cd herm_proj(cd v, int n, int np1, int fmin) {
+    if (n == 0 || n == np1) return cd{v.re, 0.0};
+    if (n <= np1 - fmin) return v;
+    return v * 0.5;
 }
 
 // rdsgtomega (fourier.f90:87-116) on catalogue distances [u0, u0 + Ucov):
@@ -322,11 +333,24 @@ __global__ void __launch_bounds__(CAT_THREADS, C <= 5 ? 4 : 2) k_cat_interp(cons
                 }
             }
         }
-        cd hv;
-        if (nn == 0 || nn == a.np1) hv = cd{v.re, 0.0};
-        else if (nn <= a.np1 - a.fmin) hv = v;
-        else hv = v * 0.5;
-        a.h[((size_t)(tl.p0 + pl) * a.nout + j) * nh + nn] = hv;
+        if (a.spec) {  // spectra mode: the combined spectrum itself, frequencies fmin..fmax
+            if (nn >= a.fmin && nn <= a.fmax)
+                a.spec[((size_t)a.orig[tl.p0 + pl] * a.nout + j) * (a.fmax - a.fmin + 1) + (nn - a.fmin)] = v;
+            continue;
+        }
+        a.h[((size_t)(tl.p0 + pl) * a.nout + j) * nh + nn] = herm_proj(v, nn, a.np1, a.fmin);
+    }
+}
+
+// Hermitian projection H_n (n = 0..np1) of arbitrary spectra x[b][n - fmin]
+// (vectorFFT_double's input ccvec), rows of h np1 + 1 apart
+__global__ void k_cat_herm(const cd* __restrict__ x, int nb, int fmin, int fmax, int np1, cd* __restrict__ h) {
+    const int nh = np1 + 1;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nh) return;
+    for (int b = blockIdx.y; b < nb; b += gridDim.y) {
+        const cd v = (n >= fmin && n <= fmax) ? x[(size_t)b * (fmax - fmin + 1) + (n - fmin)] : mk(0.0);
+        h[(size_t)b * nh + n] = herm_proj(v, n, np1, fmin);
     }
 }
 
@@ -369,6 +393,7 @@ struct dsm_cat {
     DBuf<Tile> tiles;
     DBuf<double> wt, norm, dist, coef, e, out;
     DBuf<cd> om;     // frequency-domain SGT of the covered catalogue distances
+    DBuf<cd> spec;   // spectra copied in or out (dsm_cat_spectra, dsm_cat_transform)
     DBuf<cd> h;
     std::vector<double> he;
     std::map<int, cufftHandle> plans;   // batch -> plan
@@ -562,16 +587,21 @@ void launch_interp_c(int C, const InterpArgs& a, dim3 grid, size_t smem, cudaStr
 }
 }  // namespace
 
-extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, int nout, const double* coef,
-                              double* out, int out_on_device) {
+namespace {
+// Points of dsm_cat_series (time series, spectra = false) and of
+// dsm_cat_spectra (the combined spectra before the transform, spectra =
+// true: out is complex128 [point][nout][fmax-fmin+1]).
+int cat_points(dsm_cat_t* c, int npoint, const double* distance, int nout, const double* coef, void* out,
+               int out_on_device, bool spectra) {
     if (!c) return DSM_ERR_INVALID;
+    const std::string fn = spectra ? "dsm_cat_spectra" : "dsm_cat_series";
     return cat_guard(c, [&] {
         const dsm_cat_params_t& p = c->p;
-        need(npoint >= 0 && (npoint == 0 || (distance && out)), "dsm_cat_series: null argument");
-        need(!c->sets.empty(), "dsm_cat_series: no record set added");
+        need(npoint >= 0 && (npoint == 0 || (distance && out)), fn + ": null argument");
+        need(!c->sets.empty(), fn + ": no record set added");
         const bool identity = coef == nullptr;
         if (identity) nout = p.num;
-        need(nout >= 1 && nout <= MAX_OUT, "dsm_cat_series: nout must be in [1, 64]");
+        need(nout >= 1 && nout <= MAX_OUT, fn + ": nout must be in [1, 64]");
         if (npoint == 0) return;
         DSM_CUDA(cudaSetDevice(c->dev));
         const int nh = p.np1 + 1, nwin = c->nwin();
@@ -582,9 +612,9 @@ extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, 
         std::vector<double> ww((size_t)npoint * nwmax, 0.0), wnorm(npoint);
         for (int k = 0; k < npoint; ++k) {
             const double dk = distance[k];
-            need(std::isfinite(dk), "dsm_cat_series: non-finite distance");
+            need(std::isfinite(dk), fn + ": non-finite distance");
             const double q = (dk - p.theta_min) / p.theta_delta;
-            need(std::fabs(q) < 1e9, "dsm_cat_series: distance far outside the catalogue");
+            need(std::fabs(q) < 1e9, fn + ": distance far outside the catalogue");
             const int idelta = 1 + (int)q;   // Fortran int(): truncation toward zero
             int is, ie;
             idelta_region(idelta, nhregion, p.theta_n, is, ie);
@@ -598,12 +628,12 @@ extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, 
                 ww[(size_t)k * nwmax + (kk - is)] = wv;
                 nrm = nrm + wv;
             }
-            need(nrm != 0.0 && std::isfinite(nrm), "dsm_cat_series: sinc weights sum to zero");
+            need(nrm != 0.0 && std::isfinite(nrm), fn + ": sinc weights sum to zero");
             wnorm[k] = nrm;
         }
         if (!identity)
             for (size_t i = 0; i < (size_t)npoint * nout * p.num; ++i)
-                need(std::isfinite(coef[i]), "dsm_cat_series: non-finite coefficient");
+                need(std::isfinite(coef[i]), fn + ": non-finite coefficient");
         // points sorted by window start (then distance); per-point arrays in that order
         std::vector<int> ord(npoint);
         std::iota(ord.begin(), ord.end(), 0);
@@ -677,14 +707,20 @@ extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, 
         c->orig.upload(ord.data(), npoint, c->st);
         c->tiles.upload(tiles.data(), tiles.size(), c->st);
         if (!identity) c->coef.upload(coef, (size_t)npoint * nout * p.num, c->st);
-        double* dout = out;
-        if (!out_on_device) {
-            c->out.reserve((size_t)npoint * nout * nwin);
-            dout = c->out.p;
-        }
-        c->h.reserve((size_t)pc * nout * nh);
-
         const int nf = p.fmax - p.fmin + 1;
+        double* dout = static_cast<double*>(out);
+        cd* dspec = static_cast<cd*>(out);
+        if (!out_on_device) {
+            if (spectra) {
+                c->spec.reserve((size_t)npoint * nout * nf);
+                dspec = c->spec.p;
+            } else {
+                c->out.reserve((size_t)npoint * nout * nwin);
+                dout = c->out.p;
+            }
+        }
+        if (!spectra) c->h.reserve((size_t)pc * nout * nh);
+
         const int urows = ucov + 4;
         c->om.reserve((size_t)nf * urows * nump);
         OmegaArgs oa{};
@@ -704,7 +740,7 @@ extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, 
         oa.c_red_reci = p.c_red_reci;
         oa.om = c->om.p;
         if (prof) DSM_CUDA(cudaEventRecord(c->ev[6], c->st));
-        need((size_t)urows * nump < (1u << 30), "dsm_cat_series: catalogue rows too large");
+        need((size_t)urows * nump < (1u << 30), fn + ": catalogue rows too large");
         k_cat_omega<<<dim3((urows * nump + 255) / 256, std::min(nf, 65535)), 256, 0, c->st>>>(oa);
         DSM_CUDA(cudaGetLastError());
         if (prof) DSM_CUDA(cudaEventRecord(c->ev[7], c->st));
@@ -724,6 +760,7 @@ extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, 
         a.wt = c->wt.p;
         a.coef = identity ? nullptr : c->coef.p;
         a.h = c->h.p;
+        a.spec = spectra ? dspec : nullptr;
         const size_t smem = interp_smem_bytes(nump / 4);
         double ms_i = 0, ms_f = 0, ms_w = 0;
         int nbatch = 0;
@@ -736,9 +773,20 @@ extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, 
             if (prof) DSM_CUDA(cudaEventRecord(c->ev[1], c->st));
             a.ntile = tile_begin[bi + 1] - tile_begin[bi];
             const long long nblk = (long long)a.ntile * ((nh + CAT_WARPS - 1) / CAT_WARPS);
-            need(nblk < (1LL << 31), "dsm_cat_series: too many point tiles x frequency blocks in one batch");
+            need(nblk < (1LL << 31), fn + ": too many point tiles x frequency blocks in one batch");
             launch_interp_c(nump / 4, a, dim3((unsigned)nblk), smem, c->st);
             if (prof) DSM_CUDA(cudaEventRecord(c->ev[2], c->st));
+            if (spectra) {
+                S.launches += 1;
+                ++nbatch;
+                if (prof) {
+                    DSM_CUDA(cudaEventSynchronize(c->ev[2]));
+                    float t1;
+                    cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]);
+                    ms_i += t1;
+                }
+                continue;
+            }
             const int nb = np_ * nout;
             DSM_CUFFT(cufftExecZ2D(c->plan(nb), reinterpret_cast<cufftDoubleComplex*>(c->h.p),
                                    reinterpret_cast<cufftDoubleReal*>(c->h.p)));
@@ -762,9 +810,14 @@ extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, 
                 ms_w += t3;
             }
         }
-        if (!out_on_device)
-            DSM_CUDA(cudaMemcpyAsync(out, dout, (size_t)npoint * nout * nwin * sizeof(double), cudaMemcpyDeviceToHost,
-                                     c->st));
+        if (!out_on_device) {
+            if (spectra)
+                DSM_CUDA(cudaMemcpyAsync(out, dspec, (size_t)npoint * nout * nf * sizeof(cd), cudaMemcpyDeviceToHost,
+                                         c->st));
+            else
+                DSM_CUDA(cudaMemcpyAsync(out, dout, (size_t)npoint * nout * nwin * sizeof(double),
+                                         cudaMemcpyDeviceToHost, c->st));
+        }
         if (prof) DSM_CUDA(cudaEventRecord(c->ev[5], c->st));
         DSM_CUDA(cudaStreamSynchronize(c->st));
         if (prof) {
@@ -804,6 +857,63 @@ extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, 
             }
             S.nk = 4;
         }
+    });
+}
+}  // namespace
+
+extern "C" int dsm_cat_series(dsm_cat_t* c, int npoint, const double* distance, int nout, const double* coef,
+                              double* out, int out_on_device) {
+    return cat_points(c, npoint, distance, nout, coef, out, out_on_device, false);
+}
+
+extern "C" int dsm_cat_spectra(dsm_cat_t* c, int npoint, const double* distance, int nout, const double* coef,
+                               void* out, int out_on_device) {
+    return cat_points(c, npoint, distance, nout, coef, out, out_on_device, true);
+}
+
+extern "C" int dsm_cat_transform(dsm_cat_t* c, int nseries, const void* spectra, int spectra_on_device,
+                                 double* out, int out_on_device) {
+    if (!c) return DSM_ERR_INVALID;
+    return cat_guard(c, [&] {
+        const dsm_cat_params_t& p = c->p;
+        need(nseries >= 0 && (nseries == 0 || (spectra && out)), "dsm_cat_transform: null argument");
+        if (nseries == 0) return;
+        DSM_CUDA(cudaSetDevice(c->dev));
+        const int nh = p.np1 + 1, nwin = c->nwin(), nf = p.fmax - p.fmin + 1;
+        if (spectra_on_device)
+            need(((uintptr_t)spectra % 16) == 0, "dsm_cat_transform: misaligned device spectra");
+        // series per batch: the in-place transform buffer stays under max_batch_bytes
+        const int pc = (int)std::min<size_t>((size_t)nseries, std::max<size_t>(1, c->max_batch_bytes / (nh * sizeof(cd))));
+        const cd* dx = static_cast<const cd*>(spectra);
+        if (!spectra_on_device) {
+            c->spec.upload(static_cast<const cd*>(spectra), (size_t)nseries * nf, c->st);
+            dx = c->spec.p;
+        }
+        double* dout = out;
+        if (!out_on_device) {
+            c->out.reserve((size_t)nseries * nwin);
+            dout = c->out.p;
+        }
+        c->h.reserve((size_t)pc * nh);
+        std::vector<int> iota_h(pc);
+        std::iota(iota_h.begin(), iota_h.end(), 0);
+        c->orig.upload(iota_h.data(), pc, c->st);
+        for (int b0 = 0; b0 < nseries; b0 += pc) {
+            const int nb = std::min(pc, nseries - b0);
+            k_cat_herm<<<dim3((nh + 255) / 256, std::min(nb, 65535)), 256, 0, c->st>>>(dx + (size_t)b0 * nf, nb, p.fmin,
+                                                                                      p.fmax, p.np1, c->h.p);
+            DSM_CUDA(cudaGetLastError());
+            DSM_CUFFT(cufftExecZ2D(c->plan(nb), reinterpret_cast<cufftDoubleComplex*>(c->h.p),
+                                   reinterpret_cast<cufftDoubleReal*>(c->h.p)));
+            const size_t total = (size_t)nb * nwin;
+            const int blocks = (int)std::min<size_t>((total + 255) / 256, (size_t)148 * 16);
+            k_cat_window<<<blocks, 256, 0, c->st>>>(reinterpret_cast<const double*>(c->h.p), 2 * nh, p.iwin_start,
+                                                    nwin, nb, 1, c->orig.p, c->e.p, p.tlen, dout + (size_t)b0 * nwin);
+            DSM_CUDA(cudaGetLastError());
+        }
+        if (!out_on_device)
+            DSM_CUDA(cudaMemcpyAsync(out, dout, (size_t)nseries * nwin * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        DSM_CUDA(cudaStreamSynchronize(c->st));
     });
 }
 

@@ -168,6 +168,8 @@ def lib() -> C.CDLL:
         L.dsm_cat_add.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, _ip, _dp, C.c_int]
         L.dsm_cat_clear.argtypes = [C.c_void_p]
         L.dsm_cat_series.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_void_p, C.c_int]
+        L.dsm_cat_spectra.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_void_p, C.c_int]
+        L.dsm_cat_transform.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
         L.dsm_cat_set_profiling.argtypes = [C.c_void_p, C.c_int]
         L.dsm_cat_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.dsm_cat_set_batch_bytes.argtypes = [C.c_void_p, C.c_size_t]
@@ -524,6 +526,30 @@ class Catalogue:
                                   None if cf is None else _ptr(cf, _dp), C.c_void_p(optr), on_dev)
         self._check(rc, "dsm_cat_series")
         return res
+
+    def spectra(self, distances, coef=None):
+        """Combined spectra [npoint][nout][fmax-fmin+1] (complex128) before the
+        transform (dsm_cat_spectra)."""
+        d = np.ascontiguousarray(distances, np.float64)
+        cf = None if coef is None else np.ascontiguousarray(coef, np.float64)
+        nout = self.p["num"] if cf is None else cf.shape[1]
+        nf = self.p["fmax"] - self.p["fmin"] + 1
+        res = np.zeros((d.size, nout, nf), np.complex128)
+        rc = lib().dsm_cat_spectra(self.h, d.size, _ptr(d, _dp), nout,
+                                   None if cf is None else _ptr(cf, _dp), C.c_void_p(res.ctypes.data), 0)
+        self._check(rc, "dsm_cat_spectra")
+        return res
+
+    def transform(self, spectra):
+        """vectorFFT_double of spectra [nseries][fmax-fmin+1] (complex128):
+        windowed time series [nseries][nwin] (dsm_cat_transform)."""
+        x = np.ascontiguousarray(spectra, np.complex128)
+        x2 = x.reshape(-1, x.shape[-1])
+        res = np.zeros((x2.shape[0], self.nwin), np.float64)
+        rc = lib().dsm_cat_transform(self.h, x2.shape[0], C.c_void_p(x2.ctypes.data), 0,
+                                     C.c_void_p(res.ctypes.data), 0)
+        self._check(rc, "dsm_cat_transform")
+        return res.reshape(x.shape[:-1] + (self.nwin,))
 
     def set_profiling(self, on: bool):
         self._check(lib().dsm_cat_set_profiling(self.h, int(on)), "dsm_cat_set_profiling")

@@ -377,6 +377,23 @@ int dsm_cat_clear(dsm_cat_t *cat);
 int dsm_cat_series(dsm_cat_t *cat, int npoint, const double *distance, int nout,
                    const double *coef, double *out, int out_on_device);
 
+/* The same points' combined spectra before the transform: out holds
+ * complex128 [point][j][fmax-fmin+1] for frequency indices fmin..fmax (index
+ * 0 is zero).  These are clsgt's interpolated SGT (fourier.f90:128-162)
+ * combined per point, e.g. the h3 / h4 sums that KernelMaker's kernel
+ * formulas multiply frequency by frequency before their transform
+ * (src/KernelMaker/calculateK.f90:237-323, isovpfreq). */
+int dsm_cat_spectra(dsm_cat_t *cat, int npoint, const double *distance, int nout,
+                    const double *coef, void *out, int out_on_device);
+
+/* vectorFFT_double (src/KernelMaker/fourier.f90:418-450) of nseries arbitrary
+ * spectra, complex128 [series][fmax-fmin+1] for indices fmin..fmax: the
+ * Hermitian extension, the length-2 np1 inverse transform and the window
+ * samples times exp(omegai t) / tlen * 1e3, out[series][t].  Needs no record
+ * set. */
+int dsm_cat_transform(dsm_cat_t *cat, int nseries, const void *spectra, int spectra_on_device,
+                      double *out, int out_on_device);
+
 /* Per-stage device time of the last dsm_cat_series when profiling is on:
  * kern[] holds cat_interp, cat_fft, cat_window (ms, launches, algorithmic
  * bytes); ms_total covers the whole call. */

@@ -205,3 +205,36 @@ def test_catalogue_long_transform_and_many_frequencies(built):
     want = _oracle(p, [(rec, np.arange(4), np.ones(4))], dist)
     assert got.shape == (2, 4, 61)
     assert rel_l2(got, want) <= TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fmin,c_red", [(0, 0.0), (5, 9.0)])
+def test_catalogue_spectra_and_transform_match_oracle(built, fmin, c_red):
+    """dsm_cat_spectra against the oracle's clsgt plus combination,
+    dsm_cat_transform against its vectorFFT_double (random spectra whose
+    index-0 value is nonzero too), and their composition against
+    dsm_cat_series."""
+    from oracle import catalogue as cat
+    p = _params(fmin=fmin, fmax=64, c_red_reci=c_red)
+    rec = _records(p, 20, 12)
+    rng = np.random.default_rng(13)
+    coef = rng.standard_normal((len(DIST), 6, 20))
+    c = dsmsgt.Catalogue(p)
+    c.add(rec)
+    spec = c.spectra(DIST, coef)
+    series = c.series(DIST, coef)
+    theta = p["theta_min"] + np.arange(p["theta_n"]) * p["theta_delta"]
+    om = cat.omega_sgt([(rec, np.arange(20), np.ones(20))], 20, p["fmin"], p["fmax"], theta, p["tlen"],
+                       p["c_red_reci"])
+    want = np.stack([coef[k] @ cat.clsgt(d, om, p["fmin"], p["theta_min"], p["theta_delta"], p["ipdistance"],
+                                         p["tlen"], p["c_red_reci"]).T for k, d in enumerate(DIST)])
+    assert spec.shape == want.shape
+    assert rel_l2(spec, want) <= TOL
+    assert rel_l2(c.transform(spec), series) <= 1e-12
+    x = rng.standard_normal((5, 65 - fmin)) + 1j * rng.standard_normal((5, 65 - fmin))
+    got = c.transform(x)
+    c.close()
+    ref = cat.vector_fft_double(x, p["fmin"], p["fmax"], p["np1"], p["omegai"], p["tlen"], p["iwin_start"],
+                                p["iwin_end"])
+    assert got.shape == ref.shape
+    assert rel_l2(got, ref) <= TOL
