@@ -16,6 +16,7 @@
 //   4. turns the contractions into TSGT/RSGT/SYNN (mode epilogue kernel)
 //   5. packs complex64 catalogue records when asked.
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -54,10 +55,8 @@ void Engine::init_common(int dev) {
     if (const char* e = std::getenv("DSM_TC_FLAGS")) tc_flags = (uint32_t)std::atoi(e);
     if (const char* e = std::getenv("DSM_TC_BK")) tc_bk = std::atoi(e) == 64 ? 64 : 32;
     if (const char* e = std::getenv("DSM_TC_CHUNK")) tc_chunk = std::max(0, std::atoi(e));
-    if (mixed()) {
-        tc_err.reserve(1);
-        DSM_CUDA(cudaMemset(tc_err.p, 0, sizeof(int)));
-    }
+    dflags.reserve(2);
+    DSM_CUDA(cudaMemset(dflags.p, 0, 2 * sizeof(int)));
 }
 
 Engine::~Engine() {
@@ -249,22 +248,136 @@ void Engine::lsum_group(int w0, int w1, const std::vector<int>& nord) {
         tc::Problem* dp = tcp.p + tcp_next;
         DSM_CUDA(cudaMemcpyAsync(dp, hp.data() + g, sizeof(tc::Problem) * np, cudaMemcpyHostToDevice, st));
         tcp_next += np;
-        tc::launch(tcmaps, dp, np, tiles, tc_fmt, tc_bk, tc_flags, tc_chunk, tc_err.p, nsm, st);
+        const uint32_t fl = tc_flags | (test_tc_stall ? tc::TC_TEST_STALL : 0u);
+        const unsigned long long wait_ns = test_tc_stall ? 20000000ull : tc::WAIT_NS;
+        tc::launch(tcmaps, dp, np, tiles, tc_fmt, tc_bk, fl, tc_chunk, tc_err(), nsm, st, wait_ns);
         launches++;
     }
     kend(id, tc_bytes, tflops);
     // cudaMemcpyAsync from pageable memory has consumed hp when it returns
 }
 
-void Engine::check_tc_error() {
-    if (!mixed()) return;
-    int h = 0;
-    DSM_CUDA(cudaMemcpyAsync(&h, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+// Reads the run's status words (the stream is synchronised here anyway);
+// a set word is cleared and reported, leaving the context usable.
+void Engine::check_device_flags() {
+    int h[2] = {0, 0};
+    DSM_CUDA(cudaMemcpyAsync(h, dflags.p, sizeof(h), cudaMemcpyDeviceToHost, st));
     DSM_CUDA(cudaStreamSynchronize(st));
-    if (h) {
-        DSM_CUDA(cudaMemsetAsync(tc_err.p, 0, sizeof(int), st));
-        throw Error(DSM_ERR_TIMEOUT, "a bounded wait in the tensor-core l-sum gave up");
+    if (h[DEV_WORD_TC] || h[DEV_WORD_STATUS]) {
+        DSM_CUDA(cudaMemsetAsync(dflags.p, 0, sizeof(h), st));
+        DSM_CUDA(cudaStreamSynchronize(st));
     }
+    if (h[DEV_WORD_TC]) throw Error(DSM_ERR_TIMEOUT, "a bounded wait in the tensor-core l-sum gave up");
+    if (h[DEV_WORD_STATUS] & DEV_NONFINITE)
+        throw Error(DSM_ERR_NONFINITE, "an output (TSGT, RSGT or SYNN) became Inf or NaN");
+}
+
+// sums[c][0] += |a - b|^2, sums[c][1] += |b|^2 over npt points of num
+// complex components (component fastest); a thread takes whole points
+__global__ void __launch_bounds__(256) k_cmp_sums(const double2* __restrict__ a, const double2* __restrict__ b,
+                                                  size_t npt, int num, double* __restrict__ sums) {
+    constexpr int NMAX = DSM_PSV_NUM_TSGT;
+    double dd[NMAX], rr[NMAX];
+#pragma unroll
+    for (int c = 0; c < NMAX; ++c) dd[c] = rr[c] = 0.0;
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npt; p += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < NMAX; ++c) {
+            if (c < num) {
+                const double2 x = a[p * num + c], y = b[p * num + c];
+                const double ex = x.x - y.x, ey = x.y - y.y;
+                dd[c] += ex * ex + ey * ey;
+                rr[c] += y.x * y.x + y.y * y.y;
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < NMAX; ++c) {
+        if (c >= num) break;
+        double u = dd[c], v = rr[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            u += __shfl_down_sync(0xffffffffu, u, o);
+            v += __shfl_down_sync(0xffffffffu, v, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&sums[2 * c], u);
+            atomicAdd(&sums[2 * c + 1], v);
+        }
+    }
+}
+
+static void launch_cmp(const double* a, const double* b, size_t npt, int num, double* sums, int nsm,
+                       cudaStream_t st) {
+    if (npt == 0 || num <= 0) return;
+    const unsigned grid = (unsigned)std::min<size_t>((npt + 255) / 256, (size_t)nsm * 4);
+    k_cmp_sums<<<grid, 256, 0, st>>>(reinterpret_cast<const double2*>(a), reinterpret_cast<const double2*>(b),
+                                     npt, num, sums);
+    DSM_CUDA(cudaGetLastError());
+}
+
+void Engine::check_batch(const int* ilist, int b0, int nf, const std::vector<CutState>& hc) {
+    if (!check_ref || check_stride <= 0) return;
+    std::vector<int> sub, pos;
+    for (int w = 0; w < nf; ++w)
+        if ((b0 + w) % check_stride == 0) {
+            sub.push_back(ilist[b0 + w]);
+            pos.push_back(w);
+        }
+    if (sub.empty()) return;
+    DSM_CUDA(cudaEventRecord(ev[6], st));
+    size_t pt, pr, ps;
+    out_sizes(&pt, &pr, &ps);
+    double* sums = acc_sums.p;
+    for (size_t k0 = 0; k0 < sub.size(); k0 += (size_t)check_ref->F) {
+        const int m = (int)std::min<size_t>((size_t)check_ref->F, sub.size() - k0);
+        const void *rt = nullptr, *rr = nullptr, *rs = nullptr;
+        std::vector<int> ll(m);
+        // the FP64 engine synchronises its own stream before it returns
+        check_ref->run(sub.data() + k0, m, nullptr, &rt, &rr, &rs, ll.data());
+        for (int k = 0; k < m; ++k) {
+            const int w = pos[k0 + k];
+            if (ll[k] != hc[w].llog) acc.llog_equal = 0;
+            launch_cmp(out_t.p + 2 * pt * w, static_cast<const double*>(rt) + 2 * pt * k, pt / num_t, num_t, sums,
+                       nsm, st);
+            if (rsgt_sw)
+                launch_cmp(out_r.p + 2 * pr * w, static_cast<const double*>(rr) + 2 * pr * k, pr / num_r, num_r,
+                           sums + 2 * num_t, nsm, st);
+            if (synn_sw)
+                launch_cmp(out_s.p + 2 * ps * w, static_cast<const double*>(rs) + 2 * ps * k, ps / num_s, num_s,
+                           sums + 2 * (num_t + num_r), nsm, st);
+        }
+        // the FP64 engine's next run reuses the buffers just read
+        DSM_CUDA(cudaStreamSynchronize(st));
+    }
+    acc.nfreq += (int)sub.size();
+    DSM_CUDA(cudaEventRecord(ev[7], st));
+    DSM_CUDA(cudaEventSynchronize(ev[7]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev[6], ev[7]);
+    ms_check += ms;
+}
+
+void Engine::finish_accuracy() {
+    if (!check_ref || check_stride <= 0 || acc.nfreq == 0) return;
+    const int ntot = num_t + num_r + num_s;
+    std::vector<double> h(2 * (size_t)ntot);
+    DSM_CUDA(cudaMemcpy(h.data(), acc_sums.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    auto kind = [&](int off, int num, double* out, double* mx) {
+        double tot = 0.0;
+        for (int c = 0; c < num; ++c) tot += h[2 * (off + c) + 1];
+        *mx = 0.0;
+        for (int c = 0; c < num; ++c) {
+            const double d = h[2 * (off + c)], r = h[2 * (off + c) + 1];
+            const double den = r >= 1e-20 * tot ? r : tot;  // (1e-10 of the norm)^2
+            out[c] = den > 0.0 ? std::sqrt(d / den) : std::sqrt(d);
+            *mx = std::max(*mx, out[c]);
+        }
+    };
+    kind(0, num_t, acc.tsgt, &acc.tsgt_max);
+    if (rsgt_sw) kind(num_t, num_r, acc.rsgt, &acc.rsgt_max);
+    if (synn_sw) kind(num_t + num_r, num_s, acc.synn, &acc.synn_max);
 }
 
 void Engine::build_weights(const double* d_r, const double* d_rrsta) {
@@ -391,6 +504,19 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
     launches = 0;
     rounds = 0;
     recs.clear();
+    // the test hook applies to this run only
+    struct StallOnce {
+        int& v;
+        ~StallOnce() { v = 0; }
+    } stall_once{test_tc_stall};
+    DSM_CUDA(cudaMemsetAsync(dflags.p, 0, 2 * sizeof(int), st));
+    std::memset(&acc, 0, sizeof(acc));
+    acc.llog_equal = 1;
+    ms_check = 0.0;
+    if (check_ref && check_stride > 0) {
+        acc_sums.reserve(2 * (size_t)(num_t + num_r + num_s));
+        DSM_CUDA(cudaMemsetAsync(acc_sums.p, 0, acc_sums.n * sizeof(double), st));
+    }
     cudaEvent_t e0 = ev[0], e1 = ev[1], es0 = ev[2], es1 = ev[3], eg0 = ev[4], eg1 = ev[5];
     DSM_CUDA(cudaEventRecord(e0, st));
     float ms_solve = 0, ms_lsum = 0;
@@ -458,7 +584,19 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             stats.systems += tot;
             rounds++;
             DSM_CUDA(cudaMemcpyAsync(hc.data(), cut.p, sizeof(CutState) * nf, cudaMemcpyDeviceToHost, st));
+            int hstat = 0;
+            DSM_CUDA(cudaMemcpyAsync(&hstat, dstatus(), sizeof(int), cudaMemcpyDeviceToHost, st));
             DSM_CUDA(cudaStreamSynchronize(st));
+            if (hstat & DEV_NONFINITE) {  // a cutoff probe is Inf/NaN: the solves broke down
+                join_side();
+                DSM_CUDA(cudaMemsetAsync(dflags.p, 0, 2 * sizeof(int), st));
+                DSM_CUDA(cudaStreamSynchronize(st));
+                int bad = hf[0];
+                for (int w = 0; w < nf; ++w)
+                    if (hc[w].llog < 0) { bad = hf[w]; break; }
+                throw Error(DSM_ERR_NONFINITE, "a pivot of the banded solve or the cutoff probe became Inf or NaN "
+                                               "(frequency index " + std::to_string(bad) + ")");
+            }
             bool all = true;
             for (int w = 0; w < nf; ++w) {
                 if (!hc[w].done && next[w] > maxlmax) { hc[w].done = 1; }
@@ -553,8 +691,9 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             DSM_CUDA(cudaStreamWaitEvent(st, ev_grp[0], 0));
         }
         DSM_CUDA(cudaStreamSynchronize(st));
-        check_tc_error();
+        check_device_flags();
         kcollect();
+        check_batch(ilist, b0, nf, hc);
         float a = 0, g = 0;
         cudaEventElapsedTime(&a, es0, es1);
         cudaEventElapsedTime(&g, eg0, eg1);
@@ -568,7 +707,8 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
     DSM_CUDA(cudaEventSynchronize(e1));
     float tot = 0;
     cudaEventElapsedTime(&tot, e0, e1);
-    stats.ms_total = tot;
+    finish_accuracy();
+    stats.ms_total = tot - ms_check;
     stats.ms_solve = ms_solve;
     stats.ms_lsum = ms_lsum;
     stats.launches = launches;
@@ -790,6 +930,50 @@ extern "C" long long dsm_debug_copy(dsm_ctx_t* ctx, const char* name, void* dst,
     size_t nb = std::min((size_t)bytes, have);
     if (cudaMemcpy(dst, src, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return -DSM_ERR_CUDA;
     return (long long)nb;
+}
+
+// Test hooks of the error paths (no effect on results when unused).
+// "tc_stall" = 1: the next run's tensor-core l-sum withholds one stage's
+// copies in one CTA with a 20 ms wait limit, so it must report
+// DSM_ERR_TIMEOUT and leave the context usable.
+extern "C" int dsm_debug_set(dsm_ctx_t* ctx, const char* name, int value) {
+    if (!ctx || !name) return DSM_ERR_INVALID;
+    if (std::strcmp(name, "tc_stall") == 0) {
+        if (!ctx->eng->mixed()) {
+            ctx->err = "tc_stall needs a mixed-precision context";
+            return DSM_ERR_INVALID;
+        }
+        ctx->eng->test_tc_stall = value != 0;
+        return DSM_OK;
+    }
+    ctx->err = std::string("unknown debug setting ") + name;
+    return DSM_ERR_INVALID;
+}
+
+extern "C" int dsm_set_fp64_check(dsm_ctx_t* ctx, dsm_ctx_t* ref, int stride) {
+    if (!ctx) return DSM_ERR_INVALID;
+    return guarded(ctx, [&] {
+        dsm::Engine& e = *ctx->eng;
+        if (!ref || stride <= 0) {
+            e.check_ref = nullptr;
+            e.check_stride = 0;
+            return;
+        }
+        const dsm::Engine& r = *ref->eng;
+        if (ref == ctx || r.opt.precision != DSM_PREC_FP64)
+            throw Error(DSM_ERR_INVALID, "the check context must be another context in DSM_PREC_FP64");
+        if (r.mode != e.mode || r.R != e.R || r.Th != e.Th || r.opt.device != e.opt.device ||
+            r.rsgt_sw != e.rsgt_sw || r.synn_sw != e.synn_sw)
+            throw Error(DSM_ERR_INVALID, "the check context has another mode, grid, switches or device");
+        e.check_ref = ref->eng.get();
+        e.check_stride = stride;
+    });
+}
+
+extern "C" int dsm_get_accuracy(const dsm_ctx_t* ctx, dsm_accuracy_t* a) {
+    if (!ctx || !a) return DSM_ERR_INVALID;
+    *a = ctx->eng->acc;
+    return DSM_OK;
 }
 
 extern "C" int dsm_set_profiling(dsm_ctx_t* ctx, int on) {

@@ -116,7 +116,18 @@ struct DBuf {
     void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
 };
 
-// bounded device-side error word: set by kernels, read by the host
+// device-side status words of a run: set by kernels, read by the host at
+// the synchronisations the run already has.  Word 0: a bounded wait of the
+// tensor-core l-sum gave up.  Word 1: DevErr bits.
 enum DevErr : int { DEV_OK = 0, DEV_NONFINITE = 1 };
+constexpr int DEV_WORD_TC = 0, DEV_WORD_STATUS = 1;
+
+#ifdef __CUDACC__
+// sets DEV_NONFINITE in the status word when bad (rare: no warp traffic)
+__device__ __forceinline__ void flag_nonfinite(int* status, bool bad) {
+    if (bad) atomicOr(status, DEV_NONFINITE);
+}
+__device__ __forceinline__ bool nonfinite2(double a, double b) { return !isfinite(a) || !isfinite(b); }
+#endif
 
 }  // namespace dsm

@@ -127,14 +127,20 @@ class Engine {
     DBuf<float> sB[3];               // [2Th]
     DBuf<float> Cmix;                // [F][c_total] column-major blocks
     DBuf<tc::Problem> tcp;
-    DBuf<int> tc_err, d_nord;
+    DBuf<int> d_nord;
+    DBuf<int> dflags;                // status words (DEV_WORD_TC, DEV_WORD_STATUS)
+    int* tc_err() const { return dflags.p + DEV_WORD_TC; }
+    int* dstatus() const { return dflags.p + DEV_WORD_STATUS; }
+    // test hook: the next run's tensor-core launches withhold one stage's
+    // copies in one CTA and wait at most 20 ms, so the bounded wait gives up
+    int test_tc_stall = 0;
     // mixed l-sum of a batch: buffers, tensor maps and order counts once,
     // then the split and the tensor-core launches of frequencies [w0, w1)
     void lsum_prepare(int nf, const std::vector<int>& norders);
     void lsum_group(int w0, int w1, const std::vector<int>& norders);
     tc::Maps tcmaps;
     size_t tcp_next = 0;  // next free slot of tcp in this batch
-    void check_tc_error();
+    void check_device_flags();
     // contraction output of (frequency w, |m|) for the epilogue
     const double* c64(int mi) const { return Cgemm.p + c_off(mi); }
     const float* c32(int w, int mi) const { return Cmix.p + (size_t)w * c_total() + c_off(mi); }
@@ -172,6 +178,17 @@ class Engine {
                        const double* qmu, double r0, double rrcv);
     void lmax_features(const int* ilist, int n, float* out) const;
     long long rounds = 0;            // solve rounds of the last run
+
+    // FP64 accuracy report: an FP64 engine of the same set-up recomputes
+    // every check_stride-th frequency of a run on the device; per-component
+    // sums of |x - x64|^2 and |x64|^2 accumulate in acc_sums
+    Engine* check_ref = nullptr;
+    int check_stride = 0;
+    DBuf<double> acc_sums;           // [num_t + num_r + num_s][2]
+    dsm_accuracy_t acc{};
+    double ms_check = 0.0;
+    void check_batch(const int* ilist, int b0, int nf, const std::vector<CutState>& hc);
+    void finish_accuracy();
 
     // drivers
     void run(const int* ilist, int n, dsm_out_t* host_out, const void** dt, const void** dr,

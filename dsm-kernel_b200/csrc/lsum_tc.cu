@@ -44,7 +44,6 @@ constexpr int NTHREADS = 64 + EPI_THREADS;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int SMEM_STAGES = 192 * 1024;         // operand stages
 constexpr int NHB = 4;                          // chunk buffers in tensor memory
-constexpr unsigned long long WAIT_LIMIT_NS = 1000000000ull;  // 1 s
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -77,13 +76,14 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
 }
 // Bounded wait.  Gives up when another role has aborted or after the limit
 // (then it aborts the CTA itself).
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag,
+                                          unsigned long long limit_ns) {
     const unsigned long long t0 = gtimer();
     for (uint32_t n = 0;; ++n) {
         if (mbar_try(b, parity)) return true;
         if ((n & 63) == 63) {
             if (*abort_flag) return false;
-            if (gtimer() - t0 > WAIT_LIMIT_NS) {
+            if (gtimer() - t0 > limit_ns) {
                 *abort_flag = 1;
                 return false;
             }
@@ -91,10 +91,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile
     }
 }
 // Bounded wait used while draining after an abort (ignores the flag).
-__device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity) {
+__device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity, unsigned long long limit_ns) {
     const unsigned long long t0 = gtimer();
     while (!mbar_try(b, parity))
-        if (gtimer() - t0 > WAIT_LIMIT_NS) return;
+        if (gtimer() - t0 > limit_ns) return;
 }
 
 __device__ __forceinline__ void tma_a(const CUtensorMap* m, void* dst, uint64_t* bar, int x, int y, int z, int w) {
@@ -160,7 +160,7 @@ __device__ __forceinline__ void decode(const Problem* ps, int np, int t, int& p,
 template <int BK>
 __global__ void __launch_bounds__(NTHREADS, 1)
     k_lsum_tc(const __grid_constant__ Maps maps, const Problem* __restrict__ probs, int np, int ntiles,
-              uint32_t idesc, uint32_t flags, int chunk, int* __restrict__ err) {
+              uint32_t idesc, uint32_t flags, int chunk, int* __restrict__ err, unsigned long long wait_ns) {
     constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2;
     constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
     constexpr int STAGES = SMEM_STAGES / STAGE;
@@ -215,10 +215,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 for (int kb = 0; kb < P.kblocks; ++kb, ++it) {
                     const int s = it % STAGES;
                     const uint32_t ph = (it / STAGES) & 1;
-                    if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) {
+                    if (!mbar_wait(&empty[s], ph ^ 1, abort_flag, wait_ns)) {
                         ok = false;
                         break;
                     }
+                    // test hook: CTA 0 issues nothing for its first stage
+                    if ((flags & TC_TEST_STALL) && blockIdx.x == 0 && it == 0) continue;
                     unsigned char* sp = base + s * STAGE;
                     const int x = (reverse ? P.kblocks - 1 - kb : kb) * BK;
                     mbar_expect_tx(&full[s], STAGE);
@@ -231,7 +233,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             // every issued copy has landed before the CTA may exit
             for (int s = 0; s < STAGES && s < it; ++s) {
                 const int last = s + ((it - 1 - s) / STAGES) * STAGES;
-                mbar_drain(&full[s], (last / STAGES) & 1);
+                mbar_drain(&full[s], (last / STAGES) & 1, wait_ns);
             }
         }
     } else if (warp == 1) {
@@ -253,7 +255,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     const bool cfirst = kb % ch == 0;
                     if (cfirst) {
                         hb = cc % NHB;
-                        if (!mbar_wait(&hempty[hb], ((cc / NHB) & 1) ^ 1, abort_flag)) {
+                        if (!mbar_wait(&hempty[hb], ((cc / NHB) & 1) ^ 1, abort_flag, wait_ns)) {
                             ok = false;
                             break;
                         }
@@ -261,7 +263,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                         dh = tmem + (uint32_t)(hb * BN);
                     }
                     const int s = it % STAGES;
-                    if (!mbar_wait(&full[s], (it / STAGES) & 1, abort_flag)) {
+                    if (!mbar_wait(&full[s], (it / STAGES) & 1, abort_flag, wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -290,7 +292,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             }
             // all issued MMAs complete before tensor memory is released
             mma_commit(&fin);
-            mbar_drain(&fin, 0);
+            mbar_drain(&fin, 0, wait_ns);
         }
     } else {  // ------------------------------------------------------ epilogue
         // two warps per tensor-memory lane quarter, each owning 64 columns;
@@ -312,8 +314,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             // halves the conversions and FP64 additions
             for (int c = 0; c + 1 < nch; c += 2, cc += 2) {
                 const int hb0 = cc % NHB, hb1 = (cc + 1) % NHB;
-                bool got = mbar_wait(&hfull[hb0], (cc / NHB) & 1, abort_flag);
-                got = got && mbar_wait(&hfull[hb1], ((cc + 1) / NHB) & 1, abort_flag);
+                bool got = mbar_wait(&hfull[hb0], (cc / NHB) & 1, abort_flag, wait_ns);
+                got = got && mbar_wait(&hfull[hb1], ((cc + 1) / NHB) & 1, abort_flag, wait_ns);
                 if (!__all_sync(0xffffffffu, got)) {
                     ok = false;
                     break;
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             }
             if (ok && (nch & 1)) {  // the odd last chunk
                 const int hb = cc % NHB;
-                const bool got = mbar_wait(&hfull[hb], (cc / NHB) & 1, abort_flag);
+                const bool got = mbar_wait(&hfull[hb], (cc / NHB) & 1, abort_flag, wait_ns);
                 if (!__all_sync(0xffffffffu, got)) {
                     ok = false;
                     break;
@@ -567,7 +569,7 @@ void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, in
 }
 
 void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int piece_fmt, int bk, uint32_t flags,
-            int chunk, int* d_err, int nsm, cudaStream_t st) {
+            int chunk, int* d_err, int nsm, cudaStream_t st, unsigned long long wait_ns) {
     if (np <= 0 || ntiles <= 0) return;
     if (np > MAXP) throw Error(DSM_ERR_INVALID, "too many contractions in one launch");
     // kind::f16 instruction descriptor: FP32 accumulator, both operands of
@@ -583,14 +585,14 @@ void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int pi
             DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr32 = true;
         }
-        k_lsum_tc<32><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, chunk, d_err);
+        k_lsum_tc<32><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, chunk, d_err, wait_ns);
     } else if (bk == 64) {
         static bool attr64 = false;
         if (!attr64) {
             DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             attr64 = true;
         }
-        k_lsum_tc<64><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, chunk, d_err);
+        k_lsum_tc<64><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, chunk, d_err, wait_ns);
     } else {
         throw Error(DSM_ERR_INVALID, "BK must be 32 or 64");
     }

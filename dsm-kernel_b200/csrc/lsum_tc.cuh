@@ -24,6 +24,10 @@ constexpr int MAXP = 96;         // problems per launch
 constexpr int PIECE_F16 = 0;     // fp16 pieces (11-bit significand each)
 constexpr int PIECE_BF16 = 1;    // bf16 pieces (8-bit significand each)
 constexpr uint32_t TC_REVERSE = 1;    // orders summed from high to low
+// test hook: CTA 0 withholds the copies of its first stage, so the MMA
+// issuer's bounded wait runs out and the launch reports a timeout
+constexpr uint32_t TC_TEST_STALL = 2;
+constexpr unsigned long long WAIT_NS = 1000000000ull;  // limit of every bounded wait (1 s)
 
 // One contraction of a launch: rows row0 .. row0 + M of the A map against
 // the first N columns of the B map.  Rows beyond the map and columns beyond
@@ -62,8 +66,9 @@ void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, in
 
 // Launches the persistent contraction over all tiles of probs[0..np).
 // err (device int) is set nonzero if a bounded wait inside gave up.
+// wait_ns bounds every wait inside (WAIT_NS unless a test shortens it).
 void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int piece_fmt, int bk, uint32_t flags,
-            int chunk, int* d_err, int nsm, cudaStream_t st);
+            int chunk, int* d_err, int nsm, cudaStream_t st, unsigned long long wait_ns = WAIT_NS);
 
 }  // namespace tc
 }  // namespace dsm

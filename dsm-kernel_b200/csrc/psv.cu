@@ -1580,7 +1580,8 @@ __device__ __forceinline__ double warp_prefix_max(double x, int lane) {
 }
 __global__ void k_psv_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ratl, double tlen,
                            double vtop, double rtop, const int* __restrict__ freqs,
-                           const double* __restrict__ amps, CutState* __restrict__ cut) {
+                           const double* __restrict__ amps, CutState* __restrict__ cut,
+                           int* __restrict__ status) {
     const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (w >= nf) return;
@@ -1595,6 +1596,18 @@ __global__ void k_psv_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ra
         const int l = base + lane;
         const bool in = l < l1, act = in && l >= 1;
         const double amp = act ? amps[(size_t)w * Lcap + l] : 0.0;
+        // an Inf/NaN probe means the solves broke down: stop this frequency
+        // and report it (llog -1 marks it) instead of running to maxlmax
+        if (__ballot_sync(0xffffffffu, !isfinite(amp))) {
+            if (lane == 0) {
+                flag_nonfinite(status, true);
+                c.done = 1;
+                c.norders = l1;
+                c.llog = -1;
+                cut[w] = c;
+            }
+            return;
+        }
         // maxamp at this order's m = 0 update (the m = -1 update contributes 0)
         const double pm = warp_prefix_max(act ? amp : -1.0, lane);
         const double mxl = fmax(fmax(mx, pm), 0.0);
@@ -1991,7 +2004,7 @@ class PsvEngine : public Engine {
         int id = kid("psv_cutoff_scan");
         kbegin(id);
         k_psv_scan<<<(nf + 3) / 4, 128, 0, st>>>(nf, wl, Lcap, maxlmax, ratl, tlen, vtop, rtop,
-                                                  d_freqs.p, amps.p, cut.p);
+                                                  d_freqs.p, amps.p, cut.p, dstatus());
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
     }
@@ -2010,6 +2023,7 @@ class PsvEngine : public Engine {
         e.lam = d.lam;
         e.qkp = d.qkp;
         e.fr = d.fr;
+        e.status = dstatus();
         int id = kid("psv_epilogue");
         kbegin(id);
         const bool tc = mixed();

@@ -217,6 +217,14 @@ __global__ void __launch_bounds__(EPI_THREADS) k_psv_epi(EpiDev d, int w, const 
             }
         }
     }
+    bool bad = false;
+#pragma unroll
+    for (int c = 0; c < 20; ++c) bad |= !isfinite(T[c].re) || !isfinite(T[c].im);
+    if constexpr (BACK) {
+#pragma unroll
+        for (int c = 0; c < 10; ++c) bad |= !isfinite(Rg[c].re) || !isfinite(Rg[c].im);
+    }
+    flag_nonfinite(d.status, bad);
     const size_t pt = ((size_t)w * Th + it) * R + r;
     double2* t2 = reinterpret_cast<double2*>(tsgt) + pt * 20;
 #pragma unroll
@@ -281,6 +289,10 @@ __global__ void __launch_bounds__(EPI_THREADS) k_psv_epi_surf(EpiDev d, int w, c
             if (imt == 6) { S[7] = S[7] - u3; }
         }
     }
+    bool bad = false;
+#pragma unroll
+    for (int c = 0; c < 10; ++c) bad |= !isfinite(S[c].re) || !isfinite(S[c].im);
+    flag_nonfinite(d.status, bad);
     double2* s2 = reinterpret_cast<double2*>(synn) + ((size_t)w * Th + it) * 10;
 #pragma unroll
     for (int c = 0; c < 10; ++c) s2[c] = make_double2((double)S[c].re, (double)S[c].im);

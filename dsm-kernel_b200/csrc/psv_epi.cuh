@@ -43,6 +43,7 @@ struct EpiDev {
     const int* fluid;              // [R]
     const int* rrow;               // [R+1] class index of each receiver row (fld_row)
     const double *lam, *qkp, *fr;  // [R]  lambda, Qkappa, float(r)
+    int* status;                   // run status word: DEV_NONFINITE when an output is Inf/NaN
 };
 
 // Contraction outputs C0..C2 (one per |m|, column-major, rows as fld_row,

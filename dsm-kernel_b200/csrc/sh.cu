@@ -356,7 +356,8 @@ __global__ void __launch_bounds__(128) k_sh_fields(ShDev d, const int* __restric
 // cutoff scan: one thread per frequency
 __global__ void k_sh_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ratl, double tlen,
                           double vtop, double rtop, const int* __restrict__ freqs,
-                          const double* __restrict__ amps, CutState* __restrict__ cut) {
+                          const double* __restrict__ amps, CutState* __restrict__ cut,
+                          int* __restrict__ status) {
     int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= nf) return;
     CutState c = cut[w];
@@ -377,6 +378,14 @@ __global__ void k_sh_scan(int nf, WorkList wl, int Lcap, int maxlmax, double rat
             int m = (mi == 0) ? -2 : (mi == 1 ? -1 : (mi == 2 ? 1 : 2));
             if (abs(m) > l) continue;
             double amp = ap[mi], ampratio = 0.0;
+            if (!isfinite(amp)) {  // the solves broke down: stop and report (llog -1)
+                flag_nonfinite(status, true);
+                c.done = 1;
+                c.norders = l1;
+                c.llog = -1;
+                cut[w] = c;
+                return;
+            }
             if (amp > c.maxamp) c.maxamp = amp;
             if (amp != 0.0 && c.maxamp != 0.0) ampratio = amp / c.maxamp;
             if (ampratio < ratl && l > lsuf) c.ismall++;
@@ -395,7 +404,7 @@ __global__ void k_sh_epi(ShDev d, int w, int Th, const double* __restrict__ thx,
                          const double* __restrict__ ths, const int* __restrict__ pole,
                          const double* __restrict__ rr, const TC* __restrict__ C1,
                          const TC* __restrict__ C2, double* __restrict__ tsgt,
-                         double* __restrict__ rsgt, double* __restrict__ synn) {
+                         double* __restrict__ rsgt, double* __restrict__ synn, int* __restrict__ status) {
     int idx = blockIdx.x * blockDim.x + threadIdx.x;
     const int R = d.R;
     if (idx >= Th * (R + 1)) return;
@@ -499,6 +508,13 @@ __global__ void k_sh_epi(ShDev d, int w, int Th, const double* __restrict__ thx,
                 }
             }
         }
+    }
+    {
+        bool bad = false;
+        for (int c = 0; c < 5; ++c) bad |= surf && nonfinite2(S[c].re, S[c].im);
+        for (int c = 0; c < 10; ++c) bad |= !surf && nonfinite2(T[c].re, T[c].im);
+        for (int c = 0; c < 5; ++c) bad |= !surf && rsgt && nonfinite2(Rg[c].re, Rg[c].im);
+        flag_nonfinite(status, bad);
     }
     if (surf) {
         if (synn)
@@ -670,7 +686,7 @@ class ShEngine : public Engine {
 
     void scan_chunk(int nf, const WorkList& wl) override {
         k_sh_scan<<<(nf + 31) / 32, 32, 0, st>>>(nf, wl, Lcap, maxlmax, ratl, tlen, vtop, rtop,
-                                                 d_freqs.p, amps.p, cut.p);
+                                                 d_freqs.p, amps.p, cut.p, dstatus());
         DSM_LAUNCH(*this);
     }
 
@@ -682,11 +698,11 @@ class ShEngine : public Engine {
         if (mixed())
             k_sh_epi<float><<<(n + 127) / 128, 128, 0, st>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p, c32(w, 1),
                                                              c32(w, 2), out_t.p, out_r.p,
-                                                             synn_sw ? out_s.p : nullptr);
+                                                             synn_sw ? out_s.p : nullptr, dstatus());
         else
             k_sh_epi<double><<<(n + 127) / 128, 128, 0, st>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p, c64(1),
                                                               c64(2), out_t.p, out_r.p,
-                                                              synn_sw ? out_s.p : nullptr);
+                                                              synn_sw ? out_s.p : nullptr, dstatus());
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
     }

@@ -110,8 +110,28 @@ class Stats(C.Structure):
                 for i in range(self.nk)}
 
 
+DSM_ERR_INVALID = 1
+DSM_ERR_CUDA = 2
+DSM_ERR_NONFINITE = 3
+DSM_ERR_LMAX = 4
+DSM_ERR_TIMEOUT = 5
+DSM_ERR_NOMEM = 6
+DSM_ERR_NODEVICE = 7
+
+
+class Accuracy(C.Structure):
+    _fields_ = [("nfreq", C.c_int), ("llog_equal", C.c_int), ("tsgt", C.c_double * 20),
+                ("rsgt", C.c_double * 10), ("synn", C.c_double * 10), ("tsgt_max", C.c_double),
+                ("rsgt_max", C.c_double), ("synn_max", C.c_double)]
+
+
 class DsmError(RuntimeError):
-    pass
+    """A failed library call; ``code`` is its DSM_ERR_* return code (0 when
+    the failure was found on the Python side)."""
+
+    def __init__(self, msg: str, code: int = 0):
+        super().__init__(msg)
+        self.code = code
 
 
 class CatParams(C.Structure):
@@ -151,6 +171,9 @@ def lib() -> C.CDLL:
         L.dsm_strerror.restype = C.c_char_p
         L.dsm_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.dsm_set_profiling.argtypes = [C.c_void_p, C.c_int]
+        L.dsm_debug_set.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
+        L.dsm_set_fp64_check.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        L.dsm_get_accuracy.argtypes = [C.c_void_p, C.POINTER(Accuracy)]
         L.dsm_sh_cutoff_noalloc.argtypes = [C.POINTER(ShSetup), _ip, C.c_int, _ip]
         L.dsm_tc_selftest.argtypes = [C.c_int] * 10 + [C.POINTER(C.c_double)]
         _f = C.POINTER(C.c_float)
@@ -335,7 +358,7 @@ class Context:
         rc = fn(setup.ptr, C.byref(self.opt), C.byref(self.h))
         if rc:
             msg = L.dsm_last_error(self.h).decode() if self.h.value else L.dsm_strerror(rc).decode()
-            raise DsmError(f"create failed ({rc}): {msg}")
+            raise DsmError(f"create failed ({rc}): {msg}", rc)
 
     def run(self, freqs, want32: bool = False):
         L = lib()
@@ -358,13 +381,37 @@ class Context:
             out.synn32 = y32.ctypes.data_as(_fp)
         rc = L.dsm_run_freqs(self.h, _ptr(fl, _ip), n, C.byref(out))
         if rc:
-            raise DsmError(f"dsm_run_freqs failed ({rc}): {L.dsm_last_error(self.h).decode()}")
+            raise DsmError(f"dsm_run_freqs failed ({rc}): {L.dsm_last_error(self.h).decode()}", rc)
         if want32:
             return t, r, y, llog, (t32, r32, y32)
         return t, r, y, llog
 
     def set_profiling(self, on: bool):
         lib().dsm_set_profiling(self.h, 1 if on else 0)
+
+    def set_fp64_check(self, ref, stride: int = 1):
+        """Attaches an FP64 context of the same set-up (None detaches): later
+        runs recompute every stride-th frequency in FP64 and report the
+        per-component relative L2 (dsm_set_fp64_check)."""
+        rc = lib().dsm_set_fp64_check(self.h, ref.h if ref is not None else None, stride)
+        if rc:
+            raise DsmError(f"dsm_set_fp64_check failed ({rc}): {lib().dsm_last_error(self.h).decode()}", rc)
+        self._check_ref = ref  # keeps it alive while attached
+
+    def accuracy(self) -> dict:
+        """Accuracy report of the last run (dsm_get_accuracy)."""
+        a = Accuracy()
+        lib().dsm_get_accuracy(self.h, C.byref(a))
+        nt, nr, ns = self.setup.num
+        return {"nfreq": a.nfreq, "llog_equal": bool(a.llog_equal), "tsgt": list(a.tsgt[:nt]),
+                "rsgt": list(a.rsgt[:nr]), "synn": list(a.synn[:ns]), "tsgt_max": a.tsgt_max,
+                "rsgt_max": a.rsgt_max, "synn_max": a.synn_max}
+
+    def debug_set(self, name: str, value: int = 1):
+        """Test hook of the library's error paths (dsm_debug_set)."""
+        rc = lib().dsm_debug_set(self.h, name.encode(), value)
+        if rc:
+            raise DsmError(f"dsm_debug_set failed ({rc}): {lib().dsm_last_error(self.h).decode()}", rc)
 
     def run_device(self, freqs):
         """Runs with outputs left on the device; returns llog."""
@@ -375,7 +422,7 @@ class Context:
         rc = L.dsm_run_freqs_device(self.h, _ptr(fl, _ip), len(fl), C.byref(dt), C.byref(dr),
                                     C.byref(ds), _ptr(llog, _ip))
         if rc:
-            raise DsmError(f"dsm_run_freqs_device failed ({rc}): {L.dsm_last_error(self.h).decode()}")
+            raise DsmError(f"dsm_run_freqs_device failed ({rc}): {L.dsm_last_error(self.h).decode()}", rc)
         return llog
 
     def run_host32(self, freqs, t32, r32, y32, llog):
@@ -390,7 +437,7 @@ class Context:
         out.llog = _ptr(llog, _ip)
         rc = L.dsm_run_freqs(self.h, _ptr(fl, _ip), len(fl), C.byref(out))
         if rc:
-            raise DsmError(f"dsm_run_freqs failed ({rc}): {L.dsm_last_error(self.h).decode()}")
+            raise DsmError(f"dsm_run_freqs failed ({rc}): {L.dsm_last_error(self.h).decode()}", rc)
 
     def cutoffs(self, freqs):
         """Realised cutoffs (llog) only: banded solves and the amplitude
@@ -400,7 +447,7 @@ class Context:
         llog = np.zeros(len(fl), np.int32)
         rc = L.dsm_cutoffs(self.h, _ptr(fl, _ip), len(fl), _ptr(llog, _ip))
         if rc:
-            raise DsmError(f"dsm_cutoffs failed ({rc}): {L.dsm_last_error(self.h).decode()}")
+            raise DsmError(f"dsm_cutoffs failed ({rc}): {L.dsm_last_error(self.h).decode()}", rc)
         return llog
 
     def lmax_features(self, freqs):

@@ -37,7 +37,10 @@ extern "C" {
 #define DSM_OK               0
 #define DSM_ERR_INVALID      1  /* bad argument or inconsistent set-up        */
 #define DSM_ERR_CUDA         2  /* CUDA runtime / driver / library error      */
-#define DSM_ERR_NONFINITE    3  /* a pivot or output became Inf/NaN           */
+#define DSM_ERR_NONFINITE    3  /* a pivot, cutoff probe or output became
+                                   Inf/NaN (the reference prints and carries
+                                   on, src/SGTsh/dclib.f90:36-40; the outputs
+                                   of such a call are not meaningful)        */
 #define DSM_ERR_LMAX         4  /* a cutoff needs more orders than allowed    */
 #define DSM_ERR_TIMEOUT      5  /* a bounded device wait gave up              */
 #define DSM_ERR_NOMEM        6  /* device or host allocation failed           */
@@ -249,8 +252,39 @@ typedef struct dsm_stats {
 } dsm_stats_t;
 int dsm_get_stats(const dsm_ctx_t *ctx, dsm_stats_t *stats);
 
+/* Accuracy report of a mixed-precision context (the per-output relative
+ * L2 error the precision plan asks for).  No counterpart in the reference.
+ * dsm_set_fp64_check attaches a DSM_PREC_FP64 context of the same set-up
+ * (same mode, receivers and distances, same device; the caller keeps
+ * ownership and must not destroy it while attached; NULL detaches): every
+ * later dsm_run_freqs / dsm_run_freqs_device call then recomputes every
+ * stride-th frequency of its request (request positions 0, stride, ...) on
+ * that context and compares on the device.  The comparison's time is not
+ * counted in dsm_stats_t.ms_total.  dsm_get_accuracy returns the report of
+ * the last call: per component, sqrt(sum |x - x64|^2 / sum |x64|^2) over
+ * the compared frequencies, receivers and distances; a component whose FP64
+ * values vanish identically (below 1e-10 of its array's norm, e.g. SH has no
+ * radial displacement) is measured against the whole array's norm.
+ * Entries past the mode's component count are 0. */
+typedef struct dsm_accuracy {
+    int    nfreq;           /* frequencies recomputed by the last call       */
+    int    llog_equal;      /* 1: each recomputed cutoff equals the call's   */
+    double tsgt[DSM_PSV_NUM_TSGT], rsgt[DSM_PSV_NUM_RSGT], synn[DSM_PSV_NUM_SYNN];
+    double tsgt_max, rsgt_max, synn_max;
+} dsm_accuracy_t;
+int dsm_set_fp64_check(dsm_ctx_t *ctx, dsm_ctx_t *fp64_ctx, int stride);
+int dsm_get_accuracy(const dsm_ctx_t *ctx, dsm_accuracy_t *acc);
+
 /* Turns per-kernel event timing on (1) or off (0) for later runs. */
 int dsm_set_profiling(dsm_ctx_t *ctx, int on);
+
+/* Test hook of the error paths; no counterpart in the reference (whose
+ * solvers print and carry on).  name "tc_stall", value 1: the next run of a
+ * mixed-precision context withholds one stage's copies in the tensor-core
+ * l-sum and shortens its bounded waits to 20 ms, so that run returns
+ * DSM_ERR_TIMEOUT and the context stays usable.  Unknown names return
+ * DSM_ERR_INVALID. */
+int dsm_debug_set(dsm_ctx_t *ctx, const char *name, int value);
 
 /* SH angular-order cutoff without allocating device memory.  No
  * counterpart in the reference: it returns in llog[k] the cutoff the SH

@@ -88,3 +88,52 @@ def test_psv_mixed_receivers_all_solid():
     errs = _mixed_vs_fp64(s, [3, 17, 29], dsmsgt.DSM_PREC_MIXED)
     for k, v in errs.items():
         assert max(v) <= TOL_F16, (k, v)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["psv", "sh"])
+def test_library_accuracy_report_matches_host_comparison(built, mode):
+    # dsm_set_fp64_check: the library recomputes every second frequency of
+    # the request in FP64 and reports the per-component relative L2; it must
+    # equal the same comparison made on the host from the two contexts'
+    # outputs, and leave the mixed outputs unchanged
+    s = dsmsgt.Setup(psv_small() if mode == "psv" else sh_small(), mode)
+    freqs = [2, 9, 17, 25, 30]
+    c64 = dsmsgt.Context(s, precision=dsmsgt.DSM_PREC_FP64, freq_batch=2)
+    ref = c64.run(freqs)
+    cm = dsmsgt.Context(s, precision=dsmsgt.DSM_PREC_MIXED, freq_batch=4)
+    plain = cm.run(freqs)
+    cm.set_fp64_check(c64, 2)
+    got = cm.run(freqs)
+    acc = cm.accuracy()
+    cm.set_fp64_check(None)
+    cm.close()
+    c64.close()
+    for a, b in zip(got, plain):
+        assert np.array_equal(a, b)
+    sel = [0, 2, 4]
+    assert acc["nfreq"] == 3 and acc["llog_equal"]
+    for k, (a, b) in (("tsgt", (got[0], ref[0])), ("rsgt", (got[1], ref[1])), ("synn", (got[2], ref[2]))):
+        host = per_component(a[sel], b[sel])
+        lib_ = acc[k]
+        assert len(lib_) == len(host)
+        for x, y in zip(lib_, host):
+            assert abs(x - y) <= 1e-6 * max(y, 1e-300) + 1e-300, (k, lib_, host)
+        assert acc[k + "_max"] == max(lib_)
+        assert max(lib_) <= TOL_F16
+
+
+@pytest.mark.gpu
+def test_accuracy_check_rejects_mismatched_context(built):
+    s = dsmsgt.Setup(sh_small(), "sh")
+    cm = dsmsgt.Context(s, precision=dsmsgt.DSM_PREC_MIXED)
+    other = dsmsgt.Context(s, precision=dsmsgt.DSM_PREC_MIXED)
+    with pytest.raises(dsmsgt.DsmError) as ei:
+        cm.set_fp64_check(other, 1)
+    assert ei.value.code == dsmsgt.DSM_ERR_INVALID
+    p = dsmsgt.Setup(psv_small(), "psv")
+    c64 = dsmsgt.Context(p, precision=dsmsgt.DSM_PREC_FP64)
+    with pytest.raises(dsmsgt.DsmError):
+        cm.set_fp64_check(c64, 1)
+    for c in (cm, other, c64):
+        c.close()
