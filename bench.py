@@ -1,22 +1,26 @@
 #!/usr/bin/env python
 """Benchmark of the SGT engine: frequency slices per second.
 
-Workload (default): the P-SV engine on a synthetic 1-D Earth (solid inner
-core, fluid outer core, 6 mantle/crust zones; seeded quadratic profiles),
-tlen 3276.8 s, 1024 frequencies (fmax 0.3125 Hz), source 300 km deep,
-201 receiver radii 1000-6350 km, 721 epicentral distances (0.25 deg).
-A step is one batch of frequency slices spread across the band, each fully
-processed (all orders up to the reference's cutoff, all m, all sources,
-TSGT + RSGT + SYNN on the full (r, theta) grid).
+Workload (default, psv2048): the P-SV engine on a synthetic 1-D Earth (solid
+inner core, fluid outer core, 6 mantle/crust zones; seeded quadratic
+profiles), tlen 3276.8 s, 2048 frequencies (fmax 0.625 Hz, cutoffs up to
+about 7000), source 300 km deep, 201 receiver radii 1000-6350 km, 1441
+epicentral distances (0.125 deg).  A step is one batch of frequency slices
+spread across the band, each fully processed (all orders up to the
+reference's cutoff, all m, all sources, TSGT + RSGT + SYNN on the full
+(r, theta) grid).  psv1024 (the FP64 configuration's band: 1024 frequencies,
+721 distances) and sh256 are the other workloads.
 
-  python bench.py [--gpus N --steps K --warmup W] [--precision mixed|mixed_bf16|fp64]
+  python bench.py [--gpus N --steps K --warmup W] [--workload psv2048|psv1024|sh256]
+                  [--precision mixed|mixed_bf16|fp64]
   python bench.py --impl reference ...   # CPU restatement of the reference
 
 The headline path is the mixed-precision one (split fp16 l-sum on the
 tensor cores, learned first order ranges when a trained parameter block is
 present); the plain FP64 GPU path runs the same steps for the speedup, and
-both paths' outputs on a sample of the first step give the per-component
-relative L2.
+the library's own accuracy report (an FP64 context attached to the mixed
+one) gives the per-component relative L2 on a sample of frequencies that
+includes the top of the band.
 
 One JSON line is printed by rank 0.  Under torchrun (N > 1) every rank
 processes its own frequencies (weak scaling, no collective on the data
@@ -55,27 +59,26 @@ WORKLOADS = {
 }
 
 
-# DRAM bytes per launch of a kernel on a workload's step, from an ncu
-# capture of the bench's own launches of dram__bytes_read.sum +
-# dram__bytes_write.sum (psv1024: mean of the two warm-up steps,
-# profiles/dram_traffic_psv1024.md).
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of a
+# kernel on a workload, from an ncu capture of that kernel; the line reports
+# where each figure came from next to it, and null where none was taken.
 TRAFFIC = {
-    ("psv1024", "lsum_tc"): 14.07e9,
-    ("psv1024", "psv_factor"): 21.44e9,
-    ("psv1024", "psv_substitution"): 25.09e9,
-    ("psv1024", "psv_fields"): 11.49e9,
-    ("psv1024", "lsum_split"): 12.45e9,
-    # catalogue workload, one launch each (profiles/k_cat_interp_catalogue1681.md)
-    ("catalogue", "cat_interp"): 0.672e9,
-    ("catalogue", "cat_omega"): 0.598e9,
+    ("psv1024", "lsum_tc"): (14.07e9, "ncu capture of the bench's own launches (psv1024, 16 frequencies)"),
+    ("catalogue", "cat_interp"): (0.672e9, "ncu capture of one launch (catalogue workload)"),
+    ("catalogue", "cat_omega"): (0.598e9, "ncu capture of one launch (catalogue workload)"),
 }
+
+
+def traffic(name, kernel):
+    v = TRAFFIC.get((name, kernel))
+    return (v[0], v[1]) if v else (None, "not captured for this workload")
 
 
 def workload(name: str):
     """Job (parameter file, DSM.config, model) and description of a workload."""
     import dsmsgt
     from dsmsgt import synth
-    name = {"psv": "psv1024", "sh": "sh256"}.get(name, name)
+    name = {"psv": "psv2048", "sh": "sh256"}.get(name, name)
     w = WORKLOADS[name]
     model = synth.psv_earth_model(0) if w["mode"] == "psv" else synth.sh_mantle_model(0)
     job = dsmsgt.Job(
@@ -93,11 +96,11 @@ def workload(name: str):
 
 
 def workload_mode(name: str) -> str:
-    return WORKLOADS[{"psv": "psv1024", "sh": "sh256"}.get(name, name)]["mode"]
+    return WORKLOADS[{"psv": "psv2048", "sh": "sh256"}.get(name, name)]["mode"]
 
 
 def workload_imax(name: str) -> int:
-    return WORKLOADS[{"psv": "psv1024", "sh": "sh256"}.get(name, name)]["imax"]
+    return WORKLOADS[{"psv": "psv2048", "sh": "sh256"}.get(name, name)]["imax"]
 
 
 def per_component_rel_l2(a, b):
@@ -116,7 +119,7 @@ def per_component_rel_l2(a, b):
 def load_lmax_params(name: str):
     """Trained parameter block of the learned cutoff for a workload (written
     by dsmsgt.lmax_data for that workload's band and grid), or None."""
-    name = {"psv": "psv1024", "sh": "sh256"}.get(name, name)
+    name = {"psv": "psv2048", "sh": "sh256"}.get(name, name)
     path = os.path.join(REPO, "dsm-kernel_b200", "dsmsgt", f"lmax_{name}.f32")
     if not os.path.exists(path):
         return None
@@ -178,36 +181,40 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def cpu_baseline(setup_mode: str, freqs: list[int], threads: int, slope: float | None = None):
-    """Times the oracle (the CPU FP64 restatement of the reference's
-    frequency loop, all host threads, parallel over frequencies) on a
-    bounded sample and scales to the full epicentral grid.
+CPU_THETAS = 8  # interior epicentral distances of a CPU sample
 
-    The sample keeps the workload's model, grid, source and all receivers,
-    on reduced epicentral grids: CPU time per slice is an order-solve part
-    that does not depend on the number of distances plus a part linear in
-    it (the receiver x theta loop).  A run at 7 distances gives the first;
-    the per-distance slope comes from a second run at 13 distances, or is
-    passed in from an earlier sample of the same workload."""
-    from oracle import oracle as orc
+
+def cpu_sample(name: str, freq: int, threads: int):
+    """Times the oracle (the FP64 CPU restatement of the reference's frequency
+    loop, its own set-up, no product code) on one frequency of the workload:
+    every order up to the cutoff, every receiver, all sources and outputs, on
+    CPU_THETAS interior epicentral distances spread over 0-180 deg, one
+    frequency spread over `threads` host threads.  The oracle times the parts
+    proportional to the number of distances (vector harmonics, SYNN, the
+    receiver x theta loop: the same work for every interior distance)
+    separately, so the time of the full slice is the measured rest plus that
+    part scaled to the workload's distances.  Returns (estimated seconds per
+    full slice, measured seconds, measured theta seconds, llog)."""
     import dsmsgt
-    job, desc = workload(setup_mode)
-    times = {}
-    grids = ((30.0, 7),) if slope is not None else ((30.0, 7), (15.0, 13))
+    from oracle import driver_setup, oracle as orc
+    job, desc = workload(name)
     w = WORKLOADS[desc["name"]]
-    for thd, nth in grids:
-        text = job.param_text.replace(f" {w['thdelta']!r}\n", f" {thd}\n")
-        sjob = dsmsgt.Job(text, job.conf_text, job.model_text)
-        s = dsmsgt.Setup(sjob, w["mode"])
-        assert s.theta_n == nth, (s.theta_n, nth)
-        t0 = time.perf_counter()
-        orc.run(s, freqs, threads=threads)
-        times[nth] = time.perf_counter() - t0
-    if slope is None:
-        slope = (times[13] - times[7]) / 6.0
-    t_full = times[7] + slope * (desc["thetas"] - 7)
-    value = len(freqs) / t_full
-    return value, times, slope
+    if w["mode"] != "psv":
+        raise ValueError("the CPU sample covers the P-SV workloads")
+    d = 180.0 / CPU_THETAS
+    text = job.param_text.replace(f"0.0 180.0 {w['thdelta']!r}\n", f"{d / 2!r} {180.0 - d / 2!r} {d!r}\n")
+    s = driver_setup.psv_setup(dsmsgt.Job(text, job.conf_text, job.model_text))
+    assert s.theta_n == CPU_THETAS, s.theta_n
+    _, _, _, llog, t_theta, t_total = orc.run_threads(s, [freq], threads)
+    full = float(t_total[0] - t_theta[0] + t_theta[0] * desc["thetas"] / CPU_THETAS)
+    return full, float(t_total[0]), float(t_theta[0]), int(llog[0])
+
+
+def cpu_sample_freq(k: int, imax: int, nspread: int = 20) -> int:
+    """Frequency of CPU sample k: a fixed spread of nspread indices over the
+    band (the same set whatever the step count), visited in turn."""
+    j = k % nspread
+    return 1 + int((j + 0.5) * imax / nspread)
 
 
 CAT_METRIC = "catalogue points/s (6 windowed time series per point from 30 SGT components)"
@@ -367,14 +374,16 @@ def catalogue_bench(args):
             ach = fk / (tk / 1e3) / 1e12
             rooflines[name] = {"kernel": name, "bound": "fp64", "achieved": ach, "peak": fp64,
                                "unit": "TFLOP/s (algorithmic)", "frac": ach / fp64,
-                               "traffic": TRAFFIC.get(("catalogue", name)),
+                               "traffic": traffic("catalogue", name)[0],
+                               "traffic_source": traffic("catalogue", name)[1],
                                "peak_source": "measured (FP64 FMA and tensor-core probes, this run; the larger)",
                                "avg_launch_ms": tk / max(nk, 1)}
         else:
             ach = bk / (tk / 1e3) / 1e9
             peak = peaks.get("hbm_gbs", 6650.0)
             rooflines[name] = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                               "frac": ach / peak, "traffic": TRAFFIC.get(("catalogue", name)),
+                               "frac": ach / peak, "traffic": traffic("catalogue", name)[0],
+                               "traffic_source": traffic("catalogue", name)[1],
                                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                                "avg_launch_ms": tk / max(nk, 1)}
     roof = rooflines[max(kst.items(), key=lambda kv: kv[1][0])[0]]
@@ -402,13 +411,46 @@ def catalogue_bench(args):
             "cpu_baseline": cpu, "clocks": clk}))
 
 
+def reference_arm(args):
+    """The reference's CPU implementation of the path (the oracle: the FP64
+    restatement of the Fortran frequency loop, with its own set-up), timed on
+    the host cores on a bounded sample per step: one frequency of a fixed
+    spread over the band (cpu_sample)."""
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    imax = workload_imax(args.mode)
+    _, desc = workload(args.mode)
+    for w in range(args.warmup):  # untimed: the lowest frequencies (page cache, thread start)
+        cpu_sample(args.mode, 1 + w, threads)
+    est, wall, samples = 0.0, 0.0, []
+    for k in range(args.steps):
+        f = cpu_sample_freq(k, imax)
+        full, t, th, ll = cpu_sample(args.mode, f, threads)
+        est += full
+        wall += t
+        samples.append({"freq": f, "llog": ll, "measured_s": round(t, 3), "theta_part_s": round(th, 3),
+                        "full_slice_s": round(full, 2)})
+    value = args.steps / est
+    cpu = {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": (f"one frequency per step from a fixed spread of 20 over 1..{imax}, every order to the "
+                      f"cutoff, all {desc['receivers']} receivers and outputs, {CPU_THETAS} interior epicentral "
+                      f"distances; the theta-proportional part (timed by the oracle) scaled to {desc['thetas']}"),
+           "extrapolated": f"theta loop x {desc['thetas']}/{CPU_THETAS}; solves and set-up per order measured in full",
+           "setup": "oracle's own (numpy restatement of the reference's set-up; no product library)",
+           "steps": samples}
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic", "config": desc, "cpu_baseline": cpu,
+                      "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--workload", "--mode", dest="mode", default="psv1024",
+    ap.add_argument("--workload", "--mode", dest="mode", default="psv2048",
                     choices=["psv1024", "psv2048", "sh256", "psv", "sh", "catalogue"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_bf16"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
@@ -427,36 +469,8 @@ def main():
     mode = workload_mode(args.mode)
 
     if args.impl == "reference":
-        if rank != 0:
-            return
-        threads = os.cpu_count() or 1
-        # warm-up: one tiny sample (the page cache and the oracle build)
-        for w in range(args.warmup):
-            cpu_baseline(args.mode, [1 + w], 1, slope=0.0)
-        # the per-distance slope once, on the first step's frequencies
-        slope = None
-        t_tot, n_tot, samples = 0.0, 0, []
-        for k in range(args.steps):
-            fr = step_freqs(k, threads, imax)
-            v, times, slope = cpu_baseline(args.mode, fr, threads, slope=slope)
-            t_tot += len(fr) / v
-            n_tot += len(fr)
-            samples.append(times)
-        value = n_tot / t_tot
-        _, desc = workload(args.mode)
-        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": 1e3 * t_tot / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": desc,
-                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                                 "sample": f"{threads} frequencies per step spread over the band, "
-                                           "all receivers, 7 epicentral distances per step (13 once "
-                                           "for the per-distance slope), scaled linearly to "
-                                           f"{desc['thetas']} distances"},
-                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        if rank == 0:
+            reference_arm(args)
         return
 
     import torch
@@ -494,15 +508,15 @@ def main():
         ctx.set_profiling(True)
         clocks = ClockSampler(dev)
         clocks.start()
-        kstats, ms_dev, launches, llogs, systems, padded, used = {}, 0.0, 0, [], 0, 0, 0
+        kstats, ms_dev, launches, llogs = {}, 0.0, 0, []
+        sol = {"systems": 0, "orders_used": 0, "orders_padded": 0, "solve_rounds": 0, "freqs_extended": 0}
         barrier()
         for k in range(args.steps):
             llogs.append(ctx.run_device(step_freqs(k, args.per_step, imax, rank, world)).tolist())
             st = ctx.stats()
             ms_dev += st.ms_total
-            systems += st.systems
-            padded += st.orders_padded
-            used += st.orders_used
+            for key in sol:
+                sol[key] += getattr(st, key)
             launches += st.launches - sum(v[1] for n_, v in st.kernels().items() if n_.startswith("lsum_dgemm"))
             for name, (ms, n, b, f) in st.kernels().items():
                 acc = kstats.setdefault(name, [0.0, 0, 0.0, 0.0])
@@ -511,8 +525,9 @@ def main():
         clk = clocks.stop()
         ctx.set_profiling(False)
         t_dev = max_over_ranks(ms_dev / 1e3)
-        # end to end through the C-ABI: complex64 catalogue records copied to
-        # pinned host memory every step (the frequency list goes host -> device)
+        # end to end through the C-ABI (dsm_run_freqs), host wall clock: the
+        # frequency list goes in, complex64 catalogue records come back to
+        # pinned host memory every step; the set-up is resident per context
         nt, nr, ns = setup.num
         per_t = nt * setup.r_n * setup.theta_n
         per_r = nr * setup.r_n * setup.theta_n
@@ -522,20 +537,20 @@ def main():
         hr = torch.empty(2 * per_r * F, dtype=torch.float32, pin_memory=True)
         hy = torch.empty(2 * per_s * F, dtype=torch.float32, pin_memory=True)
         ll = np.zeros(F, np.int32)
-        ms_e2e = 0.0
+        ctx.run_host32(step_freqs(0, F, imax, rank, world), ht.data_ptr(), hr.data_ptr(), hy.data_ptr(), ll)
         barrier()
+        t0 = time.perf_counter()
         for k in range(args.steps):
-            ctx.run_host32(step_freqs(k, F, imax, rank, world), ht.data_ptr(), hr.data_ptr(),
-                           hy.data_ptr(), ll)
-            ms_e2e += ctx.stats().ms_total
+            ctx.run_host32(step_freqs(k, F, imax, rank, world), ht.data_ptr(), hr.data_ptr(), hy.data_ptr(), ll)
+        t_e2e = max_over_ranks(time.perf_counter() - t0)
         barrier()
-        t_e2e = max_over_ranks(ms_e2e / 1e3)
         ctx.close()
         slices = args.steps * args.per_step * world
         return {"value": slices / t_dev, "t": t_dev, "kstats": kstats, "launches": launches,
-                "llogs": llogs, "clocks": clk, "systems": systems, "padded": padded, "used": used,
+                "llogs": llogs, "clocks": clk, "solve": sol,
                 "e2e": {"value": slices / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * F,
-                        "d2h_bytes_per_step": 8 * (per_t + per_r + per_s) * F + 4 * F}}
+                        "d2h_bytes_per_step": 8 * (per_t + per_r + per_s) * F + 4 * F,
+                        "timing": "host wall clock around dsm_run_freqs (perf_counter), records to pinned memory"}}
 
     headline_prec = {"fp64": dsmsgt.DSM_PREC_FP64, "mixed": dsmsgt.DSM_PREC_MIXED,
                      "mixed_bf16": dsmsgt.DSM_PREC_MIXED_BF16}[args.precision]
@@ -544,20 +559,23 @@ def main():
     run = measure(headline_prec, use_lmax)
     plain = measure(dsmsgt.DSM_PREC_FP64, False) if mixed and not args.no_fp64 else None
 
-    # accuracy of the headline path against the FP64 GPU path: per output
-    # component relative L2 on a sample of the first step's frequencies
+    # accuracy of the headline path against the FP64 GPU path, from the
+    # library's own report: an FP64 context attached to the mixed one
+    # recomputes every fourth frequency of the first step and the top of the
+    # band (outside the timed region)
     rel = None
     if mixed and rank == 0:
-        fr = step_freqs(0, args.per_step, imax)[:: max(1, args.per_step // 4)]
-        c64 = dsmsgt.Context(setup, precision=dsmsgt.DSM_PREC_FP64, device=dev, freq_batch=len(fr))
-        ref = c64.run(fr)
-        c64.close()
+        fr = sorted(set(step_freqs(0, args.per_step, imax)) | {imax})
+        c64 = dsmsgt.Context(setup, precision=dsmsgt.DSM_PREC_FP64, device=dev, freq_batch=4)
         cm = dsmsgt.Context(setup, precision=headline_prec, device=dev, freq_batch=len(fr))
-        got = cm.run(fr)
+        cm.set_fp64_check(c64, 1)
+        cm.run_device(fr)
+        acc = cm.accuracy()
+        cm.set_fp64_check(None)
         cm.close()
-        rel = {"frequencies": fr, "llog_equal": list(ref[3]) == list(got[3])}
-        for name, a, b_ in (("tsgt", got[0], ref[0]), ("rsgt", got[1], ref[1]), ("synn", got[2], ref[2])):
-            rel[name] = max(per_component_rel_l2(a, b_))
+        c64.close()
+        rel = {"frequencies": fr, "llog_equal": acc["llog_equal"], "tsgt": acc["tsgt_max"],
+               "rsgt": acc["rsgt_max"], "synn": acc["synn_max"], "source": "dsm_get_accuracy"}
 
     # roofline of the dominant kernel of this library (CUDA events on the
     # library's stream over the timed region)
@@ -573,6 +591,7 @@ def main():
     roof = None
     if dom:
         name, (ms, n, b, f) = dom
+        tr, tr_src = traffic(desc["name"], name)
         if f > 0:
             # algorithmic flops (one real product per row, column and order up
             # to the cutoff); the split path runs three fp16 piece products
@@ -580,38 +599,40 @@ def main():
             ach = f / (ms / 1e3) / 1e12
             peak = peaks.get("bf16_tflops", 1590.0)
             roof = {"kernel": name, "bound": "tensor", "achieved": ach, "peak": peak,
-                    "unit": "TFLOP/s", "frac": ach / peak, "traffic": TRAFFIC.get((desc["name"], name)),
-                    "peak_source": "measured" if "bf16_tflops" in peaks else "fallback",
+                    "unit": "TFLOP/s", "frac": ach / peak, "traffic": tr, "traffic_source": tr_src,
+                    "peak_source": "measured (bf16 burst)" if "bf16_tflops" in peaks else "fallback",
                     "avg_launch_ms": ms / max(n, 1), "piece_products": 3,
                     "frac_of_piece_ceiling": 3.0 * ach / peak}
         else:
             ach = b / (ms / 1e3) / 1e9
             peak = peaks.get("hbm_gbs", 6650.0)
             roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                    "frac": ach / peak, "traffic": TRAFFIC.get((desc["name"], name)),
+                    "frac": ach / peak, "traffic": tr, "traffic_source": tr_src,
                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                     "avg_launch_ms": ms / max(n, 1)}
     share = {k: round(v[0] / max(run["t"] * 1e3, 1e-9), 4) for k, v in kstats.items()}
-    tc = kstats.get("lsum_tc")
-    tensor = None
-    if tc and tc[0] > 0:
-        ach = tc[3] / (tc[0] / 1e3) / 1e12
-        peak = peaks.get("bf16_tflops", 1590.0)
-        tensor = {"kernel": "lsum_tc", "achieved": ach, "peak": peak, "unit": "TFLOP/s (algorithmic)",
-                  "frac": ach / peak, "piece_products": 3, "tensor_tflops_executed_approx": 3.0 * ach,
-                  "avg_launch_ms": tc[0] / max(tc[1], 1)}
+    # HBM-bound band kernels: algorithmic bytes over their event time
+    hbm = {}
+    for k in ("psv_factor", "psv_substitution"):
+        if k in kstats and kstats[k][0] > 0:
+            ach = kstats[k][2] / (kstats[k][0] / 1e3) / 1e9
+            peak = peaks.get("hbm_gbs", 6650.0)
+            hbm[k] = {"achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                      "alg_bytes_per_step": kstats[k][2] / args.steps, "ms_per_step": kstats[k][0] / args.steps}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        fr = step_freqs(0, min(threads, 16), imax)
-        v, times, _ = cpu_baseline(args.mode, fr, threads)
-        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{len(fr)} frequencies spread over the band, all receivers, 7 and 13 "
-                         "epicentral distances (oracle, FP64), scaled linearly to the full "
-                         f"{desc['thetas']} distances; measured s: {json.dumps(times)}"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and mode == "psv":
+        threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+        f = cpu_sample_freq(0, imax)
+        full, t, th, _ = cpu_sample(args.mode, f, threads)
+        cpu = {"value": 1.0 / full, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": (f"frequency {f}, every order to the cutoff, all receivers and outputs, {CPU_THETAS} "
+                          f"interior distances (measured {t:.1f} s, theta part {th:.1f} s), theta part scaled "
+                          f"to {desc['thetas']} distances; oracle with its own set-up"),
+               "extrapolated": f"theta loop x {desc['thetas']}/{CPU_THETAS}"}
 
     if rank == 0:
+        sol = run["solve"]
         line = {"metric": METRIC, "value": run["value"], "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1e3 * run["t"] / args.steps,
@@ -625,15 +646,15 @@ def main():
                                parallelism=f"dp{world} (frequencies per rank)",
                                l2="inputs larger than L2 (field matrices of several GB per step)"),
                 "e2e": run["e2e"], "gpu_launches": int(run["launches"]),
-                "roofline": roof, "tensor_roofline": tensor, "kernel_share": share,
+                "roofline": roof, "hbm_kernels": hbm, "kernel_share": share,
                 "cpu_baseline": cpu, "clocks": run["clocks"],
-                "solve": {"systems": run["systems"], "orders_used": run["used"],
-                          "orders_padded": run["padded"]},
+                "solve": dict(sol, slices=args.steps * args.per_step,
+                              padded_fraction=sol["orders_padded"] / max(sol["orders_used"], 1),
+                              miss_rate=sol["freqs_extended"] / max(args.steps * args.per_step, 1)),
                 "llog_first_step": run["llogs"][0]}
         if plain:
             line["fp64"] = {"value": plain["value"], "ms_per_step": 1e3 * plain["t"] / args.steps,
-                            "e2e": plain["e2e"]["value"], "systems": plain["systems"],
-                            "orders_padded": plain["padded"], "clocks": plain["clocks"],
+                            "e2e": plain["e2e"]["value"], "solve": plain["solve"], "clocks": plain["clocks"],
                             "kernel_share": {k: round(v[0] / max(plain["t"] * 1e3, 1e-9), 4)
                                              for k, v in plain["kstats"].items()}}
             line["speedup_vs_fp64"] = run["value"] / plain["value"]

@@ -557,6 +557,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
                 span[w] = (sp + 31) / 32 * 32;
             }
         }
+        const std::vector<int> span0 = span;  // first order range of each frequency
         int maxend = 0;
         for (;;) {
             std::vector<int> off(nf + 1, 0), lb(nf, 0);
@@ -608,6 +609,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
         for (int w = 0; w < nf; ++w) {
             if (hc[w].norders == 0) { hc[w].norders = maxlmax + 1; hc[w].llog = maxlmax; }
             stats.orders_padded += (long long)next[w] - hc[w].norders;
+            stats.freqs_extended += hc[w].norders > span0[w] ? 1 : 0;
         }
         join_side();
         DSM_CUDA(cudaEventRecord(es1, st));
@@ -709,6 +711,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
     cudaEventElapsedTime(&tot, e0, e1);
     finish_accuracy();
     stats.ms_total = tot - ms_check;
+    stats.solve_rounds = rounds;
     stats.ms_solve = ms_solve;
     stats.ms_lsum = ms_lsum;
     stats.launches = launches;

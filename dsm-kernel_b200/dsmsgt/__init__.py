@@ -102,7 +102,8 @@ class Stats(C.Structure):
                 ("launches", C.c_longlong), ("systems", C.c_longlong),
                 ("orders_used", C.c_longlong), ("orders_padded", C.c_longlong),
                 ("lsum_flops", C.c_double), ("solve_bytes", C.c_double),
-                ("nk", C.c_int), ("kern", KStat * 12)]
+                ("nk", C.c_int), ("kern", KStat * 12), ("solve_rounds", C.c_longlong),
+                ("freqs_extended", C.c_longlong)]
 
     def kernels(self):
         return {self.kern[i].name.decode(): (self.kern[i].ms, self.kern[i].launches,

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define DSM_ABI_VERSION 1
+#define DSM_ABI_VERSION 2
 
 /* return codes */
 #define DSM_OK               0
@@ -249,6 +249,10 @@ typedef struct dsm_stats {
     double solve_bytes;     /* algorithmic bytes of the banded solves      */
     int nk;                 /* entries of kern[] in use                    */
     dsm_kstat_t kern[DSM_MAX_KSTATS];
+    long long solve_rounds;  /* order ranges solved per batch, summed        */
+    long long freqs_extended;/* frequencies whose cutoff lay beyond their
+                                first order range (the learned cutoff's
+                                misses when it sized that range)            */
 } dsm_stats_t;
 int dsm_get_stats(const dsm_ctx_t *ctx, dsm_stats_t *stats);
 

@@ -37,6 +37,8 @@ def lib():
         for name in ("oracle_sh_run_parallel", "oracle_psv_run_parallel"):
             getattr(L, name).argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_void_p,
                                          C.c_void_p, C.c_void_p, C.POINTER(C.c_int), C.c_int]
+        L.oracle_psv_run_threads.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -64,3 +66,21 @@ def run(setup, freqs, threads: int = 1):
         else:
             L.oracle_psv_run(*args)
     return t, r, y, llog
+
+
+def run_threads(setup, freqs, threads: int):
+    """P-SV oracle with each frequency spread over ``threads`` host threads
+    (the same values as run()); returns (tsgt, rsgt, synn, llog, t_theta,
+    t_total), the last two per frequency in seconds: the time of the parts
+    proportional to the number of epicentral distances and the whole time."""
+    from dsmsgt import alloc_outputs
+    assert setup.mode == "psv"
+    fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+    n = len(fl)
+    t, r, y, llog = alloc_outputs(setup, n)
+    tth, ttot = np.zeros(n), np.zeros(n)
+    lib().oracle_psv_run_threads(C.cast(setup.ptr, C.c_void_p), fl.ctypes.data_as(C.POINTER(C.c_int)), n,
+                                 t.ctypes.data, r.ctypes.data, y.ctypes.data,
+                                 llog.ctypes.data_as(C.POINTER(C.c_int)), threads, tth.ctypes.data,
+                                 ttot.ctypes.data)
+    return t, r, y, llog, tth, ttot

@@ -13,8 +13,13 @@
 // fused multiply-add (built with -ffp-contract=off), libm sin/cos/log.
 #pragma once
 
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstddef>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 namespace oracle {
@@ -169,6 +174,79 @@ struct Uder {
         for (auto& r : u)
             for (auto& c : r) c = cplx(0.0);
     }
+};
+
+
+// Host thread pool of the oracle's parallel frequency loop: run(n, f) calls
+// f(i, t) for i in [0, n) on the pool's threads (the caller is t = 0, the
+// others 1 .. size()-1), indices handed out one at a time, and returns when
+// all have finished.
+class Pool {
+  public:
+    explicit Pool(int nthreads) : n_(nthreads < 1 ? 1 : nthreads) {
+        for (int t = 1; t < n_; ++t) th_.emplace_back([this, t] { loop(t); });
+    }
+    ~Pool() {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+            ++gen_;
+        }
+        cv_.notify_all();
+        for (auto& t : th_) t.join();
+    }
+    int size() const { return n_; }
+    void run(int n, const std::function<void(int, int)>& f) {
+        if (n <= 0) return;
+        if (n_ == 1) {
+            for (int i = 0; i < n; ++i) f(i, 0);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> g(m_);
+            job_ = &f;
+            njob_ = n;
+            next_.store(0);
+            busy_ = n_ - 1;
+            ++gen_;
+        }
+        cv_.notify_all();
+        work(0);
+        std::unique_lock<std::mutex> g(m_);
+        done_.wait(g, [this] { return busy_ == 0; });
+        job_ = nullptr;
+    }
+
+  private:
+    void work(int t) {
+        for (int i = next_.fetch_add(1); i < njob_; i = next_.fetch_add(1)) (*job_)(i, t);
+    }
+    void loop(int t) {
+        unsigned long seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> g(m_);
+                cv_.wait(g, [&] { return gen_ != seen; });
+                seen = gen_;
+                if (stop_) return;
+            }
+            work(t);
+            {
+                std::lock_guard<std::mutex> g(m_);
+                --busy_;
+            }
+            done_.notify_one();
+        }
+    }
+    int n_;
+    std::vector<std::thread> th_;
+    std::mutex m_;
+    std::condition_variable cv_, done_;
+    unsigned long gen_ = 0;
+    bool stop_ = false;
+    const std::function<void(int, int)>* job_ = nullptr;
+    int njob_ = 0, busy_ = 0;
+    std::atomic<int> next_{0};
 };
 
 }  // namespace oracle

@@ -5,6 +5,7 @@
 #include "oracle_common.hpp"
 #include "dsmsgt.h"
 
+#include <chrono>
 #include <cstring>
 
 namespace oracle {
@@ -783,8 +784,36 @@ void rea2(const dsm_psv_setup_t& s, int nn, const cplx* a /*1-based packed (4,nn
 }  // namespace
 
 // One frequency of src/SGTpsv/SGTpsv-MPI.f90:535-1152.
+//
+// The reference's l loop interleaves, per order, the banded solves of every
+// source and back-propagation right-hand side with their use (the cutoff
+// probe, SYNN and the receiver x theta accumulation).  The solves of
+// different orders are independent, so orders are taken in blocks:
+//   1. the solves of the block's orders run in parallel over orders, each
+//      keeping g0 at the rows the rest of the loop reads (the receivers'
+//      three-node stencils, which include the probe rows, and the surface
+//      rows nn-1, nn);
+//   2. in order: the vector-harmonic recurrence of each order (kept per
+//      order) and the cutoff test (calamp, the ismall > 20 exit), which
+//      fixes the last order of the block that the loop reaches;
+//   3. the accumulation of those orders, in parallel over receivers: each
+//      receiver owns its outputs and adds its terms in the reference's
+//      (l, m, source) order; SYNN is one more task of the same kind.
+// Every value is computed by the same operations, in the same order, as in
+// the sequential loop, so the results do not depend on the thread count.
+// t_theta (optional) receives the wall time of the parts whose cost is
+// proportional to the number of epicentral distances (steps 2 and 3 but the
+// cutoff test; at l = 0 the same parts of the sequential branch).
+struct PsvOrderSol {
+    std::vector<cplx> g;  // [rhs][capture row]
+};
+
 void psv_one_frequency(const dsm_psv_setup_t& s, int ifreq, cplx* tsgt, cplx* rsgt, cplx* synn,
-                       int* llog_out, double* probe_out = nullptr, int probe_n = 0) {
+                       int* llog_out, double* probe_out = nullptr, int probe_n = 0, int nthreads = 1,
+                       double* t_theta = nullptr) {
+    using clock = std::chrono::steady_clock;
+    double theta_s = 0.0;
+    if (nthreads < 1) nthreads = 1;
     const int nzone = s.nzone, nn = s.nn, r_n = s.r_n, th_n = s.theta_n;
     const int NT = DSM_PSV_NUM_TSGT, NR = DSM_PSV_NUM_RSGT, NS = DSM_PSV_NUM_SYNN;
     for (long k = 0; k < (long)NT * r_n * th_n; ++k) tsgt[k] = cplx(0.0);
@@ -845,6 +874,20 @@ void psv_one_frequency(const dsm_psv_setup_t& s, int ifreq, cplx* tsgt, cplx* rs
     std::vector<int> ksta(r_n);
     for (int ir = 0; ir < r_n; ++ir)
         ksta[ir] = s.kkdr[s.istazone[ir] - 1] + 2 * s.iista[3 * ir] - 1;
+    // rows of g0 read after a solve: the receivers' stencils g0(ksta-1 ..
+    // ksta+4) (the probe rows are those of the top receiver) and nn-1, nn
+    std::vector<int> caprow, capidx(nn + 2, -1);
+    auto addrow = [&](int j) {
+        if (capidx[j] < 0) {
+            capidx[j] = (int)caprow.size();
+            caprow.push_back(j);
+        }
+    };
+    for (int ir = 0; ir < r_n; ++ir)
+        for (int k = 0; k < 6; ++k) addrow(ksta[ir] - 1 + k);
+    addrow(nn - 1);
+    addrow(nn);
+    const int ncap = (int)caprow.size();
     std::vector<double> thr(th_n);
     for (int it = 0; it < th_n; ++it) thr[it] = s.theta[it] / 180.0 * kPi;
     std::vector<double> plm(12 * th_n, 0.0);
@@ -859,10 +902,14 @@ void psv_one_frequency(const dsm_psv_setup_t& s, int ifreq, cplx* tsgt, cplx* rs
     double maxamp = -1.0;
     int llog = s.maxlmax;
     const double* rsrc = s.ra_src;
+    const int jtmp = s.jsrc;
 
-    auto receivers = [&](int m, double lsq, const cplx* gsrc, int l0mode, bool back, int id) {
+    // receiver x theta terms of one right-hand side for receivers [ir0, ir1)
+    // with the harmonics dv / dvt / dvp of the order
+    auto receivers_range = [&](int ir0, int ir1, int m, double lsq, const cplx* gsrc, int l0mode, bool back,
+                               int id, const cplx* dv, const cplx* dvt, const cplx* dvp) {
         // gsrc: for l != 0 the 1-based g0; for l = 0 the 1-based d0
-        for (int ir = 0; ir < r_n; ++ir) {
+        for (int ir = ir0; ir < ir1; ++ir) {
             cplx gt[2] = {}, gd[2] = {};
             if (l0mode) {
                 const cplx* gp = gsrc + jsta[ir];
@@ -879,19 +926,19 @@ void psv_one_frequency(const dsm_psv_setup_t& s, int ifreq, cplx* tsgt, cplx* rs
                 d.zero();
                 int bo = 15 * it + 3 * (m + 2);
                 if (fluid) {
-                    calupfluid(gt[0], comega, s.lambda[ir], s.qkp[ir], dvec[bo], d);
+                    calupfluid(gt[0], comega, s.lambda[ir], s.qkp[ir], dv[bo], d);
                 } else {
                     cplx u[3] = {}, udr[3] = {}, udt[3] = {}, udp[3] = {};
                     if (l0mode) {
-                        calup0(gt[0], dvec.data() + bo, u);
-                        calup0(gd[0], dvec.data() + bo, udr);
-                        calup0(gt[0], dvecdt.data() + bo, udt);
-                        calup0(gt[0], dvecdp.data() + bo, udp);
+                        calup0(gt[0], dv + bo, u);
+                        calup0(gd[0], dv + bo, udr);
+                        calup0(gt[0], dvt + bo, udt);
+                        calup0(gt[0], dvp + bo, udp);
                     } else {
-                        calup(gt[0], gt[1], lsq, dvec.data() + bo, u);
-                        calup(gd[0], gd[1], lsq, dvec.data() + bo, udr);
-                        calup(gt[0], gt[1], lsq, dvecdt.data() + bo, udt);
-                        calup(gt[0], gt[1], lsq, dvecdp.data() + bo, udp);
+                        calup(gt[0], gt[1], lsq, dv + bo, u);
+                        calup(gd[0], gd[1], lsq, dv + bo, udr);
+                        calup(gt[0], gt[1], lsq, dvt + bo, udt);
+                        calup(gt[0], gt[1], lsq, dvp + bo, udp);
                     }
                     lcd_psv(u, udr, udt, udp, d, s.r[ir], thr[it]);
                 }
@@ -900,22 +947,24 @@ void psv_one_frequency(const dsm_psv_setup_t& s, int ifreq, cplx* tsgt, cplx* rs
             }
         }
     };
-
-    for (int l = 0; l <= s.maxlmax; ++l) {
-        for (int it = 0; it < th_n; ++it)
-            caldvecphi0_withplm(l, thr[it], plm.data() + 12 * it, dvec.data() + 15 * it,
-                                dvecdt.data() + 15 * it, dvecdp.data() + 15 * it);
-        if (ismall > 20) {
-            if (llog > l) llog = l;
-            break;
+    auto receivers = [&](int m, double lsq, const cplx* gsrc, int l0mode, bool back, int id) {
+        const auto t0 = clock::now();
+        receivers_range(0, r_n, m, lsq, gsrc, l0mode, back, id, dvec.data(), dvecdt.data(), dvecdp.data());
+        theta_s += std::chrono::duration<double>(clock::now() - t0).count();
+    };
+    auto synn_terms = [&](int m, int imt, double lsq, cplx g1, cplx g2, bool l0mode, const cplx* dv) {
+        if (s.synn_switch != 1) return;
+        for (int th = 0; th < th_n; ++th) {
+            cplx u[3] = {};
+            if (l0mode) calup0(g1, dv + 15 * th + 3 * (m + 2), u);
+            else calup(g1, g2, lsq, dv + 15 * th + 3 * (m + 2), u);
+            utosynn(imt, u, synn + NS * th);
         }
-        double l2 = (double)l * (double)(l + 1);
-        double lsq = std::sqrt(l2);
-        cplx rdvec[15];
-        caldveczero(l, rdvec);
-        // cala (src/SGTpsv/calmat.f90:747-789) + calbc (:795-809)
-        for (int k = 1; k <= 4 * nn; ++k) a[k] = cplx(0.0);
-        auto Ag = [&](int i, int j) -> cplx& { return a[4 * (j - 1) + i]; };
+    };
+    // cala (src/SGTpsv/calmat.f90:747-789) + calbc (:795-809) into the band a
+    auto assemble = [&](std::vector<cplx>& ab, double l2, double lsq) {
+        for (int k = 1; k <= 4 * nn; ++k) ab[k] = cplx(0.0);
+        auto Ag = [&](int i, int j) -> cplx& { return ab[4 * (j - 1) + i]; };
         for (int j = 0; j < nzone; ++j) {
             int kk = s.kkdr[j];
             Band b0{A0[j].data()}, b1{A1[j].data()}, b2{A2[j].data()};
@@ -945,97 +994,218 @@ void psv_one_frequency(const dsm_psv_setup_t& s, int ifreq, cplx* tsgt, cplx* rs
             if (s.iphase[i - 1] == 2 && s.iphase[i] == 1)
                 Ag(3, s.kkdr[i]) = -cplx(s.vrmax[i - 1] * s.vrmax[i - 1]);
         }
-        int jtmp = s.jsrc;
+    };
+    // every right-hand side of order l >= 1, in the reference's sequence:
+    // m = -2..2 (|m| <= l): imt = 1..6 (calg, the factorisation once per
+    // order, dcsbdlv0 for the excited pairs), then the back-propagated
+    // sources (m = 0: vertical force; |m| = 1: icomp 2, 3)
+    struct Scratch {
+        std::vector<cplx> a, g0, z;
+    };
+    auto solve_order = [&](int l, Scratch& sc, PsvOrderSol& o) {
+        double l2 = (double)l * (double)(l + 1);
+        double lsq = std::sqrt(l2);
+        cplx rdvec[15];
+        caldveczero(l, rdvec);
+        assemble(sc.a, l2, lsq);
         cplx ya[4], yb[4], yc[4], yd[4];
         calya(anum.data(), bnum.data(), l2, rsrc, s.r0, ya, yb, yc, yd);
+        o.g.clear();
+        auto keep = [&]() {
+            for (int k = 0; k < ncap; ++k) o.g.push_back(sc.g0[caprow[k]]);
+        };
+        const int it = itmp_l, n1 = nn - it + 1;
         for (int m = -2; m <= 2; ++m) {
             if (!(std::abs(m) <= std::abs(l))) continue;
             int ig2 = 0;
-            if (l == 0) {
-                for (int imt = 1; imt <= 6; ++imt) {
-                    double mt[3][3];
-                    setmt(imt, mt);
-                    for (auto& v : g0) v = cplx(0.0);
-                    calg(l, m, coef1[spn0], coef2[spn0], lsq, s.ecC0, s.ecF0, s.ecL0, ya, yb, yc, yd,
-                         rsrc, s.r0, mt, g0.data() + jtmp);
-                    rea2(s, nn, a.data(), g0.data(), c.data(), d0.data(), jsta.data(), nn0);
-                    int it = itmp_l0;
-                    int n0 = nn0 - it + 1;
-                    dcsymbdl0(c.data() + 2 * (it - 1), 1, n0);
-                    bool solve = (m == 0 && imt <= 3);
-                    if (solve) dcsbdlv0(c.data() + 2 * (it - 1), d0.data() + (it - 1), 1, n0, z.data());
-                    if (s.synn_switch == 1) {
-                        for (int th = 0; th < th_n; ++th) {
-                            cplx u[3] = {};
-                            calup0(d0[nn0], dvec.data() + 15 * th + 3 * (m + 2), u);
-                            utosynn(imt, u, synn + NS * th);
-                        }
+            for (int imt = 1; imt <= 6; ++imt) {
+                double mt[3][3];
+                setmt(imt, mt);
+                for (auto& v : sc.g0) v = cplx(0.0);
+                calg(l, m, coef1[spn0], coef2[spn0], lsq, s.ecC0, s.ecF0, s.ecL0, ya, yb, yc, yd, rsrc, s.r0,
+                     mt, sc.g0.data() + jtmp);
+                if ((m == -2) || (m == -l)) {
+                    if (ig2 == 0) {
+                        dcsymbdl0(sc.a.data() + 4 * (it - 1), 3, n1);
+                        ig2 = 1;
                     }
-                    receivers(m, lsq, d0.data(), 1, false, imt);
                 }
-                if (m == 0 && s.rsgt_switch == 1) {
-                    for (auto& v : g0) v = cplx(0.0);
-                    g0[nn - 1] = -conj(rdvec[0 + 3 * (m + 2)]);
-                    rea2(s, nn, a.data(), g0.data(), nullptr, d0.data(), jsta.data(), nn0);
-                    int it = itmp_l0;
-                    dcsbdlv0(c.data() + 2 * (it - 1), d0.data() + (it - 1), 1, nn0 - it + 1, z.data());
-                    receivers(m, lsq, d0.data(), 1, true, 1);
-                }
-            } else {
-                for (int imt = 1; imt <= 6; ++imt) {
-                    double mt[3][3];
-                    setmt(imt, mt);
-                    for (auto& v : g0) v = cplx(0.0);
-                    calg(l, m, coef1[spn0], coef2[spn0], lsq, s.ecC0, s.ecF0, s.ecL0, ya, yb, yc, yd,
-                         rsrc, s.r0, mt, g0.data() + jtmp);
-                    int it = itmp_l;
-                    int n1 = nn - it + 1;
-                    if ((m == -2) || (m == -l)) {
-                        if (ig2 == 0) {
-                            dcsymbdl0(a.data() + 4 * (it - 1), 3, n1);
-                            ig2 = 1;
-                        }
-                    }
-                    int am = std::abs(m);
-                    bool solve = (am == 0 && imt <= 3) || (am == 1 && (imt == 4 || imt == 5)) ||
-                                 (am == 2 && (imt == 2 || imt == 3 || imt == 6));
-                    if (solve) dcsbdlv0(a.data() + 4 * (it - 1), g0.data() + (it - 1), 3, n1, z.data());
-                    if (imt == 1) {
-                        calamp_psv(g0.data() + ksta[r_n - 1] - 1, l, lsuf, maxamp, ismall, s.ratl);
-                        if (probe_out && m == 0 && l < probe_n) {
-                            double a1 = cabs(g0[ksta[r_n - 1] - 1]), a2 = cabs(g0[ksta[r_n - 1]]);
-                            probe_out[l] = std::sqrt(a1 * a1 + a2 * a2);
-                        }
-                    }
-                    if (s.synn_switch == 1) {
-                        for (int th = 0; th < th_n; ++th) {
-                            cplx u[3] = {};
-                            calup(g0[nn - 1], g0[nn], lsq, dvec.data() + 15 * th + 3 * (m + 2), u);
-                            utosynn(imt, u, synn + NS * th);
-                        }
-                    }
-                    receivers(m, lsq, g0.data(), 0, false, imt);
-                }
-                if (m == 0 && s.rsgt_switch == 1) {
-                    for (auto& v : g0) v = cplx(0.0);
-                    g0[nn - 1] = -conj(rdvec[0 + 3 * (m + 2)]);
-                    int it = itmp_l;
-                    dcsbdlv0(a.data() + 4 * (it - 1), g0.data() + (it - 1), 3, nn - it + 1, z.data());
-                    receivers(m, lsq, g0.data(), 0, true, 1);
-                }
-                if (std::abs(m) == 1 && s.rsgt_switch == 1) {
-                    for (int icomp = 2; icomp <= 3; ++icomp) {
-                        for (auto& v : g0) v = cplx(0.0);
-                        g0[nn] = conj(rdvec[(icomp - 1) + 3 * (m + 2)]) / cplx(lsq);
-                        int it = itmp_l;
-                        dcsbdlv0(a.data() + 4 * (it - 1), g0.data() + (it - 1), 3, nn - it + 1, z.data());
-                        receivers(m, lsq, g0.data(), 0, true, icomp);
-                    }
+                int am = std::abs(m);
+                bool solve = (am == 0 && imt <= 3) || (am == 1 && (imt == 4 || imt == 5)) ||
+                             (am == 2 && (imt == 2 || imt == 3 || imt == 6));
+                if (solve) dcsbdlv0(sc.a.data() + 4 * (it - 1), sc.g0.data() + (it - 1), 3, n1, sc.z.data());
+                keep();
+            }
+            if (m == 0 && s.rsgt_switch == 1) {
+                for (auto& v : sc.g0) v = cplx(0.0);
+                sc.g0[nn - 1] = -conj(rdvec[0 + 3 * (m + 2)]);
+                dcsbdlv0(sc.a.data() + 4 * (it - 1), sc.g0.data() + (it - 1), 3, n1, sc.z.data());
+                keep();
+            }
+            if (std::abs(m) == 1 && s.rsgt_switch == 1) {
+                for (int icomp = 2; icomp <= 3; ++icomp) {
+                    for (auto& v : sc.g0) v = cplx(0.0);
+                    sc.g0[nn] = conj(rdvec[(icomp - 1) + 3 * (m + 2)]) / cplx(lsq);
+                    dcsbdlv0(sc.a.data() + 4 * (it - 1), sc.g0.data() + (it - 1), 3, n1, sc.z.data());
+                    keep();
                 }
             }
         }
+    };
+    // the cutoff test of order l >= 1 (calamp for imt = 1 of every m, in the
+    // m order of the loop) from its solutions
+    auto cutoff_order = [&](int l, const PsvOrderSol& o) {
+        int k = 0;
+        for (int m = -2; m <= 2; ++m) {
+            if (!(std::abs(m) <= std::abs(l))) continue;
+            const cplx* src = o.g.data() + (size_t)k * ncap;
+            const cplx gp[2] = {src[capidx[ksta[r_n - 1] - 1]], src[capidx[ksta[r_n - 1]]]};
+            calamp_psv(gp, l, lsuf, maxamp, ismall, s.ratl);
+            if (probe_out && m == 0 && l < probe_n) {
+                double a1 = cabs(gp[0]), a2 = cabs(gp[1]);
+                probe_out[l] = std::sqrt(a1 * a1 + a2 * a2);
+            }
+            k += 6 + (m == 0 && s.rsgt_switch == 1 ? 1 : 0) + (std::abs(m) == 1 && s.rsgt_switch == 1 ? 2 : 0);
+        }
+    };
+    // terms of order l >= 1 for receivers [ir0, ir1) (task ir0 = r_n: SYNN),
+    // in the reference's m / source sequence; gb is the task's own g0
+    auto accumulate_order = [&](int l, const PsvOrderSol& o, int ir0, int ir1, std::vector<cplx>& gb,
+                                const cplx* dv, const cplx* dvt, const cplx* dvp) {
+        double l2 = (double)l * (double)(l + 1);
+        double lsq = std::sqrt(l2);
+        int k = 0;
+        auto load = [&]() {
+            const cplx* src = o.g.data() + (size_t)k * ncap;
+            for (int q = 0; q < ncap; ++q) gb[caprow[q]] = src[q];
+            ++k;
+        };
+        const bool synn_task = ir0 == r_n;
+        for (int m = -2; m <= 2; ++m) {
+            if (!(std::abs(m) <= std::abs(l))) continue;
+            for (int imt = 1; imt <= 6; ++imt) {
+                load();
+                if (synn_task) synn_terms(m, imt, lsq, gb[nn - 1], gb[nn], false, dv);
+                else receivers_range(ir0, ir1, m, lsq, gb.data(), 0, false, imt, dv, dvt, dvp);
+            }
+            if (m == 0 && s.rsgt_switch == 1) {
+                load();
+                if (!synn_task) receivers_range(ir0, ir1, m, lsq, gb.data(), 0, true, 1, dv, dvt, dvp);
+            }
+            if (std::abs(m) == 1 && s.rsgt_switch == 1) {
+                for (int icomp = 2; icomp <= 3; ++icomp) {
+                    load();
+                    if (!synn_task) receivers_range(ir0, ir1, m, lsq, gb.data(), 0, true, icomp, dv, dvt, dvp);
+                }
+            }
+        }
+    };
+    auto harmonics = [&](int l) {
+        const auto t0 = clock::now();
+        for (int it = 0; it < th_n; ++it)
+            caldvecphi0_withplm(l, thr[it], plm.data() + 12 * it, dvec.data() + 15 * it,
+                                dvecdt.data() + 15 * it, dvecdp.data() + 15 * it);
+        theta_s += std::chrono::duration<double>(clock::now() - t0).count();
+    };
+
+    // ---- l = 0 (the compact tridiagonal of rea2; its factor stays in c)
+    harmonics(0);
+    {
+        const int l = 0;
+        double l2 = 0.0, lsq = 0.0;
+        cplx rdvec[15];
+        caldveczero(l, rdvec);
+        assemble(a, l2, lsq);
+        cplx ya[4], yb[4], yc[4], yd[4];
+        calya(anum.data(), bnum.data(), l2, rsrc, s.r0, ya, yb, yc, yd);
+        const int m = 0;
+        for (int imt = 1; imt <= 6; ++imt) {
+            double mt[3][3];
+            setmt(imt, mt);
+            for (auto& v : g0) v = cplx(0.0);
+            calg(l, m, coef1[spn0], coef2[spn0], lsq, s.ecC0, s.ecF0, s.ecL0, ya, yb, yc, yd, rsrc, s.r0, mt,
+                 g0.data() + jtmp);
+            rea2(s, nn, a.data(), g0.data(), c.data(), d0.data(), jsta.data(), nn0);
+            int it = itmp_l0;
+            int n0 = nn0 - it + 1;
+            dcsymbdl0(c.data() + 2 * (it - 1), 1, n0);
+            bool solve = (imt <= 3);
+            if (solve) dcsbdlv0(c.data() + 2 * (it - 1), d0.data() + (it - 1), 1, n0, z.data());
+            {
+                const auto t0 = clock::now();
+                synn_terms(m, imt, lsq, d0[nn0], cplx(0.0), true, dvec.data());
+                theta_s += std::chrono::duration<double>(clock::now() - t0).count();
+            }
+            receivers(m, lsq, d0.data(), 1, false, imt);
+        }
+        if (s.rsgt_switch == 1) {
+            for (auto& v : g0) v = cplx(0.0);
+            g0[nn - 1] = -conj(rdvec[0 + 3 * (m + 2)]);
+            rea2(s, nn, a.data(), g0.data(), nullptr, d0.data(), jsta.data(), nn0);
+            int it = itmp_l0;
+            dcsbdlv0(c.data() + 2 * (it - 1), d0.data() + (it - 1), 1, nn0 - it + 1, z.data());
+            receivers(m, lsq, d0.data(), 1, true, 1);
+        }
+    }
+    // ---- l >= 1 in blocks
+    Pool pool(nthreads);
+    std::vector<Scratch> scr(nthreads);
+    for (auto& sc : scr) {
+        sc.a.assign(4 * nn + 1, cplx(0.0));
+        sc.g0.assign(nn + 1, cplx(0.0));
+        sc.z.assign(nn + 1, cplx(0.0));
+    }
+    const int blk = 8 * nthreads;
+    std::vector<PsvOrderSol> sol(blk);
+    const size_t hv = (size_t)15 * th_n;
+    std::vector<cplx> hdv(blk * hv), hdt(blk * hv), hdp(blk * hv);
+    // receiver tasks of the accumulation (contiguous ranges) and SYNN
+    const int ntask = std::min(r_n, 4 * nthreads);
+    std::vector<std::vector<cplx>> gtask(ntask + 1, std::vector<cplx>(nn + 1, cplx(0.0)));
+    bool done = false;
+    for (int lb = 1; lb <= s.maxlmax && !done; lb += blk) {
+        const int le = std::min(s.maxlmax, lb + blk - 1);
+        // 1. solves, in parallel over orders (each pool thread owns a scratch)
+        pool.run(le - lb + 1, [&](int i, int t) { solve_order(lb + i, scr[t], sol[i]); });
+        // 2. harmonics and the cutoff test in order
+        int lend = le + 1;
+        {
+            const auto t0 = clock::now();
+            for (int l = lb; l <= le; ++l) {
+                for (int it = 0; it < th_n; ++it)
+                    caldvecphi0_withplm(l, thr[it], plm.data() + 12 * it, dvec.data() + 15 * it,
+                                        dvecdt.data() + 15 * it, dvecdp.data() + 15 * it);
+                const size_t o = (size_t)(l - lb) * hv;
+                std::copy(dvec.begin(), dvec.end(), hdv.begin() + o);
+                std::copy(dvecdt.begin(), dvecdt.end(), hdt.begin() + o);
+                std::copy(dvecdp.begin(), dvecdp.end(), hdp.begin() + o);
+                if (ismall > 20) {
+                    if (llog > l) llog = l;
+                    done = true;
+                    lend = l;
+                    break;
+                }
+                const auto tc = clock::now();
+                cutoff_order(l, sol[l - lb]);
+                theta_s -= std::chrono::duration<double>(clock::now() - tc).count();
+            }
+            theta_s += std::chrono::duration<double>(clock::now() - t0).count();
+        }
+        // 3. accumulation of orders lb .. lend-1, in parallel over receivers
+        const auto t0 = clock::now();
+        pool.run(ntask + 1, [&](int task, int) {
+            const int ir0 = task < ntask ? (int)((long)task * r_n / ntask) : r_n;
+            const int ir1 = task < ntask ? (int)((long)(task + 1) * r_n / ntask) : r_n;
+            for (int l = lb; l < lend; ++l) {
+                const size_t o = (size_t)(l - lb) * hv;
+                accumulate_order(l, sol[l - lb], ir0, ir1, gtask[task], hdv.data() + o, hdt.data() + o,
+                                 hdp.data() + o);
+            }
+        });
+        theta_s += std::chrono::duration<double>(clock::now() - t0).count();
     }
     *llog_out = llog;
+    if (t_theta) *t_theta = theta_s;
 }
 
 }  // namespace oracle
@@ -1061,6 +1231,33 @@ extern "C" int oracle_psv_run(const dsm_psv_setup_t* s, const int* ilist, int n,
     for (int k = 0; k < n; ++k) {
         int lg = 0;
         oracle::psv_one_frequency(*s, ilist[k], t.data(), r.data(), y.data(), &lg);
+        if (tsgt) std::memcpy(tsgt + 2 * nt * k, t.data(), sizeof(cplx) * nt);
+        if (rsgt) std::memcpy(rsgt + 2 * nr * k, r.data(), sizeof(cplx) * nr);
+        if (synn) std::memcpy(synn + 2 * ns * k, y.data(), sizeof(cplx) * ns);
+        if (llog) llog[k] = lg;
+    }
+    return 0;
+}
+
+// One frequency after another, each spread over nthreads host threads
+// (order-parallel solves, receiver-parallel theta loop); t_theta[k] (if
+// given) receives frequency k's time in its theta-proportional parts and
+// t_total[k] its whole time.
+extern "C" int oracle_psv_run_threads(const dsm_psv_setup_t* s, const int* ilist, int n, double* tsgt,
+                                      double* rsgt, double* synn, int* llog, int nthreads, double* t_theta,
+                                      double* t_total) {
+    using oracle::cplx;
+    long nt = (long)DSM_PSV_NUM_TSGT * s->r_n * s->theta_n;
+    long nr = (long)DSM_PSV_NUM_RSGT * s->r_n * s->theta_n;
+    long ns = (long)DSM_PSV_NUM_SYNN * s->theta_n;
+    std::vector<cplx> t(nt), r(nr), y(ns);
+    for (int k = 0; k < n; ++k) {
+        int lg = 0;
+        double tt = 0.0;
+        const auto t0 = std::chrono::steady_clock::now();
+        oracle::psv_one_frequency(*s, ilist[k], t.data(), r.data(), y.data(), &lg, nullptr, 0, nthreads, &tt);
+        if (t_total) t_total[k] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (t_theta) t_theta[k] = tt;
         if (tsgt) std::memcpy(tsgt + 2 * nt * k, t.data(), sizeof(cplx) * nt);
         if (rsgt) std::memcpy(rsgt + 2 * nr * k, r.data(), sizeof(cplx) * nr);
         if (synn) std::memcpy(synn + 2 * ns * k, y.data(), sizeof(cplx) * ns);
