@@ -602,6 +602,10 @@ int cat_points(dsm_cat_t* c, int npoint, const double* distance, int nout, const
         const bool identity = coef == nullptr;
         if (identity) nout = p.num;
         need(nout >= 1 && nout <= MAX_OUT, fn + ": nout must be in [1, 64]");
+        // device outputs are written with 16-byte (complex128 spectra) or
+        // 8-byte (series) stores
+        if (out_on_device)
+            need(((uintptr_t)out % (spectra ? 16 : 8)) == 0, fn + ": misaligned device output");
         if (npoint == 0) return;
         DSM_CUDA(cudaSetDevice(c->dev));
         const int nh = p.np1 + 1, nwin = c->nwin();
@@ -882,6 +886,7 @@ extern "C" int dsm_cat_transform(dsm_cat_t* c, int nseries, const void* spectra,
         const int nh = p.np1 + 1, nwin = c->nwin(), nf = p.fmax - p.fmin + 1;
         if (spectra_on_device)
             need(((uintptr_t)spectra % 16) == 0, "dsm_cat_transform: misaligned device spectra");
+        if (out_on_device) need(((uintptr_t)out % 8) == 0, "dsm_cat_transform: misaligned device output");
         // series per batch: the in-place transform buffer stays under max_batch_bytes
         const int pc = (int)std::min<size_t>((size_t)nseries, std::max<size_t>(1, c->max_batch_bytes / (nh * sizeof(cd))));
         const cd* dx = static_cast<const cd*>(spectra);

@@ -238,3 +238,31 @@ def test_catalogue_spectra_and_transform_match_oracle(built, fmin, c_red):
                                 p["iwin_end"])
     assert got.shape == ref.shape
     assert rel_l2(got, ref) <= TOL
+
+
+@pytest.mark.gpu
+def test_catalogue_rejects_misaligned_device_outputs(built):
+    """Device outputs are written with 16-byte (spectra) or 8-byte (series)
+    stores: a pointer off that alignment is rejected before anything runs.
+    The calls ask for zero points, so even without the check no kernel would
+    touch the pointer."""
+    import ctypes as C
+    import torch
+    p = _params()
+    c = dsmsgt.Catalogue(p)
+    c.add(_records(p, 20, 3))
+    buf = torch.empty(64, dtype=torch.complex128, device="cuda")
+    d = np.zeros(1)
+    L = dsmsgt.lib()
+    rc = L.dsm_cat_spectra(c.h, 0, d.ctypes.data_as(C.POINTER(C.c_double)), 20, None,
+                           C.c_void_p(buf.data_ptr() + 8), 1)
+    assert rc == dsmsgt.DSM_ERR_INVALID and b"misaligned" in L.dsm_cat_last_error(c.h)
+    rc = L.dsm_cat_series(c.h, 0, d.ctypes.data_as(C.POINTER(C.c_double)), 20, None,
+                          C.c_void_p(buf.data_ptr() + 4), 1)
+    assert rc == dsmsgt.DSM_ERR_INVALID and b"misaligned" in L.dsm_cat_last_error(c.h)
+    rc = L.dsm_cat_spectra(c.h, 0, d.ctypes.data_as(C.POINTER(C.c_double)), 20, None,
+                           C.c_void_p(buf.data_ptr() + 16), 1)
+    assert rc == dsmsgt.DSM_OK
+    got = c.series(DIST)
+    c.close()
+    assert rel_l2(got, _oracle(p, [(_records(p, 20, 3), np.arange(20), np.ones(20))], DIST)) <= TOL
