@@ -1,15 +1,17 @@
 """Oracle set-up -- test infrastructure only.
 
 An independent restatement, in numpy, of the part of the reference's P-SV
-driver that runs once before the frequency loop: input parsing, radial grid,
-receivers, source position and the element integrals
-(src/SGTpsv/SGTpsv-MPI.f90:39-477 with the routines of
-src/SGTpsv/others.f90 and src/SGTpsv/calmat.f90:1-404).  It fills the
-engine's C-ABI set-up struct (include/dsmsgt.h, dsm_psv_setup_t) from its own
-arrays, so the oracle's frequency loop (liboracle.so) and the CPU baseline
-can run without the product library.  Tests compare it element by element
-with the product's driver-side set-up (host/setup.cpp), which pins that set-up
-to a second, separately written restatement of the Fortran.
+and SH drivers that runs once before the frequency loop: input parsing,
+radial grid, receivers, source position and the element integrals
+(src/SGTpsv/SGTpsv-MPI.f90:39-477 with the routines of src/SGTpsv/others.f90
+and src/SGTpsv/calmat.f90:1-404; src/SGTsh/SGTsh-MPI.f90:33-347 with
+src/SGTsh/others.f90:380-742 and src/SGTsh/calmat.f90:1-160).  It fills the
+engine's C-ABI set-up structs (include/dsmsgt.h, dsm_psv_setup_t and
+dsm_sh_setup_t) from its own arrays, so the oracle's frequency loops
+(liboracle.so) and the CPU baseline run without the product library.  Tests
+compare it element by element with the product's driver-side set-up
+(host/setup.cpp), which pins that set-up to a second, separately written
+restatement of the Fortran.
 
 Layer loops are vectorised per zone; every element keeps the Fortran
 operation order (numpy performs one IEEE operation per element, without
@@ -226,10 +228,12 @@ class _Zone:
         self.cons = cons
 
 
-def calmatc(zone: _Zone, con, rpow: int, w1dn: int, w2dn: int) -> np.ndarray:
+def calmatc(zone: _Zone, con, rpow: int, w1dn: int, w2dn: int, symmetrise: bool = False) -> np.ndarray:
     """calmatc, src/SGTpsv/calmat.f90:1-62: 4 entries per layer,
     (j, k) = (1,1), (1,2), (2,1), (2,2), of the integral of
-    r^rpow con W_j^(w1dn) W_k^(w2dn) over the layer."""
+    r^rpow con W_j^(w1dn) W_k^(w2dn) over the layer.  The SH version
+    (src/SGTsh/calmat.f90:1-83) symmetrises when w1dn /= w2dn: diagonal
+    entries doubled, both off-diagonal entries their sum."""
     lo, hi = zone.lo, zone.hi
     rh = hi - lo
     zero = np.zeros_like(rh)
@@ -251,6 +255,9 @@ def calmatc(zone: _Zone, con, rpow: int, w1dn: int, w2dn: int) -> np.ndarray:
             if rpow > 0:
                 c = [zero] * rpow + c[:3] + [zero] * (2 - rpow)
             out[:, 2 * j + k] = _pinteg_seg(c, lo, hi, c0, c1, lo, hi)
+    if symmetrise and w1dn != w2dn:
+        off = out[:, 1] + out[:, 2]
+        out = np.stack([2.0 * out[:, 0], off, off, 2.0 * out[:, 3]], axis=1)
     return out.reshape(-1)
 
 
@@ -581,6 +588,7 @@ class PsvOracleSetup:
         s.tlen, s.omegai, s.ratl, s.maxlmax = tlen, omegai, conf["ratl"], conf["maxlmax"]
         s.imin, s.imax = par["imin"], par["imax"]
         s.rsgt_switch, s.tsgt_switch, s.synn_switch = par["rsgt"], par["tsgt"], par["synn"]
+        s._owner = self  # the struct points into arrays this object holds
         self.s = s
         self.ptr = C.pointer(s)
         self.n_nodes, self.n_unknowns = nnlayer + 1, nn
@@ -601,3 +609,174 @@ class PsvOracleSetup:
 def psv_setup(job) -> PsvOracleSetup:
     """The oracle's P-SV set-up of a job (parameter file, DSM.config, model)."""
     return PsvOracleSetup(job.param_text, job.conf_text, job.model_text)
+
+
+# ---------------------------------------------------------------- SH set-up
+class ShOracleSetup:
+    """The SH set-up struct (dsm_sh_setup_t) filled from this module's own
+    arrays (src/SGTsh/SGTsh-MPI.f90:33-347)."""
+
+    mode = "sh"
+    num = (10, 5, 5)
+
+    def __init__(self, param_text: str, conf_text: str, model_text: str):
+        from dsmsgt import ShSetup  # the ctypes layout of the C-ABI struct only
+        par, conf, full = parse_params(param_text), parse_conf(conf_text), parse_model(model_text)
+        # the outer-core cut (:83-102, :123-133): zones above the last fluid
+        # zone (ioutercore = 0 when there is none)
+        iout = 0
+        for z in range(full["nzone"]):
+            if np.all(full["vsv"][:, z] == 0.0):
+                iout = z + 1
+        nz = full["nzone"] - iout
+        if nz <= 0:
+            raise ValueError("SH: no solid zone above the outer core")
+        m = {k: (v[iout:] if v.ndim == 1 else v[:, iout:]) for k, v in full.items() if k != "nzone"}
+        m["nzone"] = nz
+        rmin, rmax = m["vrmin"][0], m["vrmax"][nz - 1]
+        tlen = par["tlen"]
+        omegai = -math.log(conf["omegai"]) / tlen
+        # receivers above rmin (:152-179)
+        rmin_, rdelta_ = par["rmin_"], par["rdelta_"]
+        r_n = int((par["rmax_"] - rmin_) / rdelta_) + 1
+        ir_ = 0
+        for i in range(1, r_n + 1):
+            if rmin_ + float(i - 1) * rdelta_ <= rmin:
+                ir_ = i
+        r_n -= ir_
+        rmin_ = rmin_ + float(ir_) * rdelta_
+        if r_n <= 0:
+            raise ValueError("SH: no receiver above rmin")
+        r_ = np.array([rmin_ + float(i) * rdelta_ for i in range(r_n)])
+        theta_n = int((par["thetamax"] - par["thetamin"]) / par["thetadelta"]) + 1
+        theta = np.array([par["thetamin"] + float(i) * par["thetadelta"] for i in range(theta_n)])
+        r0 = par["r0min"]
+        # calgrid (SH: Vs in every zone, src/SGTsh/others.f90:380-459)
+        msh = dict(m, vpv=m["vsv"])
+        _, _, dzpar = calgrid_psv(msh, rmin, rmax, par["imax"], 1, tlen)
+        nlayer = layers_psv(m, dzpar, conf["re"])  # calra (:463-495): same rule
+        nnlayer = int(nlayer.sum())
+        ra = node_radii(m, nlayer, rmin)
+        # receiver bracketing, calra2 (:500-563): global node indices
+        rrsta = np.zeros((r_n, 3))
+        iista = np.zeros((r_n, 3), np.int32)
+        itmp = 0
+        for z in range(nz):
+            for i in range(1, nlayer[z] + 1):
+                hit = (ra[itmp] < r_) & (r_ <= ra[itmp + 1])
+                for ista in np.nonzero(hit)[0]:
+                    b = itmp if i != nlayer[z] else itmp - 1
+                    rrsta[ista] = ra[b:b + 3]
+                    iista[ista] = [b + 1, b + 2, b + 3]
+                itmp += 1
+        if np.any(iista[:, 0] <= 0):
+            raise ValueError("SH: receiver outside the grid")
+        # calsp (:569-584)
+        isp, jsp = np.ones(nz, np.int32), np.ones(nz, np.int32)
+        for z in range(1, nz):
+            isp[z] = isp[z - 1] + nlayer[z - 1]
+            jsp[z] = jsp[z - 1] + 4 * nlayer[z - 1]
+        # calspo (:588-631) and calgra (:637-647)
+        ndc = nz - 1
+        if r0 < rmin or r0 > rmax:
+            raise ValueError("The source location is improper.(calspo)")
+        if r0 == rmax:
+            spo = float(nnlayer) - 0.01
+            r0 = ra[nnlayer - 1] + (spo - float(nnlayer - 1)) * (ra[nnlayer] - ra[nnlayer - 1])
+        else:
+            k = 2
+            while k <= ndc + nnlayer + 2 and not (r0 < ra[k - 1]):
+                k += 1
+            spo = float(k - 2) + (r0 - ra[k - 2]) / (ra[k - 1] - ra[k - 2])
+            if spo - float(k - 2) < 0.01:
+                spo = float(k - 2) + 0.01
+                r0 = ra[k - 2] + (spo - float(k - 2)) * (ra[k - 1] - ra[k - 2])
+            if spo - float(k - 2) > 0.99:
+                spo = float(k - 2) + 0.99
+                r0 = ra[k - 2] + (spo - float(k - 2)) * (ra[k - 1] - ra[k - 2])
+        spn = 0
+        for z in range(nz):
+            spn += 1
+            if r0 <= m["vrmax"][z]:
+                break
+        spo = spo - float(isp[spn - 1] - 1)
+        igr = int(isp[spn - 1]) + int(math.trunc(spo))
+        gra = np.array([ra[igr - 1], r0, ra[igr]])
+
+        def structure(z, x):  # calstg (:651-694) / calgstg (:699-742)
+            rho = np.array([_poly_at(m["rho"][:, z], xi, rmax) for xi in x])
+            vsv = np.array([_poly_at(m["vsv"][:, z], xi, rmax) for xi in x])
+            vsh = np.array([_poly_at(m["vsh"][:, z], xi, rmax) for xi in x])
+            return {"rho": rho, "ecL": rho * vsv * vsv, "ecN": rho * vsh * vsh}
+
+        # element integrals (:314-339)
+        t, h1, h2, h3, h4 = (np.zeros(4 * nnlayer) for _ in range(5))
+
+        def integrals(zn, cs):
+            return (calt(calmatc(zn, cs["rho"], 2, 0, 0), _lumped(zn, cs["rho"], True)),
+                    calmatc(zn, cs["ecL"], 2, 1, 1),
+                    calmatc(zn, cs["ecL"], 1, 1, 0, symmetrise=True),
+                    calt(calmatc(zn, cs["ecL"], 0, 0, 0), _lumped(zn, cs["ecL"], False)),
+                    calt(calmatc(zn, cs["ecN"], 0, 0, 0), _lumped(zn, cs["ecN"], False)))
+
+        for z in range(nz):
+            x = ra[isp[z] - 1: isp[z] - 1 + nlayer[z] + 1]
+            sl = slice(jsp[z] - 1, jsp[z] - 1 + 4 * nlayer[z])
+            t[sl], h1[sl], h2[sl], h3[sl], h4[sl] = integrals(_Zone(x, None), structure(z, x))
+        gcs = structure(spn - 1, gra)
+        mu0 = gcs["ecL"][1]
+        gt, gh1, gh2, gh3, gh4 = integrals(_Zone(gra, None), gcs)
+        ns = int(isp[spn - 1]) + int(math.trunc(spo))
+        ins = 4 * ns - 3
+
+        self._keep = []
+
+        def dp(a):
+            a = np.ascontiguousarray(a, np.float64)
+            self._keep.append(a)
+            return a.ctypes.data_as(C.POINTER(C.c_double))
+
+        def ip(a):
+            a = np.ascontiguousarray(a, np.int32)
+            self._keep.append(a)
+            return a.ctypes.data_as(C.POINTER(C.c_int))
+
+        s = ShSetup()
+        s.nzone = nz
+        s.vrmin, s.vrmax, s.vsv, s.qmu = dp(m["vrmin"]), dp(m["vrmax"]), dp(m["vsv"].T.reshape(-1)), dp(m["qmu"])
+        s.nlayer, s.isp, s.jsp = ip(nlayer), ip(isp), ip(jsp)
+        s.nnlayer = nnlayer
+        s.t, s.h1, s.h2, s.h3, s.h4 = dp(t), dp(h1), dp(h2), dp(h3), dp(h4)
+        s.spn, s.spo, s.r0, s.mu0, s.ins = spn, spo, r0, mu0, ins
+        s.gt, s.gh1, s.gh2, s.gh3, s.gh4 = dp(gt), dp(gh1), dp(gh2), dp(gh3), dp(gh4)
+        s.r_n, s.r, s.rrsta, s.iista = r_n, dp(r_), dp(rrsta.reshape(-1)), ip(iista.reshape(-1))
+        s.theta_n, s.theta = theta_n, dp(theta)
+        s.tlen, s.omegai, s.ratl, s.maxlmax = tlen, omegai, conf["ratl"], conf["maxlmax"]
+        s.imin, s.imax = par["imin"], par["imax"]
+        s.rsgt_switch, s.tsgt_switch, s.synn_switch = par["rsgt"], par["tsgt"], par["synn"]
+        s._owner = self  # the struct points into arrays this object holds
+        self.s = s
+        self.ptr = C.pointer(s)
+        self.n_nodes = self.n_unknowns = nnlayer + 1
+
+    @property
+    def r_n(self) -> int:
+        return self.s.r_n
+
+    @property
+    def theta_n(self) -> int:
+        return self.s.theta_n
+
+    def out_shapes(self, n: int):
+        nt, nr, ns = self.num
+        return ((n, self.theta_n, self.r_n, nt), (n, self.theta_n, self.r_n, nr), (n, self.theta_n, ns))
+
+
+def sh_setup(job) -> ShOracleSetup:
+    """The oracle's SH set-up of a job (parameter file, DSM.config, model)."""
+    return ShOracleSetup(job.param_text, job.conf_text, job.model_text)
+
+
+def setup(job, mode: str):
+    """The oracle's set-up of a job for mode "psv" or "sh"."""
+    return psv_setup(job) if mode == "psv" else sh_setup(job)

@@ -1,10 +1,13 @@
 """Oracle loader -- test infrastructure only.
 
 ctypes wrapper of ``oracle/build/liboracle.so``, the CPU FP64 restatement of
-the SGTsh / SGTpsv frequency loops.  Only tests/, ``__graft_entry__.smoke()``
-and the CPU-baseline leg of ``bench.py`` may import this module; the product
-(``dsm-kernel_b200``) never does.  Parity status: unpinned (the Fortran
-reference cannot be built here and ships no test vectors).
+the SGTsh / SGTpsv frequency loops; its set-ups come from
+``oracle/driver_setup.py`` (the oracle's own restatement of the drivers'
+set-up), so an oracle run maps no product library.  Only tests/,
+``__graft_entry__.smoke()`` and the CPU legs of ``bench.py`` may import this
+module; the product (``dsm-kernel_b200``) never does.  Parity status:
+unpinned (the Fortran reference cannot be built here and ships no test
+vectors).
 """
 from __future__ import annotations
 

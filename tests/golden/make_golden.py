@@ -26,11 +26,11 @@ CASES = {
 
 
 def compute(name):
-    import dsmsgt
+    """The oracle on its own set-up of the case's job."""
     import cases
-    from oracle import oracle as orc
+    from oracle import driver_setup, oracle as orc
     mode, fn, kw, freqs = CASES[name]
-    s = dsmsgt.Setup(getattr(cases, fn)(**kw), mode)
+    s = driver_setup.setup(getattr(cases, fn)(**kw), mode)
     t, r, y, llog = orc.run(s, freqs, threads=os.cpu_count() or 1)
     return s, freqs, t, r, y, llog
 

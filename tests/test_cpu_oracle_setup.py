@@ -1,9 +1,10 @@
-"""The oracle's own P-SV set-up (oracle/driver_setup.py, a numpy restatement
-of the reference's grid, receiver, source and element-integral routines)
+"""The oracle's own set-ups (oracle/driver_setup.py, a numpy restatement of
+the reference's grid, receiver, source and element-integral routines)
 against the product's driver-side set-up (host/setup.cpp through
-dsm_psv_setup_build), field by field and bit for bit: two separately written
-restatements of src/SGTpsv/SGTpsv-MPI.f90:39-477 pin each other.  Also: the
-oracle's frequency loop gives the same values on any number of threads."""
+dsm_psv_setup_build / dsm_sh_setup_build), field by field and bit for bit:
+two separately written restatements of src/SGTpsv/SGTpsv-MPI.f90:39-477 and
+src/SGTsh/SGTsh-MPI.f90:33-347 pin each other.  Also: the oracle's P-SV
+frequency loop gives the same values on any number of threads."""
 import ctypes as C
 import os
 import sys
@@ -12,7 +13,7 @@ import numpy as np
 import pytest
 
 import dsmsgt
-from cases import psv_small
+from cases import psv_small, sh_small
 
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 import bench  # noqa: E402  (the benchmark workloads' jobs)
@@ -87,3 +88,33 @@ def test_oracle_on_its_own_setup_matches_the_product_setup_run(built):
     b = orc.run(driver_setup.psv_setup(job), [5, 17])
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+SH_INT = ("nzone", "nnlayer", "spn", "ins", "r_n", "theta_n", "maxlmax", "imin", "imax", "rsgt_switch",
+          "tsgt_switch", "synn_switch")
+SH_REAL = ("spo", "r0", "mu0", "tlen", "omegai", "ratl")
+
+SH_JOBS = {
+    "sh_small": lambda: sh_small(),
+    "sh_small_seed1": lambda: sh_small(seed=1),
+    "sh256": lambda: bench.workload("sh256")[0],
+    # the outer-core cut and the receivers at or below the CMB dropped
+    "sh_on_the_psv_earth": lambda: psv_small(),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SH_JOBS))
+def test_oracle_sh_setup_equals_product_setup(built, name):
+    job = SH_JOBS[name]()
+    prod = dsmsgt.Setup(job, "sh")
+    own = driver_setup.sh_setup(job)
+    a, b = prod.s, own.s
+    bad = [f for f in SH_INT + SH_REAL if getattr(a, f) != getattr(b, f)]
+    nz, R, nl = a.nzone, a.r_n, a.nnlayer
+    for f, n in (("vrmin", nz), ("vrmax", nz), ("vsv", 4 * nz), ("qmu", nz), ("nlayer", nz), ("isp", nz),
+                 ("jsp", nz), ("t", 4 * nl), ("h1", 4 * nl), ("h2", 4 * nl), ("h3", 4 * nl), ("h4", 4 * nl),
+                 ("gt", 8), ("gh1", 8), ("gh2", 8), ("gh3", 8), ("gh4", 8), ("r", R), ("rrsta", 3 * R),
+                 ("iista", 3 * R), ("theta", a.theta_n)):
+        if not np.array_equal(_arr(getattr(a, f), n), _arr(getattr(b, f), n)):
+            bad.append(f)
+    assert bad == []

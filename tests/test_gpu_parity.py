@@ -1,7 +1,9 @@
 """CUDA engine vs the FP64 oracle (the CPU restatement of the reference).
 
 The plain FP64 path must match the oracle to 1e-10 relative L2 per output
-array, with an identical realised cutoff (llog) per frequency.
+array, with an identical realised cutoff (llog) per frequency.  The oracle
+runs on its own set-up (oracle/driver_setup.py), built from the same job as
+the engine's.
 """
 import numpy as np
 import pytest
@@ -14,10 +16,10 @@ TOL_FP64 = 1e-10
 
 
 def _compare(setup, freqs, ctx_kwargs=None, tol=TOL_FP64):
-    from oracle import oracle as orc
+    from oracle import driver_setup, oracle as orc
     ctx = dsmsgt.Context(setup, **(ctx_kwargs or {}))
     t, r, y, llog = ctx.run(freqs)
-    ot, orr, oy, ollog = orc.run(setup, freqs, threads=8)
+    ot, orr, oy, ollog = orc.run(driver_setup.setup(setup.job, setup.mode), freqs, threads=8)
     assert list(llog) == list(ollog)
     errs = {"tsgt": rel_l2(t, ot), "rsgt": rel_l2(r, orr), "synn": rel_l2(y, oy)}
     for k, v in errs.items():
