@@ -590,9 +590,13 @@ __device__ __forceinline__ void fwd_row(int k, const StepOut& so, FwdState& F, c
 // first FAC_NW of a block read their rows from global memory.  All threads
 // of a block take the same steps (the same n), so the block-wide barriers at
 // chunk boundaries are uniform; threads past nsys repeat the last system's
-// work without storing it.  The steps below the source rows run without the
-// forward-substitution state, which keeps the registers of that (long) part
-// down.
+// work without storing it.
+// The factorisation runs as two launches.  LOWER takes the steps below the
+// source rows, where the forward substitution has nothing to do (most of
+// the band), without its state, so its registers stay low and more warps
+// hide the recurrence's latency; it leaves each system's 4x4 window in
+// FacState.  UPPER resumes from that window and runs the rest with the
+// forward substitution.  Both take the same operations as one pass would.
 constexpr int FAC_THREADS = 128;
 #ifndef DSM_FAC_CH
 #define DSM_FAC_CH 16
@@ -601,10 +605,26 @@ constexpr int FAC_CH = DSM_FAC_CH;  // rows per chunk (multiple of 4)
 static_assert(FAC_CH % 4 == 0, "chunks hold whole groups of four steps");
 constexpr int FAC_NW = 4;   // frequencies staged per block
 
-template <bool FAST>
-__global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
+// window of a system between the two factorisation launches
+struct FacState {
+    cd M[4][4];
+    cd a22raw;
+};
+// first step of the upper launch: the first group of four steps that
+// reaches row ls - 4 (the forward substitution reads the three multipliers
+// before row ls) or the last four rows of the band
+__host__ __device__ __forceinline__ int fac_split(int n, int ls) {
+    const int kf = ls - 3;
+    int k = 1;
+    while (k + 3 < kf && k + 3 <= n - 4) k += 4;
+    return k;
+}
+
+template <bool FAST, bool UPPER>
+__global__ void __launch_bounds__(FAC_THREADS, UPPER ? 1 : 4) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
                                                            int nsys, int lmin, cd* __restrict__ Lst,
-                                                           cd* __restrict__ Zst, SysTail* __restrict__ tail) {
+                                                           cd* __restrict__ Zst, SysTail* __restrict__ tail,
+                                                           FacState* __restrict__ fst) {
     __shared__ __align__(16) cd sP[2][FAC_NW][FAC_CH][12];
     const int sys0 = blockIdx.x * FAC_THREADS;
     const int sysv = sys0 + threadIdx.x;
@@ -632,6 +652,7 @@ __global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* _
     c.Lst = Lst;
     c.Zst = Zst;
     const int n = c.n;
+    const int ksplit = fac_split(n, c.ls);
     // local rows 5 .. n in chunks: chunk q = rows 5 + q CH .. (global it + r - 1)
     auto stage = [&](int q, int buf) {
         const int r0 = 5 + q * FAC_CH;
@@ -643,31 +664,51 @@ __global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* _
             cp_async16(&sP[buf][wi][i][v], Prow + ((size_t)(w0 + wi) * (d.nn + 1) + c.it + r0 + i - 1) * 12 + v);
         }
     };
-    stage(0, 0);
-    cp_async_commit();
     cd M[4][4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) M[p][q] = mk(0.0);
     cd a[4];
     RowPieces rp;
-    // local rows 1..4 go to slots 1, 2, 3, 0
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-        if (p >= n) break;
-        load_row(c.P + (size_t)(c.it + p) * 12, rp);
-        assemble_row<FAST>(rp, c.l2, c.lsq, a);
-#pragma unroll
-        for (int q = 0; q <= p; ++q) M[(1 + p) & 3][(1 + q) & 3] = a[4 - (p - q) - 1];
-    }
     SysTail T;
-    // dcsbdlv0 reads a(m-1,2) = a(2,2) of the unfactored band at row 2
-    load_row(c.P + (size_t)(c.it + 1) * 12, rp);
-    assemble_row<FAST>(rp, c.l2, c.lsq, a);
-    T.a22raw = a[1];
     T.Dm1 = mk(1.0);
     T.Lnn1 = mk(0.0);
+    int k = 1;
+    if (!UPPER) {
+        stage(0, 0);
+        cp_async_commit();
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) M[p][q] = mk(0.0);
+        // local rows 1..4 go to slots 1, 2, 3, 0
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (p >= n) break;
+            load_row(c.P + (size_t)(c.it + p) * 12, rp);
+            assemble_row<FAST>(rp, c.l2, c.lsq, a);
+#pragma unroll
+            for (int q = 0; q <= p; ++q) M[(1 + p) & 3][(1 + q) & 3] = a[4 - (p - q) - 1];
+        }
+        // dcsbdlv0 reads a(m-1,2) = a(2,2) of the unfactored band at row 2
+        load_row(c.P + (size_t)(c.it + 1) * 12, rp);
+        assemble_row<FAST>(rp, c.l2, c.lsq, a);
+        T.a22raw = a[1];
+    } else {
+        const FacState& f = fst[sys];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) M[p][q] = f.M[p][q];
+        T.a22raw = f.a22raw;
+        k = ksplit;
+        // the chunk holding the row that enters at step ksplit, and, unless
+        // a chunk starts there (its boundary stages the next one), the next
+        // chunk: the single pass would have it in flight already
+        const int q0 = (k - 1) / FAC_CH;
+        stage(q0, q0 & 1);
+        if ((k - 1) % FAC_CH != 0) stage(q0 + 1, (q0 + 1) & 1);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+    }
     // row entering at step k: local row k+4, chunk (k-1)/CH, index (k-1)%CH
     auto entering = [&](int k, cd (&an)[4]) {
         if (k + 4 > n) return;
@@ -692,66 +733,77 @@ __global__ void __launch_bounds__(FAC_THREADS) k_psv_solve(PsvDev d, const cd* _
     };
     cd an[4];
     StepOut so;
-    int k = 1;
-    // steps whose multipliers the forward substitution never reads: four
-    // main steps at a time, up to the group that reaches row ls - 4
-    const int kf = c.ls - 3;
-    for (; k + 3 < kf && k + 3 <= n - 4; k += 4) {
-        boundary(k);
-        entering(k, an);
-        factor_step_main<1, FAST>(k, M, an, c, so);
-        entering(k + 1, an);
-        factor_step_main<2, FAST>(k + 1, M, an, c, so);
-        entering(k + 2, an);
-        factor_step_main<3, FAST>(k + 2, M, an, c, so);
-        entering(k + 3, an);
-        factor_step_main<0, FAST>(k + 3, M, an, c, so);
-        if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
-    }
-    // the rest, with the forward substitution
-    FwdState F;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) F.z[b][0] = F.z[b][1] = F.z[b][2] = mk(0.0);
-    F.w0_1 = F.w1_1 = F.w1_2 = F.w2_1 = F.w2_2 = F.w2_3 = mk(0.0);
-    for (;; k += 4) {
-        boundary(k);
-        if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
+    if (!UPPER) {
+        // steps whose multipliers the forward substitution never reads: four
+        // main steps at a time, up to the group that reaches row ls - 4
+        for (; k < ksplit; k += 4) {
+            boundary(k);
             entering(k, an);
             factor_step_main<1, FAST>(k, M, an, c, so);
-            fwd_row<FAST>(k, so, F, T, c);
             entering(k + 1, an);
             factor_step_main<2, FAST>(k + 1, M, an, c, so);
-            fwd_row<FAST>(k + 1, so, F, T, c);
             entering(k + 2, an);
             factor_step_main<3, FAST>(k + 2, M, an, c, so);
-            fwd_row<FAST>(k + 2, so, F, T, c);
             entering(k + 3, an);
             factor_step_main<0, FAST>(k + 3, M, an, c, so);
-            fwd_row<FAST>(k + 3, so, F, T, c);
-            if ((k + 3) % FAC_CH == 0) __syncthreads();
-            continue;
+            if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
         }
-        bool last;
-        entering(k, an);
-        last = factor_step<1, FAST>(k, M, an, T, c, so);
-        fwd_row<FAST>(k, so, F, T, c);
-        if (last) { T.Dn = M[1][1]; break; }
-        entering(k + 1, an);
-        last = factor_step<2, FAST>(k + 1, M, an, T, c, so);
-        fwd_row<FAST>(k + 1, so, F, T, c);
-        if (last) { T.Dn = M[2][2]; break; }
-        entering(k + 2, an);
-        last = factor_step<3, FAST>(k + 2, M, an, T, c, so);
-        fwd_row<FAST>(k + 2, so, F, T, c);
-        if (last) { T.Dn = M[3][3]; break; }
-        entering(k + 3, an);
-        last = factor_step<0, FAST>(k + 3, M, an, T, c, so);
-        fwd_row<FAST>(k + 3, so, F, T, c);
-        if (last) { T.Dn = M[0][0]; break; }
-        if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+        cp_async_wait<0>();  // no copy outlives the block
+        if (valid) {
+            FacState& f = fst[sys];
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) f.M[p][q] = M[p][q];
+            f.a22raw = T.a22raw;
+        }
+        return;
+    } else {
+        // the rest, with the forward substitution
+        FwdState F;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) F.z[b][0] = F.z[b][1] = F.z[b][2] = mk(0.0);
+        F.w0_1 = F.w1_1 = F.w1_2 = F.w2_1 = F.w2_2 = F.w2_3 = mk(0.0);
+        for (;; k += 4) {
+            boundary(k);
+            if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
+                entering(k, an);
+                factor_step_main<1, FAST>(k, M, an, c, so);
+                fwd_row<FAST>(k, so, F, T, c);
+                entering(k + 1, an);
+                factor_step_main<2, FAST>(k + 1, M, an, c, so);
+                fwd_row<FAST>(k + 1, so, F, T, c);
+                entering(k + 2, an);
+                factor_step_main<3, FAST>(k + 2, M, an, c, so);
+                fwd_row<FAST>(k + 2, so, F, T, c);
+                entering(k + 3, an);
+                factor_step_main<0, FAST>(k + 3, M, an, c, so);
+                fwd_row<FAST>(k + 3, so, F, T, c);
+                if ((k + 3) % FAC_CH == 0) __syncthreads();
+                continue;
+            }
+            bool last;
+            entering(k, an);
+            last = factor_step<1, FAST>(k, M, an, T, c, so);
+            fwd_row<FAST>(k, so, F, T, c);
+            if (last) { T.Dn = M[1][1]; break; }
+            entering(k + 1, an);
+            last = factor_step<2, FAST>(k + 1, M, an, T, c, so);
+            fwd_row<FAST>(k + 1, so, F, T, c);
+            if (last) { T.Dn = M[2][2]; break; }
+            entering(k + 2, an);
+            last = factor_step<3, FAST>(k + 2, M, an, T, c, so);
+            fwd_row<FAST>(k + 2, so, F, T, c);
+            if (last) { T.Dn = M[3][3]; break; }
+            entering(k + 3, an);
+            last = factor_step<0, FAST>(k + 3, M, an, T, c, so);
+            fwd_row<FAST>(k + 3, so, F, T, c);
+            if (last) { T.Dn = M[0][0]; break; }
+            if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+        }
+        cp_async_wait<0>();  // no copy outlives the block
+        if (valid) tail[sys] = T;
     }
-    cp_async_wait<0>();  // no copy outlives the block
-    if (valid) tail[sys] = T;
 }
 
 // Upward substitution of the six basis right-hand sides (dcsbdlv0, m = 3):
@@ -1675,6 +1727,7 @@ class PsvEngine : public Engine {
     DBuf<cd> B0, B1, B2, Prow, Lst, Zst, Xcap, l0scr, l0d, ab, co;
     DBuf<int4> rowasm;
     DBuf<SysTail> tails;
+    DBuf<FacState> fst;
     int jmin_loc = 1, ncap = 0;
     float* afld32(int m) { return reinterpret_cast<float*>(Afld[m].p); }
     double vtop = 0, rtop = 0;
@@ -1877,7 +1930,8 @@ class PsvEngine : public Engine {
     void alloc_batch() {
         size_t n = (size_t)d.nn - d.itmp + 1;
         const size_t ls = (size_t)(d.jsrc - d.itmp + 1);
-        size_t per = (n + 1) * 3 * 16 + (n - ls + 2) * 4 * 16 + (size_t)ncap * NB * 16 + NSLOT * NB * 16;
+        size_t per = (n + 1) * 3 * 16 + (n - ls + 2) * 4 * 16 + (size_t)ncap * NB * 16 + NSLOT * NB * 16 +
+                     sizeof(FacState);
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
         nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(65536, (fr / 3) / per));
@@ -1893,6 +1947,7 @@ class PsvEngine : public Engine {
         Zst.reserve((n - ls + 2) * 4 * nsys);
         Xcap.reserve((size_t)ncap * NB * nsys);
         tails.reserve(nsys);
+        fst.reserve(nsys);
         l0scr.reserve((size_t)F * (d.nn0 + 1) * 2);
         l0d.reserve((size_t)F * (d.nn0 + 1) * 4);
         ab.reserve((size_t)F * 320);
@@ -1963,12 +2018,20 @@ class PsvEngine : public Engine {
                                  (double)ncap * NB * 16.0;
         int id = kid("psv_factor");
         kbegin(id);
-        if (mixed())
-            k_psv_solve<true><<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
-                                                                  tails.p);
-        else
-            k_psv_solve<false><<<(nsys + 127) / 128, 128, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
-                                                                   tails.p);
+        const unsigned fgrid = (unsigned)((nsys + FAC_THREADS - 1) / FAC_THREADS);
+        if (mixed()) {
+            k_psv_solve<true, false><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
+                                                                   tails.p, fst.p);
+            DSM_LAUNCH(*this);
+            k_psv_solve<true, true><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
+                                                                  tails.p, fst.p);
+        } else {
+            k_psv_solve<false, false><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
+                                                                    tails.p, fst.p);
+            DSM_LAUNCH(*this);
+            k_psv_solve<false, true><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
+                                                                   tails.p, fst.p);
+        }
         kend(id, fac_bytes * nsys, 0.0);
         DSM_LAUNCH(*this);
         id = kid("psv_substitution");
