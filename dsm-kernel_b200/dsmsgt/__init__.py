@@ -158,6 +158,8 @@ def lib() -> C.CDLL:
                                          C.POINTER(C.c_void_p), C.POINTER(C.POINTER(ShSetup))]
         L.dsm_psv_setup_build.argtypes = [C.POINTER(Params), C.c_char_p, C.c_char_p,
                                           C.POINTER(C.c_void_p), C.POINTER(C.POINTER(PsvSetup))]
+        L.dsm_psv_setup_build_device.argtypes = [C.POINTER(Params), C.c_char_p, C.c_char_p, C.c_int,
+                                                 C.POINTER(C.c_void_p), C.POINTER(C.POINTER(PsvSetup))]
         L.dsm_bundle_free.argtypes = [C.c_void_p]
         L.dsm_bundle_info.argtypes = [C.c_void_p, _ip, _ip]
         L.dsm_host_last_error.restype = C.c_char_p
@@ -286,7 +288,9 @@ class Job:
 class Setup:
     """Driver-side set-up (grid and element integrals) built by the library."""
 
-    def __init__(self, job: Job, mode: str):
+    def __init__(self, job: Job, mode: str, device: int | None = None):
+        """device: build the P-SV element integrals on that CUDA device
+        (dsm_psv_setup_build_device) instead of the host."""
         L = lib()
         self.mode = mode
         self.job = job
@@ -303,9 +307,14 @@ class Setup:
             self.num = SH_NUM
         elif mode == "psv":
             self.ptr = C.POINTER(PsvSetup)()
-            rc = L.dsm_psv_setup_build(C.byref(self.params), job.conf_text.encode(),
-                                       job.model_text.encode(), C.byref(self._bundle),
-                                       C.byref(self.ptr))
+            if device is None:
+                rc = L.dsm_psv_setup_build(C.byref(self.params), job.conf_text.encode(),
+                                           job.model_text.encode(), C.byref(self._bundle),
+                                           C.byref(self.ptr))
+            else:
+                rc = L.dsm_psv_setup_build_device(C.byref(self.params), job.conf_text.encode(),
+                                                  job.model_text.encode(), device, C.byref(self._bundle),
+                                                  C.byref(self.ptr))
             self.num = PSV_NUM
         else:
             raise ValueError(mode)

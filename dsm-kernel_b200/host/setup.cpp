@@ -798,9 +798,17 @@ void mtrnp2(int nlayer, int p, int q, HM hm1, HM hm2) {
 // src/SGTpsv/SGTpsv-MPI.f90:98-477 and the l-independent parts of the
 // omega/l loops (calspdr, ksta, nn: :621-629; source indices :557-558,
 // :636-641).
-extern "C" int dsm_psv_setup_build(const dsm_params_t *par, const char *conf_text,
-                                   const char *model_text, dsm_bundle_t **bundle_out,
-                                   const dsm_psv_setup_t **setup_out) {
+// element integrals on the device (csrc/setup_dev.cu)
+extern "C" int dsm_psv_integrals_device(int device, int nzone, const int *iphase, const int *nlayer, const int *isp,
+                                        const int *elem, const int *hmoff, const double *ra, int nnode, double rmax,
+                                        const double *rho, const double *vpv, const double *vph, const double *vsv,
+                                        const double *vsh, const double *eta, int n_sel, int n_fel, int n_hm,
+                                        double *solid_el, double *fluid_el, double *hm_el, char *err, int errlen);
+
+namespace {
+// device < 0: element integrals on the host; otherwise on that CUDA device
+int psv_setup_build(const dsm_params_t *par, const char *conf_text, const char *model_text, int device,
+                    dsm_bundle_t **bundle_out, const dsm_psv_setup_t **setup_out) {
     try {
         if (!par || !bundle_out || !setup_out) throw std::runtime_error("null argument");
         Conf conf = parse_conf(conf_text);
@@ -1012,12 +1020,13 @@ extern "C" int dsm_psv_setup_build(const dsm_params_t *par, const char *conf_tex
         }
         // element integrals (src/SGTpsv/SGTpsv-MPI.f90:385-477)
         int n_sel = 8 * nslay, n_fel = 8 * (nllay > 0 ? nllay : 1), n_hm = 2 * (nslay + nzone);
-        std::vector<V1> S(31, V1(n_sel));  // every solid array of the reference
+        const bool on_host = device < 0;
+        std::vector<V1> S(on_host ? 31 : 0, V1(n_sel));  // every solid array of the reference
         enum { T, H1X, H1Y, H1Z, H2L, H2N, H3AX, H3AY, H3AZ, H4AL, H4AN, H5AX, H5AY, H5AZ, H6AL,
                H6AN, H3X, H3Y, H3Z, H4L, H4N, H5X, H5Y, H5Z, H6L, H6N, H7X, H7Y, H7Z, H8L, H8N };
-        V1 p1(n_fel), p2(n_fel), p3(n_fel);
-        V1 work(n_sel > n_fel ? n_sel : n_fel);
-        std::vector<std::vector<double>> hmst(14, std::vector<double>(4 * n_hm, 0.0));
+        V1 p1(on_host ? n_fel : 0), p2(on_host ? n_fel : 0), p3(on_host ? n_fel : 0);
+        V1 work(on_host ? (n_sel > n_fel ? n_sel : n_fel) : 0);
+        std::vector<std::vector<double>> hmst(on_host ? 14 : 0, std::vector<double>(4 * n_hm, 0.0));
         enum { M3X, M3Y, M3Z, M5X, M5Y, M5Z, M41L, M41N, M42L, M42N, M61L, M61N, M62L, M62N };
         const int hmlo[14] = {-2, -2, -2, -1, -1, -1, -1, -1, -2, -2, -1, -1, -2, -2};
         auto hmv = [&](int a, int col) {
@@ -1025,7 +1034,7 @@ extern "C" int dsm_psv_setup_build(const dsm_params_t *par, const char *conf_tex
         };
         const double *pv = vra.v.data();
         auto rz_of = [&](int iz) { return ra.p(isp(iz)) - 1; };
-        {
+        if (on_host) {
             int isl = 0, ill = 0;
             for (int i = 1; i <= ndc + 1; ++i) {
                 const double *rz = rz_of(i);
@@ -1164,6 +1173,7 @@ extern "C" int dsm_psv_setup_build(const dsm_params_t *par, const char *conf_tex
         s.rmin = rmin; s.rmax = rmax;
         s.n_sel = n_sel; s.n_fel = n_fel; s.n_hm = n_hm;
         {
+          if (on_host) {
             const int order[DSM_PSV_NSOLID] = {T,    H1X,  H2L,  H2N, H3AY, H4AL, H4AN,
                                                H5AY, H6AL, H6AN, H7Y, H7Z,  H8L,  H8N,
                                                H3Y,  H4L,  H4N,  H5Y, H6L,  H6N};
@@ -1183,6 +1193,29 @@ extern "C" int dsm_psv_setup_build(const dsm_params_t *par, const char *conf_tex
             for (int k = 0; k < DSM_PSV_NHM; ++k)
                 for (int e = 0; e < 4 * n_hm; ++e) hm[(size_t)k * 4 * n_hm + e] = hmst[horder[k]][e];
             s.hm_el = b->keep(hm);
+          } else {
+            std::vector<double> el((size_t)DSM_PSV_NSOLID * n_sel), fl((size_t)3 * n_fel),
+                hm((size_t)DSM_PSV_NHM * 4 * n_hm);
+            std::vector<double> cf[6];
+            const std::vector<V1> *src[6] = {&md.rho, &md.vpv, &md.vph, &md.vsv, &md.vsh, &md.eta};
+            for (int k = 0; k < 6; ++k) {
+                cf[k].resize(4 * (size_t)nzone);
+                for (int i = 1; i <= nzone; ++i)
+                    for (int j = 1; j <= 4; ++j) cf[k][4 * (i - 1) + (j - 1)] = (*src[k])[j](i);
+            }
+            char err[256] = {0};
+            const int rc = dsm_psv_integrals_device(
+                device, nzone, s.iphase, s.nlayer, s.isp, s.elem, s.hmoff, ra.v.data() + 1, nnlayer + 1, rmax,
+                cf[0].data(), cf[1].data(), cf[2].data(), cf[3].data(), cf[4].data(), cf[5].data(), n_sel, n_fel,
+                n_hm, el.data(), fl.data(), hm.data(), err, (int)sizeof(err));
+            if (rc != DSM_OK) {
+                delete b;
+                throw std::runtime_error(std::string("element integrals on the device: ") + err);
+            }
+            s.solid_el = b->keep(el);
+            s.fluid_el = b->keep(fl);
+            s.hm_el = b->keep(hm);
+          }
         }
         s.spn = spn; s.spo = spo; s.r0 = r0;
         s.ecC0 = ecC0; s.ecF0 = ecF0; s.ecL0 = ecL0;
@@ -1216,4 +1249,20 @@ extern "C" int dsm_psv_setup_build(const dsm_params_t *par, const char *conf_tex
         g_err = std::string("dsm_psv_setup_build: ") + e.what();
         return DSM_ERR_INVALID;
     }
+}
+}  // namespace
+
+extern "C" int dsm_psv_setup_build(const dsm_params_t *par, const char *conf_text, const char *model_text,
+                                   dsm_bundle_t **bundle_out, const dsm_psv_setup_t **setup_out) {
+    return psv_setup_build(par, conf_text, model_text, -1, bundle_out, setup_out);
+}
+
+extern "C" int dsm_psv_setup_build_device(const dsm_params_t *par, const char *conf_text, const char *model_text,
+                                          int device, dsm_bundle_t **bundle_out,
+                                          const dsm_psv_setup_t **setup_out) {
+    if (device < 0) {
+        g_err = "dsm_psv_setup_build_device: negative device ordinal";
+        return DSM_ERR_INVALID;
+    }
+    return psv_setup_build(par, conf_text, model_text, device, bundle_out, setup_out);
 }

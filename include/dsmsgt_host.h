@@ -46,6 +46,15 @@ int dsm_psv_setup_build(const dsm_params_t *par, const char *conf_text,
                         const char *model_text, dsm_bundle_t **bundle,
                         const dsm_psv_setup_t **setup);
 
+/* PSV with the element integrals (src/SGTpsv/SGTpsv-MPI.f90:383-477:
+ * calmatc, pinteg, caltl, calhl, calt, calh5, submat, mtrnp, calhm1,
+ * calhm2, mtrnp2) computed on CUDA device `device`, one thread per layer /
+ * node column; the rest of the set-up as dsm_psv_setup_build, and the same
+ * arrays bit for bit.  For requests that set up many models. */
+int dsm_psv_setup_build_device(const dsm_params_t *par, const char *conf_text,
+                               const char *model_text, int device, dsm_bundle_t **bundle,
+                               const dsm_psv_setup_t **setup);
+
 /* Number of radial nodes / unknowns of a bundle, for reports. */
 int dsm_bundle_info(const dsm_bundle_t *bundle, int *n_nodes, int *n_unknowns);
 
