@@ -419,7 +419,8 @@ struct FactorCtx {
     int it, n, ls, lmin, nsys, sys;
     bool store;  // false for threads that only repeat another system
     cd* Lst;
-    cd* Zst;
+    cd* Dst;     // pivots D(k) of rows k >= dmin, for the forward substitution
+    int dmin;
 };
 
 // what a step hands to the forward substitution: the pivot D(k) and the
@@ -528,75 +529,24 @@ __device__ __forceinline__ void factor_step_main(int k, cd (&M)[4][4], const cd 
     M[S0][S0] = anew[3];
 }
 
-// Forward substitution of the four source bases (dcsbdlv0, m = 3), run by
-// the factorisation itself: at step k it has D(k) and, from the three steps
-// before, L(k,k-3), L(k,k-2), L(k,k-1).  Below the first source row every
-// z is zero, so the rows start there.  zh = z / D goes to Zst.
-struct FwdState {
-    cd z[4][3];                          // z(k-3), z(k-2), z(k-1) per basis
-    cd w0_1, w1_1, w1_2, w2_1, w2_2, w2_3;  // w<p>_<d>: multiplier p of step k-d
-};
-template <bool FAST>
-__device__ __forceinline__ void fwd_row(int k, const StepOut& so, FwdState& F, const SysTail& T,
-                                        const FactorCtx& c) {
-    if (k >= c.ls) {
-        const cd l3 = F.w2_3, l2 = F.w1_2, l1 = F.w0_1;  // L(k,k-3), L(k,k-2), L(k,k-1)
-        cd rcp = mk(0.0);
-        if (FAST) rcp = crecipT<true>(so.D);
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const cd rhs = mk(c.ls + b == k ? 1.0 : 0.0);
-            const cd z0 = F.z[b][0], z1 = F.z[b][1], z2 = F.z[b][2];
-            cd zc;
-            if (k == 1) {
-                zc = rhs;
-            } else if (k == 2) {
-                zc = rhs - T.a22raw * z2;
-            } else if (FAST) {
-                cd sum = cmulT<true>(l3, z0);
-                sum = caddmulT<true>(sum, l2, z1);
-                sum = caddmulT<true>(sum, l1, z2);
-                zc = rhs - sum;
-            } else if (k == 3) {  // a(2,3) z(1) + a(3,3) z(2)
-                cd sum = mk(0.0) + l2 * z1 + l1 * z2;
-                zc = rhs - sum;
-            } else {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
-                cd sum = mk(0.0) + l3 * z0 + l2 * z1 + l1 * z2;
-                zc = rhs - sum;
-            }
-            if (c.store) c.Zst[((size_t)(k - c.ls) * 4 + b) * c.nsys + c.sys] = FAST ? cmulT<true>(zc, rcp) : zc / so.D;
-            F.z[b][0] = z1;
-            F.z[b][1] = z2;
-            F.z[b][2] = zc;
-        }
-    }
-    F.w2_3 = F.w2_2;
-    F.w2_2 = F.w2_1;
-    F.w2_1 = so.w2;
-    F.w1_2 = F.w1_1;
-    F.w1_1 = so.w1;
-    F.w0_1 = so.w0;
-}
-
-// One thread per (omega, l) system: band assembly row by row, the unpivoted
-// complex-symmetric LDL^T (dcsymbdl0) streamed through the ring window and,
-// from the first source row up, the forward substitution of the source
-// bases.  Multipliers of the rows the upward substitution needs go to Lst,
-// zh of the source bases to Zst, the last pivots to tail.  The row pieces
-// stream through shared memory: a block (128 consecutive systems:
-// consecutive orders of at most a few frequencies) copies FAC_CH rows of
-// each of its frequencies with cp.async one chunk ahead, so the recurrence
-// waits on shared-memory latency only.  Systems of frequencies beyond the
-// first FAC_NW of a block read their rows from global memory.  All threads
-// of a block take the same steps (the same n), so the block-wide barriers at
-// chunk boundaries are uniform; threads past nsys repeat the last system's
-// work without storing it.
-// The factorisation runs as two launches.  LOWER takes the steps below the
-// source rows, where the forward substitution has nothing to do (most of
-// the band), without its state, so its registers stay low and more warps
-// hide the recurrence's latency; it leaves each system's 4x4 window in
-// FacState.  UPPER resumes from that window and runs the rest with the
-// forward substitution.  Both take the same operations as one pass would.
+// One thread per (omega, l) system: band assembly row by row and the
+// unpivoted complex-symmetric LDL^T (dcsymbdl0) streamed through the ring
+// window.  Multipliers of the rows the substitutions read go to Lst, the
+// pivots of the rows the source bases' forward substitution reads (k >=
+// dmin) to Dst, the last pivots to tail.  The row pieces stream through
+// shared memory: a block (128 consecutive systems: consecutive orders of at
+// most a few frequencies) copies FAC_CH rows of each of its frequencies
+// with cp.async one chunk ahead, so the recurrence waits on shared-memory
+// latency only.  Systems of frequencies beyond the first FAC_NW of a block
+// read their rows from global memory.  All threads of a block take the same
+// steps (the same n), so the block-wide barriers at chunk boundaries are
+// uniform; threads past nsys repeat the last system's work without storing
+// it.  The forward substitution of the source bases runs afterwards
+// (k_psv_fwd) from the stored multipliers and pivots, so this kernel keeps
+// only the 4x4 window and the entering row in registers (two thirds of the
+// registers of a pass that carries the substitution too: more resident
+// warps to hide the recurrence's latency), and one factorisation can serve
+// several sources.
 constexpr int FAC_THREADS = 128;
 #ifndef DSM_FAC_CH
 #define DSM_FAC_CH 16
@@ -605,26 +555,11 @@ constexpr int FAC_CH = DSM_FAC_CH;  // rows per chunk (multiple of 4)
 static_assert(FAC_CH % 4 == 0, "chunks hold whole groups of four steps");
 constexpr int FAC_NW = 4;   // frequencies staged per block
 
-// window of a system between the two factorisation launches
-struct FacState {
-    cd M[4][4];
-    cd a22raw;
-};
-// first step of the upper launch: the first group of four steps that
-// reaches row ls - 4 (the forward substitution reads the three multipliers
-// before row ls) or the last four rows of the band
-__host__ __device__ __forceinline__ int fac_split(int n, int ls) {
-    const int kf = ls - 3;
-    int k = 1;
-    while (k + 3 < kf && k + 3 <= n - 4) k += 4;
-    return k;
-}
-
-template <bool FAST, bool UPPER>
-__global__ void __launch_bounds__(FAC_THREADS, UPPER ? 1 : 4) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
-                                                           int nsys, int lmin, cd* __restrict__ Lst,
-                                                           cd* __restrict__ Zst, SysTail* __restrict__ tail,
-                                                           FacState* __restrict__ fst) {
+template <bool FAST>
+__global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
+                                                              int nsys, int lmin, cd* __restrict__ Lst,
+                                                              SysTail* __restrict__ tail, cd* __restrict__ Dst,
+                                                              int dmin) {
     __shared__ __align__(16) cd sP[2][FAC_NW][FAC_CH][12];
     const int sys0 = blockIdx.x * FAC_THREADS;
     const int sysv = sys0 + threadIdx.x;
@@ -650,9 +585,9 @@ __global__ void __launch_bounds__(FAC_THREADS, UPPER ? 1 : 4) k_psv_solve(PsvDev
     c.sys = sys;
     c.store = valid;
     c.Lst = Lst;
-    c.Zst = Zst;
+    c.Dst = Dst;
+    c.dmin = dmin;
     const int n = c.n;
-    const int ksplit = fac_split(n, c.ls);
     // local rows 5 .. n in chunks: chunk q = rows 5 + q CH .. (global it + r - 1)
     auto stage = [&](int q, int buf) {
         const int r0 = 5 + q * FAC_CH;
@@ -664,51 +599,32 @@ __global__ void __launch_bounds__(FAC_THREADS, UPPER ? 1 : 4) k_psv_solve(PsvDev
             cp_async16(&sP[buf][wi][i][v], Prow + ((size_t)(w0 + wi) * (d.nn + 1) + c.it + r0 + i - 1) * 12 + v);
         }
     };
+    stage(0, 0);
+    cp_async_commit();
     cd M[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) M[p][q] = mk(0.0);
     cd a[4];
     RowPieces rp;
+    // local rows 1..4 go to slots 1, 2, 3, 0
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        if (p >= n) break;
+        load_row(c.P + (size_t)(c.it + p) * 12, rp);
+        assemble_row<FAST>(rp, c.l2, c.lsq, a);
+#pragma unroll
+        for (int q = 0; q <= p; ++q) M[(1 + p) & 3][(1 + q) & 3] = a[4 - (p - q) - 1];
+    }
     SysTail T;
+    // dcsbdlv0 reads a(m-1,2) = a(2,2) of the unfactored band at row 2: it
+    // goes to tail now, so nothing of it stays live through the band
+    load_row(c.P + (size_t)(c.it + 1) * 12, rp);
+    assemble_row<FAST>(rp, c.l2, c.lsq, a);
+    if (valid) tail[sys].a22raw = a[1];
     T.Dm1 = mk(1.0);
     T.Lnn1 = mk(0.0);
-    int k = 1;
-    if (!UPPER) {
-        stage(0, 0);
-        cp_async_commit();
-#pragma unroll
-        for (int p = 0; p < 4; ++p)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) M[p][q] = mk(0.0);
-        // local rows 1..4 go to slots 1, 2, 3, 0
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            if (p >= n) break;
-            load_row(c.P + (size_t)(c.it + p) * 12, rp);
-            assemble_row<FAST>(rp, c.l2, c.lsq, a);
-#pragma unroll
-            for (int q = 0; q <= p; ++q) M[(1 + p) & 3][(1 + q) & 3] = a[4 - (p - q) - 1];
-        }
-        // dcsbdlv0 reads a(m-1,2) = a(2,2) of the unfactored band at row 2
-        load_row(c.P + (size_t)(c.it + 1) * 12, rp);
-        assemble_row<FAST>(rp, c.l2, c.lsq, a);
-        T.a22raw = a[1];
-    } else {
-        const FacState& f = fst[sys];
-#pragma unroll
-        for (int p = 0; p < 4; ++p)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) M[p][q] = f.M[p][q];
-        T.a22raw = f.a22raw;
-        k = ksplit;
-        // the chunk holding the row that enters at step ksplit, and, unless
-        // a chunk starts there (its boundary stages the next one), the next
-        // chunk: the single pass would have it in flight already
-        const int q0 = (k - 1) / FAC_CH;
-        stage(q0, q0 & 1);
-        if ((k - 1) % FAC_CH != 0) stage(q0 + 1, (q0 + 1) & 1);
-        cp_async_commit();
-        cp_async_wait<0>();
-        __syncthreads();
-    }
     // row entering at step k: local row k+4, chunk (k-1)/CH, index (k-1)%CH
     auto entering = [&](int k, cd (&an)[4]) {
         if (k + 4 > n) return;
@@ -732,77 +648,105 @@ __global__ void __launch_bounds__(FAC_THREADS, UPPER ? 1 : 4) k_psv_solve(PsvDev
         }
     };
     cd an[4];
-    StepOut so;
-    if (!UPPER) {
-        // steps whose multipliers the forward substitution never reads: four
-        // main steps at a time, up to the group that reaches row ls - 4
-        for (; k < ksplit; k += 4) {
-            boundary(k);
+    StepOut so{};
+    auto keepD = [&](int k) {
+        if (c.store && k >= c.dmin) c.Dst[(size_t)(k - c.dmin) * c.nsys + c.sys] = so.D;
+    };
+    for (int k = 1;; k += 4) {
+        boundary(k);
+        if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
             entering(k, an);
             factor_step_main<1, FAST>(k, M, an, c, so);
+            keepD(k);
             entering(k + 1, an);
             factor_step_main<2, FAST>(k + 1, M, an, c, so);
+            keepD(k + 1);
             entering(k + 2, an);
             factor_step_main<3, FAST>(k + 2, M, an, c, so);
+            keepD(k + 2);
             entering(k + 3, an);
             factor_step_main<0, FAST>(k + 3, M, an, c, so);
+            keepD(k + 3);
             if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+            continue;
         }
-        cp_async_wait<0>();  // no copy outlives the block
-        if (valid) {
-            FacState& f = fst[sys];
+        bool last;
+        entering(k, an);
+        last = factor_step<1, FAST>(k, M, an, T, c, so);
+        keepD(k);
+        if (last) { T.Dn = M[1][1]; break; }
+        entering(k + 1, an);
+        last = factor_step<2, FAST>(k + 1, M, an, T, c, so);
+        keepD(k + 1);
+        if (last) { T.Dn = M[2][2]; break; }
+        entering(k + 2, an);
+        last = factor_step<3, FAST>(k + 2, M, an, T, c, so);
+        keepD(k + 2);
+        if (last) { T.Dn = M[3][3]; break; }
+        entering(k + 3, an);
+        last = factor_step<0, FAST>(k + 3, M, an, T, c, so);
+        keepD(k + 3);
+        if (last) { T.Dn = M[0][0]; break; }
+        if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+    }
+    cp_async_wait<0>();  // no copy outlives the block
+    if (valid) {
+        tail[sys].Dn = T.Dn;
+        tail[sys].Dm1 = T.Dm1;
+        tail[sys].Lnn1 = T.Lnn1;
+    }
+}
+
+// Forward substitution of the four source bases (dcsbdlv0, m = 3) of one
+// source from its first row ls up, one thread per system, from the stored
+// multipliers L(k,k-1), L(k,k-2), L(k,k-3) and pivots D(k): below ls every
+// z is zero.  zh = z / D goes to Zst.  The same operations as the
+// reference's forward loop; a factorisation serves any number of sources.
+template <bool FAST>
+__global__ void __launch_bounds__(128) k_psv_fwd(PsvDev d, int nsys, int ls, const cd* __restrict__ Lst,
+                                                 const cd* __restrict__ Dst, int dmin,
+                                                 const SysTail* __restrict__ tail, cd* __restrict__ Zst) {
+    const int sys = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sys >= nsys) return;
+    const int n = d.nn - d.itmp + 1;
+    const cd a22raw = tail[sys].a22raw;
+    auto L = [&](int row, int p) {  // multiplier p of step row (0 for rows before the band)
+        return row >= 1 ? Lst[((size_t)row * 3 + p) * nsys + sys] : mk(0.0);
+    };
+    cd z[4][3];
 #pragma unroll
-            for (int p = 0; p < 4; ++p)
+    for (int b = 0; b < 4; ++b) z[b][0] = z[b][1] = z[b][2] = mk(0.0);
+    for (int k = ls; k <= n; ++k) {
+        const cd D = Dst[(size_t)(k - dmin) * nsys + sys];
+        const cd l3 = L(k - 3, 2), l2 = L(k - 2, 1), l1 = L(k - 1, 0);  // L(k,k-3), L(k,k-2), L(k,k-1)
+        cd rcp = mk(0.0);
+        if (FAST) rcp = crecipT<true>(D);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) f.M[p][q] = M[p][q];
-            f.a22raw = T.a22raw;
-        }
-        return;
-    } else {
-        // the rest, with the forward substitution
-        FwdState F;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) F.z[b][0] = F.z[b][1] = F.z[b][2] = mk(0.0);
-        F.w0_1 = F.w1_1 = F.w1_2 = F.w2_1 = F.w2_2 = F.w2_3 = mk(0.0);
-        for (;; k += 4) {
-            boundary(k);
-            if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
-                entering(k, an);
-                factor_step_main<1, FAST>(k, M, an, c, so);
-                fwd_row<FAST>(k, so, F, T, c);
-                entering(k + 1, an);
-                factor_step_main<2, FAST>(k + 1, M, an, c, so);
-                fwd_row<FAST>(k + 1, so, F, T, c);
-                entering(k + 2, an);
-                factor_step_main<3, FAST>(k + 2, M, an, c, so);
-                fwd_row<FAST>(k + 2, so, F, T, c);
-                entering(k + 3, an);
-                factor_step_main<0, FAST>(k + 3, M, an, c, so);
-                fwd_row<FAST>(k + 3, so, F, T, c);
-                if ((k + 3) % FAC_CH == 0) __syncthreads();
-                continue;
+        for (int b = 0; b < 4; ++b) {
+            const cd rhs = mk(ls + b == k ? 1.0 : 0.0);
+            const cd z0 = z[b][0], z1 = z[b][1], z2 = z[b][2];
+            cd zc;
+            if (k == 1) {
+                zc = rhs;
+            } else if (k == 2) {
+                zc = rhs - a22raw * z2;
+            } else if (FAST) {
+                cd sum = cmulT<true>(l3, z0);
+                sum = caddmulT<true>(sum, l2, z1);
+                sum = caddmulT<true>(sum, l1, z2);
+                zc = rhs - sum;
+            } else if (k == 3) {  // a(2,3) z(1) + a(3,3) z(2)
+                cd sum = mk(0.0) + l2 * z1 + l1 * z2;
+                zc = rhs - sum;
+            } else {  // a(1,j) z(j-3) + a(2,j) z(j-2) + a(3,j) z(j-1)
+                cd sum = mk(0.0) + l3 * z0 + l2 * z1 + l1 * z2;
+                zc = rhs - sum;
             }
-            bool last;
-            entering(k, an);
-            last = factor_step<1, FAST>(k, M, an, T, c, so);
-            fwd_row<FAST>(k, so, F, T, c);
-            if (last) { T.Dn = M[1][1]; break; }
-            entering(k + 1, an);
-            last = factor_step<2, FAST>(k + 1, M, an, T, c, so);
-            fwd_row<FAST>(k + 1, so, F, T, c);
-            if (last) { T.Dn = M[2][2]; break; }
-            entering(k + 2, an);
-            last = factor_step<3, FAST>(k + 2, M, an, T, c, so);
-            fwd_row<FAST>(k + 2, so, F, T, c);
-            if (last) { T.Dn = M[3][3]; break; }
-            entering(k + 3, an);
-            last = factor_step<0, FAST>(k + 3, M, an, T, c, so);
-            fwd_row<FAST>(k + 3, so, F, T, c);
-            if (last) { T.Dn = M[0][0]; break; }
-            if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+            Zst[((size_t)(k - ls) * 4 + b) * nsys + sys] = FAST ? cmulT<true>(zc, rcp) : zc / D;
+            z[b][0] = z1;
+            z[b][1] = z2;
+            z[b][2] = zc;
         }
-        cp_async_wait<0>();  // no copy outlives the block
-        if (valid) tail[sys] = T;
     }
 }
 
@@ -1724,10 +1668,9 @@ class PsvEngine : public Engine {
         capmap, l0col, l0e1;
     DBuf<int2> caplist;
     DBuf<double> qmu, qkappa, sel, fel, hm, bcval, poly, lam, qkp, fr, r, rrsta;
-    DBuf<cd> B0, B1, B2, Prow, Lst, Zst, Xcap, l0scr, l0d, ab, co;
+    DBuf<cd> B0, B1, B2, Prow, Lst, Zst, Dst, Xcap, l0scr, l0d, ab, co;
     DBuf<int4> rowasm;
     DBuf<SysTail> tails;
-    DBuf<FacState> fst;
     int jmin_loc = 1, ncap = 0;
     float* afld32(int m) { return reinterpret_cast<float*>(Afld[m].p); }
     double vtop = 0, rtop = 0;
@@ -1930,8 +1873,7 @@ class PsvEngine : public Engine {
     void alloc_batch() {
         size_t n = (size_t)d.nn - d.itmp + 1;
         const size_t ls = (size_t)(d.jsrc - d.itmp + 1);
-        size_t per = (n + 1) * 3 * 16 + (n - ls + 2) * 4 * 16 + (size_t)ncap * NB * 16 + NSLOT * NB * 16 +
-                     sizeof(FacState);
+        size_t per = (n + 1) * 3 * 16 + (n - ls + 2) * 5 * 16 + (size_t)ncap * NB * 16 + NSLOT * NB * 16;
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
         nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(65536, (fr / 3) / per));
@@ -1945,9 +1887,9 @@ class PsvEngine : public Engine {
         Prow.reserve((size_t)F * (d.nn + 1) * 12);
         Lst.reserve((n + 1) * 3 * nsys);
         Zst.reserve((n - ls + 2) * 4 * nsys);
+        Dst.reserve((n - ls + 2) * nsys);
         Xcap.reserve((size_t)ncap * NB * nsys);
         tails.reserve(nsys);
-        fst.reserve(nsys);
         l0scr.reserve((size_t)F * (d.nn0 + 1) * 2);
         l0d.reserve((size_t)F * (d.nn0 + 1) * 4);
         ab.reserve((size_t)F * 320);
@@ -2019,19 +1961,16 @@ class PsvEngine : public Engine {
         int id = kid("psv_factor");
         kbegin(id);
         const unsigned fgrid = (unsigned)((nsys + FAC_THREADS - 1) / FAC_THREADS);
-        if (mixed()) {
-            k_psv_solve<true, false><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
-                                                                   tails.p, fst.p);
-            DSM_LAUNCH(*this);
-            k_psv_solve<true, true><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
-                                                                  tails.p, fst.p);
-        } else {
-            k_psv_solve<false, false><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
-                                                                    tails.p, fst.p);
-            DSM_LAUNCH(*this);
-            k_psv_solve<false, true><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, Zst.p,
-                                                                   tails.p, fst.p);
-        }
+        const int dmin = ls;  // pivots from the first source row up
+        if (mixed())
+            k_psv_solve<true><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, tails.p, Dst.p, dmin);
+        else
+            k_psv_solve<false><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, tails.p, Dst.p, dmin);
+        DSM_LAUNCH(*this);
+        if (mixed())
+            k_psv_fwd<true><<<fgrid, FAC_THREADS, 0, st>>>(d, nsys, ls, Lst.p, Dst.p, dmin, tails.p, Zst.p);
+        else
+            k_psv_fwd<false><<<fgrid, FAC_THREADS, 0, st>>>(d, nsys, ls, Lst.p, Dst.p, dmin, tails.p, Zst.p);
         kend(id, fac_bytes * nsys, 0.0);
         DSM_LAUNCH(*this);
         id = kid("psv_substitution");
