@@ -111,6 +111,7 @@ class Stats(C.Structure):
                 for i in range(self.nk)}
 
 
+DSM_OK = 0
 DSM_ERR_INVALID = 1
 DSM_ERR_CUDA = 2
 DSM_ERR_NONFINITE = 3
