@@ -75,6 +75,22 @@ Engine::~Engine() {
     if (st) cudaStreamDestroy(st);
 }
 
+double* Engine::out_t_src() const {
+    size_t pt, pr, ps;
+    out_sizes(&pt, &pr, &ps);
+    return out_t.p + 2 * pt * (size_t)F * src;
+}
+double* Engine::out_r_src() const {
+    size_t pt, pr, ps;
+    out_sizes(&pt, &pr, &ps);
+    return out_r.p + 2 * pr * (size_t)F * src;
+}
+double* Engine::out_s_src() const {
+    size_t pt, pr, ps;
+    out_sizes(&pt, &pr, &ps);
+    return out_s.p + 2 * ps * (size_t)F * src;
+}
+
 int Engine::kid(const char* name) {
     for (int i = 0; i < stats.nk; ++i)
         if (std::strncmp(stats.kern[i].name, name, 31) == 0) return i;
@@ -194,7 +210,7 @@ void Engine::lsum_group(int w0, int w1, const std::vector<int>& nord) {
     for (int m = m_lo; m <= 2; ++m) {
         if (!rows_m[m]) continue;
         const size_t rw = (size_t)rows_m[m];
-        const char* A = reinterpret_cast<const char*>(Afld[m].p) + (size_t)w0 * rw * Lcap * afld_bytes;
+        const char* A = reinterpret_cast<const char*>(Afld[m].p) + ((size_t)src * F + w0) * rw * Lcap * afld_bytes;
         tc::split_fields(A, afld_bytes, n, rows_m[m], Lcap, d_nord.p + w0, Apc[m].p + (size_t)w0 * rw * kcA,
                          sA[m].p + (size_t)w0 * rw, kcA, F, tc_fmt, tc_bk, st);
         launches++;
@@ -392,7 +408,7 @@ void Engine::gemm_fp64(int w, int mi, int K) {
     if (M == 0) return;
     if (afld_bytes != 8) throw Error(DSM_ERR_INVALID, "FP64 l-sum of FP32 field matrices");
     const double one = 1.0, zero = 0.0;
-    const double* A = Afld[mi].p + (size_t)w * M * Lcap;
+    const double* A = Afld[mi].p + ((size_t)src * F + w) * M * Lcap;
     int id = kid("lsum_dgemm");
     kbegin(id);
     double bytes = 0.0, flops = 0.0;
@@ -419,7 +435,7 @@ void Engine::grow_orders(int need) {
     cap = std::min(cap, maxlmax + 1 + Lc);
     if (cap < need) cap = need;
     for (int m = m_lo; m <= 2; ++m) {
-        size_t h = (size_t)F * rows_m[m];
+        size_t h = (size_t)nsrc * F * rows_m[m];
         if (h == 0) continue;
         const size_t eb = (size_t)afld_bytes, bytes = (h * cap * eb + 7) / 8 * 8;
         double* np_ = nullptr;
@@ -433,15 +449,15 @@ void Engine::grow_orders(int need) {
         Afld[m].n = bytes / 8;
     }
     double* na = nullptr;
-    if (cudaMalloc(&na, (size_t)F * cap * amp_k * sizeof(double)) != cudaSuccess)
+    if (cudaMalloc(&na, (size_t)nsrc * F * cap * amp_k * sizeof(double)) != cudaSuccess)
         throw Error(DSM_ERR_NOMEM, "cannot grow the probe table");
     DSM_CUDA(cudaMemcpy2DAsync(na, (size_t)cap * amp_k * sizeof(double), amps.p,
                                (size_t)Lcap * amp_k * sizeof(double), (size_t)Lcap * amp_k * sizeof(double),
-                               (size_t)F, cudaMemcpyDeviceToDevice, st));
+                               (size_t)nsrc * F, cudaMemcpyDeviceToDevice, st));
     DSM_CUDA(cudaStreamSynchronize(st));
     amps.release();
     amps.p = na;
-    amps.n = (size_t)F * cap * amp_k;
+    amps.n = (size_t)nsrc * F * cap * amp_k;
     Lcap = cap;
 }
 
@@ -528,13 +544,23 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
         // --- 1+2: per-omega pieces and chunked solves with the cutoff scan
         DSM_CUDA(cudaEventRecord(es0, st));
         omega_pieces(d_freqs.p, nf);
+        // cutoff state of (source s, frequency w) at s F + w
+        const size_t ncut = (size_t)nsrc * F;
         {
-            std::vector<CutState> init(nf);
+            std::vector<CutState> init(ncut);
             for (auto& c : init) { c.ismall = 0; c.done = 0; c.llog = maxlmax; c.norders = 0; c.maxamp = -1.0; }
             cut.upload(init, st);
         }
+        std::vector<CutState> hcs(ncut);
+        for (auto& c : hcs) c.done = 0;
+        // a frequency is done when every source has met its cutoff
         std::vector<CutState> hc(nf);
         for (auto& c : hc) c.done = 0;
+        auto all_sources_done = [&](int w) {
+            for (int s = 0; s < nsrc; ++s)
+                if (!hcs[(size_t)s * F + w].done) return 0;
+            return 1;
+        };
         // Rounds of ragged order ranges: every unfinished frequency continues
         // from where it stopped.  The first range of a frequency reaches past
         // lsuf (the cutoff is never below it); later ranges grow by half.
@@ -584,7 +610,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             scan_chunk(nf, wl);
             stats.systems += tot;
             rounds++;
-            DSM_CUDA(cudaMemcpyAsync(hc.data(), cut.p, sizeof(CutState) * nf, cudaMemcpyDeviceToHost, st));
+            DSM_CUDA(cudaMemcpyAsync(hcs.data(), cut.p, sizeof(CutState) * ncut, cudaMemcpyDeviceToHost, st));
             int hstat = 0;
             DSM_CUDA(cudaMemcpyAsync(&hstat, dstatus(), sizeof(int), cudaMemcpyDeviceToHost, st));
             DSM_CUDA(cudaStreamSynchronize(st));
@@ -593,27 +619,32 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
                 DSM_CUDA(cudaMemsetAsync(dflags.p, 0, 2 * sizeof(int), st));
                 DSM_CUDA(cudaStreamSynchronize(st));
                 int bad = hf[0];
-                for (int w = 0; w < nf; ++w)
-                    if (hc[w].llog < 0) { bad = hf[w]; break; }
+                for (size_t k = 0; k < ncut; ++k)
+                    if ((int)(k % F) < nf && hcs[k].llog < 0) { bad = hf[k % F]; break; }
                 throw Error(DSM_ERR_NONFINITE, "a pivot of the banded solve or the cutoff probe became Inf or NaN "
                                                "(frequency index " + std::to_string(bad) + ")");
             }
             bool all = true;
             for (int w = 0; w < nf; ++w) {
+                hc[w].done = all_sources_done(w);
                 if (!hc[w].done && next[w] > maxlmax) { hc[w].done = 1; }
                 all = all && hc[w].done;
                 if (!hc[w].done && opt.l_chunk <= 0) span[w] = std::min(4096, span[w] + span[w] / 2);
             }
             if (all) break;
         }
-        for (int w = 0; w < nf; ++w) {
-            if (hc[w].norders == 0) { hc[w].norders = maxlmax + 1; hc[w].llog = maxlmax; }
-            stats.orders_padded += (long long)next[w] - hc[w].norders;
-            stats.freqs_extended += hc[w].norders > span0[w] ? 1 : 0;
-        }
+        for (int s = 0; s < nsrc; ++s)
+            for (int w = 0; w < nf; ++w) {
+                CutState& c = hcs[(size_t)s * F + w];
+                if (c.norders == 0) { c.norders = maxlmax + 1; c.llog = maxlmax; }
+                stats.orders_padded += (long long)next[w] - c.norders;
+                stats.freqs_extended += c.norders > span0[w] ? 1 : 0;
+            }
+        // source 0's states stand for the batch where one set is reported
+        for (int w = 0; w < nf; ++w) hc[w] = hcs[w];
         join_side();
         DSM_CUDA(cudaEventRecord(es1, st));
-        if (cutoffs_only) {  // the realised cutoffs are all that was asked for
+        if (cutoffs_only) {  // the realised cutoffs (of source 0) are all that was asked for
             for (int w = 0; w < nf; ++w) {
                 if (llog_out) llog_out[b0 + w] = hc[w].llog;
                 stats.orders_used += hc[w].norders;
@@ -625,9 +656,9 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             ms_solve += a;
             continue;
         }
-        // --- 3+4: contraction and epilogue per frequency
+        // --- 3+4: contraction and epilogue per frequency, source by source
         int lneed = 1;
-        for (auto& c : hc) lneed = std::max(lneed, c.norders);
+        for (auto& c : hcs) lneed = std::max(lneed, c.norders);
         {
             int id = kid("basis_tables");
             kbegin(id);
@@ -635,57 +666,70 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             kend(id, 0.0, 0.0);
         }
         DSM_CUDA(cudaEventRecord(eg0, st));
-        std::vector<int> nord(nf);
-        for (int w = 0; w < nf; ++w) nord[w] = hc[w].norders;
-        if (mixed()) lsum_prepare(nf, nord);
-        // complex64 records for the host leave per group of frequencies on
-        // the copy stream while the next group's l-sum runs
         const bool rec32 = ho && (ho->tsgt32 || ho->rsgt32 || ho->synn32);
-        const int ngrp = !rec32 ? 1 : (nf >= 2 * MAX_OUT_GROUPS ? MAX_OUT_GROUPS : std::max(1, nf / 2));
-        if (rec32) out32.reserve(2 * (pt + pr + ps) * (size_t)nf);
-        for (int g = 0; g < ngrp; ++g) {
-            const int w0 = g * nf / ngrp, w1 = (g + 1) * nf / ngrp;
-            if (mixed()) lsum_group(w0, w1, nord);
-            for (int w = w0; w < w1; ++w) {
-                stats.orders_used += hc[w].norders;
-                if (!mixed())
-                    for (int mi = m_lo; mi <= 2; ++mi) gemm_fp64(w, mi, hc[w].norders);
-                epilogue(d_freqs.p, w, nf);
-                for (int mi = m_lo; mi <= 2; ++mi)
-                    stats.lsum_flops +=
-                        2.0 * (2.0 * full_rows(mi) + (rows_m[mi] - full_rows(mi))) * Th * hc[w].norders;
+        for (src = 0; src < nsrc; ++src) {
+            const CutState* hs = hcs.data() + (size_t)src * F;
+            dsm_out_t* hos = ho ? ho + src : nullptr;
+            std::vector<int> nord(nf);
+            for (int w = 0; w < nf; ++w) nord[w] = hs[w].norders;
+            if (mixed()) lsum_prepare(nf, nord);
+            // complex64 records for the host leave per group of frequencies on
+            // the copy stream while the next group's l-sum runs
+            const int ngrp = !rec32 ? 1 : (nf >= 2 * MAX_OUT_GROUPS ? MAX_OUT_GROUPS : std::max(1, nf / 2));
+            if (rec32) out32.reserve(2 * (pt + pr + ps) * (size_t)nf);
+            if (rec32 && src > 0) {  // this source's records reuse out32: the last source's copies first
+                DSM_CUDA(cudaEventRecord(ev_grp[0], stc));
+                DSM_CUDA(cudaStreamWaitEvent(st, ev_grp[0], 0));
             }
-            if (rec32) {
-                launch_pack32(*this, nf, w0, w1, pt, pr, ps);
-                DSM_CUDA(cudaEventRecord(ev_grp[g], st));
-                DSM_CUDA(cudaStreamWaitEvent(stc, ev_grp[g], 0));
-                const float* o = out32.p;
-                const size_t n = (size_t)(w1 - w0);
-                if (ho->tsgt32)
-                    DSM_CUDA(cudaMemcpyAsync(ho->tsgt32 + 2 * pt * (b0 + w0), o + 2 * pt * w0, 8 * pt * n,
-                                             cudaMemcpyDeviceToHost, stc));
-                if (ho->rsgt32 && rsgt_sw)
-                    DSM_CUDA(cudaMemcpyAsync(ho->rsgt32 + 2 * pr * (b0 + w0), o + 2 * pt * nf + 2 * pr * w0,
-                                             8 * pr * n, cudaMemcpyDeviceToHost, stc));
-                if (ho->synn32 && synn_sw)
-                    DSM_CUDA(cudaMemcpyAsync(ho->synn32 + 2 * ps * (b0 + w0), o + 2 * (pt + pr) * nf + 2 * ps * w0,
-                                             8 * ps * n, cudaMemcpyDeviceToHost, stc));
+            for (int g = 0; g < ngrp; ++g) {
+                const int w0 = g * nf / ngrp, w1 = (g + 1) * nf / ngrp;
+                if (mixed()) lsum_group(w0, w1, nord);
+                for (int w = w0; w < w1; ++w) {
+                    stats.orders_used += hs[w].norders;
+                    if (!mixed())
+                        for (int mi = m_lo; mi <= 2; ++mi) gemm_fp64(w, mi, hs[w].norders);
+                    epilogue(d_freqs.p, w, nf);
+                    for (int mi = m_lo; mi <= 2; ++mi)
+                        stats.lsum_flops +=
+                            2.0 * (2.0 * full_rows(mi) + (rows_m[mi] - full_rows(mi))) * Th * hs[w].norders;
+                }
+                if (rec32) {
+                    launch_pack32(*this, nf, w0, w1, pt, pr, ps);
+                    DSM_CUDA(cudaEventRecord(ev_grp[g], st));
+                    DSM_CUDA(cudaStreamWaitEvent(stc, ev_grp[g], 0));
+                    const float* o = out32.p;
+                    const size_t n = (size_t)(w1 - w0);
+                    if (hos->tsgt32)
+                        DSM_CUDA(cudaMemcpyAsync(hos->tsgt32 + 2 * pt * (b0 + w0), o + 2 * pt * w0, 8 * pt * n,
+                                                 cudaMemcpyDeviceToHost, stc));
+                    if (hos->rsgt32 && rsgt_sw)
+                        DSM_CUDA(cudaMemcpyAsync(hos->rsgt32 + 2 * pr * (b0 + w0), o + 2 * pt * nf + 2 * pr * w0,
+                                                 8 * pr * n, cudaMemcpyDeviceToHost, stc));
+                    if (hos->synn32 && synn_sw)
+                        DSM_CUDA(cudaMemcpyAsync(hos->synn32 + 2 * ps * (b0 + w0),
+                                                 o + 2 * (pt + pr) * nf + 2 * ps * w0, 8 * ps * n,
+                                                 cudaMemcpyDeviceToHost, stc));
+                }
+            }
+            // --- 5: outputs
+            if (llog_out && src == 0)
+                for (int w = 0; w < nf; ++w) llog_out[b0 + w] = hs[w].llog;
+            if (hos) {
+                if (hos->llog)
+                    for (int w = 0; w < nf; ++w) hos->llog[b0 + w] = hs[w].llog;
+                if (hos->tsgt)
+                    DSM_CUDA(cudaMemcpyAsync(hos->tsgt + 2 * pt * b0, out_t_src(), 16 * pt * nf,
+                                             cudaMemcpyDeviceToHost, st));
+                if (hos->rsgt && rsgt_sw)
+                    DSM_CUDA(cudaMemcpyAsync(hos->rsgt + 2 * pr * b0, out_r_src(), 16 * pr * nf,
+                                             cudaMemcpyDeviceToHost, st));
+                if (hos->synn && synn_sw)
+                    DSM_CUDA(cudaMemcpyAsync(hos->synn + 2 * ps * b0, out_s_src(), 16 * ps * nf,
+                                             cudaMemcpyDeviceToHost, st));
             }
         }
+        src = 0;
         DSM_CUDA(cudaEventRecord(eg1, st));
-        // --- 5: outputs
-        if (llog_out)
-            for (int w = 0; w < nf; ++w) llog_out[b0 + w] = hc[w].llog;
-        if (ho) {
-            if (ho->llog)
-                for (int w = 0; w < nf; ++w) ho->llog[b0 + w] = hc[w].llog;
-            if (ho->tsgt)
-                DSM_CUDA(cudaMemcpyAsync(ho->tsgt + 2 * pt * b0, out_t.p, 16 * pt * nf, cudaMemcpyDeviceToHost, st));
-            if (ho->rsgt && rsgt_sw)
-                DSM_CUDA(cudaMemcpyAsync(ho->rsgt + 2 * pr * b0, out_r.p, 16 * pr * nf, cudaMemcpyDeviceToHost, st));
-            if (ho->synn && synn_sw)
-                DSM_CUDA(cudaMemcpyAsync(ho->synn + 2 * ps * b0, out_s.p, 16 * ps * nf, cudaMemcpyDeviceToHost, st));
-        }
         // the next batch overwrites out32 and the outputs: its records wait
         // for this batch's copies
         if (rec32) {
@@ -695,7 +739,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
         DSM_CUDA(cudaStreamSynchronize(st));
         check_device_flags();
         kcollect();
-        check_batch(ilist, b0, nf, hc);
+        if (nsrc == 1) check_batch(ilist, b0, nf, hc);
         float a = 0, g = 0;
         cudaEventElapsedTime(&a, es0, es1);
         cudaEventElapsedTime(&g, eg0, eg1);
@@ -816,7 +860,28 @@ extern "C" int dsm_psv_create(const dsm_psv_setup_t* s, const dsm_options_t* o, 
         DSM_CUDA(cudaSetDevice(opt.device));
         auto* c = new dsm_ctx;
         try {
-            c->eng.reset(dsm::make_psv_engine(s, &opt));
+            c->eng.reset(dsm::make_psv_engine(&s, 1, &opt));
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+extern "C" int dsm_psv_create_multi(const dsm_psv_setup_t* const* setups, int nsrc, const dsm_options_t* o,
+                                    dsm_ctx_t** out) {
+    if (!setups || nsrc < 1 || !out) { g_create_err = "null argument or no source"; return DSM_ERR_INVALID; }
+    *out = nullptr;
+    dsm_options_t opt{};
+    if (o) opt = *o;
+    int rc = check_device(opt.device);
+    if (rc) return rc;
+    return guarded(nullptr, [&] {
+        DSM_CUDA(cudaSetDevice(opt.device));
+        auto* c = new dsm_ctx;
+        try {
+            c->eng.reset(dsm::make_psv_engine(setups, nsrc, &opt));
         } catch (...) {
             delete c;
             throw;
@@ -827,9 +892,25 @@ extern "C" int dsm_psv_create(const dsm_psv_setup_t* s, const dsm_options_t* o, 
 
 extern "C" int dsm_run_freqs(dsm_ctx_t* ctx, const int* ilist, int n, dsm_out_t* out) {
     if (!ctx || !ilist || !out) return DSM_ERR_INVALID;
+    if (ctx->eng->nsrc != 1) {
+        ctx->err = "a context with several sources takes dsm_run_freqs_multi";
+        return DSM_ERR_INVALID;
+    }
     return guarded(ctx, [&] {
         DSM_CUDA(cudaSetDevice(ctx->eng->opt.device));
         ctx->eng->run(ilist, n, out, nullptr, nullptr, nullptr, nullptr);
+    });
+}
+
+extern "C" int dsm_run_freqs_multi(dsm_ctx_t* ctx, const int* ilist, int n, dsm_out_t* outs, int nout) {
+    if (!ctx || !ilist || !outs) return DSM_ERR_INVALID;
+    if (nout != ctx->eng->nsrc) {
+        ctx->err = "dsm_run_freqs_multi needs one output set per source of the context";
+        return DSM_ERR_INVALID;
+    }
+    return guarded(ctx, [&] {
+        DSM_CUDA(cudaSetDevice(ctx->eng->opt.device));
+        ctx->eng->run(ilist, n, outs, nullptr, nullptr, nullptr, nullptr);
     });
 }
 
@@ -963,6 +1044,8 @@ extern "C" int dsm_set_fp64_check(dsm_ctx_t* ctx, dsm_ctx_t* ref, int stride) {
             return;
         }
         const dsm::Engine& r = *ref->eng;
+        if (e.nsrc != 1 || r.nsrc != 1)
+            throw Error(DSM_ERR_INVALID, "the FP64 check covers single-source contexts");
         if (ref == ctx || r.opt.precision != DSM_PREC_FP64)
             throw Error(DSM_ERR_INVALID, "the check context must be another context in DSM_PREC_FP64");
         if (r.mode != e.mode || r.R != e.R || r.Th != e.Th || r.opt.device != e.opt.device ||

@@ -82,6 +82,11 @@ class Engine {
 
     // batch work buffers
     int F = 0, Lc = 0, Lcap = 0;     // frequencies per batch, l chunk, A capacity
+    // Several source depths can share one banded factorisation per (omega,
+    // l) (P-SV): the per-frequency buffers below (field matrices, cutoff
+    // probes and states, outputs) hold nsrc slots of F frequencies, and src
+    // selects the slot the mode hooks and the l-sum work on.
+    int nsrc = 1, src = 0;
     int amp_k = 1;                   // cutoff probes stored per order
     DBuf<double> Afld[3];            // field matrices per |m| [F][rows][Lcap]
     int afld_bytes = 8;              // their element: FP64, or FP32 where the mode's mixed path stores them so
@@ -92,6 +97,14 @@ class Engine {
     DBuf<float> out32;                 // complex64 catalogue packing
     DBuf<int> d_freqs;
     std::vector<int> h_norders;
+
+    // source src's slot of the per-frequency buffers
+    size_t fld_off(int m) const { return (size_t)src * F * rows_m[m] * Lcap; }  // elements of Afld[m]
+    CutState* cut_src() const { return cut.p + (size_t)src * F; }
+    double* amps_src() const { return amps.p + (size_t)src * F * Lcap * amp_k; }
+    double* out_t_src() const;
+    double* out_r_src() const;
+    double* out_s_src() const;
 
     // rows of the field matrix per |m| (set by the mode)
     int rows_m[3] = {0, 0, 0};
@@ -190,13 +203,13 @@ class Engine {
     void check_batch(const int* ilist, int b0, int nf, const std::vector<CutState>& hc);
     void finish_accuracy();
 
-    // drivers
+    // drivers; host_out holds nsrc output sets (or is null)
     void run(const int* ilist, int n, dsm_out_t* host_out, const void** dt, const void** dr,
              const void** ds, int* llog);
 };
 
 Engine* make_sh_engine(const dsm_sh_setup_t* s, const dsm_options_t* o);
-Engine* make_psv_engine(const dsm_psv_setup_t* s, const dsm_options_t* o);
+Engine* make_psv_engine(const dsm_psv_setup_t* const* s, int nsrc, const dsm_options_t* o);
 
 // shared kernels (tables.cu)
 void launch_basis_tables(Engine& e, int lcap);

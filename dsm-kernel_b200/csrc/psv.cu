@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cmath>
+#include <cstring>
 #include <type_traits>
 
 #include "engine.cuh"
@@ -1672,10 +1673,24 @@ class PsvEngine : public Engine {
     DBuf<int4> rowasm;
     DBuf<SysTail> tails;
     int jmin_loc = 1, ncap = 0;
-    float* afld32(int m) { return reinterpret_cast<float*>(Afld[m].p); }
+    // one parameter set per source depth (the source fields differ), and
+    // the source polynomials they point to
+    std::vector<PsvDev> dsrc;
+    DBuf<double> polys;
+    int ls_min = 1;  // local first source row of the deepest source
+    // source s's slot of the field matrices (element type T)
+    template <class T>
+    T* afld_of(int m, int s) {
+        return reinterpret_cast<T*>(reinterpret_cast<char*>(Afld[m].p) +
+                                    (size_t)s * F * rows_m[m] * Lcap * afld_bytes);
+    }
     double vtop = 0, rtop = 0;
 
-    PsvEngine(const dsm_psv_setup_t* s, const dsm_options_t* o) {
+    PsvEngine(const dsm_psv_setup_t* const* ss, int ns, const dsm_options_t* o) {
+        if (!ss || ns < 1 || !ss[0]) throw Error(DSM_ERR_INVALID, "no PSV set-up");
+        const dsm_psv_setup_t* s = ss[0];
+        for (int k = 1; k < ns; ++k) check_same_grid(s, ss[k]);
+        nsrc = ns;
         mode = 1;
         opt = *o;
         init_common(opt.device);
@@ -1855,6 +1870,28 @@ class PsvEngine : public Engine {
         d.rowasm = rowasm.p;
         d.rcap = rcap.p; d.wv = wv.p; d.wd = wd.p; d.fluid = fluid.p; d.lam = lam.p; d.qkp = qkp.p;
         d.fr = fr.p; d.comp_src = comp_src.p; d.jsta = jsta.p;
+        // per-source parameter sets: the fields set by the source position
+        {
+            std::vector<double> pl(24 * (size_t)nsrc);
+            for (int k = 0; k < nsrc; ++k)
+                for (int i = 0; i < 24; ++i) pl[24 * (size_t)k + i] = ss[k]->src_poly[i];
+            polys.upload(pl, st);
+            dsrc.assign(nsrc, d);
+            ls_min = d.nn;
+            for (int k = 0; k < nsrc; ++k) {
+                const dsm_psv_setup_t* q = ss[k];
+                PsvDev& e = dsrc[k];
+                e.jsrc = q->jsrc;
+                e.spn = q->spn;
+                if (e.jsrc < e.itmp || e.jsrc + 3 > nn) throw Error(DSM_ERR_INVALID, "source rows outside the system");
+                e.r0 = q->r0;
+                e.ecC0 = q->ecC0; e.ecF0 = q->ecF0; e.ecL0 = q->ecL0;
+                e.ra0 = q->ra_src[0]; e.ra1 = q->ra_src[1];
+                e.poly = polys.p + 24 * (size_t)k;
+                ls_min = std::min(ls_min, e.jsrc - e.itmp + 1);
+            }
+            d = dsrc[0];
+        }
         F = opt.freq_batch > 0 ? opt.freq_batch : 8;
         Lc = opt.l_chunk > 0 ? ((opt.l_chunk + 31) / 32) * 32 : 256;
         Lcap = std::min(maxlmax + 1 + Lc, 2048);
@@ -1870,9 +1907,37 @@ class PsvEngine : public Engine {
         DSM_CUDA(cudaStreamSynchronize(st));
     }
 
+    // every source of a context shares the model, grid, receivers and
+    // distances; only the source fields may differ
+    static void check_same_grid(const dsm_psv_setup_t* a, const dsm_psv_setup_t* b) {
+        if (!b) throw Error(DSM_ERR_INVALID, "null PSV set-up");
+        auto same = [](const void* x, const void* y, size_t bytes) {
+            return bytes == 0 || (x && y && std::memcmp(x, y, bytes) == 0);
+        };
+        const bool ok =
+            a->nzone == b->nzone && a->nn == b->nn && a->r_n == b->r_n && a->theta_n == b->theta_n &&
+            a->n_sel == b->n_sel && a->n_fel == b->n_fel && a->n_hm == b->n_hm && a->rmin == b->rmin &&
+            a->rmax == b->rmax && a->tlen == b->tlen && a->omegai == b->omegai && a->ratl == b->ratl &&
+            a->maxlmax == b->maxlmax && a->rsgt_switch == b->rsgt_switch && a->synn_switch == b->synn_switch &&
+            same(a->iphase, b->iphase, sizeof(int) * a->nzone) && same(a->nlayer, b->nlayer, sizeof(int) * a->nzone) &&
+            same(a->kkdr, b->kkdr, sizeof(int) * a->nzone) && same(a->elem, b->elem, sizeof(int) * a->nzone) &&
+            same(a->hmoff, b->hmoff, sizeof(int) * a->nzone) && same(a->qmu, b->qmu, sizeof(double) * a->nzone) &&
+            same(a->qkappa, b->qkappa, sizeof(double) * a->nzone) &&
+            same(a->solid_el, b->solid_el, sizeof(double) * DSM_PSV_NSOLID * a->n_sel) &&
+            same(a->fluid_el, b->fluid_el, sizeof(double) * 3 * a->n_fel) &&
+            same(a->hm_el, b->hm_el, sizeof(double) * DSM_PSV_NHM * 4 * a->n_hm) &&
+            same(a->r, b->r, sizeof(double) * a->r_n) && same(a->rrsta, b->rrsta, sizeof(double) * 3 * a->r_n) &&
+            same(a->iista, b->iista, sizeof(int) * 3 * a->r_n) &&
+            same(a->istazone, b->istazone, sizeof(int) * a->r_n) &&
+            same(a->theta, b->theta, sizeof(double) * a->theta_n);
+        if (!ok)
+            throw Error(DSM_ERR_INVALID,
+                        "the sources of a context must share the model, grid, receivers and distances");
+    }
+
     void alloc_batch() {
         size_t n = (size_t)d.nn - d.itmp + 1;
-        const size_t ls = (size_t)(d.jsrc - d.itmp + 1);
+        const size_t ls = (size_t)ls_min;  // scratch of the deepest source's forward substitution
         size_t per = (n + 1) * 3 * 16 + (n - ls + 2) * 5 * 16 + (size_t)ncap * NB * 16 + NSLOT * NB * 16;
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
@@ -1892,17 +1957,17 @@ class PsvEngine : public Engine {
         tails.reserve(nsys);
         l0scr.reserve((size_t)F * (d.nn0 + 1) * 2);
         l0d.reserve((size_t)F * (d.nn0 + 1) * 4);
-        ab.reserve((size_t)F * 320);
+        ab.reserve((size_t)nsrc * F * 320);
         co.reserve((size_t)NSLOT * NB * nsys);
-        for (int m = 0; m < 3; ++m) Afld[m].reserve(((size_t)F * rows_m[m] * Lcap * afld_bytes + 7) / 8);
+        for (int m = 0; m < 3; ++m) Afld[m].reserve(((size_t)nsrc * F * rows_m[m] * Lcap * afld_bytes + 7) / 8);
         Cgemm.reserve(c_total());
-        cut.reserve(F);
-        amps.reserve((size_t)F * Lcap);
+        cut.reserve((size_t)nsrc * F);
+        amps.reserve((size_t)nsrc * F * Lcap);
         size_t pt, pr, ps;
         out_sizes(&pt, &pr, &ps);
-        out_t.reserve(2 * pt * F);
-        out_r.reserve(2 * pr * F);
-        out_s.reserve(2 * ps * F);
+        out_t.reserve(2 * pt * F * nsrc);
+        out_r.reserve(2 * pr * F * nsrc);
+        out_s.reserve(2 * ps * F * nsrc);
     }
 
     size_t out_sizes(size_t* nt, size_t* nr, size_t* ns) const override {
@@ -1923,92 +1988,119 @@ class PsvEngine : public Engine {
         k_psv_rows<<<dim3((d.nn + 1 + 127) / 128, nf), 128, 0, st>>>(d, B0.p, B1.p, B2.p, Prow.p);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
-        k_psv_abnum<<<(nf + 31) / 32, 32, 0, st>>>(d, fr_, nf, ab.p);
-        DSM_LAUNCH(*this);
+        for (int k = 0; k < nsrc; ++k) {
+            k_psv_abnum<<<(nf + 31) / 32, 32, 0, st>>>(dsrc[k], fr_, nf, ab.p + (size_t)k * F * 320);
+            DSM_LAUNCH(*this);
+        }
     }
 
     void solve_chunk(const int* fr_, int nf, const WorkList& wl, int nsys) override {
         if (!l0_done) {  // order 0 once per batch (its own tridiagonal system)
             // order 0 is independent of the other orders: it runs on the side
-            // stream while the band solves run, and joins before the l-sum
+            // stream while the band solves run, and joins before the l-sum.
+            // Its solve factors the compact band in place: every source
+            // rebuilds it first.
             fork_side();
             int id0 = kid("psv_order0");
             kbegin(id0, st2);
-            k_psv_l0_build<<<dim3((d.nn0 + 127) / 128, nf), 128, 0, st2>>>(d, B0.p, B1.p, B2.p, l0col.p,
-                                                                            l0e1.p, l0scr.p);
-            if (mixed()) k_psv_l0_solve<true><<<nf, 128, 0, st2>>>(d, fr_, nf, ab.p, l0scr.p, l0d.p, rsgt_sw);
-            else k_psv_l0_solve<false><<<nf, 128, 0, st2>>>(d, fr_, nf, ab.p, l0scr.p, l0d.p, rsgt_sw);
-            if (afld_bytes == 4)
-                k_psv_l0_fields<float><<<dim3((R + 1 + 127) / 128, nf), 128, 0, st2>>>(
-                    d, l0d.p, afld32(0), afld32(1), afld32(2), Lcap, rsgt_sw);
-            else
-                k_psv_l0_fields<double><<<dim3((R + 1 + 127) / 128, nf), 128, 0, st2>>>(
-                    d, l0d.p, Afld[0].p, Afld[1].p, Afld[2].p, Lcap, rsgt_sw);
+            for (int k = 0; k < nsrc; ++k) {
+                const PsvDev& e = dsrc[k];
+                const cd* abk = ab.p + (size_t)k * F * 320;
+                k_psv_l0_build<<<dim3((d.nn0 + 127) / 128, nf), 128, 0, st2>>>(e, B0.p, B1.p, B2.p, l0col.p,
+                                                                                l0e1.p, l0scr.p);
+                if (mixed()) k_psv_l0_solve<true><<<nf, 128, 0, st2>>>(e, fr_, nf, abk, l0scr.p, l0d.p, rsgt_sw);
+                else k_psv_l0_solve<false><<<nf, 128, 0, st2>>>(e, fr_, nf, abk, l0scr.p, l0d.p, rsgt_sw);
+                if (afld_bytes == 4)
+                    k_psv_l0_fields<float><<<dim3((R + 1 + 127) / 128, nf), 128, 0, st2>>>(
+                        e, l0d.p, afld_of<float>(0, k), afld_of<float>(1, k), afld_of<float>(2, k), Lcap, rsgt_sw);
+                else
+                    k_psv_l0_fields<double><<<dim3((R + 1 + 127) / 128, nf), 128, 0, st2>>>(
+                        e, l0d.p, afld_of<double>(0, k), afld_of<double>(1, k), afld_of<double>(2, k), Lcap,
+                        rsgt_sw);
+                DSM_LAUNCH(*this);
+            }
             kend(id0, 0.0, 0.0, st2);
-            DSM_LAUNCH(*this);
             l0_done = true;
         }
         // algorithmic bytes per system: the factorisation writes the three
-        // multipliers of every row the upward substitution reads (rows lmin
-        // .. n) and zh of the four source bases above the source; the
-        // substitution reads both back and stores six solutions at the
-        // captured rows
-        const int n = d.nn - d.itmp + 1, ls = d.jsrc - d.itmp + 1;
-        const int lmin = std::max(1, std::min(jmin_loc, ls - 3));
-        const double fac_bytes = (double)(n - lmin + 1) * 3 * 16.0 + (double)(n - ls + 1) * 4 * 16.0;
-        const double sub_bytes = (double)(n - jmin_loc + 1) * 3 * 16.0 + (double)(n - ls + 1) * 4 * 16.0 +
-                                 (double)ncap * NB * 16.0;
+        // multipliers of every row the substitutions read (rows lmin .. n)
+        // and the pivots above the deepest source; per source, the forward
+        // substitution writes zh of its four bases above its source, and
+        // the upward substitution reads the multipliers and zh back and
+        // stores six solutions at the captured rows
+        const int n = d.nn - d.itmp + 1;
+        const int lmin = std::max(1, std::min(jmin_loc, ls_min - 3));
+        const double fac_bytes = (double)(n - lmin + 1) * 3 * 16.0 + (double)(n - ls_min + 1) * 16.0;
         int id = kid("psv_factor");
         kbegin(id);
         const unsigned fgrid = (unsigned)((nsys + FAC_THREADS - 1) / FAC_THREADS);
-        const int dmin = ls;  // pivots from the first source row up
+        const int dmin = ls_min;  // pivots from the deepest source row up
         if (mixed())
             k_psv_solve<true><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, tails.p, Dst.p, dmin);
         else
             k_psv_solve<false><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, tails.p, Dst.p, dmin);
-        DSM_LAUNCH(*this);
-        if (mixed())
-            k_psv_fwd<true><<<fgrid, FAC_THREADS, 0, st>>>(d, nsys, ls, Lst.p, Dst.p, dmin, tails.p, Zst.p);
-        else
-            k_psv_fwd<false><<<fgrid, FAC_THREADS, 0, st>>>(d, nsys, ls, Lst.p, Dst.p, dmin, tails.p, Zst.p);
         kend(id, fac_bytes * nsys, 0.0);
         DSM_LAUNCH(*this);
-        id = kid("psv_substitution");
-        kbegin(id);
-        if (mixed())
-            k_psv_up<true><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
-                d, nsys, jmin_loc, capmap.p, caplist.p, Lst.p, Zst.p, tails.p, Xcap.p);
-        else
-            k_psv_up<false><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
-                d, nsys, jmin_loc, capmap.p, caplist.p, Lst.p, Zst.p, tails.p, Xcap.p);
-        kend(id, sub_bytes * nsys, 0.0);
-        DSM_LAUNCH(*this);
-        id = kid("psv_source_coef");
-        kbegin(id);
-        k_psv_coef<<<(nsys + 127) / 128, 128, 0, st>>>(d, fr_, wl, nsys, ab.p, co.p, rsgt_sw);
-        kend(id, 0.0, 0.0);
-        DSM_LAUNCH(*this);
-        dim3 grid((nsys + 4 * FLD_SYS - 1) / (4 * FLD_SYS), (R + 1 + FLD_REC - 1) / FLD_REC);
-        id = kid("psv_fields");
-        kbegin(id);
-        if (afld_bytes == 4)
-            k_psv_fields<float, true><<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, afld32(0), afld32(1),
-                                                            afld32(2), Lcap, amps.p);
-        else
-            k_psv_fields<double, false><<<grid, 128, 0, st>>>(d, wl, nsys, Xcap.p, co.p, Afld[0].p, Afld[1].p,
-                                                              Afld[2].p, Lcap, amps.p);
-        kend(id, 0.0, 0.0);
-        DSM_LAUNCH(*this);
-        stats.solve_bytes += (fac_bytes + sub_bytes) * nsys;
+        double sub_tot = 0.0;
+        for (int k = 0; k < nsrc; ++k) {
+            const PsvDev& e = dsrc[k];
+            const int ls = e.jsrc - e.itmp + 1;
+            const double fwd_bytes = (double)(n - ls + 1) * (4 * 16.0 + 3 * 16.0 + 16.0);
+            const double sub_bytes = (double)(n - jmin_loc + 1) * 3 * 16.0 + (double)(n - ls + 1) * 4 * 16.0 +
+                                     (double)ncap * NB * 16.0;
+            sub_tot += fwd_bytes + sub_bytes;
+            id = kid("psv_forward");
+            kbegin(id);
+            if (mixed())
+                k_psv_fwd<true><<<fgrid, FAC_THREADS, 0, st>>>(e, nsys, ls, Lst.p, Dst.p, dmin, tails.p, Zst.p);
+            else
+                k_psv_fwd<false><<<fgrid, FAC_THREADS, 0, st>>>(e, nsys, ls, Lst.p, Dst.p, dmin, tails.p, Zst.p);
+            kend(id, fwd_bytes * nsys, 0.0);
+            DSM_LAUNCH(*this);
+            id = kid("psv_substitution");
+            kbegin(id);
+            if (mixed())
+                k_psv_up<true><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
+                    e, nsys, jmin_loc, capmap.p, caplist.p, Lst.p, Zst.p, tails.p, Xcap.p);
+            else
+                k_psv_up<false><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
+                    e, nsys, jmin_loc, capmap.p, caplist.p, Lst.p, Zst.p, tails.p, Xcap.p);
+            kend(id, sub_bytes * nsys, 0.0);
+            DSM_LAUNCH(*this);
+            id = kid("psv_source_coef");
+            kbegin(id);
+            k_psv_coef<<<(nsys + 127) / 128, 128, 0, st>>>(e, fr_, wl, nsys, ab.p + (size_t)k * F * 320, co.p,
+                                                            rsgt_sw);
+            kend(id, 0.0, 0.0);
+            DSM_LAUNCH(*this);
+            dim3 grid((nsys + 4 * FLD_SYS - 1) / (4 * FLD_SYS), (R + 1 + FLD_REC - 1) / FLD_REC);
+            double* amk = amps.p + (size_t)k * F * Lcap;
+            id = kid("psv_fields");
+            kbegin(id);
+            if (afld_bytes == 4)
+                k_psv_fields<float, true><<<grid, 128, 0, st>>>(e, wl, nsys, Xcap.p, co.p, afld_of<float>(0, k),
+                                                                afld_of<float>(1, k), afld_of<float>(2, k), Lcap,
+                                                                amk);
+            else
+                k_psv_fields<double, false><<<grid, 128, 0, st>>>(e, wl, nsys, Xcap.p, co.p, afld_of<double>(0, k),
+                                                                  afld_of<double>(1, k), afld_of<double>(2, k),
+                                                                  Lcap, amk);
+            kend(id, 0.0, 0.0);
+            DSM_LAUNCH(*this);
+        }
+        stats.solve_bytes += (fac_bytes + sub_tot) * nsys;
     }
 
     void scan_chunk(int nf, const WorkList& wl) override {
         int id = kid("psv_cutoff_scan");
         kbegin(id);
-        k_psv_scan<<<(nf + 3) / 4, 128, 0, st>>>(nf, wl, Lcap, maxlmax, ratl, tlen, vtop, rtop,
-                                                  d_freqs.p, amps.p, cut.p, dstatus());
+        for (int k = 0; k < nsrc; ++k) {
+            k_psv_scan<<<(nf + 3) / 4, 128, 0, st>>>(nf, wl, Lcap, maxlmax, ratl, tlen, vtop, rtop, d_freqs.p,
+                                                      amps.p + (size_t)k * F * Lcap, cut.p + (size_t)k * F,
+                                                      dstatus());
+            DSM_LAUNCH(*this);
+        }
         kend(id, 0.0, 0.0);
-        DSM_LAUNCH(*this);
     }
 
     void epilogue(const int* fr_, int w, int nf) override {
@@ -2032,8 +2124,8 @@ class PsvEngine : public Engine {
         const void* c0 = tc ? (const void*)c32(w, 0) : (const void*)c64(0);
         const void* c1 = tc ? (const void*)c32(w, 1) : (const void*)c64(1);
         const void* c2 = tc ? (const void*)c32(w, 2) : (const void*)c64(2);
-        psvk::launch_epilogue(e, w, th.x.p, th.s.p, th.pole.p, fr_, c0, c1, c2, tc, out_t.p,
-                              rsgt_sw ? out_r.p : nullptr, synn_sw ? out_s.p : nullptr, st);
+        psvk::launch_epilogue(e, w, th.x.p, th.s.p, th.pole.p, fr_, c0, c1, c2, tc, out_t_src(),
+                              rsgt_sw ? out_r_src() : nullptr, synn_sw ? out_s_src() : nullptr, st);
         kend(id, 0.0, 0.0);
         DSM_LAUNCH(*this);
     }
@@ -2041,6 +2133,8 @@ class PsvEngine : public Engine {
 
 }  // namespace
 
-Engine* make_psv_engine(const dsm_psv_setup_t* s, const dsm_options_t* o) { return new PsvEngine(s, o); }
+Engine* make_psv_engine(const dsm_psv_setup_t* const* s, int nsrc, const dsm_options_t* o) {
+    return new PsvEngine(s, nsrc, o);
+}
 
 }  // namespace dsm

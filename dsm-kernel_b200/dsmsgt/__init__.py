@@ -167,6 +167,9 @@ def lib() -> C.CDLL:
         L.dsm_sh_create.argtypes = [C.POINTER(ShSetup), C.POINTER(Options), C.POINTER(C.c_void_p)]
         L.dsm_psv_create.argtypes = [C.POINTER(PsvSetup), C.POINTER(Options), C.POINTER(C.c_void_p)]
         L.dsm_run_freqs.argtypes = [C.c_void_p, _ip, C.c_int, C.POINTER(Out)]
+        L.dsm_psv_create_multi.argtypes = [C.POINTER(C.POINTER(PsvSetup)), C.c_int, C.POINTER(Options),
+                                           C.POINTER(C.c_void_p)]
+        L.dsm_run_freqs_multi.argtypes = [C.c_void_p, _ip, C.c_int, C.POINTER(Out), C.c_int]
         L.dsm_run_freqs_device.argtypes = [C.c_void_p, _ip, C.c_int, C.POINTER(C.c_void_p),
                                            C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), _ip]
         L.dsm_ctx_destroy.argtypes = [C.c_void_p]
@@ -489,6 +492,61 @@ class Context:
         s = Stats()
         lib().dsm_get_stats(self.h, C.byref(s))
         return s
+
+    def close(self):
+        if self.h.value:
+            lib().dsm_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MultiSourceContext:
+    """Several source depths of one P-SV model in one context
+    (dsm_psv_create_multi): each (omega, l) band is factored once and solved
+    for every source."""
+
+    def __init__(self, setups, precision: int = DSM_PREC_FP64, device: int = 0, use_lmax_predictor: int = 0,
+                 l_chunk: int = 0, freq_batch: int = 0):
+        L = lib()
+        self.setups = list(setups)
+        assert all(s.mode == "psv" for s in self.setups)
+        self.opt = Options(precision, device, use_lmax_predictor, l_chunk, freq_batch)
+        arr = (C.POINTER(PsvSetup) * len(self.setups))(*[s.ptr for s in self.setups])
+        self.h = C.c_void_p()
+        rc = L.dsm_psv_create_multi(arr, len(self.setups), C.byref(self.opt), C.byref(self.h))
+        if rc:
+            raise DsmError(f"dsm_psv_create_multi failed ({rc}): {L.dsm_last_error(None).decode()}", rc)
+
+    def run(self, freqs):
+        """[(tsgt, rsgt, synn, llog)] per source, as Context.run returns."""
+        L = lib()
+        fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+        n = len(fl)
+        res, outs = [], (Out * len(self.setups))()
+        for k, s in enumerate(self.setups):
+            t, r, y, llog = alloc_outputs(s, n)
+            res.append((t, r, y, llog))
+            outs[k].tsgt = t.ctypes.data_as(_dp)
+            outs[k].rsgt = r.ctypes.data_as(_dp)
+            outs[k].synn = y.ctypes.data_as(_dp)
+            outs[k].llog = llog.ctypes.data_as(_ip)
+        rc = L.dsm_run_freqs_multi(self.h, _ptr(fl, _ip), n, outs, len(self.setups))
+        if rc:
+            raise DsmError(f"dsm_run_freqs_multi failed ({rc}): {L.dsm_last_error(self.h).decode()}", rc)
+        return res
+
+    def set_profiling(self, on: bool):
+        lib().dsm_set_profiling(self.h, 1 if on else 0)
+
+    def stats(self) -> Stats:
+        st = Stats()
+        lib().dsm_get_stats(self.h, C.byref(st))
+        return st
 
     def close(self):
         if self.h.value:

@@ -220,6 +220,24 @@ int dsm_run_freqs_device(dsm_ctx_t *ctx, const int *ilist, int n,
                          const void **d_tsgt, const void **d_rsgt,
                          const void **d_synn, int *llog);
 
+/* Several source depths in one P-SV context.  No counterpart in the
+ * reference, which takes one source depth per run (r0max = r0min,
+ * src/SGTpsv/others.f90:52-54) and factors the band of every (omega, l)
+ * once per run (SGTpsv-MPI.f90:885-890).  setups[0..nsrc) describe the same
+ * model, grid, receivers and distances (the arrays must be equal) and differ
+ * only in the source fields (spn, spo, r0, ecC0/F0/L0, ra_src, src_poly,
+ * jsrc); each (omega, l) band is assembled and factored once and solved for
+ * every source.  Each source keeps its own cutoff test and outputs, the same
+ * values as a context of that source alone. */
+int dsm_psv_create_multi(const dsm_psv_setup_t *const *setups, int nsrc,
+                         const dsm_options_t *opt, dsm_ctx_t **ctx);
+/* dsm_run_freqs for a context of nout = nsrc sources: outs[s] receives
+ * source s's outputs (RSGT, which does not depend on the source, in every
+ * set that asks for it); complex64 records are packed when outs[0] asks for
+ * them.  dsm_run_freqs refuses a context with more than one source, and the
+ * FP64 accuracy check covers single-source contexts. */
+int dsm_run_freqs_multi(dsm_ctx_t *ctx, const int *ilist, int n, dsm_out_t *outs, int nout);
+
 int dsm_ctx_destroy(dsm_ctx_t *ctx);
 const char *dsm_last_error(const dsm_ctx_t *ctx);
 const char *dsm_strerror(int code);
