@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 
 #include "engine.cuh"
 
@@ -54,6 +55,7 @@ void Engine::init_common(int dev) {
     // order and split), overridable for measurements
     if (const char* e = std::getenv("DSM_TC_FLAGS")) tc_flags = (uint32_t)std::atoi(e);
     if (const char* e = std::getenv("DSM_TC_BK")) tc_bk = std::atoi(e) == 64 ? 64 : 32;
+    tune.tc_orders = tc_bk;
     if (const char* e = std::getenv("DSM_TC_CHUNK")) tc_chunk = std::max(0, std::atoi(e));
     dflags.reserve(2);
     DSM_CUDA(cudaMemset(dflags.p, 0, 2 * sizeof(int)));
@@ -914,6 +916,44 @@ extern "C" int dsm_run_freqs_multi(dsm_ctx_t* ctx, const int* ilist, int n, dsm_
     });
 }
 
+extern "C" int dsm_run_request(dsm_ctx_t* const* ctxs, int nctx, const int* const* ilists, const int* ns,
+                               dsm_out_t* const* outs, int* rcs) {
+    if (!ctxs || nctx <= 0 || !ilists || !ns || !outs) return DSM_ERR_INVALID;
+    if (rcs)
+        for (int k = 0; k < nctx; ++k) rcs[k] = DSM_OK;
+    auto reject = [&](int k, const char* why) {
+        if (why) ctxs[k]->err = why;
+        if (rcs) rcs[k] = DSM_ERR_INVALID;
+        return DSM_ERR_INVALID;
+    };
+    for (int k = 0; k < nctx; ++k) {
+        if (!ctxs[k]) return DSM_ERR_INVALID;
+        if (!ilists[k] || !outs[k]) return reject(k, "a request context without frequencies or outputs");
+        for (int j = 0; j < k; ++j)
+            if (ctxs[j] == ctxs[k]) return reject(k, "a context appears twice in one request");
+        if (ctxs[k]->eng->opt.device != ctxs[0]->eng->opt.device)
+            return reject(k, "the contexts of a request share one device");
+    }
+    std::vector<int> rc(nctx, DSM_OK);
+    std::vector<std::thread> th;
+    th.reserve(nctx);
+    for (int k = 0; k < nctx; ++k)
+        th.emplace_back([&, k] {
+            dsm_ctx_t* c = ctxs[k];
+            rc[k] = guarded(c, [&] {
+                DSM_CUDA(cudaSetDevice(c->eng->opt.device));
+                c->eng->run(ilists[k], ns[k], outs[k], nullptr, nullptr, nullptr, nullptr);
+            });
+        });
+    for (auto& t : th) t.join();
+    int first = DSM_OK;
+    for (int k = 0; k < nctx; ++k) {
+        if (rcs) rcs[k] = rc[k];
+        if (first == DSM_OK) first = rc[k];
+    }
+    return first;
+}
+
 extern "C" int dsm_run_freqs_device(dsm_ctx_t* ctx, const int* ilist, int n, const void** d_tsgt,
                                     const void** d_rsgt, const void** d_synn, int* llog) {
     if (!ctx || !ilist) return DSM_ERR_INVALID;
@@ -1060,6 +1100,73 @@ extern "C" int dsm_get_accuracy(const dsm_ctx_t* ctx, dsm_accuracy_t* a) {
     if (!ctx || !a) return DSM_ERR_INVALID;
     *a = ctx->eng->acc;
     return DSM_OK;
+}
+
+extern "C" int dsm_get_tuning(const dsm_ctx_t* ctx, dsm_tuning_t* t) {
+    if (!ctx || !t) return DSM_ERR_INVALID;
+    *t = ctx->eng->tune;
+    return DSM_OK;
+}
+
+extern "C" int dsm_set_tuning(dsm_ctx_t* ctx, const dsm_tuning_t* t) {
+    if (!ctx || !t) return DSM_ERR_INVALID;
+    if ((t->fac_rows != 8 && t->fac_rows != 16) || (t->fld_orders != 16 && t->fld_orders != 32) ||
+        (t->tc_orders != 32 && t->tc_orders != 64)) {
+        ctx->err = "tuning: fac_rows 8 or 16, fld_orders 16 or 32, tc_orders 32 or 64";
+        return DSM_ERR_INVALID;
+    }
+    ctx->eng->tune = *t;
+    ctx->eng->tc_bk = t->tc_orders;
+    return DSM_OK;
+}
+
+extern "C" int dsm_autotune(dsm_ctx_t* ctx, const int* ilist, int n, int reps, dsm_tuning_t* best,
+                            double* ms_best) {
+    if (!ctx || !ilist || n <= 0 || reps <= 0) return DSM_ERR_INVALID;
+    return guarded(ctx, [&] {
+        dsm::Engine& e = *ctx->eng;
+        DSM_CUDA(cudaSetDevice(e.opt.device));
+        const dsm_tuning_t keep = e.tune;
+        std::vector<dsm_tuning_t> cand;
+        const bool psv = e.mode == 1;
+        for (int fr : {16, 8}) {
+            if (!psv && fr != keep.fac_rows) continue;
+            for (int fo : {32, 16}) {
+                if (!psv && fo != keep.fld_orders) continue;
+                for (int tb : {64, 32}) {
+                    if (!e.mixed() && tb != keep.tc_orders) continue;
+                    cand.push_back({psv ? fr : keep.fac_rows, psv ? fo : keep.fld_orders, e.mixed() ? tb : keep.tc_orders});
+                }
+            }
+        }
+        double best_ms = 1e300;
+        dsm_tuning_t win = keep;
+        try {
+            for (const auto& c : cand) {
+                e.tune = c;
+                e.tc_bk = c.tc_orders;
+                e.run(ilist, n, nullptr, nullptr, nullptr, nullptr, nullptr);  // untimed
+                double ms = 0.0;
+                for (int r = 0; r < reps; ++r) {
+                    e.run(ilist, n, nullptr, nullptr, nullptr, nullptr, nullptr);
+                    ms += e.stats.ms_total;
+                }
+                ms /= reps;
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    win = c;
+                }
+            }
+        } catch (...) {
+            e.tune = keep;
+            e.tc_bk = keep.tc_orders;
+            throw;
+        }
+        e.tune = win;
+        e.tc_bk = win.tc_orders;
+        if (best) *best = win;
+        if (ms_best) *ms_best = best_ms;
+    });
 }
 
 extern "C" int dsm_set_profiling(dsm_ctx_t* ctx, int on) {

@@ -87,6 +87,8 @@ class Engine {
     // probes and states, outputs) hold nsrc slots of F frequencies, and src
     // selects the slot the mode hooks and the l-sum work on.
     int nsrc = 1, src = 0;
+    // run-time tile shapes (dsm_set_tuning, dsm_autotune)
+    dsm_tuning_t tune{16, 32, 64};
     int amp_k = 1;                   // cutoff probes stored per order
     DBuf<double> Afld[3];            // field matrices per |m| [F][rows][Lcap]
     int afld_bytes = 8;              // their element: FP64, or FP32 where the mode's mixed path stores them so

@@ -579,19 +579,14 @@ void launch(const Maps& maps, const Problem* d_probs, int np, int ntiles, int pi
                            ((uint32_t)(BM >> 4) << 24);
     const int grid = std::min(ntiles, nsm);
     const size_t smem = SMEM_STAGES + 1024;
+    // the shared-memory attribute is set on every launch: it belongs to the
+    // current device, and contexts of several devices or host threads
+    // launch here (a host call of about a microsecond)
     if (bk == 32) {
-        static bool attr32 = false;
-        if (!attr32) {
-            DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            attr32 = true;
-        }
+        DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_lsum_tc<32><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, chunk, d_err, wait_ns);
     } else if (bk == 64) {
-        static bool attr64 = false;
-        if (!attr64) {
-            DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            attr64 = true;
-        }
+        DSM_CUDA(cudaFuncSetAttribute(k_lsum_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_lsum_tc<64><<<grid, NTHREADS, smem, st>>>(maps, d_probs, np, ntiles, idesc, flags, chunk, d_err, wait_ns);
     } else {
         throw Error(DSM_ERR_INVALID, "BK must be 32 or 64");

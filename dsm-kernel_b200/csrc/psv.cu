@@ -536,7 +536,7 @@ __device__ __forceinline__ void factor_step_main(int k, cd (&M)[4][4], const cd 
 // pivots of the rows the source bases' forward substitution reads (k >=
 // dmin) to Dst, the last pivots to tail.  The row pieces stream through
 // shared memory: a block (128 consecutive systems: consecutive orders of at
-// most a few frequencies) copies FAC_CH rows of each of its frequencies
+// most a few frequencies) copies CH rows of each of its frequencies
 // with cp.async one chunk ahead, so the recurrence waits on shared-memory
 // latency only.  Systems of frequencies beyond the first FAC_NW of a block
 // read their rows from global memory.  All threads of a block take the same
@@ -549,19 +549,16 @@ __device__ __forceinline__ void factor_step_main(int k, cd (&M)[4][4], const cd 
 // warps to hide the recurrence's latency), and one factorisation can serve
 // several sources.
 constexpr int FAC_THREADS = 128;
-#ifndef DSM_FAC_CH
-#define DSM_FAC_CH 16
-#endif
-constexpr int FAC_CH = DSM_FAC_CH;  // rows per chunk (multiple of 4)
-static_assert(FAC_CH % 4 == 0, "chunks hold whole groups of four steps");
+// rows per staged chunk (CH, a multiple of 4): 8 or 16, chosen per context
+// (dsm_set_tuning / dsm_autotune)
 constexpr int FAC_NW = 4;   // frequencies staged per block
 
-template <bool FAST>
+template <bool FAST, int CH>
 __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
                                                               int nsys, int lmin, cd* __restrict__ Lst,
                                                               SysTail* __restrict__ tail, cd* __restrict__ Dst,
                                                               int dmin) {
-    __shared__ __align__(16) cd sP[2][FAC_NW][FAC_CH][12];
+    __shared__ __align__(16) cd sP[2][FAC_NW][CH][12];
     const int sys0 = blockIdx.x * FAC_THREADS;
     const int sysv = sys0 + threadIdx.x;
     const bool valid = sysv < nsys;
@@ -591,8 +588,8 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
     const int n = c.n;
     // local rows 5 .. n in chunks: chunk q = rows 5 + q CH .. (global it + r - 1)
     auto stage = [&](int q, int buf) {
-        const int r0 = 5 + q * FAC_CH;
-        const int cnt = min(FAC_CH, n - r0 + 1);
+        const int r0 = 5 + q * CH;
+        const int cnt = min(CH, n - r0 + 1);
         if (cnt <= 0) return;
         const int per = cnt * 12;
         for (int e = threadIdx.x; e < nws * per; e += FAC_THREADS) {
@@ -629,7 +626,7 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
     // row entering at step k: local row k+4, chunk (k-1)/CH, index (k-1)%CH
     auto entering = [&](int k, cd (&an)[4]) {
         if (k + 4 > n) return;
-        const int i = (k - 1) % FAC_CH, buf = ((k - 1) / FAC_CH) & 1;
+        const int i = (k - 1) % CH, buf = ((k - 1) / CH) & 1;
         if (staged) {
 #pragma unroll
             for (int v = 0; v < 12; ++v) rp.v[v] = sP[buf][ws][i][v];
@@ -638,10 +635,10 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
         }
         assemble_row<FAST>(rp, c.l2, c.lsq, an);
     };
-    // chunk boundary at k (k - 1 a multiple of FAC_CH): the next chunk's copies go out
+    // chunk boundary at k (k - 1 a multiple of CH): the next chunk's copies go out
     auto boundary = [&](int k) {
-        if ((k - 1) % FAC_CH == 0) {
-            const int q = (k - 1) / FAC_CH;
+        if ((k - 1) % CH == 0) {
+            const int q = (k - 1) / CH;
             stage(q + 1, (q + 1) & 1);
             cp_async_commit();
             cp_async_wait<1>();
@@ -668,7 +665,7 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
             entering(k + 3, an);
             factor_step_main<0, FAST>(k + 3, M, an, c, so);
             keepD(k + 3);
-            if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+            if ((k + 3) % CH == 0) __syncthreads();  // chunk fully used before its buffer refills
             continue;
         }
         bool last;
@@ -688,7 +685,7 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
         last = factor_step<0, FAST>(k + 3, M, an, T, c, so);
         keepD(k + 3);
         if (last) { T.Dn = M[0][0]; break; }
-        if ((k + 3) % FAC_CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+        if ((k + 3) % CH == 0) __syncthreads();  // chunk fully used before its buffer refills
     }
     cp_async_wait<0>();  // no copy outlives the block
     if (valid) {
@@ -1427,9 +1424,9 @@ __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restric
 // Per (omega, l >= 1, receiver group): receiver fields of every slot and the
 // cutoff probe (group 0).
 // Fields of every slot at the receivers, one thread per (system, receiver):
-// a warp holds FLD_SYS consecutive systems (orders) x FLD_REC receivers, so
-// each coefficient load serves FLD_REC receivers and each field store writes
-// FLD_SYS consecutive orders of one row (32 x 1 measured fastest of 4 x 8,
+// a warp holds FS consecutive systems (orders) x 32/FS receivers, so
+// each coefficient load serves 32/FS receivers and each field store writes
+// FS consecutive orders of one row (32 x 1 measured fastest of 4 x 8,
 // 8 x 4, 16 x 2 and 32 x 1 on the benchmark; the results do not depend on
 // it).  Values and radial derivatives of the six
 // basis solutions come from the three-node weights (interpolate, calup),
@@ -1437,11 +1434,8 @@ __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restric
 // source coefficients.  Block row 0 also writes the cutoff probe (calamp of
 // imt = 1, m = 0 at the top receiver's stencil); the last block row holds
 // the surface (rows n-1, n).
-#ifndef DSM_FLD_SYS
-#define DSM_FLD_SYS 32
-#endif
-constexpr int FLD_SYS = DSM_FLD_SYS, FLD_REC = 32 / FLD_SYS;
-static_assert(FLD_SYS * FLD_REC == 32, "a warp is FLD_SYS systems x FLD_REC receivers");
+// FS systems x 32/FS receivers per warp: 32 (default) or 16, chosen per
+// context (dsm_set_tuning / dsm_autotune)
 
 // acc + r x for a real r: FAST with fused multiply-adds
 template <bool FAST>
@@ -1452,14 +1446,14 @@ __device__ __forceinline__ cd caddmulR(cd acc, double r, cd x) {
 
 // FAST (mixed path, FP32 field storage): fused multiply-adds and one
 // reciprocal of sqrt(l(l+1)); otherwise the reference's operations.
-template <class T, bool FAST>
+template <class T, bool FAST, int FS>
 __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int nsys,
                                                     const cd* __restrict__ Xcap, const cd* __restrict__ co,
                                                     T* __restrict__ A0f, T* __restrict__ A1f, T* __restrict__ A2f,
                                                     int Lcap, double* __restrict__ amps) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int sys = (blockIdx.x * 4 + warp) * FLD_SYS + lane % FLD_SYS;
-    const int r = blockIdx.y * FLD_REC + lane / FLD_SYS;
+    const int sys = (blockIdx.x * 4 + warp) * FS + lane % FS;
+    const int r = blockIdx.y * (32 / FS) + lane / FS;
     const int R = d.R;
     if (sys >= nsys || r > R) return;
     int w, l;
@@ -2035,10 +2029,16 @@ class PsvEngine : public Engine {
         kbegin(id);
         const unsigned fgrid = (unsigned)((nsys + FAC_THREADS - 1) / FAC_THREADS);
         const int dmin = ls_min;  // pivots from the deepest source row up
-        if (mixed())
-            k_psv_solve<true><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, tails.p, Dst.p, dmin);
-        else
-            k_psv_solve<false><<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, tails.p, Dst.p, dmin);
+        auto factor = [&](auto kern) {
+            kern<<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, tails.p, Dst.p, dmin);
+        };
+        if (mixed()) {
+            if (tune.fac_rows == 8) factor(k_psv_solve<true, 8>);
+            else factor(k_psv_solve<true, 16>);
+        } else {
+            if (tune.fac_rows == 8) factor(k_psv_solve<false, 8>);
+            else factor(k_psv_solve<false, 16>);
+        }
         kend(id, fac_bytes * nsys, 0.0);
         DSM_LAUNCH(*this);
         double sub_tot = 0.0;
@@ -2073,18 +2073,20 @@ class PsvEngine : public Engine {
                                                             rsgt_sw);
             kend(id, 0.0, 0.0);
             DSM_LAUNCH(*this);
-            dim3 grid((nsys + 4 * FLD_SYS - 1) / (4 * FLD_SYS), (R + 1 + FLD_REC - 1) / FLD_REC);
+            const int fs = tune.fld_orders == 16 ? 16 : 32, frec = 32 / fs;
+            dim3 grid((nsys + 4 * fs - 1) / (4 * fs), (R + 1 + frec - 1) / frec);
             double* amk = amps.p + (size_t)k * F * Lcap;
             id = kid("psv_fields");
             kbegin(id);
-            if (afld_bytes == 4)
-                k_psv_fields<float, true><<<grid, 128, 0, st>>>(e, wl, nsys, Xcap.p, co.p, afld_of<float>(0, k),
-                                                                afld_of<float>(1, k), afld_of<float>(2, k), Lcap,
-                                                                amk);
-            else
-                k_psv_fields<double, false><<<grid, 128, 0, st>>>(e, wl, nsys, Xcap.p, co.p, afld_of<double>(0, k),
-                                                                  afld_of<double>(1, k), afld_of<double>(2, k),
-                                                                  Lcap, amk);
+            if (afld_bytes == 4) {
+                auto kern = fs == 16 ? k_psv_fields<float, true, 16> : k_psv_fields<float, true, 32>;
+                kern<<<grid, 128, 0, st>>>(e, wl, nsys, Xcap.p, co.p, afld_of<float>(0, k), afld_of<float>(1, k),
+                                           afld_of<float>(2, k), Lcap, amk);
+            } else {
+                auto kern = fs == 16 ? k_psv_fields<double, false, 16> : k_psv_fields<double, false, 32>;
+                kern<<<grid, 128, 0, st>>>(e, wl, nsys, Xcap.p, co.p, afld_of<double>(0, k), afld_of<double>(1, k),
+                                           afld_of<double>(2, k), Lcap, amk);
+            }
             kend(id, 0.0, 0.0);
             DSM_LAUNCH(*this);
         }

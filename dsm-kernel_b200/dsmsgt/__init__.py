@@ -121,6 +121,10 @@ DSM_ERR_NOMEM = 6
 DSM_ERR_NODEVICE = 7
 
 
+class Tuning(C.Structure):
+    _fields_ = [("fac_rows", C.c_int), ("fld_orders", C.c_int), ("tc_orders", C.c_int)]
+
+
 class Accuracy(C.Structure):
     _fields_ = [("nfreq", C.c_int), ("llog_equal", C.c_int), ("tsgt", C.c_double * 20),
                 ("rsgt", C.c_double * 10), ("synn", C.c_double * 10), ("tsgt_max", C.c_double),
@@ -170,6 +174,11 @@ def lib() -> C.CDLL:
         L.dsm_psv_create_multi.argtypes = [C.POINTER(C.POINTER(PsvSetup)), C.c_int, C.POINTER(Options),
                                            C.POINTER(C.c_void_p)]
         L.dsm_run_freqs_multi.argtypes = [C.c_void_p, _ip, C.c_int, C.POINTER(Out), C.c_int]
+        L.dsm_run_request.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(_ip), _ip,
+                                      C.POINTER(C.POINTER(Out)), _ip]
+        L.dsm_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+        L.dsm_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+        L.dsm_autotune.argtypes = [C.c_void_p, _ip, C.c_int, C.c_int, C.POINTER(Tuning), _dp]
         L.dsm_run_freqs_device.argtypes = [C.c_void_p, _ip, C.c_int, C.POINTER(C.c_void_p),
                                            C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), _ip]
         L.dsm_ctx_destroy.argtypes = [C.c_void_p]
@@ -421,6 +430,27 @@ class Context:
                 "rsgt": list(a.rsgt[:nr]), "synn": list(a.synn[:ns]), "tsgt_max": a.tsgt_max,
                 "rsgt_max": a.rsgt_max, "synn_max": a.synn_max}
 
+    def tuning(self) -> dict:
+        t = Tuning()
+        lib().dsm_get_tuning(self.h, C.byref(t))
+        return {"fac_rows": t.fac_rows, "fld_orders": t.fld_orders, "tc_orders": t.tc_orders}
+
+    def set_tuning(self, fac_rows: int = 16, fld_orders: int = 32, tc_orders: int = 64):
+        t = Tuning(fac_rows, fld_orders, tc_orders)
+        rc = lib().dsm_set_tuning(self.h, C.byref(t))
+        if rc:
+            raise DsmError(f"dsm_set_tuning failed ({rc}): {lib().dsm_last_error(self.h).decode()}", rc)
+
+    def autotune(self, freqs, reps: int = 2):
+        """Measures the tile shapes on this request and keeps the fastest
+        (dsm_autotune); returns (tuning dict, ms per request)."""
+        fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+        t, ms = Tuning(), C.c_double()
+        rc = lib().dsm_autotune(self.h, _ptr(fl, _ip), len(fl), reps, C.byref(t), C.byref(ms))
+        if rc:
+            raise DsmError(f"dsm_autotune failed ({rc}): {lib().dsm_last_error(self.h).decode()}", rc)
+        return {"fac_rows": t.fac_rows, "fld_orders": t.fld_orders, "tc_orders": t.tc_orders}, ms.value
+
     def debug_set(self, name: str, value: int = 1):
         """Test hook of the library's error paths (dsm_debug_set)."""
         rc = lib().dsm_debug_set(self.h, name.encode(), value)
@@ -548,6 +578,10 @@ class MultiSourceContext:
         lib().dsm_get_stats(self.h, C.byref(st))
         return st
 
+    tuning = Context.tuning
+    set_tuning = Context.set_tuning
+    autotune = Context.autotune
+
     def close(self):
         if self.h.value:
             lib().dsm_ctx_destroy(self.h)
@@ -558,6 +592,47 @@ class MultiSourceContext:
             self.close()
         except Exception:
             pass
+
+
+def run_request(contexts, freq_lists):
+    """Runs several contexts (Context or MultiSourceContext, one device)
+    together (dsm_run_request); returns, per context, the list of
+    (tsgt, rsgt, synn, llog) of its sources."""
+    L = lib()
+    n = len(contexts)
+    keep, results = [], []
+    handles = (C.c_void_p * n)()
+    ilists = (_ip * n)()
+    ns = (C.c_int * n)()
+    outs = (C.POINTER(Out) * n)()
+    for k, (ctx, freqs) in enumerate(zip(contexts, freq_lists)):
+        setups = ctx.setups if isinstance(ctx, MultiSourceContext) else [ctx.setup]
+        fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
+        o = (Out * len(setups))()
+        res = []
+        for j, s in enumerate(setups):
+            t, r, y, llog = alloc_outputs(s, len(fl))
+            res.append((t, r, y, llog))
+            o[j].tsgt = t.ctypes.data_as(_dp)
+            o[j].rsgt = r.ctypes.data_as(_dp)
+            o[j].synn = y.ctypes.data_as(_dp)
+            o[j].llog = llog.ctypes.data_as(_ip)
+        keep += [fl, o]
+        handles[k] = ctx.h.value
+        ilists[k] = _ptr(fl, _ip)
+        ns[k] = len(fl)
+        outs[k] = C.cast(o, C.POINTER(Out))
+        results.append(res)
+    rcs = np.zeros(n, np.int32)
+    rc = L.dsm_run_request(handles, n, ilists, ns, outs, _ptr(rcs, _ip))
+    if rc:
+        nz = np.nonzero(rcs)[0]
+        if len(nz) == 0:
+            raise DsmError(f"dsm_run_request failed ({rc}): {L.dsm_strerror(rc).decode()}", rc)
+        bad = int(nz[0])
+        raise DsmError(f"dsm_run_request failed ({rc}) in context {bad}: "
+                       f"{L.dsm_last_error(contexts[bad].h).decode()}", rc)
+    return results
 
 
 def cat_np1(tlen: float, fmax: int, sampling_hz: float, start: float, end: float):

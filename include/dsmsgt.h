@@ -238,6 +238,18 @@ int dsm_psv_create_multi(const dsm_psv_setup_t *const *setups, int nsrc,
  * FP64 accuracy check covers single-source contexts. */
 int dsm_run_freqs_multi(dsm_ctx_t *ctx, const int *ilist, int n, dsm_out_t *outs, int nout);
 
+/* A request of several contexts -- other models, P-SV and SH, each with one
+ * or several source depths -- run together: each context on its own host
+ * thread and CUDA streams, so the GPU overlaps one context's latency-bound
+ * band solves with another's l-sum.  No counterpart in the reference (one
+ * MPI job per model and depth).  ctxs must be distinct and on one device;
+ * for context k: ilists[k][0..ns[k]) and outs[k] (nsrc output sets, as
+ * dsm_run_freqs_multi takes them).  rcs[k] (if rcs is not NULL) receives
+ * each context's code; the call returns the first code that is not DSM_OK
+ * (the texts stay with the contexts). */
+int dsm_run_request(dsm_ctx_t *const *ctxs, int nctx, const int *const *ilists, const int *ns,
+                    dsm_out_t *const *outs, int *rcs);
+
 int dsm_ctx_destroy(dsm_ctx_t *ctx);
 const char *dsm_last_error(const dsm_ctx_t *ctx);
 const char *dsm_strerror(int code);
@@ -296,6 +308,25 @@ typedef struct dsm_accuracy {
 } dsm_accuracy_t;
 int dsm_set_fp64_check(dsm_ctx_t *ctx, dsm_ctx_t *fp64_ctx, int stride);
 int dsm_get_accuracy(const dsm_ctx_t *ctx, dsm_accuracy_t *acc);
+
+/* Tile shapes of a context, chosen at run time.  No counterpart in the
+ * reference (a CPU program with no tiles).  The defaults are the measured
+ * best on the benchmark; dsm_autotune measures the alternatives on the
+ * caller's own request and keeps the fastest. */
+typedef struct dsm_tuning {
+    int fac_rows;    /* band rows a factorisation block stages per chunk: 8 or 16 (P-SV) */
+    int fld_orders;  /* consecutive orders per warp of the receiver-field kernel: 16 or 32 (P-SV) */
+    int tc_orders;   /* orders per tensor-core stage (and FP64 chunk sum): 32 or 64 (mixed precision) */
+} dsm_tuning_t;
+int dsm_get_tuning(const dsm_ctx_t *ctx, dsm_tuning_t *t);
+int dsm_set_tuning(dsm_ctx_t *ctx, const dsm_tuning_t *t);
+/* Runs the request ilist[0..n) reps times (after one untimed run) with each
+ * combination of the tile shapes that applies to the context's mode and
+ * precision, keeps the one with the least device time and returns it in
+ * *best (and its mean time per request in *ms_best, ms).  Outputs of these
+ * runs are discarded; every combination gives results within the context's
+ * accuracy (FP64: identical values). */
+int dsm_autotune(dsm_ctx_t *ctx, const int *ilist, int n, int reps, dsm_tuning_t *best, double *ms_best);
 
 /* Turns per-kernel event timing on (1) or off (0) for later runs. */
 int dsm_set_profiling(dsm_ctx_t *ctx, int on);
