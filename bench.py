@@ -411,6 +411,130 @@ def catalogue_bench(args):
             "cpu_baseline": cpu, "clocks": clk}))
 
 
+# Batched uneven-size form, scaled to fit a few minutes of one GPU: several
+# seeded models and source depths of P-SV and SH in one request.  P-SV
+# depths of a model share one context (one factorisation per (omega, l));
+# SH contexts hold one depth each.
+BATCH = dict(tlen=3276.8, imax=1024, models=4, psv_depths_km=[10, 108, 207, 305, 404, 502, 601, 700],
+             sh_depths_km=[100, 400],
+             psv=dict(thdelta=0.25, rdelta=26.75, rmin=1000.0, rmax=6350.0),
+             sh=dict(thdelta=0.5, rdelta=28.5, rmin=3500.0, rmax=6321.5))
+
+
+def batch_setups(model: int, mode: str, depths_km):
+    import dsmsgt
+    from dsmsgt import synth
+    g = BATCH[mode]
+    text = synth.psv_earth_model(model) if mode == "psv" else synth.sh_mantle_model(model)
+    out = []
+    for d in depths_km:
+        job = dsmsgt.Job(synth.param_file(tlen=BATCH["tlen"], rmin=g["rmin"], rmax=g["rmax"], rdelta=g["rdelta"],
+                                          r0=6371.0 - d, thmin=0.0, thmax=180.0, thdelta=g["thdelta"], imin=0,
+                                          imax=BATCH["imax"]), synth.dsm_config(), text)
+        out.append(dsmsgt.Setup(job, mode))
+    return out
+
+
+def batch_bench(args):
+    """Several models x source depths, P-SV and SH, per step: per_step
+    frequencies of every context.  Timed twice over the same steps: the
+    contexts one after another with the default tile shapes, and all of them
+    in one dsm_run_request (each context on its own host thread and streams)
+    after dsm_autotune chose each context's tiles.  The unit is a
+    source-frequency slice (one frequency of one source depth, every order
+    to the cutoff, all outputs on the full grid)."""
+    import torch
+    import dsmsgt
+    prec = {"fp64": dsmsgt.DSM_PREC_FP64, "mixed": dsmsgt.DSM_PREC_MIXED,
+            "mixed_bf16": dsmsgt.DSM_PREC_MIXED_BF16}[args.precision]
+    F = args.per_step
+    imax = BATCH["imax"]
+    psv = [batch_setups(m, "psv", BATCH["psv_depths_km"]) for m in range(BATCH["models"])]
+    sh = [batch_setups(m, "sh", BATCH["sh_depths_km"]) for m in range(BATCH["models"])]
+    ctxs = ([dsmsgt.MultiSourceContext(ss, precision=prec, freq_batch=F) for ss in psv] +
+            [dsmsgt.Context(s, precision=prec, freq_batch=F) for ss in sh for s in ss])
+    nsrc = [len(c.setups) if isinstance(c, dsmsgt.MultiSourceContext) else 1 for c in ctxs]
+    per_step = F * sum(nsrc)
+
+    def freqs(step, k):  # each context its own spread of the band
+        return step_freqs(step * 7 + k, F, imax)
+
+    def sequential(step):
+        for k, c in enumerate(ctxs):
+            dsmsgt.run_request([c], [freqs(step, k)], outputs=False)
+
+    def together(step):
+        dsmsgt.run_request(ctxs, [freqs(step, k) for k in range(len(ctxs))], outputs=False)
+
+    def timed(fn):
+        for w in range(args.warmup):
+            fn(1000 + w)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(0)
+        clocks.start()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            fn(k)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        return t, clocks.stop()
+
+    t_seq, clk_seq = timed(sequential)
+    tunings = []
+    for k, c in enumerate(ctxs):
+        t, _ = c.autotune(freqs(2000, k), reps=1)
+        tunings.append(t)
+    t_req, clk = timed(together)
+    free, total = torch.cuda.mem_get_info()
+    launches = sum(c.stats().launches for c in ctxs)
+    for c in ctxs:
+        c.close()
+
+    # accuracy of the mixed path on the batch: one model's P-SV depths and
+    # one SH context, mixed against FP64 on a low and the top frequency
+    rel = None
+    if prec != dsmsgt.DSM_PREC_FP64:
+        worst = {"tsgt": 0.0, "rsgt": 0.0, "synn": 0.0}
+        fr = [3, imax]
+        for ss in (psv[1][::3],):
+            a = dsmsgt.MultiSourceContext(ss, precision=prec, freq_batch=2)
+            b = dsmsgt.MultiSourceContext(ss, precision=dsmsgt.DSM_PREC_FP64, freq_batch=2)
+            for ga, gb in zip(a.run(fr), b.run(fr)):
+                for key, x, y in zip(("tsgt", "rsgt", "synn"), ga[:3], gb[:3]):
+                    worst[key] = max(worst[key], max(per_component_rel_l2(x, y)))
+            a.close()
+            b.close()
+        a = dsmsgt.Context(sh[1][0], precision=prec, freq_batch=2)
+        b = dsmsgt.Context(sh[1][0], precision=dsmsgt.DSM_PREC_FP64, freq_batch=2)
+        for key, x, y in zip(("tsgt", "rsgt", "synn"), a.run(fr)[:3], b.run(fr)[:3]):
+            worst[key] = max(worst[key], max(per_component_rel_l2(x, y)))
+        a.close()
+        b.close()
+        rel = dict(worst, frequencies=fr, sample="model 1: P-SV depths 10, 305, 601 km and SH 100 km")
+
+    slices = args.steps * per_step
+    line = {"metric": "SGT source-frequency slices/s, batched models x depths (P-SV + SH)",
+            "value": slices / t_req, "unit": "source-freq-slices/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_req / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == dsmsgt.DSM_PREC_FP64 else "fp16x2 pieces, f32 accumulate (l-sum); f64 solves",
+            "data": "synthetic (seeded 1-D polynomial models, reference file formats)",
+            "config": {"workload": "batched models x depths", "tlen_s": BATCH["tlen"], "np": imax,
+                       "models": BATCH["models"], "psv_depths_km": BATCH["psv_depths_km"],
+                       "sh_depths_km": BATCH["sh_depths_km"], "contexts": len(ctxs),
+                       "sources": sum(nsrc), "freqs_per_context_per_step": F, "precision": args.precision,
+                       "learned_lmax": False, "psv_grid": BATCH["psv"], "sh_grid": BATCH["sh"],
+                       "l2": "inputs larger than L2", "device_memory_used_gb": round((total - free) / 1e9, 1)},
+            "timing": "host wall clock around the requests, device synchronised on both sides "
+                      "(outputs stay on the device)",
+            "sequential": {"value": slices / t_seq, "ms_per_step": 1e3 * t_seq / args.steps,
+                           "tiles": "default", "clocks": clk_seq},
+            "speedup_request_vs_sequential": t_seq / t_req,
+            "tunings": tunings, "gpu_launches": int(launches), "clocks": clk,
+            "rel_l2_vs_fp64": rel}
+    print(json.dumps(line))
+
+
 def reference_arm(args):
     """The reference's CPU implementation of the path (the oracle: the FP64
     restatement of the Fortran frequency loop, with its own set-up), timed on
@@ -451,7 +575,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", "--mode", dest="mode", default="psv2048",
-                    choices=["psv1024", "psv2048", "sh256", "psv", "sh", "catalogue"])
+                    choices=["psv1024", "psv2048", "sh256", "psv", "sh", "catalogue", "batch"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_bf16"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-lmax", dest="lmax", action="store_false", help="plain first order ranges")
@@ -460,6 +584,13 @@ def main():
     args = ap.parse_args()
     if args.mode == "catalogue":
         catalogue_bench(args)
+        return
+    if args.mode == "batch":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the batched form has no reference run "
+                              "(one model and depth per reference job)"}))
+        elif int(os.environ.get("RANK", "0")) == 0:
+            batch_bench(args)
         return
 
     rank = int(os.environ.get("RANK", "0"))
@@ -643,6 +774,7 @@ def main():
                 "data": "synthetic (seeded 1-D polynomial model, reference file formats)",
                 "config": dict(desc, precision=args.precision, slices_per_step=args.per_step,
                                learned_lmax=bool(use_lmax),
+                               depth_cutoff=(1e-20 if mixed and mode == "psv" else 0.0),
                                parallelism=f"dp{world} (frequencies per rank)",
                                l2="inputs larger than L2 (field matrices of several GB per step)"),
                 "e2e": run["e2e"], "gpu_launches": int(run["launches"]),

@@ -20,6 +20,8 @@
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <climits>
+#include <cstdint>
 #include <cstring>
 #include <thread>
 
@@ -586,17 +588,42 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             }
         }
         const std::vector<int> span0 = span;  // first order range of each frequency
+        // goal[w]: end of the order range a frequency has asked for so far.
+        // A round that cannot hold every open range shares its capacity
+        // evenly (water-filling, multiples of 32 orders) from each
+        // frequency's lowest open order, so the long low-order systems of
+        // all frequencies share a launch and later launches hold the short
+        // high-order ones (a solve launch lasts as long as its longest
+        // system's recurrence).
+        std::vector<int> goal(nf);
+        for (int w = 0; w < nf; ++w) goal[w] = std::min(maxlmax + 1, span[w]);
         int maxend = 0;
         for (;;) {
-            std::vector<int> off(nf + 1, 0), lb(nf, 0);
+            std::vector<int> off(nf + 1, 0), lb(nf, 0), need(nf, 0);
+            long long want = 0;
+            for (int w = 0; w < nf; ++w) {
+                if (!hc[w].done && next[w] <= maxlmax) need[w] = std::max(0, goal[w] - next[w]);
+                want += need[w];
+            }
+            int share = INT32_MAX;  // every open range fits
+            if (want > nsys_max) {
+                std::vector<int> sorted;
+                for (int w = 0; w < nf; ++w)
+                    if (need[w] > 0) sorted.push_back(need[w]);
+                std::sort(sorted.begin(), sorted.end());
+                long long cap = nsys_max;
+                int left = (int)sorted.size();
+                for (int v : sorted) {
+                    if ((long long)v * left > cap) break;
+                    cap -= v;
+                    --left;
+                }
+                share = left > 0 ? std::max(32, (int)(cap / left) / 32 * 32) : INT32_MAX;
+            }
             int tot = 0;
             for (int w = 0; w < nf; ++w) {
                 lb[w] = next[w];
-                int cnt = 0;
-                if (!hc[w].done && next[w] <= maxlmax) {
-                    cnt = std::min(span[w], maxlmax + 1 - next[w]);
-                    cnt = std::max(0, std::min(cnt, nsys_max - tot));
-                }
+                const int cnt = std::max(0, std::min({need[w], share, nsys_max - tot}));
                 off[w] = tot;
                 tot += cnt;
                 next[w] += cnt;
@@ -631,7 +658,10 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
                 hc[w].done = all_sources_done(w);
                 if (!hc[w].done && next[w] > maxlmax) { hc[w].done = 1; }
                 all = all && hc[w].done;
-                if (!hc[w].done && opt.l_chunk <= 0) span[w] = std::min(4096, span[w] + span[w] / 2);
+                if (!hc[w].done && next[w] >= goal[w]) {  // its range is solved: the next one grows by half
+                    if (opt.l_chunk <= 0) span[w] = std::min(4096, span[w] + span[w] / 2);
+                    goal[w] = std::min(maxlmax + 1, next[w] + span[w]);
+                }
             }
             if (all) break;
         }
@@ -918,7 +948,7 @@ extern "C" int dsm_run_freqs_multi(dsm_ctx_t* ctx, const int* ilist, int n, dsm_
 
 extern "C" int dsm_run_request(dsm_ctx_t* const* ctxs, int nctx, const int* const* ilists, const int* ns,
                                dsm_out_t* const* outs, int* rcs) {
-    if (!ctxs || nctx <= 0 || !ilists || !ns || !outs) return DSM_ERR_INVALID;
+    if (!ctxs || nctx <= 0 || !ilists || !ns) return DSM_ERR_INVALID;
     if (rcs)
         for (int k = 0; k < nctx; ++k) rcs[k] = DSM_OK;
     auto reject = [&](int k, const char* why) {
@@ -928,7 +958,7 @@ extern "C" int dsm_run_request(dsm_ctx_t* const* ctxs, int nctx, const int* cons
     };
     for (int k = 0; k < nctx; ++k) {
         if (!ctxs[k]) return DSM_ERR_INVALID;
-        if (!ilists[k] || !outs[k]) return reject(k, "a request context without frequencies or outputs");
+        if (!ilists[k] || ns[k] <= 0) return reject(k, "a request context without frequencies");
         for (int j = 0; j < k; ++j)
             if (ctxs[j] == ctxs[k]) return reject(k, "a context appears twice in one request");
         if (ctxs[k]->eng->opt.device != ctxs[0]->eng->opt.device)
@@ -942,7 +972,7 @@ extern "C" int dsm_run_request(dsm_ctx_t* const* ctxs, int nctx, const int* cons
             dsm_ctx_t* c = ctxs[k];
             rc[k] = guarded(c, [&] {
                 DSM_CUDA(cudaSetDevice(c->eng->opt.device));
-                c->eng->run(ilists[k], ns[k], outs[k], nullptr, nullptr, nullptr, nullptr);
+                c->eng->run(ilists[k], ns[k], outs ? outs[k] : nullptr, nullptr, nullptr, nullptr, nullptr);
             });
         });
     for (auto& t : th) t.join();
@@ -1099,6 +1129,20 @@ extern "C" int dsm_set_fp64_check(dsm_ctx_t* ctx, dsm_ctx_t* ref, int stride) {
 extern "C" int dsm_get_accuracy(const dsm_ctx_t* ctx, dsm_accuracy_t* a) {
     if (!ctx || !a) return DSM_ERR_INVALID;
     *a = ctx->eng->acc;
+    return DSM_OK;
+}
+
+extern "C" int dsm_set_depth_cutoff(dsm_ctx_t* ctx, double bound) {
+    if (!ctx) return DSM_ERR_INVALID;
+    if (ctx->eng->mode != 1) {
+        ctx->err = "the depth cut-off applies to P-SV contexts";
+        return DSM_ERR_INVALID;
+    }
+    if (!(bound >= 0.0 && bound < 1.0)) {
+        ctx->err = "depth cut-off bound must lie in [0, 1)";
+        return DSM_ERR_INVALID;
+    }
+    ctx->eng->depth_bound = bound;
     return DSM_OK;
 }
 

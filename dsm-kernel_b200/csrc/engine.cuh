@@ -89,6 +89,8 @@ class Engine {
     int nsrc = 1, src = 0;
     // run-time tile shapes (dsm_set_tuning, dsm_autotune)
     dsm_tuning_t tune{16, 32, 64};
+    // depth cut-off amplitude bound (P-SV; 0: the whole band, as the reference)
+    double depth_bound = 0.0;
     int amp_k = 1;                   // cutoff probes stored per order
     DBuf<double> Afld[3];            // field matrices per |m| [F][rows][Lcap]
     int afld_bytes = 8;              // their element: FP64, or FP32 where the mode's mixed path stores them so

@@ -353,6 +353,21 @@ __device__ __forceinline__ void assemble_row(const RowPieces& r, double l2, doub
         }
     }
 }
+// Depth cut-off (mixed path): rows below the system's first kept row kc
+// leave the system.  Row j < kc becomes an identity row and the couplings of
+// rows j >= kc to rows below kc vanish, so the factorisation of those rows
+// yields pivot 1 and multipliers 0, and rows >= kc are factored exactly as a
+// band that starts at kc (a zero-displacement boundary there).
+__device__ __forceinline__ void cut_row(int j, int kc, cd a[4]) {
+    if (j < kc) {
+        a[0] = a[1] = a[2] = mk(0.0);
+        a[3] = mk(1.0);
+        return;
+    }
+#pragma unroll
+    for (int p = 0; p < 3; ++p)
+        if (j - 3 + p < kc) a[p] = mk(0.0);
+}
 template <bool FAST>
 __device__ __forceinline__ cd cmulT(cd a, cd b) {
     if (FAST) return mk(fma(a.re, b.re, -a.im * b.im), fma(a.re, b.im, a.im * b.re));
@@ -557,8 +572,9 @@ template <bool FAST, int CH>
 __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
                                                               int nsys, int lmin, cd* __restrict__ Lst,
                                                               SysTail* __restrict__ tail, cd* __restrict__ Dst,
-                                                              int dmin) {
+                                                              int dmin, const int* __restrict__ kcut) {
     __shared__ __align__(16) cd sP[2][FAC_NW][CH][12];
+    __shared__ int kb_sh;
     const int sys0 = blockIdx.x * FAC_THREADS;
     const int sysv = sys0 + threadIdx.x;
     const bool valid = sysv < nsys;
@@ -586,6 +602,16 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
     c.Dst = Dst;
     c.dmin = dmin;
     const int n = c.n;
+    // First kept row of the system (depth cut-off; 1 without), of its warp
+    // (a step group boundary: all lanes of a warp take the same steps) and
+    // of the block (the first staged chunk).  Warps start at their own row.
+    const int kc = kcut ? kcut[sys] : 1;
+    const int kw = ((__reduce_min_sync(0xffffffffu, kc) - 1) & ~3) + 1;
+    if (threadIdx.x == 0) kb_sh = kw;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) atomicMin(&kb_sh, kw);
+    __syncthreads();
+    const int q0 = (kb_sh - 1) / CH;
     // local rows 5 .. n in chunks: chunk q = rows 5 + q CH .. (global it + r - 1)
     auto stage = [&](int q, int buf) {
         const int r0 = 5 + q * CH;
@@ -597,7 +623,7 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
             cp_async16(&sP[buf][wi][i][v], Prow + ((size_t)(w0 + wi) * (d.nn + 1) + c.it + r0 + i - 1) * 12 + v);
         }
     };
-    stage(0, 0);
+    stage(q0, q0 & 1);
     cp_async_commit();
     cd M[4][4];
 #pragma unroll
@@ -606,12 +632,13 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
         for (int q = 0; q < 4; ++q) M[p][q] = mk(0.0);
     cd a[4];
     RowPieces rp;
-    // local rows 1..4 go to slots 1, 2, 3, 0
+    // local rows kw .. kw+3 go to slots 1, 2, 3, 0 (kw = 1 mod 4)
 #pragma unroll
     for (int p = 0; p < 4; ++p) {
-        if (p >= n) break;
-        load_row(c.P + (size_t)(c.it + p) * 12, rp);
+        if (kw + p > n) break;
+        load_row(c.P + (size_t)(c.it + kw - 1 + p) * 12, rp);
         assemble_row<FAST>(rp, c.l2, c.lsq, a);
+        if (kcut) cut_row(kw + p, kc, a);
 #pragma unroll
         for (int q = 0; q <= p; ++q) M[(1 + p) & 3][(1 + q) & 3] = a[4 - (p - q) - 1];
     }
@@ -634,6 +661,7 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
             load_row(c.P + (size_t)(c.it + k + 3) * 12, rp);
         }
         assemble_row<FAST>(rp, c.l2, c.lsq, an);
+        if (kcut) cut_row(k + 4, kc, an);
     };
     // chunk boundary at k (k - 1 a multiple of CH): the next chunk's copies go out
     auto boundary = [&](int k) {
@@ -650,8 +678,14 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
     auto keepD = [&](int k) {
         if (c.store && k >= c.dmin) c.Dst[(size_t)(k - c.dmin) * c.nsys + c.sys] = so.D;
     };
-    for (int k = 1;; k += 4) {
+    // a cut row never reaches the end of the band (it stays below the
+    // source), so warps wait for their first row in the main branch only
+    for (int k = q0 * CH + 1;; k += 4) {
         boundary(k);
+        if (k < kw) {  // this warp's band starts further up
+            if ((k + 3) % CH == 0) __syncthreads();
+            continue;
+        }
         if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
             entering(k, an);
             factor_step_main<1, FAST>(k, M, an, c, so);
@@ -777,11 +811,16 @@ __global__ void __launch_bounds__(UP_THREADS, 2) k_psv_up(PsvDev d, int nsys, in
                                                           const int* __restrict__ capmap,
                                                           const int2* __restrict__ caplist,
                                                           const cd* __restrict__ Lst, const cd* __restrict__ Zst,
-                                                          const SysTail* __restrict__ tail, cd* __restrict__ Xcap) {
+                                                          const SysTail* __restrict__ tail, cd* __restrict__ Xcap,
+                                                          const int* __restrict__ kcut) {
     extern __shared__ __align__(16) unsigned char up_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int sys = (blockIdx.x * UP_WARPS + warp) * 32 + lane;
+    // the warp's first factored row (the factorisation's warps are the same
+    // 32 systems): rows below it hold no multipliers and no solution
+    const int kw = kcut ? ((__reduce_min_sync(0xffffffffu, kcut[min(sys, nsys - 1)]) - 1) & ~3) + 1 : 1;
     if (sys >= nsys) return;  // nothing below synchronises across lanes
+    jmin_loc = max(jmin_loc, kw);
     cd* ring = reinterpret_cast<cd*>(up_smem) + (size_t)warp * UP_WARP_CD + lane;
     const int it = d.itmp, n = d.nn - it + 1, ls = d.jsrc - it + 1;
     auto store = [&](int c, int b, cd v) { Xcap[((size_t)c * NB + b) * nsys + sys] = v; };
@@ -913,6 +952,10 @@ __global__ void __launch_bounds__(UP_THREADS, 2) k_psv_up(PsvDev d, int nsys, in
     phase(std::integral_constant<int, UP_E1>{}, std::integral_constant<int, UP_CH1>{}, top, n1);
     phase(std::integral_constant<int, UP_E2>{}, std::integral_constant<int, UP_CH2>{}, top - n1,
           top - n1 - jmin_loc + 1);
+    // captured rows below the cut: zero displacement
+    for (; cap.x >= 1; cap = caplist[++ci])
+#pragma unroll
+        for (int b = 0; b < NB; ++b) store(cap.y, b, mk(0.0));
 }
 
 // ------------------------------------------------------------ l = 0 path
@@ -1655,6 +1698,44 @@ __global__ void k_psv_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ra
     if (lane == 0) cut[w] = c;
 }
 
+// Depth cut-off of an (omega, l) system.  Below the turning depth of the
+// slowest wave the displacement decays like exp(-E(r)),
+//   E(r) = int_r^{r_s} kappa dr',  kappa^2 = ((l + 1/2) / r')^2 - (omega / v(r'))^2,
+// counting only the evanescent parts (kappa^2 > 0); v is the SV speed in
+// solid zones, and fluid zones count as never evanescent (kappa = 0), which
+// only keeps more rows.  Starting at the deepest source r_s, the first node
+// where E reaches X bounds the amplitude there by exp(-X) of the source's,
+// and a zero-displacement boundary there perturbs what reaches the source
+// and receivers above by about exp(-2X).  One thread per system, FP32 (a
+// bound, not a result); nodes: x = r, y = 1 / v^2 (huge in fluid), z = local
+// row of the node's first unknown.  kcut = that row less a margin of four,
+// at most kmax (below the source rows).
+__global__ void k_psv_cutrow(const float4* __restrict__ nodes, int ks, float X, double tlen,
+                             const int* __restrict__ freqs, WorkList wl, int nsys, int kmax, int* __restrict__ kcut) {
+    const int sys = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sys >= nsys) return;
+    int w, l;
+    wl_map(wl, sys, w, l);
+    const float om = (float)(2.0 * kPi * (double)freqs[w] / tlen);
+    const float lam2 = ((float)l + 0.5f) * ((float)l + 0.5f), om2 = om * om;
+    auto kappa = [&](float4 v) { return sqrtf(fmaxf(0.0f, lam2 / (v.x * v.x) - om2 * v.y)); };
+    float4 a = nodes[ks];
+    float ka = kappa(a), E = 0.0f;
+    int row = 1;
+    for (int k = ks - 1; k >= 0; --k) {
+        const float4 b = nodes[k];
+        const float kb = kappa(b);
+        E += 0.5f * (ka + kb) * (a.x - b.x);
+        if (E >= X) {
+            row = (int)b.z;
+            break;
+        }
+        a = b;
+        ka = kb;
+    }
+    kcut[sys] = max(1, min(row - 4, kmax));
+}
+
 // ---------------------------------------------------------------- engine
 class PsvEngine : public Engine {
   public:
@@ -1667,6 +1748,11 @@ class PsvEngine : public Engine {
     DBuf<int4> rowasm;
     DBuf<SysTail> tails;
     int jmin_loc = 1, ncap = 0;
+    // depth cut-off: nodes (radius, 1/v^2, local row) from the centre up,
+    // the node at the deepest source, the first kept row per system
+    DBuf<float4> cnodes;
+    int cnode_src = 0;
+    DBuf<int> kcut;
     // one parameter set per source depth (the source fields differ), and
     // the source polynomials they point to
     std::vector<PsvDev> dsrc;
@@ -1886,6 +1972,34 @@ class PsvEngine : public Engine {
             }
             d = dsrc[0];
         }
+        {  // nodes of the depth cut-off (the grid of calra2_psv, its unknowns of calspdr)
+            std::vector<float4> nd;
+            double r0min = s->r0;
+            for (int k = 1; k < nsrc; ++k) r0min = std::min(r0min, ss[k]->r0);
+            auto inv_v2 = [&](int z, double rr) {
+                if (s->iphase[z] != 1) return 1e30;
+                double v = 0.0, x = 1.0;
+                for (int j = 0; j < 4; ++j, x *= rr / s->rmax) v += s->vsv[4 * z + j] * x;
+                return v > 0.0 ? 1.0 / (v * v) : 1e30;
+            };
+            nd.push_back(make_float4((float)s->vrmin[0], (float)inv_v2(0, s->vrmin[0]),
+                                     (float)(s->kkdr[0] - d.itmp + 1), 0.0f));
+            for (int z = 0; z < nz; ++z) {
+                const int nl = s->nlayer[z];
+                for (int i = 1; i <= nl; ++i) {
+                    const double rr = s->vrmin[z] + (s->vrmax[z] - s->vrmin[z]) * (double)i / (double)nl;
+                    double iv = inv_v2(z, rr);
+                    if (i == nl && z + 1 < nz) iv = std::max(iv, inv_v2(z + 1, rr));  // the slower side
+                    const int row = s->kkdr[z] + (s->iphase[z] == 1 ? 2 * i : i);
+                    nd.push_back(make_float4((float)rr, (float)iv, (float)(row - d.itmp + 1), 0.0f));
+                }
+            }
+            cnode_src = 0;
+            for (int k = 0; k < (int)nd.size(); ++k)
+                if ((double)nd[k].x <= r0min) cnode_src = k;
+            cnodes.upload(nd, st);
+        }
+        depth_bound = mixed() ? 1e-20 : 0.0;
         F = opt.freq_batch > 0 ? opt.freq_batch : 8;
         Lc = opt.l_chunk > 0 ? ((opt.l_chunk + 31) / 32) * 32 : 256;
         Lcap = std::min(maxlmax + 1 + Lc, 2048);
@@ -1929,13 +2043,22 @@ class PsvEngine : public Engine {
                         "the sources of a context must share the model, grid, receivers and distances");
     }
 
+    // first local row whose multipliers a substitution reads: the deepest
+    // captured row or three rows below the deepest source
+    int lst_min() const { return std::max(1, std::min(jmin_loc, ls_min - 3)); }
+
     void alloc_batch() {
         size_t n = (size_t)d.nn - d.itmp + 1;
         const size_t ls = (size_t)ls_min;  // scratch of the deepest source's forward substitution
-        size_t per = (n + 1) * 3 * 16 + (n - ls + 2) * 5 * 16 + (size_t)ncap * NB * 16 + NSLOT * NB * 16;
+        const size_t lrows = n - (size_t)lst_min() + 2;  // multiplier rows held (from lst_min up)
+        size_t per = lrows * 3 * 16 + (n - ls + 2) * 5 * 16 + (size_t)ncap * NB * 16 + NSLOT * NB * 16;
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
         nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(65536, (fr / 3) / per));
+        // no more than a round of a batch can launch (F ranges of at most
+        // max(4096, the first range of the top frequency)): contexts that
+        // share a device leave each other room
+        nsys_max = std::min(nsys_max, std::max(1024, F * std::max(4096, first_span(imax))));
         // DSM_MAX_SYSTEMS caps the systems per solve launch (and so the
         // factor scratch) below that, e.g. for small profiling captures
         if (const char* e = std::getenv("DSM_MAX_SYSTEMS")) nsys_max = std::max(1024, std::min(nsys_max, std::atoi(e)));
@@ -1944,11 +2067,12 @@ class PsvEngine : public Engine {
         B1.reserve((size_t)F * d.ncol_tot * 4);
         B2.reserve((size_t)F * d.ncol_tot * 4);
         Prow.reserve((size_t)F * (d.nn + 1) * 12);
-        Lst.reserve((n + 1) * 3 * nsys);
+        Lst.reserve(lrows * 3 * nsys);
         Zst.reserve((n - ls + 2) * 4 * nsys);
         Dst.reserve((n - ls + 2) * nsys);
         Xcap.reserve((size_t)ncap * NB * nsys);
         tails.reserve(nsys);
+        kcut.reserve(nsys);
         l0scr.reserve((size_t)F * (d.nn0 + 1) * 2);
         l0d.reserve((size_t)F * (d.nn0 + 1) * 4);
         ab.reserve((size_t)nsrc * F * 320);
@@ -2023,14 +2147,23 @@ class PsvEngine : public Engine {
         // the upward substitution reads the multipliers and zh back and
         // stores six solutions at the captured rows
         const int n = d.nn - d.itmp + 1;
-        const int lmin = std::max(1, std::min(jmin_loc, ls_min - 3));
+        const int lmin = lst_min();
+        // Lst holds rows lmin .. n: kernels index rows from 0 off this base
+        cd* const Lb = Lst.p - (size_t)lmin * 3 * nsys;
         const double fac_bytes = (double)(n - lmin + 1) * 3 * 16.0 + (double)(n - ls_min + 1) * 16.0;
         int id = kid("psv_factor");
         kbegin(id);
         const unsigned fgrid = (unsigned)((nsys + FAC_THREADS - 1) / FAC_THREADS);
         const int dmin = ls_min;  // pivots from the deepest source row up
+        const int* kc = nullptr;
+        if (depth_bound > 0.0 && ls_min > 9) {
+            k_psv_cutrow<<<(nsys + 127) / 128, 128, 0, st>>>(cnodes.p, cnode_src, (float)-std::log(depth_bound),
+                                                             d.tlen, fr_, wl, nsys, ls_min - 8, kcut.p);
+            DSM_LAUNCH(*this);
+            kc = kcut.p;
+        }
         auto factor = [&](auto kern) {
-            kern<<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lst.p, tails.p, Dst.p, dmin);
+            kern<<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lb, tails.p, Dst.p, dmin, kc);
         };
         if (mixed()) {
             if (tune.fac_rows == 8) factor(k_psv_solve<true, 8>);
@@ -2052,19 +2185,19 @@ class PsvEngine : public Engine {
             id = kid("psv_forward");
             kbegin(id);
             if (mixed())
-                k_psv_fwd<true><<<fgrid, FAC_THREADS, 0, st>>>(e, nsys, ls, Lst.p, Dst.p, dmin, tails.p, Zst.p);
+                k_psv_fwd<true><<<fgrid, FAC_THREADS, 0, st>>>(e, nsys, ls, Lb, Dst.p, dmin, tails.p, Zst.p);
             else
-                k_psv_fwd<false><<<fgrid, FAC_THREADS, 0, st>>>(e, nsys, ls, Lst.p, Dst.p, dmin, tails.p, Zst.p);
+                k_psv_fwd<false><<<fgrid, FAC_THREADS, 0, st>>>(e, nsys, ls, Lb, Dst.p, dmin, tails.p, Zst.p);
             kend(id, fwd_bytes * nsys, 0.0);
             DSM_LAUNCH(*this);
             id = kid("psv_substitution");
             kbegin(id);
             if (mixed())
                 k_psv_up<true><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
-                    e, nsys, jmin_loc, capmap.p, caplist.p, Lst.p, Zst.p, tails.p, Xcap.p);
+                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc);
             else
                 k_psv_up<false><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
-                    e, nsys, jmin_loc, capmap.p, caplist.p, Lst.p, Zst.p, tails.p, Xcap.p);
+                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc);
             kend(id, sub_bytes * nsys, 0.0);
             DSM_LAUNCH(*this);
             id = kid("psv_source_coef");

@@ -634,6 +634,10 @@ class ShEngine : public Engine {
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
         nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(65536, (fr / 3) / per));
+        // no more than a round of a batch can launch (F ranges of at most
+        // max(4096, the first range of the top frequency)): contexts that
+        // share a device leave each other room
+        nsys_max = std::min(nsys_max, std::max(1024, F * std::max(4096, first_span(imax))));
         // DSM_MAX_SYSTEMS caps the systems per solve launch (and so the
         // factor scratch) below that, e.g. for small profiling captures
         if (const char* e = std::getenv("DSM_MAX_SYSTEMS")) nsys_max = std::max(1024, std::min(nsys_max, std::atoi(e)));

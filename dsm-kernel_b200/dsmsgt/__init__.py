@@ -176,6 +176,7 @@ def lib() -> C.CDLL:
         L.dsm_run_freqs_multi.argtypes = [C.c_void_p, _ip, C.c_int, C.POINTER(Out), C.c_int]
         L.dsm_run_request.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(_ip), _ip,
                                       C.POINTER(C.POINTER(Out)), _ip]
+        L.dsm_set_depth_cutoff.argtypes = [C.c_void_p, C.c_double]
         L.dsm_get_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         L.dsm_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         L.dsm_autotune.argtypes = [C.c_void_p, _ip, C.c_int, C.c_int, C.POINTER(Tuning), _dp]
@@ -430,6 +431,13 @@ class Context:
                 "rsgt": list(a.rsgt[:nr]), "synn": list(a.synn[:ns]), "tsgt_max": a.tsgt_max,
                 "rsgt_max": a.rsgt_max, "synn_max": a.synn_max}
 
+    def set_depth_cutoff(self, bound: float):
+        """Amplitude bound of the P-SV depth cut-off (dsm_set_depth_cutoff;
+        0 = the whole band)."""
+        rc = lib().dsm_set_depth_cutoff(self.h, float(bound))
+        if rc:
+            raise DsmError(f"dsm_set_depth_cutoff failed ({rc}): {lib().dsm_last_error(self.h).decode()}", rc)
+
     def tuning(self) -> dict:
         t = Tuning()
         lib().dsm_get_tuning(self.h, C.byref(t))
@@ -580,6 +588,7 @@ class MultiSourceContext:
 
     tuning = Context.tuning
     set_tuning = Context.set_tuning
+    set_depth_cutoff = Context.set_depth_cutoff
     autotune = Context.autotune
 
     def close(self):
@@ -594,10 +603,11 @@ class MultiSourceContext:
             pass
 
 
-def run_request(contexts, freq_lists):
+def run_request(contexts, freq_lists, outputs: bool = True):
     """Runs several contexts (Context or MultiSourceContext, one device)
     together (dsm_run_request); returns, per context, the list of
-    (tsgt, rsgt, synn, llog) of its sources."""
+    (tsgt, rsgt, synn, llog) of its sources (None with outputs=False: the
+    run only computes, for timing)."""
     L = lib()
     n = len(contexts)
     keep, results = [], []
@@ -610,7 +620,7 @@ def run_request(contexts, freq_lists):
         fl = np.ascontiguousarray(np.asarray(freqs, dtype=np.int32))
         o = (Out * len(setups))()
         res = []
-        for j, s in enumerate(setups):
+        for j, s in enumerate(setups if outputs else []):
             t, r, y, llog = alloc_outputs(s, len(fl))
             res.append((t, r, y, llog))
             o[j].tsgt = t.ctypes.data_as(_dp)
@@ -621,8 +631,8 @@ def run_request(contexts, freq_lists):
         handles[k] = ctx.h.value
         ilists[k] = _ptr(fl, _ip)
         ns[k] = len(fl)
-        outs[k] = C.cast(o, C.POINTER(Out))
-        results.append(res)
+        outs[k] = C.cast(o, C.POINTER(Out)) if outputs else C.POINTER(Out)()
+        results.append(res if outputs else None)
     rcs = np.zeros(n, np.int32)
     rc = L.dsm_run_request(handles, n, ilists, ns, outs, _ptr(rcs, _ip))
     if rc:

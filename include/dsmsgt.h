@@ -244,7 +244,9 @@ int dsm_run_freqs_multi(dsm_ctx_t *ctx, const int *ilist, int n, dsm_out_t *outs
  * band solves with another's l-sum.  No counterpart in the reference (one
  * MPI job per model and depth).  ctxs must be distinct and on one device;
  * for context k: ilists[k][0..ns[k]) and outs[k] (nsrc output sets, as
- * dsm_run_freqs_multi takes them).  rcs[k] (if rcs is not NULL) receives
+ * dsm_run_freqs_multi takes them; outs or outs[k] NULL: nothing is copied
+ * to the host, the run only computes -- for timing, as dsm_autotune runs
+ * its candidates).  rcs[k] (if rcs is not NULL) receives
  * each context's code; the call returns the first code that is not DSM_OK
  * (the texts stay with the contexts). */
 int dsm_run_request(dsm_ctx_t *const *ctxs, int nctx, const int *const *ilists, const int *ns,
@@ -313,6 +315,16 @@ int dsm_get_accuracy(const dsm_ctx_t *ctx, dsm_accuracy_t *acc);
  * reference (a CPU program with no tiles).  The defaults are the measured
  * best on the benchmark; dsm_autotune measures the alternatives on the
  * caller's own request and keeps the fastest. */
+/* Depth cut-off of the P-SV band (no counterpart in the reference, which
+ * factors every band from the centre, SGTpsv-MPI.f90:662; the DSM config's
+ * ratc names the same idea).  Below the turning depth of the slowest wave an
+ * (omega, l) solution decays; rows where a WKB bound on its amplitude
+ * relative to the source falls under `bound` leave the system (a zero
+ * displacement boundary there), which changes the outputs by about bound^2
+ * relative.  0 turns it off.  Default: 1e-20 in the mixed precision modes,
+ * 0 in DSM_PREC_FP64 (the reference's results).  P-SV contexts only. */
+int dsm_set_depth_cutoff(dsm_ctx_t *ctx, double bound);
+
 typedef struct dsm_tuning {
     int fac_rows;    /* band rows a factorisation block stages per chunk: 8 or 16 (P-SV) */
     int fld_orders;  /* consecutive orders per warp of the receiver-field kernel: 16 or 32 (P-SV) */

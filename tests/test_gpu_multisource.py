@@ -21,18 +21,41 @@ def _setups(**kw):
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec", [dsmsgt.DSM_PREC_FP64, dsmsgt.DSM_PREC_MIXED])
 def test_multisource_equals_single_source_contexts(built, prec):
+    """Bit for bit without the depth cut-off (the mixed default is turned
+    off on both sides: a context cuts at the deepest of its sources)."""
     setups = _setups()
     freqs = [2, 17, 40]
     mc = dsmsgt.MultiSourceContext(setups, precision=prec, freq_batch=2)
+    mc.set_depth_cutoff(0.0)
     got = mc.run(freqs)
     mc.close()
     for s, g in zip(setups, got):
         c = dsmsgt.Context(s, precision=prec, freq_batch=2)
+        c.set_depth_cutoff(0.0)
         want = c.run(freqs)
         c.close()
         assert list(g[3]) == list(want[3])
         for a, b in zip(g[:3], want[:3]):
             assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_multisource_with_depth_cut_close_to_single_source_contexts(built):
+    """With the mixed path's default cut-off, the shared cut (from the
+    deepest source) moves each source's outputs by far less than the path's
+    tolerance."""
+    setups = _setups()
+    freqs = [2, 17, 40]
+    mc = dsmsgt.MultiSourceContext(setups, precision=dsmsgt.DSM_PREC_MIXED, freq_batch=2)
+    got = mc.run(freqs)
+    mc.close()
+    for s, g in zip(setups, got):
+        c = dsmsgt.Context(s, precision=dsmsgt.DSM_PREC_MIXED, freq_batch=2)
+        want = c.run(freqs)
+        c.close()
+        assert list(g[3]) == list(want[3])
+        for a, b in zip(g[:3], want[:3]):
+            assert rel_l2(a, b) <= 1e-10
 
 
 @pytest.mark.gpu
