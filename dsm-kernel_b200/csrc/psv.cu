@@ -359,14 +359,10 @@ __device__ __forceinline__ void assemble_row(const RowPieces& r, double l2, doub
 // yields pivot 1 and multipliers 0, and rows >= kc are factored exactly as a
 // band that starts at kc (a zero-displacement boundary there).
 __device__ __forceinline__ void cut_row(int j, int kc, cd a[4]) {
-    if (j < kc) {
-        a[0] = a[1] = a[2] = mk(0.0);
-        a[3] = mk(1.0);
-        return;
-    }
+    // selects, no branches: the factorisation's step groups stay one block
 #pragma unroll
-    for (int p = 0; p < 3; ++p)
-        if (j - 3 + p < kc) a[p] = mk(0.0);
+    for (int p = 0; p < 3; ++p) a[p] = (j - 3 + p < kc) ? mk(0.0) : a[p];
+    a[3] = (j < kc) ? mk(1.0) : a[3];
 }
 template <bool FAST>
 __device__ __forceinline__ cd cmulT(cd a, cd b) {
@@ -663,6 +659,17 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
         assemble_row<FAST>(rp, c.l2, c.lsq, an);
         if (kcut) cut_row(k + 4, kc, an);
     };
+    // the same away from the end of the band (row k+4 exists): the row comes
+    // from shared memory or, for a frequency not staged, global memory,
+    // through one generic pointer, so a step group has no branches
+    auto entering_main = [&](int k, cd (&an)[4]) {
+        const int i = (k - 1) % CH, buf = ((k - 1) / CH) & 1;
+        const cd* src = staged ? &sP[buf][staged ? ws : 0][i][0] : c.P + (size_t)(c.it + k + 3) * 12;
+#pragma unroll
+        for (int v = 0; v < 12; ++v) rp.v[v] = src[v];
+        assemble_row<FAST>(rp, c.l2, c.lsq, an);
+        if (kcut) cut_row(k + 4, kc, an);
+    };
     // chunk boundary at k (k - 1 a multiple of CH): the next chunk's copies go out
     auto boundary = [&](int k) {
         if ((k - 1) % CH == 0) {
@@ -687,16 +694,16 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
             continue;
         }
         if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
-            entering(k, an);
+            entering_main(k, an);
             factor_step_main<1, FAST>(k, M, an, c, so);
             keepD(k);
-            entering(k + 1, an);
+            entering_main(k + 1, an);
             factor_step_main<2, FAST>(k + 1, M, an, c, so);
             keepD(k + 1);
-            entering(k + 2, an);
+            entering_main(k + 2, an);
             factor_step_main<3, FAST>(k + 2, M, an, c, so);
             keepD(k + 2);
-            entering(k + 3, an);
+            entering_main(k + 3, an);
             factor_step_main<0, FAST>(k + 3, M, an, c, so);
             keepD(k + 3);
             if ((k + 3) % CH == 0) __syncthreads();  // chunk fully used before its buffer refills
@@ -2054,7 +2061,24 @@ class PsvEngine : public Engine {
         size_t per = lrows * 3 * 16 + (n - ls + 2) * 5 * 16 + (size_t)ncap * NB * 16 + NSLOT * NB * 16;
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
-        nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(65536, (fr / 3) / per));
+        // What the rest of a run allocates later, at the order capacity the
+        // top frequency's first range needs: the field matrices (while they
+        // grow, old and new copies), the split pieces and contraction output
+        // of the mixed path, the batch outputs, and a margin.  The solve
+        // scratch takes what is left, so that a batch's first ranges fit one
+        // launch (one long low-order recurrence per batch, not one per round).
+        size_t lfut = (size_t)Lcap;
+        while (lfut < (size_t)first_span(imax) + 64 && lfut < (size_t)maxlmax + 1 + Lc) lfut *= 2;
+        lfut = std::min(lfut, (size_t)maxlmax + 1 + Lc);
+        size_t rows_all = 0;
+        for (int m = 0; m < 3; ++m) rows_all += (size_t)rows_m[m];
+        size_t pt, pr, ps;
+        out_sizes(&pt, &pr, &ps);
+        const size_t later = rows_all * lfut * (size_t)nsrc * F * afld_bytes * 3 / 2 +
+                             (mixed() ? rows_all * lfut * F * 4 + c_total() * F * 4 : c_total() * 8) +
+                             2 * (pt + pr + ps) * F * nsrc * 8 + ((size_t)4 << 30);
+        const size_t avail = fr > later ? fr - later : 0;
+        nsys_max = (int)std::max<size_t>(1024, std::min<size_t>(131072, avail / per));
         // no more than a round of a batch can launch (F ranges of at most
         // max(4096, the first range of the top frequency)): contexts that
         // share a device leave each other room
@@ -2081,8 +2105,6 @@ class PsvEngine : public Engine {
         Cgemm.reserve(c_total());
         cut.reserve((size_t)nsrc * F);
         amps.reserve((size_t)nsrc * F * Lcap);
-        size_t pt, pr, ps;
-        out_sizes(&pt, &pr, &ps);
         out_t.reserve(2 * pt * F * nsrc);
         out_r.reserve(2 * pr * F * nsrc);
         out_s.reserve(2 * ps * F * nsrc);
