@@ -633,6 +633,7 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             if (tot == 0) break;
             if (maxend > Lcap) grow_orders(maxend);
             wl_off.upload(off, st);
+            wl_host_off = off;
             wl_lb.upload(lb, st);
             WorkList wl{wl_off.p, wl_lb.p, nf};
             solve_chunk(d_freqs.p, nf, wl, tot);

@@ -183,6 +183,7 @@ class Engine {
     double vtop_ = 1.0, rtop_ = 1.0;  // top-zone Vsv sum and radius (callsuf)
     int first_span(int ifreq) const;
     DBuf<int> wl_off, wl_lb;
+    std::vector<int> wl_host_off;    // host copy of the current round's work-list offsets
     virtual void epilogue(const int* freqs_dev, int w, int nf) = 0;
     virtual size_t out_sizes(size_t* nt, size_t* nr, size_t* ns) const = 0;
 

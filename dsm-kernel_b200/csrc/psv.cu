@@ -568,10 +568,13 @@ template <bool FAST, int CH>
 __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
                                                               int nsys, int lmin, cd* __restrict__ Lst,
                                                               SysTail* __restrict__ tail, cd* __restrict__ Dst,
-                                                              int dmin, const int* __restrict__ kcut) {
+                                                              int dmin, const int* __restrict__ kcut,
+                                                              const int* __restrict__ bperm) {
     __shared__ __align__(16) cd sP[2][FAC_NW][CH][12];
     __shared__ int kb_sh;
-    const int sys0 = blockIdx.x * FAC_THREADS;
+    // bperm: blocks of the lowest orders of every frequency (the longest
+    // recurrences) first, so that they start in the first wave
+    const int sys0 = (bperm ? bperm[blockIdx.x] : (int)blockIdx.x) * FAC_THREADS;
     const int sysv = sys0 + threadIdx.x;
     const bool valid = sysv < nsys;
     const int sys = valid ? sysv : nsys - 1;
@@ -819,10 +822,11 @@ __global__ void __launch_bounds__(UP_THREADS, 2) k_psv_up(PsvDev d, int nsys, in
                                                           const int2* __restrict__ caplist,
                                                           const cd* __restrict__ Lst, const cd* __restrict__ Zst,
                                                           const SysTail* __restrict__ tail, cd* __restrict__ Xcap,
-                                                          const int* __restrict__ kcut) {
+                                                          const int* __restrict__ kcut, const int* __restrict__ bperm) {
     extern __shared__ __align__(16) unsigned char up_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int sys = (blockIdx.x * UP_WARPS + warp) * 32 + lane;
+    const int blk = bperm ? bperm[blockIdx.x] : (int)blockIdx.x;  // longest recurrences first
+    const int sys = (blk * UP_WARPS + warp) * 32 + lane;
     // the warp's first factored row (the factorisation's warps are the same
     // 32 systems): rows below it hold no multipliers and no solution
     const int kw = kcut ? ((__reduce_min_sync(0xffffffffu, kcut[min(sys, nsys - 1)]) - 1) & ~3) + 1 : 1;
@@ -1760,6 +1764,8 @@ class PsvEngine : public Engine {
     DBuf<float4> cnodes;
     int cnode_src = 0;
     DBuf<int> kcut;
+    // launch order of the 128-system blocks of a solve round
+    DBuf<int> bperm;
     // one parameter set per source depth (the source fields differ), and
     // the source polynomials they point to
     std::vector<PsvDev> dsrc;
@@ -2168,6 +2174,26 @@ class PsvEngine : public Engine {
         // substitution writes zh of its four bases above its source, and
         // the upward substitution reads the multipliers and zh back and
         // stores six solutions at the captured rows
+        // Block order: by the rank of a block inside its frequency's order
+        // range (a block holding the start of a range ranks 0), then by
+        // position.  A recurrence's length falls with the order (depth
+        // cut-off), so the low-order blocks of every frequency go first.
+        {
+            const int nblk = (nsys + FAC_THREADS - 1) / FAC_THREADS;
+            std::vector<int> rank(nblk), order(nblk);
+            for (int b = 0; b < nblk; ++b) {
+                const int s0 = b * FAC_THREADS, s1 = std::min(nsys, s0 + FAC_THREADS);
+                int r = INT32_MAX;
+                for (int w = 0; w < nf; ++w) {
+                    const int lo = std::max(s0, wl_host_off[w]), hi = std::min(s1, wl_host_off[w + 1]);
+                    if (lo < hi) r = std::min(r, (lo - wl_host_off[w]) / FAC_THREADS);
+                }
+                rank[b] = r;
+                order[b] = b;
+            }
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rank[a] < rank[b]; });
+            bperm.upload(order, st);
+        }
         const int n = d.nn - d.itmp + 1;
         const int lmin = lst_min();
         // Lst holds rows lmin .. n: kernels index rows from 0 off this base
@@ -2185,7 +2211,7 @@ class PsvEngine : public Engine {
             kc = kcut.p;
         }
         auto factor = [&](auto kern) {
-            kern<<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lb, tails.p, Dst.p, dmin, kc);
+            kern<<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lb, tails.p, Dst.p, dmin, kc, bperm.p);
         };
         if (mixed()) {
             if (tune.fac_rows == 8) factor(k_psv_solve<true, 8>);
@@ -2216,10 +2242,10 @@ class PsvEngine : public Engine {
             kbegin(id);
             if (mixed())
                 k_psv_up<true><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
-                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc);
+                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc, bperm.p);
             else
                 k_psv_up<false><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
-                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc);
+                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc, bperm.p);
             kend(id, sub_bytes * nsys, 0.0);
             DSM_LAUNCH(*this);
             id = kid("psv_source_coef");
