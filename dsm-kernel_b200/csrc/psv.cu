@@ -665,14 +665,17 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
     // the same away from the end of the band (row k+4 exists): the row comes
     // from shared memory or, for a frequency not staged, global memory,
     // through one generic pointer, so a step group has no branches
-    auto entering_main = [&](int k, cd (&an)[4]) {
+    // MASK: some lane's cut row is still within reach of the entering row
+    auto entering_main = [&](int k, cd (&an)[4], auto MASK) {
         const int i = (k - 1) % CH, buf = ((k - 1) / CH) & 1;
         const cd* src = staged ? &sP[buf][staged ? ws : 0][i][0] : c.P + (size_t)(c.it + k + 3) * 12;
 #pragma unroll
         for (int v = 0; v < 12; ++v) rp.v[v] = src[v];
         assemble_row<FAST>(rp, c.l2, c.lsq, an);
-        if (kcut) cut_row(k + 4, kc, an);
+        if constexpr (decltype(MASK)::value) cut_row(k + 4, kc, an);
     };
+    // entering rows j need the cut's selects while j < kc + 3 for some lane
+    const int kc_max = __reduce_max_sync(0xffffffffu, kc);
     // chunk boundary at k (k - 1 a multiple of CH): the next chunk's copies go out
     auto boundary = [&](int k) {
         if ((k - 1) % CH == 0) {
@@ -697,18 +700,22 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
             continue;
         }
         if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
-            entering_main(k, an);
-            factor_step_main<1, FAST>(k, M, an, c, so);
-            keepD(k);
-            entering_main(k + 1, an);
-            factor_step_main<2, FAST>(k + 1, M, an, c, so);
-            keepD(k + 1);
-            entering_main(k + 2, an);
-            factor_step_main<3, FAST>(k + 2, M, an, c, so);
-            keepD(k + 2);
-            entering_main(k + 3, an);
-            factor_step_main<0, FAST>(k + 3, M, an, c, so);
-            keepD(k + 3);
+            auto group = [&](auto MASK) {
+                entering_main(k, an, MASK);
+                factor_step_main<1, FAST>(k, M, an, c, so);
+                keepD(k);
+                entering_main(k + 1, an, MASK);
+                factor_step_main<2, FAST>(k + 1, M, an, c, so);
+                keepD(k + 1);
+                entering_main(k + 2, an, MASK);
+                factor_step_main<3, FAST>(k + 2, M, an, c, so);
+                keepD(k + 2);
+                entering_main(k + 3, an, MASK);
+                factor_step_main<0, FAST>(k + 3, M, an, c, so);
+                keepD(k + 3);
+            };
+            if (kcut && k + 4 < kc_max + 3) group(std::true_type{});  // warp-uniform
+            else group(std::false_type{});
             if ((k + 3) % CH == 0) __syncthreads();  // chunk fully used before its buffer refills
             continue;
         }
@@ -1505,9 +1512,12 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
                                                     const cd* __restrict__ Xcap, const cd* __restrict__ co,
                                                     T* __restrict__ A0f, T* __restrict__ A1f, T* __restrict__ A2f,
                                                     int Lcap, double* __restrict__ amps) {
+    // the four warps of a block take the same FS orders at 4 x 32/FS
+    // neighbouring receivers: the coefficient and capture loads of the
+    // orders are shared through L1
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int sys = (blockIdx.x * 4 + warp) * FS + lane % FS;
-    const int r = blockIdx.y * (32 / FS) + lane / FS;
+    const int sys = blockIdx.x * FS + lane % FS;
+    const int r = (blockIdx.y * 4 + warp) * (32 / FS) + lane / FS;
     const int R = d.R;
     if (sys >= nsys || r > R) return;
     int w, l;
@@ -2255,7 +2265,7 @@ class PsvEngine : public Engine {
             kend(id, 0.0, 0.0);
             DSM_LAUNCH(*this);
             const int fs = tune.fld_orders == 16 ? 16 : 32, frec = 32 / fs;
-            dim3 grid((nsys + 4 * fs - 1) / (4 * fs), (R + 1 + frec - 1) / frec);
+            dim3 grid((nsys + fs - 1) / fs, (R + 1 + 4 * frec - 1) / (4 * frec));
             double* amk = amps.p + (size_t)k * F * Lcap;
             id = kid("psv_fields");
             kbegin(id);
