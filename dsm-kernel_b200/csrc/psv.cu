@@ -565,11 +565,12 @@ constexpr int FAC_THREADS = 128;
 constexpr int FAC_NW = 4;   // frequencies staged per block
 
 template <bool FAST, int CH>
-__global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
+__global__ void __launch_bounds__(FAC_THREADS, 2) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
                                                               int nsys, int lmin, cd* __restrict__ Lst,
                                                               SysTail* __restrict__ tail, cd* __restrict__ Dst,
                                                               int dmin, const int* __restrict__ kcut,
-                                                              const int* __restrict__ bperm) {
+                                                              const int* __restrict__ bperm, int lsf,
+                                                              cd* __restrict__ Zst) {
     __shared__ __align__(16) cd sP[2][FAC_NW][CH][12];
     __shared__ int kb_sh;
     // bperm: blocks of the lowest orders of every frequency (the longest
@@ -691,52 +692,124 @@ __global__ void __launch_bounds__(FAC_THREADS, 3) k_psv_solve(PsvDev d, const cd
     auto keepD = [&](int k) {
         if (c.store && k >= c.dmin) c.Dst[(size_t)(k - c.dmin) * c.nsys + c.sys] = so.D;
     };
-    // a cut row never reaches the end of the band (it stays below the
-    // source), so warps wait for their first row in the main branch only
-    for (int k = q0 * CH + 1;; k += 4) {
+    // four main steps (rows k .. k+3, away from the end of the band); fwd
+    // runs after each step (the forward pass below, or nothing)
+    auto group = [&](int k, auto MASK, auto& fwd) {
+        entering_main(k, an, MASK);
+        factor_step_main<1, FAST>(k, M, an, c, so);
+        keepD(k);
+        fwd(k);
+        entering_main(k + 1, an, MASK);
+        factor_step_main<2, FAST>(k + 1, M, an, c, so);
+        keepD(k + 1);
+        fwd(k + 1);
+        entering_main(k + 2, an, MASK);
+        factor_step_main<3, FAST>(k + 2, M, an, c, so);
+        keepD(k + 2);
+        fwd(k + 2);
+        entering_main(k + 3, an, MASK);
+        factor_step_main<0, FAST>(k + 3, M, an, c, so);
+        keepD(k + 3);
+        fwd(k + 3);
+    };
+    auto nofwd = [](int) {};
+    auto masked = [&](int k) { return kcut && k + 4 < kc_max + 3; };  // warp-uniform
+    // Loop A: groups below the forward pass.  A cut row never reaches the
+    // end of the band (it stays below the source), so warps wait for their
+    // first row here only.
+    int k = q0 * CH + 1;
+    for (;; k += 4) {
+        if (k + 3 > n - 4 || (lsf > 3 && k + 6 >= lsf)) break;
         boundary(k);
         if (k < kw) {  // this warp's band starts further up
             if ((k + 3) % CH == 0) __syncthreads();
             continue;
         }
-        if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
-            auto group = [&](auto MASK) {
-                entering_main(k, an, MASK);
-                factor_step_main<1, FAST>(k, M, an, c, so);
-                keepD(k);
-                entering_main(k + 1, an, MASK);
-                factor_step_main<2, FAST>(k + 1, M, an, c, so);
-                keepD(k + 1);
-                entering_main(k + 2, an, MASK);
-                factor_step_main<3, FAST>(k + 2, M, an, c, so);
-                keepD(k + 2);
-                entering_main(k + 3, an, MASK);
-                factor_step_main<0, FAST>(k + 3, M, an, c, so);
-                keepD(k + 3);
-            };
-            if (kcut && k + 4 < kc_max + 3) group(std::true_type{});  // warp-uniform
-            else group(std::false_type{});
-            if ((k + 3) % CH == 0) __syncthreads();  // chunk fully used before its buffer refills
-            continue;
-        }
-        bool last;
-        entering(k, an);
-        last = factor_step<1, FAST>(k, M, an, T, c, so);
-        keepD(k);
-        if (last) { T.Dn = M[1][1]; break; }
-        entering(k + 1, an);
-        last = factor_step<2, FAST>(k + 1, M, an, T, c, so);
-        keepD(k + 1);
-        if (last) { T.Dn = M[2][2]; break; }
-        entering(k + 2, an);
-        last = factor_step<3, FAST>(k + 2, M, an, T, c, so);
-        keepD(k + 2);
-        if (last) { T.Dn = M[3][3]; break; }
-        entering(k + 3, an);
-        last = factor_step<0, FAST>(k + 3, M, an, T, c, so);
-        keepD(k + 3);
-        if (last) { T.Dn = M[0][0]; break; }
+        if (masked(k)) group(k, std::true_type{}, nofwd);
+        else group(k, std::false_type{}, nofwd);
         if ((k + 3) % CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+    }
+    // Loop B: the rest, with the forward substitution of one source's four
+    // bases (lsf > 3: its first source row; k_psv_fwd's operations, in the
+    // same order) riding along: row k takes the pivot of step k and the
+    // multipliers L(k,k-1), L(k,k-2), L(k,k-3) of the three steps before, so
+    // from three steps below the source those are kept: h0 = w0 of the last
+    // step, h1a/h1b = w1 of the last two, h2a/h2b/h2c = w2 of the last
+    // three.  Its state lives in this loop only.
+    {
+        cd fz[4][3], h0 = mk(0.0), h1a = mk(0.0), h1b = mk(0.0), h2a = mk(0.0), h2b = mk(0.0), h2c = mk(0.0);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) fz[b][0] = fz[b][1] = fz[b][2] = mk(0.0);
+        auto fwd_step = [&](int k) {
+            if (k >= lsf) {
+                const cd D = so.D, l1 = h0, l2 = h1b, l3 = h2c;
+                cd rcp = mk(0.0);
+                if (FAST) rcp = crecipT<true>(D);
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const cd rhs = mk(lsf + b == k ? 1.0 : 0.0);
+                    const cd z0 = fz[b][0], z1 = fz[b][1], z2 = fz[b][2];
+                    cd zc;
+                    if (FAST) {
+                        cd sum = cmulT<true>(l3, z0);
+                        sum = caddmulT<true>(sum, l2, z1);
+                        sum = caddmulT<true>(sum, l1, z2);
+                        zc = rhs - sum;
+                    } else {
+                        cd sum = mk(0.0) + l3 * z0 + l2 * z1 + l1 * z2;
+                        zc = rhs - sum;
+                    }
+                    if (c.store)
+                        Zst[((size_t)(k - lsf) * 4 + b) * nsys + sys] = FAST ? cmulT<true>(zc, rcp) : zc / D;
+                    fz[b][0] = z1;
+                    fz[b][1] = z2;
+                    fz[b][2] = zc;
+                }
+            }
+            h2c = h2b;
+            h2b = h2a;
+            h2a = so.w2;
+            h1b = h1a;
+            h1a = so.w1;
+            h0 = so.w0;
+        };
+        const bool fw = lsf > 3;
+        for (;; k += 4) {
+            boundary(k);
+            if (k < kw) {
+                if ((k + 3) % CH == 0) __syncthreads();
+                continue;
+            }
+            if (k + 3 <= n - 4) {  // four steps away from the end of the band (same n block-wide)
+                if (fw) group(k, std::false_type{}, fwd_step);  // the cut lies eight rows below the source
+                else if (masked(k)) group(k, std::true_type{}, nofwd);
+                else group(k, std::false_type{}, nofwd);
+                if ((k + 3) % CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+                continue;
+            }
+            bool last;
+            entering(k, an);
+            last = factor_step<1, FAST>(k, M, an, T, c, so);
+            keepD(k);
+            if (fw) fwd_step(k);
+            if (last) { T.Dn = M[1][1]; break; }
+            entering(k + 1, an);
+            last = factor_step<2, FAST>(k + 1, M, an, T, c, so);
+            keepD(k + 1);
+            if (fw) fwd_step(k + 1);
+            if (last) { T.Dn = M[2][2]; break; }
+            entering(k + 2, an);
+            last = factor_step<3, FAST>(k + 2, M, an, T, c, so);
+            keepD(k + 2);
+            if (fw) fwd_step(k + 2);
+            if (last) { T.Dn = M[3][3]; break; }
+            entering(k + 3, an);
+            last = factor_step<0, FAST>(k + 3, M, an, T, c, so);
+            keepD(k + 3);
+            if (fw) fwd_step(k + 3);
+            if (last) { T.Dn = M[0][0]; break; }
+            if ((k + 3) % CH == 0) __syncthreads();  // chunk fully used before its buffer refills
+        }
     }
     cp_async_wait<0>();  // no copy outlives the block
     if (valid) {
@@ -829,7 +902,8 @@ __global__ void __launch_bounds__(UP_THREADS, 2) k_psv_up(PsvDev d, int nsys, in
                                                           const int2* __restrict__ caplist,
                                                           const cd* __restrict__ Lst, const cd* __restrict__ Zst,
                                                           const SysTail* __restrict__ tail, cd* __restrict__ Xcap,
-                                                          const int* __restrict__ kcut, const int* __restrict__ bperm) {
+                                                          const int* __restrict__ kcut, const int* __restrict__ bperm,
+                                                          cd* __restrict__ Xprobe) {
     extern __shared__ __align__(16) unsigned char up_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int blk = bperm ? bperm[blockIdx.x] : (int)blockIdx.x;  // longest recurrences first
@@ -841,7 +915,12 @@ __global__ void __launch_bounds__(UP_THREADS, 2) k_psv_up(PsvDev d, int nsys, in
     jmin_loc = max(jmin_loc, kw);
     cd* ring = reinterpret_cast<cd*>(up_smem) + (size_t)warp * UP_WARP_CD + lane;
     const int it = d.itmp, n = d.nn - it + 1, ls = d.jsrc - it + 1;
-    auto store = [&](int c, int b, cd v) { Xcap[((size_t)c * NB + b) * nsys + sys] = v; };
+    // captured values; the cutoff probe's two rows also go to Xprobe (the
+    // amplitude test is formed by k_psv_coef)
+    auto store = [&](int c, int b, cd v) {
+        Xcap[((size_t)c * NB + b) * nsys + sys] = v;
+        if (b < 4 && (c == d.cap_p0 || c == d.cap_p1)) Xprobe[((size_t)(c == d.cap_p0 ? 0 : 1) * 4 + b) * nsys + sys] = v;
+    };
     cd x[NB][3];  // x(j+1), x(j+2), x(j+3) of each basis
     {
         const SysTail tl = tail[sys];
@@ -1428,20 +1507,36 @@ __global__ void k_psv_abnum(PsvDev d, const int* __restrict__ freqs, int nf, cd*
 // Per (omega, l >= 1): weights of the six basis solutions for every slot
 // (calya + calg for the 13 forward sources, caldveczero for the back ones).
 // Layout co[(slot * NB + b) * nsys + sys].
+// The cutoff probe of the system (calamp on
+// g0(ksta(r_n)-1), g0(ksta(r_n)) of imt = 1, m = 0) is formed here from the
+// FP64 slot-0 coefficients and the FP64 probe captures, in every mode.
 __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restrict__ freqs, WorkList wl,
                                                   int nsys, const cd* __restrict__ ab,
-                                                  cd* __restrict__ co, int back) {
+                                                  cd* __restrict__ co, int back,
+                                                  const cd* __restrict__ Xprobe, double* __restrict__ amps,
+                                                  int Lcap) {
     int sys = blockIdx.x * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
     int w, l;
     wl_map(wl, sys, w, l);
     auto put = [&](int slot, const cd* g) {
         for (int b = 0; b < NB; ++b) co[((size_t)slot * NB + b) * nsys + sys] = g[b];
+        if (slot == 0) {
+            cd p0 = mk(0.0), p1 = mk(0.0);
+            for (int b = 0; b < 4; ++b) {
+                const cd cb = g[b];
+                p0 = p0 + cb * Xprobe[(size_t)b * nsys + sys];
+                p1 = p1 + cb * Xprobe[(size_t)(4 + b) * nsys + sys];
+            }
+            const double a1 = cabs_(p0), a2 = cabs_(p1);
+            amps[(size_t)w * Lcap + l] = sqrt(a1 * a1 + a2 * a2);
+        }
     };
     cd g[NB];
     for (int b = 0; b < NB; ++b) g[b] = mk(0.0);
-    if (l == 0) {
-        for (int s = 0; s < NSLOT; ++s) put(s, g);
+    if (l == 0) {  // the order-0 kernels write this order's fields and probe
+        for (int s = 0; s < NSLOT; ++s)
+            for (int b = 0; b < NB; ++b) co[((size_t)s * NB + b) * nsys + sys] = g[b];
         return;
     }
     const double omega = 2.0 * kPi * (double)freqs[w] / d.tlen;
@@ -1498,20 +1593,52 @@ __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restric
 // FS systems x 32/FS receivers per warp: 32 (default) or 16, chosen per
 // context (dsm_set_tuning / dsm_autotune)
 
-// acc + r x for a real r: FAST with fused multiply-adds
+
+// Arithmetic of the field kernel: the reference's operations on the plain
+// path, fused multiply-adds and one reciprocal of sqrt(l(l+1)) on the mixed
+// path (whose rows are stored in FP32), both in FP64.  Measured on the
+// 2048-frequency grid, FP32 slot combinations (FP64 interpolation) raised the
+// mixed path's error to 9e-7 and FP32 interpolation to 5e-6: the derivative
+// weights difference neighbouring nodes and the bases cancel.
 template <bool FAST>
-__device__ __forceinline__ cd caddmulR(cd acc, double r, cd x) {
-    if (FAST) return mk(fma(r, x.re, acc.re), fma(r, x.im, acc.im));
-    return acc + r * x;
+struct FieldMath {
+    using V = cd;
+    using R = double;
+    __device__ static V coef(const cd* p, size_t i) { return p[i]; }
+    __device__ static V from(cd v) { return v; }
+    __device__ static V zero() { return mk(0.0); }
+    __device__ static cd interp(cd acc, double r, cd x) {  // acc + r x
+        if (FAST) return mk(fma(r, x.re, acc.re), fma(r, x.im, acc.im));
+        return acc + r * x;
+    }
+    __device__ static V addmul(V acc, V a, V b) { return caddmulT<FAST>(acc, a, b); }  // acc + a b
+    __device__ static V divl(V v, R lsq, R ilsq) { return FAST ? v * ilsq : v / lsq; }
+};
+template <class T, class V>
+__device__ __forceinline__ void put_fieldv(T* Aw, int Lcap, int nq, const PsvDev& d, int rr, int q, int f, V v) {
+    int im;
+    const long long row = psvk::fld_row(nq, d.Rs1, d.Rf, q, f, rr, &im);
+    if (row < 0) return;
+    Aw[(size_t)row * Lcap] = (T)v.re;
+    Aw[((size_t)row + im) * Lcap] = (T)v.im;
 }
 
-// FAST (mixed path, FP32 field storage): fused multiply-adds and one
-// reciprocal of sqrt(l(l+1)); otherwise the reference's operations.
-template <class T, bool FAST, int FS>
+// Field rows of every (order, receiver): 3-node interpolation of the
+// captured solutions (value and radial derivative), combined with the
+// source coefficients of each slot (calup*, locallyCartesianDerivatives
+// inputs); fluid receivers store U only.  The cutoff probe is formed by
+// k_psv_coef.
+template <bool MIXED, int FS>
 __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int nsys,
                                                     const cd* __restrict__ Xcap, const cd* __restrict__ co,
-                                                    T* __restrict__ A0f, T* __restrict__ A1f, T* __restrict__ A2f,
-                                                    int Lcap, double* __restrict__ amps) {
+                                                    typename std::conditional<MIXED, float, double>::type* __restrict__ A0f,
+                                                    typename std::conditional<MIXED, float, double>::type* __restrict__ A1f,
+                                                    typename std::conditional<MIXED, float, double>::type* __restrict__ A2f,
+                                                    int Lcap) {
+    using T = typename std::conditional<MIXED, float, double>::type;
+    using FM = FieldMath<MIXED>;
+    using V = typename FM::V;
+    using RT = typename FM::R;
     // the four warps of a block take the same FS orders at 4 x 32/FS
     // neighbouring receivers: the coefficient and capture loads of the
     // orders are shared through L1
@@ -1527,91 +1654,68 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
                             psvk::fld_rows(NS2, d.Rs1, d.Rf)};
     const int rr = d.rrow[r];
     T* Aw[3] = {A0f + (size_t)w * rows[0] * Lcap + l, A1f + (size_t)w * rows[1] * Lcap + l,
-                     A2f + (size_t)w * rows[2] * Lcap + l};
-    const double l2 = (double)l * (double)(l + 1), lsq = sqrt(l2), ilsq = FAST ? 1.0 / lsq : 0.0;
+                A2f + (size_t)w * rows[2] * Lcap + l};
+    const double l2d = (double)l * (double)(l + 1), lsqd = sqrt(l2d);
+    const RT l2 = (RT)l2d, lsq = (RT)lsqd, ilsq = (RT)(1.0 / lsqd);
     auto X = [&](int cap, int b) { return Xcap[((size_t)cap * NB + b) * nsys + sys]; };
-    auto C = [&](int s, int b) { return co[((size_t)s * NB + b) * nsys + sys]; };
-    if (r == 0) {  // probe: calamp on g0(ksta(r_n)-1), g0(ksta(r_n)) of imt = 1, m = 0
-        cd p0 = mk(0.0), p1 = mk(0.0);
-        for (int b = 0; b < 4; ++b) {
-            cd cb = C(0, b);
-            p0 = p0 + cb * X(d.cap_p0, b);
-            p1 = p1 + cb * X(d.cap_p1, b);
-        }
-        double a1 = cabs_(p0), a2 = cabs_(p1);
-        amps[(size_t)w * Lcap + l] = sqrt(a1 * a1 + a2 * a2);
-    }
+    auto C = [&](int s, int b) { return FM::coef(co, ((size_t)s * NB + b) * nsys + sys); };
     if (rr < 0) {  // fluid receiver: only U is stored
-        cd bU[NB];
-        for (int b = 0; b < NB; ++b) bU[b] = mk(0.0);
-        for (int i = 0; i < 3; ++i) {
-            const double wvi = d.wv[3 * r + i];
-            const int cu = d.rcap[6 * r + 2 * i];
-            for (int b = 0; b < NB; ++b) bU[b] = caddmulR<FAST>(bU[b], wvi, X(cu, b));
+        V bU[NB];
+        for (int b = 0; b < NB; ++b) {
+            cd u = mk(0.0);
+            for (int i = 0; i < 3; ++i) u = FM::interp(u, d.wv[3 * r + i], X(d.rcap[6 * r + 2 * i], b));
+            bU[b] = FM::from(u);
         }
         for (int s = 0; s < NSLOT; ++s) {
             const int mi = slot_mi(s), q = slot_q(s);
-            cd U = mk(0.0);
-            for (int b = 0; b < NB; ++b) {
-                if (FAST) U = caddmulT<true>(U, C(s, b), bU[b]);
-                else U = U + C(s, b) * bU[b];
-            }
-            put_field(Aw[mi], Lcap, mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2), d, rr, q, 0, U);
+            V U = FM::zero();
+            for (int b = 0; b < NB; ++b) U = FM::addmul(U, C(s, b), bU[b]);
+            put_fieldv<T>(Aw[mi], Lcap, mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2), d, rr, q, 0, U);
         }
         return;
     }
     const bool surf = r == R;
-    cd bU[NB], bV[NB], bUd[NB], bVd[NB];
-    for (int b = 0; b < NB; ++b) bU[b] = bV[b] = bUd[b] = bVd[b] = mk(0.0);
-    if (surf) {
-        for (int b = 0; b < NB; ++b) { bU[b] = X(d.cap_n1, b); bV[b] = X(d.cap_n, b); }
-    } else {
-        for (int i = 0; i < 3; ++i) {
-            double wvi = d.wv[3 * r + i], wdi = d.wd[3 * r + i];
-            int cu = d.rcap[6 * r + 2 * i], cvv = d.rcap[6 * r + 2 * i + 1];
-            for (int b = 0; b < NB; ++b) {
-                cd xu = X(cu, b), xv = X(cvv, b);
-                bU[b] = caddmulR<FAST>(bU[b], wvi, xu);
-                bV[b] = caddmulR<FAST>(bV[b], wvi, xv);
-                bUd[b] = caddmulR<FAST>(bUd[b], wdi, xu);
-                bVd[b] = caddmulR<FAST>(bVd[b], wdi, xv);
+    V bU[NB], bV[NB], bUd[NB], bVd[NB];
+    for (int b = 0; b < NB; ++b) {
+        cd u = mk(0.0), v = mk(0.0), ud = mk(0.0), vd = mk(0.0);
+        if (surf) {
+            u = X(d.cap_n1, b);
+            v = X(d.cap_n, b);
+        } else {
+            for (int i = 0; i < 3; ++i) {
+                const double wvi = d.wv[3 * r + i], wdi = d.wd[3 * r + i];
+                const cd xu = X(d.rcap[6 * r + 2 * i], b), xv = X(d.rcap[6 * r + 2 * i + 1], b);
+                u = FM::interp(u, wvi, xu);
+                v = FM::interp(v, wvi, xv);
+                ud = FM::interp(ud, wdi, xu);
+                vd = FM::interp(vd, wdi, xv);
             }
         }
+        bU[b] = FM::from(u);
+        bV[b] = FM::from(v);
+        bUd[b] = FM::from(ud);
+        bVd[b] = FM::from(vd);
     }
     for (int s = 0; s < NSLOT; ++s) {
-        int mi = slot_mi(s), q = slot_q(s);
-        bool isback = (s == 3) || (mi == 1 && (q % 4) >= 2);
-        cd U = mk(0.0), V = mk(0.0), Ud = mk(0.0), Vd = mk(0.0);
+        const int mi = slot_mi(s), q = slot_q(s);
+        const bool isback = (s == 3) || (mi == 1 && (q % 4) >= 2);
+        V U = FM::zero(), Vv = FM::zero(), Ud = FM::zero(), Vd = FM::zero();
         if (!(surf && isback)) {
             for (int b = 0; b < NB; ++b) {
-                cd cb = C(s, b);
-                if (FAST) {
-                    U = caddmulT<true>(U, cb, bU[b]);
-                    V = caddmulT<true>(V, cb, bV[b]);
-                    Ud = caddmulT<true>(Ud, cb, bUd[b]);
-                    Vd = caddmulT<true>(Vd, cb, bVd[b]);
-                } else {
-                    U = U + cb * bU[b];
-                    V = V + cb * bV[b];
-                    Ud = Ud + cb * bUd[b];
-                    Vd = Vd + cb * bVd[b];
-                }
+                const V cb = C(s, b);
+                U = FM::addmul(U, cb, bU[b]);
+                Vv = FM::addmul(Vv, cb, bV[b]);
+                Ud = FM::addmul(Ud, cb, bUd[b]);
+                Vd = FM::addmul(Vd, cb, bVd[b]);
             }
         }
-        cd Vh, Vdh;
-        if (FAST) {
-            Vh = V * ilsq;
-            Vdh = Vd * ilsq;
-        } else {
-            Vh = V / lsq;
-            Vdh = Vd / lsq;
-        }
+        const V Vh = FM::divl(Vv, lsq, ilsq), Vdh = FM::divl(Vd, lsq, ilsq);
         const int nqm = mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2);
-        put_field(Aw[mi], Lcap, nqm, d, rr, q, 0, U);
-        put_field(Aw[mi], Lcap, nqm, d, rr, q, 1, Ud);
-        put_field(Aw[mi], Lcap, nqm, d, rr, q, 2, Vh);
-        put_field(Aw[mi], Lcap, nqm, d, rr, q, 3, Vdh);
-        put_field(Aw[mi], Lcap, nqm, d, rr, q, 4, l2 * Vh);
+        put_fieldv<T>(Aw[mi], Lcap, nqm, d, rr, q, 0, U);
+        put_fieldv<T>(Aw[mi], Lcap, nqm, d, rr, q, 1, Ud);
+        put_fieldv<T>(Aw[mi], Lcap, nqm, d, rr, q, 2, Vh);
+        put_fieldv<T>(Aw[mi], Lcap, nqm, d, rr, q, 3, Vdh);
+        put_fieldv<T>(Aw[mi], Lcap, nqm, d, rr, q, 4, l2 * Vh);
     }
 }
 
@@ -1765,7 +1869,7 @@ class PsvEngine : public Engine {
         capmap, l0col, l0e1;
     DBuf<int2> caplist;
     DBuf<double> qmu, qkappa, sel, fel, hm, bcval, poly, lam, qkp, fr, r, rrsta;
-    DBuf<cd> B0, B1, B2, Prow, Lst, Zst, Dst, Xcap, l0scr, l0d, ab, co;
+    DBuf<cd> B0, B1, B2, Prow, Lst, Zst, Dst, Xcap, Xprobe, l0scr, l0d, ab, co;
     DBuf<int4> rowasm;
     DBuf<SysTail> tails;
     int jmin_loc = 1, ncap = 0;
@@ -2111,6 +2215,7 @@ class PsvEngine : public Engine {
         Zst.reserve((n - ls + 2) * 4 * nsys);
         Dst.reserve((n - ls + 2) * nsys);
         Xcap.reserve((size_t)ncap * NB * nsys);
+        Xprobe.reserve((size_t)8 * nsys);
         tails.reserve(nsys);
         kcut.reserve(nsys);
         l0scr.reserve((size_t)F * (d.nn0 + 1) * 2);
@@ -2220,8 +2325,13 @@ class PsvEngine : public Engine {
             DSM_LAUNCH(*this);
             kc = kcut.p;
         }
+        // source 0's forward pass rides along the factorisation (its first
+        // source row must lie above the band's first rows)
+        const int ls0 = dsrc[0].jsrc - dsrc[0].itmp + 1;
+        const int lsf = ls0 > 3 && ls0 + 8 <= n ? ls0 : -1;
         auto factor = [&](auto kern) {
-            kern<<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lb, tails.p, Dst.p, dmin, kc, bperm.p);
+            kern<<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lb, tails.p, Dst.p, dmin, kc, bperm.p,
+                                                lsf, Zst.p);
         };
         if (mixed()) {
             if (tune.fac_rows == 8) factor(k_psv_solve<true, 8>);
@@ -2242,7 +2352,9 @@ class PsvEngine : public Engine {
             sub_tot += fwd_bytes + sub_bytes;
             id = kid("psv_forward");
             kbegin(id);
-            if (mixed())
+            if (k == 0 && lsf > 0) {
+                // done by the factorisation
+            } else if (mixed())
                 k_psv_fwd<true><<<fgrid, FAC_THREADS, 0, st>>>(e, nsys, ls, Lb, Dst.p, dmin, tails.p, Zst.p);
             else
                 k_psv_fwd<false><<<fgrid, FAC_THREADS, 0, st>>>(e, nsys, ls, Lb, Dst.p, dmin, tails.p, Zst.p);
@@ -2252,31 +2364,31 @@ class PsvEngine : public Engine {
             kbegin(id);
             if (mixed())
                 k_psv_up<true><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
-                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc, bperm.p);
+                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc, bperm.p, Xprobe.p);
             else
                 k_psv_up<false><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
-                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc, bperm.p);
+                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc, bperm.p, Xprobe.p);
             kend(id, sub_bytes * nsys, 0.0);
             DSM_LAUNCH(*this);
             id = kid("psv_source_coef");
             kbegin(id);
+            double* amk = amps.p + (size_t)k * F * Lcap;
             k_psv_coef<<<(nsys + 127) / 128, 128, 0, st>>>(e, fr_, wl, nsys, ab.p + (size_t)k * F * 320, co.p,
-                                                            rsgt_sw);
+                                                            rsgt_sw, Xprobe.p, amk, Lcap);
             kend(id, 0.0, 0.0);
             DSM_LAUNCH(*this);
             const int fs = tune.fld_orders == 16 ? 16 : 32, frec = 32 / fs;
             dim3 grid((nsys + fs - 1) / fs, (R + 1 + 4 * frec - 1) / (4 * frec));
-            double* amk = amps.p + (size_t)k * F * Lcap;
             id = kid("psv_fields");
             kbegin(id);
             if (afld_bytes == 4) {
-                auto kern = fs == 16 ? k_psv_fields<float, true, 16> : k_psv_fields<float, true, 32>;
+                auto kern = fs == 16 ? k_psv_fields<true, 16> : k_psv_fields<true, 32>;
                 kern<<<grid, 128, 0, st>>>(e, wl, nsys, Xcap.p, co.p, afld_of<float>(0, k), afld_of<float>(1, k),
-                                           afld_of<float>(2, k), Lcap, amk);
+                                           afld_of<float>(2, k), Lcap);
             } else {
-                auto kern = fs == 16 ? k_psv_fields<double, false, 16> : k_psv_fields<double, false, 32>;
+                auto kern = fs == 16 ? k_psv_fields<false, 16> : k_psv_fields<false, 32>;
                 kern<<<grid, 128, 0, st>>>(e, wl, nsys, Xcap.p, co.p, afld_of<double>(0, k), afld_of<double>(1, k),
-                                           afld_of<double>(2, k), Lcap, amk);
+                                           afld_of<double>(2, k), Lcap);
             }
             kend(id, 0.0, 0.0);
             DSM_LAUNCH(*this);
