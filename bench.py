@@ -581,6 +581,8 @@ def main():
     ap.add_argument("--no-lmax", dest="lmax", action="store_false", help="plain first order ranges")
     ap.add_argument("--per-step", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="default tile shapes instead of the library's tuner")
     args = ap.parse_args()
     if args.mode == "catalogue":
         catalogue_bench(args)
@@ -634,6 +636,11 @@ def main():
                              use_lmax_predictor=1 if use_lmax else 0)
         if use_lmax:
             ctx.set_lmax_model(lmax_params)
+        # tile shapes chosen by the library's tuner on a step outside the
+        # timed ones (untimed), for each precision mode alike
+        tuning = None
+        if args.autotune:
+            tuning, _ = ctx.autotune(step_freqs(2000, args.per_step, imax, rank, world), reps=1)
         for w in range(args.warmup):  # untimed
             ctx.run_device(step_freqs(1000 + w, args.per_step, imax, rank, world))
         ctx.set_profiling(True)
@@ -677,7 +684,7 @@ def main():
         barrier()
         ctx.close()
         slices = args.steps * args.per_step * world
-        return {"value": slices / t_dev, "t": t_dev, "kstats": kstats, "launches": launches,
+        return {"value": slices / t_dev, "t": t_dev, "kstats": kstats, "launches": launches, "tuning": tuning,
                 "llogs": llogs, "clocks": clk, "solve": sol,
                 "e2e": {"value": slices / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * F,
                         "d2h_bytes_per_step": 8 * (per_t + per_r + per_s) * F + 4 * F,
@@ -777,7 +784,7 @@ def main():
                                depth_cutoff=(1e-20 if mixed and mode == "psv" else 0.0),
                                parallelism=f"dp{world} (frequencies per rank)",
                                l2="inputs larger than L2 (field matrices of several GB per step)"),
-                "e2e": run["e2e"], "gpu_launches": int(run["launches"]),
+                "e2e": run["e2e"], "gpu_launches": int(run["launches"]), "tuning": run["tuning"],
                 "roofline": roof, "hbm_kernels": hbm, "kernel_share": share,
                 "cpu_baseline": cpu, "clocks": run["clocks"],
                 "solve": dict(sol, slices=args.steps * args.per_step,
@@ -786,6 +793,7 @@ def main():
                 "llog_first_step": run["llogs"][0]}
         if plain:
             line["fp64"] = {"value": plain["value"], "ms_per_step": 1e3 * plain["t"] / args.steps,
+                            "tuning": plain["tuning"],
                             "e2e": plain["e2e"]["value"], "solve": plain["solve"], "clocks": plain["clocks"],
                             "kernel_share": {k: round(v[0] / max(plain["t"] * 1e3, 1e-9), 4)
                                              for k, v in plain["kstats"].items()}}

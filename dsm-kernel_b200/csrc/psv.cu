@@ -827,8 +827,9 @@ __global__ void __launch_bounds__(FAC_THREADS, 2) k_psv_solve(PsvDev d, const cd
 template <bool FAST>
 __global__ void __launch_bounds__(128) k_psv_fwd(PsvDev d, int nsys, int ls, const cd* __restrict__ Lst,
                                                  const cd* __restrict__ Dst, int dmin,
-                                                 const SysTail* __restrict__ tail, cd* __restrict__ Zst) {
-    const int sys = blockIdx.x * blockDim.x + threadIdx.x;
+                                                 const SysTail* __restrict__ tail, cd* __restrict__ Zst,
+                                                 const int* __restrict__ bperm) {
+    const int sys = (bperm ? bperm[blockIdx.x] : (int)blockIdx.x) * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
     const int n = d.nn - d.itmp + 1;
     const cd a22raw = tail[sys].a22raw;
@@ -1514,8 +1515,8 @@ __global__ void __launch_bounds__(128) k_psv_coef(PsvDev d, const int* __restric
                                                   int nsys, const cd* __restrict__ ab,
                                                   cd* __restrict__ co, int back,
                                                   const cd* __restrict__ Xprobe, double* __restrict__ amps,
-                                                  int Lcap) {
-    int sys = blockIdx.x * blockDim.x + threadIdx.x;
+                                                  int Lcap, const int* __restrict__ bperm) {
+    int sys = (bperm ? bperm[blockIdx.x] : (int)blockIdx.x) * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
     int w, l;
     wl_map(wl, sys, w, l);
@@ -1634,7 +1635,7 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
                                                     typename std::conditional<MIXED, float, double>::type* __restrict__ A0f,
                                                     typename std::conditional<MIXED, float, double>::type* __restrict__ A1f,
                                                     typename std::conditional<MIXED, float, double>::type* __restrict__ A2f,
-                                                    int Lcap) {
+                                                    int Lcap, const int* __restrict__ bperm) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using FM = FieldMath<MIXED>;
     using V = typename FM::V;
@@ -1643,7 +1644,9 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
     // neighbouring receivers: the coefficient and capture loads of the
     // orders are shared through L1
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int sys = blockIdx.x * FS + lane % FS;
+    constexpr int GPB = 128 / FS;  // order groups per 128-system block (bperm's unit)
+    const int sb = bperm ? bperm[blockIdx.x / GPB] : (int)(blockIdx.x / GPB);
+    const int sys = sb * 128 + (blockIdx.x % GPB) * FS + lane % FS;
     const int r = (blockIdx.y * 4 + warp) * (32 / FS) + lane / FS;
     const int R = d.R;
     if (sys >= nsys || r > R) return;
@@ -1836,7 +1839,8 @@ __global__ void k_psv_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ra
 // row of the node's first unknown.  kcut = that row less a margin of four,
 // at most kmax (below the source rows).
 __global__ void k_psv_cutrow(const float4* __restrict__ nodes, int ks, float X, double tlen,
-                             const int* __restrict__ freqs, WorkList wl, int nsys, int kmax, int* __restrict__ kcut) {
+                             const int* __restrict__ freqs, WorkList wl, int nsys, int kmax, int* __restrict__ kcut,
+                             int* __restrict__ blkmin) {
     const int sys = blockIdx.x * blockDim.x + threadIdx.x;
     if (sys >= nsys) return;
     int w, l;
@@ -1858,7 +1862,9 @@ __global__ void k_psv_cutrow(const float4* __restrict__ nodes, int ks, float X, 
         a = b;
         ka = kb;
     }
-    kcut[sys] = max(1, min(row - 4, kmax));
+    const int kc = max(1, min(row - 4, kmax));
+    kcut[sys] = kc;
+    atomicMin(&blkmin[sys / 128], kc);  // per 128-system block (a factorisation block)
 }
 
 // ---------------------------------------------------------------- engine
@@ -1878,8 +1884,11 @@ class PsvEngine : public Engine {
     DBuf<float4> cnodes;
     int cnode_src = 0;
     DBuf<int> kcut;
-    // launch order of the 128-system blocks of a solve round
-    DBuf<int> bperm;
+    // launch order of the 128-system blocks of a solve round, the lowest
+    // cut row per block, and the stream of the long recurrences
+    DBuf<int> bperm, blkmin;
+    cudaStream_t st3 = nullptr;
+    cudaEvent_t ev_s3a = nullptr, ev_s3b = nullptr;
     // one parameter set per source depth (the source fields differ), and
     // the source polynomials they point to
     std::vector<PsvDev> dsrc;
@@ -1901,6 +1910,13 @@ class PsvEngine : public Engine {
         mode = 1;
         opt = *o;
         init_common(opt.device);
+        {  // the long recurrences' stream: its blocks go first when SMs free up
+            int lo = 0, hi = 0;
+            DSM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            DSM_CUDA(cudaStreamCreateWithPriority(&st3, cudaStreamNonBlocking, hi));
+            DSM_CUDA(cudaEventCreateWithFlags(&ev_s3a, cudaEventDisableTiming));
+            DSM_CUDA(cudaEventCreateWithFlags(&ev_s3b, cudaEventDisableTiming));
+        }
         // the mixed path splits the fields into 11-bit pieces: FP32 storage
         // (24 bits) loses nothing it keeps and halves their traffic
         afld_bytes = mixed() ? 4 : 8;
@@ -2142,6 +2158,15 @@ class PsvEngine : public Engine {
         DSM_CUDA(cudaStreamSynchronize(st));
     }
 
+    ~PsvEngine() override {
+        if (st3) {
+            cudaStreamSynchronize(st3);
+            cudaStreamDestroy(st3);
+        }
+        if (ev_s3a) cudaEventDestroy(ev_s3a);
+        if (ev_s3b) cudaEventDestroy(ev_s3b);
+    }
+
     // every source of a context shares the model, grid, receivers and
     // distances; only the source fields may differ
     static void check_same_grid(const dsm_psv_setup_t* a, const dsm_psv_setup_t* b) {
@@ -2289,13 +2314,42 @@ class PsvEngine : public Engine {
         // substitution writes zh of its four bases above its source, and
         // the upward substitution reads the multipliers and zh back and
         // stores six solutions at the captured rows
-        // Block order: by the rank of a block inside its frequency's order
-        // range (a block holding the start of a range ranks 0), then by
-        // position.  A recurrence's length falls with the order (depth
-        // cut-off), so the low-order blocks of every frequency go first.
-        {
-            const int nblk = (nsys + FAC_THREADS - 1) / FAC_THREADS;
-            std::vector<int> rank(nblk), order(nblk);
+        const int n = d.nn - d.itmp + 1;
+        const int lmin = lst_min();
+        // Lst holds rows lmin .. n: kernels index rows from 0 off this base
+        cd* const Lb = Lst.p - (size_t)lmin * 3 * nsys;
+        const double fac_bytes = (double)(n - lmin + 1) * 3 * 16.0 + (double)(n - ls_min + 1) * 16.0;
+        const int nblk = (nsys + FAC_THREADS - 1) / FAC_THREADS;
+        const int dmin = ls_min;  // pivots from the deepest source row up
+        const int* kc = nullptr;
+        // Block order and split.  With the depth cut, each 128-system block's
+        // lowest first row comes back to the host: blocks go longest
+        // recurrence first, and those whose recurrence spans more than 60 %
+        // of the band run their whole solve chain (factorisation,
+        // substitutions, coefficients, fields) on a second stream beside the
+        // rest, so the short systems' substitutions and fields overlap the
+        // long factorisations.  Without the cut every recurrence is the
+        // whole band: blocks go by their rank inside their frequency's order
+        // range, one stream.
+        std::vector<int> order(nblk);
+        int nlong = 0;
+        if (depth_bound > 0.0 && ls_min > 9) {
+            blkmin.reserve(nblk);
+            DSM_CUDA(cudaMemsetAsync(blkmin.p, 0x7f, sizeof(int) * nblk, st));
+            k_psv_cutrow<<<(nsys + 127) / 128, 128, 0, st>>>(cnodes.p, cnode_src, (float)-std::log(depth_bound),
+                                                             d.tlen, fr_, wl, nsys, ls_min - 8, kcut.p, blkmin.p);
+            DSM_LAUNCH(*this);
+            kc = kcut.p;
+            std::vector<int> bm(nblk);
+            DSM_CUDA(cudaMemcpyAsync(bm.data(), blkmin.p, sizeof(int) * nblk, cudaMemcpyDeviceToHost, st));
+            DSM_CUDA(cudaStreamSynchronize(st));
+            for (int b = 0; b < nblk; ++b) order[b] = b;
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return bm[a] < bm[b]; });
+            const int lim = (int)(0.4 * n);
+            for (int b = 0; b < nblk; ++b) nlong += bm[b] < lim ? 1 : 0;
+            if (nlong == nblk) nlong = 0;
+        } else {
+            std::vector<int> rank(nblk);
             for (int b = 0; b < nblk; ++b) {
                 const int s0 = b * FAC_THREADS, s1 = std::min(nsys, s0 + FAC_THREADS);
                 int r = INT32_MAX;
@@ -2307,93 +2361,91 @@ class PsvEngine : public Engine {
                 order[b] = b;
             }
             std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return rank[a] < rank[b]; });
-            bperm.upload(order, st);
         }
-        const int n = d.nn - d.itmp + 1;
-        const int lmin = lst_min();
-        // Lst holds rows lmin .. n: kernels index rows from 0 off this base
-        cd* const Lb = Lst.p - (size_t)lmin * 3 * nsys;
-        const double fac_bytes = (double)(n - lmin + 1) * 3 * 16.0 + (double)(n - ls_min + 1) * 16.0;
-        int id = kid("psv_factor");
-        kbegin(id);
-        const unsigned fgrid = (unsigned)((nsys + FAC_THREADS - 1) / FAC_THREADS);
-        const int dmin = ls_min;  // pivots from the deepest source row up
-        const int* kc = nullptr;
-        if (depth_bound > 0.0 && ls_min > 9) {
-            k_psv_cutrow<<<(nsys + 127) / 128, 128, 0, st>>>(cnodes.p, cnode_src, (float)-std::log(depth_bound),
-                                                             d.tlen, fr_, wl, nsys, ls_min - 8, kcut.p);
-            DSM_LAUNCH(*this);
-            kc = kcut.p;
-        }
+        bperm.upload(order, st);
         // source 0's forward pass rides along the factorisation (its first
         // source row must lie above the band's first rows)
         const int ls0 = dsrc[0].jsrc - dsrc[0].itmp + 1;
         const int lsf = ls0 > 3 && ls0 + 8 <= n ? ls0 : -1;
-        auto factor = [&](auto kern) {
-            kern<<<fgrid, FAC_THREADS, 0, st>>>(d, Prow.p, wl, nsys, lmin, Lb, tails.p, Dst.p, dmin, kc, bperm.p,
-                                                lsf, Zst.p);
-        };
-        if (mixed()) {
-            if (tune.fac_rows == 8) factor(k_psv_solve<true, 8>);
-            else factor(k_psv_solve<true, 16>);
-        } else {
-            if (tune.fac_rows == 8) factor(k_psv_solve<false, 8>);
-            else factor(k_psv_solve<false, 16>);
-        }
-        kend(id, fac_bytes * nsys, 0.0);
-        DSM_LAUNCH(*this);
-        double sub_tot = 0.0;
-        for (int k = 0; k < nsrc; ++k) {
-            const PsvDev& e = dsrc[k];
-            const int ls = e.jsrc - e.itmp + 1;
-            const double fwd_bytes = (double)(n - ls + 1) * (4 * 16.0 + 3 * 16.0 + 16.0);
-            const double sub_bytes = (double)(n - jmin_loc + 1) * 3 * 16.0 + (double)(n - ls + 1) * 4 * 16.0 +
-                                     (double)ncap * NB * 16.0;
-            sub_tot += fwd_bytes + sub_bytes;
-            id = kid("psv_forward");
-            kbegin(id);
-            if (k == 0 && lsf > 0) {
-                // done by the factorisation
-            } else if (mixed())
-                k_psv_fwd<true><<<fgrid, FAC_THREADS, 0, st>>>(e, nsys, ls, Lb, Dst.p, dmin, tails.p, Zst.p);
-            else
-                k_psv_fwd<false><<<fgrid, FAC_THREADS, 0, st>>>(e, nsys, ls, Lb, Dst.p, dmin, tails.p, Zst.p);
-            kend(id, fwd_bytes * nsys, 0.0);
-            DSM_LAUNCH(*this);
-            id = kid("psv_substitution");
-            kbegin(id);
-            if (mixed())
-                k_psv_up<true><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
-                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc, bperm.p, Xprobe.p);
-            else
-                k_psv_up<false><<<(nsys + UP_THREADS - 1) / UP_THREADS, UP_THREADS, UP_SMEM, st>>>(
-                    e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p, tails.p, Xcap.p, kc, bperm.p, Xprobe.p);
-            kend(id, sub_bytes * nsys, 0.0);
-            DSM_LAUNCH(*this);
-            id = kid("psv_source_coef");
-            kbegin(id);
-            double* amk = amps.p + (size_t)k * F * Lcap;
-            k_psv_coef<<<(nsys + 127) / 128, 128, 0, st>>>(e, fr_, wl, nsys, ab.p + (size_t)k * F * 320, co.p,
-                                                            rsgt_sw, Xprobe.p, amk, Lcap);
-            kend(id, 0.0, 0.0);
-            DSM_LAUNCH(*this);
-            const int fs = tune.fld_orders == 16 ? 16 : 32, frec = 32 / fs;
-            dim3 grid((nsys + fs - 1) / fs, (R + 1 + 4 * frec - 1) / (4 * frec));
-            id = kid("psv_fields");
-            kbegin(id);
-            if (afld_bytes == 4) {
-                auto kern = fs == 16 ? k_psv_fields<true, 16> : k_psv_fields<true, 32>;
-                kern<<<grid, 128, 0, st>>>(e, wl, nsys, Xcap.p, co.p, afld_of<float>(0, k), afld_of<float>(1, k),
-                                           afld_of<float>(2, k), Lcap);
+        const int fs = tune.fld_orders == 16 ? 16 : 32, frec = 32 / fs;
+        // the solve chain of blocks bp[0 .. nb) on stream s
+        auto chain = [&](cudaStream_t s, const int* bp, int nb) {
+            int id = kid("psv_factor");
+            kbegin(id, s);
+            auto factor = [&](auto kern) {
+                kern<<<nb, FAC_THREADS, 0, s>>>(d, Prow.p, wl, nsys, lmin, Lb, tails.p, Dst.p, dmin, kc, bp, lsf,
+                                                Zst.p);
+            };
+            if (mixed()) {
+                if (tune.fac_rows == 8) factor(k_psv_solve<true, 8>);
+                else factor(k_psv_solve<true, 16>);
             } else {
-                auto kern = fs == 16 ? k_psv_fields<false, 16> : k_psv_fields<false, 32>;
-                kern<<<grid, 128, 0, st>>>(e, wl, nsys, Xcap.p, co.p, afld_of<double>(0, k), afld_of<double>(1, k),
-                                           afld_of<double>(2, k), Lcap);
+                if (tune.fac_rows == 8) factor(k_psv_solve<false, 8>);
+                else factor(k_psv_solve<false, 16>);
             }
-            kend(id, 0.0, 0.0);
+            kend(id, fac_bytes * std::min(nsys, nb * FAC_THREADS), 0.0, s);
             DSM_LAUNCH(*this);
+            for (int k = 0; k < nsrc; ++k) {
+                const PsvDev& e = dsrc[k];
+                const int ls = e.jsrc - e.itmp + 1;
+                const double nsb = std::min(nsys, nb * FAC_THREADS);
+                const double fwd_bytes = (double)(n - ls + 1) * (4 * 16.0 + 3 * 16.0 + 16.0);
+                const double sub_bytes = (double)(n - jmin_loc + 1) * 3 * 16.0 + (double)(n - ls + 1) * 4 * 16.0 +
+                                         (double)ncap * NB * 16.0;
+                if (!(k == 0 && lsf > 0)) {  // otherwise done by the factorisation
+                    id = kid("psv_forward");
+                    kbegin(id, s);
+                    if (mixed())
+                        k_psv_fwd<true><<<nb, FAC_THREADS, 0, s>>>(e, nsys, ls, Lb, Dst.p, dmin, tails.p, Zst.p, bp);
+                    else
+                        k_psv_fwd<false><<<nb, FAC_THREADS, 0, s>>>(e, nsys, ls, Lb, Dst.p, dmin, tails.p, Zst.p, bp);
+                    kend(id, fwd_bytes * nsb, 0.0, s);
+                    DSM_LAUNCH(*this);
+                }
+                id = kid("psv_substitution");
+                kbegin(id, s);
+                if (mixed())
+                    k_psv_up<true><<<nb, UP_THREADS, UP_SMEM, s>>>(e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p,
+                                                                  tails.p, Xcap.p, kc, bp, Xprobe.p);
+                else
+                    k_psv_up<false><<<nb, UP_THREADS, UP_SMEM, s>>>(e, nsys, jmin_loc, capmap.p, caplist.p, Lb,
+                                                                   Zst.p, tails.p, Xcap.p, kc, bp, Xprobe.p);
+                kend(id, sub_bytes * nsb, 0.0, s);
+                DSM_LAUNCH(*this);
+                id = kid("psv_source_coef");
+                kbegin(id, s);
+                double* amk = amps.p + (size_t)k * F * Lcap;
+                k_psv_coef<<<nb, 128, 0, s>>>(e, fr_, wl, nsys, ab.p + (size_t)k * F * 320, co.p, rsgt_sw,
+                                               Xprobe.p, amk, Lcap, bp);
+                kend(id, 0.0, 0.0, s);
+                DSM_LAUNCH(*this);
+                dim3 grid((unsigned)(nb * (128 / fs)), (R + 1 + 4 * frec - 1) / (4 * frec));
+                id = kid("psv_fields");
+                kbegin(id, s);
+                if (afld_bytes == 4) {
+                    auto kern = fs == 16 ? k_psv_fields<true, 16> : k_psv_fields<true, 32>;
+                    kern<<<grid, 128, 0, s>>>(e, wl, nsys, Xcap.p, co.p, afld_of<float>(0, k), afld_of<float>(1, k),
+                                              afld_of<float>(2, k), Lcap, bp);
+                } else {
+                    auto kern = fs == 16 ? k_psv_fields<false, 16> : k_psv_fields<false, 32>;
+                    kern<<<grid, 128, 0, s>>>(e, wl, nsys, Xcap.p, co.p, afld_of<double>(0, k), afld_of<double>(1, k),
+                                              afld_of<double>(2, k), Lcap, bp);
+                }
+                kend(id, 0.0, 0.0, s);
+                DSM_LAUNCH(*this);
+                stats.solve_bytes += (k == 0 ? fac_bytes : 0.0) * nsb + (fwd_bytes + sub_bytes) * nsb;
+            }
+        };
+        if (nlong > 0) {
+            DSM_CUDA(cudaEventRecord(ev_s3a, st));
+            DSM_CUDA(cudaStreamWaitEvent(st3, ev_s3a, 0));
+            chain(st3, bperm.p, nlong);                 // the long recurrences
+            chain(st, bperm.p + nlong, nblk - nlong);   // the rest
+            DSM_CUDA(cudaEventRecord(ev_s3b, st3));
+            DSM_CUDA(cudaStreamWaitEvent(st, ev_s3b, 0));
+        } else {
+            chain(st, bperm.p, nblk);
         }
-        stats.solve_bytes += (fac_bytes + sub_tot) * nsys;
     }
 
     void scan_chunk(int nf, const WorkList& wl) override {
