@@ -253,6 +253,12 @@ void Engine::lsum_group(int w0, int w1, const std::vector<int>& nord) {
                 tc_bytes += 4.0 * ((double)P.M + N) * kp + 4.0 * (double)P.M * N;
             }
         }
+    // longest contractions first: a CTA takes tiles t, t + grid, ... in
+    // list order, so the heavy tiles spread over the CTAs and the light
+    // ones fill in at the end (instead of the top frequencies' tiles
+    // trailing the launch)
+    std::stable_sort(hp.begin(), hp.end(),
+                     [](const tc::Problem& a, const tc::Problem& b) { return a.kblocks > b.kblocks; });
     if (tcp_next + hp.size() > tcp.n) throw Error(DSM_ERR_INVALID, "contraction list exceeds its buffer");
     id = kid("lsum_tc");
     kbegin(id);
