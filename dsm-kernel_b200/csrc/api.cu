@@ -576,7 +576,14 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
         // lsuf (the cutoff is never below it); later ranges grow by half.
         std::vector<int> next(nf, 0), span(nf, 0);
         std::vector<int> hf(ilist + b0, ilist + b0 + nf);
-        for (int w = 0; w < nf; ++w) span[w] = first_span(hf[w]);
+        // first ranges: the lsuf rule scaled by what the context's earlier
+        // batches needed (span_hint, 1 while the rule covers the cutoffs)
+        std::vector<int> span_rule(nf);
+        for (int w = 0; w < nf; ++w) {
+            span_rule[w] = first_span(hf[w]);
+            const double sp = std::min((double)maxlmax + 1.0, std::ceil(span_rule[w] * span_hint));
+            span[w] = opt.l_chunk > 0 ? span_rule[w] : std::max(span_rule[w], ((int)sp + 31) / 32 * 32);
+        }
         if (opt.use_lmax_predictor && pred.ready && opt.l_chunk <= 0) {
             // the network predicts log(lmax) - f0, f0 = log(1 + omega rtop /
             // vtop) (the lsuf scale); first range = lmax * 1.02 + 24, never
@@ -672,13 +679,18 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             }
             if (all) break;
         }
+        double need_ratio = 1.0;  // cutoff (+ a step group) over the lsuf rule, largest of the batch
         for (int s = 0; s < nsrc; ++s)
             for (int w = 0; w < nf; ++w) {
                 CutState& c = hcs[(size_t)s * F + w];
                 if (c.norders == 0) { c.norders = maxlmax + 1; c.llog = maxlmax; }
                 stats.orders_padded += (long long)next[w] - c.norders;
                 stats.freqs_extended += c.norders > span0[w] ? 1 : 0;
+                need_ratio = std::max(need_ratio, (c.norders + 32.0) / span_rule[w]);
             }
+        // the next batch's first ranges cover what this one needed (the
+        // amplitude test still decides every cutoff; only the work split moves)
+        if (!(opt.use_lmax_predictor && pred.ready)) span_hint = std::min(4.0, need_ratio);
         // source 0's states stand for the batch where one set is reported
         for (int w = 0; w < nf; ++w) hc[w] = hcs[w];
         join_side();
@@ -1162,8 +1174,8 @@ extern "C" int dsm_get_tuning(const dsm_ctx_t* ctx, dsm_tuning_t* t) {
 extern "C" int dsm_set_tuning(dsm_ctx_t* ctx, const dsm_tuning_t* t) {
     if (!ctx || !t) return DSM_ERR_INVALID;
     if ((t->fac_rows != 8 && t->fac_rows != 16) || (t->fld_orders != 16 && t->fld_orders != 32) ||
-        (t->tc_orders != 32 && t->tc_orders != 64)) {
-        ctx->err = "tuning: fac_rows 8 or 16, fld_orders 16 or 32, tc_orders 32 or 64";
+        (t->tc_orders != 32 && t->tc_orders != 64) || (t->fwd_merge != 0 && t->fwd_merge != 1)) {
+        ctx->err = "tuning: fac_rows 8 or 16, fld_orders 16 or 32, tc_orders 32 or 64, fwd_merge 0 or 1";
         return DSM_ERR_INVALID;
     }
     ctx->eng->tune = *t;
@@ -1186,7 +1198,11 @@ extern "C" int dsm_autotune(dsm_ctx_t* ctx, const int* ilist, int n, int reps, d
                 if (!psv && fo != keep.fld_orders) continue;
                 for (int tb : {64, 32}) {
                     if (!e.mixed() && tb != keep.tc_orders) continue;
-                    cand.push_back({psv ? fr : keep.fac_rows, psv ? fo : keep.fld_orders, e.mixed() ? tb : keep.tc_orders});
+                    for (int fm : {1, 0}) {
+                        if (!psv && fm != keep.fwd_merge) continue;
+                        cand.push_back({psv ? fr : keep.fac_rows, psv ? fo : keep.fld_orders,
+                                        e.mixed() ? tb : keep.tc_orders, psv ? fm : keep.fwd_merge});
+                    }
                 }
             }
         }

@@ -88,7 +88,7 @@ class Engine {
     // selects the slot the mode hooks and the l-sum work on.
     int nsrc = 1, src = 0;
     // run-time tile shapes (dsm_set_tuning, dsm_autotune)
-    dsm_tuning_t tune{16, 32, 64};
+    dsm_tuning_t tune{16, 32, 64, 1};
     // depth cut-off amplitude bound (P-SV; 0: the whole band, as the reference)
     double depth_bound = 0.0;
     int amp_k = 1;                   // cutoff probes stored per order
@@ -182,6 +182,7 @@ class Engine {
     int nsys_max = 0;                // systems per solve launch (scratch size)
     double vtop_ = 1.0, rtop_ = 1.0;  // top-zone Vsv sum and radius (callsuf)
     int first_span(int ifreq) const;
+    double span_hint = 1.0;          // first-range scale learned from earlier batches (run)
     DBuf<int> wl_off, wl_lb;
     std::vector<int> wl_host_off;    // host copy of the current round's work-list offsets
     virtual void epilogue(const int* freqs_dev, int w, int nf) = 0;

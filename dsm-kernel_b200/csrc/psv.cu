@@ -564,8 +564,8 @@ constexpr int FAC_THREADS = 128;
 // (dsm_set_tuning / dsm_autotune)
 constexpr int FAC_NW = 4;   // frequencies staged per block
 
-template <bool FAST, int CH>
-__global__ void __launch_bounds__(FAC_THREADS, 2) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
+template <bool FAST, int CH, bool MERGE>
+__global__ void __launch_bounds__(FAC_THREADS, MERGE ? 2 : 3) k_psv_solve(PsvDev d, const cd* __restrict__ Prow, WorkList wl,
                                                               int nsys, int lmin, cd* __restrict__ Lst,
                                                               SysTail* __restrict__ tail, cd* __restrict__ Dst,
                                                               int dmin, const int* __restrict__ kcut,
@@ -719,7 +719,7 @@ __global__ void __launch_bounds__(FAC_THREADS, 2) k_psv_solve(PsvDev d, const cd
     // first row here only.
     int k = q0 * CH + 1;
     for (;; k += 4) {
-        if (k + 3 > n - 4 || (lsf > 3 && k + 6 >= lsf)) break;
+        if (k + 3 > n - 4 || (MERGE && lsf > 3 && k + 6 >= lsf)) break;
         boundary(k);
         if (k < kw) {  // this warp's band starts further up
             if ((k + 3) % CH == 0) __syncthreads();
@@ -773,7 +773,7 @@ __global__ void __launch_bounds__(FAC_THREADS, 2) k_psv_solve(PsvDev d, const cd
             h1a = so.w1;
             h0 = so.w0;
         };
-        const bool fw = lsf > 3;
+        const bool fw = MERGE && lsf > 3;
         for (;; k += 4) {
             boundary(k);
             if (k < kw) {
@@ -2366,7 +2366,7 @@ class PsvEngine : public Engine {
         // source 0's forward pass rides along the factorisation (its first
         // source row must lie above the band's first rows)
         const int ls0 = dsrc[0].jsrc - dsrc[0].itmp + 1;
-        const int lsf = ls0 > 3 && ls0 + 8 <= n ? ls0 : -1;
+        const int lsf = tune.fwd_merge && ls0 > 3 && ls0 + 8 <= n ? ls0 : -1;
         const int fs = tune.fld_orders == 16 ? 16 : 32, frec = 32 / fs;
         // the solve chain of blocks bp[0 .. nb) on stream s
         auto chain = [&](cudaStream_t s, const int* bp, int nb) {
@@ -2376,12 +2376,22 @@ class PsvEngine : public Engine {
                 kern<<<nb, FAC_THREADS, 0, s>>>(d, Prow.p, wl, nsys, lmin, Lb, tails.p, Dst.p, dmin, kc, bp, lsf,
                                                 Zst.p);
             };
-            if (mixed()) {
-                if (tune.fac_rows == 8) factor(k_psv_solve<true, 8>);
-                else factor(k_psv_solve<true, 16>);
+            if (lsf > 0) {
+                if (mixed()) {
+                    if (tune.fac_rows == 8) factor(k_psv_solve<true, 8, true>);
+                    else factor(k_psv_solve<true, 16, true>);
+                } else {
+                    if (tune.fac_rows == 8) factor(k_psv_solve<false, 8, true>);
+                    else factor(k_psv_solve<false, 16, true>);
+                }
             } else {
-                if (tune.fac_rows == 8) factor(k_psv_solve<false, 8>);
-                else factor(k_psv_solve<false, 16>);
+                if (mixed()) {
+                    if (tune.fac_rows == 8) factor(k_psv_solve<true, 8, false>);
+                    else factor(k_psv_solve<true, 16, false>);
+                } else {
+                    if (tune.fac_rows == 8) factor(k_psv_solve<false, 8, false>);
+                    else factor(k_psv_solve<false, 16, false>);
+                }
             }
             kend(id, fac_bytes * std::min(nsys, nb * FAC_THREADS), 0.0, s);
             DSM_LAUNCH(*this);

@@ -122,7 +122,7 @@ DSM_ERR_NODEVICE = 7
 
 
 class Tuning(C.Structure):
-    _fields_ = [("fac_rows", C.c_int), ("fld_orders", C.c_int), ("tc_orders", C.c_int)]
+    _fields_ = [("fac_rows", C.c_int), ("fld_orders", C.c_int), ("tc_orders", C.c_int), ("fwd_merge", C.c_int)]
 
 
 class Accuracy(C.Structure):
@@ -192,7 +192,6 @@ def lib() -> C.CDLL:
         L.dsm_set_fp64_check.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
         L.dsm_get_accuracy.argtypes = [C.c_void_p, C.POINTER(Accuracy)]
         L.dsm_sh_cutoff_noalloc.argtypes = [C.POINTER(ShSetup), _ip, C.c_int, _ip]
-        L.dsm_tc_selftest.argtypes = [C.c_int] * 10 + [C.POINTER(C.c_double)]
         _f = C.POINTER(C.c_float)
         L.dsm_lmax_features.argtypes = [C.c_void_p, _ip, C.c_int, _f]
         L.dsm_cutoffs.argtypes = [C.c_void_p, _ip, C.c_int, _ip]
@@ -222,6 +221,24 @@ def lib() -> C.CDLL:
     return _lib
 
 
+_selftest = None
+
+
+def _selftest_lib() -> C.CDLL:
+    """The test-only library of the contraction's self-test (built beside
+    the engine's, linked against it)."""
+    global _selftest
+    if _selftest is None:
+        lib()
+        path = os.path.join(os.path.dirname(LIB_PATH), "libdsmsgt_selftest.so")
+        if not os.path.exists(path):
+            raise DsmError(f"{path} is missing: run __graft_entry__.build() first")
+        _selftest = C.CDLL(path)
+        _selftest.dsm_tc_selftest.restype = C.c_int
+        _selftest.dsm_tc_selftest.argtypes = [C.c_int] * 10 + [C.POINTER(C.c_double)]
+    return _selftest
+
+
 def tc_selftest(M: int, N: int, K: int, nfreq: int = 1, fmt: int = 0, bk: int = 32, reps: int = 0,
                 check: bool = True, flags: int = 1, chunk: int = 2) -> dict:
     """Runs the tensor-core split contraction on seeded pieces (fmt 0 fp16,
@@ -231,8 +248,9 @@ def tc_selftest(M: int, N: int, K: int, nfreq: int = 1, fmt: int = 0, bk: int = 
     Returns max |error|, max |reference|, ms per launch and the tensor
     flops of one launch."""
     L = lib()
+    T = _selftest_lib()
     res = (C.c_double * 4)()
-    rc = L.dsm_tc_selftest(M, N, K, nfreq, fmt, bk, flags, chunk, reps, int(check), res)
+    rc = T.dsm_tc_selftest(M, N, K, nfreq, fmt, bk, flags, chunk, reps, int(check), res)
     if rc:
         raise DsmError(f"dsm_tc_selftest failed ({rc}): {L.dsm_last_error(None).decode()}")
     return {"max_err": res[0], "ref_max": res[1], "ms": res[2], "flops": res[3]}
@@ -441,10 +459,11 @@ class Context:
     def tuning(self) -> dict:
         t = Tuning()
         lib().dsm_get_tuning(self.h, C.byref(t))
-        return {"fac_rows": t.fac_rows, "fld_orders": t.fld_orders, "tc_orders": t.tc_orders}
+        return {"fac_rows": t.fac_rows, "fld_orders": t.fld_orders, "tc_orders": t.tc_orders,
+                "fwd_merge": t.fwd_merge}
 
-    def set_tuning(self, fac_rows: int = 16, fld_orders: int = 32, tc_orders: int = 64):
-        t = Tuning(fac_rows, fld_orders, tc_orders)
+    def set_tuning(self, fac_rows: int = 16, fld_orders: int = 32, tc_orders: int = 64, fwd_merge: int = 1):
+        t = Tuning(fac_rows, fld_orders, tc_orders, fwd_merge)
         rc = lib().dsm_set_tuning(self.h, C.byref(t))
         if rc:
             raise DsmError(f"dsm_set_tuning failed ({rc}): {lib().dsm_last_error(self.h).decode()}", rc)
@@ -457,7 +476,8 @@ class Context:
         rc = lib().dsm_autotune(self.h, _ptr(fl, _ip), len(fl), reps, C.byref(t), C.byref(ms))
         if rc:
             raise DsmError(f"dsm_autotune failed ({rc}): {lib().dsm_last_error(self.h).decode()}", rc)
-        return {"fac_rows": t.fac_rows, "fld_orders": t.fld_orders, "tc_orders": t.tc_orders}, ms.value
+        return {"fac_rows": t.fac_rows, "fld_orders": t.fld_orders, "tc_orders": t.tc_orders,
+                "fwd_merge": t.fwd_merge}, ms.value
 
     def debug_set(self, name: str, value: int = 1):
         """Test hook of the library's error paths (dsm_debug_set)."""

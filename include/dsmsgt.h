@@ -329,6 +329,8 @@ typedef struct dsm_tuning {
     int fac_rows;    /* band rows a factorisation block stages per chunk: 8 or 16 (P-SV) */
     int fld_orders;  /* consecutive orders per warp of the receiver-field kernel: 16 or 32 (P-SV) */
     int tc_orders;   /* orders per tensor-core stage (and FP64 chunk sum): 32 or 64 (mixed precision) */
+    int fwd_merge;   /* 1: the first source's forward substitution inside the P-SV factorisation
+                        (2 blocks per SM), 0: in its own kernel after it (3 blocks per SM) */
 } dsm_tuning_t;
 int dsm_get_tuning(const dsm_ctx_t *ctx, dsm_tuning_t *t);
 int dsm_set_tuning(dsm_ctx_t *ctx, const dsm_tuning_t *t);

@@ -25,19 +25,21 @@ def test_fp64_outputs_identical_across_tile_shapes(built):
     s = dsmsgt.Setup(psv_small(), "psv")
     freqs = [1, 20, 47, 64]
     ctx = dsmsgt.Context(s, freq_batch=3)
-    assert ctx.tuning() == {"fac_rows": 16, "fld_orders": 32, "tc_orders": ctx.tuning()["tc_orders"]}
+    t0 = ctx.tuning()
+    assert t0["fac_rows"] == 16 and t0["fld_orders"] == 32 and t0["fwd_merge"] == 1
     want = ctx.run(freqs)
     for fr in (8, 16):
         for fo in (16, 32):
-            ctx.set_tuning(fac_rows=fr, fld_orders=fo)
-            _same(ctx.run(freqs), want)
+            for fm in (0, 1):
+                ctx.set_tuning(fac_rows=fr, fld_orders=fo, fwd_merge=fm)
+                _same(ctx.run(freqs), want)
     ctx.close()
 
 
 @pytest.mark.gpu
 def test_set_tuning_rejects_other_shapes(built):
     ctx = dsmsgt.Context(dsmsgt.Setup(psv_small(), "psv"))
-    for bad in ({"fac_rows": 12}, {"fld_orders": 64}, {"tc_orders": 16}):
+    for bad in ({"fac_rows": 12}, {"fld_orders": 64}, {"tc_orders": 16}, {"fwd_merge": 2}):
         with pytest.raises(dsmsgt.DsmError) as ei:
             ctx.set_tuning(**bad)
         assert ei.value.code == dsmsgt.DSM_ERR_INVALID
@@ -58,6 +60,7 @@ def test_autotune_keeps_a_valid_shape(built, prec):
     assert ms > 0.0
     assert t == ctx.tuning()
     assert t["fac_rows"] in (8, 16) and t["fld_orders"] in (16, 32) and t["tc_orders"] in (32, 64)
+    assert t["fwd_merge"] in (0, 1)
     got = ctx.run(freqs)
     ctx.close()
     assert list(got[3]) == list(want[3])
