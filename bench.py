@@ -651,12 +651,15 @@ def main():
         clocks = ClockSampler(dev)
         clocks.start()
         kstats, ms_dev, launches, llogs = {}, 0.0, 0, []
+        phases = {"solve": 0.0, "lsum": 0.0}
         sol = {"systems": 0, "orders_used": 0, "orders_padded": 0, "solve_rounds": 0, "freqs_extended": 0}
         barrier()
         for k in range(args.steps):
             llogs.append(ctx.run_device(step_freqs(k, args.per_step, imax, rank, world)).tolist())
             st = ctx.stats()
             ms_dev += st.ms_total
+            phases["solve"] += st.ms_solve
+            phases["lsum"] += st.ms_lsum
             for key in sol:
                 sol[key] += getattr(st, key)
             launches += st.launches - sum(v[1] for n_, v in st.kernels().items() if n_.startswith("lsum_dgemm"))
@@ -690,6 +693,7 @@ def main():
         slices = args.steps * args.per_step * world
         return {"value": slices / t_dev, "t": t_dev, "kstats": kstats, "launches": launches, "tuning": tuning,
                 "llogs": llogs, "clocks": clk, "solve": sol,
+                "phase_ms_per_step": {k: v / args.steps for k, v in phases.items()},
                 "e2e": {"value": slices / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * F,
                         "d2h_bytes_per_step": 8 * (per_t + per_r + per_s) * F + 4 * F,
                         "timing": "host wall clock around dsm_run_freqs (perf_counter), records to pinned memory"}}
@@ -755,7 +759,7 @@ def main():
     share = {k: round(v[0] / max(run["t"] * 1e3, 1e-9), 4) for k, v in kstats.items()}
     # HBM-bound band kernels: algorithmic bytes over their event time
     hbm = {}
-    for k in ("psv_factor", "psv_substitution"):
+    for k in ("psv_factor", "psv_substitution", "psv_factor_long", "psv_substitution_long"):
         if k in kstats and kstats[k][0] > 0:
             ach = kstats[k][2] / (kstats[k][0] / 1e3) / 1e9
             peak = peaks.get("hbm_gbs", 6650.0)
@@ -790,6 +794,7 @@ def main():
                                l2="inputs larger than L2 (field matrices of several GB per step)"),
                 "e2e": run["e2e"], "gpu_launches": int(run["launches"]), "tuning": run["tuning"],
                 "roofline": roof, "hbm_kernels": hbm, "kernel_share": share,
+                "phase_ms_per_step": run["phase_ms_per_step"],
                 "cpu_baseline": cpu, "clocks": run["clocks"],
                 "solve": dict(sol, slices=args.steps * args.per_step,
                               padded_fraction=sol["orders_padded"] / max(sol["orders_used"], 1),

@@ -46,6 +46,17 @@ void Engine::init_common(int dev) {
     DSM_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
     DSM_CUDA(cudaStreamCreateWithFlags(&stc, cudaStreamNonBlocking));
     for (auto& e : ev_grp) DSM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    {  // mixed l-sum pipeline: the contraction's stream has priority
+        int lo = 0, hi = 0;
+        DSM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        DSM_CUDA(cudaStreamCreateWithPriority(&stt, cudaStreamNonBlocking, hi));
+        DSM_CUDA(cudaStreamCreateWithFlags(&sts, cudaStreamNonBlocking));
+        DSM_CUDA(cudaStreamCreateWithFlags(&ste, cudaStreamNonBlocking));
+        for (auto& e : ev_sp) DSM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (auto& e : ev_td) DSM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        DSM_CUDA(cudaEventCreateWithFlags(&ev_lp, cudaEventDisableTiming));
+        DSM_CUDA(cudaEventCreateWithFlags(&ev_lj, cudaEventDisableTiming));
+    }
     DSM_CUBLAS(cublasCreate(&cub));
     DSM_CUBLAS(cublasSetStream(cub, st));
     for (auto& e : ev) DSM_CUDA(cudaEventCreate(&e));
@@ -59,6 +70,7 @@ void Engine::init_common(int dev) {
     if (const char* e = std::getenv("DSM_TC_BK")) tc_bk = std::atoi(e) == 64 ? 64 : 32;
     tune.tc_orders = tc_bk;
     if (const char* e = std::getenv("DSM_TC_CHUNK")) tc_chunk = std::max(0, std::atoi(e));
+    if (const char* e = std::getenv("DSM_LSUM_GROUPS")) lsum_groups = std::max(1, std::atoi(e));
     dflags.reserve(2);
     DSM_CUDA(cudaMemset(dflags.p, 0, 2 * sizeof(int)));
 }
@@ -76,6 +88,14 @@ Engine::~Engine() {
     if (stc) { cudaStreamSynchronize(stc); cudaStreamDestroy(stc); }
     for (auto& e : ev_grp)
         if (e) cudaEventDestroy(e);
+    for (cudaStream_t* s : {&sts, &ste, &stt})
+        if (*s) { cudaStreamSynchronize(*s); cudaStreamDestroy(*s); }
+    for (auto& e : ev_sp)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : ev_td)
+        if (e) cudaEventDestroy(e);
+    if (ev_lp) cudaEventDestroy(ev_lp);
+    if (ev_lj) cudaEventDestroy(ev_lj);
     if (st) cudaStreamDestroy(st);
 }
 
@@ -200,87 +220,112 @@ void Engine::lsum_prepare(int nf, const std::vector<int>& nord) {
     tcp_next = 0;
 }
 
-void Engine::lsum_group(int w0, int w1, const std::vector<int>& nord) {
-    const int n = w1 - w0;
-    if (n <= 0) return;
-    double split_bytes = 0.0, tflops = 0.0, tc_bytes = 0.0;
-    for (int m = m_lo; m <= 2; ++m)
-        for (int w = w0; w < w1; ++w) {
-            const double kp = (double)((nord[w] + tc_bk - 1) / tc_bk * tc_bk);
-            split_bytes += (double)rows_m[m] * ((double)afld_bytes * nord[w] + 4.0 * kp);
+// Problem lists of every frequency group of the batch, uploaded in one copy
+// before the first group's launches (a pageable copy per group could hold
+// the host until the stream has drained, between the groups' launches).
+void Engine::lsum_plan(const std::vector<std::vector<int>>& groups, const std::vector<int>& nord) {
+    tc_groups.clear();
+    std::vector<tc::Problem> all;
+    for (const auto& slots : groups) {
+        TcGroup G{slots, {}, 0.0, 0.0, 0.0};
+        // per (frequency, |m|): the leading rows against all 2 Th basis
+        // columns, the remaining rows against the first Th
+        std::vector<tc::Problem> hp;
+        for (int w : G.slots)
+            for (int m = m_lo; m <= 2; ++m) {
+                if (!rows_m[m]) continue;
+                const double kp = (double)((nord[w] + tc_bk - 1) / tc_bk * tc_bk);
+                G.split_bytes += (double)rows_m[m] * ((double)afld_bytes * nord[w] + 4.0 * kp);
+                const int rf = full_rows(m);
+                for (int h = 0; h < 2; ++h) {
+                    const int row0 = h == 0 ? 0 : rf, M = h == 0 ? rf : rows_m[m] - rf, N = h == 0 ? 2 * Th : Th;
+                    if (M <= 0) continue;
+                    tc::Problem P{};
+                    P.amap = m;
+                    P.z = w;
+                    P.bmap = m;
+                    P.row0 = row0;
+                    P.kblocks = (nord[w] + tc_bk - 1) / tc_bk;
+                    P.M = M;
+                    P.N = N;
+                    P.tiles_n = (N + tc::BN - 1) / tc::BN;
+                    P.C = Cmix.p + (size_t)w * c_total() + c_off(m) + row0;
+                    P.sa = sA[m].p + (size_t)w * rows_m[m] + row0;
+                    P.sb = sB[m].p;
+                    P.ldc = rows_m[m];
+                    hp.push_back(P);
+                    // algorithmic: one real product per (row, column, order) up to
+                    // the cutoff (the tensor cores run three piece products on
+                    // orders padded to BK)
+                    G.flops += 2.0 * P.M * (double)N * (double)nord[w];
+                    G.bytes += 4.0 * ((double)P.M + N) * (double)P.kblocks * tc_bk + 4.0 * (double)P.M * N;
+                }
+            }
+        // longest contractions first: a CTA takes tiles t, t + grid, ... in
+        // list order, so the heavy tiles spread over the CTAs and the light
+        // ones fill in at the end (instead of the top frequencies' tiles
+        // trailing the launch)
+        std::stable_sort(hp.begin(), hp.end(),
+                         [](const tc::Problem& a, const tc::Problem& b) { return a.kblocks > b.kblocks; });
+        for (size_t k = 0; k < hp.size(); k += tc::MAXP) {
+            const int np = (int)std::min<size_t>(tc::MAXP, hp.size() - k);
+            int tiles = 0;
+            for (int i = 0; i < np; ++i) {
+                hp[k + i].tile0 = tiles;
+                tiles += ((hp[k + i].M + tc::BM - 1) / tc::BM) * hp[k + i].tiles_n;
+            }
+            G.launches.push_back({tcp_next + all.size(), np, tiles});
+            all.insert(all.end(), hp.begin() + k, hp.begin() + k + np);
         }
-    int id = kid("lsum_split");
-    kbegin(id);
-    for (int m = m_lo; m <= 2; ++m) {
-        if (!rows_m[m]) continue;
-        const size_t rw = (size_t)rows_m[m];
-        const char* A = reinterpret_cast<const char*>(Afld[m].p) + ((size_t)src * F + w0) * rw * Lcap * afld_bytes;
-        tc::split_fields(A, afld_bytes, n, rows_m[m], Lcap, d_nord.p + w0, Apc[m].p + (size_t)w0 * rw * kcA,
-                         sA[m].p + (size_t)w0 * rw, kcA, F, tc_fmt, tc_bk, st);
-        launches++;
+        tc_groups.push_back(std::move(G));
     }
-    kend(id, split_bytes, 0.0);
+    if (tcp_next + all.size() > tcp.n) throw Error(DSM_ERR_INVALID, "contraction list exceeds its buffer");
+    // each source's lists take their own slots of tcp, so no copy overwrites
+    // a list an earlier launch may still read
+    if (!all.empty())
+        DSM_CUDA(cudaMemcpyAsync(tcp.p + tcp_next, all.data(), sizeof(tc::Problem) * all.size(),
+                                 cudaMemcpyHostToDevice, st));
+    tcp_next += all.size();
+}
 
-    // per (frequency, |m|): the leading rows against all 2 Th basis
-    // columns, the remaining rows against the first Th
-    std::vector<tc::Problem> hp;
-    for (int w = w0; w < w1; ++w)
+// Group g of the mixed l-sum: split of its field matrices on sts (after the
+// previous group's split), then its contraction launches on stt once the
+// split is done.
+void Engine::lsum_group(int g) {
+    const TcGroup& G = tc_groups[(size_t)g];
+    if (G.slots.empty()) return;
+    int id = kid("lsum_split");
+    kbegin(id, sts);
+    // one split launch per |m| and run of consecutive slots
+    std::vector<int> sl = G.slots;
+    std::sort(sl.begin(), sl.end());
+    for (size_t i = 0; i < sl.size();) {
+        size_t j = i + 1;
+        while (j < sl.size() && sl[j] == sl[j - 1] + 1) ++j;
+        const int w0 = sl[i], n = (int)(j - i);
         for (int m = m_lo; m <= 2; ++m) {
             if (!rows_m[m]) continue;
-            const int rf = full_rows(m);
-            for (int g = 0; g < 2; ++g) {
-                const int row0 = g == 0 ? 0 : rf, M = g == 0 ? rf : rows_m[m] - rf, N = g == 0 ? 2 * Th : Th;
-                if (M <= 0) continue;
-                tc::Problem P{};
-                P.amap = m;
-                P.z = w;
-                P.bmap = m;
-                P.row0 = row0;
-                P.kblocks = (nord[w] + tc_bk - 1) / tc_bk;
-                P.M = M;
-                P.N = N;
-                P.tiles_n = (N + tc::BN - 1) / tc::BN;
-                P.C = Cmix.p + (size_t)w * c_total() + c_off(m) + row0;
-                P.sa = sA[m].p + (size_t)w * rows_m[m] + row0;
-                P.sb = sB[m].p;
-                P.ldc = rows_m[m];
-                hp.push_back(P);
-                // algorithmic: one real product per (row, column, order) up to
-                // the cutoff (the tensor cores run three piece products on
-                // orders padded to BK)
-                const double kp = (double)P.kblocks * tc_bk;
-                tflops += 2.0 * P.M * (double)N * (double)nord[w];
-                tc_bytes += 4.0 * ((double)P.M + N) * kp + 4.0 * (double)P.M * N;
-            }
+            const size_t rw = (size_t)rows_m[m];
+            const char* A =
+                reinterpret_cast<const char*>(Afld[m].p) + ((size_t)src * F + w0) * rw * Lcap * afld_bytes;
+            tc::split_fields(A, afld_bytes, n, rows_m[m], Lcap, d_nord.p + w0, Apc[m].p + (size_t)w0 * rw * kcA,
+                             sA[m].p + (size_t)w0 * rw, kcA, F, tc_fmt, tc_bk, sts);
+            launches++;
         }
-    // longest contractions first: a CTA takes tiles t, t + grid, ... in
-    // list order, so the heavy tiles spread over the CTAs and the light
-    // ones fill in at the end (instead of the top frequencies' tiles
-    // trailing the launch)
-    std::stable_sort(hp.begin(), hp.end(),
-                     [](const tc::Problem& a, const tc::Problem& b) { return a.kblocks > b.kblocks; });
-    if (tcp_next + hp.size() > tcp.n) throw Error(DSM_ERR_INVALID, "contraction list exceeds its buffer");
+        i = j;
+    }
+    kend(id, G.split_bytes, 0.0, sts);
+    DSM_CUDA(cudaEventRecord(ev_sp[g % MAX_OUT_GROUPS], sts));
+    DSM_CUDA(cudaStreamWaitEvent(stt, ev_sp[g % MAX_OUT_GROUPS], 0));
     id = kid("lsum_tc");
-    kbegin(id);
-    for (size_t g = 0; g < hp.size(); g += tc::MAXP) {
-        const int np = (int)std::min<size_t>(tc::MAXP, hp.size() - g);
-        int tiles = 0;
-        for (int i = 0; i < np; ++i) {
-            hp[g + i].tile0 = tiles;
-            tiles += ((hp[g + i].M + tc::BM - 1) / tc::BM) * hp[g + i].tiles_n;
-        }
-        // each launch reads its own slots of tcp, so no copy overwrites a
-        // list an earlier launch may still read
-        tc::Problem* dp = tcp.p + tcp_next;
-        DSM_CUDA(cudaMemcpyAsync(dp, hp.data() + g, sizeof(tc::Problem) * np, cudaMemcpyHostToDevice, st));
-        tcp_next += np;
-        const uint32_t fl = tc_flags | (test_tc_stall ? tc::TC_TEST_STALL : 0u);
-        const unsigned long long wait_ns = test_tc_stall ? 20000000ull : tc::WAIT_NS;
-        tc::launch(tcmaps, dp, np, tiles, tc_fmt, tc_bk, fl, tc_chunk, tc_err(), nsm, st, wait_ns);
+    kbegin(id, stt);
+    const uint32_t fl = tc_flags | (test_tc_stall ? tc::TC_TEST_STALL : 0u);
+    const unsigned long long wait_ns = test_tc_stall ? 20000000ull : tc::WAIT_NS;
+    for (const TcLaunch& L : G.launches) {
+        tc::launch(tcmaps, tcp.p + L.first, L.np, L.tiles, tc_fmt, tc_bk, fl, tc_chunk, tc_err(), nsm, stt, wait_ns);
         launches++;
     }
-    kend(id, tc_bytes, tflops);
-    // cudaMemcpyAsync from pageable memory has consumed hp when it returns
+    kend(id, G.bytes, G.flops, stt);
 }
 
 // Reads the run's status words (the stream is synchronised here anyway);
@@ -725,42 +770,101 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             for (int w = 0; w < nf; ++w) nord[w] = hs[w].norders;
             if (mixed()) lsum_prepare(nf, nord);
             // complex64 records for the host leave per group of frequencies on
-            // the copy stream while the next group's l-sum runs
-            const int ngrp = !rec32 ? 1 : (nf >= 2 * MAX_OUT_GROUPS ? MAX_OUT_GROUPS : std::max(1, nf / 2));
+            // the copy stream while the next group's l-sum runs; the mixed
+            // path groups its frequencies in any case (its pipeline below)
+            const int ngrp = rec32 ? (nf >= 2 * MAX_OUT_GROUPS ? MAX_OUT_GROUPS : std::max(1, nf / 2))
+                                   : (mixed() ? std::max(1, std::min({lsum_groups, nf, MAX_OUT_GROUPS})) : 1);
             if (rec32) out32.reserve(2 * (pt + pr + ps) * (size_t)nf);
             if (rec32 && src > 0) {  // this source's records reuse out32: the last source's copies first
                 DSM_CUDA(cudaEventRecord(ev_grp[0], stc));
                 DSM_CUDA(cudaStreamWaitEvent(st, ev_grp[0], 0));
             }
+            // Groups of batch slots.  Plain path: consecutive slots.  Mixed
+            // path: group g's split (sts) runs while group g-1 is contracted
+            // (stt), and its epilogue and records (ste) while group g+1 is,
+            // so the groups carry equal contraction work (slots dealt by
+            // their cutoff, heaviest first, in serpentine order) and the
+            // lightest goes first (its split is the one nothing hides).
+            std::vector<std::vector<int>> groups(ngrp);
+            if (mixed()) {
+                std::vector<int> byw(nf);
+                for (int w = 0; w < nf; ++w) byw[w] = w;
+                std::stable_sort(byw.begin(), byw.end(), [&](int a, int b) { return nord[a] > nord[b]; });
+                for (int k = 0; k < nf; ++k) {
+                    const int r = k / ngrp, c = k % ngrp;
+                    groups[(r & 1) ? ngrp - 1 - c : c].push_back(byw[k]);
+                }
+                std::vector<long long> work(ngrp, 0);
+                for (int g = 0; g < ngrp; ++g)
+                    for (int w : groups[g]) work[g] += nord[w];
+                std::vector<int> go(ngrp);
+                for (int g = 0; g < ngrp; ++g) go[g] = g;
+                std::stable_sort(go.begin(), go.end(), [&](int a, int b) { return work[a] < work[b]; });
+                std::vector<std::vector<int>> sorted(ngrp);
+                for (int g = 0; g < ngrp; ++g) sorted[g] = std::move(groups[go[g]]);
+                groups = std::move(sorted);
+            } else {
+                for (int g = 0; g < ngrp; ++g)
+                    for (int w = g * nf / ngrp; w < (g + 1) * nf / ngrp; ++w) groups[g].push_back(w);
+            }
+            cudaStream_t se = st;
+            if (mixed()) {
+                lsum_plan(groups, nord);
+                DSM_CUDA(cudaEventRecord(ev_lp, st));
+                DSM_CUDA(cudaStreamWaitEvent(sts, ev_lp, 0));
+                DSM_CUDA(cudaStreamWaitEvent(stt, ev_lp, 0));
+                DSM_CUDA(cudaStreamWaitEvent(ste, ev_lp, 0));
+                se = ste;
+            }
             for (int g = 0; g < ngrp; ++g) {
-                const int w0 = g * nf / ngrp, w1 = (g + 1) * nf / ngrp;
-                if (mixed()) lsum_group(w0, w1, nord);
-                for (int w = w0; w < w1; ++w) {
+                if (mixed()) {
+                    lsum_group(g);
+                    DSM_CUDA(cudaEventRecord(ev_td[g], stt));
+                    DSM_CUDA(cudaStreamWaitEvent(ste, ev_td[g], 0));
+                }
+                for (int w : groups[g]) {
                     stats.orders_used += hs[w].norders;
                     if (!mixed())
                         for (int mi = m_lo; mi <= 2; ++mi) gemm_fp64(w, mi, hs[w].norders);
-                    epilogue(d_freqs.p, w, nf);
+                    epilogue(d_freqs.p, w, nf, se);
                     for (int mi = m_lo; mi <= 2; ++mi)
                         stats.lsum_flops +=
                             2.0 * (2.0 * full_rows(mi) + (rows_m[mi] - full_rows(mi))) * Th * hs[w].norders;
                 }
-                if (rec32) {
-                    launch_pack32(*this, nf, w0, w1, pt, pr, ps);
-                    DSM_CUDA(cudaEventRecord(ev_grp[g], st));
+                if (rec32) {  // per run of consecutive slots of the group
+                    std::vector<int> sl = groups[g];
+                    std::sort(sl.begin(), sl.end());
+                    std::vector<std::pair<int, int>> runs;
+                    for (size_t i = 0; i < sl.size();) {
+                        size_t j = i + 1;
+                        while (j < sl.size() && sl[j] == sl[j - 1] + 1) ++j;
+                        runs.push_back({sl[i], sl[j - 1] + 1});
+                        i = j;
+                    }
+                    for (const auto& r : runs) launch_pack32(*this, nf, r.first, r.second, pt, pr, ps, se);
+                    DSM_CUDA(cudaEventRecord(ev_grp[g], se));
                     DSM_CUDA(cudaStreamWaitEvent(stc, ev_grp[g], 0));
                     const float* o = out32.p;
-                    const size_t n = (size_t)(w1 - w0);
-                    if (hos->tsgt32)
-                        DSM_CUDA(cudaMemcpyAsync(hos->tsgt32 + 2 * pt * (b0 + w0), o + 2 * pt * w0, 8 * pt * n,
-                                                 cudaMemcpyDeviceToHost, stc));
-                    if (hos->rsgt32 && rsgt_sw)
-                        DSM_CUDA(cudaMemcpyAsync(hos->rsgt32 + 2 * pr * (b0 + w0), o + 2 * pt * nf + 2 * pr * w0,
-                                                 8 * pr * n, cudaMemcpyDeviceToHost, stc));
-                    if (hos->synn32 && synn_sw)
-                        DSM_CUDA(cudaMemcpyAsync(hos->synn32 + 2 * ps * (b0 + w0),
-                                                 o + 2 * (pt + pr) * nf + 2 * ps * w0, 8 * ps * n,
-                                                 cudaMemcpyDeviceToHost, stc));
+                    for (const auto& r : runs) {
+                        const int w0 = r.first;
+                        const size_t n = (size_t)(r.second - r.first);
+                        if (hos->tsgt32)
+                            DSM_CUDA(cudaMemcpyAsync(hos->tsgt32 + 2 * pt * (b0 + w0), o + 2 * pt * w0, 8 * pt * n,
+                                                     cudaMemcpyDeviceToHost, stc));
+                        if (hos->rsgt32 && rsgt_sw)
+                            DSM_CUDA(cudaMemcpyAsync(hos->rsgt32 + 2 * pr * (b0 + w0),
+                                                     o + 2 * pt * nf + 2 * pr * w0, 8 * pr * n,
+                                                     cudaMemcpyDeviceToHost, stc));
+                        if (hos->synn32 && synn_sw)
+                            DSM_CUDA(cudaMemcpyAsync(hos->synn32 + 2 * ps * (b0 + w0),
+                                                     o + 2 * (pt + pr) * nf + 2 * ps * w0, 8 * ps * n,
+                                                     cudaMemcpyDeviceToHost, stc));
+                    }
                 }
+            }
+            if (mixed()) {  // st continues after the last group's epilogue (and so its contraction)
+                DSM_CUDA(cudaEventRecord(ev_lj, ste));
+                DSM_CUDA(cudaStreamWaitEvent(st, ev_lj, 0));
             }
             // --- 5: outputs
             if (llog_out && src == 0)

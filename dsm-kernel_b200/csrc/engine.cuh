@@ -57,6 +57,14 @@ class Engine {
     cudaStream_t stc = nullptr;
     static constexpr int MAX_OUT_GROUPS = 8;
     cudaEvent_t ev_grp[MAX_OUT_GROUPS] = {};
+    // mixed l-sum pipeline over groups of a batch's frequencies: the split
+    // of the next group (sts) and the epilogue of the previous one (ste) run
+    // beside the tensor-core contraction of the current one (stt, high
+    // priority, so its CTAs are placed first as the other blocks retire)
+    cudaStream_t sts = nullptr, ste = nullptr, stt = nullptr;
+    cudaEvent_t ev_sp[MAX_OUT_GROUPS] = {}, ev_td[MAX_OUT_GROUPS] = {};
+    cudaEvent_t ev_lp = nullptr, ev_lj = nullptr;
+    int lsum_groups = 4;             // frequency groups of the pipeline (a batch without host records)
     bool side_pending = false;
     cublasHandle_t cub = nullptr;
     cudaEvent_t ev[8] = {};
@@ -154,7 +162,13 @@ class Engine {
     // mixed l-sum of a batch: buffers, tensor maps and order counts once,
     // then the split and the tensor-core launches of frequencies [w0, w1)
     void lsum_prepare(int nf, const std::vector<int>& norders);
-    void lsum_group(int w0, int w1, const std::vector<int>& norders);
+    // problem lists of all groups (each a list of batch slots), one upload
+    void lsum_plan(const std::vector<std::vector<int>>& groups, const std::vector<int>& norders);
+    // group g: split on sts, contraction launches on stt
+    void lsum_group(int g);
+    struct TcLaunch { size_t first; int np, tiles; };
+    struct TcGroup { std::vector<int> slots; std::vector<TcLaunch> launches; double split_bytes, flops, bytes; };
+    std::vector<TcGroup> tc_groups;
     tc::Maps tcmaps;
     size_t tcp_next = 0;  // next free slot of tcp in this batch
     void check_device_flags();
@@ -185,7 +199,7 @@ class Engine {
     double span_hint = 1.0;          // first-range scale learned from earlier batches (run)
     DBuf<int> wl_off, wl_lb;
     std::vector<int> wl_host_off;    // host copy of the current round's work-list offsets
-    virtual void epilogue(const int* freqs_dev, int w, int nf) = 0;
+    virtual void epilogue(const int* freqs_dev, int w, int nf, cudaStream_t s) = 0;
     virtual size_t out_sizes(size_t* nt, size_t* nr, size_t* ns) const = 0;
 
     // learned cutoff: per-context model summaries, the device network, and
@@ -221,7 +235,7 @@ Engine* make_psv_engine(const dsm_psv_setup_t* const* s, int nsrc, const dsm_opt
 void launch_basis_tables(Engine& e, int lcap);
 void launch_interp_weights(Engine& e, const double* d_r, const double* d_rrsta);
 // complex64 records of frequencies [w0, w1) of a batch of nf into out32
-void launch_pack32(Engine& e, int nf, int w0, int w1, size_t per_t, size_t per_r, size_t per_s);
+void launch_pack32(Engine& e, int nf, int w0, int w1, size_t per_t, size_t per_r, size_t per_s, cudaStream_t s);
 
 }  // namespace dsm
 

@@ -428,10 +428,18 @@ __device__ __forceinline__ void split2f(float x, int fmt, uint16_t& hi, uint16_t
 }
 
 // FP32 rows whose length is a multiple of four: one warp per row, four
-// orders per lane and step (16-byte loads, 8-byte piece stores)
-__global__ void k_split_rows_f4(const float* __restrict__ A, int nrows, int per_w, int lcap,
-                                const int* __restrict__ nord, int kcap, int bk, uint16_t* __restrict__ P,
-                                size_t piece_stride, float* __restrict__ sa, int fmt) {
+// orders per lane and load (16-byte loads, 8-byte piece stores), SPLIT_U
+// loads in flight per lane.  Blocks of four warps with few registers: the
+// split of one frequency group runs on the SMs beside the contraction of
+// the previous one, which leaves about 11.7k registers per SM, so each lane
+// keeps several loads in flight instead of relying on many warps.
+constexpr int SPLIT_THREADS = 128;
+constexpr int SPLIT_U = 4;
+__global__ void __launch_bounds__(SPLIT_THREADS) k_split_rows_f4(const float* __restrict__ A, int nrows, int per_w,
+                                                                 int lcap, const int* __restrict__ nord, int kcap,
+                                                                 int bk, uint16_t* __restrict__ P,
+                                                                 size_t piece_stride, float* __restrict__ sa,
+                                                                 int fmt) {
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= nrows) return;
@@ -439,30 +447,48 @@ __global__ void k_split_rows_f4(const float* __restrict__ A, int nrows, int per_
     const int Kp = min(kcap, (K + bk - 1) / bk * bk);
     const float4* a4 = reinterpret_cast<const float4*>(A + (size_t)row * lcap);
     float mx = 0.0f;
-    for (int i = lane; 4 * i < K; i += 32) {
-        const float4 v = a4[i];
-        mx = fmaxf(mx, fabsf(v.x));
-        if (4 * i + 1 < K) mx = fmaxf(mx, fabsf(v.y));
-        if (4 * i + 2 < K) mx = fmaxf(mx, fabsf(v.z));
-        if (4 * i + 3 < K) mx = fmaxf(mx, fabsf(v.w));
+    for (int i0 = lane; 4 * i0 < K; i0 += 32 * SPLIT_U) {
+        float4 v[SPLIT_U];
+#pragma unroll
+        for (int u = 0; u < SPLIT_U; ++u) {
+            const int i = i0 + 32 * u;
+            v[u] = 4 * i < K ? a4[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+#pragma unroll
+        for (int u = 0; u < SPLIT_U; ++u) {
+            const int i = i0 + 32 * u;
+            if (4 * i < K) mx = fmaxf(mx, fabsf(v[u].x));
+            if (4 * i + 1 < K) mx = fmaxf(mx, fabsf(v[u].y));
+            if (4 * i + 2 < K) mx = fmaxf(mx, fabsf(v[u].z));
+            if (4 * i + 3 < K) mx = fmaxf(mx, fabsf(v[u].w));
+        }
     }
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     const int e = piece_exp((double)mx);
     if (lane == 0) sa[row] = __int_as_float((127 + e) << 23);
     uint2* ph = reinterpret_cast<uint2*>(P + (size_t)row * kcap);
     uint2* pl = reinterpret_cast<uint2*>(P + piece_stride + (size_t)row * kcap);
-    for (int i = lane; 4 * i < Kp; i += 32) {
-        float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (4 * i < K) v = a4[i];
-        const float x[4] = {v.x, v.y, v.z, v.w};
-        uint16_t h[4], lo[4];
+    for (int i0 = lane; 4 * i0 < Kp; i0 += 32 * SPLIT_U) {
+        float4 v[SPLIT_U];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            h[c] = lo[c] = 0;
-            if (4 * i + c < K) split2f(ldexpf(x[c], -e), fmt, h[c], lo[c]);
+        for (int u = 0; u < SPLIT_U; ++u) {
+            const int i = i0 + 32 * u;
+            v[u] = 4 * i < K ? a4[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
-        ph[i] = make_uint2((uint32_t)h[0] | ((uint32_t)h[1] << 16), (uint32_t)h[2] | ((uint32_t)h[3] << 16));
-        pl[i] = make_uint2((uint32_t)lo[0] | ((uint32_t)lo[1] << 16), (uint32_t)lo[2] | ((uint32_t)lo[3] << 16));
+#pragma unroll
+        for (int u = 0; u < SPLIT_U; ++u) {
+            const int i = i0 + 32 * u;
+            if (4 * i >= Kp) break;
+            const float x[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+            uint16_t h[4], lo[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                h[c] = lo[c] = 0;
+                if (4 * i + c < K) split2f(ldexpf(x[c], -e), fmt, h[c], lo[c]);
+            }
+            ph[i] = make_uint2((uint32_t)h[0] | ((uint32_t)h[1] << 16), (uint32_t)h[2] | ((uint32_t)h[3] << 16));
+            pl[i] = make_uint2((uint32_t)lo[0] | ((uint32_t)lo[1] << 16), (uint32_t)lo[2] | ((uint32_t)lo[3] << 16));
+        }
     }
 }
 
@@ -548,10 +574,14 @@ void split_fields(const void* A, int in_bytes, int nf, int rows, int lcap, const
     const int n = nf * rows;
     if (n <= 0) return;
     if (kcap % bk) throw Error(DSM_ERR_INVALID, "order capacity of the split fields is not a multiple of BK");
-    if (in_bytes == 4 && lcap % 4 == 0 && kcap % 4 == 0)
-        k_split_rows_f4<<<(n + 7) / 8, 256, 0, st>>>(static_cast<const float*>(A), n, rows, lcap, d_nord, kcap, bk,
-                                                     P, (size_t)F * rows * kcap, sa, piece_fmt);
-    else if (in_bytes == 4)
+    if (in_bytes == 4 && lcap % 4 == 0 && kcap % 4 == 0) {
+        // the SMs run the contraction with most of their shared memory: the
+        // split's blocks ask for the same carveout so they can run beside it
+        DSM_CUDA(cudaFuncSetAttribute(k_split_rows_f4, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
+        k_split_rows_f4<<<(n + SPLIT_THREADS / 32 - 1) / (SPLIT_THREADS / 32), SPLIT_THREADS, 0, st>>>(
+            static_cast<const float*>(A), n, rows, lcap, d_nord, kcap, bk, P, (size_t)F * rows * kcap, sa, piece_fmt);
+    } else if (in_bytes == 4)
         k_split_rows<float><<<(n + 7) / 8, 256, 0, st>>>(static_cast<const float*>(A), n, rows, lcap, d_nord, kcap,
                                                          bk, P, (size_t)F * rows * kcap, sa, piece_fmt);
     else

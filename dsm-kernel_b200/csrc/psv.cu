@@ -30,6 +30,7 @@
 //                ismall > 20 exit, SGTpsv-MPI.f90:606-609, 902-905).
 // The epilogue (TSGT / RSGT / SYNN from the l-contractions) is psv_epi.cu.
 #include <algorithm>
+#include <climits>
 #include <cstdlib>
 #include <cmath>
 #include <cstring>
@@ -1834,37 +1835,66 @@ __global__ void k_psv_scan(int nf, WorkList wl, int Lcap, int maxlmax, double ra
 // only keeps more rows.  Starting at the deepest source r_s, the first node
 // where E reaches X bounds the amplitude there by exp(-X) of the source's,
 // and a zero-displacement boundary there perturbs what reaches the source
-// and receivers above by about exp(-2X).  One thread per system, FP32 (a
-// bound, not a result); nodes: x = r, y = 1 / v^2 (huge in fluid), z = local
-// row of the node's first unknown.  kcut = that row less a margin of four,
-// at most kmax (below the source rows).
+// and receivers above by about exp(-2X).  FP32 (a bound, not a result);
+// nodes: x = r, y = 1 / v^2 (huge in fluid), z = local row of the node's
+// first unknown.  kcut = that row less a margin of four, at most kmax
+// (below the source rows).
+// kappa grows with l at every node, and so does E: a frequency's lowest
+// order in a warp has the lowest cut row of its orders there.  The warp
+// computes the cut rows of those systems only (one per frequency it holds),
+// each walk spread over the lanes: lane j takes the interval below node
+// base - j, a prefix sum over the lanes gives E at each of the 32 nodes, and
+// the first lane where E reaches X ends the walk.  Every lane takes the
+// warp's lowest cut row, where the factorisation of its 32 systems starts
+// anyway: lanes above it keep a few more rows than their own bound needs.
 __global__ void k_psv_cutrow(const float4* __restrict__ nodes, int ks, float X, double tlen,
                              const int* __restrict__ freqs, WorkList wl, int nsys, int kmax, int* __restrict__ kcut,
                              int* __restrict__ blkmin) {
-    const int sys = blockIdx.x * blockDim.x + threadIdx.x;
-    if (sys >= nsys) return;
+    const int sysv = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
+    const bool valid = sysv < nsys;
+    const int sys = valid ? sysv : nsys - 1;
     int w, l;
     wl_map(wl, sys, w, l);
-    const float om = (float)(2.0 * kPi * (double)freqs[w] / tlen);
-    const float lam2 = ((float)l + 0.5f) * ((float)l + 0.5f), om2 = om * om;
-    auto kappa = [&](float4 v) { return sqrtf(fmaxf(0.0f, lam2 / (v.x * v.x) - om2 * v.y)); };
-    float4 a = nodes[ks];
-    float ka = kappa(a), E = 0.0f;
-    int row = 1;
-    for (int k = ks - 1; k >= 0; --k) {
-        const float4 b = nodes[k];
-        const float kb = kappa(b);
-        E += 0.5f * (ka + kb) * (a.x - b.x);
-        if (E >= X) {
-            row = (int)b.z;
-            break;
+    const int wprev = __shfl_up_sync(0xffffffffu, w, 1);
+    unsigned lead = __ballot_sync(0xffffffffu, valid && (lane == 0 || wprev != w));
+    int kc = INT_MAX;
+    while (lead) {
+        const int src = __ffs(lead) - 1;
+        lead &= lead - 1;
+        const int ws = __shfl_sync(0xffffffffu, w, src), ls = __shfl_sync(0xffffffffu, l, src);
+        const float om = (float)(2.0 * kPi * (double)freqs[ws] / tlen);
+        const float lam2 = ((float)ls + 0.5f) * ((float)ls + 0.5f), om2 = om * om;
+        auto kappa = [&](float4 v) { return sqrtf(fmaxf(0.0f, lam2 / (v.x * v.x) - om2 * v.y)); };
+        float E = 0.0f;
+        int row = 1;
+        for (int base = ks; base >= 1; base -= 32) {
+            const int k = base - lane;  // this lane's interval: node k down to node k - 1
+            const bool in = k >= 1;
+            const float4 a = nodes[in ? k : 0];
+            const float ka = kappa(a);
+            float kb = __shfl_down_sync(0xffffffffu, ka, 1);
+            float4 b = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (in) b = nodes[k - 1];
+            if (lane == 31 && in) kb = kappa(b);
+            float inc = in ? 0.5f * (ka + kb) * (a.x - b.x) : 0.0f;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float t = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += t;
+            }
+            const unsigned hit = __ballot_sync(0xffffffffu, in && E + inc >= X);
+            if (hit) {
+                const int f = __ffs(hit) - 1;
+                row = (int)__shfl_sync(0xffffffffu, b.z, f);
+                break;
+            }
+            E += __shfl_sync(0xffffffffu, inc, 31);
         }
-        a = b;
-        ka = kb;
+        kc = min(kc, max(1, min(row - 4, kmax)));
     }
-    const int kc = max(1, min(row - 4, kmax));
+    if (!valid) return;
     kcut[sys] = kc;
-    atomicMin(&blkmin[sys / 128], kc);  // per 128-system block (a factorisation block)
+    if (lane == 0) atomicMin(&blkmin[sys / 128], kc);  // per 128-system block (a factorisation block)
 }
 
 // ---------------------------------------------------------------- engine
@@ -2318,7 +2348,6 @@ class PsvEngine : public Engine {
         const int lmin = lst_min();
         // Lst holds rows lmin .. n: kernels index rows from 0 off this base
         cd* const Lb = Lst.p - (size_t)lmin * 3 * nsys;
-        const double fac_bytes = (double)(n - lmin + 1) * 3 * 16.0 + (double)(n - ls_min + 1) * 16.0;
         const int nblk = (nsys + FAC_THREADS - 1) / FAC_THREADS;
         const int dmin = ls_min;  // pivots from the deepest source row up
         const int* kc = nullptr;
@@ -2332,6 +2361,7 @@ class PsvEngine : public Engine {
         // whole band: blocks go by their rank inside their frequency's order
         // range, one stream.
         std::vector<int> order(nblk);
+        std::vector<int> brow(nblk, 1);  // first factored row of each block (the cut's block minimum)
         int nlong = 0;
         if (depth_bound > 0.0 && ls_min > 9) {
             blkmin.reserve(nblk);
@@ -2343,7 +2373,10 @@ class PsvEngine : public Engine {
             std::vector<int> bm(nblk);
             DSM_CUDA(cudaMemcpyAsync(bm.data(), blkmin.p, sizeof(int) * nblk, cudaMemcpyDeviceToHost, st));
             DSM_CUDA(cudaStreamSynchronize(st));
-            for (int b = 0; b < nblk; ++b) order[b] = b;
+            for (int b = 0; b < nblk; ++b) {
+                order[b] = b;
+                brow[b] = std::max(1, std::min(bm[b], n));
+            }
             std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return bm[a] < bm[b]; });
             const int lim = (int)(0.4 * n);
             for (int b = 0; b < nblk; ++b) nlong += bm[b] < lim ? 1 : 0;
@@ -2369,8 +2402,21 @@ class PsvEngine : public Engine {
         const int lsf = tune.fwd_merge && ls0 > 3 && ls0 + 8 <= n ? ls0 : -1;
         const int fs = tune.fld_orders == 16 ? 16 : 32, frec = 32 / fs;
         // the solve chain of blocks bp[0 .. nb) on stream s
+        // the long recurrences' chain reports its kernels under their own
+        // names (..._long): its length bounds the solve phase
         auto chain = [&](cudaStream_t s, const int* bp, int nb) {
-            int id = kid("psv_factor");
+            const std::string sfx = s == st3 ? "_long" : "";
+            // algorithmic bytes count the rows each block factors and reads
+            // (from its first factored row, or the deepest row read, up)
+            const int* ob = order.data() + (bp - bperm.p);
+            double rows_fac = 0.0, rows_sub = 0.0;
+            for (int i = 0; i < nb; ++i) {
+                const int b = ob[i], nsb_b = std::min(FAC_THREADS, nsys - b * FAC_THREADS);
+                rows_fac += (double)(n - std::max(lmin, brow[b]) + 1) * nsb_b;
+                rows_sub += (double)(n - std::max(jmin_loc, brow[b]) + 1) * nsb_b;
+            }
+            auto kname = [&](const char* base) { return kid((std::string(base) + sfx).c_str()); };
+            int id = kname("psv_factor");
             kbegin(id, s);
             auto factor = [&](auto kern) {
                 kern<<<nb, FAC_THREADS, 0, s>>>(d, Prow.p, wl, nsys, lmin, Lb, tails.p, Dst.p, dmin, kc, bp, lsf,
@@ -2393,17 +2439,17 @@ class PsvEngine : public Engine {
                     else factor(k_psv_solve<false, 16, false>);
                 }
             }
-            kend(id, fac_bytes * std::min(nsys, nb * FAC_THREADS), 0.0, s);
+            kend(id, rows_fac * 3 * 16.0 + (double)(n - ls_min + 1) * 16.0 * std::min(nsys, nb * FAC_THREADS), 0.0,
+                 s);
             DSM_LAUNCH(*this);
             for (int k = 0; k < nsrc; ++k) {
                 const PsvDev& e = dsrc[k];
                 const int ls = e.jsrc - e.itmp + 1;
                 const double nsb = std::min(nsys, nb * FAC_THREADS);
                 const double fwd_bytes = (double)(n - ls + 1) * (4 * 16.0 + 3 * 16.0 + 16.0);
-                const double sub_bytes = (double)(n - jmin_loc + 1) * 3 * 16.0 + (double)(n - ls + 1) * 4 * 16.0 +
-                                         (double)ncap * NB * 16.0;
+                const double sub_bytes = (double)(n - ls + 1) * 4 * 16.0 + (double)ncap * NB * 16.0;
                 if (!(k == 0 && lsf > 0)) {  // otherwise done by the factorisation
-                    id = kid("psv_forward");
+                    id = kname("psv_forward");
                     kbegin(id, s);
                     if (mixed())
                         k_psv_fwd<true><<<nb, FAC_THREADS, 0, s>>>(e, nsys, ls, Lb, Dst.p, dmin, tails.p, Zst.p, bp);
@@ -2412,7 +2458,7 @@ class PsvEngine : public Engine {
                     kend(id, fwd_bytes * nsb, 0.0, s);
                     DSM_LAUNCH(*this);
                 }
-                id = kid("psv_substitution");
+                id = kname("psv_substitution");
                 kbegin(id, s);
                 if (mixed())
                     k_psv_up<true><<<nb, UP_THREADS, UP_SMEM, s>>>(e, nsys, jmin_loc, capmap.p, caplist.p, Lb, Zst.p,
@@ -2420,9 +2466,9 @@ class PsvEngine : public Engine {
                 else
                     k_psv_up<false><<<nb, UP_THREADS, UP_SMEM, s>>>(e, nsys, jmin_loc, capmap.p, caplist.p, Lb,
                                                                    Zst.p, tails.p, Xcap.p, kc, bp, Xprobe.p);
-                kend(id, sub_bytes * nsb, 0.0, s);
+                kend(id, rows_sub * 3 * 16.0 + sub_bytes * nsb, 0.0, s);
                 DSM_LAUNCH(*this);
-                id = kid("psv_source_coef");
+                id = kname("psv_source_coef");
                 kbegin(id, s);
                 double* amk = amps.p + (size_t)k * F * Lcap;
                 k_psv_coef<<<nb, 128, 0, s>>>(e, fr_, wl, nsys, ab.p + (size_t)k * F * 320, co.p, rsgt_sw,
@@ -2430,7 +2476,7 @@ class PsvEngine : public Engine {
                 kend(id, 0.0, 0.0, s);
                 DSM_LAUNCH(*this);
                 dim3 grid((unsigned)(nb * (128 / fs)), (R + 1 + 4 * frec - 1) / (4 * frec));
-                id = kid("psv_fields");
+                id = kname("psv_fields");
                 kbegin(id, s);
                 if (afld_bytes == 4) {
                     auto kern = fs == 16 ? k_psv_fields<true, 16> : k_psv_fields<true, 32>;
@@ -2443,7 +2489,8 @@ class PsvEngine : public Engine {
                 }
                 kend(id, 0.0, 0.0, s);
                 DSM_LAUNCH(*this);
-                stats.solve_bytes += (k == 0 ? fac_bytes : 0.0) * nsb + (fwd_bytes + sub_bytes) * nsb;
+                stats.solve_bytes += (k == 0 ? rows_fac * 3 * 16.0 + (double)(n - ls_min + 1) * 16.0 * nsb : 0.0) +
+                                     rows_sub * 3 * 16.0 + (fwd_bytes + sub_bytes) * nsb;
             }
         };
         if (nlong > 0) {
@@ -2470,7 +2517,7 @@ class PsvEngine : public Engine {
         kend(id, 0.0, 0.0);
     }
 
-    void epilogue(const int* fr_, int w, int nf) override {
+    void epilogue(const int* fr_, int w, int nf, cudaStream_t s) override {
         (void)nf;
         psvk::EpiDev e{};
         e.R = R;
@@ -2486,14 +2533,14 @@ class PsvEngine : public Engine {
         e.fr = d.fr;
         e.status = dstatus();
         int id = kid("psv_epilogue");
-        kbegin(id);
+        kbegin(id, s);
         const bool tc = mixed();
         const void* c0 = tc ? (const void*)c32(w, 0) : (const void*)c64(0);
         const void* c1 = tc ? (const void*)c32(w, 1) : (const void*)c64(1);
         const void* c2 = tc ? (const void*)c32(w, 2) : (const void*)c64(2);
         psvk::launch_epilogue(e, w, th.x.p, th.s.p, th.pole.p, fr_, c0, c1, c2, tc, out_t_src(),
-                              rsgt_sw ? out_r_src() : nullptr, synn_sw ? out_s_src() : nullptr, st);
-        kend(id, 0.0, 0.0);
+                              rsgt_sw ? out_r_src() : nullptr, synn_sw ? out_s_src() : nullptr, s);
+        kend(id, 0.0, 0.0, s);
         DSM_LAUNCH(*this);
     }
 };

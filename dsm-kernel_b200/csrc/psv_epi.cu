@@ -16,7 +16,10 @@ namespace dsm {
 namespace psvk {
 namespace {
 
-constexpr int EPI_THREADS = 128;
+// 64-thread blocks: on the mixed path (at most 127 registers, 8k per
+// block) the epilogue of one frequency group runs on the SMs beside the
+// tensor-core contraction of the next (320 threads x 168 registers)
+constexpr int EPI_THREADS = 64;
 
 template <class RL>
 struct PointConst {
@@ -305,6 +308,12 @@ void launch_t(const EpiDev& d, int w, const double* thx, const double* ths, cons
     const TC *c0 = static_cast<const TC*>(C0), *c1 = static_cast<const TC*>(C1), *c2 = static_cast<const TC*>(C2);
     const int n = d.Th * d.R;
     const unsigned grid = (unsigned)((n + EPI_THREADS - 1) / EPI_THREADS);
+    // the mixed path's epilogue runs beside the tensor-core contraction,
+    // whose SMs hold most of their shared memory: the same carveout
+    for (const void* f : {(const void*)k_psv_epi<TC, RL, true>, (const void*)k_psv_epi<TC, RL, false>,
+                          (const void*)k_psv_epi_surf<TC, RL>})
+        DSM_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
     if (rsgt)
         k_psv_epi<TC, RL, true><<<grid, EPI_THREADS, 0, st>>>(d, w, thx, ths, pole, freqs, c0, c1, c2, tsgt, rsgt);
     else

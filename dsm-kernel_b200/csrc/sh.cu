@@ -694,20 +694,24 @@ class ShEngine : public Engine {
         DSM_LAUNCH(*this);
     }
 
-    void epilogue(const int* fr, int w, int nf) override {
+    void epilogue(const int* fr, int w, int nf, cudaStream_t s) override {
         (void)fr; (void)nf;
         int n = Th * (R + 1);
         int id = kid("sh_epilogue");
-        kbegin(id);
-        if (mixed())
-            k_sh_epi<float><<<(n + 127) / 128, 128, 0, st>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p, c32(w, 1),
-                                                             c32(w, 2), out_t.p, out_r.p,
-                                                             synn_sw ? out_s.p : nullptr, dstatus());
-        else
-            k_sh_epi<double><<<(n + 127) / 128, 128, 0, st>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p, c64(1),
-                                                              c64(2), out_t.p, out_r.p,
-                                                              synn_sw ? out_s.p : nullptr, dstatus());
-        kend(id, 0.0, 0.0);
+        kbegin(id, s);
+        // 64-thread blocks (about 10.7k registers): the mixed path's
+        // epilogue runs beside the tensor-core contraction's CTAs
+        if (mixed()) {
+            DSM_CUDA(cudaFuncSetAttribute(k_sh_epi<float>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          (int)cudaSharedmemCarveoutMaxShared));
+            k_sh_epi<float><<<(n + 63) / 64, 64, 0, s>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p, c32(w, 1),
+                                                         c32(w, 2), out_t.p, out_r.p,
+                                                         synn_sw ? out_s.p : nullptr, dstatus());
+        } else
+            k_sh_epi<double><<<(n + 63) / 64, 64, 0, s>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p, c64(1),
+                                                          c64(2), out_t.p, out_r.p,
+                                                          synn_sw ? out_s.p : nullptr, dstatus());
+        kend(id, 0.0, 0.0, s);
         DSM_LAUNCH(*this);
     }
 };

@@ -102,7 +102,7 @@ class Stats(C.Structure):
                 ("launches", C.c_longlong), ("systems", C.c_longlong),
                 ("orders_used", C.c_longlong), ("orders_padded", C.c_longlong),
                 ("lsum_flops", C.c_double), ("solve_bytes", C.c_double),
-                ("nk", C.c_int), ("kern", KStat * 12), ("solve_rounds", C.c_longlong),
+                ("nk", C.c_int), ("kern", KStat * 24), ("solve_rounds", C.c_longlong),
                 ("freqs_extended", C.c_longlong)]
 
     def kernels(self):

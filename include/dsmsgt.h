@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define DSM_ABI_VERSION 2
+#define DSM_ABI_VERSION 3
 
 /* return codes */
 #define DSM_OK               0
@@ -259,7 +259,7 @@ int dsm_abi_version(void);
 
 /* Per-kernel device time of the last run, recorded with CUDA events on the
  * context's stream when profiling is on (dsm_set_profiling). */
-#define DSM_MAX_KSTATS 12
+#define DSM_MAX_KSTATS 24
 typedef struct dsm_kstat {
     char      name[32];
     double    ms;          /* summed device time                          */

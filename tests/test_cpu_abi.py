@@ -28,7 +28,7 @@ def test_library_exports_every_declared_function(built, header):
 
 def test_abi_version_and_error_strings(built):
     L = dsmsgt.lib()
-    assert L.dsm_abi_version() == 2
+    assert L.dsm_abi_version() == 3
     for code in range(0, 8):
         s = L.dsm_strerror(code)
         assert s and len(s) >= 2
