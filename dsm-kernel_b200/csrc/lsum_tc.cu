@@ -429,11 +429,12 @@ __device__ __forceinline__ void split2f(float x, int fmt, uint16_t& hi, uint16_t
 
 // FP32 rows whose length is a multiple of four: one warp per row, four
 // orders per lane and load (16-byte loads, 8-byte piece stores), SPLIT_U
-// loads in flight per lane.  Blocks of four warps with few registers: the
-// split of one frequency group runs on the SMs beside the contraction of
-// the previous one, which leaves about 11.7k registers per SM, so each lane
-// keeps several loads in flight instead of relying on many warps.
-constexpr int SPLIT_THREADS = 128;
+// loads in flight per lane.  One-warp blocks: the split of one frequency
+// group runs on the SMs beside the contraction of the previous one, whose
+// ten warps leave registers on only two of an SM's four schedulers (each
+// scheduler has its own quarter of the register file), and a block's warps
+// go to different schedulers.
+constexpr int SPLIT_THREADS = 32;
 constexpr int SPLIT_U = 4;
 __global__ void __launch_bounds__(SPLIT_THREADS) k_split_rows_f4(const float* __restrict__ A, int nrows, int per_w,
                                                                  int lcap, const int* __restrict__ nord, int kcap,

@@ -16,10 +16,13 @@ namespace dsm {
 namespace psvk {
 namespace {
 
-// 64-thread blocks: on the mixed path (at most 127 registers, 8k per
-// block) the epilogue of one frequency group runs on the SMs beside the
-// tensor-core contraction of the next (320 threads x 168 registers)
-constexpr int EPI_THREADS = 64;
+// Threads per block.  Mixed path (FP32 contraction outputs): one-warp
+// blocks, because its epilogue of one frequency group runs on the SMs beside
+// the tensor-core contraction of the next, whose ten warps of 168 registers
+// leave room on only two of an SM's four schedulers (each has its own
+// quarter of the register file).  Plain path: 128.
+template <class TC>
+constexpr int epi_threads() { return sizeof(TC) == 4 ? 32 : 128; }
 
 template <class RL>
 struct PointConst {
@@ -83,7 +86,7 @@ struct Fields {
 
 // displacement fields of the receivers below the surface
 template <class TC, class RL, bool BACK>
-__global__ void __launch_bounds__(EPI_THREADS) k_psv_epi(EpiDev d, int w, const double* __restrict__ thx,
+__global__ void __launch_bounds__(epi_threads<TC>()) k_psv_epi(EpiDev d, int w, const double* __restrict__ thx,
                                                          const double* __restrict__ ths,
                                                          const int* __restrict__ pole,
                                                          const int* __restrict__ freqs,
@@ -241,7 +244,7 @@ __global__ void __launch_bounds__(EPI_THREADS) k_psv_epi(EpiDev d, int w, const 
 
 // surface displacement (utosynn): one thread per distance
 template <class TC, class RL>
-__global__ void __launch_bounds__(EPI_THREADS) k_psv_epi_surf(EpiDev d, int w, const double* __restrict__ thx,
+__global__ void __launch_bounds__(epi_threads<TC>()) k_psv_epi_surf(EpiDev d, int w, const double* __restrict__ thx,
                                                               const double* __restrict__ ths,
                                                               const int* __restrict__ pole,
                                                               const TC* __restrict__ C0, const TC* __restrict__ C1,
@@ -307,6 +310,7 @@ void launch_t(const EpiDev& d, int w, const double* thx, const double* ths, cons
               cudaStream_t st) {
     const TC *c0 = static_cast<const TC*>(C0), *c1 = static_cast<const TC*>(C1), *c2 = static_cast<const TC*>(C2);
     const int n = d.Th * d.R;
+    constexpr int EPI_THREADS = epi_threads<TC>();
     const unsigned grid = (unsigned)((n + EPI_THREADS - 1) / EPI_THREADS);
     // the mixed path's epilogue runs beside the tensor-core contraction,
     // whose SMs hold most of their shared memory: the same carveout
