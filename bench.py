@@ -63,15 +63,28 @@ WORKLOADS = {
 # kernel on a workload, from an ncu capture of that kernel; the line reports
 # where each figure came from next to it, and null where none was taken.
 TRAFFIC = {
-    ("psv1024", "lsum_tc"): (14.07e9, "ncu capture of the bench's own launches (psv1024, 16 frequencies)"),
     ("catalogue", "cat_interp"): (0.672e9, "ncu capture of one launch (catalogue workload)"),
     ("catalogue", "cat_omega"): (0.598e9, "ncu capture of one launch (catalogue workload)"),
 }
+# Per-unit DRAM bytes of a kernel whose full-size launch is too large for an
+# ncu capture with several metrics: measured on a small case of the same
+# workload and scaled to a launch by the units it processes (reads by the
+# orders contracted, writes by the frequencies whose output it writes).
+TRAFFIC_PER_UNIT = {
+    ("psv2048", "lsum_tc"): (0.966e9 / 3918, 0.208e9,
+                             "ncu capture of a one-frequency launch of this workload (3918 orders: 0.966 GB read, "
+                             "0.208 GB written), scaled to the launch by orders (reads) and frequencies (writes)"),
+}
 
 
-def traffic(name, kernel):
+def traffic(name, kernel, orders=None, freqs=None):
     v = TRAFFIC.get((name, kernel))
-    return (v[0], v[1]) if v else (None, "not captured for this workload")
+    if v:
+        return v[0], v[1]
+    u = TRAFFIC_PER_UNIT.get((name, kernel))
+    if u and orders is not None and freqs is not None:
+        return u[0] * orders + u[1] * freqs, u[2]
+    return None, "not captured for this workload"
 
 
 def workload(name: str):
@@ -737,7 +750,9 @@ def main():
     roof = None
     if dom:
         name, (ms, n, b, f) = dom
-        tr, tr_src = traffic(desc["name"], name)
+        sol = run["solve"]
+        tr, tr_src = traffic(desc["name"], name, orders=sol["orders_used"] / max(n, 1),
+                             freqs=args.steps * args.per_step / max(n, 1))
         if f > 0:
             # algorithmic flops (one real product per row, column and order up
             # to the cutoff); the split path runs three fp16 piece products

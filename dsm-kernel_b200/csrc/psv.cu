@@ -1867,15 +1867,26 @@ __global__ void k_psv_cutrow(const float4* __restrict__ nodes, int ks, float X, 
         auto kappa = [&](float4 v) { return sqrtf(fmaxf(0.0f, lam2 / (v.x * v.x) - om2 * v.y)); };
         float E = 0.0f;
         int row = 1;
+        // node max(k, 0) of this pass, and of the next pass (in flight
+        // while this one runs); node k - 1 is the next lane's node, or for
+        // lane 31 lane 0's node of the next pass
+        float4 an = nodes[max(ks - lane, 0)];
         for (int base = ks; base >= 1; base -= 32) {
             const int k = base - lane;  // this lane's interval: node k down to node k - 1
             const bool in = k >= 1;
-            const float4 a = nodes[in ? k : 0];
+            const float4 a = an;
+            an = nodes[max(base - 32 - lane, 0)];
             const float ka = kappa(a);
+            float bx = __shfl_down_sync(0xffffffffu, a.x, 1), bz = __shfl_down_sync(0xffffffffu, a.z, 1);
             float kb = __shfl_down_sync(0xffffffffu, ka, 1);
-            float4 b = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (in) b = nodes[k - 1];
-            if (lane == 31 && in) kb = kappa(b);
+            const float nx = __shfl_sync(0xffffffffu, an.x, 0), ny = __shfl_sync(0xffffffffu, an.y, 0),
+                        nz = __shfl_sync(0xffffffffu, an.z, 0);
+            if (lane == 31) {
+                bx = nx;
+                bz = nz;
+                kb = kappa(make_float4(nx, ny, nz, 0.0f));
+            }
+            const float4 b = make_float4(bx, 0.0f, bz, 0.0f);
             float inc = in ? 0.5f * (ka + kb) * (a.x - b.x) : 0.0f;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
