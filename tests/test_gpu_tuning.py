@@ -105,3 +105,25 @@ def test_request_rejects_a_context_twice(built):
         dsmsgt.run_request([ctx, ctx], [[1], [2]])
     assert ei.value.code == dsmsgt.DSM_ERR_INVALID
     ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["psv", "sh"])
+def test_mixed_outputs_identical_across_lsum_groups(built, mode, monkeypatch):
+    """The mixed l-sum runs in frequency groups (split, tensor-core
+    contraction and epilogue of different groups on three streams); the
+    grouping changes only the order of the launches, so the outputs are
+    bit-identical for any group count, with and without complex64 records."""
+    s = dsmsgt.Setup(psv_small() if mode == "psv" else sh_small(), mode)
+    freqs = [1, 9, 20, 33, 47, 64]
+    runs = []
+    for g in ("1", "2", "4", "8"):
+        monkeypatch.setenv("DSM_LSUM_GROUPS", g)
+        ctx = dsmsgt.Context(s, precision=dsmsgt.DSM_PREC_MIXED, freq_batch=6)
+        runs.append((ctx.run(freqs), ctx.run(freqs, want32=True)))
+        ctx.close()
+    for r, r32 in runs[1:]:
+        _same(r, runs[0][0])
+        _same(r32[:4], runs[0][1][:4])
+        for x, y in zip(r32[4], runs[0][1][4]):
+            assert np.array_equal(x, y)
