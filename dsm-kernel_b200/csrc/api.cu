@@ -51,9 +51,7 @@ void Engine::init_common(int dev) {
         DSM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
         DSM_CUDA(cudaStreamCreateWithPriority(&stt, cudaStreamNonBlocking, hi));
         DSM_CUDA(cudaStreamCreateWithFlags(&sts, cudaStreamNonBlocking));
-        DSM_CUDA(cudaStreamCreateWithFlags(&ste, cudaStreamNonBlocking));
         for (auto& e : ev_sp) DSM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        for (auto& e : ev_td) DSM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         DSM_CUDA(cudaEventCreateWithFlags(&ev_lp, cudaEventDisableTiming));
         DSM_CUDA(cudaEventCreateWithFlags(&ev_lj, cudaEventDisableTiming));
     }
@@ -88,11 +86,9 @@ Engine::~Engine() {
     if (stc) { cudaStreamSynchronize(stc); cudaStreamDestroy(stc); }
     for (auto& e : ev_grp)
         if (e) cudaEventDestroy(e);
-    for (cudaStream_t* s : {&sts, &ste, &stt})
+    for (cudaStream_t* s : {&sts, &stt})
         if (*s) { cudaStreamSynchronize(*s); cudaStreamDestroy(*s); }
     for (auto& e : ev_sp)
-        if (e) cudaEventDestroy(e);
-    for (auto& e : ev_td)
         if (e) cudaEventDestroy(e);
     if (ev_lp) cudaEventDestroy(ev_lp);
     if (ev_lj) cudaEventDestroy(ev_lj);
@@ -207,6 +203,7 @@ void Engine::lsum_prepare(int nf, const std::vector<int>& nord) {
         if (!rows_m[m]) continue;
         Apc[m].reserve((size_t)2 * F * rows_m[m] * kcA);
         sA[m].reserve((size_t)F * rows_m[m]);
+        lnzA[m].reserve((size_t)F * rows_m[m]);
     }
     Cmix.reserve((size_t)F * c_total());
     d_nord.upload(nord, st);
@@ -226,6 +223,15 @@ void Engine::lsum_prepare(int nf, const std::vector<int>& nord) {
 void Engine::lsum_plan(const std::vector<std::vector<int>>& groups, const std::vector<int>& nord) {
     tc_groups.clear();
     std::vector<tc::Problem> all;
+    {  // row-tile entries of every problem (two row groups per |m| and frequency)
+        size_t ntm = 0;
+        for (const auto& slots : groups)
+            for (size_t k = 0; k < slots.size(); ++k)
+                for (int m = m_lo; m <= 2; ++m)
+                    ntm += (size_t)(rows_m[m] + 2 * tc::BM) / tc::BM;
+        tcKb.reserve(std::max<size_t>(ntm, 1));
+    }
+    size_t kboff = 0;
     for (const auto& slots : groups) {
         TcGroup G{slots, {}, 0.0, 0.0, 0.0};
         // per (frequency, |m|): the leading rows against all 2 Th basis
@@ -253,6 +259,9 @@ void Engine::lsum_plan(const std::vector<std::vector<int>>& groups, const std::v
                     P.sa = sA[m].p + (size_t)w * rows_m[m] + row0;
                     P.sb = sB[m].p;
                     P.ldc = rows_m[m];
+                    P.lz = lnzA[m].p + (size_t)w * rows_m[m] + row0;
+                    P.kb = tcKb.p + kboff;
+                    kboff += (size_t)(M + tc::BM - 1) / tc::BM;
                     hp.push_back(P);
                     // algorithmic: one real product per (row, column, order) up to
                     // the cutoff (the tensor cores run three piece products on
@@ -288,10 +297,9 @@ void Engine::lsum_plan(const std::vector<std::vector<int>>& groups, const std::v
     tcp_next += all.size();
 }
 
-// Group g of the mixed l-sum: split of its field matrices on sts (after the
-// previous group's split), then its contraction launches on stt once the
-// split is done.
-void Engine::lsum_group(int g) {
+// Split of group g of the mixed l-sum (field pieces, row scales, each row
+// tile's order blocks) on sts.
+void Engine::lsum_split(int g) {
     const TcGroup& G = tc_groups[(size_t)g];
     if (G.slots.empty()) return;
     int id = kid("lsum_split");
@@ -309,15 +317,24 @@ void Engine::lsum_group(int g) {
             const char* A =
                 reinterpret_cast<const char*>(Afld[m].p) + ((size_t)src * F + w0) * rw * Lcap * afld_bytes;
             tc::split_fields(A, afld_bytes, n, rows_m[m], Lcap, d_nord.p + w0, Apc[m].p + (size_t)w0 * rw * kcA,
-                             sA[m].p + (size_t)w0 * rw, kcA, F, tc_fmt, tc_bk, sts);
+                             sA[m].p + (size_t)w0 * rw, kcA, F, tc_fmt, tc_bk, sts, lnzA[m].p + (size_t)w0 * rw);
             launches++;
         }
         i = j;
     }
+    // each row tile's order blocks from its rows' last nonzero orders
+    for (const TcLaunch& L : G.launches) {
+        tc::tile_orders(tcp.p + L.first, L.np, tc_bk, sts);
+        launches++;
+    }
     kend(id, G.split_bytes, 0.0, sts);
-    DSM_CUDA(cudaEventRecord(ev_sp[g % MAX_OUT_GROUPS], sts));
-    DSM_CUDA(cudaStreamWaitEvent(stt, ev_sp[g % MAX_OUT_GROUPS], 0));
-    id = kid("lsum_tc");
+}
+
+// Tensor-core contraction launches of group g on stt.
+void Engine::lsum_contract(int g) {
+    const TcGroup& G = tc_groups[(size_t)g];
+    if (G.slots.empty()) return;
+    const int id = kid("lsum_tc");
     kbegin(id, stt);
     const uint32_t fl = tc_flags | (test_tc_stall ? tc::TC_TEST_STALL : 0u);
     const unsigned long long wait_ns = test_tc_stall ? 20000000ull : tc::WAIT_NS;
@@ -780,11 +797,13 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
                 DSM_CUDA(cudaStreamWaitEvent(st, ev_grp[0], 0));
             }
             // Groups of batch slots.  Plain path: consecutive slots.  Mixed
-            // path: group g's split (sts) runs while group g-1 is contracted
-            // (stt), and its epilogue and records (ste) while group g+1 is,
-            // so the groups carry equal contraction work (slots dealt by
-            // their cutoff, heaviest first, in serpentine order) and the
-            // lightest goes first (its split is the one nothing hides).
+            // path: the splits of all groups first (sts), then each group's
+            // contraction and epilogue in order on stt, so that the complex64
+            // records of a group go to the host (stc) while later groups are
+            // contracted.  Kernels beside the contraction's CTAs made
+            // almost no progress, so nothing runs beside it.  The groups
+            // carry equal contraction work (slots dealt by their cutoff,
+            // heaviest first, in serpentine order).
             std::vector<std::vector<int>> groups(ngrp);
             if (mixed()) {
                 std::vector<int> byw(nf);
@@ -813,15 +832,13 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
                 DSM_CUDA(cudaEventRecord(ev_lp, st));
                 DSM_CUDA(cudaStreamWaitEvent(sts, ev_lp, 0));
                 DSM_CUDA(cudaStreamWaitEvent(stt, ev_lp, 0));
-                DSM_CUDA(cudaStreamWaitEvent(ste, ev_lp, 0));
-                se = ste;
+                for (int g = 0; g < ngrp; ++g) lsum_split(g);
+                DSM_CUDA(cudaEventRecord(ev_sp[0], sts));
+                DSM_CUDA(cudaStreamWaitEvent(stt, ev_sp[0], 0));
+                se = stt;
             }
             for (int g = 0; g < ngrp; ++g) {
-                if (mixed()) {
-                    lsum_group(g);
-                    DSM_CUDA(cudaEventRecord(ev_td[g], stt));
-                    DSM_CUDA(cudaStreamWaitEvent(ste, ev_td[g], 0));
-                }
+                if (mixed()) lsum_contract(g);
                 for (int w : groups[g]) {
                     stats.orders_used += hs[w].norders;
                     if (!mixed())
@@ -862,8 +879,8 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
                     }
                 }
             }
-            if (mixed()) {  // st continues after the last group's epilogue (and so its contraction)
-                DSM_CUDA(cudaEventRecord(ev_lj, ste));
+            if (mixed()) {  // st continues after the last group's epilogue
+                DSM_CUDA(cudaEventRecord(ev_lj, stt));
                 DSM_CUDA(cudaStreamWaitEvent(st, ev_lj, 0));
             }
             // --- 5: outputs

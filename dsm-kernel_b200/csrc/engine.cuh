@@ -57,14 +57,14 @@ class Engine {
     cudaStream_t stc = nullptr;
     static constexpr int MAX_OUT_GROUPS = 8;
     cudaEvent_t ev_grp[MAX_OUT_GROUPS] = {};
-    // mixed l-sum pipeline over groups of a batch's frequencies: the split
-    // of the next group (sts) and the epilogue of the previous one (ste) run
-    // beside the tensor-core contraction of the current one (stt, high
-    // priority, so its CTAs are placed first as the other blocks retire)
-    cudaStream_t sts = nullptr, ste = nullptr, stt = nullptr;
-    cudaEvent_t ev_sp[MAX_OUT_GROUPS] = {}, ev_td[MAX_OUT_GROUPS] = {};
+    // mixed l-sum of a batch in frequency groups: the splits of all groups
+    // (sts), then each group's contraction and epilogue in order (stt, high
+    // priority), the records of a group to the host (stc) while later
+    // groups run
+    cudaStream_t sts = nullptr, stt = nullptr;
+    cudaEvent_t ev_sp[MAX_OUT_GROUPS] = {};
     cudaEvent_t ev_lp = nullptr, ev_lj = nullptr;
-    int lsum_groups = 4;             // frequency groups of the pipeline (a batch without host records)
+    int lsum_groups = 1;             // frequency groups of a batch without host records (DSM_LSUM_GROUPS)
     bool side_pending = false;
     cublasHandle_t cub = nullptr;
     cudaEvent_t ev[8] = {};
@@ -151,6 +151,8 @@ class Engine {
     DBuf<uint16_t> Bpc[3];           // [2][2Th][kcB]
     DBuf<float> sB[3];               // [2Th]
     DBuf<float> Cmix;                // [F][c_total] column-major blocks
+    DBuf<int> lnzA[3];               // [F][rows]: one past each field row's last nonzero order
+    DBuf<int> tcKb;                  // order blocks of each row tile of the batch's problems
     DBuf<tc::Problem> tcp;
     DBuf<int> d_nord;
     DBuf<int> dflags;                // status words (DEV_WORD_TC, DEV_WORD_STATUS)
@@ -164,8 +166,9 @@ class Engine {
     void lsum_prepare(int nf, const std::vector<int>& norders);
     // problem lists of all groups (each a list of batch slots), one upload
     void lsum_plan(const std::vector<std::vector<int>>& groups, const std::vector<int>& norders);
-    // group g: split on sts, contraction launches on stt
-    void lsum_group(int g);
+    // group g: split (sts), contraction launches (stt)
+    void lsum_split(int g);
+    void lsum_contract(int g);
     struct TcLaunch { size_t first; int np, tiles; };
     struct TcGroup { std::vector<int> slots; std::vector<TcLaunch> launches; double split_bytes, flops, bytes; };
     std::vector<TcGroup> tc_groups;

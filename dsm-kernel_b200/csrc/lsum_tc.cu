@@ -212,7 +212,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                 int mt, nt;
                 decode(ps, np, t, p, mt, nt);
                 const Problem& P = ps[p];
-                for (int kb = 0; kb < P.kblocks; ++kb, ++it) {
+                const int kbn = P.kb ? max(0, min(P.kb[mt], P.kblocks)) : P.kblocks;  // this row tile's order blocks
+                for (int kb = 0; kb < kbn; ++kb, ++it) {
                     const int s = it % STAGES;
                     const uint32_t ph = (it / STAGES) & 1;
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag, wait_ns)) {
@@ -222,7 +223,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
                     // test hook: CTA 0 issues nothing for its first stage
                     if ((flags & TC_TEST_STALL) && blockIdx.x == 0 && it == 0) continue;
                     unsigned char* sp = base + s * STAGE;
-                    const int x = (reverse ? P.kblocks - 1 - kb : kb) * BK;
+                    const int x = (reverse ? kbn - 1 - kb : kb) * BK;
                     mbar_expect_tx(&full[s], STAGE);
                     tma_a(&maps.a[P.amap], sp, &full[s], x, P.row0 + mt * BM, P.z, 0);
                     tma_a(&maps.a[P.amap], sp + A_BYTES, &full[s], x, P.row0 + mt * BM, P.z, 1);
@@ -243,7 +244,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 int mt, nt;
                 decode(ps, np, t, p, mt, nt);
-                const int kbn = ps[p].kblocks, ch = chunk > 0 ? chunk : kbn;
+                const int kbn = ps[p].kb ? max(0, min(ps[p].kb[mt], ps[p].kblocks)) : ps[p].kblocks;
+                const int ch = chunk > 0 ? chunk : max(kbn, 1);
                 // the last column tile of a contraction runs with N cut to
                 // its columns (a multiple of 16): no MMA time on padding
                 const int nrem = ps[p].N - nt * BN;
@@ -305,7 +307,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             int mt, nt;
             decode(ps, np, t, p, mt, nt);
             const Problem& P = ps[p];
-            const int kbn = P.kblocks, ch = chunk > 0 ? chunk : kbn, nch = (kbn + ch - 1) / ch;
+            const int kbn = P.kb ? max(0, min(P.kb[mt], P.kblocks)) : P.kblocks, ch = chunk > 0 ? chunk : max(kbn, 1);
+            const int nch = (kbn + ch - 1) / ch;
             double acc[64];
 #pragma unroll
             for (int j = 0; j < 64; ++j) acc[j] = 0.0;
@@ -440,7 +443,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_split_rows_f4(const float* __
                                                                  int lcap, const int* __restrict__ nord, int kcap,
                                                                  int bk, uint16_t* __restrict__ P,
                                                                  size_t piece_stride, float* __restrict__ sa,
-                                                                 int fmt) {
+                                                                 int fmt, int* __restrict__ lnz) {
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= nrows) return;
@@ -448,6 +451,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_split_rows_f4(const float* __
     const int Kp = min(kcap, (K + bk - 1) / bk * bk);
     const float4* a4 = reinterpret_cast<const float4*>(A + (size_t)row * lcap);
     float mx = 0.0f;
+    int last = 0;  // one past the last nonzero order
     for (int i0 = lane; 4 * i0 < K; i0 += 32 * SPLIT_U) {
         float4 v[SPLIT_U];
 #pragma unroll
@@ -458,15 +462,22 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_split_rows_f4(const float* __
 #pragma unroll
         for (int u = 0; u < SPLIT_U; ++u) {
             const int i = i0 + 32 * u;
-            if (4 * i < K) mx = fmaxf(mx, fabsf(v[u].x));
-            if (4 * i + 1 < K) mx = fmaxf(mx, fabsf(v[u].y));
-            if (4 * i + 2 < K) mx = fmaxf(mx, fabsf(v[u].z));
-            if (4 * i + 3 < K) mx = fmaxf(mx, fabsf(v[u].w));
+            const float x[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (4 * i + c < K) {
+                    mx = fmaxf(mx, fabsf(x[c]));
+                    if (x[c] != 0.0f) last = 4 * i + c + 1;
+                }
         }
     }
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    last = __reduce_max_sync(0xffffffffu, last);
     const int e = piece_exp((double)mx);
-    if (lane == 0) sa[row] = __int_as_float((127 + e) << 23);
+    if (lane == 0) {
+        sa[row] = __int_as_float((127 + e) << 23);
+        if (lnz) lnz[row] = last;
+    }
     uint2* ph = reinterpret_cast<uint2*>(P + (size_t)row * kcap);
     uint2* pl = reinterpret_cast<uint2*>(P + piece_stride + (size_t)row * kcap);
     for (int i0 = lane; 4 * i0 < Kp; i0 += 32 * SPLIT_U) {
@@ -497,7 +508,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_split_rows_f4(const float* __
 template <class TIN>
 __global__ void k_split_rows(const TIN* __restrict__ A, int nrows, int per_w, int lcap,
                              const int* __restrict__ nord, int kcap, int bk, uint16_t* __restrict__ P,
-                             size_t piece_stride, float* __restrict__ sa, int fmt) {
+                             size_t piece_stride, float* __restrict__ sa, int fmt, int* __restrict__ lnz) {
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= nrows) return;
@@ -505,10 +516,19 @@ __global__ void k_split_rows(const TIN* __restrict__ A, int nrows, int per_w, in
     const int Kp = min(kcap, (K + bk - 1) / bk * bk);
     const TIN* a = A + (size_t)row * lcap;
     double mx = 0.0;
-    for (int l = lane; l < K; l += 32) mx = fmax(mx, fabs((double)a[l]));
+    int last = 0;  // one past the last nonzero order
+    for (int l = lane; l < K; l += 32) {
+        const double x = (double)a[l];
+        mx = fmax(mx, fabs(x));
+        if (x != 0.0) last = l + 1;
+    }
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    last = __reduce_max_sync(0xffffffffu, last);
     const int e = piece_exp(mx);
-    if (lane == 0) sa[row] = __int_as_float((127 + e) << 23);
+    if (lane == 0) {
+        sa[row] = __int_as_float((127 + e) << 23);
+        if (lnz) lnz[row] = last;
+    }
     uint16_t* ph = P + (size_t)row * kcap;
     uint16_t* pl = ph + piece_stride;
     for (int l = lane; l < Kp; l += 32) {
@@ -516,6 +536,20 @@ __global__ void k_split_rows(const TIN* __restrict__ A, int nrows, int per_w, in
         if (l < K) split2(scalbn((double)a[l], -e), fmt, h, lo);
         ph[l] = h;
         pl[l] = lo;
+    }
+}
+
+// One block per problem, one warp per row tile at a time.
+__global__ void k_tile_orders(const Problem* __restrict__ probs, int bk) {
+    const Problem& P = probs[blockIdx.x];
+    if (!P.kb || !P.lz) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int mtiles = (P.M + BM - 1) / BM;
+    for (int mt = warp; mt < mtiles; mt += nw) {
+        int last = 0;
+        for (int r = mt * BM + lane; r < min(P.M, (mt + 1) * BM); r += 32) last = max(last, P.lz[r]);
+        last = __reduce_max_sync(0xffffffffu, last);
+        if (lane == 0) P.kb[mt] = min(P.kblocks, (last + bk - 1) / bk);
     }
 }
 
@@ -571,7 +605,7 @@ void encode_b(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int col
 }
 
 void split_fields(const void* A, int in_bytes, int nf, int rows, int lcap, const int* d_nord, uint16_t* P,
-                  float* sa, int kcap, int F, int piece_fmt, int bk, cudaStream_t st) {
+                  float* sa, int kcap, int F, int piece_fmt, int bk, cudaStream_t st, int* lnz) {
     const int n = nf * rows;
     if (n <= 0) return;
     if (kcap % bk) throw Error(DSM_ERR_INVALID, "order capacity of the split fields is not a multiple of BK");
@@ -581,13 +615,14 @@ void split_fields(const void* A, int in_bytes, int nf, int rows, int lcap, const
         DSM_CUDA(cudaFuncSetAttribute(k_split_rows_f4, cudaFuncAttributePreferredSharedMemoryCarveout,
                                       (int)cudaSharedmemCarveoutMaxShared));
         k_split_rows_f4<<<(n + SPLIT_THREADS / 32 - 1) / (SPLIT_THREADS / 32), SPLIT_THREADS, 0, st>>>(
-            static_cast<const float*>(A), n, rows, lcap, d_nord, kcap, bk, P, (size_t)F * rows * kcap, sa, piece_fmt);
+            static_cast<const float*>(A), n, rows, lcap, d_nord, kcap, bk, P, (size_t)F * rows * kcap, sa, piece_fmt,
+            lnz);
     } else if (in_bytes == 4)
         k_split_rows<float><<<(n + 7) / 8, 256, 0, st>>>(static_cast<const float*>(A), n, rows, lcap, d_nord, kcap,
-                                                         bk, P, (size_t)F * rows * kcap, sa, piece_fmt);
+                                                         bk, P, (size_t)F * rows * kcap, sa, piece_fmt, lnz);
     else
         k_split_rows<double><<<(n + 7) / 8, 256, 0, st>>>(static_cast<const double*>(A), n, rows, lcap, d_nord,
-                                                          kcap, bk, P, (size_t)F * rows * kcap, sa, piece_fmt);
+                                                          kcap, bk, P, (size_t)F * rows * kcap, sa, piece_fmt, lnz);
     DSM_CUDA(cudaGetLastError());
 }
 
@@ -595,7 +630,13 @@ void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, in
                  cudaStream_t st) {
     if (cols <= 0) return;
     k_split_rows<double><<<(cols + 7) / 8, 256, 0, st>>>(B, cols, cols, lcap, nullptr, kcap, kcap, P,
-                                                 (size_t)cols * kcap, sb, piece_fmt);
+                                                 (size_t)cols * kcap, sb, piece_fmt, nullptr);
+    DSM_CUDA(cudaGetLastError());
+}
+
+void tile_orders(const Problem* d_probs, int np, int bk, cudaStream_t st) {
+    if (np <= 0) return;
+    k_tile_orders<<<np, 128, 0, st>>>(d_probs, bk);
     DSM_CUDA(cudaGetLastError());
 }
 

@@ -40,6 +40,12 @@ struct Problem {
     const float* sa;             // M row scales
     const float* sb;             // N column scales
     long long ldc;
+    // Order blocks of each row tile (ceil(M / BM) entries, at most kblocks),
+    // or null: kblocks for every tile.  Rows whose orders above some l are
+    // exactly zero (the depth cut-off's deep receivers) let a tile stop its
+    // order sum early.  Filled by tile_orders from lz.
+    int* kb;
+    const int* lz;               // M rows: one past the last nonzero order (or null)
 };
 
 struct Maps {
@@ -56,13 +62,18 @@ void encode_b(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int col
 // contiguous; FP64 or FP32 elements, in_bytes 8 or 4), into pieces
 // P[2][F][rows][kcap] with one power-of-two scale per row (sa[F][rows]);
 // orders at or beyond the frequency's count nord[w] become zeros up to the
-// next multiple of bk (the contraction reads whole BK blocks).
+// next multiple of bk (the contraction reads whole BK blocks).  lnz (or
+// null) receives one past each row's last nonzero order.
 void split_fields(const void* A, int in_bytes, int nf, int rows, int lcap, const int* d_nord, uint16_t* P,
-                  float* sa, int kcap, int F, int piece_fmt, int bk, cudaStream_t st);
+                  float* sa, int kcap, int F, int piece_fmt, int bk, cudaStream_t st, int* lnz = nullptr);
 // Splits the basis table B[cols][lcap] into P[2][cols][kcap] with one scale
 // per column (sb[cols]); orders >= lcap become zeros.
 void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, int kcap, int piece_fmt,
                  cudaStream_t st);
+
+// Fills each problem's kb (where both kb and lz are set): the order blocks
+// a row tile needs, ceil(max over its rows of lz / bk), at most kblocks.
+void tile_orders(const Problem* d_probs, int np, int bk, cudaStream_t st);
 
 // Launches the persistent contraction over all tiles of probs[0..np).
 // err (device int) is set nonzero if a bounded wait inside gave up.

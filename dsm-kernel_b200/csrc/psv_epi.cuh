@@ -14,9 +14,15 @@ constexpr int NFLD = 5;                   // U, U', V/lsq, V'/lsq, l(l+1) V/lsq
 // surface row, Rs1 of them, index rr >= 0) and fluid receivers (Rf, index
 // -rr - 1): a fluid receiver's strain needs only U against P.
 //   group A (contracted with both basis columns P and dP/dtheta): fields
-//     U, V/lsq, V'/lsq of the solid class, rows ((q*3 + fa)*2 + re/im)*Rs1 + rr;
+//     U, V/lsq, V'/lsq of the solid class, rows rr*6nq + (q*3 + fa)*2 + re/im;
 //   group B (against P only): fields U', l(l+1)V/lsq of the solid class,
-//     then U of the fluid receivers, rows (q*2 + re/im)*Rf + fluid index.
+//     rows rr*4nq + (q*2 + fb)*2 + re/im, then U of the fluid receivers,
+//     rows fluid index*2nq + q*2 + re/im.
+// Receiver-major: the rows of a receiver are adjacent and receivers follow
+// in radius order, so a 128-row tile of the contraction holds a few
+// neighbouring receivers.  With the depth cut-off a receiver's fields are
+// exactly zero above an order that grows with its radius, and a tile of
+// deep receivers stops its order sum early (tc::Problem::kbt).
 // Row of the real part of (q, f) for receiver class index rr, or -1 when the
 // receiver has no row for f; *im is the offset of the imaginary part.
 __host__ __device__ __forceinline__ size_t fld_rows_full(int nq, int Rs1) { return (size_t)nq * 6 * Rs1; }
@@ -24,15 +30,14 @@ __host__ __device__ __forceinline__ size_t fld_rows(int nq, int Rs1, int Rf) {
     return (size_t)nq * (10 * (size_t)Rs1 + 2 * (size_t)Rf);
 }
 __host__ __device__ __forceinline__ long long fld_row(int nq, int Rs1, int Rf, int q, int f, int rr, int* im) {
+    *im = 1;
     if (rr >= 0) {
-        *im = Rs1;
         if (f == 1 || f == 4)
-            return (long long)fld_rows_full(nq, Rs1) + ((long long)(q * 2 + (f == 4)) * 2) * Rs1 + rr;
-        return ((long long)(q * 3 + (f == 0 ? 0 : f - 1)) * 2) * Rs1 + rr;
+            return (long long)fld_rows_full(nq, Rs1) + (long long)rr * 4 * nq + (q * 2 + (f == 4)) * 2;
+        return (long long)rr * 6 * nq + (q * 3 + (f == 0 ? 0 : f - 1)) * 2;
     }
-    *im = Rf;
     if (f != 0) return -1;
-    return (long long)nq * 10 * Rs1 + (long long)(q * 2) * Rf + (-rr - 1);
+    return (long long)nq * 10 * Rs1 + (long long)(-rr - 1) * 2 * nq + q * 2;
 }
 
 // receiver data the epilogue reads
