@@ -255,10 +255,11 @@ void Engine::lsum_plan(const std::vector<std::vector<int>>& groups, const std::v
                     P.M = M;
                     P.N = N;
                     P.tiles_n = (N + tc::BN - 1) / tc::BN;
-                    P.C = Cmix.p + (size_t)w * c_total() + c_off(m) + row0;
+                    P.C = Cmix.p + (size_t)w * c_total() + c_off(m) + (c_rowmajor ? (size_t)row0 * c_ld : row0);
                     P.sa = sA[m].p + (size_t)w * rows_m[m] + row0;
                     P.sb = sB[m].p;
-                    P.ldc = rows_m[m];
+                    P.ldc = c_rowmajor ? c_ld : rows_m[m];
+                    P.rowmajor = c_rowmajor ? 1 : 0;
                     P.lz = lnzA[m].p + (size_t)w * rows_m[m] + row0;
                     P.kb = tcKb.p + kboff;
                     kboff += (size_t)(M + tc::BM - 1) / tc::BM;
@@ -487,8 +488,13 @@ void Engine::gemm_fp64(int w, int mi, int K) {
     for (int g = 0; g < 2; ++g) {
         const int row0 = g == 0 ? 0 : rf, Mg = g == 0 ? rf : M - rf, N = g == 0 ? 2 * Th : Th;
         if (Mg <= 0) continue;
-        DSM_CUBLAS(cublasDgemm(cub, CUBLAS_OP_T, CUBLAS_OP_N, Mg, N, K, &one, A + (size_t)row0 * Lcap, Lcap,
-                               basis[mi].p, lcapB, &zero, Cgemm.p + c_off(mi) + row0, M));
+        if (c_rowmajor)  // C^T (N x Mg, column-major, ld c_ld) = B^T-view x A-view
+            DSM_CUBLAS(cublasDgemm(cub, CUBLAS_OP_T, CUBLAS_OP_N, N, Mg, K, &one, basis[mi].p, lcapB,
+                                   A + (size_t)row0 * Lcap, Lcap, &zero, Cgemm.p + c_off(mi) + (size_t)row0 * c_ld,
+                                   c_ld));
+        else
+            DSM_CUBLAS(cublasDgemm(cub, CUBLAS_OP_T, CUBLAS_OP_N, Mg, N, K, &one, A + (size_t)row0 * Lcap, Lcap,
+                                   basis[mi].p, lcapB, &zero, Cgemm.p + c_off(mi) + row0, M));
         bytes += 8.0 * ((double)Mg * K + (double)K * N + (double)Mg * N);
         flops += 2.0 * Mg * N * (double)K;
         launches++;

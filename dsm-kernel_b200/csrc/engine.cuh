@@ -125,10 +125,15 @@ class Engine {
     // all rows unless it groups its fields)
     int rows_full[3] = {-1, -1, -1};
     int full_rows(int m) const { return rows_full[m] < 0 ? rows_m[m] : rows_full[m]; }
+    // Layout of the contraction outputs: column-major (ld = rows of the |m|
+    // block), or row-major with row stride c_ld >= 2 Th (a multiple of 4)
+    // where the mode's epilogue reads a row's distances together
+    bool c_rowmajor = false;
+    int c_ld = 0;
     // offset of the |m| block inside Cgemm (one frequency)
     size_t c_off(int mi) const {
         size_t off = 0;
-        for (int m = m_lo; m < mi; ++m) off += (size_t)rows_m[m] * 2 * Th;
+        for (int m = m_lo; m < mi; ++m) off += (size_t)rows_m[m] * (c_rowmajor ? (size_t)c_ld : 2 * (size_t)Th);
         return off;
     }
     size_t c_total() const { return c_off(3); }

@@ -10,7 +10,7 @@
 //               finished chunk accumulators over
 //   warps 2..9  epilogue: tcgen05.ld of the chunk accumulators (two warps
 //               per 32-lane quarter, 64 columns each), FP64 sum of the
-//               chunks, row x column scaling, coalesced column-major stores
+//               chunks, row x column scaling, column-major or row-major stores
 // Accuracy: the tensor cores add each step into the FP32 accumulator with a
 // rounding relative to the accumulator's magnitude, so a long order sum
 // loses bits in proportion to its length.  The products therefore go into
@@ -365,17 +365,41 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             const int m = mt * BM + q * 32 + lane;
             const bool mv = m < P.M;
             const double rs = mv ? (double)P.sa[m] : 0.0;
-            float* Cm = P.C + m;
+            if (P.rowmajor) {  // a row's 64 columns: 16-byte stores where a whole group of 32 lies within N
+                float* Cr = P.C + (long long)m * P.ldc;
 #pragma unroll
-            for (int g = 0; g < 2; ++g) {
-                const int n0 = nt * BN + half * 64 + g * 32;
-                if (mv) {
+                for (int g = 0; g < 2; ++g) {
+                    const int n0 = nt * BN + half * 64 + g * 32;
+                    if (!mv) continue;
+                    if (n0 + 32 <= P.N) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int n = n0 + j;
-                        if (n < P.N)
-                            Cm[(long long)n * P.ldc] =
-                                (float)(acc[g * 32 + j] * rs * (double)P.sb[n]);
+                        for (int j = 0; j < 32; j += 4) {
+                            float4 v;
+                            v.x = (float)(acc[g * 32 + j] * rs * (double)P.sb[n0 + j]);
+                            v.y = (float)(acc[g * 32 + j + 1] * rs * (double)P.sb[n0 + j + 1]);
+                            v.z = (float)(acc[g * 32 + j + 2] * rs * (double)P.sb[n0 + j + 2]);
+                            v.w = (float)(acc[g * 32 + j + 3] * rs * (double)P.sb[n0 + j + 3]);
+                            *reinterpret_cast<float4*>(Cr + n0 + j) = v;
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (n0 + j < P.N) Cr[n0 + j] = (float)(acc[g * 32 + j] * rs * (double)P.sb[n0 + j]);
+                    }
+                }
+            } else {
+                float* Cm = P.C + m;
+#pragma unroll
+                for (int g = 0; g < 2; ++g) {
+                    const int n0 = nt * BN + half * 64 + g * 32;
+                    if (mv) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int n = n0 + j;
+                            if (n < P.N)
+                                Cm[(long long)n * P.ldc] =
+                                    (float)(acc[g * 32 + j] * rs * (double)P.sb[n]);
+                        }
                     }
                 }
             }
@@ -432,12 +456,8 @@ __device__ __forceinline__ void split2f(float x, int fmt, uint16_t& hi, uint16_t
 
 // FP32 rows whose length is a multiple of four: one warp per row, four
 // orders per lane and load (16-byte loads, 8-byte piece stores), SPLIT_U
-// loads in flight per lane.  One-warp blocks: the split of one frequency
-// group runs on the SMs beside the contraction of the previous one, whose
-// ten warps leave registers on only two of an SM's four schedulers (each
-// scheduler has its own quarter of the register file), and a block's warps
-// go to different schedulers.
-constexpr int SPLIT_THREADS = 32;
+// loads in flight per lane.
+constexpr int SPLIT_THREADS = 128;
 constexpr int SPLIT_U = 4;
 __global__ void __launch_bounds__(SPLIT_THREADS) k_split_rows_f4(const float* __restrict__ A, int nrows, int per_w,
                                                                  int lcap, const int* __restrict__ nord, int kcap,
@@ -610,10 +630,6 @@ void split_fields(const void* A, int in_bytes, int nf, int rows, int lcap, const
     if (n <= 0) return;
     if (kcap % bk) throw Error(DSM_ERR_INVALID, "order capacity of the split fields is not a multiple of BK");
     if (in_bytes == 4 && lcap % 4 == 0 && kcap % 4 == 0) {
-        // the SMs run the contraction with most of their shared memory: the
-        // split's blocks ask for the same carveout so they can run beside it
-        DSM_CUDA(cudaFuncSetAttribute(k_split_rows_f4, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                      (int)cudaSharedmemCarveoutMaxShared));
         k_split_rows_f4<<<(n + SPLIT_THREADS / 32 - 1) / (SPLIT_THREADS / 32), SPLIT_THREADS, 0, st>>>(
             static_cast<const float*>(A), n, rows, lcap, d_nord, kcap, bk, P, (size_t)F * rows * kcap, sa, piece_fmt,
             lnz);

@@ -36,7 +36,7 @@ struct Problem {
     int amap, z, bmap, kblocks;  // A map (|m|), frequency slot, B map, orders / BK
     int row0;                    // first row of A (in the map) and of C
     int M, N, tiles_n, tile0;    // shape, column tiles, index of the first tile
-    float* C;                    // column-major M x N
+    float* C;                    // M x N: column-major (ldc >= M) or row-major (rowmajor, ldc >= N)
     const float* sa;             // M row scales
     const float* sb;             // N column scales
     long long ldc;
@@ -46,6 +46,7 @@ struct Problem {
     // order sum early.  Filled by tile_orders from lz.
     int* kb;
     const int* lz;               // M rows: one past the last nonzero order (or null)
+    int rowmajor;                // C row-major (ldc a multiple of 4, C 16-byte aligned)
 };
 
 struct Maps {

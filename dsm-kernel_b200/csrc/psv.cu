@@ -2194,6 +2194,11 @@ class PsvEngine : public Engine {
         rows_full[0] = (int)psvk::fld_rows_full(NS0, d.Rs1);
         rows_full[1] = (int)psvk::fld_rows_full(NS1, d.Rs1);
         rows_full[2] = (int)psvk::fld_rows_full(NS2, d.Rs1);
+        // contraction outputs row-major: the epilogue's lanes take
+        // consecutive distances of one row (the rows of a receiver are
+        // adjacent, psvk::fld_row)
+        c_rowmajor = true;
+        c_ld = (2 * Th + 3) / 4 * 4;
         alloc_batch();
         build_basis(std::min(maxlmax + 1, 2048));
         DSM_CUDA(cudaStreamSynchronize(st));
@@ -2543,6 +2548,7 @@ class PsvEngine : public Engine {
         e.qkp = d.qkp;
         e.fr = d.fr;
         e.status = dstatus();
+        e.c_ld = c_ld;
         int id = kid("psv_epilogue");
         kbegin(id, s);
         const bool tc = mixed();

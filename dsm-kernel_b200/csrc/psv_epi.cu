@@ -16,13 +16,9 @@ namespace dsm {
 namespace psvk {
 namespace {
 
-// Threads per block.  Mixed path (FP32 contraction outputs): one-warp
-// blocks, because its epilogue of one frequency group runs on the SMs beside
-// the tensor-core contraction of the next, whose ten warps of 168 registers
-// leave room on only two of an SM's four schedulers (each has its own
-// quarter of the register file).  Plain path: 128.
+// threads per block, both paths
 template <class TC>
-constexpr int epi_threads() { return sizeof(TC) == 4 ? 32 : 128; }
+constexpr int epi_threads() { return 128; }
 
 template <class RL>
 struct PointConst {
@@ -72,7 +68,7 @@ __device__ __forceinline__ Slot slot_of(int mi, int q) {
 template <class TC, class RL>
 struct Fields {
     const TC* C;
-    size_t M;
+    size_t LD;  // row stride (row-major contraction outputs)
     int nq, Rs1, Rf, Th, it, rr, q;
     // complex entry of field f against basis column b (b = 1 only for the
     // fields 0, 2, 3; fluid receivers have field 0 against P only)
@@ -80,7 +76,7 @@ struct Fields {
         int im;
         const size_t row = (size_t)fld_row(nq, Rs1, Rf, q, f, rr, &im);
         const size_t col = (size_t)b * Th + it;
-        return {(RL)C[row + M * col], (RL)C[row + im + M * col]};
+        return {(RL)C[row * LD + col], (RL)C[(row + im) * LD + col]};
     }
 };
 
@@ -97,10 +93,9 @@ __global__ void __launch_bounds__(epi_threads<TC>()) k_psv_epi(EpiDev d, int w, 
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     const int R = d.R, Th = d.Th;
     if (idx >= Th * R) return;
-    const int it = idx / R, r = idx % R;
+    const int it = idx % Th, r = idx / Th;  // consecutive lanes: consecutive distances of one receiver
     const bool isp = pole[it] != 0;
     const TC* Cm[3] = {C0, C1, C2};
-    const size_t Mm[3] = {fld_rows(NS0, d.Rs1, d.Rf), fld_rows(NS1, d.Rs1, d.Rf), fld_rows(NS2, d.Rs1, d.Rf)};
     const int rr = d.rrow[r];
     const double x = thx[it], s = ths[it];
     const PointConst<RL> pc = point_const<RL>(x, s, d.fr[r]);
@@ -130,7 +125,7 @@ __global__ void __launch_bounds__(epi_threads<TC>()) k_psv_epi(EpiDev d, int w, 
         for (int q = 0; q < nq; ++q) {
             const Slot sl = slot_of(mi, q);
             if (sl.isback && !BACK) continue;
-            const Fields<TC, RL> G{Cm[mi], Mm[mi], nq, d.Rs1, d.Rf, Th, it, rr, q};
+            const Fields<TC, RL> G{Cm[mi], (size_t)d.c_ld, nq, d.Rs1, d.Rf, Th, it, rr, q};
             const RL sigma = (sl.m < 0 && (mi & 1)) ? RL(-1) : RL(1);
             const RL mm = (RL)sl.m, m2 = mm * mm;
             C d11 = {RL(0), RL(0)}, d12 = d11, d13 = d11, d21 = d11, d22 = d11, d23 = d11, d31 = d11,
@@ -255,7 +250,6 @@ __global__ void __launch_bounds__(epi_threads<TC>()) k_psv_epi_surf(EpiDev d, in
     if (it >= Th) return;
     const bool isp = pole[it] != 0;
     const TC* Cm[3] = {C0, C1, C2};
-    const size_t Mm[3] = {fld_rows(NS0, d.Rs1, d.Rf), fld_rows(NS1, d.Rs1, d.Rf), fld_rows(NS2, d.Rs1, d.Rf)};
     const int rr = d.rrow[R];
     const RL s_inv = (RL)(1.0 / ths[it]);
     (void)thx;
@@ -269,7 +263,7 @@ __global__ void __launch_bounds__(epi_threads<TC>()) k_psv_epi_surf(EpiDev d, in
         for (int q = 0; q < nq; ++q) {
             const Slot sl = slot_of(mi, q);
             if (sl.isback) continue;  // back slots have no surface term
-            const Fields<TC, RL> G{Cm[mi], Mm[mi], nq, d.Rs1, d.Rf, Th, it, rr, q};
+            const Fields<TC, RL> G{Cm[mi], (size_t)d.c_ld, nq, d.Rs1, d.Rf, Th, it, rr, q};
             const RL sigma = (sl.m < 0 && (mi & 1)) ? RL(-1) : RL(1);
             const C PU = G(0, 0);
             C u1, u2 = {RL(0), RL(0)}, u3 = {RL(0), RL(0)};
@@ -312,12 +306,6 @@ void launch_t(const EpiDev& d, int w, const double* thx, const double* ths, cons
     const int n = d.Th * d.R;
     constexpr int EPI_THREADS = epi_threads<TC>();
     const unsigned grid = (unsigned)((n + EPI_THREADS - 1) / EPI_THREADS);
-    // the mixed path's epilogue runs beside the tensor-core contraction,
-    // whose SMs hold most of their shared memory: the same carveout
-    for (const void* f : {(const void*)k_psv_epi<TC, RL, true>, (const void*)k_psv_epi<TC, RL, false>,
-                          (const void*)k_psv_epi_surf<TC, RL>})
-        DSM_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                      (int)cudaSharedmemCarveoutMaxShared));
     if (rsgt)
         k_psv_epi<TC, RL, true><<<grid, EPI_THREADS, 0, st>>>(d, w, thx, ths, pole, freqs, c0, c1, c2, tsgt, rsgt);
     else

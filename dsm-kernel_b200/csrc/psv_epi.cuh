@@ -49,10 +49,11 @@ struct EpiDev {
     const int* rrow;               // [R+1] class index of each receiver row (fld_row)
     const double *lam, *qkp, *fr;  // [R]  lambda, Qkappa, float(r)
     int* status;                   // run status word: DEV_NONFINITE when an output is Inf/NaN
+    int c_ld;                      // row stride of the row-major contraction outputs
 };
 
-// Contraction outputs C0..C2 (one per |m|, column-major, rows as fld_row,
-// columns b*Th+it) are FP64 when tc is
+// Contraction outputs C0..C2 (one per |m|, row-major with row stride
+// c_ld, rows as fld_row, columns b*Th+it) are FP64 when tc is
 // false and FP32 (tensor-core path, FP32 arithmetic) when it is true.
 // Writes tsgt[w][Th][R][20], rsgt[w][Th][R][10] (when rsgt) and
 // synn[w][Th][10] (when synn) as complex128.

@@ -699,13 +699,8 @@ class ShEngine : public Engine {
         int n = Th * (R + 1);
         int id = kid("sh_epilogue");
         kbegin(id, s);
-        // one-warp blocks: the mixed path's epilogue runs beside the
-        // tensor-core contraction's CTAs, which leave registers on only two
-        // of an SM's four schedulers
         if (mixed()) {
-            DSM_CUDA(cudaFuncSetAttribute(k_sh_epi<float>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                          (int)cudaSharedmemCarveoutMaxShared));
-            k_sh_epi<float><<<(n + 31) / 32, 32, 0, s>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p, c32(w, 1),
+            k_sh_epi<float><<<(n + 127) / 128, 128, 0, s>>>(d, w, Th, th.x.p, th.s.p, th.pole.p, r.p, c32(w, 1),
                                                          c32(w, 2), out_t.p, out_r.p,
                                                          synn_sw ? out_s.p : nullptr, dstatus());
         } else

@@ -208,19 +208,16 @@ void launch_pack32(Engine& e, int nf, int w0, int w1, size_t per_t, size_t per_r
     float* o = e.out32.p;
     const int n = w1 - w0;
     if (n <= 0) return;
-    // one-warp blocks, so that they fit beside the tensor-core contraction
-    int grid = e.nsm * 64;
-    DSM_CUDA(cudaFuncSetAttribute(k_pack, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  (int)cudaSharedmemCarveoutMaxShared));
-    k_pack<<<grid, 32, 0, s>>>(n, e.num_t, e.R, e.Th, e.out_t_src() + 2 * per_t * w0, o + 2 * per_t * w0);
+    int grid = e.nsm * 8;
+    k_pack<<<grid, 256, 0, s>>>(n, e.num_t, e.R, e.Th, e.out_t_src() + 2 * per_t * w0, o + 2 * per_t * w0);
     DSM_LAUNCH(e);
     if (e.rsgt_sw) {
-        k_pack<<<grid, 32, 0, s>>>(n, e.num_r, e.R, e.Th, e.out_r_src() + 2 * per_r * w0,
+        k_pack<<<grid, 256, 0, s>>>(n, e.num_r, e.R, e.Th, e.out_r_src() + 2 * per_r * w0,
                                        o + 2 * per_t * nf + 2 * per_r * w0);
         DSM_LAUNCH(e);
     }
     if (e.synn_sw) {
-        k_pack<<<grid, 32, 0, s>>>(n, e.num_s, 1, e.Th, e.out_s_src() + 2 * per_s * w0,
+        k_pack<<<grid, 256, 0, s>>>(n, e.num_s, 1, e.Th, e.out_s_src() + 2 * per_s * w0,
                                        o + 2 * (per_t + per_r) * nf + 2 * per_s * w0);
         DSM_LAUNCH(e);
     }
