@@ -67,6 +67,7 @@ struct PsvDev {
     const double* poly;     // [24]
     // receivers
     const int* rcap;        // [R][6] capture index of g0(ksta-1 .. ksta+4)
+    const int* stop_row;    // [R] highest local row of each receiver's stencil (ksta+4)
     int cap_n1, cap_n;      // capture index of rows nn-1, nn
     int cap_p0, cap_p1;     // capture index of the probe rows ksta(r_n)-1, ksta(r_n)
     const double *wv, *wd;
@@ -1636,7 +1637,8 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
                                                     typename std::conditional<MIXED, float, double>::type* __restrict__ A0f,
                                                     typename std::conditional<MIXED, float, double>::type* __restrict__ A1f,
                                                     typename std::conditional<MIXED, float, double>::type* __restrict__ A2f,
-                                                    int Lcap, const int* __restrict__ bperm) {
+                                                    int Lcap, const int* __restrict__ bperm,
+                                                    const int* __restrict__ kcut) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using FM = FieldMath<MIXED>;
     using V = typename FM::V;
@@ -1663,6 +1665,22 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
     const RT l2 = (RT)l2d, lsq = (RT)lsqd, ilsq = (RT)(1.0 / lsqd);
     auto X = [&](int cap, int b) { return Xcap[((size_t)cap * NB + b) * nsys + sys]; };
     auto C = [&](int s, int b) { return FM::coef(co, ((size_t)s * NB + b) * nsys + sys); };
+    // With the depth cut-off, a receiver whose stencil lies below the
+    // system's cut row (the same for the warp's 32 orders: a factorisation
+    // warp) has zero captures, so every field is zero: written without the
+    // loads of the coefficients and captures.
+    if (kcut && r < R && d.stop_row[r] < kcut[sys]) {
+        for (int s = 0; s < NSLOT; ++s) {
+            const int mi = slot_mi(s), q = slot_q(s), nqm = mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2);
+            const V z = FM::zero();
+            if (rr < 0) {
+                put_fieldv<T>(Aw[mi], Lcap, nqm, d, rr, q, 0, z);
+                continue;
+            }
+            for (int f = 0; f < 5; ++f) put_fieldv<T>(Aw[mi], Lcap, nqm, d, rr, q, f, z);
+        }
+        return;
+    }
     if (rr < 0) {  // fluid receiver: only U is stored
         V bU[NB];
         for (int b = 0; b < NB; ++b) {
@@ -1912,7 +1930,7 @@ __global__ void k_psv_cutrow(const float4* __restrict__ nodes, int ks, float X, 
 class PsvEngine : public Engine {
   public:
     PsvDev d{};
-    DBuf<int> iphase, nlayer, kkdr, elem, hmoff, blkoff, amz, amc, bcrow, rcap, fluid, rrow, comp_src, jsta,
+    DBuf<int> iphase, nlayer, kkdr, elem, hmoff, blkoff, amz, amc, bcrow, rcap, stoprow, fluid, rrow, comp_src, jsta,
         capmap, l0col, l0e1;
     DBuf<int2> caplist;
     DBuf<double> qmu, qkappa, sel, fel, hm, bcval, poly, lam, qkp, fr, r, rrsta;
@@ -2056,6 +2074,11 @@ class PsvEngine : public Engine {
 
         jmin_loc = jmin - d.itmp + 1;
         capmap.upload(cm, st); rcap.upload(rc, st); fluid.upload(fl, st);
+        {
+            std::vector<int> rt(R);
+            for (int ir = 0; ir < R; ++ir) rt[ir] = ks[ir] + 4 - d.itmp + 1;
+            stoprow.upload(rt, st);
+        }
         {  // receiver rows of the field matrices: solid class (with the surface) and fluid
             std::vector<int> rw(R + 1);
             int ns = 0, nf = 0;
@@ -2132,7 +2155,7 @@ class PsvEngine : public Engine {
         d.blkoff = blkoff.p; d.qmu = qmu.p; d.qkappa = qkappa.p; d.sel = sel.p; d.fel = fel.p; d.hm = hm.p;
         d.amz = amz.p; d.amc = amc.p; d.bcrow = bcrow.p; d.bcval = bcval.p; d.poly = poly.p;
         d.rowasm = rowasm.p;
-        d.rcap = rcap.p; d.wv = wv.p; d.wd = wd.p; d.fluid = fluid.p; d.lam = lam.p; d.qkp = qkp.p;
+        d.rcap = rcap.p; d.stop_row = stoprow.p; d.wv = wv.p; d.wd = wd.p; d.fluid = fluid.p; d.lam = lam.p; d.qkp = qkp.p;
         d.fr = fr.p; d.comp_src = comp_src.p; d.jsta = jsta.p;
         // per-source parameter sets: the fields set by the source position
         {
@@ -2497,11 +2520,11 @@ class PsvEngine : public Engine {
                 if (afld_bytes == 4) {
                     auto kern = fs == 16 ? k_psv_fields<true, 16> : k_psv_fields<true, 32>;
                     kern<<<grid, 128, 0, s>>>(e, wl, nsys, Xcap.p, co.p, afld_of<float>(0, k), afld_of<float>(1, k),
-                                              afld_of<float>(2, k), Lcap, bp);
+                                              afld_of<float>(2, k), Lcap, bp, kc);
                 } else {
                     auto kern = fs == 16 ? k_psv_fields<false, 16> : k_psv_fields<false, 32>;
                     kern<<<grid, 128, 0, s>>>(e, wl, nsys, Xcap.p, co.p, afld_of<double>(0, k), afld_of<double>(1, k),
-                                              afld_of<double>(2, k), Lcap, bp);
+                                              afld_of<double>(2, k), Lcap, bp, kc);
                 }
                 kend(id, 0.0, 0.0, s);
                 DSM_LAUNCH(*this);
