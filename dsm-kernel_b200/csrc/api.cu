@@ -50,8 +50,7 @@ void Engine::init_common(int dev) {
         int lo = 0, hi = 0;
         DSM_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
         DSM_CUDA(cudaStreamCreateWithPriority(&stt, cudaStreamNonBlocking, hi));
-        DSM_CUDA(cudaStreamCreateWithFlags(&sts, cudaStreamNonBlocking));
-        for (auto& e : ev_sp) DSM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+
         DSM_CUDA(cudaEventCreateWithFlags(&ev_lp, cudaEventDisableTiming));
         DSM_CUDA(cudaEventCreateWithFlags(&ev_lj, cudaEventDisableTiming));
     }
@@ -86,10 +85,7 @@ Engine::~Engine() {
     if (stc) { cudaStreamSynchronize(stc); cudaStreamDestroy(stc); }
     for (auto& e : ev_grp)
         if (e) cudaEventDestroy(e);
-    for (cudaStream_t* s : {&sts, &stt})
-        if (*s) { cudaStreamSynchronize(*s); cudaStreamDestroy(*s); }
-    for (auto& e : ev_sp)
-        if (e) cudaEventDestroy(e);
+    if (stt) { cudaStreamSynchronize(stt); cudaStreamDestroy(stt); }
     if (ev_lp) cudaEventDestroy(ev_lp);
     if (ev_lj) cudaEventDestroy(ev_lj);
     if (st) cudaStreamDestroy(st);
@@ -299,12 +295,12 @@ void Engine::lsum_plan(const std::vector<std::vector<int>>& groups, const std::v
 }
 
 // Split of group g of the mixed l-sum (field pieces, row scales, each row
-// tile's order blocks) on sts.
+// tile's order blocks) on stt.
 void Engine::lsum_split(int g) {
     const TcGroup& G = tc_groups[(size_t)g];
     if (G.slots.empty()) return;
     int id = kid("lsum_split");
-    kbegin(id, sts);
+    kbegin(id, stt);
     // one split launch per |m| and run of consecutive slots
     std::vector<int> sl = G.slots;
     std::sort(sl.begin(), sl.end());
@@ -318,17 +314,17 @@ void Engine::lsum_split(int g) {
             const char* A =
                 reinterpret_cast<const char*>(Afld[m].p) + ((size_t)src * F + w0) * rw * Lcap * afld_bytes;
             tc::split_fields(A, afld_bytes, n, rows_m[m], Lcap, d_nord.p + w0, Apc[m].p + (size_t)w0 * rw * kcA,
-                             sA[m].p + (size_t)w0 * rw, kcA, F, tc_fmt, tc_bk, sts, lnzA[m].p + (size_t)w0 * rw);
+                             sA[m].p + (size_t)w0 * rw, kcA, F, tc_fmt, tc_bk, stt, lnzA[m].p + (size_t)w0 * rw);
             launches++;
         }
         i = j;
     }
     // each row tile's order blocks from its rows' last nonzero orders
     for (const TcLaunch& L : G.launches) {
-        tc::tile_orders(tcp.p + L.first, L.np, tc_bk, sts);
+        tc::tile_orders(tcp.p + L.first, L.np, tc_bk, stt);
         launches++;
     }
-    kend(id, G.split_bytes, 0.0, sts);
+    kend(id, G.split_bytes, 0.0, stt);
 }
 
 // Tensor-core contraction launches of group g on stt.
@@ -803,31 +799,26 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
                 DSM_CUDA(cudaStreamWaitEvent(st, ev_grp[0], 0));
             }
             // Groups of batch slots.  Plain path: consecutive slots.  Mixed
-            // path: the splits of all groups first (sts), then each group's
-            // contraction and epilogue in order on stt, so that the complex64
-            // records of a group go to the host (stc) while later groups are
-            // contracted.  Kernels beside the contraction's CTAs made
-            // almost no progress, so nothing runs beside it.  The groups
-            // carry equal contraction work (slots dealt by their cutoff,
-            // heaviest first, in serpentine order).
+            // path, in order on stt: the first group's split, contraction and
+            // epilogue, then the other groups' splits and each group's
+            // contraction and epilogue, so that the complex64 records of a
+            // group go to the host (stc) while later groups are contracted.
+            // (Kernels beside the contraction's CTAs made almost no progress,
+            // so nothing runs beside it.)
             std::vector<std::vector<int>> groups(ngrp);
             if (mixed()) {
+                // the lightest frequency alone first (its records start the
+                // host copies early), the others dealt by their cutoff,
+                // heaviest first, in serpentine order
                 std::vector<int> byw(nf);
                 for (int w = 0; w < nf; ++w) byw[w] = w;
                 std::stable_sort(byw.begin(), byw.end(), [&](int a, int b) { return nord[a] > nord[b]; });
-                for (int k = 0; k < nf; ++k) {
-                    const int r = k / ngrp, c = k % ngrp;
-                    groups[(r & 1) ? ngrp - 1 - c : c].push_back(byw[k]);
+                const int first = ngrp > 1 ? 1 : 0, rest = ngrp - first;
+                if (first) groups[0].push_back(byw[nf - 1]);
+                for (int k = 0; k < nf - first; ++k) {
+                    const int r = k / rest, c = k % rest;
+                    groups[first + ((r & 1) ? rest - 1 - c : c)].push_back(byw[k]);
                 }
-                std::vector<long long> work(ngrp, 0);
-                for (int g = 0; g < ngrp; ++g)
-                    for (int w : groups[g]) work[g] += nord[w];
-                std::vector<int> go(ngrp);
-                for (int g = 0; g < ngrp; ++g) go[g] = g;
-                std::stable_sort(go.begin(), go.end(), [&](int a, int b) { return work[a] < work[b]; });
-                std::vector<std::vector<int>> sorted(ngrp);
-                for (int g = 0; g < ngrp; ++g) sorted[g] = std::move(groups[go[g]]);
-                groups = std::move(sorted);
             } else {
                 for (int g = 0; g < ngrp; ++g)
                     for (int w = g * nf / ngrp; w < (g + 1) * nf / ngrp; ++w) groups[g].push_back(w);
@@ -836,14 +827,14 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             if (mixed()) {
                 lsum_plan(groups, nord);
                 DSM_CUDA(cudaEventRecord(ev_lp, st));
-                DSM_CUDA(cudaStreamWaitEvent(sts, ev_lp, 0));
                 DSM_CUDA(cudaStreamWaitEvent(stt, ev_lp, 0));
-                for (int g = 0; g < ngrp; ++g) lsum_split(g);
-                DSM_CUDA(cudaEventRecord(ev_sp[0], sts));
-                DSM_CUDA(cudaStreamWaitEvent(stt, ev_sp[0], 0));
+                lsum_split(0);
                 se = stt;
             }
             for (int g = 0; g < ngrp; ++g) {
+                // the other groups' splits once the first group's records are on their way
+                if (mixed() && g == 1)
+                    for (int h = 1; h < ngrp; ++h) lsum_split(h);
                 if (mixed()) lsum_contract(g);
                 for (int w : groups[g]) {
                     stats.orders_used += hs[w].norders;

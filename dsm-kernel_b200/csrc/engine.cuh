@@ -57,12 +57,11 @@ class Engine {
     cudaStream_t stc = nullptr;
     static constexpr int MAX_OUT_GROUPS = 8;
     cudaEvent_t ev_grp[MAX_OUT_GROUPS] = {};
-    // mixed l-sum of a batch in frequency groups: the splits of all groups
-    // (sts), then each group's contraction and epilogue in order (stt, high
-    // priority), the records of a group to the host (stc) while later
-    // groups run
-    cudaStream_t sts = nullptr, stt = nullptr;
-    cudaEvent_t ev_sp[MAX_OUT_GROUPS] = {};
+    // mixed l-sum of a batch in frequency groups, in order on stt (high
+    // priority): the first group's split, contraction and epilogue, then
+    // the other groups' splits and each group's contraction and epilogue;
+    // the records of a group go to the host (stc) while later groups run
+    cudaStream_t stt = nullptr;
     cudaEvent_t ev_lp = nullptr, ev_lj = nullptr;
     int lsum_groups = 1;             // frequency groups of a batch without host records (DSM_LSUM_GROUPS)
     bool side_pending = false;
@@ -171,7 +170,7 @@ class Engine {
     void lsum_prepare(int nf, const std::vector<int>& norders);
     // problem lists of all groups (each a list of batch slots), one upload
     void lsum_plan(const std::vector<std::vector<int>>& groups, const std::vector<int>& norders);
-    // group g: split (sts), contraction launches (stt)
+    // group g: split, contraction launches (both on stt)
     void lsum_split(int g);
     void lsum_contract(int g);
     struct TcLaunch { size_t first; int np, tiles; };
