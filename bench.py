@@ -71,9 +71,9 @@ TRAFFIC = {
 # workload and scaled to a launch by the units it processes (reads by the
 # orders contracted, writes by the frequencies whose output it writes).
 TRAFFIC_PER_UNIT = {
-    ("psv2048", "lsum_tc"): (0.966e9 / 3918, 0.208e9,
-                             "ncu capture of a one-frequency launch of this workload (3918 orders: 0.966 GB read, "
-                             "0.208 GB written), scaled to the launch by orders (reads) and frequencies (writes)"),
+    ("psv2048", "lsum_tc"): (0.5074e9 / 4281, 0.378e9 / 2,
+                             "ncu capture of a two-frequency launch of this workload (4281 orders: 0.507 GB read, "
+                             "0.378 GB written), scaled to the launch by orders (reads) and frequencies (writes)"),
 }
 
 
@@ -665,6 +665,7 @@ def main():
         clocks.start()
         kstats, ms_dev, launches, llogs = {}, 0.0, 0, []
         phases = {"solve": 0.0, "lsum": 0.0}
+        exec_flops = 0.0
         sol = {"systems": 0, "orders_used": 0, "orders_padded": 0, "solve_rounds": 0, "freqs_extended": 0}
         barrier()
         for k in range(args.steps):
@@ -673,6 +674,7 @@ def main():
             ms_dev += st.ms_total
             phases["solve"] += st.ms_solve
             phases["lsum"] += st.ms_lsum
+            exec_flops += st.lsum_flops_exec
             for key in sol:
                 sol[key] += getattr(st, key)
             launches += st.launches - sum(v[1] for n_, v in st.kernels().items() if n_.startswith("lsum_dgemm"))
@@ -707,6 +709,7 @@ def main():
         return {"value": slices / t_dev, "t": t_dev, "kstats": kstats, "launches": launches, "tuning": tuning,
                 "llogs": llogs, "clocks": clk, "solve": sol,
                 "phase_ms_per_step": {k: v / args.steps for k, v in phases.items()},
+                "exec_flops": exec_flops,
                 "e2e": {"value": slices / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * F,
                         "d2h_bytes_per_step": 8 * (per_t + per_r + per_s) * F + 4 * F,
                         "timing": "host wall clock around dsm_run_freqs (perf_counter), records to pinned memory"}}
@@ -764,6 +767,13 @@ def main():
                     "peak_source": "measured (bf16 burst)" if "bf16_tflops" in peaks else "fallback",
                     "avg_launch_ms": ms / max(n, 1), "piece_products": 3,
                     "frac_of_piece_ceiling": 3.0 * ach / peak}
+            if run.get("exec_flops", 0.0) > 0:
+                # the row tiles stop at their rows' last nonzero order (the
+                # depth cut zeroes deep receivers' high orders): executed
+                # products, three fp16 pieces each, against the same peak
+                ache = run["exec_flops"] / (ms / 1e3) / 1e12
+                roof.update({"executed_fraction_of_algorithmic": run["exec_flops"] / f,
+                             "achieved_executed": ache, "frac_executed_of_piece_ceiling": 3.0 * ache / peak})
         else:
             ach = b / (ms / 1e3) / 1e9
             peak = peaks.get("hbm_gbs", 6650.0)

@@ -285,6 +285,8 @@ void Engine::lsum_plan(const std::vector<std::vector<int>>& groups, const std::v
         }
         tc_groups.push_back(std::move(G));
     }
+    tc_plan = all;
+    tc_kbn = kboff;
     if (tcp_next + all.size() > tcp.n) throw Error(DSM_ERR_INVALID, "contraction list exceeds its buffer");
     // each source's lists take their own slots of tcp, so no copy overwrites
     // a list an earlier launch may still read
@@ -292,6 +294,21 @@ void Engine::lsum_plan(const std::vector<std::vector<int>>& groups, const std::v
         DSM_CUDA(cudaMemcpyAsync(tcp.p + tcp_next, all.data(), sizeof(tc::Problem) * all.size(),
                                  cudaMemcpyHostToDevice, st));
     tcp_next += all.size();
+}
+
+// Flops the last plan's contraction executed: each row tile runs its own
+// order blocks (tile_orders); read back when profiling, after the batch.
+void Engine::count_exec_flops() {
+    if (!prof || tc_plan.empty() || tc_kbn == 0) return;
+    std::vector<int> kb(tc_kbn);
+    DSM_CUDA(cudaMemcpy(kb.data(), tcKb.p, sizeof(int) * tc_kbn, cudaMemcpyDeviceToHost));
+    for (const tc::Problem& P : tc_plan) {
+        const size_t off = (size_t)(P.kb - tcKb.p);
+        for (int mt = 0; mt * tc::BM < P.M; ++mt) {
+            const int rows = std::min(tc::BM, P.M - mt * tc::BM);
+            stats.lsum_flops_exec += 2.0 * rows * (double)P.N * (double)std::min(kb[off + mt], P.kblocks) * tc_bk;
+        }
+    }
 }
 
 // Split of group g of the mixed l-sum (field pieces, row scales, each row
@@ -879,6 +896,10 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             if (mixed()) {  // st continues after the last group's epilogue
                 DSM_CUDA(cudaEventRecord(ev_lj, stt));
                 DSM_CUDA(cudaStreamWaitEvent(st, ev_lj, 0));
+                if (prof) {  // executed flops (row-tile order counts) before the next source reuses them
+                    DSM_CUDA(cudaStreamSynchronize(stt));
+                    count_exec_flops();
+                }
             }
             // --- 5: outputs
             if (llog_out && src == 0)

@@ -176,6 +176,9 @@ class Engine {
     struct TcLaunch { size_t first; int np, tiles; };
     struct TcGroup { std::vector<int> slots; std::vector<TcLaunch> launches; double split_bytes, flops, bytes; };
     std::vector<TcGroup> tc_groups;
+    std::vector<tc::Problem> tc_plan;  // the problems of the last plan (host copy)
+    size_t tc_kbn = 0;                 // row-tile entries of the last plan
+    void count_exec_flops();           // adds the executed contraction flops (profiling)
     tc::Maps tcmaps;
     size_t tcp_next = 0;  // next free slot of tcp in this batch
     void check_device_flags();

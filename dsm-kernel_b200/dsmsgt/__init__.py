@@ -103,7 +103,7 @@ class Stats(C.Structure):
                 ("orders_used", C.c_longlong), ("orders_padded", C.c_longlong),
                 ("lsum_flops", C.c_double), ("solve_bytes", C.c_double),
                 ("nk", C.c_int), ("kern", KStat * 24), ("solve_rounds", C.c_longlong),
-                ("freqs_extended", C.c_longlong)]
+                ("freqs_extended", C.c_longlong), ("lsum_flops_exec", C.c_double)]
 
     def kernels(self):
         return {self.kern[i].name.decode(): (self.kern[i].ms, self.kern[i].launches,

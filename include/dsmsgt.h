@@ -285,6 +285,9 @@ typedef struct dsm_stats {
     long long freqs_extended;/* frequencies whose cutoff lay beyond their
                                 first order range (the learned cutoff's
                                 misses when it sized that range)            */
+    double lsum_flops_exec;  /* flops the mixed contraction executed: row
+                                tiles stop at their rows' last nonzero order
+                                (counted when profiling is on, else 0)      */
 } dsm_stats_t;
 int dsm_get_stats(const dsm_ctx_t *ctx, dsm_stats_t *stats);
 
