@@ -71,3 +71,43 @@ def test_cut_bound_validation(built):
     with pytest.raises(dsmsgt.DsmError):
         h.set_depth_cutoff(1e-20)
     h.close()
+
+
+@pytest.mark.gpu
+def test_mixed_row_tiles_stop_at_last_nonzero_order(built):
+    """With the cut a deep receiver's fields are exactly zero above an order
+    that grows with its radius; the mixed contraction's row tiles (a few
+    neighbouring receivers each) stop at their rows' last nonzero order.
+    On the benchmark grid that leaves well under the dense products, the
+    outputs still match the FP64 path to the mixed path's tolerance, also
+    without the cut (where only fields that underflow FP32 are zero), and
+    the executed products never exceed the dense ones padded to whole
+    64-order blocks."""
+    job, _ = bench.workload("psv2048")
+    w = bench.WORKLOADS["psv2048"]
+    job = dsmsgt.Job(job.param_text.replace(f"0.0 180.0 {w['thdelta']!r}\n", "0.0 180.0 30.0\n"),
+                     job.conf_text, job.model_text)
+    s = dsmsgt.Setup(job, "psv")
+    freqs = [700, 2048]
+    ref = dsmsgt.Context(s, precision=dsmsgt.DSM_PREC_FP64, freq_batch=2)
+    want = ref.run(freqs)
+    ref.close()
+    c = dsmsgt.Context(s, precision=dsmsgt.DSM_PREC_MIXED, freq_batch=2)
+    c.set_profiling(True)
+    got = c.run(freqs)
+    st = c.stats()
+    assert st.lsum_flops > 0 and st.lsum_flops_exec < 0.8 * st.lsum_flops, (st.lsum_flops_exec, st.lsum_flops)
+    assert list(got[3]) == list(want[3])
+    for x, y in zip(got[:3], want[:3]):
+        for i in range(len(freqs)):
+            assert rel_l2(x[i], y[i]) <= 1e-6
+    assert st.lsum_flops_exec <= 1.05 * st.lsum_flops
+    c.set_depth_cutoff(0.0)
+    got = c.run(freqs)
+    st = c.stats()
+    assert 0 < st.lsum_flops_exec <= 1.05 * st.lsum_flops
+    assert list(got[3]) == list(want[3])
+    for x, y in zip(got[:3], want[:3]):
+        for i in range(len(freqs)):
+            assert rel_l2(x[i], y[i]) <= 1e-6
+    c.close()
