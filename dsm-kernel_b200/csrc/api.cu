@@ -318,6 +318,8 @@ void Engine::lsum_split(int g) {
     if (G.slots.empty()) return;
     int id = kid("lsum_split");
     kbegin(id, stt);
+    // zero orders recorded by the field kernels of this batch (the cut on)
+    const bool zf_ok = use_zfirst && depth_bound > 0.0 && afld_bytes == 4;
     // one split launch per |m| and run of consecutive slots
     std::vector<int> sl = G.slots;
     std::sort(sl.begin(), sl.end());
@@ -331,7 +333,8 @@ void Engine::lsum_split(int g) {
             const char* A =
                 reinterpret_cast<const char*>(Afld[m].p) + ((size_t)src * F + w0) * rw * Lcap * afld_bytes;
             tc::split_fields(A, afld_bytes, n, rows_m[m], Lcap, d_nord.p + w0, Apc[m].p + (size_t)w0 * rw * kcA,
-                             sA[m].p + (size_t)w0 * rw, kcA, F, tc_fmt, tc_bk, stt, lnzA[m].p + (size_t)w0 * rw);
+                             sA[m].p + (size_t)w0 * rw, kcA, F, tc_fmt, tc_bk, stt, lnzA[m].p + (size_t)w0 * rw,
+                             zf_ok ? zfirst.p + ((size_t)src * F + w0) * (R + 1) : nullptr, rowrec[m].p, R + 1);
             launches++;
         }
         i = j;

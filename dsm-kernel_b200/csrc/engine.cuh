@@ -156,6 +156,12 @@ class Engine {
     DBuf<float> sB[3];               // [2Th]
     DBuf<float> Cmix;                // [F][c_total] column-major blocks
     DBuf<int> lnzA[3];               // [F][rows]: one past each field row's last nonzero order
+    // Where the mode knows that a receiver's fields are zero from some order
+    // on (P-SV with the depth cut), zfirst[src][F][R+1] holds that order per
+    // receiver row (INT_MAX-like: none) and rowrec[m][row] the receiver row of
+    // each field row; the split reads a row only up to it
+    DBuf<int> zfirst, rowrec[3];
+    bool use_zfirst = false;
     DBuf<int> tcKb;                  // order blocks of each row tile of the batch's problems
     DBuf<tc::Problem> tcp;
     DBuf<int> d_nord;

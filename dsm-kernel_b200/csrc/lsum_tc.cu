@@ -463,21 +463,25 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_split_rows_f4(const float* __
                                                                  int lcap, const int* __restrict__ nord, int kcap,
                                                                  int bk, uint16_t* __restrict__ P,
                                                                  size_t piece_stride, float* __restrict__ sa,
-                                                                 int fmt, int* __restrict__ lnz) {
+                                                                 int fmt, int* __restrict__ lnz,
+                                                                 const int* __restrict__ zf,
+                                                                 const int* __restrict__ rowrec, int R1) {
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= nrows) return;
     const int K = nord ? min(nord[row / per_w], lcap) : lcap;
     const int Kp = min(kcap, (K + bk - 1) / bk * bk);
+    // orders at or above Kr are known to be zero: not read
+    const int Kr = zf ? min(K, zf[(row / per_w) * R1 + rowrec[row % per_w]]) : K;
     const float4* a4 = reinterpret_cast<const float4*>(A + (size_t)row * lcap);
     float mx = 0.0f;
     int last = 0;  // one past the last nonzero order
-    for (int i0 = lane; 4 * i0 < K; i0 += 32 * SPLIT_U) {
+    for (int i0 = lane; 4 * i0 < Kr; i0 += 32 * SPLIT_U) {
         float4 v[SPLIT_U];
 #pragma unroll
         for (int u = 0; u < SPLIT_U; ++u) {
             const int i = i0 + 32 * u;
-            v[u] = 4 * i < K ? a4[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            v[u] = 4 * i < Kr ? a4[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
 #pragma unroll
         for (int u = 0; u < SPLIT_U; ++u) {
@@ -485,7 +489,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_split_rows_f4(const float* __
             const float x[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
 #pragma unroll
             for (int c = 0; c < 4; ++c)
-                if (4 * i + c < K) {
+                if (4 * i + c < Kr) {
                     mx = fmaxf(mx, fabsf(x[c]));
                     if (x[c] != 0.0f) last = 4 * i + c + 1;
                 }
@@ -505,7 +509,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS) k_split_rows_f4(const float* __
 #pragma unroll
         for (int u = 0; u < SPLIT_U; ++u) {
             const int i = i0 + 32 * u;
-            v[u] = 4 * i < K ? a4[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            v[u] = 4 * i < Kr ? a4[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
 #pragma unroll
         for (int u = 0; u < SPLIT_U; ++u) {
@@ -625,14 +629,15 @@ void encode_b(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int col
 }
 
 void split_fields(const void* A, int in_bytes, int nf, int rows, int lcap, const int* d_nord, uint16_t* P,
-                  float* sa, int kcap, int F, int piece_fmt, int bk, cudaStream_t st, int* lnz) {
+                  float* sa, int kcap, int F, int piece_fmt, int bk, cudaStream_t st, int* lnz, const int* zf,
+                  const int* rowrec, int R1) {
     const int n = nf * rows;
     if (n <= 0) return;
     if (kcap % bk) throw Error(DSM_ERR_INVALID, "order capacity of the split fields is not a multiple of BK");
     if (in_bytes == 4 && lcap % 4 == 0 && kcap % 4 == 0) {
         k_split_rows_f4<<<(n + SPLIT_THREADS / 32 - 1) / (SPLIT_THREADS / 32), SPLIT_THREADS, 0, st>>>(
             static_cast<const float*>(A), n, rows, lcap, d_nord, kcap, bk, P, (size_t)F * rows * kcap, sa, piece_fmt,
-            lnz);
+            lnz, zf, rowrec, R1);
     } else if (in_bytes == 4)
         k_split_rows<float><<<(n + 7) / 8, 256, 0, st>>>(static_cast<const float*>(A), n, rows, lcap, d_nord, kcap,
                                                          bk, P, (size_t)F * rows * kcap, sa, piece_fmt, lnz);

@@ -65,8 +65,12 @@ void encode_b(CUtensorMap* m, const void* base, int piece_fmt, int kcap, int col
 // orders at or beyond the frequency's count nord[w] become zeros up to the
 // next multiple of bk (the contraction reads whole BK blocks).  lnz (or
 // null) receives one past each row's last nonzero order.
+// zf (or null): per frequency of the run, R1 entries; a row whose receiver
+// row rowrec[row] has zf < K is zero from that order on and is read only up
+// to it.
 void split_fields(const void* A, int in_bytes, int nf, int rows, int lcap, const int* d_nord, uint16_t* P,
-                  float* sa, int kcap, int F, int piece_fmt, int bk, cudaStream_t st, int* lnz = nullptr);
+                  float* sa, int kcap, int F, int piece_fmt, int bk, cudaStream_t st, int* lnz = nullptr,
+                  const int* zf = nullptr, const int* rowrec = nullptr, int R1 = 0);
 // Splits the basis table B[cols][lcap] into P[2][cols][kcap] with one scale
 // per column (sb[cols]); orders >= lcap become zeros.
 void split_bases(const double* B, int cols, int lcap, uint16_t* P, float* sb, int kcap, int piece_fmt,

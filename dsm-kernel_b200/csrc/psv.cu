@@ -1638,7 +1638,7 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
                                                     typename std::conditional<MIXED, float, double>::type* __restrict__ A1f,
                                                     typename std::conditional<MIXED, float, double>::type* __restrict__ A2f,
                                                     int Lcap, const int* __restrict__ bperm,
-                                                    const int* __restrict__ kcut) {
+                                                    const int* __restrict__ kcut, int* __restrict__ zfirst) {
     using T = typename std::conditional<MIXED, float, double>::type;
     using FM = FieldMath<MIXED>;
     using V = typename FM::V;
@@ -1670,6 +1670,9 @@ __global__ void __launch_bounds__(128) k_psv_fields(PsvDev d, WorkList wl, int n
     // warp) has zero captures, so every field is zero: written without the
     // loads of the coefficients and captures.
     if (kcut && r < R && d.stop_row[r] < kcut[sys]) {
+        // the cut row grows with the order, so this receiver's fields are
+        // zero from here on: its lowest order in the warp records that
+        if (zfirst && lane % FS == 0) atomicMin(zfirst + (size_t)w * (R + 1) + r, l);
         for (int s = 0; s < NSLOT; ++s) {
             const int mi = slot_mi(s), q = slot_q(s), nqm = mi == 0 ? NS0 : (mi == 1 ? NS1 : NS2);
             const V z = FM::zero();
@@ -2222,6 +2225,36 @@ class PsvEngine : public Engine {
         // adjacent, psvk::fld_row)
         c_rowmajor = true;
         c_ld = (2 * Th + 3) / 4 * 4;
+        {  // receiver row (0..R) of each field row, for the split's zero orders
+            std::vector<int> solid_r(d.Rs1, R), fluid_r(std::max(d.Rf, 1), 0);
+            std::vector<int> rw(R + 1);
+            DSM_CUDA(cudaStreamSynchronize(st));  // rrow was uploaded on st
+            DSM_CUDA(cudaMemcpy(rw.data(), rrow.p, sizeof(int) * (R + 1), cudaMemcpyDeviceToHost));
+            for (int ir = 0; ir < R; ++ir) {
+                if (rw[ir] >= 0) solid_r[rw[ir]] = ir;
+                else fluid_r[-rw[ir] - 1] = ir;
+            }
+            const int nqs[3] = {NS0, NS1, NS2};
+            for (int m = 0; m < 3; ++m) {
+                std::vector<int> rr_of(rows_m[m], R);
+                for (int rr = 0; rr < d.Rs1; ++rr)
+                    for (int q = 0; q < nqs[m]; ++q)
+                        for (int f = 0; f < 5; ++f) {
+                            int im;
+                            const long long row = psvk::fld_row(nqs[m], d.Rs1, d.Rf, q, f, rr, &im);
+                            rr_of[row] = rr_of[row + im] = solid_r[rr];
+                        }
+                for (int fi = 0; fi < d.Rf; ++fi)
+                    for (int q = 0; q < nqs[m]; ++q) {
+                        int im;
+                        const long long row = psvk::fld_row(nqs[m], d.Rs1, d.Rf, q, 0, -fi - 1, &im);
+                        rr_of[row] = rr_of[row + im] = fluid_r[fi];
+                    }
+                rowrec[m].upload(rr_of, st);
+            }
+            zfirst.reserve((size_t)nsrc * F * (R + 1));
+            use_zfirst = mixed();
+        }
         alloc_batch();
         build_basis(std::min(maxlmax + 1, 2048));
         DSM_CUDA(cudaStreamSynchronize(st));
@@ -2335,6 +2368,8 @@ class PsvEngine : public Engine {
     bool l0_done = false;
     void omega_pieces(const int* fr_, int nf) override {
         l0_done = false;
+        // first zero order per receiver row: none yet (0x7f7f7f7f)
+        if (use_zfirst) DSM_CUDA(cudaMemsetAsync(zfirst.p, 0x7f, sizeof(int) * (size_t)nsrc * F * (R + 1), st));
         dim3 grid((d.ncol_tot + 127) / 128, nf);
         int id = kid("psv_omega_blocks");
         kbegin(id);
@@ -2520,11 +2555,12 @@ class PsvEngine : public Engine {
                 if (afld_bytes == 4) {
                     auto kern = fs == 16 ? k_psv_fields<true, 16> : k_psv_fields<true, 32>;
                     kern<<<grid, 128, 0, s>>>(e, wl, nsys, Xcap.p, co.p, afld_of<float>(0, k), afld_of<float>(1, k),
-                                              afld_of<float>(2, k), Lcap, bp, kc);
+                                              afld_of<float>(2, k), Lcap, bp, kc,
+                                              use_zfirst && kc ? zfirst.p + (size_t)k * F * (R + 1) : nullptr);
                 } else {
                     auto kern = fs == 16 ? k_psv_fields<false, 16> : k_psv_fields<false, 32>;
                     kern<<<grid, 128, 0, s>>>(e, wl, nsys, Xcap.p, co.p, afld_of<double>(0, k), afld_of<double>(1, k),
-                                              afld_of<double>(2, k), Lcap, bp, kc);
+                                              afld_of<double>(2, k), Lcap, bp, kc, nullptr);
                 }
                 kend(id, 0.0, 0.0, s);
                 DSM_LAUNCH(*this);
