@@ -827,17 +827,20 @@ void Engine::run(const int* ilist, int n, dsm_out_t* ho, const void** dt, const 
             // so nothing runs beside it.)
             std::vector<std::vector<int>> groups(ngrp);
             if (mixed()) {
-                // the lightest frequency alone first (its records start the
-                // host copies early), the others dealt by their cutoff,
+                // the lightest frequencies first (a fifth of the batch: their
+                // records start the host copies early and keep the copy
+                // engine busy while the other groups' splits and the next
+                // contraction run), the others dealt by their cutoff,
                 // heaviest first, in serpentine order
                 std::vector<int> byw(nf);
                 for (int w = 0; w < nf; ++w) byw[w] = w;
                 std::stable_sort(byw.begin(), byw.end(), [&](int a, int b) { return nord[a] > nord[b]; });
-                const int first = ngrp > 1 ? 1 : 0, rest = ngrp - first;
-                if (first) groups[0].push_back(byw[nf - 1]);
-                for (int k = 0; k < nf - first; ++k) {
+                const int nfirst = ngrp > 1 ? std::max(1, std::min(nf / 5, nf - (ngrp - 1))) : 0;
+                const int gfirst = ngrp > 1 ? 1 : 0, rest = ngrp - gfirst;
+                for (int k = 0; k < nfirst; ++k) groups[0].push_back(byw[nf - 1 - k]);
+                for (int k = 0; k < nf - nfirst; ++k) {
                     const int r = k / rest, c = k % rest;
-                    groups[first + ((r & 1) ? rest - 1 - c : c)].push_back(byw[k]);
+                    groups[gfirst + ((r & 1) ? rest - 1 - c : c)].push_back(byw[k]);
                 }
             } else {
                 for (int g = 0; g < ngrp; ++g)
