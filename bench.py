@@ -598,11 +598,14 @@ def main():
     # plain, 3.0 % learned), so the default run uses the plain ranges
     ap.add_argument("--lmax", dest="lmax", action="store_true",
                     help="first order ranges from the trained cutoff block of the workload")
-    ap.add_argument("--per-step", type=int, default=16)
+    ap.add_argument("--per-step", type=int, default=None,
+                    help="frequency slices per step (default 20; 4 per context for --workload batch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="default tile shapes instead of the library's tuner")
     args = ap.parse_args()
+    if args.per_step is None:
+        args.per_step = 4 if args.mode == "batch" else 20
     if args.mode == "catalogue":
         catalogue_bench(args)
         return
