@@ -6,13 +6,14 @@ inner core, fluid outer core, 6 mantle/crust zones; seeded quadratic
 profiles), tlen 3276.8 s, 2048 frequencies (fmax 0.625 Hz, cutoffs up to
 about 7000), source 300 km deep, 201 receiver radii 1000-6350 km, 1441
 epicentral distances (0.125 deg).  A step is one batch of frequency slices
-spread across the band, each fully processed (all orders up to the
-reference's cutoff, all m, all sources, TSGT + RSGT + SYNN on the full
-(r, theta) grid).  psv1024 (the FP64 configuration's band: 1024 frequencies,
-721 distances) and sh256 are the other workloads.
+(20 by default, --per-step) spread across the band, each fully processed
+(all orders up to the reference's cutoff, all m, all sources, TSGT + RSGT +
+SYNN on the full (r, theta) grid).  psv1024 (the FP64 configuration's
+band: 1024 frequencies, 721 distances), sh256, the catalogue consumer and
+the batched models x depths request are the other workloads.
 
-  python bench.py [--gpus N --steps K --warmup W] [--workload psv2048|psv1024|sh256]
-                  [--precision mixed|mixed_bf16|fp64]
+  python bench.py [--gpus N --steps K --warmup W] [--workload psv2048|psv1024|sh256|catalogue|batch]
+                  [--precision mixed|mixed_bf16|fp64] [--per-step F]
   python bench.py --impl reference ...   # CPU restatement of the reference
 
 The headline path is the mixed-precision one (split fp16 l-sum on the
