@@ -152,29 +152,80 @@ def step_freqs(step: int, per_step: int, imax: int, rank: int = 0, world: int = 
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """Samples the SM clock, power and clock-event reasons of the bench's GPU
+    during the timed region.  The GPU is found by its PCI bus id (CUDA and
+    NVML number devices differently under CUDA_VISIBLE_DEVICES).  NVML is
+    read every 10 ms from a thread (reads only: no setting is changed);
+    without NVML, nvidia-smi is polled every 0.2 s."""
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
-        self.rows = []
+        self.rows = []   # (sm MHz, max sm MHz, watts, set of active reason names)
+        self.source = None
         self._stop = threading.Event()
         self._t = None
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(device)
+            self.bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        except Exception:
+            self.bus = None
+
+    def _nvml(self):
+        import pynvml
+        pynvml.nvmlInit()
+        h = pynvml.nvmlDeviceGetHandleByPciBusId(self.bus) if self.bus else \
+            pynvml.nvmlDeviceGetHandleByIndex(self.device)
+        masks = [pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                 pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap]
+        mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+        def read():
+            sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+            w = pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0
+            bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+            return sm, mx, w, {n for n, m in zip(self.NAMES, masks) if bits & m}
+        read()
+        return read, pynvml.nvmlShutdown
+
+    def _smi(self):
+        ident = self.bus if self.bus else str(self.device)
+
+        def read():
+            out = subprocess.run(["nvidia-smi", f"--id={ident}", f"--query-gpu={self.Q}",
+                                  "--format=csv,noheader,nounits"], capture_output=True,
+                                 text=True, timeout=5).stdout.strip()
+            f = [x.strip() for x in out.split(",")]
+            if len(f) < 7:
+                raise RuntimeError(out)
+            num = lambda s: float(s) if s.replace(".", "").isdigit() else float("nan")
+            return (num(f[0]), num(f[1]), num(f[2]),
+                    {n for n, s in zip(self.NAMES, f[3:7]) if s.lower().startswith("active")})
+        return read, lambda: None
 
     def start(self):
+        try:
+            read, close = self._nvml()
+            self.source, period = "nvml", 0.01
+        except Exception:
+            read, close = self._smi()
+            self.source, period = "nvidia-smi", 0.2
+
         def run():
             while not self._stop.is_set():
                 try:
-                    out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits"], capture_output=True,
-                                         text=True, timeout=5).stdout.strip()
-                    if out:
-                        self.rows.append([x.strip() for x in out.split(",")])
+                    self.rows.append(read())
                 except Exception:
                     pass
-                self._stop.wait(0.2)
+                self._stop.wait(period)
+            try:
+                close()
+            except Exception:
+                pass
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
 
@@ -182,17 +233,16 @@ class ClockSampler:
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
-        mhz = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
-        reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            for k, nm in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
-                    reasons.add(nm)
+        mhz = [r[0] for r in self.rows if r[0] == r[0]]
+        mx = [r[1] for r in self.rows if r[1] == r[1]]
+        watts = [r[2] for r in self.rows if r[2] == r[2]]
+        reasons = set().union(*[r[3] for r in self.rows]) if self.rows else set()
         return {"sm_mhz": float(np.median(mhz)) if mhz else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(self.rows)}
+                "sm_max_mhz": max(mx) if mx else None,
+                "sm_mhz_min": min(mhz) if mhz else None,
+                "power_w_median": round(float(np.median(watts)), 1) if watts else None,
+                "reasons": sorted(reasons), "samples": len(self.rows),
+                "source": self.source, "pci_bus_id": self.bus}
 
 
 CPU_THETAS = 8  # interior epicentral distances of a CPU sample
