@@ -12,7 +12,7 @@ SYNN on the full (r, theta) grid).  psv1024 (the FP64 configuration's
 band: 1024 frequencies, 721 distances), sh256, the catalogue consumer and
 the batched models x depths request are the other workloads.
 
-  python bench.py [--gpus N --steps K --warmup W] [--workload psv2048|psv1024|sh256|catalogue|batch]
+  python bench.py [--gpus N --steps K --warmup W] [--workload psv2048|psv1024|sh256|catalogue|kernels|batch]
                   [--precision mixed|mixed_bf16|fp64] [--per-step F]
   python bench.py --impl reference ...   # CPU restatement of the reference
 
@@ -475,6 +475,137 @@ def catalogue_bench(args):
             "cpu_baseline": cpu, "clocks": clk}))
 
 
+KER_METRIC = "kernel points/s (isotropic P and S kernels: 3 products, transforms, Butterworth filter, sums)"
+KER_UNIT = "points/s"
+
+
+def kernels_inputs(seed: int, p, npt: int, nr: int):
+    rng = np.random.default_rng(seed)
+    nf = p["fmax"] - p["fmin"] + 1
+    nwin = p["iwin_end"] - p["iwin_start"] + 1
+    fs = 2 * p["np1"] / p["tlen"]
+    h = [(rng.standard_normal((npt, 6, nf)) + 1j * rng.standard_normal((npt, 6, nf))) for _ in range(2)]
+    kp = dict(types=3, nfilter=0, fclp=[0.005], fchp=[0.05], npoles=4, sampling_hz=fs,
+              nt1=[p["iwin_start"] + nwin // 8], nt2=[p["iwin_end"] - nwin // 8],
+              coeff=rng.standard_normal((nwin, nr, 8, 1)),
+              jacobian=rng.standard_normal((nf, nr)) + 1j * rng.standard_normal((nf, nr)))
+    ir = rng.integers(0, nr, npt).astype(np.int32)
+    return h[0], h[1], kp, ir
+
+
+def kernels_bench(args):
+    """Per-point kernel formulas: one step = the isotropic P and S kernels
+    (types 1, 3, 4, 5, 7, 8; one broad-band filter, the reference's nfilter
+    = 0, 4 Butterworth sections) of the catalogue workload's 1681 points,
+    from h3 / h4 spectra resident on the device."""
+    w = CAT_WORKLOAD
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    p = catalogue_params()
+    npt, nr = w["points"], 4
+    nwin = p["iwin_end"] - p["iwin_start"] + 1
+    nf = p["fmax"] - p["fmin"] + 1
+    cfg = {"workload": "kernels", "points": npt, "np1": p["np1"], "window_samples": nwin,
+           "frequencies": nf, "radii": nr, "filters": 1, "npoles": 4,
+           "l2": "inputs larger than L2 (h3 and h4 spectra: 661 MB per step)"}
+
+    def cpu(h3, h4, kp, ir, nsample):
+        from oracle import catalogue as cat
+        q = dict(kp, nr=nr, nktype=8)
+        t0 = time.perf_counter()
+        cat.iso_kernels(p, q, ir[:nsample], h3[:nsample], h4[:nsample])
+        return nsample / (time.perf_counter() - t0)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        h3, h4, kp, ir = kernels_inputs(0, p, 64, nr)
+        cpu(h3, h4, kp, ir, 4)
+        vals = [cpu(h3, h4, kp, ir, 64) for _ in range(args.steps)]
+        value = len(vals) / sum(1.0 / v for v in vals)
+        print(json.dumps({"impl": "reference", "metric": KER_METRIC, "value": value, "unit": KER_UNIT,
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1e3 * 64 / value, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                          "cpu_baseline": {"value": value, "unit": KER_UNIT, "cores": 1, "kind": "port",
+                                           "sample": "oracle on 64 points per step (numpy, one thread); "
+                                                     "ms_per_step is that sample's time"},
+                          "e2e": {"value": value, "unit": KER_UNIT, "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    import dsmsgt
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    h3, h4, kp, ir = kernels_inputs(rank, p, npt, nr)
+    d3 = torch.from_numpy(h3).to(f"cuda:{dev}")
+    d4 = torch.from_numpy(h4).to(f"cuda:{dev}")
+    c = dsmsgt.Catalogue(p, device=dev)
+    c.set_kernel_params(kp["types"], kp["nfilter"], kp["fclp"], kp["fchp"], kp["npoles"], kp["sampling_hz"],
+                        kp["nt1"], kp["nt2"], kp["coeff"], kp["jacobian"])
+    ker = torch.zeros((npt, 1, 9), dtype=torch.float64, device=f"cuda:{dev}")
+    irr = np.ascontiguousarray(ir, np.int32)
+    L = dsmsgt.lib()
+
+    def step():
+        rc = L.dsm_cat_kernels(c.h, npt, dsmsgt._ptr(irr, dsmsgt._ip), d3.data_ptr(), d4.data_ptr(), 1,
+                               ker.data_ptr(), None, 1)
+        assert rc == 0, L.dsm_cat_last_error(c.h).decode()
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    clk = clocks.stop()
+    # end to end: spectra from host memory, kernels back to the host
+    c.kernels(ir, h3, h4)
+    t_e2e = 0.0
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        c.kernels(ir, h3, h4)
+        t_e2e += time.perf_counter() - t1
+    c.close()
+    peaks = {}
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except Exception:
+        pass
+    # algorithmic bytes of a step: h3 and h4 read once, the three transform
+    # rows written, transformed in place (read + written) and read by the filter
+    nh = p["np1"] + 1
+    alg = 2 * npt * 6 * nf * 16 + 3 * npt * nh * 16 * 4
+    ach = alg * args.steps / t / 1e9
+    peak = peaks.get("hbm_gbs", 6650.0)
+    cpu_b = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v = cpu(h3, h4, kp, ir, 64)
+        cpu_b = {"value": v, "unit": KER_UNIT, "cores": 1, "kind": "port",
+                 "sample": "oracle on 64 of the 1681 points (numpy, one thread)"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": KER_METRIC, "value": args.steps * npt * world / t, "unit": KER_UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded spectra, coefficients and jacobian)", "config": cfg,
+            "timing": "host clock around synchronous calls on device-resident spectra",
+            "e2e": {"value": args.steps * npt / t_e2e, "unit": KER_UNIT,
+                    "h2d_bytes_per_step": int(h3.nbytes + h4.nbytes + irr.nbytes),
+                    "d2h_bytes_per_step": int(npt * 9 * 8)},
+            "gpu_launches": 2 * args.steps,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "traffic": None, "scope": "whole call (products, cuFFT, filter and sums)",
+                         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+            "cpu_baseline": cpu_b, "clocks": clk}))
+
+
 # Batched uneven-size form, scaled to fit a few minutes and the memory of
 # one GPU: several seeded models and source depths of P-SV and SH in one
 # request (all contexts resident at once; an 8-depth P-SV context's field
@@ -641,7 +772,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", "--mode", dest="mode", default="psv2048",
-                    choices=["psv1024", "psv2048", "sh256", "psv", "sh", "catalogue", "batch"])
+                    choices=["psv1024", "psv2048", "sh256", "psv", "sh", "catalogue", "kernels", "batch"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_bf16"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     # The plain first ranges pad 2.0 % of the orders on the 2048-frequency
@@ -659,6 +790,9 @@ def main():
         args.per_step = 4 if args.mode == "batch" else 20
     if args.mode == "catalogue":
         catalogue_bench(args)
+        return
+    if args.mode == "kernels":
+        kernels_bench(args)
         return
     if args.mode == "batch":
         if args.impl == "reference":

@@ -45,6 +45,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <map>
 #include <memory>
@@ -368,9 +369,146 @@ __global__ void k_cat_window(const double* __restrict__ y, int row, int iws, int
     }
 }
 
+// ---- per-point isotropic kernels (calculateKernel, calculateK.f90:131-235) ----
+
+constexpr int KER_MAXFL = 16;   // filters ift = 0..nfilter
+constexpr int KER_MAXNP = 10;   // Butterworth sections (bwfilt.f90:135)
+
+// Frequency products of isovpfreq (calculateK.f90:261-265) and isovsfreq
+// (:367-374 du; :395-403 duq with jacobianFuji), each times 1e3, written as
+// the Hermitian projection H_n (n = 0..np1) that vectorFFT_double
+// transforms: rows (batch point, series) np1 + 1 apart, series in the order
+// P du, S du, S duq of the types present.  The operation order is the
+// reference's (sums left to right, complex products (ac - bd, ad + bc)).
+struct KerSpecArgs {
+    const cd *h3, *h4;   // [point][6][nf]
+    const cd* jac;       // jacobianFuji [n - fmin][nr]
+    const int* ir;       // [point], 0-based radius
+    int p0, nb, nr, fmin, fmax, np1, types, ns;
+    cd* h;
+};
+
+__global__ void __launch_bounds__(256) k_ker_spec(const KerSpecArgs a) {
+    const int nh = a.np1 + 1, nf = a.fmax - a.fmin + 1;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nh) return;
+    for (int b = blockIdx.y; b < a.nb; b += gridDim.y) {
+        const int pt = a.p0 + b;
+        cd up = mk(0.0), us = mk(0.0), uq = mk(0.0);
+        if (n >= a.fmin && n <= a.fmax) {
+            const cd* x = a.h3 + (size_t)pt * 6 * nf + (n - a.fmin);
+            const cd* y = a.h4 + (size_t)pt * 6 * nf + (n - a.fmin);
+            cd g[6], q[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                g[k] = x[(size_t)k * nf];
+                q[k] = y[(size_t)k * nf];
+            }
+            if (a.types & DSM_KER_VP) up = -((g[0] + g[1] + g[2]) * (q[0] + q[1] + q[2])) * 1.0e3;
+            if (a.types & DSM_KER_VS) {
+                const cd p4 = g[3] * q[3], p5 = g[4] * q[4], p6 = g[5] * q[5];
+                const cd c1 = g[0] * (q[1] + q[2]), c2 = g[1] * (q[0] + q[2]), c3 = g[2] * (q[0] + q[1]);
+                us = (-(2.0 * (p4 + p5 + p6)) + c1 + c2 + c3) * 1.0e3;
+                const cd d1 = g[0] * q[0], d2 = g[1] * q[1], d3 = g[2] * q[2];
+                cd v = -(4.0 * (p4 + p5 + p6)) + (2.0 / 3.0) * (c1 + c2 + c3) - (4.0 / 3.0) * (d1 + d2 + d3);
+                v = v * a.jac[(size_t)(n - a.fmin) * a.nr + a.ir[pt]];
+                uq = v * 1.0e3;
+            }
+        }
+        cd* row = a.h + (size_t)b * a.ns * nh + n;
+        if (a.types & DSM_KER_VP) {
+            *row = herm_proj(up, n, a.np1, a.fmin);
+            row += nh;
+        }
+        if (a.types & DSM_KER_VS) {
+            row[0] = herm_proj(us, n, a.np1, a.fmin);
+            row[nh] = herm_proj(uq, n, a.np1, a.fmin);
+        }
+    }
+}
+
+// One thread per (batch point, series, filter): the window samples of the
+// transform (vectorFFT_double's exp(omegai t) / tlen * 1e3, as k_cat_window
+// forms them), the forward Butterworth recursion of rekurs (bwfilt.f90:54-90)
+// and the trapezoid sums of the series' kernel types over nt1..nt2 with half
+// weights at both ends (calculateK.f90:302-321, :497-513), in sample order.
+struct KerTimeArgs {
+    const double* y;      // transform rows, 2 (np1 + 1) reals apart
+    const double* e;      // exp(omegai t / samplingHz) over the window
+    const double* coeff;  // coeff(0:nfilter, 1:nktype, 1:nr, window), Fortran order
+    const double* fc;     // [filter][a | b1 | b2][KER_MAXNP]
+    const int *nt1, *nt2; // window-relative, per filter
+    const int* ir;
+    int p0, nb, ns, nfl, nr, nktype, nwin, iws, row, types;
+    double tlen;
+    double* ker;          // [point][nfl][nktype + 1]
+    double* filt;         // [point][ns][nfl][nwin] or null
+};
+
+template <int NP>
+__global__ void __launch_bounds__(128) k_ker_time(const KerTimeArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nb * a.ns * a.nfl) return;
+    const int f = i % a.nfl, s = (i / a.nfl) % a.ns, b = i / (a.nfl * a.ns);
+    const int pt = a.p0 + b;
+    // series kind: 0 P du (types 1, 3, 4), 1 S du (5, 7), 2 S duq (8)
+    const int kind = (a.types & DSM_KER_VP) ? s : s + 1;
+    const int nk = kind == 0 ? 3 : kind == 1 ? 2 : 1;
+    int kt[3];
+    kt[0] = kind == 0 ? 1 : kind == 1 ? 5 : 8;
+    kt[1] = kind == 0 ? 3 : 7;
+    kt[2] = 4;
+    double A[NP], B1[NP], B2[NP], z1[NP], z2[NP];
+    const double* fc = a.fc + (size_t)f * 3 * KER_MAXNP;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        A[k] = fc[k];
+        B1[k] = fc[KER_MAXNP + k];
+        B2[k] = fc[2 * KER_MAXNP + k];
+        z1[k] = 0.0;
+        z2[k] = 0.0;
+    }
+    double x1 = 0.0, x2 = 0.0;
+    const int t1 = a.nt1[f], t2 = a.nt2[f];
+    const int tend = a.filt ? a.nwin : t2 + 1;
+    const double* yr = a.y + ((size_t)b * a.ns + s) * a.row + a.iws;
+    const size_t cstride = (size_t)a.nfl * a.nktype * a.nr;
+    const double* cb = a.coeff + (size_t)a.ir[pt] * a.nktype * a.nfl + f;
+    double* fo = a.filt ? a.filt + (((size_t)pt * a.ns + s) * a.nfl + f) * a.nwin : nullptr;
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int t = 0; t < tend; ++t) {
+        const double x = yr[t] * a.e[t] / a.tlen * 1.0e3;
+        double z[NP];
+        z[0] = A[0] * (x - x2) - B1[0] * z1[0] - B2[0] * z2[0];
+#pragma unroll
+        for (int k = 1; k < NP; ++k) z[k] = A[k] * (z[k - 1] - z2[k - 1]) - B1[k] * z1[k] - B2[k] * z2[k];
+        x2 = x1;
+        x1 = x;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            z2[k] = z1[k];
+            z1[k] = z[k];
+        }
+        const double v = z[NP - 1];
+        if (fo) fo[t] = v;
+        if (t < t1 || t > t2) continue;
+        const double* c = cb + (size_t)t * cstride;
+        for (int j = 0; j < nk; ++j) {
+            const double ck = c[(size_t)(kt[j] - 1) * a.nfl];
+            // isovpfreq halves as coeff * duf / 2, isovsfreq as 0.5 * coeff * duf
+            const double half = kind == 0 ? ck * v / 2.0 : 0.5 * ck * v;
+            if (t == t1) acc[j] = acc[j] + half;
+            if (t > t1 && t < t2) acc[j] = acc[j] + ck * v;
+            if (t == t2) acc[j] = acc[j] + half;
+        }
+    }
+    double* ko = a.ker + ((size_t)pt * a.nfl + f) * (a.nktype + 1);
+    for (int j = 0; j < nk; ++j) ko[kt[j]] = acc[j];
+}
+
 }  // namespace cat
 
-#define DSM_CUFFT(x)                                                                        \
+#define DSM_CUFFT(x)                                                                      \
     do {                                                                                    \
         cufftResult r_ = (x);                                                               \
         if (r_ != CUFFT_SUCCESS)                                                            \
@@ -401,6 +539,13 @@ struct dsm_cat {
     bool profiling = false;
     dsm_stats_t stats{};
     cudaEvent_t ev[8]{};
+    // per-point kernels (dsm_cat_set_kernel_params): filters, integration
+    // windows, coeff and jacobianFuji resident on the device
+    bool kset = false;
+    int ktypes = 0, kns = 0, knfl = 0, knp = 0, knr = 0, knkt = 0;
+    DBuf<double> kcoef, kfc, kker, kfilt;
+    DBuf<cd> kjac, kh3, kh4;
+    DBuf<int> knt, kir;
 
     ~dsm_cat() {
         if (dev >= 0) cudaSetDevice(dev);
@@ -918,6 +1063,213 @@ extern "C" int dsm_cat_transform(dsm_cat_t* c, int nseries, const void* spectra,
         }
         if (!out_on_device)
             DSM_CUDA(cudaMemcpyAsync(out, dout, (size_t)nseries * nwin * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        DSM_CUDA(cudaStreamSynchronize(c->st));
+    });
+}
+
+namespace {
+// bpcoeff (src/KernelMaker/bwfilt.f90:124-166): the npoles second-order
+// sections a, b1, b2 of the recursive band-pass [f1, f2] (Hz) at step dt.
+// The reference builds its poles from single-precision complex values:
+// cexp(cmplx(0, phase)) is a single-precision exponential (cos and sin
+// rounded to single here), cmplx(w0, 0) and cmplx(w1 w2, 0) round their
+// real parts to single; only s(1..npoles) of the 2 npoles roots are used.
+void bpcoeff(double f1, double f2, int npoles, double dt, double* a, double* b1, double* b2) {
+    const double pi = 3.141592653589793;
+    const double d2 = 2.0 / dt;
+    const double w1 = d2 * std::tan(2.0 * pi * f1 / d2);
+    const double w2 = d2 * std::tan(2.0 * pi * f2 / d2);
+    const double w0 = 0.5 * (w2 - w1);
+    auto cm = [](std::complex<double> x, std::complex<double> y) {
+        return std::complex<double>(x.real() * y.real() - x.imag() * y.imag(),
+                                    x.real() * y.imag() + x.imag() * y.real());
+    };
+    std::complex<double> s[2 * KER_MAXNP];
+    for (int n = 1, i = 0; n <= npoles; ++n, i += 2) {
+        const float ph = (float)((double)(2 * n - 1 + npoles) * pi / (double)(2 * npoles));
+        const std::complex<double> p((double)(float)std::cos((double)ph), (double)(float)std::sin((double)ph));
+        const std::complex<double> t1 = cm(p, std::complex<double>((double)(float)w0, 0.0));
+        const std::complex<double> t2 = std::sqrt(cm(t1, t1) - std::complex<double>((double)(float)(w1 * w2), 0.0));
+        s[i] = t1 + t2;
+        s[i + 1] = t1 - t2;
+    }
+    for (int n = 0; n < npoles; ++n) {
+        const double ssum = 2.0 * s[n].real();
+        const double sprod = s[n].real() * s[n].real() - s[n].imag() * (-s[n].imag());
+        const double fact1 = d2 * d2 - d2 * ssum + sprod;
+        const double fact2 = 2.0 * (sprod - d2 * d2);
+        const double fact3 = d2 * d2 + d2 * ssum + sprod;
+        a[n] = 2.0 * d2 * w0 / fact1;
+        b1[n] = fact2 / fact1;
+        b2[n] = fact3 / fact1;
+    }
+}
+
+template <int NP>
+void launch_ker_time(const KerTimeArgs& a, int threads, cudaStream_t st) {
+    k_ker_time<NP><<<(threads + 127) / 128, 128, 0, st>>>(a);
+}
+void launch_ker_time_np(int np, const KerTimeArgs& a, int threads, cudaStream_t st) {
+    switch (np) {
+        case 1: launch_ker_time<1>(a, threads, st); break;
+        case 2: launch_ker_time<2>(a, threads, st); break;
+        case 3: launch_ker_time<3>(a, threads, st); break;
+        case 4: launch_ker_time<4>(a, threads, st); break;
+        case 5: launch_ker_time<5>(a, threads, st); break;
+        case 6: launch_ker_time<6>(a, threads, st); break;
+        case 7: launch_ker_time<7>(a, threads, st); break;
+        case 8: launch_ker_time<8>(a, threads, st); break;
+        case 9: launch_ker_time<9>(a, threads, st); break;
+        default: launch_ker_time<10>(a, threads, st); break;
+    }
+    DSM_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+extern "C" int dsm_cat_set_kernel_params(dsm_cat_t* c, const dsm_cat_kernel_params_t* kp) {
+    if (!c) return DSM_ERR_INVALID;
+    return cat_guard(c, [&] {
+        const char* fn = "dsm_cat_set_kernel_params";
+        need(kp != nullptr, std::string(fn) + ": null parameters");
+        const dsm_cat_params_t& p = c->p;
+        const int nwin = c->nwin(), nf = p.fmax - p.fmin + 1;
+        need(kp->types >= 1 && kp->types <= (DSM_KER_VP | DSM_KER_VS), std::string(fn) + ": types must be VP, VS or both");
+        need(kp->nfilter >= 0 && kp->nfilter < KER_MAXFL, std::string(fn) + ": nfilter must be in [0, 15]");
+        need(kp->npoles >= 1 && kp->npoles <= KER_MAXNP, std::string(fn) + ": npoles must be in [1, 10]");
+        need(std::isfinite(kp->sampling_hz) && kp->sampling_hz > 0, std::string(fn) + ": sampling_hz must be positive");
+        need(kp->nr >= 1 && kp->nktype >= 8, std::string(fn) + ": nr >= 1 and nktype >= 8 required");
+        need(kp->fclp && kp->fchp && kp->nt1 && kp->nt2 && kp->coeff, std::string(fn) + ": null argument");
+        need(!(kp->types & DSM_KER_VS) || kp->jacobian, std::string(fn) + ": VS kernels need jacobianFuji");
+        const int nfl = kp->nfilter + 1;
+        std::vector<double> fc((size_t)nfl * 3 * KER_MAXNP, 0.0);
+        std::vector<int> nt(2 * nfl);
+        for (int f = 0; f < nfl; ++f) {
+            need(std::isfinite(kp->fclp[f]) && std::isfinite(kp->fchp[f]), std::string(fn) + ": non-finite corner frequency");
+            need(kp->nt1[f] >= p.iwin_start && kp->nt1[f] <= kp->nt2[f] && kp->nt2[f] <= p.iwin_end,
+                 std::string(fn) + ": nt1/nt2 must satisfy iwin_start <= nt1 <= nt2 <= iwin_end");
+            double* q = fc.data() + (size_t)f * 3 * KER_MAXNP;
+            bpcoeff(kp->fclp[f], kp->fchp[f], kp->npoles, 1.0 / kp->sampling_hz, q, q + KER_MAXNP, q + 2 * KER_MAXNP);
+            for (int k = 0; k < 3 * KER_MAXNP; ++k)
+                need(std::isfinite(q[k]), std::string(fn) + ": the filter's coefficients are not finite");
+            nt[f] = kp->nt1[f] - p.iwin_start;
+            nt[nfl + f] = kp->nt2[f] - p.iwin_start;
+        }
+        const size_t ncoef = (size_t)nwin * kp->nr * kp->nktype * nfl;
+        for (size_t i = 0; i < ncoef; ++i) need(std::isfinite(kp->coeff[i]), std::string(fn) + ": non-finite coeff");
+        DSM_CUDA(cudaSetDevice(c->dev));
+        c->kset = false;
+        c->kfc.upload(fc, c->st);
+        c->knt.upload(nt, c->st);
+        c->kcoef.upload(kp->coeff, ncoef, c->st);
+        if (kp->types & DSM_KER_VS) {
+            const cd* j = static_cast<const cd*>(kp->jacobian);
+            for (size_t i = 0; i < (size_t)nf * kp->nr; ++i)
+                need(std::isfinite(j[i].re) && std::isfinite(j[i].im), std::string(fn) + ": non-finite jacobian");
+            c->kjac.upload(j, (size_t)nf * kp->nr, c->st);
+        }
+        DSM_CUDA(cudaStreamSynchronize(c->st));
+        c->ktypes = kp->types;
+        c->kns = ((kp->types & DSM_KER_VP) ? 1 : 0) + ((kp->types & DSM_KER_VS) ? 2 : 0);
+        c->knfl = nfl;
+        c->knp = kp->npoles;
+        c->knr = kp->nr;
+        c->knkt = kp->nktype;
+        c->kset = true;
+    });
+}
+
+extern "C" int dsm_cat_kernels(dsm_cat_t* c, int npoint, const int* ir, const void* h3, const void* h4,
+                               int spectra_on_device, double* ker, double* filtered, int out_on_device) {
+    if (!c) return DSM_ERR_INVALID;
+    return cat_guard(c, [&] {
+        const char* fn = "dsm_cat_kernels";
+        need(c->kset, std::string(fn) + ": dsm_cat_set_kernel_params has not been called");
+        need(npoint >= 0 && (npoint == 0 || (ir && h3 && h4 && ker)), std::string(fn) + ": null argument");
+        if (spectra_on_device)
+            need(((uintptr_t)h3 % 16) == 0 && ((uintptr_t)h4 % 16) == 0, std::string(fn) + ": misaligned device spectra");
+        if (out_on_device)
+            need(((uintptr_t)ker % 8) == 0 && ((uintptr_t)filtered % 8) == 0, std::string(fn) + ": misaligned device output");
+        if (npoint == 0) return;
+        for (int k = 0; k < npoint; ++k)
+            need(ir[k] >= 0 && ir[k] < c->knr, std::string(fn) + ": radius index out of range");
+        const dsm_cat_params_t& p = c->p;
+        const int nh = p.np1 + 1, nf = p.fmax - p.fmin + 1, nwin = c->nwin();
+        const int ns = c->kns, nfl = c->knfl, nkt1 = c->knkt + 1;
+        DSM_CUDA(cudaSetDevice(c->dev));
+        c->kir.upload(ir, npoint, c->st);
+        const cd* d3 = static_cast<const cd*>(h3);
+        const cd* d4 = static_cast<const cd*>(h4);
+        if (!spectra_on_device) {
+            c->kh3.upload(d3, (size_t)npoint * 6 * nf, c->st);
+            c->kh4.upload(d4, (size_t)npoint * 6 * nf, c->st);
+            d3 = c->kh3.p;
+            d4 = c->kh4.p;
+        }
+        double* dker = ker;
+        double* dfilt = filtered;
+        if (!out_on_device) {
+            c->kker.reserve((size_t)npoint * nfl * nkt1);
+            dker = c->kker.p;
+            if (filtered) {
+                c->kfilt.reserve((size_t)npoint * ns * nfl * nwin);
+                dfilt = c->kfilt.p;
+            }
+        }
+        DSM_CUDA(cudaMemsetAsync(dker, 0, (size_t)npoint * nfl * nkt1 * sizeof(double), c->st));
+        // points per batch: the in-place transform buffer stays under max_batch_bytes
+        const int pc = (int)std::min<size_t>(
+            (size_t)npoint, std::max<size_t>(1, c->max_batch_bytes / ((size_t)ns * nh * sizeof(cd))));
+        c->h.reserve((size_t)pc * ns * nh);
+        KerSpecArgs sa{};
+        sa.h3 = d3;
+        sa.h4 = d4;
+        sa.jac = c->kjac.p;
+        sa.ir = c->kir.p;
+        sa.nr = c->knr;
+        sa.fmin = p.fmin;
+        sa.fmax = p.fmax;
+        sa.np1 = p.np1;
+        sa.types = c->ktypes;
+        sa.ns = ns;
+        sa.h = c->h.p;
+        KerTimeArgs ta{};
+        ta.y = reinterpret_cast<const double*>(c->h.p);
+        ta.e = c->e.p;
+        ta.coeff = c->kcoef.p;
+        ta.fc = c->kfc.p;
+        ta.nt1 = c->knt.p;
+        ta.nt2 = c->knt.p + nfl;
+        ta.ir = c->kir.p;
+        ta.ns = ns;
+        ta.nfl = nfl;
+        ta.nr = c->knr;
+        ta.nktype = c->knkt;
+        ta.nwin = nwin;
+        ta.iws = p.iwin_start;
+        ta.row = 2 * nh;
+        ta.types = c->ktypes;
+        ta.tlen = p.tlen;
+        ta.ker = dker;
+        ta.filt = dfilt;
+        for (int b0 = 0; b0 < npoint; b0 += pc) {
+            const int nb = std::min(pc, npoint - b0);
+            sa.p0 = b0;
+            sa.nb = nb;
+            k_ker_spec<<<dim3((nh + 255) / 256, std::min(nb, 65535)), 256, 0, c->st>>>(sa);
+            DSM_CUDA(cudaGetLastError());
+            DSM_CUFFT(cufftExecZ2D(c->plan(nb * ns), reinterpret_cast<cufftDoubleComplex*>(c->h.p),
+                                   reinterpret_cast<cufftDoubleReal*>(c->h.p)));
+            ta.p0 = b0;
+            ta.nb = nb;
+            launch_ker_time_np(c->knp, ta, nb * ns * nfl, c->st);
+        }
+        if (!out_on_device) {
+            DSM_CUDA(cudaMemcpyAsync(ker, dker, (size_t)npoint * nfl * nkt1 * sizeof(double), cudaMemcpyDeviceToHost,
+                                     c->st));
+            if (filtered)
+                DSM_CUDA(cudaMemcpyAsync(filtered, dfilt, (size_t)npoint * ns * nfl * nwin * sizeof(double),
+                                         cudaMemcpyDeviceToHost, c->st));
+        }
         DSM_CUDA(cudaStreamSynchronize(c->st));
     });
 }

@@ -148,6 +148,15 @@ class CatParams(C.Structure):
                 ("device", C.c_int)]
 
 
+class CatKernelParams(C.Structure):
+    _fields_ = [("types", C.c_int), ("nfilter", C.c_int), ("fclp", C.POINTER(C.c_double)),
+                ("fchp", C.POINTER(C.c_double)), ("npoles", C.c_int), ("sampling_hz", C.c_double),
+                ("nt1", C.POINTER(C.c_int)), ("nt2", C.POINTER(C.c_int)), ("nr", C.c_int), ("nktype", C.c_int),
+                ("coeff", C.POINTER(C.c_double)), ("jacobian", C.c_void_p)]
+
+
+KER_VP, KER_VS = 1, 2
+
 _lib = None
 
 
@@ -209,6 +218,9 @@ def lib() -> C.CDLL:
         L.dsm_cat_series.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_void_p, C.c_int]
         L.dsm_cat_spectra.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_void_p, C.c_int]
         L.dsm_cat_transform.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+        L.dsm_cat_set_kernel_params.argtypes = [C.c_void_p, C.POINTER(CatKernelParams)]
+        L.dsm_cat_kernels.argtypes = [C.c_void_p, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                      C.c_void_p, C.c_int]
         L.dsm_cat_set_profiling.argtypes = [C.c_void_p, C.c_int]
         L.dsm_cat_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
         L.dsm_cat_set_batch_bytes.argtypes = [C.c_void_p, C.c_size_t]
@@ -771,6 +783,51 @@ class Catalogue:
                                      C.c_void_p(res.ctypes.data), 0)
         self._check(rc, "dsm_cat_transform")
         return res.reshape(x.shape[:-1] + (self.nwin,))
+
+    def set_kernel_params(self, types: int, nfilter: int, fclp, fchp, npoles: int, sampling_hz: float,
+                          nt1, nt2, coeff, jacobian=None):
+        """Filters, integration windows and the reference's coeff(0:nfilter,
+        1:nktype, 1:nr, window) / jacobianFuji(1:nr, fmin:fmax) arrays
+        (numpy, Fortran order: coeff of shape [nwin][nr][nktype][nfilter+1]
+        C-ordered, jacobian [nf][nr]) for dsm_cat_kernels."""
+        nfl = nfilter + 1
+        self._kp = dict(
+            fclp=np.ascontiguousarray(fclp, np.float64), fchp=np.ascontiguousarray(fchp, np.float64),
+            nt1=np.ascontiguousarray(nt1, np.int32), nt2=np.ascontiguousarray(nt2, np.int32),
+            coeff=np.ascontiguousarray(coeff, np.float64),
+            jac=None if jacobian is None else np.ascontiguousarray(jacobian, np.complex128))
+        k = self._kp
+        assert k["coeff"].ndim == 4 and k["coeff"].shape[0] == self.nwin and k["coeff"].shape[3] == nfl
+        kp = CatKernelParams(types=types, nfilter=nfilter, fclp=_ptr(k["fclp"], _dp), fchp=_ptr(k["fchp"], _dp),
+                             npoles=npoles, sampling_hz=sampling_hz, nt1=_ptr(k["nt1"], _ip),
+                             nt2=_ptr(k["nt2"], _ip), nr=k["coeff"].shape[1], nktype=k["coeff"].shape[2],
+                             coeff=_ptr(k["coeff"], _dp),
+                             jacobian=None if k["jac"] is None else C.c_void_p(k["jac"].ctypes.data))
+        self._check(lib().dsm_cat_set_kernel_params(self.h, C.byref(kp)), "dsm_cat_set_kernel_params")
+        self._ker_shape = (nfl, k["coeff"].shape[2] + 1)
+        self._ker_ns = (1 if types & KER_VP else 0) + (2 if types & KER_VS else 0)
+
+    def kernels(self, ir, h3, h4, filtered: bool = False):
+        """tmpker [point][nfilter+1][nktype+1] of points with radius indices
+        ir and spectra h3, h4 [point][6][nf] (numpy complex128, or torch CUDA
+        tensors), plus the filtered series [point][series][nfilter+1][nwin]
+        when filtered is set (dsm_cat_kernels)."""
+        irr = np.ascontiguousarray(ir, np.int32)
+        n = irr.size
+        if hasattr(h3, "data_ptr"):
+            assert h3.is_cuda and h4.is_cuda and h3.is_contiguous() and h4.is_contiguous()
+            p3, p4, on_dev = h3.data_ptr(), h4.data_ptr(), 1
+        else:
+            h3 = np.ascontiguousarray(h3, np.complex128)
+            h4 = np.ascontiguousarray(h4, np.complex128)
+            p3, p4, on_dev = h3.ctypes.data, h4.ctypes.data, 0
+        ker = np.zeros((n,) + self._ker_shape, np.float64)
+        filt = np.zeros((n, self._ker_ns, self._ker_shape[0], self.nwin), np.float64) if filtered else None
+        rc = lib().dsm_cat_kernels(self.h, n, _ptr(irr, _ip), C.c_void_p(p3), C.c_void_p(p4), on_dev,
+                                   C.c_void_p(ker.ctypes.data),
+                                   None if filt is None else C.c_void_p(filt.ctypes.data), 0)
+        self._check(rc, "dsm_cat_kernels")
+        return (ker, filt) if filtered else ker
 
     def set_profiling(self, on: bool):
         self._check(lib().dsm_cat_set_profiling(self.h, int(on)), "dsm_cat_set_profiling")

@@ -498,6 +498,54 @@ int dsm_cat_spectra(dsm_cat_t *cat, int npoint, const double *distance, int nout
 int dsm_cat_transform(dsm_cat_t *cat, int nseries, const void *spectra, int spectra_on_device,
                       double *out, int out_on_device);
 
+/* Per-point isotropic sensitivity kernels from the h3 / h4 spectra, the
+ * body of KernelMaker's calculateKernel after its rsgt2h3freq /
+ * tsgt2h4freq (src/KernelMaker/calculateK.f90:131-235):
+ *   isovpfreq  calculateK.f90:237-323  types 1, 3, 4 (P-wave speed)
+ *   isovsfreq  calculateK.f90:327-518  types 5, 7, 8 (S-wave speed, Q_mu
+ *              through jacobianFuji)
+ *   bwfilt / rekurs / bpcoeff  src/KernelMaker/bwfilt.f90 (forward
+ *              recursive Butterworth band-pass, irek = 0)
+ * Per point: the frequency products (x 1e3), vectorFFT_double of each
+ * product, the Butterworth filter of every filter ift = 0..nfilter, and the
+ * trapezoid sum over samples nt1(ift)..nt2(ift) against coeff.
+ * dsm_cat_set_kernel_params uploads what every point shares; the arrays
+ * are the reference's own, in Fortran order. */
+#define DSM_KER_VP 1   /* types 1, 3, 4 (isovpfreq) */
+#define DSM_KER_VS 2   /* types 5, 7, 8 (isovsfreq) */
+typedef struct dsm_cat_kernel_params {
+    int    types;          /* DSM_KER_VP | DSM_KER_VS                          */
+    int    nfilter;        /* filters 0..nfilter (nfilter < 16)               */
+    const double *fclp, *fchp;   /* corner frequencies (Hz), nfilter+1 each */
+    int    npoles;         /* npButterworth, 1..10                            */
+    double sampling_hz;    /* samplingHz; the filter's step is 1/sampling_hz  */
+    const int *nt1, *nt2;  /* integration samples per filter (same indices as
+                              iwin_start/iwin_end, iwin_start <= nt1 <= nt2 <=
+                              iwin_end), nfilter+1 each                      */
+    int    nr;             /* radii of coeff and jacobian                      */
+    int    nktype;         /* tmpker(0:nktype, ...) and coeff(.., 1:nktype, ..);
+                              >= 8 (the reference's nktype is 8)              */
+    const double *coeff;   /* coeff(0:nfilter, 1:nktype, 1:nr,
+                              iwin_start:iwin_end), host                      */
+    const void *jacobian;  /* jacobianFuji(1:nr, fmin:fmax) complex128, host;
+                              needed for DSM_KER_VS                          */
+} dsm_cat_kernel_params_t;
+
+int dsm_cat_set_kernel_params(dsm_cat_t *cat, const dsm_cat_kernel_params_t *kp);
+
+/* Kernels of npoint points.  ir[p] (0-based) selects point p's radius in
+ * coeff and jacobian; h3 and h4 are complex128 [point][6][fmax-fmin+1]
+ * (rr, tt, pp, rt, rp, tp, as rsgt2h3freq / tsgt2h4freq order them; e.g.
+ * the output of dsm_cat_spectra with the per-point combinations), on the
+ * device when spectra_on_device = 1.  ker receives tmpker(0:nktype,
+ * 0:nfilter) of every point, [point][nfilter+1][nktype+1] (types not
+ * computed are 0).  filtered (NULL: not written) receives the filtered
+ * series duf of P, duf of S and duqf, each present type's series in that
+ * order, [point][series][nfilter+1][nwin].  With out_on_device = 1, ker
+ * and filtered are device pointers. */
+int dsm_cat_kernels(dsm_cat_t *cat, int npoint, const int *ir, const void *h3, const void *h4,
+                    int spectra_on_device, double *ker, double *filtered, int out_on_device);
+
 /* Per-stage device time of the last dsm_cat_series when profiling is on:
  * kern[] holds cat_interp, cat_fft, cat_window (ms, launches, algorithmic
  * bytes); ms_total covers the whole call. */

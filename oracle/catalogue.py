@@ -28,6 +28,7 @@ node); the reference itself (Fortran) cannot be built here.
 """
 from __future__ import annotations
 
+import cmath
 import math
 from functools import lru_cache
 
@@ -270,3 +271,156 @@ def series(p: dict, sets, distances, coef=None) -> np.ndarray:
         outs.append(vector_fft_double(h, p["fmin"], p["fmax"], p["np1"], p["omegai"], p["tlen"],
                                       p["iwin_start"], p["iwin_end"]))
     return np.stack(outs)
+
+
+# ---------------------------------------------------------------------------
+# Per-point isotropic kernels: calculateKernel's isovpfreq / isovsfreq with
+# the Butterworth filter of bwfilt.f90 and the trapezoid sum over nt1..nt2.
+# ---------------------------------------------------------------------------
+
+def _f32(x: float) -> float:
+    """A real rounded to single precision (Fortran cmplx() without a kind)."""
+    return float(np.float32(x))
+
+
+def bpcoeff(f1: float, f2: float, npoles: int, dt: float):
+    """bpcoeff (src/KernelMaker/bwfilt.f90:124-166): coefficients a, b1, b2
+    of the npoles second-order sections of the recursive band-pass.
+
+    The reference forms the poles through single-precision complex values:
+    cexp(cmplx(0, phase)) is a single-precision exponential (here cos and
+    sin rounded to single), and cmplx(w0, 0), cmplx(w1 w2, 0) round their
+    real parts to single.  Only s(1..npoles) of the 2 npoles roots enter
+    the coefficients (:154-162)."""
+    if npoles > 10:
+        raise ValueError("npoles greater than 10")
+    pi = 3.141592653589793
+    d2 = 2.0 / dt
+    w1 = d2 * math.tan(2.0 * pi * f1 / d2)
+    w2 = d2 * math.tan(2.0 * pi * f2 / d2)
+    w0 = 0.5 * (w2 - w1)
+    s = []
+    for n in range(1, npoles + 1):
+        ph = _f32(float(2 * n - 1 + npoles) * pi / float(2 * npoles))
+        p = complex(_f32(math.cos(ph)), _f32(math.sin(ph)))
+        t1 = p * complex(_f32(w0), 0.0)
+        t2 = cmath.sqrt(t1 * t1 - complex(_f32(w1 * w2), 0.0))
+        s += [t1 + t2, t1 - t2]
+    a = np.zeros(npoles)
+    b1 = np.zeros(npoles)
+    b2 = np.zeros(npoles)
+    for n in range(npoles):
+        ssum = 2.0 * s[n].real
+        sprod = (s[n] * s[n].conjugate()).real
+        fact1 = d2 * d2 - d2 * ssum + sprod
+        fact2 = 2.0 * (sprod - d2 * d2)
+        fact3 = d2 * d2 + d2 * ssum + sprod
+        a[n] = 2.0 * d2 * w0 / fact1
+        b1[n] = fact2 / fact1
+        b2[n] = fact3 / fact1
+    return a, b1, b2
+
+
+def rekurs(x: np.ndarray, a, b1, b2) -> np.ndarray:
+    """rekurs (bwfilt.f90:54-117), forward pass only (irek = 0, as
+    calculateK.f90 calls bwfilt), vectorised over the leading axes of x
+    (samples on the last axis)."""
+    x = np.asarray(x, np.float64)
+    npoles = len(a)
+    lead = x.shape[:-1]
+    z1 = [np.zeros(lead) for _ in range(npoles)]
+    z2 = [np.zeros(lead) for _ in range(npoles)]
+    x1 = np.zeros(lead)
+    x2 = np.zeros(lead)
+    y = np.empty_like(x)
+    for n in range(x.shape[-1]):
+        z = [None] * npoles
+        z[0] = a[0] * (x[..., n] - x2) - b1[0] * z1[0] - b2[0] * z2[0]
+        for i in range(1, npoles):
+            z[i] = a[i] * (z[i - 1] - z2[i - 1]) - b1[i] * z1[i] - b2[i] * z2[i]
+        x2 = x1
+        x1 = x[..., n]
+        z2 = z1
+        z1 = z
+        y[..., n] = z[npoles - 1]
+    return y
+
+
+def iso_products(h3: np.ndarray, h4: np.ndarray, jac=None, types: int = 3):
+    """The frequency products of isovpfreq (calculateK.f90:261-265) and
+    isovsfreq (:367-374, :395-403) for h3, h4 [..., 6, nf]; jac [..., nf]
+    is jacobianFuji at the point's radius.  Returns the spectra in the
+    order P (du), S (du), S (duq) of the types present."""
+    out = []
+    if types & 1:
+        out.append(-(h3[..., 0, :] + h3[..., 1, :] + h3[..., 2, :])
+                   * (h4[..., 0, :] + h4[..., 1, :] + h4[..., 2, :]) * 1.0e3)
+    if types & 2:
+        p4 = h3[..., 3, :] * h4[..., 3, :]
+        p5 = h3[..., 4, :] * h4[..., 4, :]
+        p6 = h3[..., 5, :] * h4[..., 5, :]
+        c1 = h3[..., 0, :] * (h4[..., 1, :] + h4[..., 2, :])
+        c2 = h3[..., 1, :] * (h4[..., 0, :] + h4[..., 2, :])
+        c3 = h3[..., 2, :] * (h4[..., 0, :] + h4[..., 1, :])
+        du = (-2.0 * (p4 + p5 + p6) + c1 + c2 + c3) * 1.0e3
+        d1 = h3[..., 0, :] * h4[..., 0, :]
+        d2 = h3[..., 1, :] * h4[..., 1, :]
+        d3 = h3[..., 2, :] * h4[..., 2, :]
+        duq = (-(4.0 * (p4 + p5 + p6)) + 2.0 / 3.0 * (c1 + c2 + c3) - 4.0 / 3.0 * (d1 + d2 + d3))
+        duq = duq * jac * 1.0e3
+        out += [du, duq]
+    return np.stack(out, axis=-2)
+
+
+# (series, coeff type) pairs whose trapezoid sums fill tmpker: P du -> 1, 3, 4;
+# S du -> 5, 7; S duq -> 8 (calculateK.f90:302-321, :497-513)
+def _series_types(types: int):
+    st = []
+    if types & 1:
+        st.append((1, 3, 4))
+    if types & 2:
+        st += [(5, 7), (8,)]
+    return st
+
+
+def iso_kernels(p: dict, kp: dict, ir, h3, h4):
+    """tmpker [point][nfilter+1][nktype+1] and the filtered series
+    [point][series][nfilter+1][nwin] of calculateKernel's isotropic part.
+
+    p: the catalogue parameters (fmin, fmax, np1, tlen, omegai, iwin_start,
+       iwin_end); kp: types, nfilter, fclp, fchp, npoles, sampling_hz, nt1,
+       nt2, nr, nktype, coeff (Fortran order, as a flat array), jacobian
+       (Fortran order, complex128 flat)."""
+    ir = np.asarray(ir)
+    h3 = np.asarray(h3, np.complex128)
+    h4 = np.asarray(h4, np.complex128)
+    nf = p["fmax"] - p["fmin"] + 1
+    iws, iwe = p["iwin_start"], p["iwin_end"]
+    nwin = iwe - iws + 1
+    nfl, nkt, nr = kp["nfilter"] + 1, kp["nktype"], kp["nr"]
+    jac = None
+    if kp["types"] & 2:
+        jac = np.asarray(kp["jacobian"], np.complex128).reshape(nf, nr).T[ir]   # [point][nf]
+    spec = iso_products(h3, h4, jac, kp["types"])                            # [point][series][nf]
+    du = vector_fft_double(spec, p["fmin"], p["fmax"], p["np1"], p["omegai"], p["tlen"], iws, iwe)
+    coeff = np.asarray(kp["coeff"], np.float64).reshape(nwin, nr, nkt, nfl)   # [t][ir][k-1][ift]
+    npt, ns = du.shape[0], du.shape[1]
+    filt = np.empty((npt, ns, nfl, nwin))
+    ker = np.zeros((npt, nfl, nkt + 1))
+    dt = 1.0 / kp["sampling_hz"]
+    st = _series_types(kp["types"])
+    for f in range(nfl):
+        a, b1, b2 = bpcoeff(kp["fclp"][f], kp["fchp"][f], kp["npoles"], dt)
+        y = rekurs(du, a, b1, b2)                                             # [point][series][nwin]
+        filt[:, :, f, :] = y
+        t1, t2 = kp["nt1"][f] - iws, kp["nt2"][f] - iws
+        for s, ks in enumerate(st):
+            for k in ks:
+                c = coeff[:, ir, k - 1, f].T                                  # [point][nwin]
+                acc = np.zeros(npt)
+                acc = acc + c[:, t1] * y[:, s, t1] / 2.0
+                for t in range(t1 + 1, t2):
+                    acc = acc + c[:, t] * y[:, s, t]
+                acc = acc + c[:, t2] * y[:, s, t2] / 2.0
+                ker[:, f, k] = acc
+    return ker, filt

@@ -1,0 +1,191 @@
+"""Per-point isotropic kernels on the device (dsm_cat_set_kernel_params,
+dsm_cat_kernels: calculateKernel's isovpfreq / isovsfreq, the Butterworth
+filter of bwfilt and the trapezoid sum) against the oracle restatement.
+
+Bar: 1e-10 relative L2 on every point's tmpker and on the filtered series
+(FP64 throughout; the differences are the transform's rounding carried
+through the recursive filter).  Cases: both kernel families and each alone,
+several filters with their own integration windows (nt1 = nt2 included),
+1, 4 and 10 filter sections, points at several radii, host and device
+spectra and outputs, batches split by the buffer limit (identical results),
+the composition with dsm_cat_spectra on a record set, a larger transform,
+and argument checks that leave the handle usable."""
+import numpy as np
+import pytest
+
+import dsmsgt
+from conftest import rel_l2
+
+TOL = 1e-10
+
+
+def _params(**kw):
+    p = dict(num=20, theta_n=61, theta_min=0.0, theta_delta=0.5, fmin=0, fmax=48, np1=64, tlen=819.2,
+             omegai=np.log(100.0) / 819.2, ipdistance=5.0, c_red_reci=0.0, iwin_start=3, iwin_end=120)
+    p.update(kw)
+    return p
+
+
+def _kparams(p, nr, nfilter, types, rng, npoles=4):
+    nwin = p["iwin_end"] - p["iwin_start"] + 1
+    nf = p["fmax"] - p["fmin"] + 1
+    fs = 2 * p["np1"] / p["tlen"]
+    nt1 = [p["iwin_start"] + 5 + k for k in range(nfilter + 1)]
+    nt2 = [p["iwin_end"] - 7 - 2 * k for k in range(nfilter + 1)]
+    if nfilter >= 2:
+        nt2[2] = nt1[2]                     # a one-sample window: both half weights
+    return dict(types=types, nfilter=nfilter,
+                fclp=[fs * 0.02 * (k + 1) for k in range(nfilter + 1)],
+                fchp=[fs * 0.2 + fs * 0.02 * k for k in range(nfilter + 1)],
+                npoles=npoles, sampling_hz=fs, nt1=nt1, nt2=nt2,
+                coeff=rng.standard_normal((nwin, nr, 8, nfilter + 1)),
+                jacobian=rng.standard_normal((nf, nr)) + 1j * rng.standard_normal((nf, nr)))
+
+
+def _spectra(rng, npoint, nf):
+    shp = (npoint, 6, nf)
+    return (rng.standard_normal(shp) + 1j * rng.standard_normal(shp),
+            rng.standard_normal(shp) + 1j * rng.standard_normal(shp))
+
+
+def _oracle(p, kp, ir, h3, h4):
+    from oracle import catalogue as cat
+    q = dict(kp, nr=kp["coeff"].shape[1], nktype=kp["coeff"].shape[2])
+    return cat.iso_kernels(p, q, ir, h3, h4)
+
+
+def _device(p, kp, ir, h3, h4, batch_bytes=None):
+    c = dsmsgt.Catalogue(p)
+    if batch_bytes:
+        c.set_batch_bytes(batch_bytes)
+    c.set_kernel_params(kp["types"], kp["nfilter"], kp["fclp"], kp["fchp"], kp["npoles"], kp["sampling_hz"],
+                        kp["nt1"], kp["nt2"], kp["coeff"], kp["jacobian"])
+    ker, filt = c.kernels(ir, h3, h4, filtered=True)
+    c.close()
+    return ker, filt
+
+
+def _check(got, want):
+    ker, filt = got
+    wk, wf = want
+    assert ker.shape == wk.shape and filt.shape == wf.shape
+    assert rel_l2(filt, wf) <= TOL
+    assert rel_l2(ker, wk) <= TOL
+    for k in range(ker.shape[0]):
+        assert rel_l2(ker[k], wk[k]) <= TOL, k
+    assert np.all(ker[wk == 0.0] == 0.0)     # types not computed stay zero
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("types", [1, 2, 3])
+@pytest.mark.parametrize("npoles", [1, 4, 10])
+def test_kernels_match_oracle(built, types, npoles):
+    rng = np.random.default_rng(100 + 10 * types + npoles)
+    p = _params()
+    nf = p["fmax"] - p["fmin"] + 1
+    kp = _kparams(p, 4, 2, types, rng, npoles)
+    ir = np.array([0, 3, 1, 1, 2, 3, 0])
+    h3, h4 = _spectra(rng, ir.size, nf)
+    _check(_device(p, kp, ir, h3, h4), _oracle(p, kp, ir, h3, h4))
+
+
+@pytest.mark.gpu
+def test_kernels_partial_spectrum_and_batches(built):
+    rng = np.random.default_rng(7)
+    p = _params(fmin=5, fmax=64, iwin_start=0, iwin_end=127)
+    nf = p["fmax"] - p["fmin"] + 1
+    kp = _kparams(p, 2, 1, 3, rng)
+    ir = rng.integers(0, 2, 37)
+    h3, h4 = _spectra(rng, ir.size, nf)
+    want = _oracle(p, kp, ir, h3, h4)
+    one = _device(p, kp, ir, h3, h4)
+    _check(one, want)
+    # one point per batch: the same kernels and series, bit for bit
+    small = _device(p, kp, ir, h3, h4, batch_bytes=1 << 20)
+    assert np.array_equal(one[0], small[0]) and np.array_equal(one[1], small[1])
+
+
+@pytest.mark.gpu
+def test_kernels_device_pointers_and_spectra_composition(built):
+    import torch
+    rng = np.random.default_rng(9)
+    p = _params(c_red_reci=6.0)
+    nf = p["fmax"] - p["fmin"] + 1
+    rec = (rng.standard_normal((nf, p["theta_n"], 20)) + 1j * rng.standard_normal((nf, p["theta_n"], 20)))
+    dist = np.array([1.3, 7.25, 12.0, 29.0])
+    coef3 = rng.standard_normal((dist.size, 6, 20))
+    coef4 = rng.standard_normal((dist.size, 6, 20))
+    c = dsmsgt.Catalogue(p)
+    c.add(rec.astype(np.complex64))
+    h3 = c.spectra(dist, coef3)
+    h4 = c.spectra(dist, coef4)
+    kp = _kparams(p, 3, 0, 3, rng)
+    c.set_kernel_params(kp["types"], kp["nfilter"], kp["fclp"], kp["fchp"], kp["npoles"], kp["sampling_hz"],
+                        kp["nt1"], kp["nt2"], kp["coeff"], kp["jacobian"])
+    ir = np.array([2, 0, 1, 2])
+    host = c.kernels(ir, h3, h4, filtered=True)
+    _check(host, _oracle(p, kp, ir, h3, h4))
+    d3 = torch.from_numpy(h3).cuda()
+    d4 = torch.from_numpy(h4).cuda()
+    dev = c.kernels(ir, d3, d4, filtered=True)
+    assert np.array_equal(host[0], dev[0]) and np.array_equal(host[1], dev[1])
+    # device outputs through the C-ABI directly
+    ko = torch.zeros(host[0].shape, dtype=torch.float64, device="cuda")
+    fo = torch.zeros(host[1].shape, dtype=torch.float64, device="cuda")
+    irr = np.ascontiguousarray(ir, np.int32)
+    rc = dsmsgt.lib().dsm_cat_kernels(c.h, ir.size, dsmsgt._ptr(irr, dsmsgt._ip), d3.data_ptr(), d4.data_ptr(), 1,
+                                      ko.data_ptr(), fo.data_ptr(), 1)
+    assert rc == 0
+    assert np.array_equal(ko.cpu().numpy(), host[0]) and np.array_equal(fo.cpu().numpy(), host[1])
+    c.close()
+
+
+@pytest.mark.gpu
+def test_kernels_larger_transform(built):
+    rng = np.random.default_rng(21)
+    p = _params(fmax=700, np1=1024, tlen=3276.8, omegai=np.log(100.0) / 3276.8, iwin_start=100,
+                iwin_end=1800)
+    nf = p["fmax"] - p["fmin"] + 1
+    kp = _kparams(p, 5, 3, 3, rng)
+    ir = rng.integers(0, 5, 96)
+    h3, h4 = _spectra(rng, ir.size, nf)
+    _check(_device(p, kp, ir, h3, h4), _oracle(p, kp, ir, h3, h4))
+
+
+@pytest.mark.gpu
+def test_kernels_reject_bad_calls_and_stay_usable(built):
+    rng = np.random.default_rng(4)
+    p = _params()
+    nf = p["fmax"] - p["fmin"] + 1
+    kp = _kparams(p, 2, 0, 3, rng)
+    h3, h4 = _spectra(rng, 2, nf)
+    c = dsmsgt.Catalogue(p)
+    with pytest.raises(dsmsgt.DsmError, match="set_kernel_params has not been called"):
+        c._ker_shape, c._ker_ns = (1, 9), 3
+        c.kernels([0, 1], h3, h4)
+
+    def setp(**kw):
+        q = dict(kp)
+        q.update(kw)
+        c.set_kernel_params(q["types"], q["nfilter"], q["fclp"], q["fchp"], q["npoles"], q["sampling_hz"],
+                            q["nt1"], q["nt2"], q["coeff"], q["jacobian"])
+
+    with pytest.raises(dsmsgt.DsmError, match="npoles"):
+        setp(npoles=11)
+    with pytest.raises(dsmsgt.DsmError, match="nt1/nt2"):
+        setp(nt1=[p["iwin_start"] - 1])
+    with pytest.raises(dsmsgt.DsmError, match="nt1/nt2"):
+        setp(nt1=[50], nt2=[40])
+    with pytest.raises(dsmsgt.DsmError, match="jacobianFuji"):
+        setp(jacobian=None)
+    bad = kp["coeff"].copy()
+    bad[3, 1, 4, 0] = np.nan
+    with pytest.raises(dsmsgt.DsmError, match="non-finite coeff"):
+        setp(coeff=bad)
+    setp()
+    with pytest.raises(dsmsgt.DsmError, match="radius index"):
+        c.kernels([0, 2], h3, h4)
+    ker, filt = c.kernels([1, 0], h3, h4, filtered=True)
+    want = _oracle(p, kp, np.array([1, 0]), h3, h4)
+    _check((ker, filt), want)
+    c.close()
