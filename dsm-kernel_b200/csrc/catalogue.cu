@@ -1274,6 +1274,118 @@ extern "C" int dsm_cat_kernels(dsm_cat_t* c, int npoint, const int* ir, const vo
     });
 }
 
+namespace {
+// a real combination of the catalogue components (the coefficient row of one
+// h3 / h4 entry), with the arithmetic the reference's formulas use
+template <int N>
+struct Comb {
+    double c[N] = {};
+    static Comb e(int k) {   // component k (1-based, as tsgtF(k) / rsgtF(k))
+        Comb r;
+        r.c[k - 1] = 1.0;
+        return r;
+    }
+    friend Comb operator+(Comb a, const Comb& b) {
+        for (int i = 0; i < N; ++i) a.c[i] += b.c[i];
+        return a;
+    }
+    friend Comb operator-(Comb a, const Comb& b) {
+        for (int i = 0; i < N; ++i) a.c[i] -= b.c[i];
+        return a;
+    }
+    friend Comb operator-(Comb a) {
+        for (int i = 0; i < N; ++i) a.c[i] = -a.c[i];
+        return a;
+    }
+    friend Comb operator*(Comb a, double m) {
+        for (int i = 0; i < N; ++i) a.c[i] *= m;
+        return a;
+    }
+};
+}  // namespace
+
+extern "C" int dsm_cat_h3h4_coef(int npoint, const double* ang, char compo, const double* mt, double* coef3,
+                                 double* coef4) {
+    return cat_guard(nullptr, [&] {
+        const char* fn = "dsm_cat_h3h4_coef";
+        need(npoint >= 0 && (npoint == 0 || ang), std::string(fn) + ": null argument");
+        need(!coef4 || mt, std::string(fn) + ": h4 needs the moment tensor");
+        need(!coef3 || compo == 'Z' || compo == 'R' || compo == 'T', std::string(fn) + ": compo must be Z, R or T");
+        using C10 = Comb<10>;
+        using C20 = Comb<20>;
+        for (int p = 0; p < npoint; ++p) {
+            const double* a = ang + (size_t)p * 12;
+            for (int k = 0; k < 12; ++k) need(std::isfinite(a[k]), std::string(fn) + ": non-finite angle factor");
+            const double crq = a[0], srq = a[1], crq2 = a[2], srq2 = a[3];
+            const double csq = a[4], ssq = a[5], csq2 = a[6], ssq2 = a[7];
+            const double cqs = a[8], sqs = a[9], cqs2 = a[10], sqs2 = a[11];
+            if (coef3) {
+                // rsgt2h3freq (fourier.f90:278-320); order rr, tt, pp, rt, rp, tp
+                C10 h[6];
+                auto F = [](int k) { return C10::e(k); };
+                if (compo == 'Z') {
+                    h[0] = F(1);
+                    h[1] = F(3) * crq2 - F(4);
+                    h[2] = -F(3) * crq2 - F(4);
+                    h[3] = F(2) * (2.0 * crq);
+                    h[4] = F(2) * (2.0 * srq);
+                    h[5] = F(3) * (2.0 * srq2);
+                } else if (compo == 'R') {
+                    h[0] = F(5);
+                    h[1] = -F(7) * crq2 - F(6);
+                    h[2] = F(7) * crq2 - F(6);
+                    h[3] = F(9) * (4.0 * crq);
+                    h[4] = F(9) * (4.0 * srq);
+                    h[5] = F(7) * (-2.0 * srq2);
+                } else {
+                    // the reference writes h3(3) = -h3(3) (:314), negating the
+                    // previous call's value; the transverse pp entry is -tt
+                    h[1] = F(8) * srq2;
+                    h[2] = -h[1];
+                    h[3] = F(10) * (2.0 * srq);
+                    h[4] = F(10) * (-2.0 * crq);
+                    h[5] = F(8) * (-2.0 * crq2);
+                }
+                for (int j = 0; j < 6; ++j)
+                    for (int k = 0; k < 10; ++k) coef3[((size_t)p * 6 + j) * 10 + k] = h[j].c[k];
+            }
+            if (coef4) {
+                // tsgt2h4freq (fourier.f90:322-415): the 4th-order TSGT
+                // double-dotted with the moment tensor mt(1..6)
+                auto F = [](int k) { return C20::e(k); };
+                const C20 t01 = F(7) * cqs, t02 = F(7) * sqs, t03 = F(8) * csq, t04 = F(8) * ssq;
+                const C20 t05 = F(9) * cqs2, t06 = F(10) * csq2, t07 = F(11) * csq2, t08 = F(11) * ssq2;
+                const C20 t09 = F(12) * cqs2, t10 = F(12) * sqs2;
+                const C20 t11 = F(13) * (csq * cqs - ssq * sqs), t12 = F(13) * (ssq * cqs + csq * sqs);
+                const C20 t13 = F(14) * (csq * cqs + ssq * sqs), t14 = F(14) * (ssq * cqs - csq * sqs);
+                const C20 t15 = F(15) * (csq2 * cqs - ssq2 * sqs), t16 = F(15) * (ssq2 * cqs + csq2 * sqs);
+                const C20 t17 = F(17) * (csq * cqs2 - ssq * sqs2), t18 = F(17) * (ssq * cqs2 + csq * sqs2);
+                const C20 t19 = F(19) * (csq2 * cqs2 - ssq2 * sqs2), t20 = F(19) * (ssq2 * cqs2 + csq2 * sqs2);
+                const C20 t21 = F(20) * (csq2 * cqs2 + ssq2 * sqs2), t22 = F(20) * (ssq2 * cqs2 - csq2 * sqs2);
+                const C20 t23 = F(16) * (csq2 * cqs + ssq2 * sqs), t24 = F(16) * (ssq2 * cqs - csq2 * sqs);
+                const C20 t25 = F(18) * (csq * cqs2 + ssq * sqs2), t26 = F(18) * (ssq * cqs2 - csq * sqs2);
+                C20 h[6];
+                h[0] = F(1) * mt[0] + (t05 - F(2)) * mt[1] + (-t05 - F(2)) * mt[2] -
+                       F(5) * (cqs * mt[3] + sqs * mt[4]) + F(9) * (sqs2 * mt[5]);
+                h[1] = (t06 - F(3)) * mt[0] + (t21 + t19 - t07 - t09 + F(4)) * mt[1] +
+                       (-t21 - t19 - t07 + t09 + F(4)) * mt[2] + (t23 - t15 + t01) * mt[3] +
+                       (-t24 - t16 + t02) * mt[4] + (-t22 + t20 - t10) * mt[5];
+                h[2] = (-t06 - F(3)) * mt[0] + (-t21 - t19 + t07 - t09 + F(4)) * mt[1] +
+                       (t21 + t19 + t07 + t09 + F(4)) * mt[2] + (-t23 + t15 + t01) * mt[3] +
+                       (t24 + t16 + t02) * mt[4] + (t22 - t20 - t10) * mt[5];
+                h[3] = -F(6) * (csq * mt[0]) + (t25 - t17 + t03) * mt[1] + (-t25 + t17 + t03) * mt[2] +
+                       (-t13 + t11) * mt[3] + (t14 + t12) * mt[4] + (-t26 - t18) * mt[5];
+                h[4] = -F(6) * (ssq * mt[0]) + (t26 - t18 + t04) * mt[1] + (-t26 + t18 + t04) * mt[2] +
+                       (-t14 + t12) * mt[3] + (-t13 - t11) * mt[4] + (t25 + t17) * mt[5];
+                h[5] = F(10) * (ssq2 * mt[0]) + (t22 + t20 - t08) * mt[1] + (-t22 - t20 - t08) * mt[2] +
+                       (t24 - t16) * mt[3] + (t23 + t15) * mt[4] + (t21 - t19) * mt[5];
+                for (int j = 0; j < 6; ++j)
+                    for (int k = 0; k < 20; ++k) coef4[((size_t)p * 6 + j) * 20 + k] = h[j].c[k];
+            }
+        }
+    });
+}
+
 extern "C" int dsm_cat_set_profiling(dsm_cat_t* c, int on) {
     if (!c) return DSM_ERR_INVALID;
     c->profiling = on != 0;

@@ -218,6 +218,7 @@ def lib() -> C.CDLL:
         L.dsm_cat_series.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_void_p, C.c_int]
         L.dsm_cat_spectra.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_void_p, C.c_int]
         L.dsm_cat_transform.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+        L.dsm_cat_h3h4_coef.argtypes = [C.c_int, _dp, C.c_char, _dp, C.c_void_p, C.c_void_p]
         L.dsm_cat_set_kernel_params.argtypes = [C.c_void_p, C.POINTER(CatKernelParams)]
         L.dsm_cat_kernels.argtypes = [C.c_void_p, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                       C.c_void_p, C.c_int]
@@ -696,6 +697,22 @@ def fp64_peak(device: int = 0, mma: bool = False) -> float:
     if rc:
         raise DsmError(f"dsm_fp64_peak failed ({rc}): {lib().dsm_cat_last_error(None).decode()}")
     return v.value
+
+
+def cat_h3h4_coef(ang, compo: str = "Z", mt=None):
+    """Combination matrices of rsgt2h3freq ([point][6][10]) and
+    tsgt2h4freq ([point][6][20], None without mt) for points with the 12
+    angle factors ang [point][12] (dsm_cat_h3h4_coef; host only)."""
+    a = np.ascontiguousarray(ang, np.float64).reshape(-1, 12)
+    n = a.shape[0]
+    c3 = np.zeros((n, 6, 10), np.float64)
+    c4 = None if mt is None else np.zeros((n, 6, 20), np.float64)
+    m = None if mt is None else np.ascontiguousarray(mt, np.float64)
+    rc = lib().dsm_cat_h3h4_coef(n, _ptr(a, _dp), compo.encode(), None if m is None else _ptr(m, _dp),
+                                 C.c_void_p(c3.ctypes.data), None if c4 is None else C.c_void_p(c4.ctypes.data))
+    if rc:
+        raise DsmError(f"dsm_cat_h3h4_coef failed ({rc}): {lib().dsm_cat_last_error(None).decode()}", rc)
+    return c3, c4
 
 
 class Catalogue:

@@ -498,6 +498,23 @@ int dsm_cat_spectra(dsm_cat_t *cat, int npoint, const double *distance, int nout
 int dsm_cat_transform(dsm_cat_t *cat, int nseries, const void *spectra, int spectra_on_device,
                       double *out, int out_on_device);
 
+/* The per-point combination matrices that turn interpolated catalogue
+ * components into the h3 / h4 spectra of the kernel formulas, for
+ * dsm_cat_spectra's coef argument.  Replaces
+ *   rsgt2h3freq  src/KernelMaker/fourier.f90:278-320 (receiver side, 10
+ *                RSGT components, compo 'Z', 'R' or 'T')
+ *   tsgt2h4freq  src/KernelMaker/fourier.f90:322-415 (source side, 20 TSGT
+ *                components double-dotted with the moment tensor mt(1..6))
+ * ang holds per point the 12 factors of the angles module, in the order
+ * crq, srq, crq2, srq2, csq, ssq, csq2, ssq2, cqs, sqs, cqs2, sqs2
+ * (calculateSineCosine, src/KernelMaker/others.f90:768-826).  coef3
+ * receives [point][6][10], coef4 [point][6][20] (rows rr, tt, pp, rt, rp,
+ * tp); either may be NULL.  Host arithmetic only; needs no device.  For
+ * compo 'T' the pp row is minus the tt row (the reference negates the
+ * previous call's h3(3), fourier.f90:314). */
+int dsm_cat_h3h4_coef(int npoint, const double *ang, char compo, const double *mt, double *coef3,
+                      double *coef4);
+
 /* Per-point isotropic sensitivity kernels from the h3 / h4 spectra, the
  * body of KernelMaker's calculateKernel after its rsgt2h3freq /
  * tsgt2h4freq (src/KernelMaker/calculateK.f90:131-235):

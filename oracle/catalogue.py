@@ -424,3 +424,71 @@ def iso_kernels(p: dict, kp: dict, ir, h3, h4):
                 acc = acc + c[:, t2] * y[:, s, t2] / 2.0
                 ker[:, f, k] = acc
     return ker, filt
+
+
+def rsgt2h3freq(rsgtF, ang, compo: str):
+    """rsgt2h3freq (src/KernelMaker/fourier.f90:278-320) on interpolated
+    RSGT spectra rsgtF [10][nf] at one point; ang = (crq, srq, crq2, srq2,
+    ...) as the angles module holds them.  h3 [6][nf] in the order rr, tt,
+    pp, rt, rp, tp.  For compo 'T' the reference's h3(3) = -h3(3) (:314)
+    negates the previous point's value; the transverse pp entry is -tt."""
+    F = lambda k: rsgtF[k - 1]
+    crq, srq, crq2, srq2 = ang[0], ang[1], ang[2], ang[3]
+    h = np.zeros((6,) + np.shape(rsgtF[0]), np.complex128)
+    if compo == "Z":
+        h[0] = F(1)
+        h[1] = F(3) * crq2 - F(4)
+        h[2] = -F(3) * crq2 - F(4)
+        h[3] = 2.0 * F(2) * crq
+        h[4] = 2.0 * F(2) * srq
+        h[5] = 2.0 * F(3) * srq2
+    elif compo == "R":
+        h[0] = F(5)
+        h[1] = -(F(7)) * crq2 - F(6)
+        h[2] = (F(7)) * crq2 - F(6)
+        h[3] = 4.0 * (F(9)) * crq
+        h[4] = 4.0 * (F(9)) * srq
+        h[5] = -2.0 * (F(7)) * srq2
+    else:
+        h[1] = (F(8)) * srq2
+        h[2] = -h[1]
+        h[3] = 2.0 * (F(10)) * srq
+        h[4] = -2.0 * (F(10)) * crq
+        h[5] = -2.0 * (F(8)) * crq2
+    return h
+
+
+def tsgt2h4freq(tsgtF, ang, mt):
+    """tsgt2h4freq (src/KernelMaker/fourier.f90:322-415) on interpolated
+    TSGT spectra tsgtF [20][nf] at one point: the 4th-order TSGT double-
+    dotted with the moment tensor mt(1..6); h4 [6][nf]."""
+    F = lambda k: tsgtF[k - 1]
+    csq, ssq, csq2, ssq2, cqs, sqs, cqs2, sqs2 = ang[4:12]
+    m = mt
+    t01 = F(7) * cqs; t02 = F(7) * sqs; t03 = F(8) * csq; t04 = F(8) * ssq
+    t05 = F(9) * cqs2; t06 = F(10) * csq2; t07 = F(11) * csq2; t08 = F(11) * ssq2
+    t09 = F(12) * cqs2; t10 = F(12) * sqs2
+    t11 = F(13) * (csq * cqs - ssq * sqs); t12 = F(13) * (ssq * cqs + csq * sqs)
+    t13 = F(14) * (csq * cqs + ssq * sqs); t14 = F(14) * (ssq * cqs - csq * sqs)
+    t15 = F(15) * (csq2 * cqs - ssq2 * sqs); t16 = F(15) * (ssq2 * cqs + csq2 * sqs)
+    t17 = F(17) * (csq * cqs2 - ssq * sqs2); t18 = F(17) * (ssq * cqs2 + csq * sqs2)
+    t19 = F(19) * (csq2 * cqs2 - ssq2 * sqs2); t20 = F(19) * (ssq2 * cqs2 + csq2 * sqs2)
+    t21 = F(20) * (csq2 * cqs2 + ssq2 * sqs2); t22 = F(20) * (ssq2 * cqs2 - csq2 * sqs2)
+    t23 = F(16) * (csq2 * cqs + ssq2 * sqs); t24 = F(16) * (ssq2 * cqs - csq2 * sqs)
+    t25 = F(18) * (csq * cqs2 + ssq * sqs2); t26 = F(18) * (ssq * cqs2 - csq * sqs2)
+    h = np.zeros((6,) + np.shape(tsgtF[0]), np.complex128)
+    h[0] = (F(1) * m[0] + (t05 - F(2)) * m[1] + (-t05 - F(2)) * m[2]
+            - F(5) * (cqs * m[3] + sqs * m[4]) + F(9) * sqs2 * m[5])
+    h[1] = ((t06 - F(3)) * m[0] + (t21 + t19 - t07 - t09 + F(4)) * m[1]
+            + (-t21 - t19 - t07 + t09 + F(4)) * m[2] + (t23 - t15 + t01) * m[3]
+            + (-t24 - t16 + t02) * m[4] + (-t22 + t20 - t10) * m[5])
+    h[2] = ((-t06 - F(3)) * m[0] + (-t21 - t19 + t07 - t09 + F(4)) * m[1]
+            + (t21 + t19 + t07 + t09 + F(4)) * m[2] + (-t23 + t15 + t01) * m[3]
+            + (t24 + t16 + t02) * m[4] + (t22 - t20 - t10) * m[5])
+    h[3] = (-F(6) * csq * m[0] + (t25 - t17 + t03) * m[1] + (-t25 + t17 + t03) * m[2]
+            + (-t13 + t11) * m[3] + (t14 + t12) * m[4] + (-t26 - t18) * m[5])
+    h[4] = ((-F(6) * ssq) * m[0] + (t26 - t18 + t04) * m[1] + (-t26 + t18 + t04) * m[2]
+            + (-t14 + t12) * m[3] + (-t13 - t11) * m[4] + (t25 + t17) * m[5])
+    h[5] = (F(10) * ssq2 * m[0] + (t22 + t20 - t08) * m[1] + (-t22 - t20 - t08) * m[2]
+            + (t24 - t16) * m[3] + (t23 + t15) * m[4] + (t21 - t19) * m[5])
+    return h

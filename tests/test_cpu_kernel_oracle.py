@@ -137,3 +137,47 @@ def test_kernel_is_the_trapezoid_of_coeff_times_the_filtered_series():
                     assert abs(ker[pt, f, k] - want) <= 1e-12 * max(1.0, abs(want))
         for k in (0, 2, 6):
             assert np.all(ker[:, f, k] == 0.0)
+
+
+def _angles(rng, n):
+    ph = rng.uniform(0, 2 * np.pi, (n, 3))            # phirq, phisq, phiqs
+    cols = []
+    for k in range(3):
+        cols += [np.cos(ph[:, k]), np.sin(ph[:, k]), np.cos(2 * ph[:, k]), np.sin(2 * ph[:, k])]
+    return np.stack(cols, axis=1)                       # crq, srq, crq2, srq2, csq, ..., sqs2
+
+
+@pytest.mark.parametrize("compo", ["Z", "R", "T"])
+def test_c_abi_h3h4_matrices_reproduce_the_reference_formulas(built, compo):
+    """dsm_cat_h3h4_coef (host code, no device) against the oracle's
+    rsgt2h3freq / tsgt2h4freq applied to spectra: the matrices times the
+    components equal the formulas."""
+    import dsmsgt
+    rng = np.random.default_rng(ord(compo))
+    ang = _angles(rng, 5)
+    mt = rng.standard_normal(6)
+    c3, c4 = dsmsgt.cat_h3h4_coef(ang, compo, mt)
+    assert c3.shape == (5, 6, 10) and c4.shape == (5, 6, 20)
+    for p in range(5):
+        r = rng.standard_normal((10, 33)) + 1j * rng.standard_normal((10, 33))
+        t = rng.standard_normal((20, 33)) + 1j * rng.standard_normal((20, 33))
+        w3 = cat.rsgt2h3freq(r, ang[p], compo)
+        w4 = cat.tsgt2h4freq(t, ang[p], mt)
+        assert np.abs(c3[p] @ r - w3).max() <= 1e-13 * np.abs(w3).max()
+        assert np.abs(c4[p] @ t - w4).max() <= 1e-13 * np.abs(w4).max()
+    # each h4 row is linear in the moment tensor
+    mt2 = rng.standard_normal(6)
+    _, a = dsmsgt.cat_h3h4_coef(ang, compo, mt2)
+    _, b = dsmsgt.cat_h3h4_coef(ang, compo, mt + 2.0 * mt2)
+    assert np.abs(b - (c4 + 2.0 * a)).max() <= 1e-13 * np.abs(b).max()
+
+
+def test_c_abi_h3h4_rejects_bad_arguments(built):
+    import dsmsgt
+    ang = _angles(np.random.default_rng(0), 2)
+    with pytest.raises(dsmsgt.DsmError, match="compo"):
+        dsmsgt.cat_h3h4_coef(ang, "X")
+    bad = ang.copy()
+    bad[1, 3] = np.inf
+    with pytest.raises(dsmsgt.DsmError, match="non-finite"):
+        dsmsgt.cat_h3h4_coef(bad, "Z")

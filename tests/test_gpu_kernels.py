@@ -189,3 +189,56 @@ def test_kernels_reject_bad_calls_and_stay_usable(built):
     want = _oracle(p, kp, np.array([1, 0]), h3, h4)
     _check((ker, filt), want)
     c.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("compo", ["Z", "T"])
+def test_calculate_kernel_end_to_end(built, compo):
+    """calculateKernel for points of one radius from the records: the RSGT
+    catalogue interpolated at each point's receiver distance with the
+    rsgt2h3freq matrices, the TSGT catalogue at its source distance with the
+    tsgt2h4freq matrices (dsm_cat_h3h4_coef), then dsm_cat_kernels; against
+    the oracle's clsgt, rsgt2h3freq, tsgt2h4freq and iso_kernels."""
+    from oracle import catalogue as cat
+    rng = np.random.default_rng(55)
+    pr = _params(num=10, c_red_reci=4.0)
+    pt = _params(num=20, c_red_reci=4.0)
+    nf = pr["fmax"] - pr["fmin"] + 1
+    shp = (nf, pr["theta_n"])
+    rrec = (rng.standard_normal(shp + (10,)) + 1j * rng.standard_normal(shp + (10,))).astype(np.complex64)
+    trec = (rng.standard_normal(shp + (20,)) + 1j * rng.standard_normal(shp + (20,))).astype(np.complex64)
+    npt = 6
+    deltar = rng.uniform(2.0, 28.0, npt)
+    deltas = rng.uniform(2.0, 28.0, npt)
+    ph = rng.uniform(0, 2 * np.pi, (npt, 3))
+    ang = np.stack([f(m * ph[:, k]) for k in range(3) for m, f in ((1, np.cos), (1, np.sin), (2, np.cos), (2, np.sin))],
+                   axis=1)
+    mt = rng.standard_normal(6)
+    c3, c4 = dsmsgt.cat_h3h4_coef(ang, compo, mt)
+    cr = dsmsgt.Catalogue(pr)
+    cr.add(rrec)
+    ct = dsmsgt.Catalogue(pt)
+    ct.add(trec)
+    h3 = cr.spectra(deltar, c3)
+    h4 = ct.spectra(deltas, c4)
+    kp = _kparams(pt, 2, 1, 3, rng)
+    ct.set_kernel_params(kp["types"], kp["nfilter"], kp["fclp"], kp["fchp"], kp["npoles"], kp["sampling_hz"],
+                         kp["nt1"], kp["nt2"], kp["coeff"], kp["jacobian"])
+    ir = rng.integers(0, 2, npt)
+    got = ct.kernels(ir, h3, h4, filtered=True)
+    cr.close()
+    ct.close()
+    theta = pr["theta_min"] + np.arange(pr["theta_n"]) * pr["theta_delta"]
+    omr = cat.omega_sgt([(rrec, np.arange(10), np.ones(10))], 10, pr["fmin"], pr["fmax"], theta, pr["tlen"], 4.0)
+    omt = cat.omega_sgt([(trec, np.arange(20), np.ones(20))], 20, pt["fmin"], pt["fmax"], theta, pt["tlen"], 4.0)
+    w3, w4 = [], []
+    for k in range(npt):
+        fr = cat.clsgt(float(deltar[k]), omr, pr["fmin"], pr["theta_min"], pr["theta_delta"], pr["ipdistance"],
+                       pr["tlen"], 4.0)
+        ft = cat.clsgt(float(deltas[k]), omt, pt["fmin"], pt["theta_min"], pt["theta_delta"], pt["ipdistance"],
+                       pt["tlen"], 4.0)
+        w3.append(cat.rsgt2h3freq(fr.T, ang[k], compo))
+        w4.append(cat.tsgt2h4freq(ft.T, ang[k], mt))
+    w3, w4 = np.stack(w3), np.stack(w4)
+    assert rel_l2(h3, w3) <= TOL and rel_l2(h4, w4) <= TOL
+    _check(got, _oracle(pt, kp, ir, w3, w4))
