@@ -9,8 +9,9 @@ epicentral distances (0.125 deg).  A step is one batch of frequency slices
 (20 by default, --per-step) spread across the band, each fully processed
 (all orders up to the reference's cutoff, all m, all sources, TSGT + RSGT +
 SYNN on the full (r, theta) grid).  psv1024 (the FP64 configuration's
-band: 1024 frequencies, 721 distances), sh256, the catalogue consumer and
-the batched models x depths request are the other workloads.
+band: 1024 frequencies, 721 distances), sh256, the catalogue consumer, its
+per-point kernel formulas (kernels) and the batched models x depths request
+are the other workloads.
 
   python bench.py [--gpus N --steps K --warmup W] [--workload psv2048|psv1024|sh256|catalogue|kernels|batch]
                   [--precision mixed|mixed_bf16|fp64] [--per-step F]
