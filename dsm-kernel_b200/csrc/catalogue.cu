@@ -445,8 +445,11 @@ struct KerTimeArgs {
     double* filt;         // [point][ns][nfl][nwin] or null
 };
 
+constexpr int KER_TB = 32;   // one warp per block: the 3 x points x filters threads spread over every SM
+constexpr int KER_CH = 8;    // samples (and their coefficients) loaded ahead of the recursion
+
 template <int NP>
-__global__ void __launch_bounds__(128) k_ker_time(const KerTimeArgs a) {
+__global__ void __launch_bounds__(KER_TB) k_ker_time(const KerTimeArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.nb * a.ns * a.nfl) return;
     const int f = i % a.nfl, s = (i / a.nfl) % a.ns, b = i / (a.nfl * a.ns);
@@ -454,10 +457,9 @@ __global__ void __launch_bounds__(128) k_ker_time(const KerTimeArgs a) {
     // series kind: 0 P du (types 1, 3, 4), 1 S du (5, 7), 2 S duq (8)
     const int kind = (a.types & DSM_KER_VP) ? s : s + 1;
     const int nk = kind == 0 ? 3 : kind == 1 ? 2 : 1;
-    int kt[3];
-    kt[0] = kind == 0 ? 1 : kind == 1 ? 5 : 8;
-    kt[1] = kind == 0 ? 3 : 7;
-    kt[2] = 4;
+    const int kt0 = kind == 0 ? 1 : kind == 1 ? 5 : 8;
+    const int kt1 = kind == 0 ? 3 : kind == 1 ? 7 : kt0;
+    const int kt2 = kind == 0 ? 4 : kt1;
     double A[NP], B1[NP], B2[NP], z1[NP], z2[NP];
     const double* fc = a.fc + (size_t)f * 3 * KER_MAXNP;
 #pragma unroll
@@ -474,36 +476,72 @@ __global__ void __launch_bounds__(128) k_ker_time(const KerTimeArgs a) {
     const double* yr = a.y + ((size_t)b * a.ns + s) * a.row + a.iws;
     const size_t cstride = (size_t)a.nfl * a.nktype * a.nr;
     const double* cb = a.coeff + (size_t)a.ir[pt] * a.nktype * a.nfl + f;
+    const size_t o0 = (size_t)(kt0 - 1) * a.nfl, o1 = (size_t)(kt1 - 1) * a.nfl, o2 = (size_t)(kt2 - 1) * a.nfl;
     double* fo = a.filt ? a.filt + (((size_t)pt * a.ns + s) * a.nfl + f) * a.nwin : nullptr;
-    double acc[3] = {0.0, 0.0, 0.0};
-    for (int t = 0; t < tend; ++t) {
-        const double x = yr[t] * a.e[t] / a.tlen * 1.0e3;
-        double z[NP];
-        z[0] = A[0] * (x - x2) - B1[0] * z1[0] - B2[0] * z2[0];
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    for (int t0 = 0; t0 < tend; t0 += KER_CH) {
+        // the chunk's samples and coefficients first (independent loads, all
+        // in flight together); indices clamped into the window, so every
+        // load stays inside the transform row and coeff
+        double xs[KER_CH], c0[KER_CH], c1[KER_CH], c2[KER_CH];
 #pragma unroll
-        for (int k = 1; k < NP; ++k) z[k] = A[k] * (z[k - 1] - z2[k - 1]) - B1[k] * z1[k] - B2[k] * z2[k];
-        x2 = x1;
-        x1 = x;
-#pragma unroll
-        for (int k = 0; k < NP; ++k) {
-            z2[k] = z1[k];
-            z1[k] = z[k];
+        for (int j = 0; j < KER_CH; ++j) {
+            const int t = min(t0 + j, tend - 1);
+            xs[j] = yr[t] * a.e[t] / a.tlen * 1.0e3;
         }
-        const double v = z[NP - 1];
-        if (fo) fo[t] = v;
-        if (t < t1 || t > t2) continue;
-        const double* c = cb + (size_t)t * cstride;
-        for (int j = 0; j < nk; ++j) {
-            const double ck = c[(size_t)(kt[j] - 1) * a.nfl];
+        const bool in = t0 + KER_CH > t1 && t0 <= t2;
+        if (in) {
+#pragma unroll
+            for (int j = 0; j < KER_CH; ++j) {
+                const double* c = cb + (size_t)min(max(t0 + j, t1), t2) * cstride;
+                c0[j] = c[o0];
+                c1[j] = c[o1];
+                c2[j] = c[o2];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < KER_CH; ++j) {
+            const int t = t0 + j;
+            if (t >= tend) break;
+            double z[NP];
+            z[0] = A[0] * (xs[j] - x2) - B1[0] * z1[0] - B2[0] * z2[0];
+#pragma unroll
+            for (int k = 1; k < NP; ++k) z[k] = A[k] * (z[k - 1] - z2[k - 1]) - B1[k] * z1[k] - B2[k] * z2[k];
+            x2 = x1;
+            x1 = xs[j];
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                z2[k] = z1[k];
+                z1[k] = z[k];
+            }
+            const double v = z[NP - 1];
+            if (fo) fo[t] = v;
+            if (t < t1 || t > t2) continue;
             // isovpfreq halves as coeff * duf / 2, isovsfreq as 0.5 * coeff * duf
-            const double half = kind == 0 ? ck * v / 2.0 : 0.5 * ck * v;
-            if (t == t1) acc[j] = acc[j] + half;
-            if (t > t1 && t < t2) acc[j] = acc[j] + ck * v;
-            if (t == t2) acc[j] = acc[j] + half;
+            const double h0 = kind == 0 ? c0[j] * v / 2.0 : 0.5 * c0[j] * v;
+            const double h1 = kind == 0 ? c1[j] * v / 2.0 : 0.5 * c1[j] * v;
+            const double h2 = c2[j] * v / 2.0;
+            if (t == t1) {
+                acc0 = acc0 + h0;
+                acc1 = acc1 + h1;
+                acc2 = acc2 + h2;
+            }
+            if (t > t1 && t < t2) {
+                acc0 = acc0 + c0[j] * v;
+                acc1 = acc1 + c1[j] * v;
+                acc2 = acc2 + c2[j] * v;
+            }
+            if (t == t2) {
+                acc0 = acc0 + h0;
+                acc1 = acc1 + h1;
+                acc2 = acc2 + h2;
+            }
         }
     }
     double* ko = a.ker + ((size_t)pt * a.nfl + f) * (a.nktype + 1);
-    for (int j = 0; j < nk; ++j) ko[kt[j]] = acc[j];
+    ko[kt0] = acc0;
+    if (nk > 1) ko[kt1] = acc1;
+    if (nk > 2) ko[kt2] = acc2;
 }
 
 }  // namespace cat
@@ -1107,7 +1145,7 @@ void bpcoeff(double f1, double f2, int npoles, double dt, double* a, double* b1,
 
 template <int NP>
 void launch_ker_time(const KerTimeArgs& a, int threads, cudaStream_t st) {
-    k_ker_time<NP><<<(threads + 127) / 128, 128, 0, st>>>(a);
+    k_ker_time<NP><<<(threads + KER_TB - 1) / KER_TB, KER_TB, 0, st>>>(a);
 }
 void launch_ker_time_np(int np, const KerTimeArgs& a, int threads, cudaStream_t st) {
     switch (np) {
