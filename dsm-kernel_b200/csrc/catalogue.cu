@@ -427,66 +427,196 @@ __global__ void __launch_bounds__(256) k_ker_spec(const KerSpecArgs a) {
     }
 }
 
-// One thread per (batch point, series, filter): the window samples of the
-// transform (vectorFFT_double's exp(omegai t) / tlen * 1e3, as k_cat_window
-// forms them), the forward Butterworth recursion of rekurs (bwfilt.f90:54-90)
-// and the trapezoid sums of the series' kernel types over nt1..nt2 with half
-// weights at both ends (calculateK.f90:302-321, :497-513), in sample order.
+// The filter and trapezoid stage runs per (batch point, series, filter)
+// "item".  The forward Butterworth recursion of rekurs (bwfilt.f90:54-90) is
+// linear in its state (the last two inputs and both delayed outputs of every
+// section), so the samples 0..T-1 an item needs are cut into G segments of
+// L samples: k_ker_seg_zs runs every segment but the last from a zero state
+// and keeps its end state; k_ker_seg_chain walks the segments in order,
+// start(g+1) = P start(g) + end_zero(g), with P the recursion's transfer
+// over L samples without input (formed on the host); k_ker_time then runs
+// each segment from its true start state, producing the filtered samples
+// and the segment's part of the trapezoid sums of the series' kernel types
+// over nt1..nt2 (half weights at both ends, calculateK.f90:302-321,
+// :497-513); k_ker_seg_sum adds the parts in segment order.  The samples
+// are vectorFFT_double's window (exp(omegai t) / tlen * 1e3, as
+// k_cat_window forms them).
 struct KerTimeArgs {
     const double* y;      // transform rows, 2 (np1 + 1) reals apart
     const double* e;      // exp(omegai t / samplingHz) over the window
     const double* coeff;  // coeff(0:nfilter, 1:nktype, 1:nr, window), Fortran order
     const double* fc;     // [filter][a | b1 | b2][KER_MAXNP]
+    const double* P;      // [filter][D][D] transfer over L samples, D = 2 + 2 NP
     const int *nt1, *nt2; // window-relative, per filter
     const int* ir;
-    int p0, nb, ns, nfl, nr, nktype, nwin, iws, row, types;
+    int p0, nb, ns, nfl, nr, nktype, nwin, iws, row, types, gmax;
+    int segL[KER_MAXFL], segG[KER_MAXFL];
     double tlen;
+    double* zs;           // [item][gmax][D] zero-state end states
+    double* st;           // [item][gmax][D] segment start states
+    double* part;         // [item][gmax][3] trapezoid parts
     double* ker;          // [point][nfl][nktype + 1]
     double* filt;         // [point][ns][nfl][nwin] or null
 };
 
-constexpr int KER_TB = 32;   // one warp per block: the 3 x points x filters threads spread over every SM
+constexpr int KER_TB = 32;   // one warp per block
 constexpr int KER_CH = 8;    // samples (and their coefficients) loaded ahead of the recursion
+
+// kernel types fed by series s: kind 0 P du (1, 3, 4), 1 S du (5, 7), 2 S duq (8)
+__device__ __forceinline__ void ker_types(const KerTimeArgs& a, int s, int& kind, int& nk, int& k0, int& k1, int& k2) {
+    kind = (a.types & DSM_KER_VP) ? s : s + 1;
+    nk = kind == 0 ? 3 : kind == 1 ? 2 : 1;
+    k0 = kind == 0 ? 1 : kind == 1 ? 5 : 8;
+    k1 = kind == 0 ? 3 : kind == 1 ? 7 : k0;
+    k2 = kind == 0 ? 4 : k1;
+}
+
+template <int NP>
+struct Bw {
+    double A[NP], B1[NP], B2[NP], z1[NP], z2[NP], x1, x2;
+    __device__ __forceinline__ void load(const double* fc) {
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            A[k] = fc[k];
+            B1[k] = fc[KER_MAXNP + k];
+            B2[k] = fc[2 * KER_MAXNP + k];
+            z1[k] = 0.0;
+            z2[k] = 0.0;
+        }
+        x1 = 0.0;
+        x2 = 0.0;
+    }
+    // state order: x1, x2, z1[0..NP), z2[0..NP)
+    __device__ __forceinline__ void set_state(const double* q) {
+        x1 = q[0];
+        x2 = q[1];
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            z1[k] = q[2 + k];
+            z2[k] = q[2 + NP + k];
+        }
+    }
+    __device__ __forceinline__ void get_state(double* q) const {
+        q[0] = x1;
+        q[1] = x2;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            q[2 + k] = z1[k];
+            q[2 + NP + k] = z2[k];
+        }
+    }
+    // one sample of rekurs (bwfilt.f90:75-89)
+    __device__ __forceinline__ double step(double x) {
+        double z[NP];
+        z[0] = A[0] * (x - x2) - B1[0] * z1[0] - B2[0] * z2[0];
+#pragma unroll
+        for (int k = 1; k < NP; ++k) z[k] = A[k] * (z[k - 1] - z2[k - 1]) - B1[k] * z1[k] - B2[k] * z2[k];
+        x2 = x1;
+        x1 = x;
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            z2[k] = z1[k];
+            z1[k] = z[k];
+        }
+        return z[NP - 1];
+    }
+};
+
+struct KerItem {
+    int it, g, f, s, b, G, L, tb, te;
+};
+__device__ __forceinline__ bool ker_item(const KerTimeArgs& a, KerItem& q, bool need_last) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nb * a.ns * a.nfl * a.gmax) return false;
+    q.g = i % a.gmax;
+    q.it = i / a.gmax;
+    q.f = q.it % a.nfl;
+    q.s = (q.it / a.nfl) % a.ns;
+    q.b = q.it / (a.nfl * a.ns);
+    q.G = a.segG[q.f];
+    q.L = a.segL[q.f];
+    if (q.g >= (need_last ? q.G : q.G - 1)) return false;
+    const int T = a.filt ? a.nwin : a.nt2[q.f] + 1;
+    q.tb = q.g * q.L;
+    q.te = min(q.tb + q.L, T);
+    return true;
+}
+
+template <int NP>
+__global__ void __launch_bounds__(KER_TB) k_ker_seg_zs(const KerTimeArgs a) {
+    KerItem q;
+    if (!ker_item(a, q, false)) return;
+    Bw<NP> w;
+    w.load(a.fc + (size_t)q.f * 3 * KER_MAXNP);
+    const double* yr = a.y + ((size_t)q.b * a.ns + q.s) * a.row + a.iws;
+    for (int t0 = q.tb; t0 < q.te; t0 += KER_CH) {
+        double xs[KER_CH];
+#pragma unroll
+        for (int j = 0; j < KER_CH; ++j) {
+            const int t = min(t0 + j, q.te - 1);
+            xs[j] = yr[t] * a.e[t] / a.tlen * 1.0e3;
+        }
+#pragma unroll
+        for (int j = 0; j < KER_CH; ++j)
+            if (t0 + j < q.te) w.step(xs[j]);
+    }
+    w.get_state(a.zs + ((size_t)q.it * a.gmax + q.g) * (2 + 2 * NP));
+}
+
+template <int NP>
+__global__ void __launch_bounds__(KER_TB) k_ker_seg_chain(const KerTimeArgs a) {
+    constexpr int D = 2 + 2 * NP;
+    const int it = blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= a.nb * a.ns * a.nfl) return;
+    const int f = it % a.nfl, G = a.segG[f];
+    const double* P = a.P + (size_t)f * D * D;
+    double S[D];
+#pragma unroll
+    for (int r = 0; r < D; ++r) S[r] = 0.0;
+    for (int g = 0; g + 1 < G; ++g) {
+        const double* F = a.zs + ((size_t)it * a.gmax + g) * D;
+        double N[D];
+#pragma unroll
+        for (int r = 0; r < D; ++r) {
+            double v = F[r];
+#pragma unroll
+            for (int c = 0; c < D; ++c) v = v + P[r * D + c] * S[c];
+            N[r] = v;
+        }
+        double* o = a.st + ((size_t)it * a.gmax + g + 1) * D;
+#pragma unroll
+        for (int r = 0; r < D; ++r) {
+            S[r] = N[r];
+            o[r] = N[r];
+        }
+    }
+}
 
 template <int NP>
 __global__ void __launch_bounds__(KER_TB) k_ker_time(const KerTimeArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nb * a.ns * a.nfl) return;
-    const int f = i % a.nfl, s = (i / a.nfl) % a.ns, b = i / (a.nfl * a.ns);
-    const int pt = a.p0 + b;
-    // series kind: 0 P du (types 1, 3, 4), 1 S du (5, 7), 2 S duq (8)
-    const int kind = (a.types & DSM_KER_VP) ? s : s + 1;
-    const int nk = kind == 0 ? 3 : kind == 1 ? 2 : 1;
-    const int kt0 = kind == 0 ? 1 : kind == 1 ? 5 : 8;
-    const int kt1 = kind == 0 ? 3 : kind == 1 ? 7 : kt0;
-    const int kt2 = kind == 0 ? 4 : kt1;
-    double A[NP], B1[NP], B2[NP], z1[NP], z2[NP];
-    const double* fc = a.fc + (size_t)f * 3 * KER_MAXNP;
-#pragma unroll
-    for (int k = 0; k < NP; ++k) {
-        A[k] = fc[k];
-        B1[k] = fc[KER_MAXNP + k];
-        B2[k] = fc[2 * KER_MAXNP + k];
-        z1[k] = 0.0;
-        z2[k] = 0.0;
-    }
-    double x1 = 0.0, x2 = 0.0;
-    const int t1 = a.nt1[f], t2 = a.nt2[f];
-    const int tend = a.filt ? a.nwin : t2 + 1;
-    const double* yr = a.y + ((size_t)b * a.ns + s) * a.row + a.iws;
+    KerItem q;
+    if (!ker_item(a, q, true)) return;
+    int kind, nk, kt0, kt1, kt2;
+    ker_types(a, q.s, kind, nk, kt0, kt1, kt2);
+    Bw<NP> w;
+    w.load(a.fc + (size_t)q.f * 3 * KER_MAXNP);
+    if (q.g > 0) w.set_state(a.st + ((size_t)q.it * a.gmax + q.g) * (2 + 2 * NP));
+    const int pt = a.p0 + q.b;
+    const int t1 = a.nt1[q.f], t2 = a.nt2[q.f];
+    const double* yr = a.y + ((size_t)q.b * a.ns + q.s) * a.row + a.iws;
     const size_t cstride = (size_t)a.nfl * a.nktype * a.nr;
-    const double* cb = a.coeff + (size_t)a.ir[pt] * a.nktype * a.nfl + f;
+    const double* cb = a.coeff + (size_t)a.ir[pt] * a.nktype * a.nfl + q.f;
     const size_t o0 = (size_t)(kt0 - 1) * a.nfl, o1 = (size_t)(kt1 - 1) * a.nfl, o2 = (size_t)(kt2 - 1) * a.nfl;
-    double* fo = a.filt ? a.filt + (((size_t)pt * a.ns + s) * a.nfl + f) * a.nwin : nullptr;
+    double* fo = a.filt ? a.filt + (((size_t)pt * a.ns + q.s) * a.nfl + q.f) * a.nwin : nullptr;
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-    for (int t0 = 0; t0 < tend; t0 += KER_CH) {
+    for (int t0 = q.tb; t0 < q.te; t0 += KER_CH) {
         // the chunk's samples and coefficients first (independent loads, all
-        // in flight together); indices clamped into the window, so every
-        // load stays inside the transform row and coeff
+        // in flight together); indices clamped into the segment and into
+        // nt1..nt2, so every load stays inside the transform row and coeff
         double xs[KER_CH], c0[KER_CH], c1[KER_CH], c2[KER_CH];
 #pragma unroll
         for (int j = 0; j < KER_CH; ++j) {
-            const int t = min(t0 + j, tend - 1);
+            const int t = min(t0 + j, q.te - 1);
             xs[j] = yr[t] * a.e[t] / a.tlen * 1.0e3;
         }
         const bool in = t0 + KER_CH > t1 && t0 <= t2;
@@ -502,19 +632,8 @@ __global__ void __launch_bounds__(KER_TB) k_ker_time(const KerTimeArgs a) {
 #pragma unroll
         for (int j = 0; j < KER_CH; ++j) {
             const int t = t0 + j;
-            if (t >= tend) break;
-            double z[NP];
-            z[0] = A[0] * (xs[j] - x2) - B1[0] * z1[0] - B2[0] * z2[0];
-#pragma unroll
-            for (int k = 1; k < NP; ++k) z[k] = A[k] * (z[k - 1] - z2[k - 1]) - B1[k] * z1[k] - B2[k] * z2[k];
-            x2 = x1;
-            x1 = xs[j];
-#pragma unroll
-            for (int k = 0; k < NP; ++k) {
-                z2[k] = z1[k];
-                z1[k] = z[k];
-            }
-            const double v = z[NP - 1];
+            if (t >= q.te) break;
+            const double v = w.step(xs[j]);
             if (fo) fo[t] = v;
             if (t < t1 || t > t2) continue;
             // isovpfreq halves as coeff * duf / 2, isovsfreq as 0.5 * coeff * duf
@@ -538,7 +657,26 @@ __global__ void __launch_bounds__(KER_TB) k_ker_time(const KerTimeArgs a) {
             }
         }
     }
-    double* ko = a.ker + ((size_t)pt * a.nfl + f) * (a.nktype + 1);
+    double* pp = a.part + ((size_t)q.it * a.gmax + q.g) * 3;
+    pp[0] = acc0;
+    pp[1] = acc1;
+    pp[2] = acc2;
+}
+
+__global__ void __launch_bounds__(128) k_ker_seg_sum(const KerTimeArgs a) {
+    const int it = blockIdx.x * blockDim.x + threadIdx.x;
+    if (it >= a.nb * a.ns * a.nfl) return;
+    const int f = it % a.nfl, s = (it / a.nfl) % a.ns, b = it / (a.nfl * a.ns);
+    int kind, nk, kt0, kt1, kt2;
+    ker_types(a, s, kind, nk, kt0, kt1, kt2);
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    for (int g = 0; g < a.segG[f]; ++g) {
+        const double* pp = a.part + ((size_t)it * a.gmax + g) * 3;
+        acc0 = acc0 + pp[0];
+        acc1 = acc1 + pp[1];
+        acc2 = acc2 + pp[2];
+    }
+    double* ko = a.ker + ((size_t)(a.p0 + b) * a.nfl + f) * (a.nktype + 1);
     ko[kt0] = acc0;
     if (nk > 1) ko[kt1] = acc1;
     if (nk > 2) ko[kt2] = acc2;
@@ -581,7 +719,9 @@ struct dsm_cat {
     // windows, coeff and jacobianFuji resident on the device
     bool kset = false;
     int ktypes = 0, kns = 0, knfl = 0, knp = 0, knr = 0, knkt = 0;
-    DBuf<double> kcoef, kfc, kker, kfilt;
+    DBuf<double> kcoef, kfc, kker, kfilt, kzs, kst, kpart, kP;
+    std::vector<double> kfc_h;   // host copies for the segment transfers
+    std::vector<int> knt_h;
     DBuf<cd> kjac, kh3, kh4;
     DBuf<int> knt, kir;
 
@@ -1144,21 +1284,60 @@ void bpcoeff(double f1, double f2, int npoles, double dt, double* a, double* b1,
 }
 
 template <int NP>
-void launch_ker_time(const KerTimeArgs& a, int threads, cudaStream_t st) {
-    k_ker_time<NP><<<(threads + KER_TB - 1) / KER_TB, KER_TB, 0, st>>>(a);
+void launch_ker_time(const KerTimeArgs& a, cudaStream_t st) {
+    const int nit = a.nb * a.ns * a.nfl, nthr = nit * a.gmax;
+    if (a.gmax > 1) {
+        k_ker_seg_zs<NP><<<(nthr + KER_TB - 1) / KER_TB, KER_TB, 0, st>>>(a);
+        k_ker_seg_chain<NP><<<(nit + KER_TB - 1) / KER_TB, KER_TB, 0, st>>>(a);
+    }
+    k_ker_time<NP><<<(nthr + KER_TB - 1) / KER_TB, KER_TB, 0, st>>>(a);
+    k_ker_seg_sum<<<(nit + 127) / 128, 128, 0, st>>>(a);
 }
-void launch_ker_time_np(int np, const KerTimeArgs& a, int threads, cudaStream_t st) {
+
+// transfer of the recursion over L samples without input, [D][D] row-major
+// (column j: the state after L steps from unit state j), D = 2 + 2 npoles
+void ker_transfer(const double* fc, int np, int L, double* P) {
+    const int D = 2 + 2 * np;
+    std::vector<double> q(D);
+    for (int j = 0; j < D; ++j) {
+        std::fill(q.begin(), q.end(), 0.0);
+        q[j] = 1.0;
+        double x1 = q[0], x2 = q[1], z1[KER_MAXNP], z2[KER_MAXNP], z[KER_MAXNP];
+        for (int k = 0; k < np; ++k) {
+            z1[k] = q[2 + k];
+            z2[k] = q[2 + np + k];
+        }
+        for (int t = 0; t < L; ++t) {
+            z[0] = fc[0] * (0.0 - x2) - fc[KER_MAXNP] * z1[0] - fc[2 * KER_MAXNP] * z2[0];
+            for (int k = 1; k < np; ++k)
+                z[k] = fc[k] * (z[k - 1] - z2[k - 1]) - fc[KER_MAXNP + k] * z1[k] - fc[2 * KER_MAXNP + k] * z2[k];
+            x2 = x1;
+            x1 = 0.0;
+            for (int k = 0; k < np; ++k) {
+                z2[k] = z1[k];
+                z1[k] = z[k];
+            }
+        }
+        P[0 * D + j] = x1;
+        P[1 * D + j] = x2;
+        for (int k = 0; k < np; ++k) {
+            P[(2 + k) * D + j] = z1[k];
+            P[(2 + np + k) * D + j] = z2[k];
+        }
+    }
+}
+void launch_ker_time_np(int np, const KerTimeArgs& a, cudaStream_t st) {
     switch (np) {
-        case 1: launch_ker_time<1>(a, threads, st); break;
-        case 2: launch_ker_time<2>(a, threads, st); break;
-        case 3: launch_ker_time<3>(a, threads, st); break;
-        case 4: launch_ker_time<4>(a, threads, st); break;
-        case 5: launch_ker_time<5>(a, threads, st); break;
-        case 6: launch_ker_time<6>(a, threads, st); break;
-        case 7: launch_ker_time<7>(a, threads, st); break;
-        case 8: launch_ker_time<8>(a, threads, st); break;
-        case 9: launch_ker_time<9>(a, threads, st); break;
-        default: launch_ker_time<10>(a, threads, st); break;
+        case 1: launch_ker_time<1>(a, st); break;
+        case 2: launch_ker_time<2>(a, st); break;
+        case 3: launch_ker_time<3>(a, st); break;
+        case 4: launch_ker_time<4>(a, st); break;
+        case 5: launch_ker_time<5>(a, st); break;
+        case 6: launch_ker_time<6>(a, st); break;
+        case 7: launch_ker_time<7>(a, st); break;
+        case 8: launch_ker_time<8>(a, st); break;
+        case 9: launch_ker_time<9>(a, st); break;
+        default: launch_ker_time<10>(a, st); break;
     }
     DSM_CUDA(cudaGetLastError());
 }
@@ -1198,6 +1377,8 @@ extern "C" int dsm_cat_set_kernel_params(dsm_cat_t* c, const dsm_cat_kernel_para
         c->kset = false;
         c->kfc.upload(fc, c->st);
         c->knt.upload(nt, c->st);
+        c->kfc_h = fc;
+        c->knt_h = nt;
         c->kcoef.upload(kp->coeff, ncoef, c->st);
         if (kp->types & DSM_KER_VS) {
             const cd* j = static_cast<const cd*>(kp->jacobian);
@@ -1289,6 +1470,27 @@ extern "C" int dsm_cat_kernels(dsm_cat_t* c, int npoint, const int* ir, const vo
         ta.tlen = p.tlen;
         ta.ker = dker;
         ta.filt = dfilt;
+        // segments of each filter's samples (at least 32 samples, at most 16
+        // segments) and their transfers
+        const int D = 2 + 2 * c->knp;
+        std::vector<double> Ph((size_t)nfl * D * D);
+        ta.gmax = 1;
+        for (int f = 0; f < nfl; ++f) {
+            const int T = filtered ? nwin : c->knt_h[nfl + f] + 1;
+            const int L = std::max(32, (T + 15) / 16);
+            ta.segL[f] = L;
+            ta.segG[f] = (T + L - 1) / L;
+            ta.gmax = std::max(ta.gmax, ta.segG[f]);
+            ker_transfer(c->kfc_h.data() + (size_t)f * 3 * KER_MAXNP, c->knp, L, Ph.data() + (size_t)f * D * D);
+        }
+        c->kP.upload(Ph, c->st);
+        ta.P = c->kP.p;
+        c->kzs.reserve((size_t)pc * ns * nfl * ta.gmax * D);
+        c->kst.reserve((size_t)pc * ns * nfl * ta.gmax * D);
+        c->kpart.reserve((size_t)pc * ns * nfl * ta.gmax * 3);
+        ta.zs = c->kzs.p;
+        ta.st = c->kst.p;
+        ta.part = c->kpart.p;
         for (int b0 = 0; b0 < npoint; b0 += pc) {
             const int nb = std::min(pc, npoint - b0);
             sa.p0 = b0;
@@ -1299,7 +1501,7 @@ extern "C" int dsm_cat_kernels(dsm_cat_t* c, int npoint, const int* ir, const vo
                                    reinterpret_cast<cufftDoubleReal*>(c->h.p)));
             ta.p0 = b0;
             ta.nb = nb;
-            launch_ker_time_np(c->knp, ta, nb * ns * nfl, c->st);
+            launch_ker_time_np(c->knp, ta, c->st);
         }
         if (!out_on_device) {
             DSM_CUDA(cudaMemcpyAsync(ker, dker, (size_t)npoint * nfl * nkt1 * sizeof(double), cudaMemcpyDeviceToHost,
