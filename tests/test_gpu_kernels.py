@@ -242,3 +242,28 @@ def test_calculate_kernel_end_to_end(built, compo):
     w3, w4 = np.stack(w3), np.stack(w4)
     assert rel_l2(h3, w3) <= TOL and rel_l2(h4, w4) <= TOL
     _check(got, _oracle(pt, kp, ir, w3, w4))
+
+
+@pytest.mark.gpu
+def test_kernels_without_series_mixed_segment_counts(built):
+    """Without the filtered output an item runs only up to its filter's
+    nt2, so filters whose windows end early run as one segment and the
+    others as several; the kernels match the oracle either way."""
+    rng = np.random.default_rng(31)
+    p = _params(fmax=200, np1=256, tlen=1638.4, omegai=np.log(100.0) / 1638.4, iwin_start=10, iwin_end=500)
+    nf = p["fmax"] - p["fmin"] + 1
+    kp = _kparams(p, 3, 3, 3, rng)
+    kp["nt1"] = [12, 14, 20, 11]
+    kp["nt2"] = [30, 200, 490, 11]          # 21, 191, 481 and 2 samples from the window start
+    ir = rng.integers(0, 3, 23)
+    h3, h4 = _spectra(rng, ir.size, nf)
+    c = dsmsgt.Catalogue(p)
+    c.set_kernel_params(kp["types"], kp["nfilter"], kp["fclp"], kp["fchp"], kp["npoles"], kp["sampling_hz"],
+                        kp["nt1"], kp["nt2"], kp["coeff"], kp["jacobian"])
+    ker = c.kernels(ir, h3, h4)
+    ker2, _ = c.kernels(ir, h3, h4, filtered=True)
+    c.close()
+    wk, _ = _oracle(p, kp, ir, h3, h4)
+    assert rel_l2(ker, wk) <= TOL and rel_l2(ker2, wk) <= TOL
+    for f in range(4):
+        assert rel_l2(ker[:, f], wk[:, f]) <= TOL, f
