@@ -1435,9 +1435,28 @@ extern "C" int dsm_cat_kernels(dsm_cat_t* c, int npoint, const int* ir, const vo
             }
         }
         DSM_CUDA(cudaMemsetAsync(dker, 0, (size_t)npoint * nfl * nkt1 * sizeof(double), c->st));
-        // points per batch: the in-place transform buffer stays under max_batch_bytes
-        const int pc = (int)std::min<size_t>(
-            (size_t)npoint, std::max<size_t>(1, c->max_batch_bytes / ((size_t)ns * nh * sizeof(cd))));
+        // segments of each filter's samples (at least 32 samples, at most 16
+        // segments) and their transfers
+        const int D = 2 + 2 * c->knp;
+        std::vector<double> Ph((size_t)nfl * D * D);
+        int gmax = 1;
+        int segL[KER_MAXFL], segG[KER_MAXFL];
+        for (int f = 0; f < nfl; ++f) {
+            const int T = filtered ? nwin : c->knt_h[nfl + f] + 1;
+            const int L = std::max(32, (T + 15) / 16);
+            segL[f] = L;
+            segG[f] = (T + L - 1) / L;
+            gmax = std::max(gmax, segG[f]);
+            ker_transfer(c->kfc_h.data() + (size_t)f * 3 * KER_MAXNP, c->knp, L, Ph.data() + (size_t)f * D * D);
+        }
+        // points per batch: the in-place transform rows and the segment
+        // scratch (end and start states, trapezoid parts) stay under
+        // max_batch_bytes, and the stage's threads fit an int
+        const size_t per_point =
+            (size_t)ns * nh * sizeof(cd) + (size_t)ns * nfl * gmax * (2 * D + 3) * sizeof(double);
+        size_t pcs = std::min<size_t>((size_t)npoint, std::max<size_t>(1, c->max_batch_bytes / per_point));
+        pcs = std::min<size_t>(pcs, ((size_t)1 << 30) / ((size_t)ns * nfl * gmax));
+        const int pc = (int)std::max<size_t>(1, pcs);
         c->h.reserve((size_t)pc * ns * nh);
         KerSpecArgs sa{};
         sa.h3 = d3;
@@ -1470,24 +1489,16 @@ extern "C" int dsm_cat_kernels(dsm_cat_t* c, int npoint, const int* ir, const vo
         ta.tlen = p.tlen;
         ta.ker = dker;
         ta.filt = dfilt;
-        // segments of each filter's samples (at least 32 samples, at most 16
-        // segments) and their transfers
-        const int D = 2 + 2 * c->knp;
-        std::vector<double> Ph((size_t)nfl * D * D);
-        ta.gmax = 1;
+        ta.gmax = gmax;
         for (int f = 0; f < nfl; ++f) {
-            const int T = filtered ? nwin : c->knt_h[nfl + f] + 1;
-            const int L = std::max(32, (T + 15) / 16);
-            ta.segL[f] = L;
-            ta.segG[f] = (T + L - 1) / L;
-            ta.gmax = std::max(ta.gmax, ta.segG[f]);
-            ker_transfer(c->kfc_h.data() + (size_t)f * 3 * KER_MAXNP, c->knp, L, Ph.data() + (size_t)f * D * D);
+            ta.segL[f] = segL[f];
+            ta.segG[f] = segG[f];
         }
         c->kP.upload(Ph, c->st);
         ta.P = c->kP.p;
-        c->kzs.reserve((size_t)pc * ns * nfl * ta.gmax * D);
-        c->kst.reserve((size_t)pc * ns * nfl * ta.gmax * D);
-        c->kpart.reserve((size_t)pc * ns * nfl * ta.gmax * 3);
+        c->kzs.reserve((size_t)pc * ns * nfl * gmax * D);
+        c->kst.reserve((size_t)pc * ns * nfl * gmax * D);
+        c->kpart.reserve((size_t)pc * ns * nfl * gmax * 3);
         ta.zs = c->kzs.p;
         ta.st = c->kst.p;
         ta.part = c->kpart.p;
