@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(256) k_ker_spec(const KerSpecArgs a) {
 struct KerTimeArgs {
     const double* y;      // transform rows, 2 (np1 + 1) reals apart
     const double* e;      // exp(omegai t / samplingHz) over the window
-    const double* coeff;  // coeff(0:nfilter, 1:nktype, 1:nr, window), Fortran order
+    const double* coeff;  // coeff, sample-major: [ir][k - 1][filter][window sample]
     const double* fc;     // [filter][a | b1 | b2][KER_MAXNP]
     const double* P;      // [filter][D][D] transfer over L samples, D = 2 + 2 NP
     const int *nt1, *nt2; // window-relative, per filter
@@ -604,9 +604,9 @@ __global__ void __launch_bounds__(KER_TB) k_ker_time(const KerTimeArgs a) {
     const int pt = a.p0 + q.b;
     const int t1 = a.nt1[q.f], t2 = a.nt2[q.f];
     const double* yr = a.y + ((size_t)q.b * a.ns + q.s) * a.row + a.iws;
-    const size_t cstride = (size_t)a.nfl * a.nktype * a.nr;
-    const double* cb = a.coeff + (size_t)a.ir[pt] * a.nktype * a.nfl + q.f;
-    const size_t o0 = (size_t)(kt0 - 1) * a.nfl, o1 = (size_t)(kt1 - 1) * a.nfl, o2 = (size_t)(kt2 - 1) * a.nfl;
+    const double* cb = a.coeff + ((size_t)a.ir[pt] * a.nktype * a.nfl + q.f) * a.nwin;
+    const size_t ks = (size_t)a.nfl * a.nwin;
+    const size_t o0 = (kt0 - 1) * ks, o1 = (kt1 - 1) * ks, o2 = (kt2 - 1) * ks;
     double* fo = a.filt ? a.filt + (((size_t)pt * a.ns + q.s) * a.nfl + q.f) * a.nwin : nullptr;
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
     for (int t0 = q.tb; t0 < q.te; t0 += KER_CH) {
@@ -623,7 +623,7 @@ __global__ void __launch_bounds__(KER_TB) k_ker_time(const KerTimeArgs a) {
         if (in) {
 #pragma unroll
             for (int j = 0; j < KER_CH; ++j) {
-                const double* c = cb + (size_t)min(max(t0 + j, t1), t2) * cstride;
+                const double* c = cb + min(max(t0 + j, t1), t2);
                 c0[j] = c[o0];
                 c1[j] = c[o1];
                 c2[j] = c[o2];
@@ -1373,13 +1373,19 @@ extern "C" int dsm_cat_set_kernel_params(dsm_cat_t* c, const dsm_cat_kernel_para
         }
         const size_t ncoef = (size_t)nwin * kp->nr * kp->nktype * nfl;
         for (size_t i = 0; i < ncoef; ++i) need(std::isfinite(kp->coeff[i]), std::string(fn) + ": non-finite coeff");
+        // sample-major on the device, [ir][k - 1][filter][sample]: a thread's
+        // coefficients of consecutive samples are adjacent
+        std::vector<double> ct(ncoef);
+        const size_t rows = (size_t)kp->nr * kp->nktype * nfl;
+        for (int t = 0; t < nwin; ++t)
+            for (size_t r = 0; r < rows; ++r) ct[r * nwin + t] = kp->coeff[(size_t)t * rows + r];
         DSM_CUDA(cudaSetDevice(c->dev));
         c->kset = false;
         c->kfc.upload(fc, c->st);
         c->knt.upload(nt, c->st);
         c->kfc_h = fc;
         c->knt_h = nt;
-        c->kcoef.upload(kp->coeff, ncoef, c->st);
+        c->kcoef.upload(ct, c->st);
         if (kp->types & DSM_KER_VS) {
             const cd* j = static_cast<const cd*>(kp->jacobian);
             for (size_t i = 0; i < (size_t)nf * kp->nr; ++i)
