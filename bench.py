@@ -556,15 +556,24 @@ def kernels_bench(args):
 
     for _ in range(args.warmup):
         step()
+    c.set_profiling(True)
     clocks = ClockSampler(dev)
     clocks.start()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    ms, kst = 0.0, {}
     for _ in range(args.steps):
         step()
+        st = c.stats()
+        ms += st.ms_total
+        for name, (tk, nk, bk, _) in st.kernels().items():
+            a_ = kst.setdefault(name, [0.0, 0, 0.0])
+            a_[0] += tk; a_[1] += nk; a_[2] += bk
     torch.cuda.synchronize()
-    t = time.perf_counter() - t0
+    t_wall = time.perf_counter() - t0
     clk = clocks.stop()
+    c.set_profiling(False)
+    t = ms / 1e3
     # end to end: spectra from host memory, kernels back to the host
     c.kernels(ir, h3, h4)
     t_e2e = 0.0
@@ -579,12 +588,20 @@ def kernels_bench(args):
             peaks = json.load(fh)
     except Exception:
         pass
-    # algorithmic bytes of a step: h3 and h4 read once, the three transform
-    # rows written, transformed in place (read + written) and read by the filter
-    nh = p["np1"] + 1
-    alg = 2 * npt * 6 * nf * 16 + 3 * npt * nh * 16 * 4
-    ach = alg * args.steps / t / 1e9
+    # per stage: algorithmic bytes (the library's count) over the stage's
+    # event time; the line's roofline is the longest stage's
     peak = peaks.get("hbm_gbs", 6650.0)
+    psrc = "measured" if "hbm_gbs" in peaks else "fallback"
+    stages = {}
+    for name, (tk, nk, bk) in kst.items():
+        ach_k = bk / (tk / 1e3) / 1e9
+        stages[name] = {"kernel": name, "bound": "hbm" if name != "ker_filter" else "latency (sequential recursion)",
+                        "achieved": ach_k, "peak": peak, "unit": "GB/s", "frac": ach_k / peak,
+                        "avg_launch_ms": tk / max(nk, 1), "launches": nk, "alg_bytes_per_step": bk / args.steps,
+                        "peak_source": psrc}
+    top = max(kst.items(), key=lambda kv: kv[1][0])[0]
+    alg = sum(v[2] for v in kst.values())
+    ach = alg / t / 1e9
     cpu_b = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v = cpu(h3, h4, kp, ir, 64)
@@ -596,14 +613,17 @@ def kernels_bench(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded spectra, coefficients and jacobian)", "config": cfg,
-            "timing": "host clock around synchronous calls on device-resident spectra",
+            "timing": "CUDA events of the library (profiling on) over the device work of each call; "
+                      f"host clock around the same calls: {1e3 * t_wall / args.steps:.3f} ms per step",
             "e2e": {"value": args.steps * npt / t_e2e, "unit": KER_UNIT,
                     "h2d_bytes_per_step": int(h3.nbytes + h4.nbytes + irr.nbytes),
                     "d2h_bytes_per_step": int(npt * 9 * 8)},
-            "gpu_launches": 2 * args.steps,
-            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                         "traffic": None, "scope": "whole call (products, cuFFT, filter and sums)",
-                         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+            "gpu_launches": int(sum(v[1] for k_, v in kst.items() if k_ != "ker_fft")),
+            "roofline": dict(stages[top], traffic=None),
+            "stage_rooflines": stages,
+            "call_roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                              "scope": "whole call (products, cuFFT, filter and sums)", "peak_source": psrc},
+            "kernel_share": {k_: round(v[0] / max(ms, 1e-9), 4) for k_, v in kst.items()},
             "cpu_baseline": cpu_b, "clocks": clk}))
 
 

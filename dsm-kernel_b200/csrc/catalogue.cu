@@ -1508,18 +1508,42 @@ extern "C" int dsm_cat_kernels(dsm_cat_t* c, int npoint, const int* ir, const vo
         ta.zs = c->kzs.p;
         ta.st = c->kst.p;
         ta.part = c->kpart.p;
+        auto& S = c->stats;
+        S = dsm_stats_t{};
+        const bool prof = c->profiling;
+        if (prof) DSM_CUDA(cudaEventRecord(c->ev[0], c->st));
+        double ms_s = 0, ms_f = 0, ms_t = 0;
+        int nbatch = 0;
+        const int fl_launches = (ta.gmax > 1 ? 4 : 2);
         for (int b0 = 0; b0 < npoint; b0 += pc) {
             const int nb = std::min(pc, npoint - b0);
             sa.p0 = b0;
             sa.nb = nb;
+            if (prof) DSM_CUDA(cudaEventRecord(c->ev[1], c->st));
             k_ker_spec<<<dim3((nh + 255) / 256, std::min(nb, 65535)), 256, 0, c->st>>>(sa);
             DSM_CUDA(cudaGetLastError());
+            if (prof) DSM_CUDA(cudaEventRecord(c->ev[2], c->st));
             DSM_CUFFT(cufftExecZ2D(c->plan(nb * ns), reinterpret_cast<cufftDoubleComplex*>(c->h.p),
                                    reinterpret_cast<cufftDoubleReal*>(c->h.p)));
+            if (prof) DSM_CUDA(cudaEventRecord(c->ev[3], c->st));
             ta.p0 = b0;
             ta.nb = nb;
             launch_ker_time_np(c->knp, ta, c->st);
+            S.launches += 1 + fl_launches;
+            ++nbatch;
+            if (prof) {
+                DSM_CUDA(cudaEventRecord(c->ev[4], c->st));
+                DSM_CUDA(cudaEventSynchronize(c->ev[4]));
+                float t1, t2, t3;
+                cudaEventElapsedTime(&t1, c->ev[1], c->ev[2]);
+                cudaEventElapsedTime(&t2, c->ev[2], c->ev[3]);
+                cudaEventElapsedTime(&t3, c->ev[3], c->ev[4]);
+                ms_s += t1;
+                ms_f += t2;
+                ms_t += t3;
+            }
         }
+        if (prof) DSM_CUDA(cudaEventRecord(c->ev[5], c->st));
         if (!out_on_device) {
             DSM_CUDA(cudaMemcpyAsync(ker, dker, (size_t)npoint * nfl * nkt1 * sizeof(double), cudaMemcpyDeviceToHost,
                                      c->st));
@@ -1528,6 +1552,32 @@ extern "C" int dsm_cat_kernels(dsm_cat_t* c, int npoint, const int* ir, const vo
                                          cudaMemcpyDeviceToHost, c->st));
         }
         DSM_CUDA(cudaStreamSynchronize(c->st));
+        if (prof) {
+            float tt;
+            cudaEventElapsedTime(&tt, c->ev[0], c->ev[5]);
+            S.ms_total = tt;
+            // algorithmic bytes: h3 and h4 read once and the transform rows
+            // written (products); the rows read and written (transform); the
+            // samples each item integrates or writes read once, the filtered
+            // series and the kernels written (filter stage)
+            double samples = 0;
+            for (int f = 0; f < nfl; ++f) samples += filtered ? nwin : c->knt_h[nfl + f] + 1;
+            const double rows = (double)npoint * ns * nh * sizeof(cd);
+            const double by[3] = {2.0 * npoint * 6 * nf * sizeof(cd) + rows, 2.0 * rows,
+                                  (double)npoint * ns * samples * sizeof(double) * (filtered ? 2.0 : 1.0) +
+                                      (double)npoint * nfl * nkt1 * sizeof(double)};
+            const char* nm[3] = {"ker_spec", "ker_fft", "ker_filter"};
+            const double ms[3] = {ms_s, ms_f, ms_t};
+            const long long nl[3] = {nbatch, nbatch, (long long)nbatch * fl_launches};
+            for (int k = 0; k < 3; ++k) {
+                snprintf(S.kern[k].name, sizeof(S.kern[k].name), "%s", nm[k]);
+                S.kern[k].ms = ms[k];
+                S.kern[k].launches = nl[k];
+                S.kern[k].alg_bytes = by[k];
+                S.kern[k].alg_flops = 0.0;
+            }
+            S.nk = 3;
+        }
     });
 }
 

@@ -565,7 +565,10 @@ int dsm_cat_kernels(dsm_cat_t *cat, int npoint, const int *ir, const void *h3, c
 
 /* Per-stage device time of the last dsm_cat_series when profiling is on:
  * kern[] holds cat_interp, cat_fft, cat_window (ms, launches, algorithmic
- * bytes); ms_total covers the whole call. */
+ * bytes); ms_total covers the whole call.  After dsm_cat_kernels: ker_spec
+ * (products into transform rows), ker_fft, ker_filter (segment end states,
+ * their chain, the filter reruns with the trapezoid parts and their sum);
+ * ms_total covers the device work between the uploads and the copies back. */
 int dsm_cat_set_profiling(dsm_cat_t *cat, int on);
 int dsm_cat_get_stats(const dsm_cat_t *cat, dsm_stats_t *stats);
 
