@@ -563,31 +563,36 @@ __global__ void __launch_bounds__(KER_TB) k_ker_seg_zs(const KerTimeArgs a) {
     w.get_state(a.zs + ((size_t)q.it * a.gmax + q.g) * (2 + 2 * NP));
 }
 
+// D lanes per item (32 / D items per warp): lane r keeps state component r
+// and row r of P, and gathers the other components by shuffles; the sums
+// run in the same order as a one-thread matrix-vector product
 template <int NP>
 __global__ void __launch_bounds__(KER_TB) k_ker_seg_chain(const KerTimeArgs a) {
     constexpr int D = 2 + 2 * NP;
-    const int it = blockIdx.x * blockDim.x + threadIdx.x;
-    if (it >= a.nb * a.ns * a.nfl) return;
-    const int f = it % a.nfl, G = a.segG[f];
-    const double* P = a.P + (size_t)f * D * D;
-    double S[D];
+    constexpr int IPW = 32 / D;
+    const int lane = threadIdx.x & 31;
+    const int slot = lane / D, r = lane - slot * D;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int it = warp * IPW + slot;
+    const bool act = slot < IPW && it < a.nb * a.ns * a.nfl;
+    const int itc = act ? it : 0;
+    const int f = itc % a.nfl, G = act ? a.segG[f] : 1;
+    double prow[D];
 #pragma unroll
-    for (int r = 0; r < D; ++r) S[r] = 0.0;
-    for (int g = 0; g + 1 < G; ++g) {
-        const double* F = a.zs + ((size_t)it * a.gmax + g) * D;
-        double N[D];
+    for (int c = 0; c < D; ++c) prow[c] = a.P[((size_t)f * D + r) * D + c];
+    int gw = G;   // the warp's longest chain: every lane takes part in every shuffle
 #pragma unroll
-        for (int r = 0; r < D; ++r) {
-            double v = F[r];
+    for (int o = 16; o; o >>= 1) gw = max(gw, __shfl_xor_sync(0xffffffffu, gw, o));
+    const int base = slot * D;
+    double S = 0.0;
+    for (int g = 0; g + 1 < gw; ++g) {
+        const bool live = act && g + 1 < G;
+        double v = live ? a.zs[((size_t)itc * a.gmax + g) * D + r] : 0.0;
 #pragma unroll
-            for (int c = 0; c < D; ++c) v = v + P[r * D + c] * S[c];
-            N[r] = v;
-        }
-        double* o = a.st + ((size_t)it * a.gmax + g + 1) * D;
-#pragma unroll
-        for (int r = 0; r < D; ++r) {
-            S[r] = N[r];
-            o[r] = N[r];
+        for (int c = 0; c < D; ++c) v = v + prow[c] * __shfl_sync(0xffffffffu, S, (base + c) & 31);
+        if (live) {
+            S = v;
+            a.st[((size_t)itc * a.gmax + g + 1) * D + r] = v;
         }
     }
 }
@@ -1288,7 +1293,8 @@ void launch_ker_time(const KerTimeArgs& a, cudaStream_t st) {
     const int nit = a.nb * a.ns * a.nfl, nthr = nit * a.gmax;
     if (a.gmax > 1) {
         k_ker_seg_zs<NP><<<(nthr + KER_TB - 1) / KER_TB, KER_TB, 0, st>>>(a);
-        k_ker_seg_chain<NP><<<(nit + KER_TB - 1) / KER_TB, KER_TB, 0, st>>>(a);
+        constexpr int ipw = 32 / (2 + 2 * NP);
+        k_ker_seg_chain<NP><<<(nit + ipw - 1) / ipw, KER_TB, 0, st>>>(a);
     }
     k_ker_time<NP><<<(nthr + KER_TB - 1) / KER_TB, KER_TB, 0, st>>>(a);
     k_ker_seg_sum<<<(nit + 127) / 128, 128, 0, st>>>(a);
