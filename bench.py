@@ -415,7 +415,7 @@ def catalogue_bench(args):
             a[0] += t; a[1] += n; a[2] += b; a[3] += f
     torch.cuda.synchronize()
     clk = clocks.stop()
-    # end to end: host records (pageable numpy) copied in, series copied out
+    # end to end: host records (numpy views of pinned memory) copied in, series copied out
     for k in range(2):
         step(k, True)
     t_e2e = 0.0
