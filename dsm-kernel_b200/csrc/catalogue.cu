@@ -668,6 +668,29 @@ __global__ void __launch_bounds__(KER_TB) k_ker_time(const KerTimeArgs a) {
     pp[2] = acc2;
 }
 
+// The filters alone on window series (calculateRSGT / calculateTSGT,
+// calculateK.f90:1-130): one thread per (series, filter), the samples in
+// order (rekurs, bwfilt.f90:75-89), the next 8 loaded ahead.
+template <int NP>
+__global__ void __launch_bounds__(KER_TB) k_cat_bwfilt(const double* __restrict__ in, int nseries, int nfl, int nwin,
+                                                       const double* __restrict__ fc, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nseries * nfl) return;
+    const int f = i % nfl, sr = i / nfl;
+    Bw<NP> w;
+    w.load(fc + (size_t)f * 3 * KER_MAXNP);
+    const double* x = in + (size_t)sr * nwin;
+    double* y = out + ((size_t)sr * nfl + f) * nwin;
+    for (int t0 = 0; t0 < nwin; t0 += KER_CH) {
+        double xs[KER_CH];
+#pragma unroll
+        for (int j = 0; j < KER_CH; ++j) xs[j] = x[min(t0 + j, nwin - 1)];
+#pragma unroll
+        for (int j = 0; j < KER_CH; ++j)
+            if (t0 + j < nwin) y[t0 + j] = w.step(xs[j]);
+    }
+}
+
 __global__ void __launch_bounds__(128) k_ker_seg_sum(const KerTimeArgs a) {
     const int it = blockIdx.x * blockDim.x + threadIdx.x;
     if (it >= a.nb * a.ns * a.nfl) return;
@@ -724,7 +747,7 @@ struct dsm_cat {
     // windows, coeff and jacobianFuji resident on the device
     bool kset = false;
     int ktypes = 0, kns = 0, knfl = 0, knp = 0, knr = 0, knkt = 0;
-    DBuf<double> kcoef, kfc, kker, kfilt, kzs, kst, kpart, kP;
+    DBuf<double> kcoef, kfc, kker, kfilt, kzs, kst, kpart, kP, kfin;
     std::vector<double> kfc_h;   // host copies for the segment transfers
     std::vector<int> knt_h;
     DBuf<cd> kjac, kh3, kh4;
@@ -1584,6 +1607,54 @@ extern "C" int dsm_cat_kernels(dsm_cat_t* c, int npoint, const int* ir, const vo
             }
             S.nk = 3;
         }
+    });
+}
+
+namespace {
+template <int NP>
+void launch_bwfilt(const double* in, int nseries, int nfl, int nwin, const double* fc, double* out, cudaStream_t st) {
+    const int n = nseries * nfl;
+    k_cat_bwfilt<NP><<<(n + KER_TB - 1) / KER_TB, KER_TB, 0, st>>>(in, nseries, nfl, nwin, fc, out);
+}
+}  // namespace
+
+extern "C" int dsm_cat_filter(dsm_cat_t* c, int nseries, const double* in, double* out, int on_device) {
+    if (!c) return DSM_ERR_INVALID;
+    return cat_guard(c, [&] {
+        const char* fn = "dsm_cat_filter";
+        need(c->kset, std::string(fn) + ": dsm_cat_set_kernel_params has not been called");
+        need(nseries >= 0 && (nseries == 0 || (in && out)), std::string(fn) + ": null argument");
+        if (on_device)
+            need(((uintptr_t)in % 8) == 0 && ((uintptr_t)out % 8) == 0, std::string(fn) + ": misaligned device pointer");
+        if (nseries == 0) return;
+        const int nwin = c->nwin(), nfl = c->knfl;
+        need((long long)nseries * nfl < (1LL << 30), std::string(fn) + ": too many series");
+        DSM_CUDA(cudaSetDevice(c->dev));
+        const double* din = in;
+        double* dout = out;
+        if (!on_device) {
+            c->kfin.upload(in, (size_t)nseries * nwin, c->st);
+            din = c->kfin.p;
+            c->kfilt.reserve((size_t)nseries * nfl * nwin);
+            dout = c->kfilt.p;
+        }
+        switch (c->knp) {
+            case 1: launch_bwfilt<1>(din, nseries, nfl, nwin, c->kfc.p, dout, c->st); break;
+            case 2: launch_bwfilt<2>(din, nseries, nfl, nwin, c->kfc.p, dout, c->st); break;
+            case 3: launch_bwfilt<3>(din, nseries, nfl, nwin, c->kfc.p, dout, c->st); break;
+            case 4: launch_bwfilt<4>(din, nseries, nfl, nwin, c->kfc.p, dout, c->st); break;
+            case 5: launch_bwfilt<5>(din, nseries, nfl, nwin, c->kfc.p, dout, c->st); break;
+            case 6: launch_bwfilt<6>(din, nseries, nfl, nwin, c->kfc.p, dout, c->st); break;
+            case 7: launch_bwfilt<7>(din, nseries, nfl, nwin, c->kfc.p, dout, c->st); break;
+            case 8: launch_bwfilt<8>(din, nseries, nfl, nwin, c->kfc.p, dout, c->st); break;
+            case 9: launch_bwfilt<9>(din, nseries, nfl, nwin, c->kfc.p, dout, c->st); break;
+            default: launch_bwfilt<10>(din, nseries, nfl, nwin, c->kfc.p, dout, c->st); break;
+        }
+        DSM_CUDA(cudaGetLastError());
+        if (!on_device)
+            DSM_CUDA(cudaMemcpyAsync(out, dout, (size_t)nseries * nfl * nwin * sizeof(double), cudaMemcpyDeviceToHost,
+                                     c->st));
+        DSM_CUDA(cudaStreamSynchronize(c->st));
     });
 }
 

@@ -219,6 +219,7 @@ def lib() -> C.CDLL:
         L.dsm_cat_spectra.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp, C.c_void_p, C.c_int]
         L.dsm_cat_transform.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int]
         L.dsm_cat_h3h4_coef.argtypes = [C.c_int, _dp, C.c_char, _dp, C.c_void_p, C.c_void_p]
+        L.dsm_cat_filter.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
         L.dsm_cat_set_kernel_params.argtypes = [C.c_void_p, C.POINTER(CatKernelParams)]
         L.dsm_cat_kernels.argtypes = [C.c_void_p, C.c_int, _ip, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                       C.c_void_p, C.c_int]
@@ -845,6 +846,17 @@ class Catalogue:
                                    None if filt is None else C.c_void_p(filt.ctypes.data), 0)
         self._check(rc, "dsm_cat_kernels")
         return (ker, filt) if filtered else ker
+
+    def filter(self, series):
+        """The filters set by set_kernel_params applied to window series
+        [..., nwin] (numpy): [..., nfilter+1, nwin] (dsm_cat_filter)."""
+        x = np.ascontiguousarray(series, np.float64)
+        x2 = x.reshape(-1, self.nwin)
+        nfl = self._ker_shape[0]
+        res = np.zeros((x2.shape[0], nfl, self.nwin), np.float64)
+        rc = lib().dsm_cat_filter(self.h, x2.shape[0], C.c_void_p(x2.ctypes.data), C.c_void_p(res.ctypes.data), 0)
+        self._check(rc, "dsm_cat_filter")
+        return res.reshape(x.shape[:-1] + (nfl, self.nwin))
 
     def set_profiling(self, on: bool):
         self._check(lib().dsm_cat_set_profiling(self.h, int(on)), "dsm_cat_set_profiling")

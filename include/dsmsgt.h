@@ -563,6 +563,15 @@ int dsm_cat_set_kernel_params(dsm_cat_t *cat, const dsm_cat_kernel_params_t *kp)
 int dsm_cat_kernels(dsm_cat_t *cat, int npoint, const int *ir, const void *h3, const void *h4,
                     int spectra_on_device, double *ker, double *filtered, int out_on_device);
 
+/* The Butterworth filters of dsm_cat_set_kernel_params (every filter
+ * ift = 0..nfilter, forward recursion of bwfilt, src/KernelMaker/bwfilt.f90)
+ * applied to arbitrary window series: in [nseries][nwin], out
+ * [nseries][nfilter+1][nwin] (device pointers when on_device = 1).  With
+ * dsm_cat_series on the h3 / h4 matrices of dsm_cat_h3h4_coef this is
+ * calculateRSGT / calculateTSGT (src/KernelMaker/calculateK.f90:1-130),
+ * whose video outputs sample the filtered series every jtstep samples. */
+int dsm_cat_filter(dsm_cat_t *cat, int nseries, const double *in, double *out, int on_device);
+
 /* Per-stage device time of the last dsm_cat_series when profiling is on:
  * kern[] holds cat_interp, cat_fft, cat_window (ms, launches, algorithmic
  * bytes); ms_total covers the whole call.  After dsm_cat_kernels: ker_spec

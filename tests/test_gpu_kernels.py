@@ -267,3 +267,54 @@ def test_kernels_without_series_mixed_segment_counts(built):
     assert rel_l2(ker, wk) <= TOL and rel_l2(ker2, wk) <= TOL
     for f in range(4):
         assert rel_l2(ker[:, f], wk[:, f]) <= TOL, f
+
+
+@pytest.mark.gpu
+def test_calculate_rsgt_video_series(built):
+    """calculateRSGT (calculateK.f90:1-64): the RSGT catalogue at each
+    point's receiver distance, the rsgt2h3freq combinations transformed
+    (dsm_cat_series with the dsm_cat_h3h4_coef matrices) and filtered by
+    every filter (dsm_cat_filter); against the oracle's clsgt,
+    rsgt2h3freq, vectorFFT_double and rekurs.  Device pointers give the
+    same values."""
+    import torch
+    from oracle import catalogue as cat
+    rng = np.random.default_rng(77)
+    p = _params(num=10, c_red_reci=3.0)
+    nf = p["fmax"] - p["fmin"] + 1
+    shp = (nf, p["theta_n"], 10)
+    rec = (rng.standard_normal(shp) + 1j * rng.standard_normal(shp)).astype(np.complex64)
+    npt = 5
+    dist = rng.uniform(2.0, 28.0, npt)
+    ph = rng.uniform(0, 2 * np.pi, (npt, 3))
+    ang = np.stack([f(m * ph[:, k]) for k in range(3) for m, f in ((1, np.cos), (1, np.sin), (2, np.cos), (2, np.sin))],
+                   axis=1)
+    c3, _ = dsmsgt.cat_h3h4_coef(ang, "R")
+    c = dsmsgt.Catalogue(p)
+    c.add(rec)
+    kp = _kparams(p, 1, 2, 3, rng, npoles=6)
+    c.set_kernel_params(kp["types"], kp["nfilter"], kp["fclp"], kp["fchp"], kp["npoles"], kp["sampling_hz"],
+                        kp["nt1"], kp["nt2"], kp["coeff"], kp["jacobian"])
+    ser = c.series(dist, c3)                                   # [point][6][nwin]
+    got = c.filter(ser)                                        # [point][6][3][nwin]
+    din = torch.from_numpy(ser).cuda()
+    dout = torch.zeros(got.shape, dtype=torch.float64, device="cuda")
+    rc = dsmsgt.lib().dsm_cat_filter(c.h, npt * 6, din.data_ptr(), dout.data_ptr(), 1)
+    assert rc == 0
+    assert np.array_equal(dout.cpu().numpy(), got)
+    c.close()
+    theta = p["theta_min"] + np.arange(p["theta_n"]) * p["theta_delta"]
+    om = cat.omega_sgt([(rec, np.arange(10), np.ones(10))], 10, p["fmin"], p["fmax"], theta, p["tlen"], 3.0)
+    want = np.empty_like(got)
+    for k in range(npt):
+        fr = cat.clsgt(float(dist[k]), om, p["fmin"], p["theta_min"], p["theta_delta"], p["ipdistance"],
+                       p["tlen"], 3.0)
+        h3 = cat.rsgt2h3freq(fr.T, ang[k], "R")
+        du = cat.vector_fft_double(h3, p["fmin"], p["fmax"], p["np1"], p["omegai"], p["tlen"],
+                                   p["iwin_start"], p["iwin_end"])
+        for f in range(3):
+            a, b1, b2 = cat.bpcoeff(kp["fclp"][f], kp["fchp"][f], 6, 1.0 / kp["sampling_hz"])
+            want[k, :, f] = cat.rekurs(du, a, b1, b2)
+    assert rel_l2(got, want) <= TOL
+    for k in range(npt):
+        assert rel_l2(got[k], want[k]) <= TOL, k
